@@ -1,0 +1,268 @@
+/*
+ * uha_b200.h — C ABI of the B200 query engine for the HNSVW importance-sampling
+ * nearest-neighbour indexes (flat, hierarchical and exact; L1 and L2).
+ *
+ * Plain pointers and sizes only. Every entry point returns a uha_status; on
+ * failure uha_last_error() holds a message for the calling thread. Status codes
+ * map one-to-one onto the C++ exception types the reference API throws, so a
+ * C++ binding can rethrow exactly what the reference would have thrown.
+ *
+ * Each declaration names the reference interface it replaces (paths are
+ * relative to the reference project root).
+ */
+#ifndef UHA_B200_H
+#define UHA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. Reference exception mapping:
+ *   UHA_INVALID_ARGUMENT -> std::invalid_argument (shapes, capacity, foreign
+ *                           workspace, non-finite rows or sampled query values)
+ *   UHA_LENGTH_ERROR     -> std::length_error     (size overflow, grid limits)
+ *   UHA_RUNTIME_ERROR    -> std::runtime_error    (CUDA failure, no device)
+ *   UHA_OVERFLOW_ERROR   -> std::overflow_error   (non-finite projected results)
+ *   UHA_OUT_OF_RANGE     -> std::out_of_range     (sampled column >= dimension)
+ *   UHA_DOMAIN_ERROR     -> std::domain_error     (invalid sampling probability)
+ *   UHA_LOGIC_ERROR      -> std::logic_error
+ * (src/core/cuda_dense_l2_scan_index.cu:26-32 check_cuda; src/core/finite_values.hpp:12-66) */
+typedef enum uha_status {
+    UHA_OK = 0,
+    UHA_INVALID_ARGUMENT = 1,
+    UHA_LENGTH_ERROR = 2,
+    UHA_RUNTIME_ERROR = 3,
+    UHA_OVERFLOW_ERROR = 4,
+    UHA_OUT_OF_RANGE = 5,
+    UHA_DOMAIN_ERROR = 6,
+    UHA_LOGIC_ERROR = 7
+} uha_status;
+
+typedef enum uha_metric {
+    UHA_L2 = 0,
+    UHA_L1 = 1
+} uha_metric;
+
+/* Query strategies. The first two keep the reference enumerator values of
+ * CudaDenseL2QueryStrategy / CudaSampledCoordinateL2QueryStrategy /
+ * CudaHierarchicalL{1,2}QueryStrategy (include/ultrahigh_ann/core/
+ * cuda_dense_l2_scan_index.hpp:17-23).
+ *   UHA_DIRECT: binary32 scan on CUDA cores with a certified error bound per
+ *     distance; queries whose winner is not certified are re-scored by
+ *     replaying the reference CPU's binary64 operation sequence, so the
+ *     returned index equals the reference CPU index on every query.
+ *   UHA_GEMM: the reference's unrefined binary32 norm identity
+ *     ||r||^2 + ||q||^2 - 2 r.q (L2 only; L1 treats it as DIRECT). */
+typedef enum uha_strategy {
+    UHA_DIRECT = 0,
+    UHA_GEMM = 1
+} uha_strategy;
+
+typedef struct uha_index uha_index;
+typedef struct uha_workspace uha_workspace;
+typedef struct uha_rng uha_rng;
+
+/* include/ultrahigh_ann/core/index_space_usage.hpp:9-14 */
+typedef struct uha_space_usage {
+    uint64_t index_payload_bytes;
+    uint64_t query_workspace_payload_bytes;
+    uint64_t unique_query_coordinates;
+    uint64_t sampled_multiplicity;
+} uha_space_usage;
+
+/* include/ultrahigh_ann/core/cuda_runtime_info.hpp:9-18 */
+typedef struct uha_device_info {
+    int device;
+    char device_name[256];
+    int compute_capability_major;
+    int compute_capability_minor;
+    uint64_t total_global_memory_bytes;
+    int compiled_runtime_version;
+    int runtime_version;
+    int driver_version;
+} uha_device_info;
+
+/* Per-query diagnostics of the last uha_query call on a workspace. */
+typedef struct uha_query_stats {
+    uint64_t query_count;
+    uint64_t certified_queries;   /* winner certified by the binary32 bound */
+    uint64_t replayed_queries;    /* winner settled by the binary64 replay */
+    uint64_t kernel_launches;     /* kernels this library launched for the call */
+    double scan_ms;               /* device time of the scan kernel (timing on) */
+    double device_ms;             /* device time from first enqueue to results */
+} uha_query_stats;
+
+/* GPU probability-build report (include/ultrahigh_ann/hnsvw25/l2/
+ * importance_sampling.hpp:23-41, l1/importance_sampling.hpp:22-40). */
+typedef struct uha_probability_report {
+    uint64_t pair_count;
+    uint64_t device_working_set_bytes;
+    double host_to_device_ms;
+    double inverse_distance_ms;
+    double coordinate_maximum_ms;
+    double device_to_host_ms;
+    double total_ms;
+} uha_probability_report;
+
+/* Message of the calling thread's last failed call ("" when none). */
+const char* uha_last_error(void);
+
+/* 1 when a usable CUDA device is visible, else 0.
+ * Replaces cuda_dense_l2_scan_available() and its siblings
+ * (include/ultrahigh_ann/core/cuda_dense_l2_scan_index.hpp:14). */
+int uha_cuda_available(void);
+
+/* Replaces cuda_runtime_info(int) (include/ultrahigh_ann/core/
+ * cuda_runtime_info.hpp:22-23; src/core/cuda_runtime_info.cu:11-38).
+ * UHA_RUNTIME_ERROR when the device is not usable. */
+uha_status uha_device_info_get(int device, uha_device_info* out);
+
+/* ---------------------------------------------------------------- indexes */
+
+/* Exact (full-coordinate) scan over an r x d row-major float matrix.
+ * Replaces CudaDenseL2ScanIndex(const DenseMatrix&, int)
+ * (include/ultrahigh_ann/core/cuda_dense_l2_scan_index.hpp:47-48),
+ * CudaDenseL1ScanIndex(const DenseMatrix&, int)
+ * (include/ultrahigh_ann/core/cuda_dense_l1_scan_index.hpp:39-40) and the
+ * CudaExactL{1,2}Index facades (include/ultrahigh_ann/exact/l2/
+ * cuda_exact_l2_index.hpp:27-28, exact/l1/cuda_exact_l1_index.hpp:25-26).
+ * The rows are copied; the caller keeps ownership of `rows`. */
+uha_status uha_exact_index_create(int device, uha_metric metric,
+                                  const float* rows, uint64_t row_count,
+                                  uint64_t dimension, uha_index** out);
+
+/* Weighted L1 scan sum_j w_j |r_j - q_j| with binary32 weights.
+ * Replaces CudaDenseL1ScanIndex(const DenseMatrix&, std::span<const float>,
+ * int) (include/ultrahigh_ann/core/cuda_dense_l1_scan_index.hpp:41-43). */
+uha_status uha_weighted_l1_index_create(int device, const float* rows,
+                                        uint64_t row_count, uint64_t dimension,
+                                        const float* weights,
+                                        uha_index** out);
+
+/* Sampled-coordinate (flat) index from a coordinate sample
+ * {columns[i], multiplicities[i], inverse_probabilities[i]}, i < k, kept in
+ * ascending column order. The embedding (L2: rows scaled by
+ * float(sqrt(mult * inv_p)); L1: unscaled rows and weights mult * inv_p) is
+ * built on the device. Replaces CudaSampledCoordinateL{1,2}AnnIndex(
+ * const DenseMatrix&, CoordinateSample, int)
+ * (include/ultrahigh_ann/coordinate_sampling/cuda_sampled_coordinate_l2_ann_index.hpp:54-56,
+ *  cuda_sampled_coordinate_l1_ann_index.hpp:48-50). */
+uha_status uha_sampled_index_create(int device, uha_metric metric,
+                                    const float* rows, uint64_t row_count,
+                                    uint64_t dimension,
+                                    const uint64_t* columns,
+                                    const uint64_t* multiplicities,
+                                    const double* inverse_probabilities,
+                                    uint64_t sample_size, uha_index** out);
+
+void uha_index_destroy(uha_index* index);
+
+/* Replaces space_usage() of every CUDA index class, with the reference byte
+ * formulas (e.g. include/ultrahigh_ann/core/cuda_dense_l2_scan_index.hpp:85). */
+uha_status uha_index_space_usage(const uha_index* index, uha_space_usage* out);
+
+/* device() / device_name() of every CUDA index class. */
+uha_status uha_index_device(const uha_index* index, int* device,
+                            char* name, uint64_t name_capacity);
+
+/* --------------------------------------------------------------- queries */
+
+/* Replaces make_query_workspace(std::size_t) (e.g. include/ultrahigh_ann/
+ * core/cuda_dense_l2_scan_index.hpp:56-57). A workspace belongs to one index
+ * and one caller thread; it owns a CUDA stream and its scratch buffers. */
+uha_status uha_workspace_create(const uha_index* index,
+                                uint64_t maximum_batch_size,
+                                uha_workspace** out);
+void uha_workspace_destroy(uha_workspace* workspace);
+
+/* maximum_batch_size() and payload_bytes() (the reference's logical payload
+ * formula, e.g. tests/exact/l2/cuda_exact_l2_index_test.cpp:96-108). */
+uha_status uha_workspace_info(const uha_workspace* workspace,
+                              uint64_t* maximum_batch_size,
+                              uint64_t* payload_bytes);
+
+/* Answer query_count queries, a row-major query_count x dimension float
+ * matrix in ORIGINAL coordinates. queries_on_device != 0 means `queries` is a
+ * device pointer on the index's device (query_device_batch,
+ * include/ultrahigh_ann/core/cuda_dense_l2_scan_index.hpp:73-79); otherwise it
+ * is host memory and the host-to-device copy is part of the call
+ * (query_batch, e.g. cuda_dense_l2_scan_index.hpp:62-66 and
+ * coordinate_sampling/cuda_sampled_coordinate_l2_ann_index.hpp:70-82).
+ * out_indices (host, query_count entries) receives the row index per query;
+ * out_distances (host, nullable) the distance that selected it (squared L2,
+ * L1 or median |diff|). Only sampled coordinates are read or validated. */
+uha_status uha_query(const uha_index* index, uha_workspace* workspace,
+                     const float* queries, uint64_t query_count,
+                     int queries_on_device, uha_strategy strategy,
+                     uint64_t* out_indices, double* out_distances);
+
+/* Diagnostics of the last uha_query on this workspace. */
+uha_status uha_workspace_last_stats(const uha_workspace* workspace,
+                                    uha_query_stats* out);
+
+/* With enabled != 0, every uha_query on this workspace records CUDA events on
+ * the workspace stream around the scan kernel and around the whole device
+ * pipeline, reported in uha_query_stats.scan_ms / device_ms. */
+uha_status uha_workspace_set_timing(uha_workspace* workspace, int enabled);
+
+/* ---------------------------------------------------------- index build */
+
+/* Importance probabilities on the device. L2: p_j = max over row pairs of
+ * min(1, (a_j-b_j)^2 / ||a-b||^2); L1: p_j = max over pairs of
+ * |a_j-b_j| / ||a-b||_1; pairs at distance zero are skipped. Pair distances
+ * and the normalisation are binary64. Replaces
+ * compute_l2_importance_probabilities_gpu (include/ultrahigh_ann/hnsvw25/l2/
+ * importance_sampling.hpp:49-52) and compute_l1_importance_probabilities_gpu
+ * (include/ultrahigh_ann/hnsvw25/l1/importance_sampling.hpp:45-48). */
+uha_status uha_importance_probabilities(int device, uha_metric metric,
+                                        const float* rows, uint64_t row_count,
+                                        uint64_t dimension,
+                                        double* out_probabilities,
+                                        uha_probability_report* report);
+
+/* std::mt19937_64 engine shared by the host-side draws below, so that one
+ * engine passes through sampling and projection in the reference order. */
+uha_status uha_rng_create(uint64_t seed, uha_rng** out);
+void uha_rng_destroy(uha_rng* rng);
+/* Textual engine state (operator<< of std::mt19937_64). *length receives the
+ * size needed including the terminating zero. */
+uha_status uha_rng_state(const uha_rng* rng, char* buffer, uint64_t capacity,
+                         uint64_t* length);
+uha_status uha_rng_set_state(uha_rng* rng, const char* state);
+
+/* Coordinate sample: for each j with p_j > 0, multiplicity ~ Binomial(
+ * repetitions, p_j); kept when positive, in ascending j. Same engine draws as
+ * build_coordinate_sample (include/ultrahigh_ann/coordinate_sampling/
+ * coordinate_sampling.hpp:13-16). Outputs need room for `dimension` entries;
+ * *sample_size receives k. */
+uha_status uha_sample_coordinates(const double* probabilities,
+                                  uint64_t dimension, uint64_t repetitions,
+                                  uha_rng* rng, uint64_t* columns,
+                                  uint64_t* multiplicities,
+                                  double* inverse_probabilities,
+                                  uint64_t* sample_size);
+
+/* Row-major p x k Rademacher-JL matrix (aggregated signs per sampled column)
+ * in the reference's draw order (src/hnsvw25/l2/hierarchical/
+ * l2_hierarchical_projection.cpp:53-77). */
+uha_status uha_jl_matrix(const uint64_t* multiplicities,
+                         const double* inverse_probabilities,
+                         uint64_t sample_size, uint64_t projection_dimension,
+                         uha_rng* rng, double* out);
+
+/* Row-major p x k Cauchy matrix in the reference's draw order
+ * (src/hnsvw25/l1/hierarchical/l1_hierarchical_projection.cpp:54-77). */
+uha_status uha_cauchy_matrix(const uint64_t* multiplicities,
+                             const double* inverse_probabilities,
+                             uint64_t sample_size,
+                             uint64_t projection_dimension, uha_rng* rng,
+                             double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* UHA_B200_H */

@@ -1,0 +1,304 @@
+// ORACLE — test infrastructure only. A C wrapper over the reference's own CPU
+// classes, compiled by oracle/Makefile against the reference's headers and
+// linked with its CPU sources into oracle/_ref/libref.so. Tests use it to pin
+// the oracle restatement (oracle/uha_oracle.cpp) and the engine; bench.py's
+// reference arm times it on the host cores. Nothing here runs on a GPU.
+#include "ultrahigh_ann/coordinate_sampling/coordinate_sampling.hpp"
+#include "ultrahigh_ann/coordinate_sampling/sampled_coordinate_l1_ann_index.hpp"
+#include "ultrahigh_ann/coordinate_sampling/sampled_coordinate_l2_ann_index.hpp"
+#include "ultrahigh_ann/core/dense_l2_scan_index.hpp"
+#include "ultrahigh_ann/exact/l1/exact_l1_index.hpp"
+#include "ultrahigh_ann/exact/l2/exact_l2_index.hpp"
+#include "ultrahigh_ann/hnsvw25/l1/hierarchical/hierarchical_l1_ann_index.hpp"
+#include "ultrahigh_ann/hnsvw25/l1/importance_sampling.hpp"
+#include "ultrahigh_ann/hnsvw25/l2/hierarchical/hierarchical_l2_ann_index.hpp"
+#include "ultrahigh_ann/hnsvw25/l2/importance_sampling.hpp"
+#include "hnsvw25/l1/hierarchical/l1_hierarchical_projection.hpp"
+#include "hnsvw25/l2/hierarchical/l2_hierarchical_projection.hpp"
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <mutex>
+#include <random>
+#include <span>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+using namespace ultrahigh_ann;
+
+namespace {
+
+thread_local std::string g_error;
+
+// 0 ok; 1 invalid_argument; 2 length_error; 3 runtime_error;
+// 4 overflow_error; 5 out_of_range; 6 domain_error; 7 other
+template <typename F>
+int guarded(F&& f)
+{
+    try {
+        f();
+        return 0;
+    } catch (const std::invalid_argument& e) {
+        g_error = e.what();
+        return 1;
+    } catch (const std::length_error& e) {
+        g_error = e.what();
+        return 2;
+    } catch (const std::overflow_error& e) {
+        g_error = e.what();
+        return 4;
+    } catch (const std::out_of_range& e) {
+        g_error = e.what();
+        return 5;
+    } catch (const std::domain_error& e) {
+        g_error = e.what();
+        return 6;
+    } catch (const std::runtime_error& e) {
+        g_error = e.what();
+        return 3;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return 7;
+    }
+}
+
+DenseMatrix matrix(const float* v, uint64_t r, uint64_t d)
+{
+    return DenseMatrix(std::vector<float>(v, v + r * d), r, d);
+}
+
+CoordinateSample sample_of(const uint64_t* cols, const uint64_t* mult,
+                           const double* invp, uint64_t k)
+{
+    CoordinateSample s;
+    for (uint64_t i = 0; i < k; ++i) {
+        s.columns.push_back(SampledColumn{cols[i], mult[i], invp[i]});
+    }
+    return s;
+}
+
+// Runs body(begin, end) over [0, n) on `threads` std::threads.
+template <typename F>
+void split(uint64_t n, int threads, F body)
+{
+    threads = std::max(1, threads);
+    std::vector<std::thread> pool;
+    std::exception_ptr error;
+    std::mutex m;
+    const uint64_t per = (n + threads - 1) / threads;
+    for (int t = 0; t < threads; ++t) {
+        const uint64_t b = std::min(n, t * per);
+        const uint64_t e = std::min(n, b + per);
+        if (b >= e) {
+            break;
+        }
+        pool.emplace_back([&, b, e] {
+            try {
+                body(b, e);
+            } catch (...) {
+                std::lock_guard<std::mutex> g(m);
+                error = std::current_exception();
+            }
+        });
+    }
+    for (auto& th : pool) {
+        th.join();
+    }
+    if (error) {
+        std::rethrow_exception(error);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ref_last_error(void)
+{
+    return g_error.c_str();
+}
+
+// build_coordinate_sample; engine state after sampling is written to state_out.
+int ref_sample(const double* probs, uint64_t d, uint64_t repetitions,
+               uint64_t seed, uint64_t* cols, uint64_t* mult, double* invp,
+               uint64_t* k, char* state_out, uint64_t state_capacity)
+{
+    return guarded([&] {
+        std::mt19937_64 engine(seed);
+        const CoordinateSample s = build_coordinate_sample(
+            std::span<const double>(probs, d), repetitions, engine);
+        *k = s.columns.size();
+        for (uint64_t i = 0; i < s.columns.size(); ++i) {
+            cols[i] = s.columns[i].source_column;
+            mult[i] = s.columns[i].multiplicity;
+            invp[i] = s.columns[i].inverse_probability;
+        }
+        if (state_out != nullptr) {
+            std::ostringstream os;
+            os << engine;
+            const std::string st = os.str();
+            if (st.size() + 1 <= state_capacity) {
+                std::memcpy(state_out, st.c_str(), st.size() + 1);
+            }
+        }
+    });
+}
+
+// policy: 0 sequential, 1 cpu_parallel
+int ref_probabilities(int metric, const float* rows, uint64_t r, uint64_t d,
+                      int policy, double* out)
+{
+    return guarded([&] {
+        const DenseMatrix m = matrix(rows, r, d);
+        const ExecutionPolicy p =
+            policy == 0 ? ExecutionPolicy::sequential : ExecutionPolicy::cpu_parallel;
+        const std::vector<double> v = metric == 0
+                                          ? compute_l2_importance_probabilities(m, p)
+                                          : compute_l1_importance_probabilities(m, p);
+        std::copy(v.begin(), v.end(), out);
+    });
+}
+
+// ExactL2Index::query_batch; strategy: 0 sequential, 1 parallel_queries
+int ref_exact_l2(const float* rows, uint64_t r, uint64_t d,
+                 const float* queries, uint64_t n, int strategy, uint64_t* out)
+{
+    return guarded([&] {
+        const DenseMatrix m = matrix(rows, r, d);
+        const ExactL2Index index(m);
+        std::vector<std::size_t> o(n);
+        index.query_batch(std::span<const float>(queries, n * d), n, o,
+                          strategy == 0 ? CpuDenseL2QueryStrategy::sequential
+                                        : CpuDenseL2QueryStrategy::parallel_queries);
+        std::copy(o.begin(), o.end(), out);
+    });
+}
+
+// ExactL1Index::query from `threads` threads over disjoint query ranges
+int ref_exact_l1(const float* rows, uint64_t r, uint64_t d,
+                 const float* queries, uint64_t n, int threads, uint64_t* out)
+{
+    return guarded([&] {
+        const DenseMatrix m = matrix(rows, r, d);
+        const ExactL1Index index(m);
+        split(n, threads, [&](uint64_t b, uint64_t e) {
+            for (uint64_t q = b; q < e; ++q) {
+                out[q] = index.query(std::span<const float>(queries + q * d, d));
+            }
+        });
+    });
+}
+
+// SampledCoordinateL2AnnIndex(input, CoordinateSample)::query_batch
+int ref_sampled_l2(const float* rows, uint64_t r, uint64_t d,
+                   const uint64_t* cols, const uint64_t* mult,
+                   const double* invp, uint64_t k, const float* queries,
+                   uint64_t n, int strategy, uint64_t* out)
+{
+    return guarded([&] {
+        const DenseMatrix m = matrix(rows, r, d);
+        const SampledCoordinateL2AnnIndex index(m, sample_of(cols, mult, invp, k));
+        std::vector<std::size_t> o(n);
+        index.query_batch(std::span<const float>(queries, n * d), n, o,
+                          strategy == 0 ? CpuDenseL2QueryStrategy::sequential
+                                        : CpuDenseL2QueryStrategy::parallel_queries);
+        std::copy(o.begin(), o.end(), out);
+    });
+}
+
+// SampledCoordinateL1AnnIndex(input, CoordinateSample)::query on threads
+int ref_sampled_l1(const float* rows, uint64_t r, uint64_t d,
+                   const uint64_t* cols, const uint64_t* mult,
+                   const double* invp, uint64_t k, const float* queries,
+                   uint64_t n, int threads, uint64_t* out)
+{
+    return guarded([&] {
+        const DenseMatrix m = matrix(rows, r, d);
+        const SampledCoordinateL1AnnIndex index(m, sample_of(cols, mult, invp, k));
+        split(n, threads, [&](uint64_t b, uint64_t e) {
+            for (uint64_t q = b; q < e; ++q) {
+                out[q] = index.query(std::span<const float>(queries + q * d, d));
+            }
+        });
+    });
+}
+
+// Hierarchical{L2,L1}AnnIndex(input, probabilities, repetitions, p, engine)
+// seeded with `seed`; queries answered with query() on `threads` threads.
+// The engine state after construction is written to state_out.
+int ref_hierarchical(int metric, const float* rows, uint64_t r, uint64_t d,
+                     const double* probs, uint64_t repetitions, uint64_t p,
+                     uint64_t seed, const float* queries, uint64_t n,
+                     int threads, uint64_t* out, char* state_out,
+                     uint64_t state_capacity)
+{
+    return guarded([&] {
+        const DenseMatrix m = matrix(rows, r, d);
+        std::mt19937_64 engine(seed);
+        const std::span<const double> pr(probs, d);
+        auto run = [&](const auto& index) {
+            split(n, threads, [&](uint64_t b, uint64_t e) {
+                auto ws = index.make_query_workspace();
+                for (uint64_t q = b; q < e; ++q) {
+                    out[q] =
+                        index.query(std::span<const float>(queries + q * d, d), ws);
+                }
+            });
+        };
+        if (metric == 0) {
+            const HierarchicalL2AnnIndex index(m, pr, repetitions, p, engine);
+            run(index);
+        } else {
+            const HierarchicalL1AnnIndex index(m, pr, repetitions, p, engine);
+            run(index);
+        }
+        if (state_out != nullptr) {
+            std::ostringstream os;
+            os << engine;
+            const std::string st = os.str();
+            if (st.size() + 1 <= state_capacity) {
+                std::memcpy(state_out, st.c_str(), st.size() + 1);
+            }
+        }
+    });
+}
+
+// detail::build_l{2,1}_hierarchical_projection: the binary64 projection matrix
+// (p x k) and projected representatives (r x p).
+int ref_projection(int metric, const float* rows, uint64_t r, uint64_t d,
+                   const uint64_t* cols, const uint64_t* mult,
+                   const double* invp, uint64_t k, uint64_t p,
+                   const char* state, uint64_t seed, double* matrix_out,
+                   double* reps_out)
+{
+    return guarded([&] {
+        const DenseMatrix m = matrix(rows, r, d);
+        std::mt19937_64 engine(seed);
+        if (state != nullptr) {
+            std::istringstream is{std::string(state)};
+            is >> engine;
+        }
+        if (metric == 0) {
+            auto proj = detail::build_l2_hierarchical_projection(
+                m, sample_of(cols, mult, invp, k), p, engine);
+            std::copy(proj.jl_matrix.values().begin(), proj.jl_matrix.values().end(),
+                      matrix_out);
+            std::copy(proj.projected_representatives.values().begin(),
+                      proj.projected_representatives.values().end(), reps_out);
+        } else {
+            auto proj = detail::build_l1_hierarchical_projection(
+                m, sample_of(cols, mult, invp, k), p, engine);
+            std::copy(proj.cauchy_matrix.values().begin(),
+                      proj.cauchy_matrix.values().end(), matrix_out);
+            std::copy(proj.projected_representatives.values().begin(),
+                      proj.projected_representatives.values().end(), reps_out);
+        }
+    });
+}
+
+}  // extern "C"

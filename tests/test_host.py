@@ -1,0 +1,117 @@
+"""Host-side logic of the engine that needs no GPU: the C-ABI library loads
+and exports every entry point include/uha_b200.h declares, the host sampler
+and projection draws reproduce the reference's (same engine, same
+distributions, same order), and errors map onto the reference's exception
+types."""
+from __future__ import annotations
+
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import ultrahigh_ann_b200 as uha
+from conftest import ROOT, engine_state, golden, golden_inputs
+from ultrahigh_ann_b200 import _abi
+
+
+def declared_functions() -> set[str]:
+    names = set()
+    for header in (ROOT / "include").glob("*.h"):
+        text = header.read_text()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"\b(uha_[a-z0-9_]+)\s*\(", text))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _abi.load()
+    declared = declared_functions()
+    assert declared, "no declarations found"
+    for name in sorted(declared):
+        assert hasattr(lib, name), f"{name} declared but not exported"
+    assert declared == set(_abi.SIGNATURES), "ctypes table and header differ"
+
+
+def test_library_is_built_for_sm100a():
+    data = _abi.LIBRARY_PATH.read_bytes()
+    assert b"sm_100a" in data
+
+
+def test_no_device_is_reported_as_runtime_error_or_none():
+    if uha.cuda_available():
+        pytest.skip("a CUDA device is visible")
+    assert uha.cuda_runtime_info() is None
+    with pytest.raises(uha.CudaRuntimeError):
+        uha.CudaExactL2Index(np.zeros((3, 2), np.float32))
+
+
+@pytest.mark.parametrize("name", ["flat_l2_t8", "flat_l1_t8", "flat_l2_t32"])
+def test_host_sampler_reproduces_reference_sample(name):
+    g = golden(name)
+    rng = uha.MT19937_64(int(g["seed"]))
+    sample = uha.build_coordinate_sample(g["probabilities"], int(g["repetitions"]), rng)
+    assert np.array_equal(sample.source_columns, g["columns"])
+    assert np.array_equal(sample.multiplicities, g["multiplicities"])
+    assert np.array_equal(sample.inverse_probabilities, g["inverse_probabilities"])
+    assert rng.state() == engine_state(g["engine_state"])
+
+
+@pytest.mark.parametrize("name", ["hier_l2_p16", "hier_l2_p15", "hier_l1_p16",
+                                  "hier_l1_p15"])
+def test_host_projection_draws_reproduce_reference(name):
+    g = golden(name)
+    rng = uha.MT19937_64(int(g["seed"]))
+    sample = uha.build_coordinate_sample(g["probabilities"], int(g["repetitions"]), rng)
+    p = int(g["projection_dimension"])
+    draw = uha.build_jl_matrix if "l2" in name else uha.build_cauchy_matrix
+    matrix = draw(sample, p, rng)
+    assert np.array_equal(matrix, g["projection"])
+    # one engine through sampling and projection, as the reference constructor
+    assert rng.state() == engine_state(g["engine_state_after"])
+
+
+def test_sampler_rejects_invalid_probabilities_as_domain_error():
+    rng = uha.MT19937_64(1)
+    with pytest.raises(uha.DomainError):
+        uha.build_coordinate_sample(np.array([0.5, 1.5]), 4, rng)
+    with pytest.raises(uha.DomainError):
+        uha.build_coordinate_sample(np.array([np.nan]), 4, rng)
+    with pytest.raises(uha.DomainError):
+        uha.build_coordinate_sample(np.array([-0.1]), 4, rng)
+
+
+def test_sampler_edge_cases():
+    rng = uha.MT19937_64(1234)
+    # p = 1 -> multiplicity T and 1/p = 1 (tests/hnsvw25/l2/importance_sampling_test.cpp:290-319)
+    s = uha.build_coordinate_sample(np.array([1.0, 0.0, 1.0]), 7, rng)
+    assert list(s.source_columns) == [0, 2]
+    assert list(s.multiplicities) == [7, 7]
+    assert list(s.inverse_probabilities) == [1.0, 1.0]
+    # zero repetitions or all-zero probabilities -> empty sample
+    assert len(uha.build_coordinate_sample(np.array([0.5, 0.5]), 0, rng)) == 0
+    assert len(uha.build_coordinate_sample(np.zeros(10), 8, rng)) == 0
+    assert len(uha.build_coordinate_sample(np.zeros(0), 8, rng)) == 0
+
+
+def test_engine_state_roundtrip():
+    a = uha.MT19937_64(77)
+    uha.build_coordinate_sample(np.full(100, 0.3), 5, a)
+    b = uha.MT19937_64(0)
+    b.set_state(a.state())
+    assert a == b
+    with pytest.raises(uha.InvalidArgument):
+        b.set_state("not an engine state")
+
+
+def test_projection_rejects_zero_dimension():
+    s = uha.CoordinateSample([0], [1], [2.0])
+    with pytest.raises(uha.InvalidArgument):
+        uha.build_jl_matrix(s, 0, uha.MT19937_64(1))
+
+
+def test_golden_inputs_are_consistent():
+    rows, queries = golden_inputs()
+    assert rows.dtype == np.float32 and queries.dtype == np.float32
+    assert rows.shape[1] == queries.shape[1]

@@ -1,0 +1,124 @@
+"""ctypes declarations of the C ABI in include/uha_b200.h.
+
+The shared library is built in-tree (ultrahigh_ann_b200/libuha_b200.so). There
+is no fallback: when the library is missing or fails to load, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import (POINTER, c_char, c_char_p, c_double, c_int, c_uint64,
+                    c_void_p)
+from pathlib import Path
+
+LIBRARY_PATH = Path(__file__).resolve().parent / "libuha_b200.so"
+
+# uha_status
+OK = 0
+INVALID_ARGUMENT = 1
+LENGTH_ERROR = 2
+RUNTIME_ERROR = 3
+OVERFLOW_ERROR = 4
+OUT_OF_RANGE = 5
+DOMAIN_ERROR = 6
+LOGIC_ERROR = 7
+
+# uha_metric
+L2 = 0
+L1 = 1
+
+# uha_strategy
+DIRECT = 0
+GEMM = 1
+
+
+class SpaceUsage(ctypes.Structure):
+    _fields_ = [("index_payload_bytes", c_uint64),
+                ("query_workspace_payload_bytes", c_uint64),
+                ("unique_query_coordinates", c_uint64),
+                ("sampled_multiplicity", c_uint64)]
+
+
+class DeviceInfo(ctypes.Structure):
+    _fields_ = [("device", c_int),
+                ("device_name", c_char * 256),
+                ("compute_capability_major", c_int),
+                ("compute_capability_minor", c_int),
+                ("total_global_memory_bytes", c_uint64),
+                ("compiled_runtime_version", c_int),
+                ("runtime_version", c_int),
+                ("driver_version", c_int)]
+
+
+class QueryStats(ctypes.Structure):
+    _fields_ = [("query_count", c_uint64),
+                ("certified_queries", c_uint64),
+                ("replayed_queries", c_uint64),
+                ("kernel_launches", c_uint64),
+                ("scan_ms", c_double),
+                ("device_ms", c_double)]
+
+
+class ProbabilityReport(ctypes.Structure):
+    _fields_ = [("pair_count", c_uint64),
+                ("device_working_set_bytes", c_uint64),
+                ("host_to_device_ms", c_double),
+                ("inverse_distance_ms", c_double),
+                ("coordinate_maximum_ms", c_double),
+                ("device_to_host_ms", c_double),
+                ("total_ms", c_double)]
+
+
+_F = POINTER(ctypes.c_float)
+_D = POINTER(c_double)
+_U = POINTER(c_uint64)
+_H = POINTER(c_void_p)
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "uha_last_error": (c_char_p, []),
+    "uha_cuda_available": (c_int, []),
+    "uha_device_info_get": (c_int, [c_int, POINTER(DeviceInfo)]),
+    "uha_exact_index_create": (c_int, [c_int, c_int, c_void_p, c_uint64, c_uint64, _H]),
+    "uha_weighted_l1_index_create": (c_int, [c_int, c_void_p, c_uint64, c_uint64, c_void_p, _H]),
+    "uha_sampled_index_create": (c_int, [c_int, c_int, c_void_p, c_uint64, c_uint64,
+                                          c_void_p, c_void_p, c_void_p, c_uint64, _H]),
+    "uha_index_destroy": (None, [c_void_p]),
+    "uha_index_space_usage": (c_int, [c_void_p, POINTER(SpaceUsage)]),
+    "uha_index_device": (c_int, [c_void_p, POINTER(c_int), c_char_p, c_uint64]),
+    "uha_workspace_create": (c_int, [c_void_p, c_uint64, _H]),
+    "uha_workspace_destroy": (None, [c_void_p]),
+    "uha_workspace_info": (c_int, [c_void_p, _U, _U]),
+    "uha_query": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_int, c_int,
+                          c_void_p, c_void_p]),
+    "uha_workspace_last_stats": (c_int, [c_void_p, POINTER(QueryStats)]),
+    "uha_workspace_set_timing": (c_int, [c_void_p, c_int]),
+    "uha_importance_probabilities": (c_int, [c_int, c_int, c_void_p, c_uint64, c_uint64,
+                                              c_void_p, POINTER(ProbabilityReport)]),
+    "uha_rng_create": (c_int, [c_uint64, _H]),
+    "uha_rng_destroy": (None, [c_void_p]),
+    "uha_rng_state": (c_int, [c_void_p, c_char_p, c_uint64, _U]),
+    "uha_rng_set_state": (c_int, [c_void_p, c_char_p]),
+    "uha_sample_coordinates": (c_int, [c_void_p, c_uint64, c_uint64, c_void_p,
+                                        c_void_p, c_void_p, c_void_p, _U]),
+    "uha_jl_matrix": (c_int, [c_void_p, c_void_p, c_uint64, c_uint64, c_void_p, c_void_p]),
+    "uha_cauchy_matrix": (c_int, [c_void_p, c_void_p, c_uint64, c_uint64, c_void_p, c_void_p]),
+}
+
+_lib: ctypes.CDLL | None = None
+
+
+def load() -> ctypes.CDLL:
+    """Loads the engine library once; raises if it is absent."""
+    global _lib
+    if _lib is None:
+        if not LIBRARY_PATH.exists():
+            raise RuntimeError(
+                f"CUDA engine library {LIBRARY_PATH} is missing; build it with "
+                "`python -c 'import __graft_entry__ as g; g.build()'`")
+        lib = ctypes.CDLL(str(LIBRARY_PATH))
+        for name, (restype, argtypes) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = restype
+            fn.argtypes = argtypes
+        _lib = lib
+    return _lib

@@ -1,0 +1,584 @@
+"""Python mirror of the reference's CUDA index API over the engine's C ABI.
+
+Class and method names, argument meaning and error types follow the
+reference's C++ headers under include/ultrahigh_ann/ (for example
+core/cuda_dense_l2_scan_index.hpp, coordinate_sampling/
+cuda_sampled_coordinate_l2_ann_index.hpp, hnsvw25/l2/flat/cuda_l2_ann_index.hpp,
+hnsvw25/l2/hierarchical/cuda_hierarchical_l2_ann_index.hpp). C++ exception
+types map onto Python exceptions:
+
+    std::invalid_argument -> InvalidArgument     std::length_error -> LengthError
+    std::runtime_error    -> CudaRuntimeError    std::overflow_error -> ResultOverflowError
+    std::out_of_range     -> OutOfRange          std::domain_error -> DomainError
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import _abi
+
+
+class InvalidArgument(ValueError):
+    """std::invalid_argument."""
+
+
+class LengthError(ValueError):
+    """std::length_error."""
+
+
+class CudaRuntimeError(RuntimeError):
+    """std::runtime_error (CUDA failure or no usable device)."""
+
+
+class ResultOverflowError(OverflowError):
+    """std::overflow_error (non-finite projected or median results)."""
+
+
+class OutOfRange(IndexError):
+    """std::out_of_range."""
+
+
+class DomainError(ValueError):
+    """std::domain_error."""
+
+
+class LogicError(RuntimeError):
+    """std::logic_error."""
+
+
+_ERRORS = {
+    _abi.INVALID_ARGUMENT: InvalidArgument,
+    _abi.LENGTH_ERROR: LengthError,
+    _abi.RUNTIME_ERROR: CudaRuntimeError,
+    _abi.OVERFLOW_ERROR: ResultOverflowError,
+    _abi.OUT_OF_RANGE: OutOfRange,
+    _abi.DOMAIN_ERROR: DomainError,
+    _abi.LOGIC_ERROR: LogicError,
+}
+
+
+def _check(status: int) -> None:
+    if status != _abi.OK:
+        message = _abi.load().uha_last_error().decode(errors="replace")
+        raise _ERRORS.get(status, CudaRuntimeError)(message)
+
+
+def _ptr(array: np.ndarray) -> ctypes.c_void_p:
+    return ctypes.c_void_p(array.ctypes.data) if array.size else ctypes.c_void_p(0)
+
+
+class QueryStrategy(enum.IntEnum):
+    """CudaDenseL2QueryStrategy and siblings
+    (include/ultrahigh_ann/core/cuda_dense_l2_scan_index.hpp:17-23)."""
+
+    direct = _abi.DIRECT
+    gemm = _abi.GEMM
+
+
+CudaDenseL2QueryStrategy = QueryStrategy
+CudaExactL2QueryStrategy = QueryStrategy
+CudaSampledCoordinateL2QueryStrategy = QueryStrategy
+CudaHierarchicalL2QueryStrategy = QueryStrategy
+CudaHierarchicalL1QueryStrategy = QueryStrategy
+
+
+class ExecutionPolicy(enum.Enum):
+    """include/ultrahigh_ann/hnsvw25/execution_policy.hpp:7-12. The engine
+    builds probabilities on the device for the gpu policies."""
+
+    sequential = "sequential"
+    cpu_parallel = "cpu_parallel"
+    gpu_fp32 = "gpu_fp32"
+    gpu_cublas_fp32 = "gpu_cublas_fp32"
+
+
+@dataclass(frozen=True)
+class IndexSpaceUsage:
+    """include/ultrahigh_ann/core/index_space_usage.hpp:9-14."""
+
+    index_payload_bytes: int
+    query_workspace_payload_bytes: int
+    unique_query_coordinates: int
+    sampled_multiplicity: int
+
+
+@dataclass(frozen=True)
+class CudaRuntimeInfo:
+    """include/ultrahigh_ann/core/cuda_runtime_info.hpp:9-18."""
+
+    device: int
+    device_name: str
+    compute_capability_major: int
+    compute_capability_minor: int
+    total_global_memory_bytes: int
+    compiled_runtime_version: int
+    runtime_version: int
+    driver_version: int
+
+
+def cuda_runtime_info(device: int = 0) -> Optional[CudaRuntimeInfo]:
+    """Device metadata, or None without a usable device
+    (include/ultrahigh_ann/core/cuda_runtime_info.hpp:20-23)."""
+    info = _abi.DeviceInfo()
+    if _abi.load().uha_device_info_get(device, ctypes.byref(info)) != _abi.OK:
+        return None
+    return CudaRuntimeInfo(info.device, info.device_name.decode(),
+                           info.compute_capability_major,
+                           info.compute_capability_minor,
+                           info.total_global_memory_bytes,
+                           info.compiled_runtime_version, info.runtime_version,
+                           info.driver_version)
+
+
+def cuda_available() -> bool:
+    return bool(_abi.load().uha_cuda_available())
+
+
+class MT19937_64:
+    """std::mt19937_64 shared by the host-side draws (sampling, projections).
+    The default seed is the standard's 5489."""
+
+    def __init__(self, seed: int = 5489):
+        handle = ctypes.c_void_p()
+        _check(_abi.load().uha_rng_create(ctypes.c_uint64(seed), ctypes.byref(handle)))
+        self._handle = handle
+
+    def __del__(self):
+        if getattr(self, "_handle", None):
+            _abi.load().uha_rng_destroy(self._handle)
+            self._handle = None
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._handle
+
+    def state(self) -> str:
+        lib = _abi.load()
+        length = ctypes.c_uint64()
+        _check(lib.uha_rng_state(self._handle, None, 0, ctypes.byref(length)))
+        buf = ctypes.create_string_buffer(length.value)
+        _check(lib.uha_rng_state(self._handle, buf, length.value, ctypes.byref(length)))
+        return buf.value.decode()
+
+    def set_state(self, state: str) -> None:
+        _check(_abi.load().uha_rng_set_state(self._handle, state.encode()))
+
+    def __eq__(self, other: object) -> bool:
+        return isinstance(other, MT19937_64) and self.state() == other.state()
+
+
+@dataclass(frozen=True)
+class SampledColumn:
+    """include/ultrahigh_ann/coordinate_sampling/coordinate_sample.hpp:10-14."""
+
+    source_column: int
+    multiplicity: int
+    inverse_probability: float
+
+
+class CoordinateSample:
+    """The multiset I as three parallel arrays in ascending column order
+    (include/ultrahigh_ann/coordinate_sampling/coordinate_sample.hpp:16-18)."""
+
+    def __init__(self, columns=(), multiplicities=(), inverse_probabilities=()):
+        self.source_columns = np.ascontiguousarray(columns, dtype=np.uint64)
+        self.multiplicities = np.ascontiguousarray(multiplicities, dtype=np.uint64)
+        self.inverse_probabilities = np.ascontiguousarray(inverse_probabilities,
+                                                          dtype=np.float64)
+        if not (self.source_columns.shape == self.multiplicities.shape
+                == self.inverse_probabilities.shape):
+            raise InvalidArgument("coordinate sample arrays differ in length")
+
+    @classmethod
+    def from_columns(cls, columns) -> "CoordinateSample":
+        cols = list(columns)
+        return cls([c.source_column for c in cols], [c.multiplicity for c in cols],
+                   [c.inverse_probability for c in cols])
+
+    @property
+    def columns(self) -> list[SampledColumn]:
+        return [SampledColumn(int(c), int(m), float(p)) for c, m, p in
+                zip(self.source_columns, self.multiplicities, self.inverse_probabilities)]
+
+    def __len__(self) -> int:
+        return int(self.source_columns.size)
+
+    def sampled_multiplicity(self) -> int:
+        return int(self.multiplicities.sum())
+
+
+def build_coordinate_sample(probabilities, repetitions: int,
+                            random_engine: MT19937_64) -> CoordinateSample:
+    """include/ultrahigh_ann/coordinate_sampling/coordinate_sampling.hpp:13-16."""
+    p = np.ascontiguousarray(probabilities, dtype=np.float64)
+    d = p.size
+    cols = np.empty(d, dtype=np.uint64)
+    mult = np.empty(d, dtype=np.uint64)
+    inv = np.empty(d, dtype=np.float64)
+    k = ctypes.c_uint64()
+    _check(_abi.load().uha_sample_coordinates(
+        _ptr(p), d, ctypes.c_uint64(repetitions), random_engine.handle,
+        _ptr(cols), _ptr(mult), _ptr(inv), ctypes.byref(k)))
+    n = k.value
+    return CoordinateSample(cols[:n], mult[:n], inv[:n])
+
+
+build_l2_importance_sample = build_coordinate_sample
+build_l1_importance_sample = build_coordinate_sample
+
+
+def build_jl_matrix(sample: CoordinateSample, projection_dimension: int,
+                    random_engine: MT19937_64) -> np.ndarray:
+    """p x k aggregated Rademacher-JL matrix in the reference's draw order
+    (src/hnsvw25/l2/hierarchical/l2_hierarchical_projection.cpp:53-77)."""
+    out = np.empty((projection_dimension, len(sample)), dtype=np.float64)
+    _check(_abi.load().uha_jl_matrix(
+        _ptr(sample.multiplicities), _ptr(sample.inverse_probabilities),
+        len(sample), projection_dimension, random_engine.handle, _ptr(out)))
+    return out
+
+
+def build_cauchy_matrix(sample: CoordinateSample, projection_dimension: int,
+                        random_engine: MT19937_64) -> np.ndarray:
+    """p x k Cauchy matrix in the reference's draw order
+    (src/hnsvw25/l1/hierarchical/l1_hierarchical_projection.cpp:54-77)."""
+    out = np.empty((projection_dimension, len(sample)), dtype=np.float64)
+    _check(_abi.load().uha_cauchy_matrix(
+        _ptr(sample.multiplicities), _ptr(sample.inverse_probabilities),
+        len(sample), projection_dimension, random_engine.handle, _ptr(out)))
+    return out
+
+
+@dataclass
+class ProbabilityResult:
+    """L{1,2}GpuProbabilityResult (include/ultrahigh_ann/hnsvw25/l2/
+    importance_sampling.hpp:31-41)."""
+
+    probabilities: np.ndarray
+    device_name: str
+    device: int
+    pair_count: int
+    device_working_set_bytes: int
+    host_to_device_ms: float
+    inverse_distance_ms: float
+    coordinate_maximum_ms: float
+    device_to_host_ms: float
+    total_ms: float
+
+
+def _matrix(values) -> np.ndarray:
+    m = np.ascontiguousarray(values, dtype=np.float32)
+    if m.ndim != 2:
+        raise InvalidArgument("representative matrix must be two-dimensional")
+    return m
+
+
+def _probabilities_gpu(metric: int, representatives, device: int) -> ProbabilityResult:
+    rows = _matrix(representatives)
+    out = np.zeros(rows.shape[1], dtype=np.float64)
+    rep = _abi.ProbabilityReport()
+    _check(_abi.load().uha_importance_probabilities(
+        device, metric, _ptr(rows), rows.shape[0], rows.shape[1], _ptr(out),
+        ctypes.byref(rep)))
+    info = cuda_runtime_info(device)
+    return ProbabilityResult(out, info.device_name if info else "", device,
+                             rep.pair_count, rep.device_working_set_bytes,
+                             rep.host_to_device_ms, rep.inverse_distance_ms,
+                             rep.coordinate_maximum_ms, rep.device_to_host_ms,
+                             rep.total_ms)
+
+
+def compute_l2_importance_probabilities_gpu(representatives, device: int = 0,
+                                            pair_chunks: int = 128) -> ProbabilityResult:
+    """include/ultrahigh_ann/hnsvw25/l2/importance_sampling.hpp:49-52."""
+    if pair_chunks <= 0:
+        raise InvalidArgument("GPU pair chunk count must be positive")
+    return _probabilities_gpu(_abi.L2, representatives, device)
+
+
+def compute_l1_importance_probabilities_gpu(representatives, device: int = 0,
+                                            pair_chunks: int = 128) -> ProbabilityResult:
+    """include/ultrahigh_ann/hnsvw25/l1/importance_sampling.hpp:45-48."""
+    if pair_chunks <= 0:
+        raise InvalidArgument("GPU pair chunk count must be positive")
+    return _probabilities_gpu(_abi.L1, representatives, device)
+
+
+class QueryWorkspace:
+    """Per-caller device buffers sized for a maximum batch
+    (e.g. include/ultrahigh_ann/core/cuda_dense_l2_scan_index.hpp:28-45)."""
+
+    def __init__(self, index: "_CudaIndex", maximum_batch_size: int):
+        handle = ctypes.c_void_p()
+        if maximum_batch_size < 0:
+            raise InvalidArgument("workspace batch size must be positive")
+        _check(_abi.load().uha_workspace_create(index._handle,
+                                                ctypes.c_uint64(maximum_batch_size),
+                                                ctypes.byref(handle)))
+        self._handle = handle
+        self._index = index  # keeps the index alive while the workspace lives
+
+    def __del__(self):
+        if getattr(self, "_handle", None):
+            _abi.load().uha_workspace_destroy(self._handle)
+            self._handle = None
+
+    def maximum_batch_size(self) -> int:
+        b = ctypes.c_uint64()
+        _check(_abi.load().uha_workspace_info(self._handle, ctypes.byref(b), None))
+        return b.value
+
+    def payload_bytes(self) -> int:
+        p = ctypes.c_uint64()
+        _check(_abi.load().uha_workspace_info(self._handle, None, ctypes.byref(p)))
+        return p.value
+
+    def last_stats(self) -> dict:
+        s = _abi.QueryStats()
+        _check(_abi.load().uha_workspace_last_stats(self._handle, ctypes.byref(s)))
+        return {"query_count": s.query_count, "certified_queries": s.certified_queries,
+                "replayed_queries": s.replayed_queries,
+                "kernel_launches": s.kernel_launches, "scan_ms": s.scan_ms,
+                "device_ms": s.device_ms}
+
+    def set_timing(self, enabled: bool) -> None:
+        """Records CUDA events around the scan kernel and the device pipeline
+        of every query on this workspace (see last_stats())."""
+        _check(_abi.load().uha_workspace_set_timing(self._handle, int(enabled)))
+
+
+class _CudaIndex:
+    _handle: ctypes.c_void_p = None
+    _dimension: int = 0
+
+    def _adopt(self, handle: ctypes.c_void_p, dimension: int) -> None:
+        self._handle = handle
+        self._dimension = dimension
+
+    def __del__(self):
+        if getattr(self, "_handle", None):
+            _abi.load().uha_index_destroy(self._handle)
+            self._handle = None
+
+    @property
+    def dimension(self) -> int:
+        return self._dimension
+
+    def make_query_workspace(self, maximum_batch_size: int) -> QueryWorkspace:
+        return QueryWorkspace(self, maximum_batch_size)
+
+    def _run(self, queries_ptr: int, query_count: int, on_device: bool,
+             output: np.ndarray, workspace: QueryWorkspace, strategy,
+             distances: Optional[np.ndarray]) -> None:
+        if not isinstance(workspace, QueryWorkspace):
+            raise InvalidArgument("CUDA workspace belongs to a different index")
+        dist_ptr = ctypes.c_void_p(distances.ctypes.data) if distances is not None else None
+        _check(_abi.load().uha_query(self._handle, workspace._handle,
+                                     ctypes.c_void_p(queries_ptr),
+                                     ctypes.c_uint64(query_count), int(on_device),
+                                     int(strategy), ctypes.c_void_p(output.ctypes.data),
+                                     dist_ptr))
+
+    def query_batch(self, queries, query_count: int, output,
+                    workspace: QueryWorkspace, strategy=QueryStrategy.direct,
+                    distances: Optional[np.ndarray] = None) -> np.ndarray:
+        """Row-major query_count x dimension host queries; output receives one
+        row index per query (a writable uint64 array of query_count entries,
+        or None to allocate one). Returns the output array."""
+        q = np.ascontiguousarray(queries, dtype=np.float32).reshape(-1)
+        if q.size != query_count * self._dimension:
+            raise InvalidArgument("query batch dimensions do not match index dimension")
+        out = self._output(output, query_count)
+        if distances is not None and (distances.dtype != np.float64
+                                      or distances.size != query_count):
+            raise InvalidArgument("distance output must be float64 of query_count")
+        self._run(q.ctypes.data if q.size else 0, query_count, False, out,
+                  workspace, strategy, distances)
+        return out
+
+    def query_device_batch(self, device_queries: int, query_count: int, output,
+                           workspace: QueryWorkspace, strategy=QueryStrategy.direct,
+                           distances: Optional[np.ndarray] = None) -> np.ndarray:
+        """device_queries is a device pointer (int) to a row-major
+        query_count x dimension float matrix on this index's device."""
+        out = self._output(output, query_count)
+        self._run(int(device_queries), query_count, True, out, workspace, strategy,
+                  distances)
+        return out
+
+    def query(self, query, workspace: QueryWorkspace,
+              strategy=QueryStrategy.direct) -> int:
+        q = np.ascontiguousarray(query, dtype=np.float32).reshape(-1)
+        if q.size != self._dimension:
+            raise InvalidArgument("query dimension does not match index dimension")
+        return int(self.query_batch(q, 1, None, workspace, strategy)[0])
+
+    @staticmethod
+    def _output(output, query_count: int) -> np.ndarray:
+        if output is None:
+            return np.zeros(query_count, dtype=np.uint64)
+        if (not isinstance(output, np.ndarray) or output.dtype != np.uint64
+                or output.size != query_count or not output.flags.c_contiguous):
+            raise InvalidArgument("CUDA output size does not match query count")
+        return output
+
+    def space_usage(self) -> IndexSpaceUsage:
+        u = _abi.SpaceUsage()
+        _check(_abi.load().uha_index_space_usage(self._handle, ctypes.byref(u)))
+        return IndexSpaceUsage(u.index_payload_bytes, u.query_workspace_payload_bytes,
+                               u.unique_query_coordinates, u.sampled_multiplicity)
+
+    def device(self) -> int:
+        d = ctypes.c_int()
+        _check(_abi.load().uha_index_device(self._handle, ctypes.byref(d), None, 0))
+        return d.value
+
+    def device_name(self) -> str:
+        buf = ctypes.create_string_buffer(256)
+        _check(_abi.load().uha_index_device(self._handle, None, buf, 256))
+        return buf.value.decode()
+
+
+class CudaDenseL2ScanIndex(_CudaIndex):
+    """include/ultrahigh_ann/core/cuda_dense_l2_scan_index.hpp:27-91."""
+
+    def __init__(self, representatives, device: int = 0):
+        rows = _matrix(representatives)
+        handle = ctypes.c_void_p()
+        _check(_abi.load().uha_exact_index_create(device, _abi.L2, _ptr(rows),
+                                                  rows.shape[0], rows.shape[1],
+                                                  ctypes.byref(handle)))
+        self._adopt(handle, rows.shape[1])
+
+
+class CudaExactL2Index(CudaDenseL2ScanIndex):
+    """include/ultrahigh_ann/exact/l2/cuda_exact_l2_index.hpp:22-59."""
+
+
+class CudaDenseL1ScanIndex(_CudaIndex):
+    """include/ultrahigh_ann/core/cuda_dense_l1_scan_index.hpp:18-74; the
+    weighted form evaluates sum_j w_j |r_j - q_j|."""
+
+    def __init__(self, representatives, coordinate_weights=None, device: int = 0):
+        rows = _matrix(representatives)
+        handle = ctypes.c_void_p()
+        lib = _abi.load()
+        if coordinate_weights is None:
+            _check(lib.uha_exact_index_create(device, _abi.L1, _ptr(rows),
+                                              rows.shape[0], rows.shape[1],
+                                              ctypes.byref(handle)))
+        else:
+            w = np.ascontiguousarray(coordinate_weights, dtype=np.float32).reshape(-1)
+            if w.size != rows.shape[1]:
+                raise InvalidArgument("coordinate weight dimension does not match")
+            _check(lib.uha_weighted_l1_index_create(device, _ptr(rows), rows.shape[0],
+                                                    rows.shape[1], _ptr(w),
+                                                    ctypes.byref(handle)))
+        self._adopt(handle, rows.shape[1])
+
+    def query_batch(self, queries, query_count, output, workspace,
+                    strategy=QueryStrategy.direct, distances=None):
+        return super().query_batch(queries, query_count, output, workspace,
+                                   QueryStrategy.direct, distances)
+
+
+class CudaExactL1Index(CudaDenseL1ScanIndex):
+    """include/ultrahigh_ann/exact/l1/cuda_exact_l1_index.hpp:20-54."""
+
+    def __init__(self, representatives, device: int = 0):
+        super().__init__(representatives, None, device)
+
+
+def _resolve_sample(input_rows: np.ndarray, probabilities, repetitions,
+                    random_engine, coordinate_sample) -> CoordinateSample:
+    if coordinate_sample is not None:
+        if isinstance(coordinate_sample, CoordinateSample):
+            return coordinate_sample
+        return CoordinateSample.from_columns(coordinate_sample)
+    p = np.ascontiguousarray(probabilities, dtype=np.float64)
+    if p.size != input_rows.shape[1]:
+        raise InvalidArgument("sampling probability dimension does not match input")
+    return build_coordinate_sample(p, repetitions, random_engine)
+
+
+class _CudaSampledIndex(_CudaIndex):
+    _metric = _abi.L2
+
+    def __init__(self, input, probabilities=None, repetitions=None,
+                 random_engine=None, device: int = 0, *, coordinate_sample=None):
+        rows = _matrix(input)
+        sample = _resolve_sample(rows, probabilities, repetitions, random_engine,
+                                 coordinate_sample)
+        handle = ctypes.c_void_p()
+        _check(_abi.load().uha_sampled_index_create(
+            device, self._metric, _ptr(rows), rows.shape[0], rows.shape[1],
+            _ptr(sample.source_columns), _ptr(sample.multiplicities),
+            _ptr(sample.inverse_probabilities), len(sample), ctypes.byref(handle)))
+        self._adopt(handle, rows.shape[1])
+        self.coordinate_sample = sample
+
+
+class CudaSampledCoordinateL2AnnIndex(_CudaSampledIndex):
+    """include/ultrahigh_ann/coordinate_sampling/cuda_sampled_coordinate_l2_ann_index.hpp:23-93."""
+
+    _metric = _abi.L2
+
+
+class CudaSampledCoordinateL1AnnIndex(_CudaSampledIndex):
+    """include/ultrahigh_ann/coordinate_sampling/cuda_sampled_coordinate_l1_ann_index.hpp:20-82."""
+
+    _metric = _abi.L1
+
+    def query_batch(self, queries, query_count, output, workspace,
+                    strategy=QueryStrategy.direct, distances=None):
+        return super().query_batch(queries, query_count, output, workspace,
+                                   QueryStrategy.direct, distances)
+
+
+def _probabilities_for(metric: int, rows: np.ndarray, policy: ExecutionPolicy,
+                       device: int) -> np.ndarray:
+    if policy in (ExecutionPolicy.gpu_fp32, ExecutionPolicy.gpu_cublas_fp32):
+        if metric == _abi.L1 and policy == ExecutionPolicy.gpu_cublas_fp32:
+            raise InvalidArgument("gpu_cublas_fp32 is unavailable for L1 probability "
+                                  "computation")
+        return _probabilities_gpu(metric, rows, device).probabilities
+    raise InvalidArgument(
+        "CPU probability policies belong to the reference CPU library; pass "
+        "importance_probabilities computed there instead")
+
+
+class CudaFlatL2AnnIndex(CudaSampledCoordinateL2AnnIndex):
+    """include/ultrahigh_ann/hnsvw25/l2/flat/cuda_l2_ann_index.hpp:15-60. With
+    importance_probabilities=None the probabilities are built on the device
+    (the gpu_fp32 default policy)."""
+
+    def __init__(self, input, repetitions: int, random_engine: MT19937_64,
+                 device: int = 0,
+                 probability_execution_policy: ExecutionPolicy = ExecutionPolicy.gpu_fp32,
+                 *, importance_probabilities=None):
+        rows = _matrix(input)
+        if importance_probabilities is None:
+            importance_probabilities = _probabilities_for(
+                _abi.L2, rows, probability_execution_policy, device)
+        super().__init__(rows, importance_probabilities, repetitions, random_engine,
+                         device)
+
+
+class CudaFlatL1AnnIndex(CudaSampledCoordinateL1AnnIndex):
+    """include/ultrahigh_ann/hnsvw25/l1/flat/cuda_l1_ann_index.hpp:15-50."""
+
+    def __init__(self, input, repetitions: int, random_engine: MT19937_64,
+                 device: int = 0,
+                 probability_execution_policy: ExecutionPolicy = ExecutionPolicy.gpu_fp32,
+                 *, importance_probabilities=None):
+        rows = _matrix(input)
+        if importance_probabilities is None:
+            importance_probabilities = _probabilities_for(
+                _abi.L1, rows, probability_execution_policy, device)
+        super().__init__(rows, importance_probabilities, repetitions, random_engine,
+                         device)

@@ -1,0 +1,73 @@
+"""Builds the engine's shared library libuha_b200.so in-tree with nvcc.
+
+Every CUDA translation unit is compiled for sm_100a only
+(-gencode arch=compute_100a,code=sm_100a) with -lineinfo; host C++ units are
+compiled by nvcc's host compiler. Objects go to ultrahigh_ann_b200/_build/ and
+are rebuilt when a source or header is newer than the object.
+"""
+from __future__ import annotations
+
+import concurrent.futures
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+PACKAGE = Path(__file__).resolve().parent
+ROOT = PACKAGE.parent
+CSRC = PACKAGE / "csrc"
+BUILD = PACKAGE / "_build"
+LIBRARY = PACKAGE / "libuha_b200.so"
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
+          f"-I{ROOT / 'include'}", f"-I{CSRC}"]
+
+
+def _sources() -> list[Path]:
+    return sorted(list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cpp")))
+
+
+def _headers() -> list[Path]:
+    return sorted(list(CSRC.glob("*.h")) + list((ROOT / "include").glob("*.h")))
+
+
+def _stale(target: Path, deps: list[Path]) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(d.stat().st_mtime > t for d in deps)
+
+
+def _compile(src: Path, verbose: bool) -> Path:
+    obj = BUILD / (src.name + ".o")
+    if not _stale(obj, [src, *_headers(), Path(__file__)]):
+        return obj
+    cmd = [NVCC, *ARCH, *COMMON, "-c", str(src), "-o", str(obj)]
+    if src.suffix == ".cu":
+        cmd[1:1] = ["-Xptxas", "-v"] if verbose else []
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {src.name}:\n{res.stdout}\n{res.stderr}")
+    if verbose and res.stderr:
+        sys.stderr.write(res.stderr)
+    return obj
+
+
+def build(verbose: bool = False) -> Path:
+    """Compiles the library if any input changed; returns its path."""
+    BUILD.mkdir(exist_ok=True)
+    sources = _sources()
+    with concurrent.futures.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as pool:
+        objects = list(pool.map(lambda s: _compile(s, verbose), sources))
+    if _stale(LIBRARY, objects):
+        cmd = [NVCC, *ARCH, "-shared", "-o", str(LIBRARY), *map(str, objects),
+               "--cudart", "static"]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")
+    return LIBRARY
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv))

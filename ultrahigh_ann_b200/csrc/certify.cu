@@ -1,0 +1,360 @@
+// Argmin with lowest-index tie-break, certified against the reference CPU.
+//
+// The reference CPU scans (src/core/dense_l2_scan_index.cpp:25-41,
+// src/exact/l1/exact_l1_index.cpp:26-57,
+// src/coordinate_sampling/sampled_coordinate_l1_ann_index.cpp:119-154) keep the
+// first row with the smallest binary64 distance. The device computes binary32
+// distances D with a known bound |D_cpu - D| <= rel * D + abs. Per query:
+//   U* = min over rows of (D + err)            (an upper bound on the CPU min)
+//   candidates = rows with D - err <= U*        (every row that can be the min)
+// One candidate means the CPU's answer is known. Otherwise the candidates are
+// re-scored by replaying the CPU's binary64 operation sequence (the same
+// operations in the same order, no contraction) and the lexicographic minimum
+// of (distance, row) is the CPU's argmin.
+#include "common.h"
+#include "kernels.h"
+
+#include <cfloat>
+
+namespace uha {
+namespace {
+
+constexpr int kFinalizeThreads = 256;
+constexpr int kResolveThreads = 512;
+
+struct Bounds2 {
+    float lower;
+    float upper;
+};
+
+__device__ __forceinline__ Bounds2 bound_of(float d, Bound b)
+{
+    if (!(d <= FLT_MAX)) {
+        // binary32 overflow: the true distance is at least of order FLT_MAX
+        return {1.0e38f, __int_as_float(0x7f800000)};
+    }
+    const float err = __fadd_ru(__fmul_ru(b.rel, d), b.abs);
+    return {fmaxf(0.f, __fsub_rd(d, err)), __fadd_ru(d, err)};
+}
+
+__device__ __forceinline__ float row_distance(const PartialView& v, uint32_t q,
+                                              uint32_t row)
+{
+    float d = 0.f;
+    for (uint32_t c = 0; c < v.chunks; ++c) {
+        d += v.partials[(static_cast<uint64_t>(c) * v.batch + q) * v.rows +
+                        row];
+    }
+    return d;
+}
+
+// Two smallest lower bounds (with the row of the smallest) and the smallest
+// upper bound seen by a thread / warp / block.
+struct Summary {
+    float min_upper;
+    float first;
+    float second;
+    uint32_t first_row;
+    float first_distance;
+};
+
+__device__ __forceinline__ void summary_insert(Summary& s, float lower,
+                                               float upper, uint32_t row,
+                                               float distance)
+{
+    s.min_upper = fminf(s.min_upper, upper);
+    if (lower < s.first || (lower == s.first && row < s.first_row)) {
+        s.second = s.first;
+        s.first = lower;
+        s.first_row = row;
+        s.first_distance = distance;
+    } else if (lower < s.second) {
+        s.second = lower;
+    }
+}
+
+__device__ __forceinline__ Summary summary_merge(const Summary& a,
+                                                 const Summary& b)
+{
+    Summary r;
+    r.min_upper = fminf(a.min_upper, b.min_upper);
+    const bool a_first =
+        a.first < b.first || (a.first == b.first && a.first_row < b.first_row);
+    const Summary& lo = a_first ? a : b;
+    const Summary& hi = a_first ? b : a;
+    r.first = lo.first;
+    r.first_row = lo.first_row;
+    r.first_distance = lo.first_distance;
+    r.second = fminf(lo.second, hi.first);
+    return r;
+}
+
+__device__ __forceinline__ Summary shfl_summary(const Summary& s, int offset)
+{
+    Summary o;
+    o.min_upper = __shfl_xor_sync(0xffffffffu, s.min_upper, offset);
+    o.first = __shfl_xor_sync(0xffffffffu, s.first, offset);
+    o.second = __shfl_xor_sync(0xffffffffu, s.second, offset);
+    o.first_row = __shfl_xor_sync(0xffffffffu, s.first_row, offset);
+    o.first_distance = __shfl_xor_sync(0xffffffffu, s.first_distance, offset);
+    return o;
+}
+
+__global__ void __launch_bounds__(kFinalizeThreads)
+    finalize_certified_kernel(PartialView view, Bound bound, Result* results,
+                              uint32_t* ambiguous, uint32_t* ambiguous_count)
+{
+    const uint32_t q = blockIdx.x;
+    const float inf = __int_as_float(0x7f800000);
+    Summary s{inf, inf, inf, 0xffffffffu, inf};
+    for (uint32_t row = threadIdx.x; row < view.rows; row += blockDim.x) {
+        const float d = row_distance(view, q, row);
+        const Bounds2 b = bound_of(d, bound);
+        summary_insert(s, b.lower, b.upper, row, d);
+    }
+    for (int offset = 16; offset > 0; offset /= 2) {
+        s = summary_merge(s, shfl_summary(s, offset));
+    }
+    __shared__ Summary warp_summaries[kFinalizeThreads / 32];
+    const int warp = threadIdx.x / 32;
+    const int lane = threadIdx.x % 32;
+    if (lane == 0) {
+        warp_summaries[warp] = s;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        s = lane < kFinalizeThreads / 32
+                ? warp_summaries[lane]
+                : Summary{inf, inf, inf, 0xffffffffu, inf};
+        for (int offset = 16; offset > 0; offset /= 2) {
+            s = summary_merge(s, shfl_summary(s, offset));
+        }
+        if (lane == 0) {
+            if (s.second > s.min_upper) {
+                results[q] = Result{s.first_row, s.first_distance};
+            } else {
+                const uint32_t slot = atomicAdd(ambiguous_count, 1u);
+                ambiguous[slot] = q;
+                results[q] = Result{0xffffffffu, s.first_distance};
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ unsigned int ordered_bits(float f)
+{
+    const unsigned int u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+__global__ void __launch_bounds__(kFinalizeThreads)
+    finalize_gemm_kernel(PartialView view, const float* row_norms,
+                         const float* query_norms, Result* results)
+{
+    const uint32_t q = blockIdx.x;
+    const float qn = query_norms[q];
+    unsigned long long best = ~0ull;
+    for (uint32_t row = threadIdx.x; row < view.rows; row += blockDim.x) {
+        const float dot = row_distance(view, q, row);
+        const float d =
+            __fsub_rn(__fadd_rn(row_norms[row], qn), __fmul_rn(2.0f, dot));
+        const unsigned long long key =
+            (static_cast<unsigned long long>(ordered_bits(d)) << 32) | row;
+        best = key < best ? key : best;
+    }
+    for (int offset = 16; offset > 0; offset /= 2) {
+        const unsigned long long o = __shfl_xor_sync(0xffffffffu, best, offset);
+        best = o < best ? o : best;
+    }
+    __shared__ unsigned long long warp_best[kFinalizeThreads / 32];
+    const int warp = threadIdx.x / 32;
+    const int lane = threadIdx.x % 32;
+    if (lane == 0) {
+        warp_best[warp] = best;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        best = lane < kFinalizeThreads / 32 ? warp_best[lane] : ~0ull;
+        for (int offset = 16; offset > 0; offset /= 2) {
+            const unsigned long long o =
+                __shfl_xor_sync(0xffffffffu, best, offset);
+            best = o < best ? o : best;
+        }
+        if (lane == 0) {
+            const unsigned int bits = static_cast<unsigned int>(best >> 32);
+            const unsigned int raw =
+                (bits & 0x80000000u) ? (bits & 0x7fffffffu) : ~bits;
+            results[q] = Result{static_cast<uint32_t>(best & 0xffffffffu),
+                                __uint_as_float(raw)};
+        }
+    }
+}
+
+// Reference CPU distance of one row, replayed by one warp. Every lane ends
+// with the same value. Terms are formed in parallel; the additions are applied
+// in the CPU's order through warp broadcasts.
+__device__ double replay_row(const ReplayInputs& in, const float* qrow,
+                             const float* rrow, int lane)
+{
+    double s = 0.0;
+    if (in.op == ReplayOp::l1_grouped4) {
+        // std::transform_reduce over random-access ranges (libstdc++ <numeric>):
+        // init += ((t0 + t1) + (t2 + t3)) per full group of four, then the
+        // remaining terms one by one.
+        const uint64_t groups = in.dim / 4;
+        for (uint64_t base = 0; base < groups; base += 32) {
+            const uint64_t g = base + lane;
+            double v3 = 0.0;
+            if (g < groups) {
+                const uint64_t i = 4 * g;
+                const double t0 = fabs(__dsub_rn(qrow[i], rrow[i]));
+                const double t1 = fabs(__dsub_rn(qrow[i + 1], rrow[i + 1]));
+                const double t2 = fabs(__dsub_rn(qrow[i + 2], rrow[i + 2]));
+                const double t3 = fabs(__dsub_rn(qrow[i + 3], rrow[i + 3]));
+                v3 = __dadd_rn(__dadd_rn(t0, t1), __dadd_rn(t2, t3));
+            }
+            const uint64_t n = groups - base < 32 ? groups - base : 32;
+            for (uint64_t j = 0; j < n; ++j) {
+                s = __dadd_rn(s, __shfl_sync(0xffffffffu, v3, static_cast<int>(j)));
+            }
+        }
+        for (uint64_t i = 4 * groups; i < in.dim; ++i) {
+            s = __dadd_rn(s, fabs(__dsub_rn(qrow[i], rrow[i])));
+        }
+        return s;
+    }
+    for (uint64_t base = 0; base < in.dim; base += 32) {
+        const uint64_t i = base + lane;
+        double t = 0.0;
+        if (i < in.dim) {
+            const double diff =
+                __dsub_rn(static_cast<double>(qrow[i]), static_cast<double>(rrow[i]));
+            if (in.op == ReplayOp::l2_sequential) {
+                t = __dmul_rn(diff, diff);
+            } else {
+                t = __dmul_rn(in.weights64[i], fabs(diff));
+            }
+        }
+        const uint64_t n = in.dim - base < 32 ? in.dim - base : 32;
+        for (uint64_t j = 0; j < n; ++j) {
+            s = __dadd_rn(s, __shfl_sync(0xffffffffu, t, static_cast<int>(j)));
+        }
+    }
+    return s;
+}
+
+__device__ __forceinline__ bool lex_less(double a, uint32_t ar, double b,
+                                         uint32_t br)
+{
+    return a < b || (a == b && ar < br);
+}
+
+__global__ void __launch_bounds__(kResolveThreads)
+    resolve_kernel(PartialView view, Bound bound, ReplayInputs in,
+                   const uint32_t* ambiguous, uint32_t ambiguous_count,
+                   Result* results, double* exact_distances)
+{
+    const uint32_t slot = blockIdx.x;
+    if (slot >= ambiguous_count) {
+        return;
+    }
+    const uint32_t q = ambiguous[slot];
+    const int warp = threadIdx.x / 32;
+    const int lane = threadIdx.x % 32;
+    constexpr int warps = kResolveThreads / 32;
+    const float inf = __int_as_float(0x7f800000);
+
+    // U* = min over rows of the upper bound (same arithmetic as finalize)
+    float min_upper = inf;
+    for (uint32_t row = threadIdx.x; row < view.rows; row += blockDim.x) {
+        min_upper = fminf(min_upper, bound_of(row_distance(view, q, row), bound).upper);
+    }
+    for (int offset = 16; offset > 0; offset /= 2) {
+        min_upper = fminf(min_upper, __shfl_xor_sync(0xffffffffu, min_upper, offset));
+    }
+    __shared__ float warp_min[warps];
+    __shared__ double warp_best[warps];
+    __shared__ uint32_t warp_best_row[warps];
+    if (lane == 0) {
+        warp_min[warp] = min_upper;
+    }
+    __syncthreads();
+    min_upper = warp_min[0];
+    for (int w = 1; w < warps; ++w) {
+        min_upper = fminf(min_upper, warp_min[w]);
+    }
+
+    const float* qrow = in.queries + static_cast<uint64_t>(q) * in.padded_dim;
+    double best = __longlong_as_double(0x7ff0000000000000ll);
+    uint32_t best_row = 0xffffffffu;
+    for (uint32_t base = warp * 32; base < view.rows; base += warps * 32) {
+        const uint32_t row = base + lane;
+        bool candidate = false;
+        if (row < view.rows) {
+            candidate = bound_of(row_distance(view, q, row), bound).lower <= min_upper;
+        }
+        unsigned int mask = __ballot_sync(0xffffffffu, candidate);
+        while (mask != 0u) {
+            const int bit = __ffs(mask) - 1;
+            mask &= mask - 1u;
+            const uint32_t crow = base + bit;
+            const double s = replay_row(
+                in, qrow, in.rows + static_cast<uint64_t>(crow) * in.padded_dim,
+                lane);
+            if (lex_less(s, crow, best, best_row)) {
+                best = s;
+                best_row = crow;
+            }
+        }
+    }
+    if (lane == 0) {
+        warp_best[warp] = best;
+        warp_best_row[warp] = best_row;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 0; w < warps; ++w) {
+            if (lex_less(warp_best[w], warp_best_row[w], best, best_row)) {
+                best = warp_best[w];
+                best_row = warp_best_row[w];
+            }
+        }
+        results[q] = Result{best_row, static_cast<float>(best)};
+        exact_distances[q] = best;
+    }
+}
+
+}  // namespace
+
+void launch_finalize_certified(PartialView view, Bound bound, Result* results,
+                               uint32_t* ambiguous, uint32_t* ambiguous_count,
+                               cudaStream_t stream)
+{
+    finalize_certified_kernel<<<view.batch, kFinalizeThreads, 0, stream>>>(
+        view, bound, results, ambiguous, ambiguous_count);
+    check_cuda(cudaGetLastError(), "cannot launch finalize kernel");
+}
+
+void launch_finalize_gemm(PartialView view, const float* row_norms,
+                          const float* query_norms, Result* results,
+                          cudaStream_t stream)
+{
+    finalize_gemm_kernel<<<view.batch, kFinalizeThreads, 0, stream>>>(
+        view, row_norms, query_norms, results);
+    check_cuda(cudaGetLastError(), "cannot launch gemm finalize kernel");
+}
+
+void launch_resolve(PartialView view, Bound bound, ReplayInputs in,
+                    const uint32_t* ambiguous, uint32_t ambiguous_count,
+                    Result* results, double* exact_distances,
+                    cudaStream_t stream)
+{
+    if (ambiguous_count == 0) {
+        return;
+    }
+    resolve_kernel<<<ambiguous_count, kResolveThreads, 0, stream>>>(
+        view, bound, in, ambiguous, ambiguous_count, results, exact_distances);
+    check_cuda(cudaGetLastError(), "cannot launch resolve kernel");
+}
+
+}  // namespace uha

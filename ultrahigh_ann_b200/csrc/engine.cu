@@ -1,0 +1,946 @@
+// C-ABI implementation: device-resident indexes, per-caller workspaces and
+// the query pipeline
+//
+//   H2D (host queries only) -> prepare (gather/scale/validate) -> scan
+//   -> finalize (certified argmin | binary32 norm identity)
+//   -> D2H -> [resolve: binary64 replay of uncertified queries -> D2H]
+//
+// on the workspace's own stream. The resolve step runs only when the
+// finalize kernel reported uncertified queries.
+#include "common.h"
+#include "kernels.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+using uha::checked_add;
+using uha::checked_mul;
+using uha::check_cuda;
+using uha::DeviceBuffer;
+using uha::DeviceGuard;
+using uha::fail;
+using uha::guarded;
+using uha::PinnedBuffer;
+
+namespace {
+
+enum class IndexKind { exact, weighted, sampled };
+
+constexpr uint64_t kColumnAlign = 4;  // padded row length: 16-byte multiple
+constexpr uint64_t kMaxExtent = 0x7fffffffull;
+
+}  // namespace
+
+struct uha_index {
+    int device = 0;
+    std::string device_name;
+    int sm_count = 148;
+    IndexKind kind = IndexKind::exact;
+    uha_metric metric = UHA_L2;
+    uint64_t rows = 0;
+    uint64_t dimension = 0;   // original query dimension d
+    uint64_t scan_dim = 0;    // columns scanned (d or k)
+    uint64_t padded_dim = 0;  // scan_dim rounded up to kColumnAlign
+    uint64_t sample_size = 0;
+    uint64_t sampled_multiplicity = 0;
+    DeviceBuffer<float> scan_rows;   // rows x padded_dim
+    DeviceBuffer<float> row_norms;   // rows (L2, norm-identity strategy)
+    DeviceBuffer<float> weights32;   // padded_dim (weighted L1 scan)
+    DeviceBuffer<double> weights64;  // scan_dim (weighted L1 replay)
+    DeviceBuffer<uint32_t> columns;  // sample_size (sampled)
+    DeviceBuffer<float> scales;      // sample_size (sampled L2)
+    uha_space_usage usage{};
+};
+
+struct uha_workspace {
+    const uha_index* owner = nullptr;
+    uint64_t max_batch = 0;
+    uint64_t payload_bytes = 0;
+    cudaStream_t stream = nullptr;
+    DeviceBuffer<float> raw_queries;
+    DeviceBuffer<float> prepared;
+    DeviceBuffer<float> query_norms;
+    DeviceBuffer<float> partials;
+    DeviceBuffer<uha::Result> results;
+    DeviceBuffer<double> exact;
+    DeviceBuffer<uint32_t> ambiguous;
+    DeviceBuffer<uint32_t> counters;  // [0] ambiguous count, [1] error flag
+    PinnedBuffer<uha::Result> host_results;
+    PinnedBuffer<double> host_exact;
+    PinnedBuffer<uint32_t> host_counters;
+    uha_query_stats last{};
+    bool timing = false;
+    cudaEvent_t events[4] = {nullptr, nullptr, nullptr, nullptr};
+
+    ~uha_workspace()
+    {
+        for (cudaEvent_t e : events) {
+            if (e != nullptr) {
+                cudaEventDestroy(e);
+            }
+        }
+        if (stream != nullptr) {
+            cudaStreamDestroy(stream);
+        }
+    }
+};
+
+namespace {
+
+void require(bool condition, uha_status status, const char* message)
+{
+    if (!condition) {
+        fail(status, message);
+    }
+}
+
+void select_device(uha_index& index, int device)
+{
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        fail(UHA_RUNTIME_ERROR, "no usable CUDA device");
+    }
+    require(device >= 0 && device < count, UHA_INVALID_ARGUMENT,
+            "CUDA device index is out of range");
+    cudaDeviceProp prop{};
+    check_cuda(cudaGetDeviceProperties(&prop, device),
+               "cannot query CUDA device properties");
+    index.device = device;
+    index.device_name = prop.name;
+    index.sm_count = prop.multiProcessorCount;
+}
+
+void validate_rows(const float* rows, uint64_t r, uint64_t d)
+{
+    require(r != 0, UHA_INVALID_ARGUMENT,
+            "CUDA index expects at least one representative");
+    require(r <= kMaxExtent && d <= kMaxExtent, UHA_LENGTH_ERROR,
+            "CUDA index dimensions exceed the device grid limits");
+    checked_mul(r, d, "representative matrix");
+    require(rows != nullptr || d == 0, UHA_INVALID_ARGUMENT,
+            "representative matrix must not be null");
+}
+
+// Uploads a host r x d matrix into the padded r x pd device layout.
+void upload_padded(DeviceBuffer<float>& dst, const float* src, uint64_t r,
+                   uint64_t d, uint64_t pd)
+{
+    dst.allocate(checked_mul(r, pd, "padded representative matrix"));
+    if (dst.size() == 0) {
+        return;
+    }
+    check_cuda(cudaMemset(dst.get(), 0, dst.bytes()),
+               "cannot clear representative matrix");
+    if (d != 0) {
+        check_cuda(cudaMemcpy2D(dst.get(), pd * sizeof(float), src,
+                                d * sizeof(float), d * sizeof(float), r,
+                                cudaMemcpyHostToDevice),
+                   "cannot copy representatives to the CUDA device");
+    }
+}
+
+template <typename T>
+void upload(DeviceBuffer<T>& dst, const T* src, uint64_t count)
+{
+    dst.allocate(count);
+    if (count != 0) {
+        check_cuda(cudaMemcpy(dst.get(), src, count * sizeof(T),
+                              cudaMemcpyHostToDevice),
+                   "cannot copy index data to the CUDA device");
+    }
+}
+
+void compute_row_norms(uha_index& index)
+{
+    index.row_norms.allocate(index.rows);
+    if (index.padded_dim == 0) {
+        check_cuda(cudaMemset(index.row_norms.get(), 0, index.row_norms.bytes()),
+                   "cannot clear row norms");
+        return;
+    }
+    uha::launch_row_norms(index.scan_rows.get(), index.rows, index.padded_dim,
+                          index.row_norms.get(), nullptr);
+    check_cuda(cudaDeviceSynchronize(), "row norm kernel failed");
+}
+
+uint64_t workspace_payload(const uha_index& index, uint64_t b)
+{
+    const uint64_t r = index.rows;
+    const uint64_t f = sizeof(float);
+    const uint64_t z = sizeof(std::size_t);
+    switch (index.kind) {
+    case IndexKind::exact:
+    case IndexKind::weighted:
+        if (index.metric == UHA_L2) {
+            return b * index.dimension * f + b * r * f + b * f + b * z;
+        }
+        return b * index.dimension * f + b * r * f + b * z;
+    case IndexKind::sampled:
+        if (index.metric == UHA_L2) {
+            return 2 * (b * index.sample_size * f) + b * r * f + b * f + b * z;
+        }
+        return 2 * (b * index.sample_size * f) + b * r * f + b * z;
+    }
+    return 0;
+}
+
+// Relative and absolute certification bound for a binary32 distance built
+// from per-term relative error (1 + u)^term_roundings and `depth` sequential
+// binary32 additions, against the CPU's binary64 sum over `terms` terms.
+uha::Bound make_bound(uint32_t depth, uint64_t terms, int term_roundings)
+{
+    const double u32 = std::ldexp(1.0, -24);
+    const double u64 = std::ldexp(1.0, -53);
+    const double n32 = static_cast<double>(depth) + term_roundings + 1;
+    const double n64 = static_cast<double>(terms) + 3;
+    const double g32 = n32 * u32 / (1.0 - n32 * u32);
+    const double g64 = n64 * u64 / (1.0 - n64 * u64);
+    const double rel = 1.01 * (g32 + g64) / (1.0 - g32) + 4 * u32;
+    const double abs = std::ldexp(n32 + 4, -149) * 4;
+    return uha::Bound{
+        std::nextafter(static_cast<float>(rel), 1.0f),
+        std::max(static_cast<float>(abs), std::ldexp(1.0f, -140)),
+    };
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ device
+
+extern "C" int uha_cuda_available(void)
+{
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return count > 0 ? 1 : 0;
+}
+
+extern "C" uha_status uha_device_info_get(int device, uha_device_info* out)
+{
+    return guarded([&] {
+        require(out != nullptr, UHA_INVALID_ARGUMENT,
+                "output pointer must not be null");
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 ||
+            device >= count) {
+            cudaGetLastError();
+            fail(UHA_RUNTIME_ERROR, "no usable CUDA device");
+        }
+        cudaDeviceProp prop{};
+        check_cuda(cudaGetDeviceProperties(&prop, device),
+                   "cannot query CUDA device properties");
+        std::memset(out, 0, sizeof(*out));
+        out->device = device;
+        std::strncpy(out->device_name, prop.name, sizeof(out->device_name) - 1);
+        out->compute_capability_major = prop.major;
+        out->compute_capability_minor = prop.minor;
+        out->total_global_memory_bytes = prop.totalGlobalMem;
+        out->compiled_runtime_version = CUDART_VERSION;
+        check_cuda(cudaRuntimeGetVersion(&out->runtime_version),
+                   "cannot query CUDA runtime version");
+        check_cuda(cudaDriverGetVersion(&out->driver_version),
+                   "cannot query CUDA driver version");
+    });
+}
+
+// ----------------------------------------------------------------- indexes
+
+extern "C" uha_status uha_exact_index_create(int device, uha_metric metric,
+                                             const float* rows,
+                                             uint64_t row_count,
+                                             uint64_t dimension,
+                                             uha_index** out)
+{
+    return guarded([&] {
+        require(out != nullptr, UHA_INVALID_ARGUMENT,
+                "output pointer must not be null");
+        require(metric == UHA_L2 || metric == UHA_L1, UHA_INVALID_ARGUMENT,
+                "unknown metric");
+        validate_rows(rows, row_count, dimension);
+        const uint64_t total = row_count * dimension;
+        for (uint64_t i = 0; i < total; ++i) {
+            if (!std::isfinite(rows[i])) {
+                fail(UHA_INVALID_ARGUMENT, "representatives must be finite");
+            }
+        }
+        auto index = std::make_unique<uha_index>();
+        select_device(*index, device);
+        DeviceGuard guard(device);
+        index->kind = IndexKind::exact;
+        index->metric = metric;
+        index->rows = row_count;
+        index->dimension = dimension;
+        index->scan_dim = dimension;
+        index->padded_dim = uha::round_up(dimension, kColumnAlign);
+        require(index->padded_dim <= kMaxExtent, UHA_LENGTH_ERROR,
+                "CUDA index dimensions exceed the device grid limits");
+        upload_padded(index->scan_rows, rows, row_count, dimension,
+                      index->padded_dim);
+        const uint64_t f = sizeof(float);
+        if (metric == UHA_L2) {
+            compute_row_norms(*index);
+            index->usage.index_payload_bytes =
+                row_count * dimension * f + row_count * f;
+        } else {
+            index->usage.index_payload_bytes = row_count * dimension * f;
+        }
+        index->usage.query_workspace_payload_bytes = 0;
+        index->usage.unique_query_coordinates = dimension;
+        index->usage.sampled_multiplicity = dimension;
+        *out = index.release();
+    });
+}
+
+extern "C" uha_status uha_weighted_l1_index_create(int device,
+                                                   const float* rows,
+                                                   uint64_t row_count,
+                                                   uint64_t dimension,
+                                                   const float* weights,
+                                                   uha_index** out)
+{
+    return guarded([&] {
+        require(out != nullptr, UHA_INVALID_ARGUMENT,
+                "output pointer must not be null");
+        validate_rows(rows, row_count, dimension);
+        require(weights != nullptr || dimension == 0, UHA_INVALID_ARGUMENT,
+                "coordinate weights must not be null");
+        for (uint64_t i = 0; i < row_count * dimension; ++i) {
+            if (!std::isfinite(rows[i])) {
+                fail(UHA_INVALID_ARGUMENT, "representatives must be finite");
+            }
+        }
+        for (uint64_t i = 0; i < dimension; ++i) {
+            if (!std::isfinite(weights[i]) || weights[i] < 0.0f) {
+                fail(UHA_INVALID_ARGUMENT,
+                     "coordinate weights must be finite and nonnegative");
+            }
+        }
+        auto index = std::make_unique<uha_index>();
+        select_device(*index, device);
+        DeviceGuard guard(device);
+        index->kind = IndexKind::weighted;
+        index->metric = UHA_L1;
+        index->rows = row_count;
+        index->dimension = dimension;
+        index->scan_dim = dimension;
+        index->padded_dim = uha::round_up(dimension, kColumnAlign);
+        upload_padded(index->scan_rows, rows, row_count, dimension,
+                      index->padded_dim);
+        std::vector<float> w32(index->padded_dim, 0.0f);
+        std::vector<double> w64(dimension);
+        for (uint64_t i = 0; i < dimension; ++i) {
+            w32[i] = weights[i];
+            w64[i] = static_cast<double>(weights[i]);
+        }
+        upload(index->weights32, w32.data(), w32.size());
+        upload(index->weights64, w64.data(), w64.size());
+        const uint64_t f = sizeof(float);
+        index->usage.index_payload_bytes =
+            row_count * dimension * f + dimension * f;
+        index->usage.unique_query_coordinates = dimension;
+        index->usage.sampled_multiplicity = dimension;
+        *out = index.release();
+    });
+}
+
+extern "C" uha_status uha_sampled_index_create(
+    int device, uha_metric metric, const float* rows, uint64_t row_count,
+    uint64_t dimension, const uint64_t* columns, const uint64_t* multiplicities,
+    const double* inverse_probabilities, uint64_t sample_size, uha_index** out)
+{
+    return guarded([&] {
+        require(out != nullptr, UHA_INVALID_ARGUMENT,
+                "output pointer must not be null");
+        require(metric == UHA_L2 || metric == UHA_L1, UHA_INVALID_ARGUMENT,
+                "unknown metric");
+        validate_rows(rows, row_count, dimension);
+        require(sample_size == 0 ||
+                    (columns != nullptr && multiplicities != nullptr &&
+                     inverse_probabilities != nullptr),
+                UHA_INVALID_ARGUMENT, "coordinate sample must not be null");
+        require(sample_size <= kMaxExtent, UHA_LENGTH_ERROR,
+                "coordinate sample exceeds the device grid limits");
+        uint64_t multiplicity_sum = 0;
+        std::vector<uint32_t> cols(sample_size);
+        std::vector<float> scales(sample_size);
+        std::vector<float> w32(uha::round_up(sample_size, kColumnAlign), 0.0f);
+        std::vector<double> w64(sample_size);
+        for (uint64_t i = 0; i < sample_size; ++i) {
+            if (columns[i] >= dimension) {
+                fail(UHA_OUT_OF_RANGE, "sampled column index out of range");
+            }
+            if (multiplicities[i] == 0 ||
+                !std::isfinite(inverse_probabilities[i]) ||
+                inverse_probabilities[i] <= 0.0) {
+                fail(UHA_INVALID_ARGUMENT,
+                     "sampled columns require positive finite weights");
+            }
+            if (multiplicity_sum > UINT64_MAX - multiplicities[i]) {
+                fail(UHA_LENGTH_ERROR, "sampled multiplicity overflows");
+            }
+            multiplicity_sum += multiplicities[i];
+            // weight = double(multiplicity) * (1/p), as in
+            // l2_coordinate_embedding.cpp:56-57 and l1_coordinate_embedding.cpp:53-54
+            const double weight = static_cast<double>(multiplicities[i]) *
+                                  inverse_probabilities[i];
+            if (metric == UHA_L2) {
+                const float scale = static_cast<float>(std::sqrt(weight));
+                if (!std::isfinite(weight) || weight <= 0.0 ||
+                    !std::isfinite(scale) || scale <= 0.0f) {
+                    fail(UHA_INVALID_ARGUMENT,
+                         "sampled coordinate weight is not representable in "
+                         "float32");
+                }
+                scales[i] = scale;
+            } else {
+                const float fw = static_cast<float>(weight);
+                if (!std::isfinite(weight) || weight <= 0.0 ||
+                    !std::isfinite(fw) || fw <= 0.0f) {
+                    fail(UHA_INVALID_ARGUMENT,
+                         "sampled coordinate weight is not representable in "
+                         "float32");
+                }
+                w32[i] = fw;
+                w64[i] = weight;
+            }
+            cols[i] = static_cast<uint32_t>(columns[i]);
+        }
+        // Validate the sampled representative values (only sampled columns
+        // are part of the index) and, for L2, their scaled binary32 values.
+        for (uint64_t r = 0; r < row_count; ++r) {
+            const float* row = rows + r * dimension;
+            for (uint64_t i = 0; i < sample_size; ++i) {
+                const float v = row[cols[i]];
+                if (!std::isfinite(v)) {
+                    fail(UHA_INVALID_ARGUMENT,
+                         "sampled representatives must be finite");
+                }
+                if (metric == UHA_L2 && !std::isfinite(v * scales[i])) {
+                    fail(UHA_INVALID_ARGUMENT,
+                         "transformed representatives must be finite");
+                }
+            }
+        }
+
+        auto index = std::make_unique<uha_index>();
+        select_device(*index, device);
+        DeviceGuard guard(device);
+        index->kind = IndexKind::sampled;
+        index->metric = metric;
+        index->rows = row_count;
+        index->dimension = dimension;
+        index->scan_dim = sample_size;
+        index->sample_size = sample_size;
+        index->sampled_multiplicity = multiplicity_sum;
+        index->padded_dim = uha::round_up(sample_size, kColumnAlign);
+        upload(index->columns, cols.data(), cols.size());
+        if (metric == UHA_L2) {
+            upload(index->scales, scales.data(), scales.size());
+        } else {
+            upload(index->weights32, w32.data(), w32.size());
+            upload(index->weights64, w64.data(), w64.size());
+        }
+        // Gather (and scale) the sampled columns of the rows on the device.
+        if (index->padded_dim != 0) {
+            DeviceBuffer<float> source(checked_mul(row_count, dimension,
+                                                   "representative matrix"));
+            check_cuda(cudaMemcpy(source.get(), rows, source.bytes(),
+                                  cudaMemcpyHostToDevice),
+                       "cannot copy representatives to the CUDA device");
+            index->scan_rows.allocate(row_count * index->padded_dim);
+            uha::launch_gather_rows(source.get(), row_count, dimension,
+                                    index->columns.get(),
+                                    metric == UHA_L2 ? index->scales.get()
+                                                     : nullptr,
+                                    sample_size, index->scan_rows.get(),
+                                    index->padded_dim, nullptr);
+            check_cuda(cudaDeviceSynchronize(), "row gather kernel failed");
+        }
+        const uint64_t f = sizeof(float);
+        const uint64_t k = sample_size;
+        if (metric == UHA_L2) {
+            compute_row_norms(*index);
+            index->usage.index_payload_bytes = row_count * k * f +
+                                               row_count * f +
+                                               k * sizeof(std::size_t) + k * f;
+        } else {
+            index->usage.index_payload_bytes =
+                row_count * k * f + k * f + k * sizeof(std::size_t);
+        }
+        index->usage.query_workspace_payload_bytes = 0;
+        index->usage.unique_query_coordinates = k;
+        index->usage.sampled_multiplicity = multiplicity_sum;
+        *out = index.release();
+    });
+}
+
+extern "C" void uha_index_destroy(uha_index* index)
+{
+    if (index != nullptr) {
+        int previous = 0;
+        const bool ok = cudaGetDevice(&previous) == cudaSuccess;
+        cudaSetDevice(index->device);
+        delete index;
+        if (ok) {
+            cudaSetDevice(previous);
+        }
+    }
+}
+
+extern "C" uha_status uha_index_space_usage(const uha_index* index,
+                                            uha_space_usage* out)
+{
+    return guarded([&] {
+        require(index != nullptr && out != nullptr, UHA_INVALID_ARGUMENT,
+                "index and output must not be null");
+        *out = index->usage;
+    });
+}
+
+extern "C" uha_status uha_index_device(const uha_index* index, int* device,
+                                       char* name, uint64_t name_capacity)
+{
+    return guarded([&] {
+        require(index != nullptr, UHA_INVALID_ARGUMENT,
+                "index must not be null");
+        if (device != nullptr) {
+            *device = index->device;
+        }
+        if (name != nullptr && name_capacity > 0) {
+            const uint64_t n =
+                std::min<uint64_t>(index->device_name.size(), name_capacity - 1);
+            std::memcpy(name, index->device_name.data(), n);
+            name[n] = '\0';
+        }
+    });
+}
+
+// -------------------------------------------------------------- workspaces
+
+extern "C" uha_status uha_workspace_create(const uha_index* index,
+                                           uint64_t maximum_batch_size,
+                                           uha_workspace** out)
+{
+    return guarded([&] {
+        require(index != nullptr && out != nullptr, UHA_INVALID_ARGUMENT,
+                "index and output must not be null");
+        require(maximum_batch_size != 0, UHA_INVALID_ARGUMENT,
+                "workspace batch size must be positive");
+        require(maximum_batch_size <= kMaxExtent, UHA_LENGTH_ERROR,
+                "workspace batch size exceeds the device grid limits");
+        checked_mul(maximum_batch_size, index->dimension, "query workspace");
+        checked_mul(maximum_batch_size, index->rows, "distance workspace");
+        DeviceGuard guard(index->device);
+        auto ws = std::make_unique<uha_workspace>();
+        ws->owner = index;
+        ws->max_batch = maximum_batch_size;
+        ws->payload_bytes = workspace_payload(*index, maximum_batch_size);
+        check_cuda(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking),
+                   "cannot create CUDA stream");
+        const uint64_t b = maximum_batch_size;
+        ws->raw_queries.allocate(b * index->dimension);
+        ws->prepared.allocate(b * index->padded_dim);
+        ws->query_norms.allocate(b);
+        ws->results.allocate(b);
+        ws->exact.allocate(b);
+        ws->ambiguous.allocate(b);
+        ws->counters.allocate(2);
+        ws->host_results.allocate(b);
+        ws->host_exact.allocate(b);
+        ws->host_counters.allocate(2);
+        for (cudaEvent_t& e : ws->events) {
+            check_cuda(cudaEventCreate(&e), "cannot create CUDA event");
+        }
+        *out = ws.release();
+    });
+}
+
+extern "C" void uha_workspace_destroy(uha_workspace* workspace)
+{
+    if (workspace != nullptr) {
+        int previous = 0;
+        const bool ok = cudaGetDevice(&previous) == cudaSuccess;
+        if (workspace->owner != nullptr) {
+            cudaSetDevice(workspace->owner->device);
+        }
+        delete workspace;
+        if (ok) {
+            cudaSetDevice(previous);
+        }
+    }
+}
+
+extern "C" uha_status uha_workspace_info(const uha_workspace* workspace,
+                                         uint64_t* maximum_batch_size,
+                                         uint64_t* payload_bytes)
+{
+    return guarded([&] {
+        require(workspace != nullptr, UHA_INVALID_ARGUMENT,
+                "workspace must not be null");
+        if (maximum_batch_size != nullptr) {
+            *maximum_batch_size = workspace->max_batch;
+        }
+        if (payload_bytes != nullptr) {
+            *payload_bytes = workspace->payload_bytes;
+        }
+    });
+}
+
+extern "C" uha_status uha_workspace_set_timing(uha_workspace* workspace,
+                                               int enabled)
+{
+    return guarded([&] {
+        require(workspace != nullptr, UHA_INVALID_ARGUMENT,
+                "workspace must not be null");
+        workspace->timing = enabled != 0;
+    });
+}
+
+extern "C" uha_status uha_workspace_last_stats(const uha_workspace* workspace,
+                                               uha_query_stats* out)
+{
+    return guarded([&] {
+        require(workspace != nullptr && out != nullptr, UHA_INVALID_ARGUMENT,
+                "workspace and output must not be null");
+        *out = workspace->last;
+    });
+}
+
+// ------------------------------------------------------------------ query
+
+extern "C" uha_status uha_query(const uha_index* index, uha_workspace* ws,
+                                const float* queries, uint64_t query_count,
+                                int queries_on_device, uha_strategy strategy,
+                                uint64_t* out_indices, double* out_distances)
+{
+    return guarded([&] {
+        require(index != nullptr, UHA_INVALID_ARGUMENT, "index must not be null");
+        require(ws != nullptr && ws->owner == index, UHA_INVALID_ARGUMENT,
+                "CUDA workspace belongs to a different index");
+        require(query_count <= ws->max_batch, UHA_INVALID_ARGUMENT,
+                "query count exceeds CUDA workspace capacity");
+        require(strategy == UHA_DIRECT || strategy == UHA_GEMM,
+                UHA_INVALID_ARGUMENT, "unknown CUDA query strategy");
+        ws->last = uha_query_stats{};
+        ws->last.query_count = query_count;
+        if (query_count == 0) {
+            return;
+        }
+        require(out_indices != nullptr, UHA_INVALID_ARGUMENT,
+                "output must not be null");
+        require(queries != nullptr || index->dimension == 0,
+                UHA_INVALID_ARGUMENT, "query pointer must not be null");
+
+        DeviceGuard guard(index->device);
+        cudaStream_t stream = ws->stream;
+        const uint64_t n = query_count;
+
+        if (index->padded_dim == 0) {
+            // Nothing to compare: every distance is zero and row 0 wins
+            // (empty sample or zero dimension).
+            for (uint64_t q = 0; q < n; ++q) {
+                out_indices[q] = 0;
+                if (out_distances != nullptr) {
+                    out_distances[q] = 0.0;
+                }
+            }
+            ws->last.certified_queries = n;
+            return;
+        }
+
+        if (ws->timing) {
+            check_cuda(cudaEventRecord(ws->events[0], stream), "event");
+        }
+        const float* source = queries;
+        if (!queries_on_device) {
+            check_cuda(cudaMemcpyAsync(ws->raw_queries.get(), queries,
+                                       n * index->dimension * sizeof(float),
+                                       cudaMemcpyHostToDevice, stream),
+                       "cannot copy queries to the CUDA device");
+            source = ws->raw_queries.get();
+        }
+        check_cuda(cudaMemsetAsync(ws->counters.get(), 0,
+                                   ws->counters.bytes(), stream),
+                   "cannot clear query counters");
+        int* error_flag = reinterpret_cast<int*>(ws->counters.get() + 1);
+        uint64_t launches = 1;
+        if (index->kind == IndexKind::sampled) {
+            uha::launch_prepare_sampled(
+                source, n, index->dimension, index->columns.get(),
+                index->metric == UHA_L2 ? index->scales.get() : nullptr,
+                index->sample_size, ws->prepared.get(), index->padded_dim,
+                error_flag, stream);
+        } else {
+            uha::launch_prepare_dense(source, n, index->dimension,
+                                      ws->prepared.get(), index->padded_dim,
+                                      error_flag, stream);
+        }
+
+        const bool gemm = strategy == UHA_GEMM && index->metric == UHA_L2;
+        uha::ScanOp op = uha::ScanOp::l2;
+        if (gemm) {
+            op = uha::ScanOp::dot;
+        } else if (index->metric == UHA_L1) {
+            op = index->weights32.size() != 0 ? uha::ScanOp::l1_weighted
+                                              : uha::ScanOp::l1;
+        }
+        const uha::ScanPlan plan = uha::plan_scan(index->rows, index->padded_dim,
+                                                  n, index->sm_count);
+        const uint64_t partial_count =
+            checked_mul(checked_mul(plan.chunks, n, "partials"), index->rows,
+                        "partials");
+        if (ws->partials.size() < partial_count) {
+            // Grows once per workspace to the largest plan used so far.
+            ws->partials.allocate(partial_count);
+        }
+        if (ws->timing) {
+            check_cuda(cudaEventRecord(ws->events[1], stream), "event");
+        }
+        uha::launch_scan(plan, op, index->scan_rows.get(), index->rows,
+                         index->padded_dim, index->weights32.get(),
+                         ws->prepared.get(), n, ws->partials.get(), stream);
+        if (ws->timing) {
+            check_cuda(cudaEventRecord(ws->events[2], stream), "event");
+        }
+        ++launches;
+
+        const uha::PartialView view{ws->partials.get(), plan.chunks,
+                                    static_cast<uint32_t>(n),
+                                    static_cast<uint32_t>(index->rows)};
+        const int term_roundings = op == uha::ScanOp::l1 ? 1 : 2;
+        const uha::Bound bound =
+            make_bound(plan.depth, index->scan_dim, term_roundings);
+        if (gemm) {
+            uha::launch_query_norms(ws->prepared.get(), n, index->padded_dim,
+                                    ws->query_norms.get(), stream);
+            uha::launch_finalize_gemm(view, index->row_norms.get(),
+                                      ws->query_norms.get(), ws->results.get(),
+                                      stream);
+            launches += 2;
+        } else {
+            uha::launch_finalize_certified(view, bound, ws->results.get(),
+                                           ws->ambiguous.get(),
+                                           ws->counters.get(), stream);
+            ++launches;
+        }
+        check_cuda(cudaMemcpyAsync(ws->host_results.get(), ws->results.get(),
+                                   n * sizeof(uha::Result),
+                                   cudaMemcpyDeviceToHost, stream),
+                   "cannot copy query results from the CUDA device");
+        check_cuda(cudaMemcpyAsync(ws->host_counters.get(), ws->counters.get(),
+                                   ws->counters.bytes(), cudaMemcpyDeviceToHost,
+                                   stream),
+                   "cannot copy query counters from the CUDA device");
+        if (ws->timing) {
+            check_cuda(cudaEventRecord(ws->events[3], stream), "event");
+        }
+        check_cuda(cudaStreamSynchronize(stream), "CUDA query failed");
+        if (ws->timing) {
+            float ms = 0.f;
+            check_cuda(cudaEventElapsedTime(&ms, ws->events[1], ws->events[2]),
+                       "event");
+            ws->last.scan_ms = ms;
+            check_cuda(cudaEventElapsedTime(&ms, ws->events[0], ws->events[3]),
+                       "event");
+            ws->last.device_ms = ms;
+        }
+
+        const uint32_t flag = ws->host_counters.get()[1];
+        if (flag != 0) {
+            if (index->kind == IndexKind::sampled) {
+                fail(UHA_INVALID_ARGUMENT,
+                     (flag & 1u) ? "sampled query coordinate must be finite"
+                                 : "weighted sampled query coordinate must be "
+                                   "finite");
+            }
+            fail(UHA_INVALID_ARGUMENT, "queries must be finite");
+        }
+        const uint32_t ambiguous = gemm ? 0 : ws->host_counters.get()[0];
+        std::vector<uint32_t> replayed;
+        if (ambiguous != 0) {
+            uha::ReplayInputs in{};
+            in.rows = index->scan_rows.get();
+            in.queries = ws->prepared.get();
+            in.dim = index->scan_dim;
+            in.padded_dim = index->padded_dim;
+            in.weights64 = index->weights64.get();
+            if (index->metric == UHA_L2) {
+                in.op = uha::ReplayOp::l2_sequential;
+            } else if (index->weights64.size() != 0) {
+                in.op = uha::ReplayOp::l1_weighted_sequential;
+            } else {
+                in.op = uha::ReplayOp::l1_grouped4;
+            }
+            uha::launch_resolve(view, bound, in, ws->ambiguous.get(), ambiguous,
+                                ws->results.get(), ws->exact.get(), stream);
+            ++launches;
+            replayed.resize(ambiguous);
+            check_cuda(cudaMemcpyAsync(replayed.data(), ws->ambiguous.get(),
+                                       ambiguous * sizeof(uint32_t),
+                                       cudaMemcpyDeviceToHost, stream),
+                       "cannot copy replay list from the CUDA device");
+            check_cuda(cudaMemcpyAsync(ws->host_results.get(), ws->results.get(),
+                                       n * sizeof(uha::Result),
+                                       cudaMemcpyDeviceToHost, stream),
+                       "cannot copy query results from the CUDA device");
+            check_cuda(cudaMemcpyAsync(ws->host_exact.get(), ws->exact.get(),
+                                       n * sizeof(double),
+                                       cudaMemcpyDeviceToHost, stream),
+                       "cannot copy replayed distances from the CUDA device");
+            if (ws->timing) {
+                check_cuda(cudaEventRecord(ws->events[3], stream), "event");
+            }
+            check_cuda(cudaStreamSynchronize(stream), "CUDA replay failed");
+            if (ws->timing) {
+                float ms = 0.f;
+                check_cuda(cudaEventElapsedTime(&ms, ws->events[0], ws->events[3]),
+                           "event");
+                ws->last.device_ms = ms;
+            }
+        }
+        const uha::Result* res = ws->host_results.get();
+        for (uint64_t q = 0; q < n; ++q) {
+            out_indices[q] = res[q].row;
+            if (out_distances != nullptr) {
+                out_distances[q] = static_cast<double>(res[q].distance);
+            }
+        }
+        for (uint32_t q : replayed) {
+            if (out_distances != nullptr) {
+                out_distances[q] = ws->host_exact.get()[q];
+            }
+        }
+        ws->last.certified_queries = n - ambiguous;
+        ws->last.replayed_queries = ambiguous;
+        ws->last.kernel_launches = launches;
+    });
+}
+
+// ---------------------------------------------------------- probabilities
+
+extern "C" uha_status uha_importance_probabilities(
+    int device, uha_metric metric, const float* rows, uint64_t row_count,
+    uint64_t dimension, double* out, uha_probability_report* report)
+{
+    return guarded([&] {
+        require(metric == UHA_L2 || metric == UHA_L1, UHA_INVALID_ARGUMENT,
+                "unknown metric");
+        require(out != nullptr || dimension == 0, UHA_INVALID_ARGUMENT,
+                "output must not be null");
+        require(rows != nullptr || row_count * dimension == 0,
+                UHA_INVALID_ARGUMENT, "representative matrix must not be null");
+        checked_mul(row_count, dimension, "representative matrix");
+        for (uint64_t i = 0; i < row_count * dimension; ++i) {
+            if (!std::isfinite(rows[i])) {
+                fail(UHA_INVALID_ARGUMENT, "representatives must be finite");
+            }
+        }
+        uha_probability_report rep{};
+        rep.pair_count = row_count < 2 ? 0 : row_count * (row_count - 1) / 2;
+        for (uint64_t j = 0; j < dimension; ++j) {
+            out[j] = 0.0;
+        }
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+            cudaGetLastError();
+            fail(UHA_RUNTIME_ERROR, "no usable CUDA device");
+        }
+        require(device >= 0 && device < count, UHA_INVALID_ARGUMENT,
+                "CUDA device index is out of range");
+        if (row_count < 2 || dimension == 0) {
+            if (report != nullptr) {
+                *report = rep;
+            }
+            return;
+        }
+        require(row_count <= 65535ull * 32, UHA_LENGTH_ERROR,
+                "probability construction supports at most 2097120 rows");
+        DeviceGuard guard(device);
+        const uint64_t need = checked_add(
+            checked_add(checked_mul(row_count, dimension * sizeof(float), "rows"),
+                        checked_mul(row_count, row_count * sizeof(double),
+                                    "pair matrix"),
+                        "probability working set"),
+            dimension * sizeof(double), "probability working set");
+        size_t free_bytes = 0;
+        size_t total_bytes = 0;
+        check_cuda(cudaMemGetInfo(&free_bytes, &total_bytes),
+                   "cannot query CUDA memory");
+        if (need > free_bytes) {
+            fail(UHA_RUNTIME_ERROR,
+                 "probability working set exceeds free device memory");
+        }
+        rep.device_working_set_bytes = need;
+        cudaStream_t stream = nullptr;
+        check_cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking),
+                   "cannot create CUDA stream");
+        struct StreamOwner {
+            cudaStream_t s;
+            ~StreamOwner() { cudaStreamDestroy(s); }
+        } owner{stream};
+        cudaEvent_t ev[5];
+        for (auto& e : ev) {
+            check_cuda(cudaEventCreate(&e), "cannot create CUDA event");
+        }
+        struct EventOwner {
+            cudaEvent_t* e;
+            ~EventOwner()
+            {
+                for (int i = 0; i < 5; ++i) {
+                    cudaEventDestroy(e[i]);
+                }
+            }
+        } event_owner{ev};
+        DeviceBuffer<float> d_rows(row_count * dimension);
+        DeviceBuffer<double> inverse(row_count * row_count);
+        DeviceBuffer<unsigned long long> maxima(dimension);
+        check_cuda(cudaEventRecord(ev[0], stream), "event");
+        check_cuda(cudaMemcpyAsync(d_rows.get(), rows, d_rows.bytes(),
+                                   cudaMemcpyHostToDevice, stream),
+                   "cannot copy representatives to the CUDA device");
+        check_cuda(cudaMemsetAsync(inverse.get(), 0, inverse.bytes(), stream),
+                   "cannot clear pair matrix");
+        check_cuda(cudaMemsetAsync(maxima.get(), 0, maxima.bytes(), stream),
+                   "cannot clear column maxima");
+        check_cuda(cudaEventRecord(ev[1], stream), "event");
+        const int m = metric == UHA_L2 ? 0 : 1;
+        uha::launch_pair_distances(m, d_rows.get(), row_count, dimension,
+                                   inverse.get(), stream);
+        check_cuda(cudaEventRecord(ev[2], stream), "event");
+        uha::launch_coordinate_maxima(m, d_rows.get(), row_count, dimension,
+                                      inverse.get(), maxima.get(), stream);
+        check_cuda(cudaEventRecord(ev[3], stream), "event");
+        std::vector<unsigned long long> bits(dimension);
+        check_cuda(cudaMemcpyAsync(bits.data(), maxima.get(), maxima.bytes(),
+                                   cudaMemcpyDeviceToHost, stream),
+                   "cannot copy probabilities from the CUDA device");
+        check_cuda(cudaEventRecord(ev[4], stream), "event");
+        check_cuda(cudaStreamSynchronize(stream), "probability kernels failed");
+        for (uint64_t j = 0; j < dimension; ++j) {
+            double v = 0.0;
+            std::memcpy(&v, &bits[j], sizeof(v));
+            out[j] = metric == UHA_L2 ? std::min(1.0, v) : v;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[0], ev[1]);
+        rep.host_to_device_ms = ms;
+        cudaEventElapsedTime(&ms, ev[1], ev[2]);
+        rep.inverse_distance_ms = ms;
+        cudaEventElapsedTime(&ms, ev[2], ev[3]);
+        rep.coordinate_maximum_ms = ms;
+        cudaEventElapsedTime(&ms, ev[3], ev[4]);
+        rep.device_to_host_ms = ms;
+        cudaEventElapsedTime(&ms, ev[0], ev[4]);
+        rep.total_ms = ms;
+        if (report != nullptr) {
+            *report = rep;
+        }
+    });
+}

@@ -1,0 +1,120 @@
+// Launch interface of the engine's CUDA kernels (host side). Each launcher
+// enqueues on the given stream and returns without synchronising.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace uha {
+
+// What a scan accumulates per (query, row) over the sampled/projected columns.
+enum class ScanOp : int {
+    l2 = 0,        // sum (q - r)^2
+    l1 = 1,        // sum |q - r|
+    l1_weighted = 2,  // sum w * |q - r|
+    dot = 3,       // sum q * r  (binary32 norm-identity strategy)
+};
+
+// How the certifying replay reproduces the reference CPU sum.
+enum class ReplayOp : int {
+    l2_sequential = 0,       // s += (double(q) - double(r))^2, in column order
+    l1_grouped4 = 1,         // std::transform_reduce grouping of |q - r|
+    l1_weighted_sequential = 2,  // s += w64 * |double(q) - double(r)|
+    l2_projected = 3,        // binary64 projected query vs binary64 rows
+    median_projected = 4,    // median |double diff| (nth_element semantics)
+};
+
+// Device view of the per-(chunk, query, row) partial sums of a scan.
+struct PartialView {
+    float* partials;      // [chunks][batch][rows]
+    uint32_t chunks;
+    uint32_t batch;
+    uint32_t rows;
+};
+
+// Certification parameters: a binary32 distance D certifies the reference
+// CPU's binary64 distance to lie in [D - (rel * D + abs), D + (rel * D + abs)].
+struct Bound {
+    float rel;
+    float abs;
+};
+
+struct Result {
+    uint32_t row;
+    float distance;
+};
+
+// ---- query preparation (gather / copy + finiteness validation)
+void launch_prepare_dense(const float* queries, uint64_t batch, uint64_t dim,
+                          float* out, uint64_t padded_dim, int* error_flag,
+                          cudaStream_t stream);
+void launch_prepare_sampled(const float* queries, uint64_t batch, uint64_t dim,
+                            const uint32_t* columns, const float* scales,
+                            uint64_t sample_size, float* out,
+                            uint64_t padded_dim, int* error_flag,
+                            cudaStream_t stream);
+void launch_query_norms(const float* prepared, uint64_t batch,
+                        uint64_t padded_dim, float* norms, cudaStream_t stream);
+
+// ---- scans: write partial sums for every (chunk, query, row)
+// Returns the number of chunks used (stored in PartialView.chunks by the
+// caller) and the accumulation depth for the error bound.
+struct ScanPlan {
+    uint32_t chunks;
+    uint32_t depth;        // longest chain of binary32 additions per distance
+    int kernel;            // 0 = stream kernel, 1 = tile kernel
+    uint32_t k_per_split;  // tile kernel: columns per split
+    int queries_per_pass;  // stream kernel: queries per CTA (1, 2, 4 or 8)
+};
+ScanPlan plan_scan(uint64_t rows, uint64_t padded_dim, uint64_t batch,
+                   int sm_count);
+void launch_scan(const ScanPlan& plan, ScanOp op, const float* rows,
+                 uint64_t row_count, uint64_t padded_dim, const float* weights,
+                 const float* queries, uint64_t batch, float* partials,
+                 cudaStream_t stream);
+
+// ---- certification
+// Sums partials per (query,row), applies the bound, writes certified results
+// and appends uncertified query ids to `ambiguous` (count in *ambiguous_count).
+void launch_finalize_certified(PartialView view, Bound bound, Result* results,
+                               uint32_t* ambiguous, uint32_t* ambiguous_count,
+                               cudaStream_t stream);
+// Binary32 norm identity (no certification), lowest index on ties.
+void launch_finalize_gemm(PartialView view, const float* row_norms,
+                          const float* query_norms, Result* results,
+                          cudaStream_t stream);
+// Replays the reference CPU arithmetic for every candidate row of each
+// ambiguous query and writes the exact winner.
+struct ReplayInputs {
+    ReplayOp op;
+    const float* rows;         // [rows][padded_dim]
+    const float* queries;      // [batch][padded_dim]
+    const double* weights64;   // l1_weighted_sequential
+    uint64_t dim;              // columns to replay
+    uint64_t padded_dim;
+};
+void launch_resolve(PartialView view, Bound bound, ReplayInputs in,
+                    const uint32_t* ambiguous, uint32_t ambiguous_count,
+                    Result* results, double* exact_distances,
+                    cudaStream_t stream);
+
+// ---- build-time helpers
+void launch_gather_rows(const float* source, uint64_t row_count, uint64_t dim,
+                        const uint32_t* columns, const float* scales,
+                        uint64_t sample_size, float* out, uint64_t padded_dim,
+                        cudaStream_t stream);
+void launch_row_norms(const float* rows, uint64_t row_count,
+                      uint64_t padded_dim, float* norms, cudaStream_t stream);
+
+// ---- importance probabilities (binary64 pair distances and normalisation)
+void launch_pair_distances(int metric, const float* rows, uint64_t row_count,
+                           uint64_t dim, double* inverse_distances,
+                           cudaStream_t stream);
+void launch_coordinate_maxima(int metric, const float* rows,
+                              uint64_t row_count, uint64_t dim,
+                              const double* inverse_distances,
+                              unsigned long long* maxima_bits,
+                              cudaStream_t stream);
+
+}  // namespace uha

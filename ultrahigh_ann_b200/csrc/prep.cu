@@ -1,0 +1,187 @@
+// Query preparation and index-build kernels.
+//
+// Query side (one launch per batch):
+// * dense: copy the B x d queries into the padded B x kp layout (kp a multiple
+//   of 4 so every row starts on a 16-byte boundary) and flag non-finite
+//   values (reference: detail::validate_finite_values(queries, "queries"),
+//   src/core/cuda_dense_l2_scan_index.cu:611).
+// * sampled: gather the sampled columns of each query, scale them for L2 with
+//   one binary32 multiply (the host pack of the reference,
+//   src/coordinate_sampling/l2_coordinate_embedding.cpp:114-124, and the
+//   unscaled L1 pack, l1_coordinate_embedding.cpp:103-109) and flag
+//   non-finite sampled values or products. Unsampled columns are never read.
+//
+// Build side: the same gather applied to the representative rows
+// (l2_coordinate_embedding.cpp:71-79, filter_columns.cpp:10-36) and the row
+// norms of the binary32 norm-identity strategy.
+#include "common.h"
+#include "kernels.h"
+
+namespace uha {
+namespace {
+
+constexpr int kThreads = 256;
+
+// error_flag bits: 1 = non-finite (sampled) query value,
+//                  2 = non-finite weighted/scaled value
+__global__ void prepare_dense_kernel(const float* __restrict__ queries,
+                                     uint64_t batch, uint64_t dim,
+                                     float* __restrict__ out,
+                                     uint64_t padded_dim, int* error_flag)
+{
+    const uint64_t total = batch * padded_dim;
+    for (uint64_t idx = blockIdx.x * static_cast<uint64_t>(blockDim.x) +
+                        threadIdx.x;
+         idx < total; idx += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t b = idx / padded_dim;
+        const uint64_t i = idx - b * padded_dim;
+        float v = 0.f;
+        if (i < dim) {
+            v = queries[b * dim + i];
+            if (!isfinite(v)) {
+                atomicOr(error_flag, 1);
+            }
+        }
+        out[idx] = v;
+    }
+}
+
+__global__ void prepare_sampled_kernel(const float* __restrict__ queries,
+                                       uint64_t batch, uint64_t dim,
+                                       const uint32_t* __restrict__ columns,
+                                       const float* __restrict__ scales,
+                                       uint64_t sample_size,
+                                       float* __restrict__ out,
+                                       uint64_t padded_dim, int* error_flag)
+{
+    const uint64_t total = batch * padded_dim;
+    for (uint64_t idx = blockIdx.x * static_cast<uint64_t>(blockDim.x) +
+                        threadIdx.x;
+         idx < total; idx += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t b = idx / padded_dim;
+        const uint64_t i = idx - b * padded_dim;
+        float v = 0.f;
+        if (i < sample_size) {
+            v = queries[b * dim + columns[i]];
+            if (!isfinite(v)) {
+                atomicOr(error_flag, 1);
+            }
+            if (scales != nullptr) {
+                v = __fmul_rn(v, scales[i]);
+                if (!isfinite(v)) {
+                    atomicOr(error_flag, 2);
+                }
+            }
+        }
+        out[idx] = v;
+    }
+}
+
+__global__ void query_norms_kernel(const float* __restrict__ prepared,
+                                   uint64_t batch, uint64_t padded_dim,
+                                   float* __restrict__ norms)
+{
+    const uint64_t warp_id =
+        (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) / 32;
+    const int lane = threadIdx.x % 32;
+    if (warp_id >= batch) {
+        return;
+    }
+    const float* row = prepared + warp_id * padded_dim;
+    float acc = 0.f;
+    for (uint64_t i = lane; i < padded_dim; i += 32) {
+        acc = fmaf(row[i], row[i], acc);
+    }
+    for (int offset = 16; offset > 0; offset /= 2) {
+        acc += __shfl_xor_sync(0xffffffffu, acc, offset);
+    }
+    if (lane == 0) {
+        norms[warp_id] = acc;
+    }
+}
+
+__global__ void gather_rows_kernel(const float* __restrict__ source,
+                                   uint64_t row_count, uint64_t dim,
+                                   const uint32_t* __restrict__ columns,
+                                   const float* __restrict__ scales,
+                                   uint64_t sample_size,
+                                   float* __restrict__ out,
+                                   uint64_t padded_dim)
+{
+    const uint64_t total = row_count * padded_dim;
+    for (uint64_t idx = blockIdx.x * static_cast<uint64_t>(blockDim.x) +
+                        threadIdx.x;
+         idx < total; idx += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t r = idx / padded_dim;
+        const uint64_t i = idx - r * padded_dim;
+        float v = 0.f;
+        if (i < sample_size) {
+            v = source[r * dim + columns[i]];
+            if (scales != nullptr) {
+                v = __fmul_rn(v, scales[i]);
+            }
+        }
+        out[idx] = v;
+    }
+}
+
+uint32_t grid_for(uint64_t total)
+{
+    const uint64_t blocks = (total + kThreads - 1) / kThreads;
+    return static_cast<uint32_t>(blocks < 148ull * 64 ? (blocks == 0 ? 1 : blocks)
+                                                      : 148ull * 64);
+}
+
+}  // namespace
+
+void launch_prepare_dense(const float* queries, uint64_t batch, uint64_t dim,
+                          float* out, uint64_t padded_dim, int* error_flag,
+                          cudaStream_t stream)
+{
+    prepare_dense_kernel<<<grid_for(batch * padded_dim), kThreads, 0, stream>>>(
+        queries, batch, dim, out, padded_dim, error_flag);
+    check_cuda(cudaGetLastError(), "cannot launch query preparation kernel");
+}
+
+void launch_prepare_sampled(const float* queries, uint64_t batch, uint64_t dim,
+                            const uint32_t* columns, const float* scales,
+                            uint64_t sample_size, float* out,
+                            uint64_t padded_dim, int* error_flag,
+                            cudaStream_t stream)
+{
+    prepare_sampled_kernel<<<grid_for(batch * padded_dim), kThreads, 0,
+                             stream>>>(queries, batch, dim, columns, scales,
+                                       sample_size, out, padded_dim,
+                                       error_flag);
+    check_cuda(cudaGetLastError(), "cannot launch query gather kernel");
+}
+
+void launch_query_norms(const float* prepared, uint64_t batch,
+                        uint64_t padded_dim, float* norms, cudaStream_t stream)
+{
+    const uint64_t threads = batch * 32;
+    query_norms_kernel<<<static_cast<uint32_t>((threads + kThreads - 1) /
+                                               kThreads),
+                         kThreads, 0, stream>>>(prepared, batch, padded_dim,
+                                                norms);
+    check_cuda(cudaGetLastError(), "cannot launch query norm kernel");
+}
+
+void launch_gather_rows(const float* source, uint64_t row_count, uint64_t dim,
+                        const uint32_t* columns, const float* scales,
+                        uint64_t sample_size, float* out, uint64_t padded_dim,
+                        cudaStream_t stream)
+{
+    gather_rows_kernel<<<grid_for(row_count * padded_dim), kThreads, 0,
+                         stream>>>(source, row_count, dim, columns, scales,
+                                   sample_size, out, padded_dim);
+    check_cuda(cudaGetLastError(), "cannot launch row gather kernel");
+}
+
+void launch_row_norms(const float* rows, uint64_t row_count,
+                      uint64_t padded_dim, float* norms, cudaStream_t stream)
+{
+    launch_query_norms(rows, row_count, padded_dim, norms, stream);
+}
+
+}  // namespace uha

@@ -1,0 +1,201 @@
+// Importance probabilities on the device.
+//
+// Reference semantics (src/hnsvw25/l2/importance_sampling.cpp:19-45,
+// src/hnsvw25/l1/importance_sampling.cpp:19-47): for every pair of rows a < b
+// with nonzero distance, L2 contributes min(1, (a_j - b_j)^2 / ||a - b||^2) and
+// L1 contributes |a_j - b_j| / ||a - b||_1 to column j; p_j is the maximum
+// contribution. Pair distances and the per-column maxima use binary64 (the
+// normalisation of the probabilities), so the result agrees with the CPU's
+// binary64 loop to a few ulps.
+//
+// Stage 1 (pair kernel): a 32 x 32 block of pairs per CTA, columns staged
+// through shared memory in 64-column slabs; each thread accumulates four
+// pairs. The inverse distance of every pair a < b (0 for zero distance and for
+// a >= b) is written to an r x r matrix.
+// Stage 2 (column kernel): a CTA owns 256 columns and one 32-row block A and
+// walks every row block B >= A; per pair the contribution is formed with the
+// inverse distance and folded into a per-column maximum. Zero inverse
+// distances contribute 0, so no branch is needed. Column maxima are combined
+// across CTAs with a 64-bit atomicMax on the bit pattern (nonnegative binary64
+// values order like their bit patterns).
+#include "common.h"
+#include "kernels.h"
+
+namespace uha {
+namespace {
+
+constexpr int kPairBlock = 32;
+constexpr int kPairSlab = 64;
+constexpr int kColumns = 256;
+
+__global__ void __launch_bounds__(256)
+    pair_distance_kernel(int metric, const float* __restrict__ rows,
+                         uint32_t row_count, uint64_t dim,
+                         double* __restrict__ inverse)
+{
+    const uint32_t ta = blockIdx.y;
+    const uint32_t tb = blockIdx.x;
+    if (tb < ta) {
+        return;
+    }
+    __shared__ float sa[kPairBlock][kPairSlab + 1];
+    __shared__ float sb[kPairBlock][kPairSlab + 1];
+    const int ty = threadIdx.x / 8;  // 0..31: row a within block
+    const int tx = threadIdx.x % 8;  // b = tx + 8 j
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    const uint32_t a0 = ta * kPairBlock;
+    const uint32_t b0 = tb * kPairBlock;
+    for (uint64_t c0 = 0; c0 < dim; c0 += kPairSlab) {
+        for (int i = threadIdx.x; i < kPairBlock * kPairSlab; i += blockDim.x) {
+            const int r = i / kPairSlab;
+            const int c = i % kPairSlab;
+            const uint64_t col = c0 + c;
+            float va = 0.f;
+            float vb = 0.f;
+            if (col < dim) {
+                if (a0 + r < row_count) {
+                    va = rows[static_cast<uint64_t>(a0 + r) * dim + col];
+                }
+                if (b0 + r < row_count) {
+                    vb = rows[static_cast<uint64_t>(b0 + r) * dim + col];
+                }
+            }
+            sa[r][c] = va;
+            sb[r][c] = vb;
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int c = 0; c < kPairSlab; ++c) {
+            const double va = sa[ty][c];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const double d = va - static_cast<double>(sb[tx + 8 * j][c]);
+                if (metric == 0) {
+                    acc[j] = fma(d, d, acc[j]);
+                } else {
+                    acc[j] += fabs(d);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    const uint32_t a = a0 + ty;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const uint32_t b = b0 + tx + 8 * j;
+        if (a < row_count && b < row_count && a < b && acc[j] != 0.0) {
+            inverse[static_cast<uint64_t>(a) * row_count + b] = 1.0 / acc[j];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kColumns)
+    coordinate_max_kernel(int metric, const float* __restrict__ rows,
+                          uint32_t row_count, uint64_t dim,
+                          const double* __restrict__ inverse,
+                          unsigned long long* __restrict__ maxima_bits)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* sinv = reinterpret_cast<double*>(smem);                 // [32][32]
+    float* sa = reinterpret_cast<float*>(sinv + kPairBlock * kPairBlock);  // [32][256]
+    float* sb = sa + kPairBlock * kColumns;                          // [32][256]
+
+    const uint64_t col = blockIdx.x * static_cast<uint64_t>(kColumns) +
+                         threadIdx.x;
+    const uint32_t ta = blockIdx.y;
+    const uint32_t a0 = ta * kPairBlock;
+    const uint32_t blocks = (row_count + kPairBlock - 1) / kPairBlock;
+
+    for (int r = 0; r < kPairBlock; ++r) {
+        float v = 0.f;
+        if (a0 + r < row_count && col < dim) {
+            v = rows[static_cast<uint64_t>(a0 + r) * dim + col];
+        }
+        sa[r * kColumns + threadIdx.x] = v;
+    }
+    double m = 0.0;
+    for (uint32_t tb = ta; tb < blocks; ++tb) {
+        const uint32_t b0 = tb * kPairBlock;
+        __syncthreads();
+        for (int r = 0; r < kPairBlock; ++r) {
+            float v = 0.f;
+            if (b0 + r < row_count && col < dim) {
+                v = rows[static_cast<uint64_t>(b0 + r) * dim + col];
+            }
+            sb[r * kColumns + threadIdx.x] = v;
+        }
+        for (int i = threadIdx.x; i < kPairBlock * kPairBlock; i += blockDim.x) {
+            const int ra = i / kPairBlock;
+            const int rb = i % kPairBlock;
+            double v = 0.0;
+            if (a0 + ra < row_count && b0 + rb < row_count) {
+                v = inverse[static_cast<uint64_t>(a0 + ra) * row_count + b0 + rb];
+            }
+            sinv[i] = v;
+        }
+        __syncthreads();
+        for (int ra = 0; ra < kPairBlock; ++ra) {
+            const double va = sa[ra * kColumns + threadIdx.x];
+#pragma unroll 8
+            for (int rb = 0; rb < kPairBlock; ++rb) {
+                const double d = va - static_cast<double>(sb[rb * kColumns + threadIdx.x]);
+                const double w = sinv[ra * kPairBlock + rb];
+                const double c = metric == 0 ? (d * d) * w : fabs(d) * w;
+                m = fmax(m, c);
+            }
+        }
+    }
+    if (col < dim && m > 0.0) {
+        atomicMax(maxima_bits + col,
+                  static_cast<unsigned long long>(__double_as_longlong(m)));
+    }
+}
+
+}  // namespace
+
+void launch_pair_distances(int metric, const float* rows, uint64_t row_count,
+                           uint64_t dim, double* inverse_distances,
+                           cudaStream_t stream)
+{
+    const uint32_t blocks =
+        static_cast<uint32_t>((row_count + kPairBlock - 1) / kPairBlock);
+    if (blocks > 65535u) {
+        fail(UHA_LENGTH_ERROR, "probability pair grid exceeds device limit");
+    }
+    const dim3 grid(blocks, blocks);
+    pair_distance_kernel<<<grid, 256, 0, stream>>>(
+        metric, rows, static_cast<uint32_t>(row_count), dim, inverse_distances);
+    check_cuda(cudaGetLastError(), "cannot launch pair distance kernel");
+}
+
+void launch_coordinate_maxima(int metric, const float* rows,
+                              uint64_t row_count, uint64_t dim,
+                              const double* inverse_distances,
+                              unsigned long long* maxima_bits,
+                              cudaStream_t stream)
+{
+    const uint32_t blocks =
+        static_cast<uint32_t>((row_count + kPairBlock - 1) / kPairBlock);
+    const uint64_t column_blocks = (dim + kColumns - 1) / kColumns;
+    if (column_blocks > 0x7fffffffull || blocks > 65535u) {
+        fail(UHA_LENGTH_ERROR, "probability column grid exceeds device limit");
+    }
+    const size_t smem = kPairBlock * kPairBlock * sizeof(double) +
+                        2 * kPairBlock * kColumns * sizeof(float);
+    static bool configured[kMaxDevices] = {};
+    const int dev = current_device();
+    if (!configured[dev]) {
+        check_cuda(cudaFuncSetAttribute(coordinate_max_kernel,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(smem)),
+                   "cannot configure probability column kernel");
+        configured[dev] = true;
+    }
+    const dim3 grid(static_cast<uint32_t>(column_blocks), blocks);
+    coordinate_max_kernel<<<grid, kColumns, smem, stream>>>(
+        metric, rows, static_cast<uint32_t>(row_count), dim, inverse_distances,
+        maxima_bits);
+    check_cuda(cudaGetLastError(), "cannot launch probability column kernel");
+}
+
+}  // namespace uha
