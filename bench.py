@@ -1,0 +1,403 @@
+#!/usr/bin/env python
+"""Benchmark of the HNSVW query path on B200.
+
+Workload (headline): the exact L2 index over r = 7,028 reference rows in
+d = 60,660 coordinates (the row-level TCGA-shaped synthetic workload), 8,192
+queries per step answered one query at a time (batch 1). A step is one pass
+over the 8,192 queries, as one trial of the reference benchmark's
+measure_queries loop. Each answer is the reference CPU's argmin, bit-exact
+(certified binary32 scan + binary64 replay of uncertified queries).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 runs under torchrun as independent replicas: every rank holds a copy of
+the index and answers its own 8,192 queries (weak scaling, no collective on the
+data path); timing is the max over ranks. `--impl reference` times the
+reference's own CPU implementation (its library compiled from source into
+oracle/_ref) on the host cores, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+ROWS, DIM, QUERIES = 7028, 60660, 8192
+METRIC = "queries/s at r=7028,d=60660 (agreement vs FP64 exact); %HBM peak; p99 latency"
+WORKLOAD = "exact_l2_r7028_d60660_b1"
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    p.add_argument("--batch", type=int, default=1)
+    p.add_argument("--queries", type=int, default=QUERIES)
+    p.add_argument("--no-suite", action="store_true",
+                   help="skip the secondary configurations")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def measured_peaks() -> dict:
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        return json.loads(path.read_text())
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "fallback": True}
+
+
+class ClockSampler:
+    """nvidia-smi sampled every 200 ms while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        self.file.flush()
+        self.file.seek(0)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for line in self.file.read().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.file.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": mx or None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def profile_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary."""
+    path = ROOT / "profiles" / "traffic.json"
+    if not path.exists():
+        return None
+    entry = json.loads(path.read_text()).get(kernel)
+    return None if entry is None else entry.get("dram_bytes_per_launch")
+
+
+# --------------------------------------------------------------- engine arm
+def run_engine(args):
+    import torch
+
+    import ultrahigh_ann_b200 as uha
+    from ultrahigh_ann_b200 import synthetic
+
+    world, rank, local = dist_env()
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    device = torch.cuda.current_device()
+
+    # weak scaling: every rank answers its own query set against the same rows
+    ds = synthetic.row_dataset(rows=ROWS, classes=33, queries=args.queries, d=DIM,
+                               seed=1, query_stream=rank)
+    B = args.batch
+    n = args.queries
+    index = uha.CudaExactL2Index(ds.rows, device=device)
+    qdev = torch.from_numpy(ds.queries).to(f"cuda:{device}")
+    ws = index.make_query_workspace(B)
+    ws.set_timing(True)
+    stream = torch.cuda.ExternalStream(ws.stream_handle())
+    out = np.zeros(n, np.uint64)
+
+    def one_step(acc=None):
+        base = qdev.data_ptr()
+        for s in range(0, n, B):
+            e = min(n, s + B)
+            t = time.perf_counter()
+            index.query_device_batch(base + s * DIM * 4, e - s, out[s:e], ws)
+            if acc is not None:
+                st = ws.last_stats()
+                acc["lat"].append((time.perf_counter() - t) * 1e3)
+                acc["scan_ms"] += st["scan_ms"]
+                acc["scan_launches"] += 1
+                acc["launches"] += st["kernel_launches"]
+                acc["replayed"] += st["replayed_queries"]
+
+    for _ in range(args.warmup):
+        one_step()
+    acc = {"lat": [], "scan_ms": 0.0, "scan_launches": 0, "launches": 0, "replayed": 0}
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(device) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            one_step(acc)
+        stop.record(stream)
+        stop.synchronize()
+        torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    elapsed_ms = start.elapsed_time(stop)
+    if world > 1:
+        t = torch.tensor([elapsed_ms], device=f"cuda:{device}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    value = world * n * args.steps / (elapsed_ms / 1e3)
+
+    # roofline of the dominant kernel (the batch-1 stream scan)
+    peaks = measured_peaks()
+    scan_avg_ms = acc["scan_ms"] / max(1, acc["scan_launches"])
+    alg_bytes = ROWS * DIM * 4 + B * DIM * 4
+    achieved = alg_bytes / (scan_avg_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1),
+                "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": round(achieved / peaks["hbm_gbs"], 4),
+                "traffic": profile_traffic("stream_scan_kernel<1,0>"),
+                "kernel": "stream_scan_kernel<1,0>",
+                "algorithmic_bytes_per_launch": alg_bytes,
+                "avg_launch_ms": round(scan_avg_ms, 5),
+                "peak_source": "measured" if not peaks.get("fallback") else "fallback"}
+
+    # end to end through the public API: host queries (pinned), H2D and the
+    # result read inside the timed region
+    host_q = torch.from_numpy(ds.queries).pin_memory()
+    host_np = host_q.numpy()
+    e2e_steps = 1
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for s in range(0, n, B):
+            e = min(n, s + B)
+            index.query_batch(host_np[s:e], e - s, out[s:e], ws)
+    e2e_s = time.perf_counter() - t0
+    e2e = {"value": round(n * e2e_steps / e2e_s, 2), "unit": "queries/s",
+           "h2d_bytes_per_step": n * DIM * 4,
+           "d2h_bytes_per_step": n * 8 + (n // B) * 8,
+           "path": "uha_query (C ABI) with host queries"}
+
+    line = {"metric": METRIC, "value": round(value, 2), "unit": "queries/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(elapsed_ms / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 scan, f64 certification replay", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "rows": ROWS, "dimension": DIM,
+                       "queries_per_step": n, "batch": B, "index": "exact",
+                       "metric": "l2", "strategy": "direct (certified)",
+                       "parallelism": f"replicas x{world}",
+                       "l2_flush": "inputs larger than L2 (rows 1.71 GB, queries 1.99 GB)"},
+            "roofline": roofline,
+            "latency_ms": {"p50": round(float(np.percentile(acc["lat"], 50)), 4),
+                           "p99": round(float(np.percentile(acc["lat"], 99)), 4),
+                           "scope": "per query_device_batch call, host wall clock"},
+            "replayed_queries": acc["replayed"],
+            "agreement_vs_fp64_exact": None,
+            "e2e": e2e, "gpu_launches": acc["launches"]}
+    line["clocks"] = clocks.summary()
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"], agree = cpu_baseline(ds, index, ws)
+        line["agreement_vs_fp64_exact"] = agree
+    if rank == 0 and not args.no_suite and world == 1:
+        del qdev
+        torch.cuda.empty_cache()
+        line["suite"] = suite(ds, index)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def cpu_baseline(ds, index, ws):
+    """The reference's own ExactL2Index (oracle/_ref) on all host cores, on a
+    bounded sample of the same queries. Also checks the engine's answers on
+    that sample against it (agreement with the binary64 exact scan)."""
+    from oracle import oracle as O
+
+    threads = os.cpu_count() or 1
+    ref = O.RefExactIndex("l2", ds.rows)
+    probe = ds.queries[:threads]
+    t = time.perf_counter()
+    ref.query_batch(probe, threads)
+    per = (time.perf_counter() - t) / probe.shape[0]
+    sample = int(min(ds.queries.shape[0], max(threads, 15.0 / per)))
+    sample = max(threads, sample // threads * threads)
+    q = ds.queries[:sample]
+    t = time.perf_counter()
+    expected = ref.query_batch(q, threads)
+    secs = time.perf_counter() - t
+    got = np.zeros(sample, np.uint64)
+    for s in range(sample):
+        index.query_batch(q[s], 1, got[s:s + 1], ws)
+    agree = float(np.mean(got == expected))
+    return ({"value": round(sample / secs, 3), "unit": "queries/s", "cores": threads,
+             "kind": "reference",
+             "sample": f"{sample} of the {ds.queries.shape[0]} queries, "
+                       f"ExactL2Index::query_batch parallel_queries, "
+                       f"{threads} OpenMP threads ({secs:.1f} s)"}, agree)
+
+
+def suite(ds, exact_index):
+    """Secondary configurations of the same data: batches 64 and 1024, L1, and
+    the flat (importance-sampled) indexes with their agreement against the
+    exact argmin (the engine's exact index, itself bit-exact to the reference's
+    binary64 scan)."""
+    import torch
+
+    import ultrahigh_ann_b200 as uha
+
+    out = []
+    nq = 2048
+    qdev = torch.from_numpy(ds.queries[:nq]).cuda()
+
+    def timeit(index, B, n):
+        ws = index.make_query_workspace(B)
+        res = np.zeros(n, np.uint64)
+        index.query_device_batch(qdev.data_ptr(), min(B, n), res[:min(B, n)], ws)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        repl = 0
+        for s in range(0, n, B):
+            e = min(n, s + B)
+            index.query_device_batch(qdev.data_ptr() + s * DIM * 4, e - s, res[s:e], ws)
+            repl += ws.last_stats()["replayed_queries"]
+        return res, n / (time.perf_counter() - t), repl
+
+    exact_ans = {}
+    for metric, index in (("l2", exact_index), ("l1", uha.CudaExactL1Index(ds.rows))):
+        for B, n in ((1, 64), (64, 512), (1024, 2048)):
+            res, qps, repl = timeit(index, B, n)
+            if B == 1024:
+                exact_ans[metric] = res
+            out.append({"index": "exact", "metric": metric, "batch": B,
+                        "queries_per_s": round(qps, 1), "replayed": repl})
+    for metric, prob_fn, cls in (
+            ("l2", uha.compute_l2_importance_probabilities_gpu,
+             uha.CudaSampledCoordinateL2AnnIndex),
+            ("l1", uha.compute_l1_importance_probabilities_gpu,
+             uha.CudaSampledCoordinateL1AnnIndex)):
+        probs = prob_fn(ds.rows)
+        for T in (32, 128):
+            index = cls(ds.rows, probs.probabilities, T, uha.MT19937_64(0))
+            for B, n in ((1, 512), (64, 2048), (1024, 2048)):
+                res, qps, repl = timeit(index, B, n)
+                entry = {"index": "flat", "metric": metric, "T": T,
+                         "k": len(index.coordinate_sample), "batch": B,
+                         "queries_per_s": round(qps, 1), "replayed": repl}
+                if B == 1024:
+                    entry["agreement_vs_fp64_exact"] = round(
+                        float(np.mean(res == exact_ans[metric])), 4)
+                out.append(entry)
+            out[-1]["probability_build_ms"] = round(probs.total_ms, 1)
+    return out
+
+
+# ------------------------------------------------------------ reference arm
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from ultrahigh_ann_b200 import synthetic
+
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "reference library oracle/_ref/libref.so "
+                                         "was not built"}))
+        return
+    threads = os.cpu_count() or 1
+    ds = synthetic.row_dataset(rows=ROWS, classes=33, queries=args.queries, d=DIM,
+                               seed=1)
+    ref = O.RefExactIndex("l2", ds.rows)
+    probe = ds.queries[:threads]
+    t = time.perf_counter()
+    ref.query_batch(probe, threads)
+    per = (time.perf_counter() - t) / probe.shape[0]
+    # each step: a bounded sample sized for ~8 s of host work
+    sample = int(max(threads, min(args.queries, 8.0 / per)))
+    sample = max(threads, sample // threads * threads)
+    for w in range(args.warmup):
+        ref.query_batch(ds.queries[:threads], threads)
+    t = time.perf_counter()
+    for k in range(args.steps):
+        s = (k * sample) % max(1, args.queries - sample)
+        ref.query_batch(ds.queries[s:s + sample], threads)
+    secs = time.perf_counter() - t
+    value = sample * args.steps / secs
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(value, 3),
+        "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(secs * 1e3 / args.steps, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "rows": ROWS, "dimension": DIM,
+                   "queries_per_step": sample, "batch": args.batch, "index": "exact",
+                   "metric": "l2"},
+        "cpu_baseline": {"value": round(value, 3), "unit": "queries/s",
+                         "cores": threads, "kind": "reference",
+                         "sample": f"{sample} queries per step, ExactL2Index::"
+                                   f"query_batch parallel_queries, {threads} threads"},
+        "e2e": {"value": round(value, 3), "unit": "queries/s",
+                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_engine(args)
+
+
+if __name__ == "__main__":
+    main()

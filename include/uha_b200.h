@@ -203,6 +203,10 @@ uha_status uha_query(const uha_index* index, uha_workspace* workspace,
 uha_status uha_workspace_last_stats(const uha_workspace* workspace,
                                     uha_query_stats* out);
 
+/* The CUDA stream (cudaStream_t) the workspace enqueues its work on, so a
+ * caller can order its own work or record timing events against it. */
+void* uha_workspace_stream(const uha_workspace* workspace);
+
 /* With enabled != 0, every uha_query on this workspace records CUDA events on
  * the workspace stream around the scan kernel and around the whole device
  * pipeline, reported in uha_query_stats.scan_ms / device_ms. */

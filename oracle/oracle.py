@@ -112,6 +112,12 @@ def ref_lib() -> ctypes.CDLL:
         lib.ref_projection.argtypes = [c_int, c_void_p, c_uint64, c_uint64, c_void_p,
                                        c_void_p, c_void_p, c_uint64, c_uint64, c_char_p,
                                        c_uint64, c_void_p, c_void_p]
+        lib.ref_exact_create.restype = c_void_p
+        lib.ref_exact_create.argtypes = [c_int, c_void_p, c_uint64, c_uint64]
+        lib.ref_exact_destroy.restype = None
+        lib.ref_exact_destroy.argtypes = [c_void_p]
+        lib.ref_exact_query.restype = c_int
+        lib.ref_exact_query.argtypes = [c_void_p, c_void_p, c_uint64, c_int, c_void_p]
         _ref = lib
     return _ref
 
@@ -276,6 +282,30 @@ def ref_exact(metric: str, rows, queries, threads: int = 1):
         _ref_check(ref_lib().ref_exact_l1(_p(rows), rows.shape[0], rows.shape[1], _p(q),
                                           q.shape[0], threads, _p(out)))
     return out
+
+
+class RefExactIndex:
+    """A persistent reference ExactL2Index / ExactL1Index (CPU)."""
+
+    def __init__(self, metric: str, rows):
+        self._rows = _f32(rows)
+        self.dimension = self._rows.shape[1]
+        self._h = ref_lib().ref_exact_create(0 if metric == "l2" else 1, _p(self._rows),
+                                             self._rows.shape[0], self._rows.shape[1])
+        if not self._h:
+            raise ReferenceError_(1, ref_lib().ref_last_error().decode())
+
+    def query_batch(self, queries, threads: int) -> np.ndarray:
+        q = _f32(queries).reshape(-1, self.dimension)
+        out = np.zeros(q.shape[0], np.uint64)
+        _ref_check(ref_lib().ref_exact_query(self._h, _p(q), q.shape[0], threads,
+                                             _p(out)))
+        return out
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            ref_lib().ref_exact_destroy(self._h)
+            self._h = None
 
 
 def ref_sampled(metric: str, rows, cols, mult, invp, queries, threads: int = 1):

@@ -16,8 +16,11 @@
 #include "hnsvw25/l1/hierarchical/l1_hierarchical_projection.hpp"
 #include "hnsvw25/l2/hierarchical/l2_hierarchical_projection.hpp"
 
+#include <omp.h>
+
 #include <algorithm>
 #include <cstdint>
+#include <memory>
 #include <cstring>
 #include <exception>
 #include <mutex>
@@ -121,6 +124,61 @@ extern "C" {
 const char* ref_last_error(void)
 {
     return g_error.c_str();
+}
+
+// A persistent reference exact index (for timing: the matrix copy stays out of
+// the timed calls). metric 0: ExactL2Index, 1: ExactL1Index.
+struct RefExact {
+    DenseMatrix matrix;
+    std::unique_ptr<ExactL2Index> l2;
+    std::unique_ptr<ExactL1Index> l1;
+};
+
+void* ref_exact_create(int metric, const float* rows, uint64_t r, uint64_t d)
+{
+    try {
+        auto h = std::make_unique<RefExact>();
+        h->matrix = matrix(rows, r, d);
+        if (metric == 0) {
+            h->l2 = std::make_unique<ExactL2Index>(h->matrix);
+        } else {
+            h->l1 = std::make_unique<ExactL1Index>(h->matrix);
+        }
+        return h.release();
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return nullptr;
+    }
+}
+
+void ref_exact_destroy(void* handle)
+{
+    delete static_cast<RefExact*>(handle);
+}
+
+// L2: query_batch with parallel_queries on `threads` OpenMP threads (sequential
+// when threads == 1); L1: query() on `threads` std::threads.
+int ref_exact_query(void* handle, const float* queries, uint64_t n,
+                    int threads, uint64_t* out)
+{
+    return guarded([&] {
+        auto* h = static_cast<RefExact*>(handle);
+        const uint64_t d = h->matrix.cols();
+        if (h->l2) {
+            omp_set_num_threads(std::max(1, threads));
+            std::vector<std::size_t> o(n);
+            h->l2->query_batch(std::span<const float>(queries, n * d), n, o,
+                               threads > 1 ? CpuDenseL2QueryStrategy::parallel_queries
+                                           : CpuDenseL2QueryStrategy::sequential);
+            std::copy(o.begin(), o.end(), out);
+        } else {
+            split(n, threads, [&](uint64_t b, uint64_t e) {
+                for (uint64_t q = b; q < e; ++q) {
+                    out[q] = h->l1->query(std::span<const float>(queries + q * d, d));
+                }
+            });
+        }
+    });
 }
 
 // build_coordinate_sample; engine state after sampling is written to state_out.

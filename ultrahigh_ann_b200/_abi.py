@@ -92,6 +92,7 @@ SIGNATURES = {
                           c_void_p, c_void_p]),
     "uha_workspace_last_stats": (c_int, [c_void_p, POINTER(QueryStats)]),
     "uha_workspace_set_timing": (c_int, [c_void_p, c_int]),
+    "uha_workspace_stream": (c_void_p, [c_void_p]),
     "uha_importance_probabilities": (c_int, [c_int, c_int, c_void_p, c_uint64, c_uint64,
                                               c_void_p, POINTER(ProbabilityReport)]),
     "uha_rng_create": (c_int, [c_uint64, _H]),

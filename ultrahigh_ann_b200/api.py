@@ -346,6 +346,10 @@ class QueryWorkspace:
                 "kernel_launches": s.kernel_launches, "scan_ms": s.scan_ms,
                 "device_ms": s.device_ms}
 
+    def stream_handle(self) -> int:
+        """cudaStream_t of the workspace as an integer."""
+        return int(_abi.load().uha_workspace_stream(self._handle) or 0)
+
     def set_timing(self, enabled: bool) -> None:
         """Records CUDA events around the scan kernel and the device pipeline
         of every query on this workspace (see last_stats())."""

@@ -37,13 +37,28 @@ __device__ __forceinline__ Bounds2 bound_of(float d, Bound b)
     return {fmaxf(0.f, __fsub_rd(d, err)), __fadd_ru(d, err)};
 }
 
+// Sum of the chunk partials of one (query, row) in chunk order. The loads are
+// issued four at a time; the additions keep the sequential order, so finalize
+// and resolve compute bit-identical distances.
 __device__ __forceinline__ float row_distance(const PartialView& v, uint32_t q,
                                               uint32_t row)
 {
+    const uint64_t stride = static_cast<uint64_t>(v.batch) * v.rows;
+    const float* p = v.partials + static_cast<uint64_t>(q) * v.rows + row;
     float d = 0.f;
-    for (uint32_t c = 0; c < v.chunks; ++c) {
-        d += v.partials[(static_cast<uint64_t>(c) * v.batch + q) * v.rows +
-                        row];
+    uint32_t c = 0;
+    for (; c + 4 <= v.chunks; c += 4) {
+        const float a0 = p[(c + 0) * stride];
+        const float a1 = p[(c + 1) * stride];
+        const float a2 = p[(c + 2) * stride];
+        const float a3 = p[(c + 3) * stride];
+        d += a0;
+        d += a1;
+        d += a2;
+        d += a3;
+    }
+    for (; c < v.chunks; ++c) {
+        d += p[c * stride];
     }
     return d;
 }
@@ -100,24 +115,16 @@ __device__ __forceinline__ Summary shfl_summary(const Summary& s, int offset)
     return o;
 }
 
-__global__ void __launch_bounds__(kFinalizeThreads)
-    finalize_certified_kernel(PartialView view, Bound bound, Result* results,
-                              uint32_t* ambiguous, uint32_t* ambiguous_count)
+__device__ Summary block_reduce_summary(Summary s)
 {
-    const uint32_t q = blockIdx.x;
     const float inf = __int_as_float(0x7f800000);
-    Summary s{inf, inf, inf, 0xffffffffu, inf};
-    for (uint32_t row = threadIdx.x; row < view.rows; row += blockDim.x) {
-        const float d = row_distance(view, q, row);
-        const Bounds2 b = bound_of(d, bound);
-        summary_insert(s, b.lower, b.upper, row, d);
-    }
     for (int offset = 16; offset > 0; offset /= 2) {
         s = summary_merge(s, shfl_summary(s, offset));
     }
     __shared__ Summary warp_summaries[kFinalizeThreads / 32];
     const int warp = threadIdx.x / 32;
     const int lane = threadIdx.x % 32;
+    __syncthreads();
     if (lane == 0) {
         warp_summaries[warp] = s;
     }
@@ -129,15 +136,76 @@ __global__ void __launch_bounds__(kFinalizeThreads)
         for (int offset = 16; offset > 0; offset /= 2) {
             s = summary_merge(s, shfl_summary(s, offset));
         }
-        if (lane == 0) {
-            if (s.second > s.min_upper) {
-                results[q] = Result{s.first_row, s.first_distance};
-            } else {
-                const uint32_t slot = atomicAdd(ambiguous_count, 1u);
-                ambiguous[slot] = q;
-                results[q] = Result{0xffffffffu, s.first_distance};
-            }
+    }
+    return s;  // valid in thread 0
+}
+
+__device__ void decide(const Summary& s, uint32_t q, Result* results,
+                       uint32_t* ambiguous, uint32_t* ambiguous_count,
+                       float* query_upper)
+{
+    query_upper[q] = s.min_upper;
+    if (s.second > s.min_upper) {
+        results[q] = Result{s.first_row, s.first_distance};
+    } else {
+        const uint32_t slot = atomicAdd(ambiguous_count, 1u);
+        ambiguous[slot] = q;
+        results[q] = Result{0xffffffffu, s.first_distance};
+    }
+}
+
+// grid = (row blocks, batch). Every CTA summarises kFinalizeThreads rows of
+// one query; the last CTA of a query to finish merges the block summaries.
+__global__ void __launch_bounds__(kFinalizeThreads)
+    finalize_certified_kernel(PartialView view, Bound bound, Result* results,
+                              uint32_t* ambiguous, uint32_t* ambiguous_count,
+                              Summary* block_summaries, uint32_t* done,
+                              float* query_upper)
+{
+    const uint32_t q = blockIdx.y;
+    const uint32_t blocks = gridDim.x;
+    const float inf = __int_as_float(0x7f800000);
+    Summary s{inf, inf, inf, 0xffffffffu, inf};
+    const uint32_t row = blockIdx.x * kFinalizeThreads + threadIdx.x;
+    if (row < view.rows) {
+        const float d = row_distance(view, q, row);
+        const Bounds2 b = bound_of(d, bound);
+        summary_insert(s, b.lower, b.upper, row, d);
+    }
+    s = block_reduce_summary(s);
+    if (blocks == 1) {
+        if (threadIdx.x == 0) {
+            decide(s, q, results, ambiguous, ambiguous_count, query_upper);
         }
+        return;
+    }
+    __shared__ bool is_last;
+    if (threadIdx.x == 0) {
+        block_summaries[static_cast<uint64_t>(q) * blocks + blockIdx.x] = s;
+        __threadfence();
+        is_last = atomicAdd(done + q, 1u) == blocks - 1;
+    }
+    __syncthreads();
+    if (!is_last) {
+        return;
+    }
+    __threadfence();
+    Summary m{inf, inf, inf, 0xffffffffu, inf};
+    for (uint32_t i = threadIdx.x; i < blocks; i += kFinalizeThreads) {
+        const volatile Summary* src =
+            block_summaries + static_cast<uint64_t>(q) * blocks + i;
+        Summary b;
+        b.min_upper = src->min_upper;
+        b.first = src->first;
+        b.second = src->second;
+        b.first_row = src->first_row;
+        b.first_distance = src->first_distance;
+        m = summary_merge(m, b);
+    }
+    m = block_reduce_summary(m);
+    if (threadIdx.x == 0) {
+        decide(m, q, results, ambiguous, ambiguous_count, query_upper);
+        done[q] = 0;
     }
 }
 
@@ -252,7 +320,8 @@ __device__ __forceinline__ bool lex_less(double a, uint32_t ar, double b,
 __global__ void __launch_bounds__(kResolveThreads)
     resolve_kernel(PartialView view, Bound bound, ReplayInputs in,
                    const uint32_t* ambiguous, uint32_t ambiguous_count,
-                   Result* results, double* exact_distances)
+                   const float* query_upper, Result* results,
+                   double* exact_distances)
 {
     const uint32_t slot = blockIdx.x;
     if (slot >= ambiguous_count) {
@@ -262,27 +331,11 @@ __global__ void __launch_bounds__(kResolveThreads)
     const int warp = threadIdx.x / 32;
     const int lane = threadIdx.x % 32;
     constexpr int warps = kResolveThreads / 32;
-    const float inf = __int_as_float(0x7f800000);
 
-    // U* = min over rows of the upper bound (same arithmetic as finalize)
-    float min_upper = inf;
-    for (uint32_t row = threadIdx.x; row < view.rows; row += blockDim.x) {
-        min_upper = fminf(min_upper, bound_of(row_distance(view, q, row), bound).upper);
-    }
-    for (int offset = 16; offset > 0; offset /= 2) {
-        min_upper = fminf(min_upper, __shfl_xor_sync(0xffffffffu, min_upper, offset));
-    }
-    __shared__ float warp_min[warps];
+    // U*: the smallest upper bound over all rows, recorded by finalize
+    const float min_upper = query_upper[q];
     __shared__ double warp_best[warps];
     __shared__ uint32_t warp_best_row[warps];
-    if (lane == 0) {
-        warp_min[warp] = min_upper;
-    }
-    __syncthreads();
-    min_upper = warp_min[0];
-    for (int w = 1; w < warps; ++w) {
-        min_upper = fminf(min_upper, warp_min[w]);
-    }
 
     const float* qrow = in.queries + static_cast<uint64_t>(q) * in.padded_dim;
     double best = __longlong_as_double(0x7ff0000000000000ll);
@@ -324,14 +377,48 @@ __global__ void __launch_bounds__(kResolveThreads)
     }
 }
 
+// Carves the finalize scratch region: per-(query, row block) summaries, the
+// per-query completion counters (zero between calls) and U* per query.
+struct FinalizeScratch {
+    Summary* summaries;
+    uint32_t* done;
+    float* query_upper;
+};
+
+FinalizeScratch finalize_scratch(void* base, uint32_t batch, uint32_t rows)
+{
+    const uint64_t blocks = (rows + kFinalizeThreads - 1) / kFinalizeThreads;
+    char* p = static_cast<char*>(base);
+    FinalizeScratch fs;
+    fs.summaries = reinterpret_cast<Summary*>(p);
+    p += batch * blocks * sizeof(Summary);
+    p = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
+    fs.done = reinterpret_cast<uint32_t*>(p);
+    p += batch * sizeof(uint32_t);
+    p = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
+    fs.query_upper = reinterpret_cast<float*>(p);
+    return fs;
+}
+
 }  // namespace
+
+uint64_t finalize_scratch_bytes(uint64_t batch, uint64_t rows)
+{
+    const uint64_t blocks = (rows + kFinalizeThreads - 1) / kFinalizeThreads;
+    return batch * blocks * sizeof(Summary) + batch * sizeof(uint32_t) +
+           batch * sizeof(float) + 64;
+}
 
 void launch_finalize_certified(PartialView view, Bound bound, Result* results,
                                uint32_t* ambiguous, uint32_t* ambiguous_count,
-                               cudaStream_t stream)
+                               void* scratch, cudaStream_t stream)
 {
-    finalize_certified_kernel<<<view.batch, kFinalizeThreads, 0, stream>>>(
-        view, bound, results, ambiguous, ambiguous_count);
+    const uint32_t blocks = (view.rows + kFinalizeThreads - 1) / kFinalizeThreads;
+    FinalizeScratch fs = finalize_scratch(scratch, view.batch, view.rows);
+    finalize_certified_kernel<<<dim3(blocks, view.batch), kFinalizeThreads, 0,
+                                stream>>>(view, bound, results, ambiguous,
+                                          ambiguous_count, fs.summaries, fs.done,
+                                          fs.query_upper);
     check_cuda(cudaGetLastError(), "cannot launch finalize kernel");
 }
 
@@ -346,14 +433,16 @@ void launch_finalize_gemm(PartialView view, const float* row_norms,
 
 void launch_resolve(PartialView view, Bound bound, ReplayInputs in,
                     const uint32_t* ambiguous, uint32_t ambiguous_count,
-                    Result* results, double* exact_distances,
+                    void* scratch, Result* results, double* exact_distances,
                     cudaStream_t stream)
 {
     if (ambiguous_count == 0) {
         return;
     }
+    FinalizeScratch fs = finalize_scratch(scratch, view.batch, view.rows);
     resolve_kernel<<<ambiguous_count, kResolveThreads, 0, stream>>>(
-        view, bound, in, ambiguous, ambiguous_count, results, exact_distances);
+        view, bound, in, ambiguous, ambiguous_count, fs.query_upper, results,
+        exact_distances);
     check_cuda(cudaGetLastError(), "cannot launch resolve kernel");
 }
 

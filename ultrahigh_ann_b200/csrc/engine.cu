@@ -69,6 +69,7 @@ struct uha_workspace {
     DeviceBuffer<double> exact;
     DeviceBuffer<uint32_t> ambiguous;
     DeviceBuffer<uint32_t> counters;  // [0] ambiguous count, [1] error flag
+    DeviceBuffer<unsigned char> finalize_scratch;
     PinnedBuffer<uha::Result> host_results;
     PinnedBuffer<double> host_exact;
     PinnedBuffer<uint32_t> host_counters;
@@ -552,6 +553,11 @@ extern "C" uha_status uha_workspace_create(const uha_index* index,
         ws->exact.allocate(b);
         ws->ambiguous.allocate(b);
         ws->counters.allocate(2);
+        ws->finalize_scratch.allocate(
+            uha::finalize_scratch_bytes(b, index->rows));
+        check_cuda(cudaMemset(ws->finalize_scratch.get(), 0,
+                              ws->finalize_scratch.bytes()),
+                   "cannot clear finalize scratch");
         ws->host_results.allocate(b);
         ws->host_exact.allocate(b);
         ws->host_counters.allocate(2);
@@ -591,6 +597,12 @@ extern "C" uha_status uha_workspace_info(const uha_workspace* workspace,
             *payload_bytes = workspace->payload_bytes;
         }
     });
+}
+
+extern "C" void* uha_workspace_stream(const uha_workspace* workspace)
+{
+    return workspace == nullptr ? nullptr
+                                : static_cast<void*>(workspace->stream);
 }
 
 extern "C" uha_status uha_workspace_set_timing(uha_workspace* workspace,
@@ -727,7 +739,8 @@ extern "C" uha_status uha_query(const uha_index* index, uha_workspace* ws,
         } else {
             uha::launch_finalize_certified(view, bound, ws->results.get(),
                                            ws->ambiguous.get(),
-                                           ws->counters.get(), stream);
+                                           ws->counters.get(),
+                                           ws->finalize_scratch.get(), stream);
             ++launches;
         }
         check_cuda(cudaMemcpyAsync(ws->host_results.get(), ws->results.get(),
@@ -779,7 +792,8 @@ extern "C" uha_status uha_query(const uha_index* index, uha_workspace* ws,
                 in.op = uha::ReplayOp::l1_grouped4;
             }
             uha::launch_resolve(view, bound, in, ws->ambiguous.get(), ambiguous,
-                                ws->results.get(), ws->exact.get(), stream);
+                                ws->finalize_scratch.get(), ws->results.get(),
+                                ws->exact.get(), stream);
             ++launches;
             replayed.resize(ambiguous);
             check_cuda(cudaMemcpyAsync(replayed.data(), ws->ambiguous.get(),

@@ -77,9 +77,13 @@ void launch_scan(const ScanPlan& plan, ScanOp op, const float* rows,
 // ---- certification
 // Sums partials per (query,row), applies the bound, writes certified results
 // and appends uncertified query ids to `ambiguous` (count in *ambiguous_count).
+// Scratch of the certified finalize/resolve pair (per-query merge state). It
+// must be zero when the workspace is created; finalize leaves its counters at
+// zero after every call.
+uint64_t finalize_scratch_bytes(uint64_t batch, uint64_t rows);
 void launch_finalize_certified(PartialView view, Bound bound, Result* results,
                                uint32_t* ambiguous, uint32_t* ambiguous_count,
-                               cudaStream_t stream);
+                               void* scratch, cudaStream_t stream);
 // Binary32 norm identity (no certification), lowest index on ties.
 void launch_finalize_gemm(PartialView view, const float* row_norms,
                           const float* query_norms, Result* results,
@@ -96,7 +100,7 @@ struct ReplayInputs {
 };
 void launch_resolve(PartialView view, Bound bound, ReplayInputs in,
                     const uint32_t* ambiguous, uint32_t ambiguous_count,
-                    Result* results, double* exact_distances,
+                    void* scratch, Result* results, double* exact_distances,
                     cudaStream_t stream);
 
 // ---- build-time helpers

@@ -60,14 +60,18 @@ def centroid_dataset(classes: int = 33, queries: int = 3013,
 
 def row_dataset(rows: int = 7028, classes: int = 33, queries: int = 8192,
                 d: int = TCGA_DIMENSION, sigma: float = 0.8,
-                zero_fraction: float = 0.4, seed: int = 1) -> Dataset:
+                zero_fraction: float = 0.4, seed: int = 1,
+                query_stream: int = 0) -> Dataset:
     """The row-level workload: every reference row is a latent class centroid
-    plus noise; the masked coordinates stay zero in every row."""
-    rng = np.random.default_rng(seed)
+    plus noise; the masked coordinates stay zero in every row. Queries come
+    from their own random stream, so `query_stream` selects an independent
+    query set over the same rows (one per replica in a multi-GPU run)."""
+    rng = np.random.default_rng([seed, 0])
     cent, mask = _centroids(rng, classes, d, zero_fraction)
     row_labels = rng.integers(0, classes, size=rows)
     r = _noisy(rng, cent, row_labels, sigma)
     r[:, mask] = 0.0
-    q_labels = rng.integers(0, classes, size=queries)
-    q = _noisy(rng, cent, q_labels, sigma)
+    qrng = np.random.default_rng([seed, 1, query_stream])
+    q_labels = qrng.integers(0, classes, size=queries)
+    q = _noisy(qrng, cent, q_labels, sigma)
     return Dataset(r, q, q_labels, row_labels)
