@@ -378,7 +378,9 @@ __global__ void __launch_bounds__(kResolveThreads)
 }
 
 // Carves the finalize scratch region: per-(query, row block) summaries, the
-// per-query completion counters (zero between calls) and U* per query.
+// per-query completion counters (zero between calls) and U* per query. The
+// layout depends only on the workspace capacity, never on the batch of one
+// call, so the counters stay at fixed addresses across calls.
 struct FinalizeScratch {
     Summary* summaries;
     uint32_t* done;
@@ -411,10 +413,12 @@ uint64_t finalize_scratch_bytes(uint64_t batch, uint64_t rows)
 
 void launch_finalize_certified(PartialView view, Bound bound, Result* results,
                                uint32_t* ambiguous, uint32_t* ambiguous_count,
-                               void* scratch, cudaStream_t stream)
+                               void* scratch, uint64_t capacity,
+                               cudaStream_t stream)
 {
     const uint32_t blocks = (view.rows + kFinalizeThreads - 1) / kFinalizeThreads;
-    FinalizeScratch fs = finalize_scratch(scratch, view.batch, view.rows);
+    FinalizeScratch fs = finalize_scratch(scratch, static_cast<uint32_t>(capacity),
+                                          view.rows);
     finalize_certified_kernel<<<dim3(blocks, view.batch), kFinalizeThreads, 0,
                                 stream>>>(view, bound, results, ambiguous,
                                           ambiguous_count, fs.summaries, fs.done,
@@ -433,13 +437,14 @@ void launch_finalize_gemm(PartialView view, const float* row_norms,
 
 void launch_resolve(PartialView view, Bound bound, ReplayInputs in,
                     const uint32_t* ambiguous, uint32_t ambiguous_count,
-                    void* scratch, Result* results, double* exact_distances,
-                    cudaStream_t stream)
+                    void* scratch, uint64_t capacity, Result* results,
+                    double* exact_distances, cudaStream_t stream)
 {
     if (ambiguous_count == 0) {
         return;
     }
-    FinalizeScratch fs = finalize_scratch(scratch, view.batch, view.rows);
+    FinalizeScratch fs = finalize_scratch(scratch, static_cast<uint32_t>(capacity),
+                                          view.rows);
     resolve_kernel<<<ambiguous_count, kResolveThreads, 0, stream>>>(
         view, bound, in, ambiguous, ambiguous_count, fs.query_upper, results,
         exact_distances);

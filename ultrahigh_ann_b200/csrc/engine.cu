@@ -740,7 +740,8 @@ extern "C" uha_status uha_query(const uha_index* index, uha_workspace* ws,
             uha::launch_finalize_certified(view, bound, ws->results.get(),
                                            ws->ambiguous.get(),
                                            ws->counters.get(),
-                                           ws->finalize_scratch.get(), stream);
+                                           ws->finalize_scratch.get(),
+                                           ws->max_batch, stream);
             ++launches;
         }
         check_cuda(cudaMemcpyAsync(ws->host_results.get(), ws->results.get(),
@@ -792,8 +793,8 @@ extern "C" uha_status uha_query(const uha_index* index, uha_workspace* ws,
                 in.op = uha::ReplayOp::l1_grouped4;
             }
             uha::launch_resolve(view, bound, in, ws->ambiguous.get(), ambiguous,
-                                ws->finalize_scratch.get(), ws->results.get(),
-                                ws->exact.get(), stream);
+                                ws->finalize_scratch.get(), ws->max_batch,
+                                ws->results.get(), ws->exact.get(), stream);
             ++launches;
             replayed.resize(ambiguous);
             check_cuda(cudaMemcpyAsync(replayed.data(), ws->ambiguous.get(),

@@ -81,9 +81,12 @@ void launch_scan(const ScanPlan& plan, ScanOp op, const float* rows,
 // must be zero when the workspace is created; finalize leaves its counters at
 // zero after every call.
 uint64_t finalize_scratch_bytes(uint64_t batch, uint64_t rows);
+// `capacity` is the batch capacity the scratch was sized for
+// (finalize_scratch_bytes); view.batch may be smaller.
 void launch_finalize_certified(PartialView view, Bound bound, Result* results,
                                uint32_t* ambiguous, uint32_t* ambiguous_count,
-                               void* scratch, cudaStream_t stream);
+                               void* scratch, uint64_t capacity,
+                               cudaStream_t stream);
 // Binary32 norm identity (no certification), lowest index on ties.
 void launch_finalize_gemm(PartialView view, const float* row_norms,
                           const float* query_norms, Result* results,
@@ -100,8 +103,8 @@ struct ReplayInputs {
 };
 void launch_resolve(PartialView view, Bound bound, ReplayInputs in,
                     const uint32_t* ambiguous, uint32_t ambiguous_count,
-                    void* scratch, Result* results, double* exact_distances,
-                    cudaStream_t stream);
+                    void* scratch, uint64_t capacity, Result* results,
+                    double* exact_distances, cudaStream_t stream);
 
 // ---- build-time helpers
 void launch_gather_rows(const float* source, uint64_t row_count, uint64_t dim,
