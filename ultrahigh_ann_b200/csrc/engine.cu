@@ -8,6 +8,7 @@
 // on the workspace's own stream. The resolve step runs only when the
 // finalize kernel reported uncertified queries.
 #include "common.h"
+#include "index_types.h"
 #include "kernels.h"
 
 #include <algorithm>
@@ -26,69 +27,9 @@ using uha::fail;
 using uha::guarded;
 using uha::PinnedBuffer;
 
-namespace {
-
-enum class IndexKind { exact, weighted, sampled };
-
-constexpr uint64_t kColumnAlign = 4;  // padded row length: 16-byte multiple
-constexpr uint64_t kMaxExtent = 0x7fffffffull;
-
-}  // namespace
-
-struct uha_index {
-    int device = 0;
-    std::string device_name;
-    int sm_count = 148;
-    IndexKind kind = IndexKind::exact;
-    uha_metric metric = UHA_L2;
-    uint64_t rows = 0;
-    uint64_t dimension = 0;   // original query dimension d
-    uint64_t scan_dim = 0;    // columns scanned (d or k)
-    uint64_t padded_dim = 0;  // scan_dim rounded up to kColumnAlign
-    uint64_t sample_size = 0;
-    uint64_t sampled_multiplicity = 0;
-    DeviceBuffer<float> scan_rows;   // rows x padded_dim
-    DeviceBuffer<float> row_norms;   // rows (L2, norm-identity strategy)
-    DeviceBuffer<float> weights32;   // padded_dim (weighted L1 scan)
-    DeviceBuffer<double> weights64;  // scan_dim (weighted L1 replay)
-    DeviceBuffer<uint32_t> columns;  // sample_size (sampled)
-    DeviceBuffer<float> scales;      // sample_size (sampled L2)
-    uha_space_usage usage{};
-};
-
-struct uha_workspace {
-    const uha_index* owner = nullptr;
-    uint64_t max_batch = 0;
-    uint64_t payload_bytes = 0;
-    cudaStream_t stream = nullptr;
-    DeviceBuffer<float> raw_queries;
-    DeviceBuffer<float> prepared;
-    DeviceBuffer<float> query_norms;
-    DeviceBuffer<float> partials;
-    DeviceBuffer<uha::Result> results;
-    DeviceBuffer<double> exact;
-    DeviceBuffer<uint32_t> ambiguous;
-    DeviceBuffer<uint32_t> counters;  // [0] ambiguous count, [1] error flag
-    DeviceBuffer<unsigned char> finalize_scratch;
-    PinnedBuffer<uha::Result> host_results;
-    PinnedBuffer<double> host_exact;
-    PinnedBuffer<uint32_t> host_counters;
-    uha_query_stats last{};
-    bool timing = false;
-    cudaEvent_t events[4] = {nullptr, nullptr, nullptr, nullptr};
-
-    ~uha_workspace()
-    {
-        for (cudaEvent_t e : events) {
-            if (e != nullptr) {
-                cudaEventDestroy(e);
-            }
-        }
-        if (stream != nullptr) {
-            cudaStreamDestroy(stream);
-        }
-    }
-};
+using uha::IndexKind;
+using uha::kColumnAlign;
+using uha::kMaxExtent;
 
 namespace {
 
@@ -190,10 +131,14 @@ uint64_t workspace_payload(const uha_index& index, uint64_t b)
     return 0;
 }
 
+}  // namespace
+
+namespace uha {
+
 // Relative and absolute certification bound for a binary32 distance built
 // from per-term relative error (1 + u)^term_roundings and `depth` sequential
 // binary32 additions, against the CPU's binary64 sum over `terms` terms.
-uha::Bound make_bound(uint32_t depth, uint64_t terms, int term_roundings)
+Bound make_bound(uint32_t depth, uint64_t terms, int term_roundings)
 {
     const double u32 = std::ldexp(1.0, -24);
     const double u64 = std::ldexp(1.0, -53);
@@ -203,13 +148,15 @@ uha::Bound make_bound(uint32_t depth, uint64_t terms, int term_roundings)
     const double g64 = n64 * u64 / (1.0 - n64 * u64);
     const double rel = 1.01 * (g32 + g64) / (1.0 - g32) + 4 * u32;
     const double abs = std::ldexp(n32 + 4, -149) * 4;
-    return uha::Bound{
+    return Bound{
         std::nextafter(static_cast<float>(rel), 1.0f),
         std::max(static_cast<float>(abs), std::ldexp(1.0f, -140)),
     };
 }
 
-}  // namespace
+}  // namespace uha
+
+using uha::make_bound;
 
 // ------------------------------------------------------------------ device
 

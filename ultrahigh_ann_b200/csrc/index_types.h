@@ -1,0 +1,78 @@
+// Internal definitions of the opaque C-ABI handles (uha_index,
+// uha_workspace) shared by the engine's translation units.
+#pragma once
+
+#include "common.h"
+#include "kernels.h"
+
+#include <cstdint>
+#include <string>
+
+namespace uha {
+
+enum class IndexKind { exact, weighted, sampled };
+
+constexpr uint64_t kColumnAlign = 4;  // padded row length: 16-byte multiple
+constexpr uint64_t kMaxExtent = 0x7fffffffull;
+
+// Relative and absolute certification bound for a binary32 distance (defined
+// in engine.cu).
+Bound make_bound(uint32_t depth, uint64_t terms, int term_roundings);
+
+}  // namespace uha
+
+struct uha_index {
+    int device = 0;
+    std::string device_name;
+    int sm_count = 148;
+    uha::IndexKind kind = uha::IndexKind::exact;
+    uha_metric metric = UHA_L2;
+    uint64_t rows = 0;
+    uint64_t dimension = 0;   // original query dimension d
+    uint64_t scan_dim = 0;    // columns scanned (d or k)
+    uint64_t padded_dim = 0;  // scan_dim rounded up to kColumnAlign
+    uint64_t sample_size = 0;
+    uint64_t sampled_multiplicity = 0;
+    uha::DeviceBuffer<float> scan_rows;   // rows x padded_dim
+    uha::DeviceBuffer<float> row_norms;   // rows (L2, norm-identity strategy)
+    uha::DeviceBuffer<float> weights32;   // padded_dim (weighted L1 scan)
+    uha::DeviceBuffer<double> weights64;  // scan_dim (weighted L1 replay)
+    uha::DeviceBuffer<uint32_t> columns;  // sample_size (sampled)
+    uha::DeviceBuffer<float> scales;      // sample_size (sampled L2)
+    uha_space_usage usage{};
+};
+
+struct uha_workspace {
+    const uha_index* owner = nullptr;
+    uint64_t max_batch = 0;
+    uint64_t payload_bytes = 0;
+    cudaStream_t stream = nullptr;
+    uha::DeviceBuffer<float> raw_queries;
+    uha::DeviceBuffer<float> prepared;
+    uha::DeviceBuffer<float> query_norms;
+    uha::DeviceBuffer<float> partials;
+    uha::DeviceBuffer<uha::Result> results;
+    uha::DeviceBuffer<double> exact;
+    uha::DeviceBuffer<uint32_t> ambiguous;
+    uha::DeviceBuffer<uint32_t> counters;  // [0] ambiguous count, [1] error flag
+    uha::DeviceBuffer<unsigned char> finalize_scratch;
+    uha::PinnedBuffer<uha::Result> host_results;
+    uha::PinnedBuffer<double> host_exact;
+    uha::PinnedBuffer<uint32_t> host_counters;
+    uha_query_stats last{};
+    bool timing = false;
+    cudaEvent_t events[4] = {nullptr, nullptr, nullptr, nullptr};
+
+    ~uha_workspace()
+    {
+        for (cudaEvent_t e : events) {
+            if (e != nullptr) {
+                cudaEventDestroy(e);
+            }
+        }
+        if (stream != nullptr) {
+            cudaStreamDestroy(stream);
+        }
+    }
+};
+
