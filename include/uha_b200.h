@@ -199,6 +199,29 @@ uha_status uha_query(const uha_index* index, uha_workspace* workspace,
                      int queries_on_device, uha_strategy strategy,
                      uint64_t* out_indices, double* out_distances);
 
+/* Certified query of at most 8 device-resident queries that allocates no
+ * memory: no workspace, no cudaMalloc/cudaFree, no allocating library call.
+ * It has no counterpart in the reference; it exists for callers that cannot
+ * allocate while they answer queries (a server whose device memory is
+ * reserved up front by its own pool, code that must not allocate while other
+ * threads capture CUDA graphs, embedded callers with a fixed footprint).
+ * `queries` is a device pointer to query_count x dimension floats on the
+ * index's device; out_indices (uint64_t) and out_distances (double, nullable)
+ * are device pointers with query_count entries; `stream` is the cudaStream_t
+ * to run on (NULL: the legacy default stream). The call returns after the
+ * results are written (it synchronises `stream`). Results and errors equal
+ * uha_query's with UHA_DIRECT.
+ * Scratch: one static 32 MiB device array per GPU that loads the library,
+ * held until the process exits. The first call on a device resolves its
+ * address (cudaGetSymbolAddress) and keeps it; make that first call before
+ * any stream capture. Batches whose scratch would exceed 32 MiB, or more than
+ * 8 queries, fail with UHA_LENGTH_ERROR. All calls share the array: calls
+ * that overlap on the GPU (other threads, other streams) race and must be
+ * serialised by the caller. */
+uha_status uha_query_noalloc(const uha_index* index, const float* queries,
+                             uint64_t query_count, uint64_t* out_indices,
+                             double* out_distances, void* stream);
+
 /* Diagnostics of the last uha_query on this workspace. */
 uha_status uha_workspace_last_stats(const uha_workspace* workspace,
                                     uha_query_stats* out);
