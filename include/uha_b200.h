@@ -158,6 +158,26 @@ uha_status uha_sampled_index_create(int device, uha_metric metric,
                                     const double* inverse_probabilities,
                                     uint64_t sample_size, uha_index** out);
 
+/* Hierarchical index: sampled coordinates plus a p x k binary64 projection
+ * (Rademacher-JL for L2, Cauchy for L1) drawn on the host with the
+ * reference's random sequence (uha_jl_matrix / uha_cauchy_matrix). Projected
+ * rows are formed on the device in binary64 with the reference's summation
+ * order. Replaces CudaHierarchicalL{1,2}AnnIndex(const DenseMatrix&,
+ * CoordinateSample, std::size_t, std::mt19937_64&, int)
+ * (include/ultrahigh_ann/hnsvw25/l2/hierarchical/cuda_hierarchical_l2_ann_index.hpp:70-73,
+ *  l1/hierarchical/cuda_hierarchical_l1_ann_index.hpp:74-77). */
+uha_status uha_hierarchical_index_create(int device, uha_metric metric,
+                                         const float* rows,
+                                         uint64_t row_count,
+                                         uint64_t dimension,
+                                         const uint64_t* columns,
+                                         const uint64_t* multiplicities,
+                                         const double* inverse_probabilities,
+                                         uint64_t sample_size,
+                                         const double* projection,
+                                         uint64_t projection_dimension,
+                                         uha_index** out);
+
 void uha_index_destroy(uha_index* index);
 
 /* Replaces space_usage() of every CUDA index class, with the reference byte
@@ -199,8 +219,8 @@ uha_status uha_query(const uha_index* index, uha_workspace* workspace,
                      int queries_on_device, uha_strategy strategy,
                      uint64_t* out_indices, double* out_distances);
 
-/* Certified query of at most 8 device-resident queries that allocates no
- * memory: no workspace, no cudaMalloc/cudaFree, no allocating library call.
+/* Certified query of at most 8 device-resident queries against an exact or
+ * flat index that allocates no memory: no workspace, no cudaMalloc/cudaFree, no allocating library call.
  * It has no counterpart in the reference; it exists for callers that cannot
  * allocate while they answer queries (a server whose device memory is
  * reserved up front by its own pool, code that must not allocate while other
@@ -249,6 +269,17 @@ uha_status uha_importance_probabilities(int device, uha_metric metric,
                                         uint64_t dimension,
                                         double* out_probabilities,
                                         uha_probability_report* report);
+
+/* The same probabilities on the host cores with the reference CPU policies'
+ * binary64 arithmetic, bit-identical to its sequential loop for any thread
+ * count. Replaces the sequential / cpu_parallel policies of
+ * compute_l{1,2}_importance_probabilities (src/hnsvw25/l2/
+ * importance_sampling.cpp:126-144, src/hnsvw25/l1/importance_sampling.cpp:115-134). */
+uha_status uha_importance_probabilities_host(uha_metric metric,
+                                             const float* rows,
+                                             uint64_t row_count,
+                                             uint64_t dimension, int threads,
+                                             double* out_probabilities);
 
 /* std::mt19937_64 engine shared by the host-side draws below, so that one
  * engine passes through sampling and projection in the reference order. */

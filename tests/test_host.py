@@ -115,3 +115,21 @@ def test_golden_inputs_are_consistent():
     rows, queries = golden_inputs()
     assert rows.dtype == np.float32 and queries.dtype == np.float32
     assert rows.shape[1] == queries.shape[1]
+
+
+@pytest.mark.parametrize("threads", [1, 3, 8])
+def test_host_probabilities_are_the_reference_cpu_policy(threads):
+    rows, _ = golden_inputs()
+    for metric in ("l2", "l1"):
+        p = uha.compute_importance_probabilities_host(metric, rows, threads)
+        assert np.array_equal(p, golden(f"probabilities_{metric}")["probabilities"])
+
+
+def test_host_probabilities_edge_cases():
+    one = np.ones((1, 5), np.float32)
+    assert np.array_equal(uha.compute_importance_probabilities_host("l2", one), np.zeros(5))
+    same = np.ones((3, 4), np.float32)  # every pair at distance zero is skipped
+    assert np.array_equal(uha.compute_importance_probabilities_host("l1", same), np.zeros(4))
+    with pytest.raises(uha.InvalidArgument):
+        uha.compute_importance_probabilities_host(
+            "l2", np.array([[np.nan, 0.0], [1.0, 1.0]], np.float32))

@@ -82,6 +82,9 @@ SIGNATURES = {
     "uha_weighted_l1_index_create": (c_int, [c_int, c_void_p, c_uint64, c_uint64, c_void_p, _H]),
     "uha_sampled_index_create": (c_int, [c_int, c_int, c_void_p, c_uint64, c_uint64,
                                           c_void_p, c_void_p, c_void_p, c_uint64, _H]),
+    "uha_hierarchical_index_create": (c_int, [c_int, c_int, c_void_p, c_uint64, c_uint64,
+                                               c_void_p, c_void_p, c_void_p, c_uint64,
+                                               c_void_p, c_uint64, _H]),
     "uha_index_destroy": (None, [c_void_p]),
     "uha_index_space_usage": (c_int, [c_void_p, POINTER(SpaceUsage)]),
     "uha_index_device": (c_int, [c_void_p, POINTER(c_int), c_char_p, c_uint64]),
@@ -97,6 +100,8 @@ SIGNATURES = {
     "uha_workspace_stream": (c_void_p, [c_void_p]),
     "uha_importance_probabilities": (c_int, [c_int, c_int, c_void_p, c_uint64, c_uint64,
                                               c_void_p, POINTER(ProbabilityReport)]),
+    "uha_importance_probabilities_host": (c_int, [c_int, c_void_p, c_uint64, c_uint64,
+                                                   c_int, c_void_p]),
     "uha_rng_create": (c_int, [c_uint64, _H]),
     "uha_rng_destroy": (None, [c_void_p]),
     "uha_rng_state": (c_int, [c_void_p, c_char_p, c_uint64, _U]),

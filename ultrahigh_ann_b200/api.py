@@ -544,16 +544,46 @@ class CudaSampledCoordinateL1AnnIndex(_CudaSampledIndex):
                                    QueryStrategy.direct, distances)
 
 
+def compute_importance_probabilities_host(metric: str, representatives,
+                                          threads: int = 0) -> np.ndarray:
+    """The reference CPU policies' probabilities on the host cores
+    (bit-identical to its sequential loop for any thread count)."""
+    import os
+    rows = _matrix(representatives)
+    out = np.zeros(rows.shape[1], dtype=np.float64)
+    _check(_abi.load().uha_importance_probabilities_host(
+        _abi.L2 if metric == "l2" else _abi.L1, _ptr(rows), rows.shape[0],
+        rows.shape[1], int(threads or os.cpu_count() or 1), _ptr(out)))
+    return out
+
+
+def compute_l2_importance_probabilities(representatives,
+                                        execution_policy=ExecutionPolicy.sequential,
+                                        device: int = 0) -> np.ndarray:
+    """include/ultrahigh_ann/hnsvw25/l2/importance_sampling.hpp:56-58."""
+    return _probabilities_for(_abi.L2, _matrix(representatives), execution_policy,
+                              device)
+
+
+def compute_l1_importance_probabilities(representatives,
+                                        execution_policy=ExecutionPolicy.sequential,
+                                        device: int = 0) -> np.ndarray:
+    """include/ultrahigh_ann/hnsvw25/l1/importance_sampling.hpp:52-57."""
+    return _probabilities_for(_abi.L1, _matrix(representatives), execution_policy,
+                              device)
+
+
 def _probabilities_for(metric: int, rows: np.ndarray, policy: ExecutionPolicy,
                        device: int) -> np.ndarray:
     if policy in (ExecutionPolicy.gpu_fp32, ExecutionPolicy.gpu_cublas_fp32):
         if metric == _abi.L1 and policy == ExecutionPolicy.gpu_cublas_fp32:
             raise InvalidArgument("gpu_cublas_fp32 is unavailable for L1 probability "
-                                  "computation")
+                                  "computation; L1 distance has no "
+                                  "matrix-multiplication identity")
         return _probabilities_gpu(metric, rows, device).probabilities
-    raise InvalidArgument(
-        "CPU probability policies belong to the reference CPU library; pass "
-        "importance_probabilities computed there instead")
+    threads = 1 if policy == ExecutionPolicy.sequential else 0
+    return compute_importance_probabilities_host(
+        "l2" if metric == _abi.L2 else "l1", rows, threads)
 
 
 class CudaFlatL2AnnIndex(CudaSampledCoordinateL2AnnIndex):
@@ -574,11 +604,13 @@ class CudaFlatL2AnnIndex(CudaSampledCoordinateL2AnnIndex):
 
 
 class CudaFlatL1AnnIndex(CudaSampledCoordinateL1AnnIndex):
-    """include/ultrahigh_ann/hnsvw25/l1/flat/cuda_l1_ann_index.hpp:15-50."""
+    """include/ultrahigh_ann/hnsvw25/l1/flat/cuda_l1_ann_index.hpp:15-50. The
+    convenience constructor's default probability policy is sequential
+    (src/hnsvw25/l1/flat/cuda_l1_ann_index.cpp:39-46)."""
 
     def __init__(self, input, repetitions: int, random_engine: MT19937_64,
                  device: int = 0,
-                 probability_execution_policy: ExecutionPolicy = ExecutionPolicy.gpu_fp32,
+                 probability_execution_policy: ExecutionPolicy = ExecutionPolicy.sequential,
                  *, importance_probabilities=None):
         rows = _matrix(input)
         if importance_probabilities is None:
@@ -586,3 +618,68 @@ class CudaFlatL1AnnIndex(CudaSampledCoordinateL1AnnIndex):
                 _abi.L1, rows, probability_execution_policy, device)
         super().__init__(rows, importance_probabilities, repetitions, random_engine,
                          device)
+
+
+class _CudaHierarchicalIndex(_CudaIndex):
+    _metric = _abi.L2
+
+    def __init__(self, input, repetitions=None, projection_dimension=None,
+                 random_engine=None, device: int = 0,
+                 probability_execution_policy: Optional[ExecutionPolicy] = None, *,
+                 importance_probabilities=None, coordinate_sample=None):
+        rows = _matrix(input)
+        if rows.shape[0] == 0:
+            raise InvalidArgument(
+                "hierarchical index expects at least one representative")
+        if projection_dimension is None or int(projection_dimension) <= 0:
+            raise InvalidArgument("projection_dimension has to be a positive integer")
+        if random_engine is None:
+            raise InvalidArgument("a random engine is required")
+        if coordinate_sample is not None:
+            sample = (coordinate_sample if isinstance(coordinate_sample,
+                                                      CoordinateSample)
+                      else CoordinateSample.from_columns(coordinate_sample))
+        else:
+            if importance_probabilities is None:
+                policy = probability_execution_policy or self._default_policy
+                importance_probabilities = _probabilities_for(self._metric, rows,
+                                                              policy, device)
+            sample = _resolve_sample(rows, importance_probabilities, repetitions,
+                                     random_engine, None)
+        if len(sample) == 0 and rows.shape[0] > 1:
+            raise CudaRuntimeError("importance sampling selected no coordinates")
+        p = int(projection_dimension)
+        draw = build_jl_matrix if self._metric == _abi.L2 else build_cauchy_matrix
+        matrix = draw(sample, p, random_engine)
+        handle = ctypes.c_void_p()
+        _check(_abi.load().uha_hierarchical_index_create(
+            device, self._metric, _ptr(rows), rows.shape[0], rows.shape[1],
+            _ptr(sample.source_columns), _ptr(sample.multiplicities),
+            _ptr(sample.inverse_probabilities), len(sample), _ptr(matrix), p,
+            ctypes.byref(handle)))
+        self._adopt(handle, rows.shape[1])
+        self.coordinate_sample = sample
+        self.projection = matrix
+
+
+class CudaHierarchicalL2AnnIndex(_CudaHierarchicalIndex):
+    """include/ultrahigh_ann/hnsvw25/l2/hierarchical/cuda_hierarchical_l2_ann_index.hpp:33-104:
+    sampled coordinates, Rademacher-JL projection to p coordinates, squared-L2
+    scan of the projected rows. Default probability policy gpu_fp32."""
+
+    _metric = _abi.L2
+    _default_policy = ExecutionPolicy.gpu_fp32
+
+
+class CudaHierarchicalL1AnnIndex(_CudaHierarchicalIndex):
+    """include/ultrahigh_ann/hnsvw25/l1/hierarchical/cuda_hierarchical_l1_ann_index.hpp:34-108:
+    sampled coordinates, Cauchy projection, median-|diff| scan. Default
+    probability policy sequential (cuda_hierarchical_l1_ann_index.cpp:221-228)."""
+
+    _metric = _abi.L1
+    _default_policy = ExecutionPolicy.sequential
+
+    def query_batch(self, queries, query_count, output, workspace,
+                    strategy=QueryStrategy.direct, distances=None):
+        return super().query_batch(queries, query_count, output, workspace,
+                                   QueryStrategy.direct, distances)

@@ -27,14 +27,33 @@ struct Bounds2 {
     float upper;
 };
 
-__device__ __forceinline__ Bounds2 bound_of(float d, Bound b)
+__device__ __forceinline__ Bounds2 bound_of(float d, const Bound& b,
+                                            uint32_t row, uint32_t q)
 {
+    const float inf = __int_as_float(0x7f800000);
     if (!(d <= FLT_MAX)) {
-        // binary32 overflow: the true distance is at least of order FLT_MAX
-        return {1.0e38f, __int_as_float(0x7f800000)};
+        // binary32 overflow: no finite upper bound; every row below stays a
+        // candidate and the replay decides
+        return {0.f, inf};
     }
-    const float err = __fadd_ru(__fmul_ru(b.rel, d), b.abs);
-    return {fmaxf(0.f, __fsub_rd(d, err)), __fadd_ru(d, err)};
+    if (b.mode == BoundMode::plain) {
+        const float err = __fadd_ru(__fmul_ru(b.rel, d), b.abs);
+        return {fmaxf(0.f, __fsub_rd(d, err)), __fadd_ru(d, err)};
+    }
+    const float e = __fadd_ru(b.row_err[row], b.query_err[q]);
+    if (b.mode == BoundMode::median) {
+        const float err = __fadd_ru(__fadd_ru(__fmul_ru(b.rel, d), e), b.abs);
+        return {fmaxf(0.f, __fsub_rd(d, err)), __fadd_ru(d, err)};
+    }
+    // projected_l2: ||a|| within e of ||b|| (triangle inequality on the
+    // projected difference vectors)
+    const float lo_root =
+        fmaxf(0.f, __fsub_rd(__fsqrt_rd(__fmul_rd(d, __fsub_rd(1.f, b.rel))), e));
+    const float hi_root =
+        __fadd_ru(__fsqrt_ru(__fmul_ru(d, __fadd_ru(1.f, b.rel))), e);
+    const float lo = __fmul_rd(__fmul_rd(lo_root, lo_root), __fsub_rd(1.f, b.cpu_rel));
+    const float hi = __fmul_ru(__fmul_ru(hi_root, hi_root), __fadd_ru(1.f, b.cpu_rel));
+    return {fmaxf(0.f, __fsub_rd(lo, b.abs)), __fadd_ru(hi, b.abs)};
 }
 
 // Sum of the chunk partials of one (query, row) in chunk order. The loads are
@@ -169,7 +188,7 @@ __global__ void __launch_bounds__(kFinalizeThreads)
     const uint32_t row = blockIdx.x * kFinalizeThreads + threadIdx.x;
     if (row < view.rows) {
         const float d = row_distance(view, q, row);
-        const Bounds2 b = bound_of(d, bound);
+        const Bounds2 b = bound_of(d, bound, row, q);
         summary_insert(s, b.lower, b.upper, row, d);
     }
     s = block_reduce_summary(s);
@@ -311,6 +330,72 @@ __device__ double replay_row(const ReplayInputs& in, const float* qrow,
     return s;
 }
 
+// Reference binary64 squared distance between a projected row and the
+// projected query (hierarchical_l2_ann_index.cpp:63-77): s += (r_j - y_j)^2
+// in j order.
+__device__ double replay_projected_l2(const double* row, const double* y,
+                                      uint64_t p, int lane)
+{
+    double s = 0.0;
+    for (uint64_t base = 0; base < p; base += 32) {
+        const uint64_t j = base + lane;
+        double t = 0.0;
+        if (j < p) {
+            const double diff = __dsub_rn(row[j], y[j]);
+            t = __dmul_rn(diff, diff);
+        }
+        const uint64_t n = p - base < 32 ? p - base : 32;
+        for (uint64_t i = 0; i < n; ++i) {
+            s = __dadd_rn(s, __shfl_sync(0xffffffffu, t, static_cast<int>(i)));
+        }
+    }
+    return s;
+}
+
+// Number of j < p with |row_j - y_j| (as binary64 bits) below `bound`.
+__device__ uint32_t count_below(const double* row, const double* y, uint64_t p,
+                                unsigned long long bound, int lane)
+{
+    uint32_t c = 0;
+    for (uint64_t j = lane; j < p; j += 32) {
+        const unsigned long long bits = static_cast<unsigned long long>(
+            __double_as_longlong(fabs(__dsub_rn(row[j], y[j]))));
+        c += bits < bound ? 1u : 0u;
+    }
+    return __reduce_add_sync(0xffffffffu, c);
+}
+
+// The k-th smallest (0-based) |row_j - y_j|: binary search on the bit pattern
+// (nonnegative binary64 values order like their bits).
+__device__ double select_abs_diff(const double* row, const double* y,
+                                  uint64_t p, uint32_t k, int lane)
+{
+    unsigned long long prefix = 0;
+    for (int bit = 62; bit >= 0; --bit) {
+        const unsigned long long trial = prefix | (1ull << bit);
+        if (count_below(row, y, p, trial, lane) <= k) {
+            prefix = trial;
+        }
+    }
+    return __longlong_as_double(static_cast<long long>(prefix));
+}
+
+// Reference median of |r_j - y_j| with the even-p midpoint
+// (hierarchical_l1_ann_index.cpp:65-99): nth_element puts the (p/2)-th
+// smallest at the upper middle; the lower middle is the largest of the
+// smaller half; median = lower + (upper - lower) * 0.5.
+__device__ double replay_median(const double* row, const double* y, uint64_t p,
+                                int lane)
+{
+    const uint32_t mid = static_cast<uint32_t>(p / 2);
+    const double upper = select_abs_diff(row, y, p, mid, lane);
+    if (p % 2 != 0) {
+        return upper;
+    }
+    const double lower = select_abs_diff(row, y, p, mid - 1, lane);
+    return __dadd_rn(lower, __dmul_rn(__dsub_rn(upper, lower), 0.5));
+}
+
 __device__ __forceinline__ bool lex_less(double a, uint32_t ar, double b,
                                          uint32_t br)
 {
@@ -338,22 +423,49 @@ __global__ void __launch_bounds__(kResolveThreads)
     __shared__ uint32_t warp_best_row[warps];
 
     const float* qrow = in.queries + static_cast<uint64_t>(q) * in.padded_dim;
+    const bool projected = in.op == ReplayOp::l2_projected ||
+                           in.op == ReplayOp::median_projected;
+    extern __shared__ double projected_query[];
+    if (projected) {
+        // the reference's binary64 query projection
+        // (l2_hierarchical_projection.cpp:186-198): y_j = sum_i double(x_i) *
+        // P[j][i] in i order, one thread per j
+        for (uint64_t j = threadIdx.x; j < in.proj_dim; j += blockDim.x) {
+            const double* coeff = in.projection64 + j * in.dim;
+            double y = 0.0;
+            for (uint64_t i = 0; i < in.dim; ++i) {
+                y = __dadd_rn(y, __dmul_rn(static_cast<double>(qrow[i]), coeff[i]));
+            }
+            projected_query[j] = y;
+        }
+        __syncthreads();
+    }
     double best = __longlong_as_double(0x7ff0000000000000ll);
     uint32_t best_row = 0xffffffffu;
     for (uint32_t base = warp * 32; base < view.rows; base += warps * 32) {
         const uint32_t row = base + lane;
         bool candidate = false;
         if (row < view.rows) {
-            candidate = bound_of(row_distance(view, q, row), bound).lower <= min_upper;
+            candidate = bound_of(row_distance(view, q, row), bound, row, q).lower <=
+                        min_upper;
         }
         unsigned int mask = __ballot_sync(0xffffffffu, candidate);
         while (mask != 0u) {
             const int bit = __ffs(mask) - 1;
             mask &= mask - 1u;
             const uint32_t crow = base + bit;
-            const double s = replay_row(
-                in, qrow, in.rows + static_cast<uint64_t>(crow) * in.padded_dim,
-                lane);
+            double s;
+            if (in.op == ReplayOp::l2_projected) {
+                s = replay_projected_l2(in.rows64 + crow * in.proj_dim,
+                                        projected_query, in.proj_dim, lane);
+            } else if (in.op == ReplayOp::median_projected) {
+                s = replay_median(in.rows64 + crow * in.proj_dim,
+                                  projected_query, in.proj_dim, lane);
+            } else {
+                s = replay_row(in, qrow,
+                               in.rows + static_cast<uint64_t>(crow) * in.padded_dim,
+                               lane);
+            }
             if (lex_less(s, crow, best, best_row)) {
                 best = s;
                 best_row = crow;
@@ -445,7 +557,16 @@ void launch_resolve(PartialView view, Bound bound, ReplayInputs in,
     }
     FinalizeScratch fs = finalize_scratch(scratch, static_cast<uint32_t>(capacity),
                                           view.rows);
-    resolve_kernel<<<ambiguous_count, kResolveThreads, 0, stream>>>(
+    const bool projected = in.op == ReplayOp::l2_projected ||
+                           in.op == ReplayOp::median_projected;
+    const size_t smem = projected ? in.proj_dim * sizeof(double) : 0;
+    if (smem > 48 * 1024) {
+        check_cuda(cudaFuncSetAttribute(resolve_kernel,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(smem)),
+                   "cannot configure resolve kernel");
+    }
+    resolve_kernel<<<ambiguous_count, kResolveThreads, smem, stream>>>(
         view, bound, in, ambiguous, ambiguous_count, fs.query_upper, results,
         exact_distances);
     check_cuda(cudaGetLastError(), "cannot launch resolve kernel");

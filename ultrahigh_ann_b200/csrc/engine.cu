@@ -127,6 +127,18 @@ uint64_t workspace_payload(const uha_index& index, uint64_t b)
             return 2 * (b * index.sample_size * f) + b * r * f + b * f + b * z;
         }
         return 2 * (b * index.sample_size * f) + b * r * f + b * z;
+    case IndexKind::hierarchical: {
+        // host sampled values, device sampled + projected values, the
+        // projection's flag, then the scan buffers
+        const uint64_t k = index.sample_size;
+        const uint64_t p = index.projection_dimension;
+        if (index.metric == UHA_L2) {
+            return 2 * (b * k * f) + 2 * (b * p * f) + sizeof(int) + b * r * f +
+                   b * f + b * z;
+        }
+        return 2 * (b * k * f) + b * p * f + sizeof(int) + b * r * f + b * z +
+               sizeof(int);
+    }
     }
     return 0;
 }
@@ -429,6 +441,162 @@ extern "C" uha_status uha_sampled_index_create(
     });
 }
 
+
+namespace {
+
+// Per-unit coefficient of the binary32 query projection's certified error:
+// |y32_j - y64_j| <= coefficient * sum_i |x_i P32_ji| (binary32 two-level sum
+// over k terms, binary32 rounding of the coefficients, the CPU's own binary64
+// rounding).
+double projection_error_per_abs(uint64_t k)
+{
+    const double u32 = std::ldexp(1.0, -24);
+    const double u64 = std::ldexp(1.0, -53);
+    const double n = 32.0 + static_cast<double>((k + 31) / 32) + 3.0;
+    const double g32 = n * u32 / (1.0 - n * u32);
+    const double g32b = (n + 1) * u32 / (1.0 - (n + 1) * u32);
+    const double n64 = static_cast<double>(k) + 3.0;
+    const double g64 = n64 * u64 / (1.0 - n64 * u64);
+    return 1.01 * (g32 + u32 * (1 + 2 * u32) + g64 * (1 + u32)) * (1 + g32b) /
+           (1 - g32b);
+}
+
+}  // namespace
+
+extern "C" uha_status uha_hierarchical_index_create(
+    int device, uha_metric metric, const float* rows, uint64_t row_count,
+    uint64_t dimension, const uint64_t* columns, const uint64_t* multiplicities,
+    const double* inverse_probabilities, uint64_t sample_size,
+    const double* projection, uint64_t projection_dimension, uha_index** out)
+{
+    return guarded([&] {
+        require(out != nullptr, UHA_INVALID_ARGUMENT,
+                "output pointer must not be null");
+        require(metric == UHA_L2 || metric == UHA_L1, UHA_INVALID_ARGUMENT,
+                "unknown metric");
+        validate_rows(rows, row_count, dimension);
+        const uint64_t k = sample_size;
+        const uint64_t p = projection_dimension;
+        require(p != 0, UHA_INVALID_ARGUMENT,
+                "projection_dimension has to be a positive integer");
+        if (k == 0 && row_count > 1) {
+            fail(UHA_RUNTIME_ERROR, "importance sampling selected no coordinates");
+        }
+        require(k == 0 || (columns != nullptr && multiplicities != nullptr &&
+                           inverse_probabilities != nullptr &&
+                           projection != nullptr),
+                UHA_INVALID_ARGUMENT, "coordinate sample must not be null");
+        require(k <= kMaxExtent, UHA_LENGTH_ERROR,
+                "coordinate sample exceeds the device grid limits");
+        require(p <= (metric == UHA_L2 ? 16384u : 1024u), UHA_LENGTH_ERROR,
+                "projection dimension exceeds the supported maximum "
+                "(16384 for L2, 1024 for L1)");
+        checked_mul(p, k, "projection matrix");
+        uint64_t multiplicity_sum = 0;
+        std::vector<uint32_t> cols(k);
+        for (uint64_t i = 0; i < k; ++i) {
+            if (columns[i] >= dimension) {
+                fail(UHA_OUT_OF_RANGE, "sampled column index out of range");
+            }
+            if (multiplicities[i] == 0 ||
+                !std::isfinite(inverse_probabilities[i]) ||
+                inverse_probabilities[i] <= 0.0) {
+                fail(UHA_INVALID_ARGUMENT,
+                     "sampled columns require positive finite weights");
+            }
+            if (multiplicity_sum > UINT64_MAX - multiplicities[i]) {
+                fail(UHA_LENGTH_ERROR, "sampled multiplicity overflows");
+            }
+            multiplicity_sum += multiplicities[i];
+            cols[i] = static_cast<uint32_t>(columns[i]);
+        }
+        const uint64_t kp = uha::round_up(k, kColumnAlign);
+        const uint64_t pp = uha::round_up(p, kColumnAlign);
+        std::vector<float> proj32(p * kp, 0.0f);
+        for (uint64_t j = 0; j < p; ++j) {
+            for (uint64_t i = 0; i < k; ++i) {
+                const double c = projection[j * k + i];
+                const float f = static_cast<float>(c);
+                if (!std::isfinite(c)) {
+                    fail(UHA_OVERFLOW_ERROR, "projection coefficient is not finite");
+                }
+                if (!std::isfinite(f)) {
+                    fail(UHA_OVERFLOW_ERROR,
+                         "binary32 projection coefficient is not finite");
+                }
+                proj32[j * kp + i] = f;
+            }
+        }
+
+        auto index = std::make_unique<uha_index>();
+        select_device(*index, device);
+        DeviceGuard guard(device);
+        index->kind = IndexKind::hierarchical;
+        index->metric = metric;
+        index->rows = row_count;
+        index->dimension = dimension;
+        index->sample_size = k;
+        index->padded_sample = kp;
+        index->sampled_multiplicity = multiplicity_sum;
+        index->projection_dimension = p;
+        index->scan_dim = p;
+        index->padded_dim = pp;
+        upload(index->columns, cols.data(), cols.size());
+        upload(index->projection64, projection, p * k);
+        upload(index->projection32, proj32.data(), proj32.size());
+
+        DeviceBuffer<int> bad(1);
+        check_cuda(cudaMemset(bad.get(), 0, sizeof(int)), "cannot clear flag");
+        DeviceBuffer<float> sampled(std::max<uint64_t>(1, row_count * kp));
+        check_cuda(cudaMemset(sampled.get(), 0, sampled.bytes()),
+                   "cannot clear sampled rows");
+        if (k != 0) {
+            DeviceBuffer<float> source(checked_mul(row_count, dimension,
+                                                   "representative matrix"));
+            check_cuda(cudaMemcpy(source.get(), rows, source.bytes(),
+                                  cudaMemcpyHostToDevice),
+                       "cannot copy representatives to the CUDA device");
+            uha::launch_gather_rows(source.get(), row_count, dimension,
+                                    index->columns.get(), nullptr, k,
+                                    sampled.get(), kp, nullptr);
+        }
+        index->rows64.allocate(row_count * p);
+        uha::launch_project_rows64(sampled.get(), row_count, kp, k,
+                                   index->projection64.get(), p,
+                                   index->rows64.get(), bad.get(), nullptr);
+        index->scan_rows.allocate(row_count * pp);
+        index->row_err.allocate(row_count);
+        uha::launch_narrow_rows(index->rows64.get(), row_count, p,
+                                index->scan_rows.get(), pp, index->row_err.get(),
+                                metric == UHA_L2, bad.get(), nullptr);
+        int host_bad = 0;
+        check_cuda(cudaMemcpy(&host_bad, bad.get(), sizeof(int),
+                              cudaMemcpyDeviceToHost),
+                   "row projection failed");
+        if (host_bad & 1) {
+            fail(UHA_OVERFLOW_ERROR, "projected representatives is not finite");
+        }
+        if (host_bad & 2) {
+            fail(UHA_OVERFLOW_ERROR,
+                 "binary32 projected representative is not finite");
+        }
+        const uint64_t f = sizeof(float);
+        const uint64_t column_bytes = 2 * sizeof(uint64_t) + sizeof(double);
+        if (metric == UHA_L2) {
+            compute_row_norms(*index);
+            index->usage.index_payload_bytes = row_count * p * f + row_count * f +
+                                               k * column_bytes + p * k * f;
+        } else {
+            index->usage.index_payload_bytes =
+                k * column_bytes + p * k * f + row_count * p * f;
+        }
+        index->usage.query_workspace_payload_bytes = 0;
+        index->usage.unique_query_coordinates = k;
+        index->usage.sampled_multiplicity = multiplicity_sum;
+        *out = index.release();
+    });
+}
+
 extern "C" void uha_index_destroy(uha_index* index)
 {
     if (index != nullptr) {
@@ -494,7 +662,13 @@ extern "C" uha_status uha_workspace_create(const uha_index* index,
                    "cannot create CUDA stream");
         const uint64_t b = maximum_batch_size;
         ws->raw_queries.allocate(b * index->dimension);
-        ws->prepared.allocate(b * index->padded_dim);
+        if (index->kind == IndexKind::hierarchical) {
+            ws->prepared.allocate(b * index->padded_sample);
+            ws->projected.allocate(b * index->padded_dim);
+            ws->query_err.allocate(b);
+        } else {
+            ws->prepared.allocate(b * index->padded_dim);
+        }
         ws->query_norms.allocate(b);
         ws->results.allocate(b);
         ws->exact.allocate(b);
@@ -601,6 +775,18 @@ extern "C" uha_status uha_query(const uha_index* index, uha_workspace* ws,
         cudaStream_t stream = ws->stream;
         const uint64_t n = query_count;
 
+        if (index->kind == IndexKind::hierarchical && index->rows == 1) {
+            // A one-row hierarchy answers row 0 without projecting (or
+            // validating) the query (hierarchical_l2_ann_index.cpp:164-166).
+            for (uint64_t q = 0; q < n; ++q) {
+                out_indices[q] = 0;
+                if (out_distances != nullptr) {
+                    out_distances[q] = 0.0;
+                }
+            }
+            ws->last.certified_queries = n;
+            return;
+        }
         if (index->padded_dim == 0) {
             // Nothing to compare: every distance is zero and row 0 wins
             // (empty sample or zero dimension).
@@ -630,7 +816,22 @@ extern "C" uha_status uha_query(const uha_index* index, uha_workspace* ws,
                    "cannot clear query counters");
         int* error_flag = reinterpret_cast<int*>(ws->counters.get() + 1);
         uint64_t launches = 1;
-        if (index->kind == IndexKind::sampled) {
+        const bool hierarchical = index->kind == IndexKind::hierarchical;
+        const float* scan_queries = ws->prepared.get();
+        if (hierarchical) {
+            uha::launch_prepare_sampled(source, n, index->dimension,
+                                        index->columns.get(), nullptr,
+                                        index->sample_size, ws->prepared.get(),
+                                        index->padded_sample, error_flag, stream);
+            uha::launch_project_queries(
+                ws->prepared.get(), n, index->padded_sample, index->sample_size,
+                index->projection32.get(), index->projection_dimension,
+                ws->projected.get(), index->padded_dim, ws->query_err.get(),
+                projection_error_per_abs(index->sample_size),
+                index->metric == UHA_L2, error_flag, stream);
+            scan_queries = ws->projected.get();
+            launches += 2;
+        } else if (index->kind == IndexKind::sampled) {
             uha::launch_prepare_sampled(
                 source, n, index->dimension, index->columns.get(),
                 index->metric == UHA_L2 ? index->scales.get() : nullptr,
@@ -650,8 +851,13 @@ extern "C" uha_status uha_query(const uha_index* index, uha_workspace* ws,
             op = index->weights32.size() != 0 ? uha::ScanOp::l1_weighted
                                               : uha::ScanOp::l1;
         }
-        const uha::ScanPlan plan = uha::plan_scan(index->rows, index->padded_dim,
-                                                  n, index->sm_count);
+        const bool median = hierarchical && index->metric == UHA_L1;
+        uha::ScanPlan plan = uha::plan_scan(index->rows, index->padded_dim, n,
+                                            index->sm_count);
+        if (median) {
+            plan.chunks = 1;
+            plan.depth = 0;
+        }
         const uint64_t partial_count =
             checked_mul(checked_mul(plan.chunks, n, "partials"), index->rows,
                         "partials");
@@ -662,9 +868,15 @@ extern "C" uha_status uha_query(const uha_index* index, uha_workspace* ws,
         if (ws->timing) {
             check_cuda(cudaEventRecord(ws->events[1], stream), "event");
         }
-        uha::launch_scan(plan, op, index->scan_rows.get(), index->rows,
-                         index->padded_dim, index->weights32.get(),
-                         ws->prepared.get(), n, ws->partials.get(), stream);
+        if (median) {
+            uha::launch_median_scan(index->scan_rows.get(), index->rows,
+                                    index->padded_dim, index->projection_dimension,
+                                    scan_queries, n, ws->partials.get(), stream);
+        } else {
+            uha::launch_scan(plan, op, index->scan_rows.get(), index->rows,
+                             index->padded_dim, index->weights32.get(),
+                             scan_queries, n, ws->partials.get(), stream);
+        }
         if (ws->timing) {
             check_cuda(cudaEventRecord(ws->events[2], stream), "event");
         }
@@ -674,10 +886,25 @@ extern "C" uha_status uha_query(const uha_index* index, uha_workspace* ws,
                                     static_cast<uint32_t>(n),
                                     static_cast<uint32_t>(index->rows)};
         const int term_roundings = op == uha::ScanOp::l1 ? 1 : 2;
-        const uha::Bound bound =
-            make_bound(plan.depth, index->scan_dim, term_roundings);
+        uha::Bound bound = make_bound(plan.depth, index->scan_dim, term_roundings);
+        if (hierarchical) {
+            bound.row_err = index->row_err.get();
+            bound.query_err = ws->query_err.get();
+            if (median) {
+                // binary32 |diff| and midpoint roundings; the binary64 ones
+                bound.mode = uha::BoundMode::median;
+                bound.rel = std::ldexp(6.0f, -24);
+                bound.abs = std::ldexp(1.0f, -126);
+            } else {
+                bound.mode = uha::BoundMode::projected_l2;
+                const double n64 = static_cast<double>(index->scan_dim) + 3;
+                const double g64 = n64 * std::ldexp(1.0, -53);
+                bound.cpu_rel =
+                    std::nextafter(static_cast<float>(1.01 * g64), 1.0f);
+            }
+        }
         if (gemm) {
-            uha::launch_query_norms(ws->prepared.get(), n, index->padded_dim,
+            uha::launch_query_norms(scan_queries, n, index->padded_dim,
                                     ws->query_norms.get(), stream);
             uha::launch_finalize_gemm(view, index->row_norms.get(),
                                       ws->query_norms.get(), ws->results.get(),
@@ -715,6 +942,12 @@ extern "C" uha_status uha_query(const uha_index* index, uha_workspace* ws,
 
         const uint32_t flag = ws->host_counters.get()[1];
         if (flag != 0) {
+            if (flag & 1u && hierarchical) {
+                fail(UHA_INVALID_ARGUMENT, "sampled query coordinate must be finite");
+            }
+            if (flag & 4u) {
+                fail(UHA_OVERFLOW_ERROR, "projected query is not finite");
+            }
             if (index->kind == IndexKind::sampled) {
                 fail(UHA_INVALID_ARGUMENT,
                      (flag & 1u) ? "sampled query coordinate must be finite"
@@ -732,7 +965,15 @@ extern "C" uha_status uha_query(const uha_index* index, uha_workspace* ws,
             in.dim = index->scan_dim;
             in.padded_dim = index->padded_dim;
             in.weights64 = index->weights64.get();
-            if (index->metric == UHA_L2) {
+            if (hierarchical) {
+                in.op = median ? uha::ReplayOp::median_projected
+                               : uha::ReplayOp::l2_projected;
+                in.dim = index->sample_size;
+                in.padded_dim = index->padded_sample;
+                in.rows64 = index->rows64.get();
+                in.projection64 = index->projection64.get();
+                in.proj_dim = index->projection_dimension;
+            } else if (index->metric == UHA_L2) {
                 in.op = uha::ReplayOp::l2_sequential;
             } else if (index->weights64.size() != 0) {
                 in.op = uha::ReplayOp::l1_weighted_sequential;

@@ -1,5 +1,5 @@
-// Host-side index-build draws: the coordinate sample and the hierarchical
-// projection matrices.
+// Host-side index build: the coordinate sample, the hierarchical projection
+// matrices and the CPU-policy importance probabilities.
 //
 // These stay on the host on purpose. The index set I and the projection
 // coefficients are defined by std::mt19937_64 together with libstdc++'s
@@ -11,11 +11,14 @@
 // src/hnsvw25/l1/hierarchical/l1_hierarchical_projection.cpp:54-77).
 #include "common.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <random>
 #include <sstream>
 #include <string>
+#include <thread>
+#include <vector>
 
 struct uha_rng {
     std::mt19937_64 engine;
@@ -227,6 +230,111 @@ extern "C" uha_status uha_cauchy_matrix(const uint64_t* multiplicities,
                          "Cauchy projection coefficient is not finite");
                 }
                 out[index++] = coefficient;
+            }
+        }
+    });
+}
+
+// Importance probabilities on the host cores with the reference CPU policies'
+// arithmetic (src/hnsvw25/l2/importance_sampling.cpp:19-45,
+// src/hnsvw25/l1/importance_sampling.cpp:19-47): binary64 pair distances (L2
+// sequential sum of squares; L1 in std::transform_reduce's grouping of four),
+// then the per-column maximum of min(1, d_j^2 / ||a-b||^2) or |d_j| / ||a-b||_1.
+// First rows are split over `threads` threads with private maxima; the maximum
+// is exact, so the result is bit-identical to the sequential loop.
+
+namespace {
+
+double pair_l2(const float* a, const float* b, uint64_t d)
+{
+    double s = 0.0;
+    for (uint64_t i = 0; i < d; ++i) {
+        const double diff = static_cast<double>(a[i]) - static_cast<double>(b[i]);
+        s += diff * diff;
+    }
+    return s;
+}
+
+double pair_l1(const float* a, const float* b, uint64_t d)
+{
+    auto t = [&](uint64_t i) {
+        return std::abs(static_cast<double>(a[i]) - static_cast<double>(b[i]));
+    };
+    double init = 0.0;
+    uint64_t i = 0;
+    for (; d - i >= 4; i += 4) {
+        const double v1 = t(i) + t(i + 1);
+        const double v2 = t(i + 2) + t(i + 3);
+        init = init + (v1 + v2);
+    }
+    for (; i < d; ++i) {
+        init = init + t(i);
+    }
+    return init;
+}
+
+}  // namespace
+
+extern "C" uha_status uha_importance_probabilities_host(
+    uha_metric metric, const float* rows, uint64_t row_count,
+    uint64_t dimension, int threads, double* out)
+{
+    return guarded([&] {
+        if (metric != UHA_L2 && metric != UHA_L1) {
+            fail(UHA_INVALID_ARGUMENT, "unknown metric");
+        }
+        if ((rows == nullptr && row_count * dimension != 0) ||
+            (out == nullptr && dimension != 0)) {
+            fail(UHA_INVALID_ARGUMENT, "matrix and output must not be null");
+        }
+        uha::checked_mul(row_count, dimension, "representative matrix");
+        for (uint64_t i = 0; i < row_count * dimension; ++i) {
+            if (!std::isfinite(rows[i])) {
+                fail(UHA_INVALID_ARGUMENT, "representatives must be finite");
+            }
+        }
+        std::fill(out, out + dimension, 0.0);
+        if (row_count < 2 || dimension == 0) {
+            return;
+        }
+        const int workers = static_cast<int>(std::max<uint64_t>(
+            1, std::min<uint64_t>(static_cast<uint64_t>(std::max(1, threads)),
+                                  row_count - 1)));
+        std::vector<std::vector<double>> local(workers,
+                                               std::vector<double>(dimension, 0.0));
+        std::vector<std::thread> pool;
+        for (int w = 0; w < workers; ++w) {
+            pool.emplace_back([&, w] {
+                std::vector<double>& m = local[w];
+                for (uint64_t a = w; a + 1 < row_count; a += workers) {
+                    const float* ra = rows + a * dimension;
+                    for (uint64_t b = a + 1; b < row_count; ++b) {
+                        const float* rb = rows + b * dimension;
+                        const double dist = metric == UHA_L2
+                                                ? pair_l2(ra, rb, dimension)
+                                                : pair_l1(ra, rb, dimension);
+                        if (dist == 0.0) {
+                            continue;
+                        }
+                        const double inv = 1.0 / dist;
+                        for (uint64_t j = 0; j < dimension; ++j) {
+                            const double diff = static_cast<double>(ra[j]) -
+                                                static_cast<double>(rb[j]);
+                            const double v = metric == UHA_L2
+                                                 ? std::min(1.0, diff * diff * inv)
+                                                 : std::abs(diff) * inv;
+                            m[j] = std::max(m[j], v);
+                        }
+                    }
+                }
+            });
+        }
+        for (auto& t : pool) {
+            t.join();
+        }
+        for (const auto& m : local) {
+            for (uint64_t j = 0; j < dimension; ++j) {
+                out[j] = std::max(out[j], m[j]);
             }
         }
     });

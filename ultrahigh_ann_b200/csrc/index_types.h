@@ -10,7 +10,7 @@
 
 namespace uha {
 
-enum class IndexKind { exact, weighted, sampled };
+enum class IndexKind { exact, weighted, sampled, hierarchical };
 
 constexpr uint64_t kColumnAlign = 4;  // padded row length: 16-byte multiple
 constexpr uint64_t kMaxExtent = 0x7fffffffull;
@@ -39,6 +39,13 @@ struct uha_index {
     uha::DeviceBuffer<double> weights64;  // scan_dim (weighted L1 replay)
     uha::DeviceBuffer<uint32_t> columns;  // sample_size (sampled)
     uha::DeviceBuffer<float> scales;      // sample_size (sampled L2)
+    // hierarchical: scan_dim = p; scan_rows = binary32 projected rows
+    uint64_t projection_dimension = 0;
+    uint64_t padded_sample = 0;             // sample_size rounded up
+    uha::DeviceBuffer<double> rows64;       // rows x p (binary64 projected)
+    uha::DeviceBuffer<double> projection64; // p x sample_size
+    uha::DeviceBuffer<float> projection32;  // p x padded_sample
+    uha::DeviceBuffer<float> row_err;       // rows
     uha_space_usage usage{};
 };
 
@@ -49,6 +56,8 @@ struct uha_workspace {
     cudaStream_t stream = nullptr;
     uha::DeviceBuffer<float> raw_queries;
     uha::DeviceBuffer<float> prepared;
+    uha::DeviceBuffer<float> projected;   // hierarchical: batch x padded p
+    uha::DeviceBuffer<float> query_err;   // hierarchical: batch
     uha::DeviceBuffer<float> query_norms;
     uha::DeviceBuffer<float> partials;
     uha::DeviceBuffer<uha::Result> results;

@@ -33,11 +33,24 @@ struct PartialView {
     uint32_t rows;
 };
 
-// Certification parameters: a binary32 distance D certifies the reference
-// CPU's binary64 distance to lie in [D - (rel * D + abs), D + (rel * D + abs)].
+// Certification parameters. For a binary32 distance D of row `row` and query
+// `q` the reference CPU's binary64 distance lies in
+//   plain:        [D - (rel D + abs), D + (rel D + abs)]
+//   projected_l2: [((sqrt(D (1 - rel)) - E)+)^2 (1 - cpu_rel) - abs,
+//                  (sqrt(D (1 + rel)) + E)^2 (1 + cpu_rel) + abs]
+//   median:       [D - (rel D + E + abs), D + (rel D + E + abs)]
+// with E = row_err[row] + query_err[q]: the Euclidean (projected_l2) or
+// maximum (median) norm of the binary32-vs-binary64 error of the projected
+// row and the projected query.
+enum class BoundMode : int { plain = 0, projected_l2 = 1, median = 2 };
+
 struct Bound {
     float rel;
     float abs;
+    BoundMode mode = BoundMode::plain;
+    const float* row_err = nullptr;
+    const float* query_err = nullptr;
+    float cpu_rel = 0.f;
 };
 
 struct Result {
@@ -96,15 +109,47 @@ void launch_finalize_gemm(PartialView view, const float* row_norms,
 struct ReplayInputs {
     ReplayOp op;
     const float* rows;         // [rows][padded_dim]
-    const float* queries;      // [batch][padded_dim]
+    const float* queries;      // [batch][padded_dim] (projected ops: the
+                               // gathered sampled values)
     const double* weights64;   // l1_weighted_sequential
-    uint64_t dim;              // columns to replay
+    uint64_t dim;              // columns to replay (projected ops: k)
     uint64_t padded_dim;
+    const double* rows64 = nullptr;        // projected ops: [rows][proj_dim]
+    const double* projection64 = nullptr;  // projected ops: [proj_dim][dim]
+    uint64_t proj_dim = 0;
 };
 void launch_resolve(PartialView view, Bound bound, ReplayInputs in,
                     const uint32_t* ambiguous, uint32_t ambiguous_count,
                     void* scratch, uint64_t capacity, Result* results,
                     double* exact_distances, cudaStream_t stream);
+
+// ---- hierarchical index (projection)
+// Binary64 projected rows reps[row][j] = sum_i double(sampled[row][i]) *
+// projection[j][i] in i order; `bad` is set when a result is not finite.
+void launch_project_rows64(const float* sampled, uint64_t row_count,
+                           uint64_t padded_k, uint64_t k,
+                           const double* projection, uint64_t p, double* reps,
+                           int* bad, cudaStream_t stream);
+// reps64 -> binary32 padded rows and the per-row error norm
+// (euclidean: 2-norm, else max-norm) of float(reps) - reps.
+void launch_narrow_rows(const double* reps, uint64_t row_count, uint64_t p,
+                        float* out, uint64_t padded_p, float* row_err,
+                        bool euclidean, int* bad, cudaStream_t stream);
+// Binary32 projection of gathered queries with its certified error norm:
+// y[b][j] = sum_i x[b][i] proj32[j][i]; query_err[b] bounds the distance
+// between y[b] and the reference's binary64 projection (2-norm if
+// euclidean, else max-norm). error_flag |= 4 for a non-finite projection.
+void launch_project_queries(const float* gathered, uint64_t batch,
+                            uint64_t padded_k, uint64_t k,
+                            const float* proj32, uint64_t p, float* out,
+                            uint64_t padded_p, float* query_err,
+                            double err_per_abs, bool euclidean,
+                            int* error_flag, cudaStream_t stream);
+// Median of |rows[row][j] - queries[q][j]| over j < p per (query, row),
+// written as one chunk of partials.
+void launch_median_scan(const float* rows, uint64_t row_count,
+                        uint64_t padded_p, uint64_t p, const float* queries,
+                        uint64_t batch, float* partials, cudaStream_t stream);
 
 // ---- build-time helpers
 void launch_gather_rows(const float* source, uint64_t row_count, uint64_t dim,

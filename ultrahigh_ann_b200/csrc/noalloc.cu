@@ -95,6 +95,10 @@ extern "C" uha_status uha_query_noalloc(const uha_index* index,
         if (index == nullptr) {
             fail(UHA_INVALID_ARGUMENT, "index must not be null");
         }
+        if (index->kind == uha::IndexKind::hierarchical) {
+            fail(UHA_INVALID_ARGUMENT,
+                 "uha_query_noalloc serves exact and flat indexes only");
+        }
         if (query_count == 0) {
             return;
         }
