@@ -99,16 +99,17 @@ def test_hierarchical_l2_reference_fixture(oracle_module):
     assert usage.unique_query_coordinates == 2 and usage.sampled_multiplicity == 2
     assert ws.payload_bytes() == (2 * (4 * 2 * 4) + 2 * (4 * 7 * 4) + 4 +
                                   4 * 3 * 4 + 4 * 4 + 4 * 8)
-    queries = np.array([0.5, 10.0, 0.25, 20.0, 3.8, -10.0, 1.1, 20.0,
-                        2.0, 10.0, 0.5, 20.0, 2.0, -10.0, 5.0, 20.0], np.float32)
+    queries = np.array([0.2, 10.0, 0.1, 20.0, 3.9, -10.0, 1.1, 20.0,
+                        2.1, 10.0, 4.8, 20.0, 1.0, -10.0, 2.0, 20.0], np.float32)
     expected, _ = oracle_module.hierarchical(
         "l2", rows, index.coordinate_sample.source_columns, index.projection, queries)
     assert np.array_equal(index.query_batch(queries, 4, None, ws), expected)
     assert np.array_equal(index.query_batch(queries, 4, None, ws, uha.QueryStrategy.gemm),
                           expected)
     # unsampled non-finite values are ignored; sampled ones are rejected
-    assert index.query(np.array([0.5, np.nan, 0.25, np.inf], np.float32), ws) == \
-        expected[0]
+    unsampled = np.array([0.2, np.nan, 0.1, np.inf], np.float32)
+    assert index.query(unsampled, ws) == expected[0]
+    assert index.query(unsampled, ws, uha.QueryStrategy.gemm) == expected[0]
     with pytest.raises(uha.InvalidArgument):
         index.query(np.array([np.nan, 0.0, 0.25, 0.0], np.float32), ws)
     with pytest.raises(uha.InvalidArgument):

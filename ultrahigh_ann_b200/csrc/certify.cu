@@ -489,6 +489,41 @@ __global__ void __launch_bounds__(kResolveThreads)
     }
 }
 
+// The reference binary64 distance of each query's selected row (hierarchical
+// indexes: their binary32 projected distances can differ from the reference's
+// by more than 1e-5 relative when rows are close, so the reported distance is
+// replayed). One CTA per query: the binary64 projected query, then one warp
+// replays the selected row.
+__global__ void __launch_bounds__(kResolveThreads)
+    refine_kernel(ReplayInputs in, const Result* results,
+                  double* exact_distances)
+{
+    const uint32_t q = blockIdx.x;
+    extern __shared__ double projected_query[];
+    const float* qrow = in.queries + static_cast<uint64_t>(q) * in.padded_dim;
+    for (uint64_t j = threadIdx.x; j < in.proj_dim; j += blockDim.x) {
+        const double* coeff = in.projection64 + j * in.dim;
+        double y = 0.0;
+        for (uint64_t i = 0; i < in.dim; ++i) {
+            y = __dadd_rn(y, __dmul_rn(static_cast<double>(qrow[i]), coeff[i]));
+        }
+        projected_query[j] = y;
+    }
+    __syncthreads();
+    if (threadIdx.x >= 32) {
+        return;
+    }
+    const int lane = threadIdx.x;
+    const uint32_t row = results[q].row;
+    const double* r = in.rows64 + static_cast<uint64_t>(row) * in.proj_dim;
+    const double s = in.op == ReplayOp::median_projected
+                         ? replay_median(r, projected_query, in.proj_dim, lane)
+                         : replay_projected_l2(r, projected_query, in.proj_dim, lane);
+    if (lane == 0) {
+        exact_distances[q] = s;
+    }
+}
+
 // Carves the finalize scratch region: per-(query, row block) summaries, the
 // per-query completion counters (zero between calls) and U* per query. The
 // layout depends only on the workspace capacity, never on the batch of one
@@ -515,6 +550,22 @@ FinalizeScratch finalize_scratch(void* base, uint32_t batch, uint32_t rows)
 }
 
 }  // namespace
+
+void launch_refine_winners(ReplayInputs in, const Result* results,
+                           uint32_t batch, double* exact_distances,
+                           cudaStream_t stream)
+{
+    const size_t smem = in.proj_dim * sizeof(double);
+    if (smem > 48 * 1024) {
+        check_cuda(cudaFuncSetAttribute(refine_kernel,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(smem)),
+                   "cannot configure refine kernel");
+    }
+    refine_kernel<<<batch, kResolveThreads, smem, stream>>>(in, results,
+                                                            exact_distances);
+    check_cuda(cudaGetLastError(), "cannot launch refine kernel");
+}
 
 uint64_t finalize_scratch_bytes(uint64_t batch, uint64_t rows)
 {

@@ -177,6 +177,14 @@ private:
 
 void set_last_error(const char* message);
 
+// Clears a non-sticky error left in the runtime by an earlier call whose
+// status was not checked (for example a destructor), so the checks of the
+// next call report only their own failures.
+inline void clear_stale_cuda_error()
+{
+    static_cast<void>(cudaGetLastError());
+}
+
 // Runs the body of a C-ABI entry point and turns exceptions into status codes.
 template <typename F>
 uha_status guarded(F&& body)

@@ -42,6 +42,7 @@ void require(bool condition, uha_status status, const char* message)
 
 void select_device(uha_index& index, int device)
 {
+    uha::clear_stale_cuda_error();
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
         cudaGetLastError();
@@ -607,6 +608,7 @@ extern "C" void uha_index_destroy(uha_index* index)
         if (ok) {
             cudaSetDevice(previous);
         }
+        uha::clear_stale_cuda_error();
     }
 }
 
@@ -656,6 +658,7 @@ extern "C" uha_status uha_workspace_create(const uha_index* index,
         DeviceGuard guard(index->device);
         auto ws = std::make_unique<uha_workspace>();
         ws->owner = index;
+        ws->device = index->device;
         ws->max_batch = maximum_batch_size;
         ws->payload_bytes = workspace_payload(*index, maximum_batch_size);
         check_cuda(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking),
@@ -694,13 +697,12 @@ extern "C" void uha_workspace_destroy(uha_workspace* workspace)
     if (workspace != nullptr) {
         int previous = 0;
         const bool ok = cudaGetDevice(&previous) == cudaSuccess;
-        if (workspace->owner != nullptr) {
-            cudaSetDevice(workspace->owner->device);
-        }
+        cudaSetDevice(workspace->device);
         delete workspace;
         if (ok) {
             cudaSetDevice(previous);
         }
+        uha::clear_stale_cuda_error();
     }
 }
 
@@ -772,6 +774,7 @@ extern "C" uha_status uha_query(const uha_index* index, uha_workspace* ws,
                 UHA_INVALID_ARGUMENT, "query pointer must not be null");
 
         DeviceGuard guard(index->device);
+        uha::clear_stale_cuda_error();
         cudaStream_t stream = ws->stream;
         const uint64_t n = query_count;
 
@@ -1008,11 +1011,35 @@ extern "C" uha_status uha_query(const uha_index* index, uha_workspace* ws,
                 ws->last.device_ms = ms;
             }
         }
+        const bool refine = hierarchical && !gemm && out_distances != nullptr;
+        if (refine) {
+            // reported distances of a hierarchy: the reference's binary64
+            // value of each selected row
+            uha::ReplayInputs in{};
+            in.op = median ? uha::ReplayOp::median_projected
+                           : uha::ReplayOp::l2_projected;
+            in.queries = ws->prepared.get();
+            in.dim = index->sample_size;
+            in.padded_dim = index->padded_sample;
+            in.rows64 = index->rows64.get();
+            in.projection64 = index->projection64.get();
+            in.proj_dim = index->projection_dimension;
+            uha::launch_refine_winners(in, ws->results.get(),
+                                       static_cast<uint32_t>(n), ws->exact.get(),
+                                       stream);
+            ++launches;
+            check_cuda(cudaMemcpyAsync(ws->host_exact.get(), ws->exact.get(),
+                                       n * sizeof(double), cudaMemcpyDeviceToHost,
+                                       stream),
+                       "cannot copy refined distances from the CUDA device");
+            check_cuda(cudaStreamSynchronize(stream), "CUDA refine failed");
+        }
         const uha::Result* res = ws->host_results.get();
         for (uint64_t q = 0; q < n; ++q) {
             out_indices[q] = res[q].row;
             if (out_distances != nullptr) {
-                out_distances[q] = static_cast<double>(res[q].distance);
+                out_distances[q] = refine ? ws->host_exact.get()[q]
+                                          : static_cast<double>(res[q].distance);
             }
         }
         for (uint32_t q : replayed) {

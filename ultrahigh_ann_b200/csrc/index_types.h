@@ -51,6 +51,7 @@ struct uha_index {
 
 struct uha_workspace {
     const uha_index* owner = nullptr;
+    int device = 0;  // the owner's device, kept so destruction never reads the owner
     uint64_t max_batch = 0;
     uint64_t payload_bytes = 0;
     cudaStream_t stream = nullptr;

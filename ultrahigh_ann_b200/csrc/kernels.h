@@ -123,6 +123,12 @@ void launch_resolve(PartialView view, Bound bound, ReplayInputs in,
                     void* scratch, uint64_t capacity, Result* results,
                     double* exact_distances, cudaStream_t stream);
 
+// Reference binary64 distance of every query's selected row (projected
+// replay ops only).
+void launch_refine_winners(ReplayInputs in, const Result* results,
+                           uint32_t batch, double* exact_distances,
+                           cudaStream_t stream);
+
 // ---- hierarchical index (projection)
 // Binary64 projected rows reps[row][j] = sum_i double(sampled[row][i]) *
 // projection[j][i] in i order; `bad` is set when a result is not finite.

@@ -112,6 +112,7 @@ extern "C" uha_status uha_query_noalloc(const uha_index* index,
                  "query and output device pointers must not be null");
         }
         uha::DeviceGuard guard(index->device);
+        uha::clear_stale_cuda_error();
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         const uint64_t n = query_count;
 
