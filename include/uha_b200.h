@@ -99,6 +99,7 @@ typedef struct uha_query_stats {
  * importance_sampling.hpp:23-41, l1/importance_sampling.hpp:22-40). */
 typedef struct uha_probability_report {
     uint64_t pair_count;
+    uint64_t pair_chunks;     /* launches the pairs were split into */
     uint64_t device_working_set_bytes;
     double host_to_device_ms;
     double inverse_distance_ms;
@@ -257,16 +258,29 @@ uha_status uha_workspace_set_timing(uha_workspace* workspace, int enabled);
 
 /* ---------------------------------------------------------- index build */
 
+/* Pair-distance method of the device probability build. DIRECT sums squared
+ * (or absolute) differences per pair; GRAM (L2 only) forms the r x r Gram
+ * matrix and recomputes cancellation-prone pairs directly, as the reference's
+ * cuBLAS backend does (src/hnsvw25/l2/cuda_importance_sampling.cu:332-364). */
+typedef enum uha_pair_backend {
+    UHA_PAIRS_DIRECT = 0,
+    UHA_PAIRS_GRAM = 1
+} uha_pair_backend;
+
 /* Importance probabilities on the device. L2: p_j = max over row pairs of
  * min(1, (a_j-b_j)^2 / ||a-b||^2); L1: p_j = max over pairs of
  * |a_j-b_j| / ||a-b||_1; pairs at distance zero are skipped. Pair distances
- * and the normalisation are binary64. Replaces
+ * and the normalisation are binary64. The per-column maxima are folded in
+ * min(pair_chunks, pairs) launches over consecutive pair ranges, which bounds
+ * the duration of each kernel (pair_chunks must be positive). Replaces
  * compute_l2_importance_probabilities_gpu (include/ultrahigh_ann/hnsvw25/l2/
  * importance_sampling.hpp:49-52) and compute_l1_importance_probabilities_gpu
  * (include/ultrahigh_ann/hnsvw25/l1/importance_sampling.hpp:45-48). */
 uha_status uha_importance_probabilities(int device, uha_metric metric,
                                         const float* rows, uint64_t row_count,
                                         uint64_t dimension,
+                                        uha_pair_backend backend,
+                                        uint64_t pair_chunks,
                                         double* out_probabilities,
                                         uha_probability_report* report);
 

@@ -26,6 +26,10 @@ LOGIC_ERROR = 7
 L2 = 0
 L1 = 1
 
+# uha_pair_backend
+PAIRS_DIRECT = 0
+PAIRS_GRAM = 1
+
 # uha_strategy
 DIRECT = 0
 GEMM = 1
@@ -60,6 +64,7 @@ class QueryStats(ctypes.Structure):
 
 class ProbabilityReport(ctypes.Structure):
     _fields_ = [("pair_count", c_uint64),
+                ("pair_chunks", c_uint64),
                 ("device_working_set_bytes", c_uint64),
                 ("host_to_device_ms", c_double),
                 ("inverse_distance_ms", c_double),
@@ -99,7 +104,8 @@ SIGNATURES = {
     "uha_workspace_set_timing": (c_int, [c_void_p, c_int]),
     "uha_workspace_stream": (c_void_p, [c_void_p]),
     "uha_importance_probabilities": (c_int, [c_int, c_int, c_void_p, c_uint64, c_uint64,
-                                              c_void_p, POINTER(ProbabilityReport)]),
+                                              c_int, c_uint64, c_void_p,
+                                              POINTER(ProbabilityReport)]),
     "uha_importance_probabilities_host": (c_int, [c_int, c_void_p, c_uint64, c_uint64,
                                                    c_int, c_void_p]),
     "uha_rng_create": (c_int, [c_uint64, _H]),

@@ -263,6 +263,7 @@ class ProbabilityResult:
     device_name: str
     device: int
     pair_count: int
+    pair_chunks: int
     device_working_set_bytes: int
     host_to_device_ms: float
     inverse_distance_ms: float
@@ -278,27 +279,35 @@ def _matrix(values) -> np.ndarray:
     return m
 
 
-def _probabilities_gpu(metric: int, representatives, device: int) -> ProbabilityResult:
+def _probabilities_gpu(metric: int, representatives, device: int,
+                       gram: bool = False, pair_chunks: int = 128) -> ProbabilityResult:
     rows = _matrix(representatives)
     out = np.zeros(rows.shape[1], dtype=np.float64)
     rep = _abi.ProbabilityReport()
     _check(_abi.load().uha_importance_probabilities(
-        device, metric, _ptr(rows), rows.shape[0], rows.shape[1], _ptr(out),
-        ctypes.byref(rep)))
+        device, metric, _ptr(rows), rows.shape[0], rows.shape[1],
+        _abi.PAIRS_GRAM if gram else _abi.PAIRS_DIRECT, ctypes.c_uint64(pair_chunks),
+        _ptr(out), ctypes.byref(rep)))
     info = cuda_runtime_info(device)
     return ProbabilityResult(out, info.device_name if info else "", device,
-                             rep.pair_count, rep.device_working_set_bytes,
+                             rep.pair_count, rep.pair_chunks, rep.device_working_set_bytes,
                              rep.host_to_device_ms, rep.inverse_distance_ms,
                              rep.coordinate_maximum_ms, rep.device_to_host_ms,
                              rep.total_ms)
 
 
 def compute_l2_importance_probabilities_gpu(representatives, device: int = 0,
-                                            pair_chunks: int = 128) -> ProbabilityResult:
-    """include/ultrahigh_ann/hnsvw25/l2/importance_sampling.hpp:49-52."""
+                                            pair_chunks: int = 128,
+                                            distance_backend: str = "direct"
+                                            ) -> ProbabilityResult:
+    """include/ultrahigh_ann/hnsvw25/l2/importance_sampling.hpp:49-52;
+    distance_backend "direct" or "gram" (the reference's "cublas" backend)."""
     if pair_chunks <= 0:
         raise InvalidArgument("GPU pair chunk count must be positive")
-    return _probabilities_gpu(_abi.L2, representatives, device)
+    if distance_backend not in ("direct", "gram", "cublas"):
+        raise InvalidArgument("unknown L2 GPU distance backend")
+    return _probabilities_gpu(_abi.L2, representatives, device,
+                              gram=distance_backend != "direct", pair_chunks=pair_chunks)
 
 
 def compute_l1_importance_probabilities_gpu(representatives, device: int = 0,
@@ -306,7 +315,7 @@ def compute_l1_importance_probabilities_gpu(representatives, device: int = 0,
     """include/ultrahigh_ann/hnsvw25/l1/importance_sampling.hpp:45-48."""
     if pair_chunks <= 0:
         raise InvalidArgument("GPU pair chunk count must be positive")
-    return _probabilities_gpu(_abi.L1, representatives, device)
+    return _probabilities_gpu(_abi.L1, representatives, device, pair_chunks=pair_chunks)
 
 
 class QueryWorkspace:
@@ -580,7 +589,9 @@ def _probabilities_for(metric: int, rows: np.ndarray, policy: ExecutionPolicy,
             raise InvalidArgument("gpu_cublas_fp32 is unavailable for L1 probability "
                                   "computation; L1 distance has no "
                                   "matrix-multiplication identity")
-        return _probabilities_gpu(metric, rows, device).probabilities
+        return _probabilities_gpu(metric, rows, device,
+                                  gram=policy == ExecutionPolicy.gpu_cublas_fp32
+                                  ).probabilities
     threads = 1 if policy == ExecutionPolicy.sequential else 0
     return compute_importance_probabilities_host(
         "l2" if metric == _abi.L2 else "l1", rows, threads)

@@ -1057,11 +1057,20 @@ extern "C" uha_status uha_query(const uha_index* index, uha_workspace* ws,
 
 extern "C" uha_status uha_importance_probabilities(
     int device, uha_metric metric, const float* rows, uint64_t row_count,
-    uint64_t dimension, double* out, uha_probability_report* report)
+    uint64_t dimension, uha_pair_backend backend, uint64_t pair_chunks,
+    double* out, uha_probability_report* report)
 {
     return guarded([&] {
+        require(pair_chunks != 0, UHA_INVALID_ARGUMENT,
+                "GPU pair chunk count must be positive");
         require(metric == UHA_L2 || metric == UHA_L1, UHA_INVALID_ARGUMENT,
                 "unknown metric");
+        require(backend == UHA_PAIRS_DIRECT || backend == UHA_PAIRS_GRAM,
+                UHA_INVALID_ARGUMENT, "unknown pair-distance backend");
+        require(!(metric == UHA_L1 && backend == UHA_PAIRS_GRAM),
+                UHA_INVALID_ARGUMENT,
+                "L1 distance has no matrix-multiplication identity");
+        const bool gram = backend == UHA_PAIRS_GRAM;
         require(out != nullptr || dimension == 0, UHA_INVALID_ARGUMENT,
                 "output must not be null");
         require(rows != nullptr || row_count * dimension == 0,
@@ -1074,6 +1083,9 @@ extern "C" uha_status uha_importance_probabilities(
         }
         uha_probability_report rep{};
         rep.pair_count = row_count < 2 ? 0 : row_count * (row_count - 1) / 2;
+        rep.pair_chunks = rep.pair_count == 0
+                              ? 0
+                              : (dimension == 0 ? 1 : std::min(pair_chunks, rep.pair_count));
         for (uint64_t j = 0; j < dimension; ++j) {
             out[j] = 0.0;
         }
@@ -1093,10 +1105,12 @@ extern "C" uha_status uha_importance_probabilities(
         require(row_count <= 65535ull * 32, UHA_LENGTH_ERROR,
                 "probability construction supports at most 2097120 rows");
         DeviceGuard guard(device);
+        const uint64_t pair_bytes =
+            checked_mul(row_count, row_count * sizeof(double), "pair matrix");
         const uint64_t need = checked_add(
             checked_add(checked_mul(row_count, dimension * sizeof(float), "rows"),
-                        checked_mul(row_count, row_count * sizeof(double),
-                                    "pair matrix"),
+                        gram ? checked_add(pair_bytes, pair_bytes, "pair matrix")
+                             : pair_bytes,
                         "probability working set"),
             dimension * sizeof(double), "probability working set");
         size_t free_bytes = 0;
@@ -1130,6 +1144,7 @@ extern "C" uha_status uha_importance_probabilities(
         } event_owner{ev};
         DeviceBuffer<float> d_rows(row_count * dimension);
         DeviceBuffer<double> inverse(row_count * row_count);
+        DeviceBuffer<double> gram_matrix(gram ? row_count * row_count : 0);
         DeviceBuffer<unsigned long long> maxima(dimension);
         check_cuda(cudaEventRecord(ev[0], stream), "event");
         check_cuda(cudaMemcpyAsync(d_rows.get(), rows, d_rows.bytes(),
@@ -1141,11 +1156,22 @@ extern "C" uha_status uha_importance_probabilities(
                    "cannot clear column maxima");
         check_cuda(cudaEventRecord(ev[1], stream), "event");
         const int m = metric == UHA_L2 ? 0 : 1;
-        uha::launch_pair_distances(m, d_rows.get(), row_count, dimension,
-                                   inverse.get(), stream);
+        if (gram) {
+            uha::launch_gram_inverse_distances(d_rows.get(), row_count, dimension,
+                                               gram_matrix.get(), inverse.get(),
+                                               stream);
+        } else {
+            uha::launch_pair_distances(m, d_rows.get(), row_count, dimension,
+                                       inverse.get(), stream);
+        }
         check_cuda(cudaEventRecord(ev[2], stream), "event");
-        uha::launch_coordinate_maxima(m, d_rows.get(), row_count, dimension,
-                                      inverse.get(), maxima.get(), stream);
+        for (uint64_t c = 0; c < rep.pair_chunks; ++c) {
+            const uint64_t begin = rep.pair_count * c / rep.pair_chunks;
+            const uint64_t end = rep.pair_count * (c + 1) / rep.pair_chunks;
+            uha::launch_coordinate_maxima(m, d_rows.get(), row_count, dimension,
+                                          inverse.get(), maxima.get(), begin, end,
+                                          stream);
+        }
         check_cuda(cudaEventRecord(ev[3], stream), "event");
         std::vector<unsigned long long> bits(dimension);
         check_cuda(cudaMemcpyAsync(bits.data(), maxima.get(), maxima.bytes(),

@@ -169,10 +169,19 @@ void launch_row_norms(const float* rows, uint64_t row_count,
 void launch_pair_distances(int metric, const float* rows, uint64_t row_count,
                            uint64_t dim, double* inverse_distances,
                            cudaStream_t stream);
+// L2 pair distances through the binary64 Gram identity with direct
+// recomputation of cancellation-prone pairs; `gram` holds r x r doubles.
+void launch_gram_inverse_distances(const float* rows, uint64_t row_count,
+                                   uint64_t dim, double* gram,
+                                   double* inverse_distances,
+                                   cudaStream_t stream);
+// Folds the pairs [pair_begin, pair_end) of the row-major order of pairs
+// a < b into the per-column maxima (one launch per chunk of pairs).
 void launch_coordinate_maxima(int metric, const float* rows,
                               uint64_t row_count, uint64_t dim,
                               const double* inverse_distances,
                               unsigned long long* maxima_bits,
+                              uint64_t pair_begin, uint64_t pair_end,
                               cudaStream_t stream);
 
 }  // namespace uha

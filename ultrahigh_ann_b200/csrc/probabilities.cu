@@ -89,11 +89,105 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// Gram backend, stage 1: G[a][b] = sum_j a_j b_j in binary64 for a <= b,
+// same tiling as the pair kernel.
+__global__ void __launch_bounds__(256)
+    gram_kernel(const float* __restrict__ rows, uint32_t row_count, uint64_t dim,
+                double* __restrict__ gram)
+{
+    const uint32_t ta = blockIdx.y;
+    const uint32_t tb = blockIdx.x;
+    if (tb < ta) {
+        return;
+    }
+    __shared__ float sa[kPairBlock][kPairSlab + 1];
+    __shared__ float sb[kPairBlock][kPairSlab + 1];
+    const int ty = threadIdx.x / 8;
+    const int tx = threadIdx.x % 8;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    const uint32_t a0 = ta * kPairBlock;
+    const uint32_t b0 = tb * kPairBlock;
+    for (uint64_t c0 = 0; c0 < dim; c0 += kPairSlab) {
+        for (int i = threadIdx.x; i < kPairBlock * kPairSlab; i += blockDim.x) {
+            const int r = i / kPairSlab;
+            const int c = i % kPairSlab;
+            const uint64_t col = c0 + c;
+            float va = 0.f;
+            float vb = 0.f;
+            if (col < dim) {
+                if (a0 + r < row_count) {
+                    va = rows[static_cast<uint64_t>(a0 + r) * dim + col];
+                }
+                if (b0 + r < row_count) {
+                    vb = rows[static_cast<uint64_t>(b0 + r) * dim + col];
+                }
+            }
+            sa[r][c] = va;
+            sb[r][c] = vb;
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int c = 0; c < kPairSlab; ++c) {
+            const double va = sa[ty][c];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                acc[j] = fma(va, static_cast<double>(sb[tx + 8 * j][c]), acc[j]);
+            }
+        }
+        __syncthreads();
+    }
+    const uint32_t a = a0 + ty;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const uint32_t b = b0 + tx + 8 * j;
+        if (a < row_count && b < row_count && a <= b) {
+            gram[static_cast<uint64_t>(a) * row_count + b] = acc[j];
+        }
+    }
+}
+
+// Gram backend, stage 2: ||a - b||^2 = G_aa + G_bb - 2 G_ab. The identity's
+// absolute error is at most about (dim + 2) * 2^-53 * (G_aa + G_bb); pairs
+// where that could exceed 2^-24 of the result (binary32-level accuracy) are
+// recomputed directly as a binary64 sum of squared differences.
+__global__ void gram_to_inverse_kernel(const double* __restrict__ gram,
+                                       const float* __restrict__ rows,
+                                       uint32_t row_count, uint64_t dim,
+                                       double* __restrict__ inverse)
+{
+    const uint64_t pairs = static_cast<uint64_t>(row_count) * row_count;
+    for (uint64_t idx = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+         idx < pairs; idx += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t a = static_cast<uint32_t>(idx / row_count);
+        const uint32_t b = static_cast<uint32_t>(idx - uint64_t(a) * row_count);
+        if (a >= b) {
+            continue;
+        }
+        const double na = gram[uint64_t(a) * row_count + a];
+        const double nb = gram[uint64_t(b) * row_count + b];
+        double sd = na + nb - 2.0 * gram[idx];
+        const double cancellation =
+            static_cast<double>(dim + 2) * 1.1102230246251565e-16 * 16777216.0;
+        if (!(sd > cancellation * (na + nb))) {
+            const float* ra = rows + uint64_t(a) * dim;
+            const float* rb = rows + uint64_t(b) * dim;
+            sd = 0.0;
+            for (uint64_t j = 0; j < dim; ++j) {
+                const double d = static_cast<double>(ra[j]) - static_cast<double>(rb[j]);
+                sd = fma(d, d, sd);
+            }
+        }
+        inverse[idx] = sd != 0.0 ? 1.0 / sd : 0.0;
+    }
+}
+
 __global__ void __launch_bounds__(kColumns)
     coordinate_max_kernel(int metric, const float* __restrict__ rows,
                           uint32_t row_count, uint64_t dim,
                           const double* __restrict__ inverse,
-                          unsigned long long* __restrict__ maxima_bits)
+                          unsigned long long* __restrict__ maxima_bits,
+                          uint32_t first_block, uint64_t pair_begin,
+                          uint64_t pair_end)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     double* sinv = reinterpret_cast<double*>(smem);                 // [32][32]
@@ -102,9 +196,10 @@ __global__ void __launch_bounds__(kColumns)
 
     const uint64_t col = blockIdx.x * static_cast<uint64_t>(kColumns) +
                          threadIdx.x;
-    const uint32_t ta = blockIdx.y;
+    const uint32_t ta = first_block + blockIdx.y;
     const uint32_t a0 = ta * kPairBlock;
     const uint32_t blocks = (row_count + kPairBlock - 1) / kPairBlock;
+    const uint64_t r64 = row_count;
 
     for (int r = 0; r < kPairBlock; ++r) {
         float v = 0.f;
@@ -128,8 +223,15 @@ __global__ void __launch_bounds__(kColumns)
             const int ra = i / kPairBlock;
             const int rb = i % kPairBlock;
             double v = 0.0;
-            if (a0 + ra < row_count && b0 + rb < row_count) {
-                v = inverse[static_cast<uint64_t>(a0 + ra) * row_count + b0 + rb];
+            const uint64_t a = a0 + ra;
+            const uint64_t b = b0 + rb;
+            if (a < b && b < row_count) {
+                // position of (a, b) in the row-major order of pairs a < b;
+                // pairs outside this launch's chunk contribute nothing
+                const uint64_t pair = a * (2 * r64 - a - 1) / 2 + (b - a - 1);
+                if (pair >= pair_begin && pair < pair_end) {
+                    v = inverse[a * row_count + b];
+                }
             }
             sinv[i] = v;
         }
@@ -168,12 +270,46 @@ void launch_pair_distances(int metric, const float* rows, uint64_t row_count,
     check_cuda(cudaGetLastError(), "cannot launch pair distance kernel");
 }
 
+void launch_gram_inverse_distances(const float* rows, uint64_t row_count,
+                                   uint64_t dim, double* gram,
+                                   double* inverse_distances,
+                                   cudaStream_t stream)
+{
+    const uint32_t blocks =
+        static_cast<uint32_t>((row_count + kPairBlock - 1) / kPairBlock);
+    if (blocks > 65535u) {
+        fail(UHA_LENGTH_ERROR, "probability pair grid exceeds device limit");
+    }
+    gram_kernel<<<dim3(blocks, blocks), 256, 0, stream>>>(
+        rows, static_cast<uint32_t>(row_count), dim, gram);
+    check_cuda(cudaGetLastError(), "cannot launch Gram kernel");
+    gram_to_inverse_kernel<<<148 * 16, 256, 0, stream>>>(
+        gram, rows, static_cast<uint32_t>(row_count), dim, inverse_distances);
+    check_cuda(cudaGetLastError(), "cannot launch Gram refinement kernel");
+}
+
 void launch_coordinate_maxima(int metric, const float* rows,
                               uint64_t row_count, uint64_t dim,
                               const double* inverse_distances,
                               unsigned long long* maxima_bits,
+                              uint64_t pair_begin, uint64_t pair_end,
                               cudaStream_t stream)
 {
+    if (pair_begin >= pair_end) {
+        return;
+    }
+    // row of the first and last pair of the chunk
+    auto row_of = [&](uint64_t pair) {
+        uint64_t a = 0;
+        uint64_t before = 0;
+        while (before + (row_count - a - 1) <= pair) {
+            before += row_count - a - 1;
+            ++a;
+        }
+        return a;
+    };
+    const uint32_t first_block = static_cast<uint32_t>(row_of(pair_begin) / kPairBlock);
+    const uint32_t last_block = static_cast<uint32_t>(row_of(pair_end - 1) / kPairBlock);
     const uint32_t blocks =
         static_cast<uint32_t>((row_count + kPairBlock - 1) / kPairBlock);
     const uint64_t column_blocks = (dim + kColumns - 1) / kColumns;
@@ -191,10 +327,10 @@ void launch_coordinate_maxima(int metric, const float* rows,
                    "cannot configure probability column kernel");
         configured[dev] = true;
     }
-    const dim3 grid(static_cast<uint32_t>(column_blocks), blocks);
+    const dim3 grid(static_cast<uint32_t>(column_blocks), last_block - first_block + 1);
     coordinate_max_kernel<<<grid, kColumns, smem, stream>>>(
         metric, rows, static_cast<uint32_t>(row_count), dim, inverse_distances,
-        maxima_bits);
+        maxima_bits, first_block, pair_begin, pair_end);
     check_cuda(cudaGetLastError(), "cannot launch probability column kernel");
 }
 
