@@ -188,12 +188,10 @@ def run_engine(args):
         torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
-    elapsed_ms = start.elapsed_time(stop)
-    if world > 1:
-        t = torch.tensor([elapsed_ms], device=f"cuda:{device}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
-    value = world * n * args.steps / (elapsed_ms / 1e3)
+    from ultrahigh_ann_b200 import replicas
+    elapsed_ms = replicas.max_over_ranks(start.elapsed_time(stop),
+                                         device=f"cuda:{device}")
+    value = replicas.whole_job_rate(n * args.steps, world, elapsed_ms / 1e3)
 
     # roofline of the dominant kernel (the batch-1 stream scan)
     peaks = measured_peaks()
