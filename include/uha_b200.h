@@ -243,6 +243,20 @@ uha_status uha_query_noalloc(const uha_index* index, const float* queries,
                              uint64_t query_count, uint64_t* out_indices,
                              double* out_distances, void* stream);
 
+/* query_count queries in consecutive batches of `batch` (at most the
+ * workspace capacity), each batch answered exactly as one uha_query call
+ * would answer it. All batches are enqueued back to back on the workspace
+ * stream and the call synchronises once; host queries are copied batch by
+ * batch. A non-finite (sampled) query value anywhere fails the whole call.
+ * uha_query is uha_query_many with one batch. (No reference counterpart:
+ * the reference's benchmark loops over query_batch per chunk,
+ * src/benchmarks/nearest_neighbor_benchmark.cpp:386-413.) */
+uha_status uha_query_many(const uha_index* index, uha_workspace* workspace,
+                          const float* queries, uint64_t query_count,
+                          uint64_t batch, int queries_on_device,
+                          uha_strategy strategy, uint64_t* out_indices,
+                          double* out_distances);
+
 /* Diagnostics of the last uha_query on this workspace. */
 uha_status uha_workspace_last_stats(const uha_workspace* workspace,
                                     uha_query_stats* out);

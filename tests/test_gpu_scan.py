@@ -295,3 +295,30 @@ def test_flat_facade_defaults_to_gpu_probabilities(oracle_module):
     wb = b.make_query_workspace(4)
     assert np.array_equal(a.query_batch(SAMPLED_QUERIES, 4, None, wa),
                           b.query_batch(SAMPLED_QUERIES, 4, None, wb))
+
+
+@pytest.mark.parametrize("kind", ["exact_l2", "exact_l1", "flat_l2", "hier_l1"])
+def test_query_many_equals_per_batch_calls(oracle_module, kind):
+    ds = synthetic.row_dataset(rows=300, classes=5, queries=45, d=2000, seed=31)
+    if kind.startswith("exact"):
+        index = (uha.CudaExactL2Index if kind == "exact_l2" else uha.CudaExactL1Index)(ds.rows)
+    elif kind == "flat_l2":
+        probs = oracle_module.probabilities("l2", ds.rows)
+        index = uha.CudaSampledCoordinateL2AnnIndex(ds.rows, probs, 16, uha.MT19937_64(1))
+    else:
+        probs = oracle_module.probabilities("l1", ds.rows)
+        index = uha.CudaHierarchicalL1AnnIndex(ds.rows, 8, 16, uha.MT19937_64(2),
+                                               importance_probabilities=probs)
+    for batch in (1, 4, 9):
+        ws = index.make_query_workspace(batch)
+        dist = np.zeros(45, np.float64)
+        many = index.query_many(ds.queries, 45, batch, None, ws, distances=dist)
+        single, sdist = run(index, ds.queries, batch)
+        assert np.array_equal(many, single)
+        assert np.array_equal(dist, sdist)
+    with pytest.raises(uha.InvalidArgument):
+        index.query_many(ds.queries, 45, 10, None, index.make_query_workspace(9))
+    bad = ds.queries.copy()
+    bad[30, :] = np.nan
+    with pytest.raises(uha.InvalidArgument):
+        index.query_many(bad, 45, 4, None, index.make_query_workspace(4))

@@ -98,6 +98,8 @@ SIGNATURES = {
     "uha_workspace_info": (c_int, [c_void_p, _U, _U]),
     "uha_query": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_int, c_int,
                           c_void_p, c_void_p]),
+    "uha_query_many": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_uint64, c_int,
+                               c_int, c_void_p, c_void_p]),
     "uha_query_noalloc": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_void_p,
                                   c_void_p]),
     "uha_workspace_last_stats": (c_int, [c_void_p, POINTER(QueryStats)]),

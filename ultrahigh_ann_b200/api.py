@@ -424,6 +424,32 @@ class _CudaIndex:
                   distances)
         return out
 
+    def query_many(self, queries, query_count: int, batch: int, output,
+                   workspace: QueryWorkspace, strategy=QueryStrategy.direct,
+                   distances: Optional[np.ndarray] = None,
+                   on_device: bool = False) -> np.ndarray:
+        """query_count queries answered in consecutive batches of `batch`
+        (each batch exactly as one query_batch call), enqueued back to back
+        and synchronised once. `queries` is a host array, or a device pointer
+        (int) when on_device."""
+        if not isinstance(workspace, QueryWorkspace):
+            raise InvalidArgument("CUDA workspace belongs to a different index")
+        out = self._output(output, query_count)
+        if on_device:
+            ptr = int(queries)
+        else:
+            q = np.ascontiguousarray(queries, dtype=np.float32).reshape(-1)
+            if q.size != query_count * self._dimension:
+                raise InvalidArgument("query batch dimensions do not match index dimension")
+            ptr = q.ctypes.data if q.size else 0
+        dist_ptr = ctypes.c_void_p(distances.ctypes.data) if distances is not None else None
+        _check(_abi.load().uha_query_many(self._handle, workspace._handle,
+                                          ctypes.c_void_p(ptr), ctypes.c_uint64(query_count),
+                                          ctypes.c_uint64(batch), int(on_device),
+                                          int(strategy), ctypes.c_void_p(out.ctypes.data),
+                                          dist_ptr))
+        return out
+
     def query(self, query, workspace: QueryWorkspace,
               strategy=QueryStrategy.direct) -> int:
         q = np.ascontiguousarray(query, dtype=np.float32).reshape(-1)

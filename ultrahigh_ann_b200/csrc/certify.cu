@@ -10,7 +10,9 @@
 // One candidate means the CPU's answer is known. Otherwise the candidates are
 // re-scored by replaying the CPU's binary64 operation sequence (the same
 // operations in the same order, no contraction) and the lexicographic minimum
-// of (distance, row) is the CPU's argmin.
+// of (distance, row) is the CPU's argmin. The replay runs inside the argmin
+// kernel, in the block that merges the query's summaries, so a query batch
+// needs no host decision between its kernels.
 #include "common.h"
 #include "kernels.h"
 
@@ -20,7 +22,6 @@ namespace uha {
 namespace {
 
 constexpr int kFinalizeThreads = 256;
-constexpr int kResolveThreads = 512;
 
 struct Bounds2 {
     float lower;
@@ -157,75 +158,6 @@ __device__ Summary block_reduce_summary(Summary s)
         }
     }
     return s;  // valid in thread 0
-}
-
-__device__ void decide(const Summary& s, uint32_t q, Result* results,
-                       uint32_t* ambiguous, uint32_t* ambiguous_count,
-                       float* query_upper)
-{
-    query_upper[q] = s.min_upper;
-    if (s.second > s.min_upper) {
-        results[q] = Result{s.first_row, s.first_distance};
-    } else {
-        const uint32_t slot = atomicAdd(ambiguous_count, 1u);
-        ambiguous[slot] = q;
-        results[q] = Result{0xffffffffu, s.first_distance};
-    }
-}
-
-// grid = (row blocks, batch). Every CTA summarises kFinalizeThreads rows of
-// one query; the last CTA of a query to finish merges the block summaries.
-__global__ void __launch_bounds__(kFinalizeThreads)
-    finalize_certified_kernel(PartialView view, Bound bound, Result* results,
-                              uint32_t* ambiguous, uint32_t* ambiguous_count,
-                              Summary* block_summaries, uint32_t* done,
-                              float* query_upper)
-{
-    const uint32_t q = blockIdx.y;
-    const uint32_t blocks = gridDim.x;
-    const float inf = __int_as_float(0x7f800000);
-    Summary s{inf, inf, inf, 0xffffffffu, inf};
-    const uint32_t row = blockIdx.x * kFinalizeThreads + threadIdx.x;
-    if (row < view.rows) {
-        const float d = row_distance(view, q, row);
-        const Bounds2 b = bound_of(d, bound, row, q);
-        summary_insert(s, b.lower, b.upper, row, d);
-    }
-    s = block_reduce_summary(s);
-    if (blocks == 1) {
-        if (threadIdx.x == 0) {
-            decide(s, q, results, ambiguous, ambiguous_count, query_upper);
-        }
-        return;
-    }
-    __shared__ bool is_last;
-    if (threadIdx.x == 0) {
-        block_summaries[static_cast<uint64_t>(q) * blocks + blockIdx.x] = s;
-        __threadfence();
-        is_last = atomicAdd(done + q, 1u) == blocks - 1;
-    }
-    __syncthreads();
-    if (!is_last) {
-        return;
-    }
-    __threadfence();
-    Summary m{inf, inf, inf, 0xffffffffu, inf};
-    for (uint32_t i = threadIdx.x; i < blocks; i += kFinalizeThreads) {
-        const volatile Summary* src =
-            block_summaries + static_cast<uint64_t>(q) * blocks + i;
-        Summary b;
-        b.min_upper = src->min_upper;
-        b.first = src->first;
-        b.second = src->second;
-        b.first_row = src->first_row;
-        b.first_distance = src->first_distance;
-        m = summary_merge(m, b);
-    }
-    m = block_reduce_summary(m);
-    if (threadIdx.x == 0) {
-        decide(m, q, results, ambiguous, ambiguous_count, query_upper);
-        done[q] = 0;
-    }
 }
 
 __device__ __forceinline__ unsigned int ordered_bits(float f)
@@ -402,76 +334,139 @@ __device__ __forceinline__ bool lex_less(double a, uint32_t ar, double b,
     return a < b || (a == b && ar < br);
 }
 
-__global__ void __launch_bounds__(kResolveThreads)
-    resolve_kernel(PartialView view, Bound bound, ReplayInputs in,
-                   const uint32_t* ambiguous, uint32_t ambiguous_count,
-                   const float* query_upper, Result* results,
-                   double* exact_distances)
+// Reference binary64 query projection (l2_hierarchical_projection.cpp:186-198)
+// into `y`: y_j = sum_i double(x_i) * P[j][i] in i order, one thread per j.
+__device__ void project_query64(const ReplayInputs& in, const float* x, double* y)
 {
-    const uint32_t slot = blockIdx.x;
-    if (slot >= ambiguous_count) {
-        return;
+    for (uint64_t j = threadIdx.x; j < in.proj_dim; j += blockDim.x) {
+        const double* coeff = in.projection64 + j * in.dim;
+        double acc = 0.0;
+        for (uint64_t i = 0; i < in.dim; ++i) {
+            acc = __dadd_rn(acc, __dmul_rn(static_cast<double>(x[i]), coeff[i]));
+        }
+        y[j] = acc;
     }
-    const uint32_t q = ambiguous[slot];
-    const int warp = threadIdx.x / 32;
-    const int lane = threadIdx.x % 32;
-    constexpr int warps = kResolveThreads / 32;
+}
 
-    // U*: the smallest upper bound over all rows, recorded by finalize
-    const float min_upper = query_upper[q];
-    __shared__ double warp_best[warps];
-    __shared__ uint32_t warp_best_row[warps];
+__host__ __device__ __forceinline__ bool projected_op(ReplayOp op)
+{
+    return op == ReplayOp::l2_projected || op == ReplayOp::median_projected;
+}
 
-    const float* qrow = in.queries + static_cast<uint64_t>(q) * in.padded_dim;
-    const bool projected = in.op == ReplayOp::l2_projected ||
-                           in.op == ReplayOp::median_projected;
-    extern __shared__ double projected_query[];
-    if (projected) {
-        // the reference's binary64 query projection
-        // (l2_hierarchical_projection.cpp:186-198): y_j = sum_i double(x_i) *
-        // P[j][i] in i order, one thread per j
-        for (uint64_t j = threadIdx.x; j < in.proj_dim; j += blockDim.x) {
-            const double* coeff = in.projection64 + j * in.dim;
-            double y = 0.0;
-            for (uint64_t i = 0; i < in.dim; ++i) {
-                y = __dadd_rn(y, __dmul_rn(static_cast<double>(qrow[i]), coeff[i]));
-            }
-            projected_query[j] = y;
+// Reference distance of one candidate row, replayed by one warp.
+__device__ double replay_candidate(const ReplayInputs& in, const float* qrow,
+                                   const double* y, uint32_t row, int lane)
+{
+    if (in.op == ReplayOp::l2_projected) {
+        return replay_projected_l2(in.rows64 + uint64_t(row) * in.proj_dim, y,
+                                   in.proj_dim, lane);
+    }
+    if (in.op == ReplayOp::median_projected) {
+        return replay_median(in.rows64 + uint64_t(row) * in.proj_dim, y,
+                             in.proj_dim, lane);
+    }
+    return replay_row(in, qrow, in.rows + uint64_t(row) * in.padded_dim, lane);
+}
+
+// grid = (row blocks, batch). Every CTA summarises kFinalizeThreads rows of
+// one query; the last CTA of the query to finish merges the summaries. A
+// certified query is answered there; otherwise the same CTA replays every
+// candidate row (D - err <= U*) in binary64, one warp per candidate, and keeps
+// the lexicographic minimum of (distance, row). exact_distances[q] is the
+// replayed distance, or NaN when the query was certified.
+__global__ void __launch_bounds__(kFinalizeThreads)
+    argmin_kernel(PartialView view, Bound bound, ReplayInputs in, Result* results,
+                  double* exact_distances, Summary* block_summaries,
+                  uint32_t* done, uint32_t* replay_count)
+{
+    const uint32_t q = blockIdx.y;
+    const uint32_t blocks = gridDim.x;
+    const float inf = __int_as_float(0x7f800000);
+    Summary s{inf, inf, inf, 0xffffffffu, inf};
+    const uint32_t row = blockIdx.x * kFinalizeThreads + threadIdx.x;
+    if (row < view.rows) {
+        const float d = row_distance(view, q, row);
+        const Bounds2 b = bound_of(d, bound, row, q);
+        summary_insert(s, b.lower, b.upper, row, d);
+    }
+    s = block_reduce_summary(s);
+    __shared__ bool is_last;
+    if (blocks > 1) {
+        if (threadIdx.x == 0) {
+            block_summaries[static_cast<uint64_t>(q) * blocks + blockIdx.x] = s;
+            __threadfence();
+            is_last = atomicAdd(done + q, 1u) == blocks - 1;
         }
         __syncthreads();
+        if (!is_last) {
+            return;
+        }
+        __threadfence();
+        Summary m{inf, inf, inf, 0xffffffffu, inf};
+        for (uint32_t i = threadIdx.x; i < blocks; i += kFinalizeThreads) {
+            const volatile Summary* src =
+                block_summaries + static_cast<uint64_t>(q) * blocks + i;
+            Summary b;
+            b.min_upper = src->min_upper;
+            b.first = src->first;
+            b.second = src->second;
+            b.first_row = src->first_row;
+            b.first_distance = src->first_distance;
+            m = summary_merge(m, b);
+        }
+        s = block_reduce_summary(m);
+        if (threadIdx.x == 0) {
+            done[q] = 0;
+        }
     }
+    __shared__ bool certified;
+    __shared__ float min_upper;
+    if (threadIdx.x == 0) {
+        certified = s.second > s.min_upper;
+        min_upper = s.min_upper;
+        if (certified) {
+            results[q] = Result{s.first_row, s.first_distance};
+            exact_distances[q] = __longlong_as_double(0x7ff8000000000000ll);
+        } else {
+            atomicAdd(replay_count, 1u);
+        }
+    }
+    __syncthreads();
+    if (certified) {
+        return;
+    }
+
+    const float* qrow = in.queries + static_cast<uint64_t>(q) * in.padded_dim;
+    extern __shared__ double projected_query[];
+    if (projected_op(in.op)) {
+        project_query64(in, qrow, projected_query);
+        __syncthreads();
+    }
+    constexpr int warps = kFinalizeThreads / 32;
+    const int warp = threadIdx.x / 32;
+    const int lane = threadIdx.x % 32;
     double best = __longlong_as_double(0x7ff0000000000000ll);
     uint32_t best_row = 0xffffffffu;
     for (uint32_t base = warp * 32; base < view.rows; base += warps * 32) {
-        const uint32_t row = base + lane;
+        const uint32_t r = base + lane;
         bool candidate = false;
-        if (row < view.rows) {
-            candidate = bound_of(row_distance(view, q, row), bound, row, q).lower <=
-                        min_upper;
+        if (r < view.rows) {
+            candidate = bound_of(row_distance(view, q, r), bound, r, q).lower <= min_upper;
         }
         unsigned int mask = __ballot_sync(0xffffffffu, candidate);
         while (mask != 0u) {
             const int bit = __ffs(mask) - 1;
             mask &= mask - 1u;
             const uint32_t crow = base + bit;
-            double s;
-            if (in.op == ReplayOp::l2_projected) {
-                s = replay_projected_l2(in.rows64 + crow * in.proj_dim,
-                                        projected_query, in.proj_dim, lane);
-            } else if (in.op == ReplayOp::median_projected) {
-                s = replay_median(in.rows64 + crow * in.proj_dim,
-                                  projected_query, in.proj_dim, lane);
-            } else {
-                s = replay_row(in, qrow,
-                               in.rows + static_cast<uint64_t>(crow) * in.padded_dim,
-                               lane);
-            }
-            if (lex_less(s, crow, best, best_row)) {
-                best = s;
+            const double d = replay_candidate(in, qrow, projected_query, crow, lane);
+            if (lex_less(d, crow, best, best_row)) {
+                best = d;
                 best_row = crow;
             }
         }
     }
+    __shared__ double warp_best[warps];
+    __shared__ uint32_t warp_best_row[warps];
     if (lane == 0) {
         warp_best[warp] = best;
         warp_best_row[warp] = best_row;
@@ -494,58 +489,56 @@ __global__ void __launch_bounds__(kResolveThreads)
 // by more than 1e-5 relative when rows are close, so the reported distance is
 // replayed). One CTA per query: the binary64 projected query, then one warp
 // replays the selected row.
-__global__ void __launch_bounds__(kResolveThreads)
-    refine_kernel(ReplayInputs in, const Result* results,
-                  double* exact_distances)
+__global__ void __launch_bounds__(kFinalizeThreads)
+    refine_kernel(ReplayInputs in, const Result* results, double* exact_distances)
 {
     const uint32_t q = blockIdx.x;
     extern __shared__ double projected_query[];
     const float* qrow = in.queries + static_cast<uint64_t>(q) * in.padded_dim;
-    for (uint64_t j = threadIdx.x; j < in.proj_dim; j += blockDim.x) {
-        const double* coeff = in.projection64 + j * in.dim;
-        double y = 0.0;
-        for (uint64_t i = 0; i < in.dim; ++i) {
-            y = __dadd_rn(y, __dmul_rn(static_cast<double>(qrow[i]), coeff[i]));
-        }
-        projected_query[j] = y;
-    }
+    project_query64(in, qrow, projected_query);
     __syncthreads();
     if (threadIdx.x >= 32) {
         return;
     }
-    const int lane = threadIdx.x;
-    const uint32_t row = results[q].row;
-    const double* r = in.rows64 + static_cast<uint64_t>(row) * in.proj_dim;
-    const double s = in.op == ReplayOp::median_projected
-                         ? replay_median(r, projected_query, in.proj_dim, lane)
-                         : replay_projected_l2(r, projected_query, in.proj_dim, lane);
-    if (lane == 0) {
-        exact_distances[q] = s;
+    const double d = replay_candidate(in, qrow, projected_query, results[q].row,
+                                      threadIdx.x);
+    if (threadIdx.x == 0) {
+        exact_distances[q] = d;
     }
 }
 
-// Carves the finalize scratch region: per-(query, row block) summaries, the
-// per-query completion counters (zero between calls) and U* per query. The
-// layout depends only on the workspace capacity, never on the batch of one
-// call, so the counters stay at fixed addresses across calls.
+void set_dynamic_smem(const void* kernel, size_t smem)
+{
+    if (smem > 48 * 1024) {
+        check_cuda(cudaFuncSetAttribute(kernel,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(smem)),
+                   "cannot configure replay shared memory");
+    }
+}
+
+size_t replay_smem(const ReplayInputs& in)
+{
+    return projected_op(in.op) ? in.proj_dim * sizeof(double) : 0;
+}
+// Carves the argmin scratch region: per-(query, row block) summaries and the
+// per-query completion counters (zero between calls). The layout depends only
+// on the workspace capacity, never on the batch of one call, so the counters
+// stay at fixed addresses across calls.
 struct FinalizeScratch {
     Summary* summaries;
     uint32_t* done;
-    float* query_upper;
 };
 
-FinalizeScratch finalize_scratch(void* base, uint32_t batch, uint32_t rows)
+FinalizeScratch finalize_scratch(void* base, uint32_t capacity, uint32_t rows)
 {
     const uint64_t blocks = (rows + kFinalizeThreads - 1) / kFinalizeThreads;
     char* p = static_cast<char*>(base);
     FinalizeScratch fs;
     fs.summaries = reinterpret_cast<Summary*>(p);
-    p += batch * blocks * sizeof(Summary);
+    p += capacity * blocks * sizeof(Summary);
     p = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
     fs.done = reinterpret_cast<uint32_t*>(p);
-    p += batch * sizeof(uint32_t);
-    p = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
-    fs.query_upper = reinterpret_cast<float*>(p);
     return fs;
 }
 
@@ -555,38 +548,32 @@ void launch_refine_winners(ReplayInputs in, const Result* results,
                            uint32_t batch, double* exact_distances,
                            cudaStream_t stream)
 {
-    const size_t smem = in.proj_dim * sizeof(double);
-    if (smem > 48 * 1024) {
-        check_cuda(cudaFuncSetAttribute(refine_kernel,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(smem)),
-                   "cannot configure refine kernel");
-    }
-    refine_kernel<<<batch, kResolveThreads, smem, stream>>>(in, results,
-                                                            exact_distances);
+    const size_t smem = replay_smem(in);
+    set_dynamic_smem(reinterpret_cast<const void*>(refine_kernel), smem);
+    refine_kernel<<<batch, kFinalizeThreads, smem, stream>>>(in, results,
+                                                             exact_distances);
     check_cuda(cudaGetLastError(), "cannot launch refine kernel");
 }
 
 uint64_t finalize_scratch_bytes(uint64_t batch, uint64_t rows)
 {
     const uint64_t blocks = (rows + kFinalizeThreads - 1) / kFinalizeThreads;
-    return batch * blocks * sizeof(Summary) + batch * sizeof(uint32_t) +
-           batch * sizeof(float) + 64;
+    return batch * blocks * sizeof(Summary) + batch * sizeof(uint32_t) + 64;
 }
 
-void launch_finalize_certified(PartialView view, Bound bound, Result* results,
-                               uint32_t* ambiguous, uint32_t* ambiguous_count,
-                               void* scratch, uint64_t capacity,
-                               cudaStream_t stream)
+void launch_argmin(PartialView view, Bound bound, ReplayInputs in,
+                   Result* results, double* exact_distances, void* scratch,
+                   uint64_t capacity, uint32_t* replay_count, cudaStream_t stream)
 {
     const uint32_t blocks = (view.rows + kFinalizeThreads - 1) / kFinalizeThreads;
     FinalizeScratch fs = finalize_scratch(scratch, static_cast<uint32_t>(capacity),
                                           view.rows);
-    finalize_certified_kernel<<<dim3(blocks, view.batch), kFinalizeThreads, 0,
-                                stream>>>(view, bound, results, ambiguous,
-                                          ambiguous_count, fs.summaries, fs.done,
-                                          fs.query_upper);
-    check_cuda(cudaGetLastError(), "cannot launch finalize kernel");
+    const size_t smem = replay_smem(in);
+    set_dynamic_smem(reinterpret_cast<const void*>(argmin_kernel), smem);
+    argmin_kernel<<<dim3(blocks, view.batch), kFinalizeThreads, smem, stream>>>(
+        view, bound, in, results, exact_distances, fs.summaries, fs.done,
+        replay_count);
+    check_cuda(cudaGetLastError(), "cannot launch argmin kernel");
 }
 
 void launch_finalize_gemm(PartialView view, const float* row_norms,
@@ -596,31 +583,6 @@ void launch_finalize_gemm(PartialView view, const float* row_norms,
     finalize_gemm_kernel<<<view.batch, kFinalizeThreads, 0, stream>>>(
         view, row_norms, query_norms, results);
     check_cuda(cudaGetLastError(), "cannot launch gemm finalize kernel");
-}
-
-void launch_resolve(PartialView view, Bound bound, ReplayInputs in,
-                    const uint32_t* ambiguous, uint32_t ambiguous_count,
-                    void* scratch, uint64_t capacity, Result* results,
-                    double* exact_distances, cudaStream_t stream)
-{
-    if (ambiguous_count == 0) {
-        return;
-    }
-    FinalizeScratch fs = finalize_scratch(scratch, static_cast<uint32_t>(capacity),
-                                          view.rows);
-    const bool projected = in.op == ReplayOp::l2_projected ||
-                           in.op == ReplayOp::median_projected;
-    const size_t smem = projected ? in.proj_dim * sizeof(double) : 0;
-    if (smem > 48 * 1024) {
-        check_cuda(cudaFuncSetAttribute(resolve_kernel,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(smem)),
-                   "cannot configure resolve kernel");
-    }
-    resolve_kernel<<<ambiguous_count, kResolveThreads, smem, stream>>>(
-        view, bound, in, ambiguous, ambiguous_count, fs.query_upper, results,
-        exact_distances);
-    check_cuda(cudaGetLastError(), "cannot launch resolve kernel");
 }
 
 }  // namespace uha

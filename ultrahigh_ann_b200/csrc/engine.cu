@@ -673,9 +673,8 @@ extern "C" uha_status uha_workspace_create(const uha_index* index,
             ws->prepared.allocate(b * index->padded_dim);
         }
         ws->query_norms.allocate(b);
-        ws->results.allocate(b);
-        ws->exact.allocate(b);
-        ws->ambiguous.allocate(b);
+        ws->call_results.allocate(b);
+        ws->call_exact.allocate(b);
         ws->counters.allocate(2);
         ws->finalize_scratch.allocate(
             uha::finalize_scratch_bytes(b, index->rows));
@@ -750,184 +749,310 @@ extern "C" uha_status uha_workspace_last_stats(const uha_workspace* workspace,
 
 // ------------------------------------------------------------------ query
 
+namespace {
+
+// One query batch's kernels on the workspace stream: gather / copy with
+// validation, (projection), scan, certified argmin with in-kernel replay (or
+// the norm identity), (the replayed distance of each selected row of a
+// hierarchy). `results` / `exact` receive this batch's answers; flags and the
+// replay count accumulate in ws.counters.
+struct BatchContext {
+    const uha_index* index;
+    uha_workspace* ws;
+    uha_strategy strategy;
+    bool want_distances;
+};
+
+uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
+                       uha::Result* results, double* exact, bool time_scan,
+                       cudaEvent_t scan_start, cudaEvent_t scan_stop)
+{
+    const uha_index* index = c.index;
+    uha_workspace* ws = c.ws;
+    cudaStream_t stream = ws->stream;
+    int* error_flag = reinterpret_cast<int*>(ws->counters.get() + 1);
+    uint32_t* replay_count = ws->counters.get();
+    uint64_t launches = 0;
+
+    const bool hierarchical = index->kind == IndexKind::hierarchical;
+    const float* scan_queries = ws->prepared.get();
+    if (hierarchical) {
+        uha::launch_prepare_sampled(source, n, index->dimension, index->columns.get(),
+                                    nullptr, index->sample_size, ws->prepared.get(),
+                                    index->padded_sample, error_flag, stream);
+        uha::launch_project_queries(
+            ws->prepared.get(), n, index->padded_sample, index->sample_size,
+            index->projection32.get(), index->projection_dimension,
+            ws->projected.get(), index->padded_dim, ws->query_err.get(),
+            projection_error_per_abs(index->sample_size), index->metric == UHA_L2,
+            error_flag, stream);
+        scan_queries = ws->projected.get();
+        launches += 3;
+    } else if (index->kind == IndexKind::sampled) {
+        uha::launch_prepare_sampled(
+            source, n, index->dimension, index->columns.get(),
+            index->metric == UHA_L2 ? index->scales.get() : nullptr,
+            index->sample_size, ws->prepared.get(), index->padded_dim, error_flag,
+            stream);
+        ++launches;
+    } else {
+        uha::launch_prepare_dense(source, n, index->dimension, ws->prepared.get(),
+                                  index->padded_dim, error_flag, stream);
+        ++launches;
+    }
+
+    const bool gemm = c.strategy == UHA_GEMM && index->metric == UHA_L2;
+    uha::ScanOp op = uha::ScanOp::l2;
+    if (gemm) {
+        op = uha::ScanOp::dot;
+    } else if (index->metric == UHA_L1) {
+        op = index->weights32.size() != 0 ? uha::ScanOp::l1_weighted : uha::ScanOp::l1;
+    }
+    const bool median = hierarchical && index->metric == UHA_L1;
+    uha::ScanPlan plan = uha::plan_scan(index->rows, index->padded_dim, n,
+                                        index->sm_count);
+    if (median) {
+        plan.chunks = 1;
+        plan.depth = 0;
+    }
+    const uint64_t partial_count =
+        checked_mul(checked_mul(plan.chunks, n, "partials"), index->rows, "partials");
+    if (ws->partials.size() < partial_count) {
+        // Grows to the largest plan used so far; the previous contents are not
+        // needed (stream order: earlier kernels have consumed them).
+        check_cuda(cudaStreamSynchronize(stream), "CUDA query failed");
+        ws->partials.allocate(partial_count);
+    }
+    if (time_scan) {
+        check_cuda(cudaEventRecord(scan_start, stream), "event");
+    }
+    if (median) {
+        uha::launch_median_scan(index->scan_rows.get(), index->rows, index->padded_dim,
+                                index->projection_dimension, scan_queries, n,
+                                ws->partials.get(), stream);
+    } else {
+        uha::launch_scan(plan, op, index->scan_rows.get(), index->rows,
+                         index->padded_dim, index->weights32.get(), scan_queries, n,
+                         ws->partials.get(), stream);
+    }
+    if (time_scan) {
+        check_cuda(cudaEventRecord(scan_stop, stream), "event");
+    }
+    ++launches;
+
+    const uha::PartialView view{ws->partials.get(), plan.chunks,
+                                static_cast<uint32_t>(n),
+                                static_cast<uint32_t>(index->rows)};
+    if (gemm) {
+        uha::launch_query_norms(scan_queries, n, index->padded_dim,
+                                ws->query_norms.get(), stream);
+        uha::launch_finalize_gemm(view, index->row_norms.get(), ws->query_norms.get(),
+                                  results, stream);
+        check_cuda(cudaMemsetAsync(exact, 0xff, n * sizeof(double), stream),
+                   "cannot clear distances");
+        return launches + 2;
+    }
+
+    const int term_roundings = op == uha::ScanOp::l1 ? 1 : 2;
+    uha::Bound bound = make_bound(plan.depth, index->scan_dim, term_roundings);
+    uha::ReplayInputs in{};
+    in.rows = index->scan_rows.get();
+    in.queries = ws->prepared.get();
+    in.dim = index->scan_dim;
+    in.padded_dim = index->padded_dim;
+    in.weights64 = index->weights64.get();
+    if (hierarchical) {
+        bound.row_err = index->row_err.get();
+        bound.query_err = ws->query_err.get();
+        if (median) {
+            // binary32 |diff| and midpoint roundings; the binary64 ones
+            bound.mode = uha::BoundMode::median;
+            bound.rel = std::ldexp(6.0f, -24);
+            bound.abs = std::ldexp(1.0f, -126);
+        } else {
+            bound.mode = uha::BoundMode::projected_l2;
+            const double n64 = static_cast<double>(index->scan_dim) + 3;
+            const double g64 = n64 * std::ldexp(1.0, -53);
+            bound.cpu_rel = std::nextafter(static_cast<float>(1.01 * g64), 1.0f);
+        }
+        in.op = median ? uha::ReplayOp::median_projected : uha::ReplayOp::l2_projected;
+        in.dim = index->sample_size;
+        in.padded_dim = index->padded_sample;
+        in.rows64 = index->rows64.get();
+        in.projection64 = index->projection64.get();
+        in.proj_dim = index->projection_dimension;
+    } else if (index->metric == UHA_L2) {
+        in.op = uha::ReplayOp::l2_sequential;
+    } else if (index->weights64.size() != 0) {
+        in.op = uha::ReplayOp::l1_weighted_sequential;
+    } else {
+        in.op = uha::ReplayOp::l1_grouped4;
+    }
+    uha::launch_argmin(view, bound, in, results, exact, ws->finalize_scratch.get(),
+                       ws->max_batch, replay_count, stream);
+    ++launches;
+    if (hierarchical && c.want_distances) {
+        // reported distances of a hierarchy: the reference's binary64 value of
+        // each selected row
+        uha::launch_refine_winners(in, results, static_cast<uint32_t>(n), exact, stream);
+        ++launches;
+    }
+    return launches;
+}
+
+void fill_trivial(uint64_t n, uint64_t* out_indices, double* out_distances)
+{
+    for (uint64_t q = 0; q < n; ++q) {
+        out_indices[q] = 0;
+        if (out_distances != nullptr) {
+            out_distances[q] = 0.0;
+        }
+    }
+}
+
+// The host side of one call: check the status words (synchronised), then
+// convert Result / replayed distances into the caller's arrays.
+void finish_call(const uha_index* index, uha_workspace* ws, uint64_t n,
+                 const uha::Result* results, const double* exact,
+                 uint64_t* out_indices, double* out_distances)
+{
+    const uint32_t flag = ws->host_counters.get()[1];
+    if (flag != 0) {
+        if ((flag & 1u) && index->kind == IndexKind::hierarchical) {
+            fail(UHA_INVALID_ARGUMENT, "sampled query coordinate must be finite");
+        }
+        if (flag & 4u) {
+            fail(UHA_OVERFLOW_ERROR, "projected query is not finite");
+        }
+        if (index->kind == IndexKind::sampled) {
+            fail(UHA_INVALID_ARGUMENT,
+                 (flag & 1u) ? "sampled query coordinate must be finite"
+                             : "weighted sampled query coordinate must be finite");
+        }
+        fail(UHA_INVALID_ARGUMENT, "queries must be finite");
+    }
+    for (uint64_t q = 0; q < n; ++q) {
+        out_indices[q] = results[q].row;
+        if (out_distances != nullptr) {
+            out_distances[q] = std::isnan(exact[q]) ? static_cast<double>(results[q].distance)
+                                                    : exact[q];
+        }
+    }
+    const uint32_t replayed = ws->host_counters.get()[0];
+    ws->last.replayed_queries = replayed;
+    ws->last.certified_queries = n - std::min<uint64_t>(n, replayed);
+}
+
+void validate_query_call(const uha_index* index, uha_workspace* ws,
+                         const float* queries, uint64_t count, uint64_t batch,
+                         uha_strategy strategy, const uint64_t* out_indices)
+{
+    require(index != nullptr, UHA_INVALID_ARGUMENT, "index must not be null");
+    require(ws != nullptr && ws->owner == index, UHA_INVALID_ARGUMENT,
+            "CUDA workspace belongs to a different index");
+    require(batch <= ws->max_batch, UHA_INVALID_ARGUMENT,
+            "query count exceeds CUDA workspace capacity");
+    require(strategy == UHA_DIRECT || strategy == UHA_GEMM, UHA_INVALID_ARGUMENT,
+            "unknown CUDA query strategy");
+    if (count != 0) {
+        require(out_indices != nullptr, UHA_INVALID_ARGUMENT, "output must not be null");
+        require(queries != nullptr || index->dimension == 0, UHA_INVALID_ARGUMENT,
+                "query pointer must not be null");
+    }
+}
+
+// Event pairs for timing the scan of every batch of a call.
+void ensure_scan_events(uha_workspace* ws, uint64_t batches)
+{
+    while (ws->scan_events.size() < 2 * batches) {
+        cudaEvent_t e = nullptr;
+        check_cuda(cudaEventCreate(&e), "cannot create CUDA event");
+        ws->scan_events.push_back(e);
+    }
+}
+
+}  // namespace
+
 extern "C" uha_status uha_query(const uha_index* index, uha_workspace* ws,
                                 const float* queries, uint64_t query_count,
                                 int queries_on_device, uha_strategy strategy,
                                 uint64_t* out_indices, double* out_distances)
 {
+    return uha_query_many(index, ws, queries, query_count, query_count == 0 ? 1 : query_count,
+                          queries_on_device, strategy, out_indices, out_distances);
+}
+
+extern "C" uha_status uha_query_many(const uha_index* index, uha_workspace* ws,
+                                     const float* queries, uint64_t query_count,
+                                     uint64_t batch, int queries_on_device,
+                                     uha_strategy strategy, uint64_t* out_indices,
+                                     double* out_distances)
+{
     return guarded([&] {
-        require(index != nullptr, UHA_INVALID_ARGUMENT, "index must not be null");
-        require(ws != nullptr && ws->owner == index, UHA_INVALID_ARGUMENT,
-                "CUDA workspace belongs to a different index");
-        require(query_count <= ws->max_batch, UHA_INVALID_ARGUMENT,
-                "query count exceeds CUDA workspace capacity");
-        require(strategy == UHA_DIRECT || strategy == UHA_GEMM,
-                UHA_INVALID_ARGUMENT, "unknown CUDA query strategy");
+        require(batch != 0, UHA_INVALID_ARGUMENT, "batch size must be positive");
+        validate_query_call(index, ws, queries, query_count,
+                            std::min(batch, query_count == 0 ? batch : query_count),
+                            strategy, out_indices);
         ws->last = uha_query_stats{};
         ws->last.query_count = query_count;
         if (query_count == 0) {
             return;
         }
-        require(out_indices != nullptr, UHA_INVALID_ARGUMENT,
-                "output must not be null");
-        require(queries != nullptr || index->dimension == 0,
-                UHA_INVALID_ARGUMENT, "query pointer must not be null");
+        if ((index->kind == IndexKind::hierarchical && index->rows == 1) ||
+            index->padded_dim == 0) {
+            // A one-row hierarchy answers row 0 without projecting (or
+            // validating) the query (hierarchical_l2_ann_index.cpp:164-166);
+            // with no sampled coordinate every distance is zero and row 0 wins.
+            fill_trivial(query_count, out_indices, out_distances);
+            ws->last.certified_queries = query_count;
+            return;
+        }
 
         DeviceGuard guard(index->device);
         uha::clear_stale_cuda_error();
         cudaStream_t stream = ws->stream;
         const uint64_t n = query_count;
-
-        if (index->kind == IndexKind::hierarchical && index->rows == 1) {
-            // A one-row hierarchy answers row 0 without projecting (or
-            // validating) the query (hierarchical_l2_ann_index.cpp:164-166).
-            for (uint64_t q = 0; q < n; ++q) {
-                out_indices[q] = 0;
-                if (out_distances != nullptr) {
-                    out_distances[q] = 0.0;
-                }
-            }
-            ws->last.certified_queries = n;
-            return;
+        const uint64_t batches = (n + batch - 1) / batch;
+        // device-side answers of the whole call
+        if (ws->call_results.size() < n) {
+            ws->call_results.allocate(n);
+            ws->call_exact.allocate(n);
+            ws->host_results.allocate(n);
+            ws->host_exact.allocate(n);
         }
-        if (index->padded_dim == 0) {
-            // Nothing to compare: every distance is zero and row 0 wins
-            // (empty sample or zero dimension).
-            for (uint64_t q = 0; q < n; ++q) {
-                out_indices[q] = 0;
-                if (out_distances != nullptr) {
-                    out_distances[q] = 0.0;
-                }
-            }
-            ws->last.certified_queries = n;
-            return;
-        }
-
         if (ws->timing) {
+            ensure_scan_events(ws, batches);
             check_cuda(cudaEventRecord(ws->events[0], stream), "event");
         }
-        const float* source = queries;
-        if (!queries_on_device) {
-            check_cuda(cudaMemcpyAsync(ws->raw_queries.get(), queries,
-                                       n * index->dimension * sizeof(float),
-                                       cudaMemcpyHostToDevice, stream),
-                       "cannot copy queries to the CUDA device");
-            source = ws->raw_queries.get();
-        }
-        check_cuda(cudaMemsetAsync(ws->counters.get(), 0,
-                                   ws->counters.bytes(), stream),
+        check_cuda(cudaMemsetAsync(ws->counters.get(), 0, ws->counters.bytes(), stream),
                    "cannot clear query counters");
-        int* error_flag = reinterpret_cast<int*>(ws->counters.get() + 1);
-        uint64_t launches = 1;
-        const bool hierarchical = index->kind == IndexKind::hierarchical;
-        const float* scan_queries = ws->prepared.get();
-        if (hierarchical) {
-            uha::launch_prepare_sampled(source, n, index->dimension,
-                                        index->columns.get(), nullptr,
-                                        index->sample_size, ws->prepared.get(),
-                                        index->padded_sample, error_flag, stream);
-            uha::launch_project_queries(
-                ws->prepared.get(), n, index->padded_sample, index->sample_size,
-                index->projection32.get(), index->projection_dimension,
-                ws->projected.get(), index->padded_dim, ws->query_err.get(),
-                projection_error_per_abs(index->sample_size),
-                index->metric == UHA_L2, error_flag, stream);
-            scan_queries = ws->projected.get();
-            launches += 2;
-        } else if (index->kind == IndexKind::sampled) {
-            uha::launch_prepare_sampled(
-                source, n, index->dimension, index->columns.get(),
-                index->metric == UHA_L2 ? index->scales.get() : nullptr,
-                index->sample_size, ws->prepared.get(), index->padded_dim,
-                error_flag, stream);
-        } else {
-            uha::launch_prepare_dense(source, n, index->dimension,
-                                      ws->prepared.get(), index->padded_dim,
-                                      error_flag, stream);
-        }
-
-        const bool gemm = strategy == UHA_GEMM && index->metric == UHA_L2;
-        uha::ScanOp op = uha::ScanOp::l2;
-        if (gemm) {
-            op = uha::ScanOp::dot;
-        } else if (index->metric == UHA_L1) {
-            op = index->weights32.size() != 0 ? uha::ScanOp::l1_weighted
-                                              : uha::ScanOp::l1;
-        }
-        const bool median = hierarchical && index->metric == UHA_L1;
-        uha::ScanPlan plan = uha::plan_scan(index->rows, index->padded_dim, n,
-                                            index->sm_count);
-        if (median) {
-            plan.chunks = 1;
-            plan.depth = 0;
-        }
-        const uint64_t partial_count =
-            checked_mul(checked_mul(plan.chunks, n, "partials"), index->rows,
-                        "partials");
-        if (ws->partials.size() < partial_count) {
-            // Grows once per workspace to the largest plan used so far.
-            ws->partials.allocate(partial_count);
-        }
-        if (ws->timing) {
-            check_cuda(cudaEventRecord(ws->events[1], stream), "event");
-        }
-        if (median) {
-            uha::launch_median_scan(index->scan_rows.get(), index->rows,
-                                    index->padded_dim, index->projection_dimension,
-                                    scan_queries, n, ws->partials.get(), stream);
-        } else {
-            uha::launch_scan(plan, op, index->scan_rows.get(), index->rows,
-                             index->padded_dim, index->weights32.get(),
-                             scan_queries, n, ws->partials.get(), stream);
-        }
-        if (ws->timing) {
-            check_cuda(cudaEventRecord(ws->events[2], stream), "event");
-        }
-        ++launches;
-
-        const uha::PartialView view{ws->partials.get(), plan.chunks,
-                                    static_cast<uint32_t>(n),
-                                    static_cast<uint32_t>(index->rows)};
-        const int term_roundings = op == uha::ScanOp::l1 ? 1 : 2;
-        uha::Bound bound = make_bound(plan.depth, index->scan_dim, term_roundings);
-        if (hierarchical) {
-            bound.row_err = index->row_err.get();
-            bound.query_err = ws->query_err.get();
-            if (median) {
-                // binary32 |diff| and midpoint roundings; the binary64 ones
-                bound.mode = uha::BoundMode::median;
-                bound.rel = std::ldexp(6.0f, -24);
-                bound.abs = std::ldexp(1.0f, -126);
-            } else {
-                bound.mode = uha::BoundMode::projected_l2;
-                const double n64 = static_cast<double>(index->scan_dim) + 3;
-                const double g64 = n64 * std::ldexp(1.0, -53);
-                bound.cpu_rel =
-                    std::nextafter(static_cast<float>(1.01 * g64), 1.0f);
+        const BatchContext ctx{index, ws, strategy, out_distances != nullptr};
+        uint64_t launches = 0;
+        for (uint64_t b = 0; b < batches; ++b) {
+            const uint64_t start = b * batch;
+            const uint64_t count = std::min(batch, n - start);
+            const float* source = queries + start * index->dimension;
+            if (!queries_on_device) {
+                check_cuda(cudaMemcpyAsync(ws->raw_queries.get(), source,
+                                           count * index->dimension * sizeof(float),
+                                           cudaMemcpyHostToDevice, stream),
+                           "cannot copy queries to the CUDA device");
+                source = ws->raw_queries.get();
             }
+            launches += enqueue_batch(ctx, source, count, ws->call_results.get() + start,
+                                      ws->call_exact.get() + start, ws->timing,
+                                      ws->timing ? ws->scan_events[2 * b] : nullptr,
+                                      ws->timing ? ws->scan_events[2 * b + 1] : nullptr);
         }
-        if (gemm) {
-            uha::launch_query_norms(scan_queries, n, index->padded_dim,
-                                    ws->query_norms.get(), stream);
-            uha::launch_finalize_gemm(view, index->row_norms.get(),
-                                      ws->query_norms.get(), ws->results.get(),
-                                      stream);
-            launches += 2;
-        } else {
-            uha::launch_finalize_certified(view, bound, ws->results.get(),
-                                           ws->ambiguous.get(),
-                                           ws->counters.get(),
-                                           ws->finalize_scratch.get(),
-                                           ws->max_batch, stream);
-            ++launches;
-        }
-        check_cuda(cudaMemcpyAsync(ws->host_results.get(), ws->results.get(),
-                                   n * sizeof(uha::Result),
-                                   cudaMemcpyDeviceToHost, stream),
-                   "cannot copy query results from the CUDA device");
-        check_cuda(cudaMemcpyAsync(ws->host_counters.get(), ws->counters.get(),
-                                   ws->counters.bytes(), cudaMemcpyDeviceToHost,
+        check_cuda(cudaMemcpyAsync(ws->host_results.get(), ws->call_results.get(),
+                                   n * sizeof(uha::Result), cudaMemcpyDeviceToHost,
                                    stream),
+                   "cannot copy query results from the CUDA device");
+        check_cuda(cudaMemcpyAsync(ws->host_exact.get(), ws->call_exact.get(),
+                                   n * sizeof(double), cudaMemcpyDeviceToHost, stream),
+                   "cannot copy query distances from the CUDA device");
+        check_cuda(cudaMemcpyAsync(ws->host_counters.get(), ws->counters.get(),
+                                   ws->counters.bytes(), cudaMemcpyDeviceToHost, stream),
                    "cannot copy query counters from the CUDA device");
         if (ws->timing) {
             check_cuda(cudaEventRecord(ws->events[3], stream), "event");
@@ -935,121 +1060,20 @@ extern "C" uha_status uha_query(const uha_index* index, uha_workspace* ws,
         check_cuda(cudaStreamSynchronize(stream), "CUDA query failed");
         if (ws->timing) {
             float ms = 0.f;
-            check_cuda(cudaEventElapsedTime(&ms, ws->events[1], ws->events[2]),
-                       "event");
-            ws->last.scan_ms = ms;
-            check_cuda(cudaEventElapsedTime(&ms, ws->events[0], ws->events[3]),
-                       "event");
+            double scan = 0.0;
+            for (uint64_t b = 0; b < batches; ++b) {
+                check_cuda(cudaEventElapsedTime(&ms, ws->scan_events[2 * b],
+                                                ws->scan_events[2 * b + 1]),
+                           "event");
+                scan += ms;
+            }
+            ws->last.scan_ms = scan;
+            check_cuda(cudaEventElapsedTime(&ms, ws->events[0], ws->events[3]), "event");
             ws->last.device_ms = ms;
         }
-
-        const uint32_t flag = ws->host_counters.get()[1];
-        if (flag != 0) {
-            if (flag & 1u && hierarchical) {
-                fail(UHA_INVALID_ARGUMENT, "sampled query coordinate must be finite");
-            }
-            if (flag & 4u) {
-                fail(UHA_OVERFLOW_ERROR, "projected query is not finite");
-            }
-            if (index->kind == IndexKind::sampled) {
-                fail(UHA_INVALID_ARGUMENT,
-                     (flag & 1u) ? "sampled query coordinate must be finite"
-                                 : "weighted sampled query coordinate must be "
-                                   "finite");
-            }
-            fail(UHA_INVALID_ARGUMENT, "queries must be finite");
-        }
-        const uint32_t ambiguous = gemm ? 0 : ws->host_counters.get()[0];
-        std::vector<uint32_t> replayed;
-        if (ambiguous != 0) {
-            uha::ReplayInputs in{};
-            in.rows = index->scan_rows.get();
-            in.queries = ws->prepared.get();
-            in.dim = index->scan_dim;
-            in.padded_dim = index->padded_dim;
-            in.weights64 = index->weights64.get();
-            if (hierarchical) {
-                in.op = median ? uha::ReplayOp::median_projected
-                               : uha::ReplayOp::l2_projected;
-                in.dim = index->sample_size;
-                in.padded_dim = index->padded_sample;
-                in.rows64 = index->rows64.get();
-                in.projection64 = index->projection64.get();
-                in.proj_dim = index->projection_dimension;
-            } else if (index->metric == UHA_L2) {
-                in.op = uha::ReplayOp::l2_sequential;
-            } else if (index->weights64.size() != 0) {
-                in.op = uha::ReplayOp::l1_weighted_sequential;
-            } else {
-                in.op = uha::ReplayOp::l1_grouped4;
-            }
-            uha::launch_resolve(view, bound, in, ws->ambiguous.get(), ambiguous,
-                                ws->finalize_scratch.get(), ws->max_batch,
-                                ws->results.get(), ws->exact.get(), stream);
-            ++launches;
-            replayed.resize(ambiguous);
-            check_cuda(cudaMemcpyAsync(replayed.data(), ws->ambiguous.get(),
-                                       ambiguous * sizeof(uint32_t),
-                                       cudaMemcpyDeviceToHost, stream),
-                       "cannot copy replay list from the CUDA device");
-            check_cuda(cudaMemcpyAsync(ws->host_results.get(), ws->results.get(),
-                                       n * sizeof(uha::Result),
-                                       cudaMemcpyDeviceToHost, stream),
-                       "cannot copy query results from the CUDA device");
-            check_cuda(cudaMemcpyAsync(ws->host_exact.get(), ws->exact.get(),
-                                       n * sizeof(double),
-                                       cudaMemcpyDeviceToHost, stream),
-                       "cannot copy replayed distances from the CUDA device");
-            if (ws->timing) {
-                check_cuda(cudaEventRecord(ws->events[3], stream), "event");
-            }
-            check_cuda(cudaStreamSynchronize(stream), "CUDA replay failed");
-            if (ws->timing) {
-                float ms = 0.f;
-                check_cuda(cudaEventElapsedTime(&ms, ws->events[0], ws->events[3]),
-                           "event");
-                ws->last.device_ms = ms;
-            }
-        }
-        const bool refine = hierarchical && !gemm && out_distances != nullptr;
-        if (refine) {
-            // reported distances of a hierarchy: the reference's binary64
-            // value of each selected row
-            uha::ReplayInputs in{};
-            in.op = median ? uha::ReplayOp::median_projected
-                           : uha::ReplayOp::l2_projected;
-            in.queries = ws->prepared.get();
-            in.dim = index->sample_size;
-            in.padded_dim = index->padded_sample;
-            in.rows64 = index->rows64.get();
-            in.projection64 = index->projection64.get();
-            in.proj_dim = index->projection_dimension;
-            uha::launch_refine_winners(in, ws->results.get(),
-                                       static_cast<uint32_t>(n), ws->exact.get(),
-                                       stream);
-            ++launches;
-            check_cuda(cudaMemcpyAsync(ws->host_exact.get(), ws->exact.get(),
-                                       n * sizeof(double), cudaMemcpyDeviceToHost,
-                                       stream),
-                       "cannot copy refined distances from the CUDA device");
-            check_cuda(cudaStreamSynchronize(stream), "CUDA refine failed");
-        }
-        const uha::Result* res = ws->host_results.get();
-        for (uint64_t q = 0; q < n; ++q) {
-            out_indices[q] = res[q].row;
-            if (out_distances != nullptr) {
-                out_distances[q] = refine ? ws->host_exact.get()[q]
-                                          : static_cast<double>(res[q].distance);
-            }
-        }
-        for (uint32_t q : replayed) {
-            if (out_distances != nullptr) {
-                out_distances[q] = ws->host_exact.get()[q];
-            }
-        }
-        ws->last.certified_queries = n - ambiguous;
-        ws->last.replayed_queries = ambiguous;
         ws->last.kernel_launches = launches;
+        finish_call(index, ws, n, ws->host_results.get(), ws->host_exact.get(),
+                    out_indices, out_distances);
     });
 }
 

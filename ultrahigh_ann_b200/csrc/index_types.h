@@ -7,6 +7,7 @@
 
 #include <cstdint>
 #include <string>
+#include <vector>
 
 namespace uha {
 
@@ -61,10 +62,9 @@ struct uha_workspace {
     uha::DeviceBuffer<float> query_err;   // hierarchical: batch
     uha::DeviceBuffer<float> query_norms;
     uha::DeviceBuffer<float> partials;
-    uha::DeviceBuffer<uha::Result> results;
-    uha::DeviceBuffer<double> exact;
-    uha::DeviceBuffer<uint32_t> ambiguous;
-    uha::DeviceBuffer<uint32_t> counters;  // [0] ambiguous count, [1] error flag
+    uha::DeviceBuffer<uha::Result> call_results;  // one call's answers
+    uha::DeviceBuffer<double> call_exact;         // replayed distances (NaN: none)
+    uha::DeviceBuffer<uint32_t> counters;  // [0] replayed queries, [1] error flag
     uha::DeviceBuffer<unsigned char> finalize_scratch;
     uha::PinnedBuffer<uha::Result> host_results;
     uha::PinnedBuffer<double> host_exact;
@@ -72,6 +72,7 @@ struct uha_workspace {
     uha_query_stats last{};
     bool timing = false;
     cudaEvent_t events[4] = {nullptr, nullptr, nullptr, nullptr};
+    std::vector<cudaEvent_t> scan_events;  // start/stop of each batch's scan
 
     ~uha_workspace()
     {
@@ -79,6 +80,9 @@ struct uha_workspace {
             if (e != nullptr) {
                 cudaEventDestroy(e);
             }
+        }
+        for (cudaEvent_t e : scan_events) {
+            cudaEventDestroy(e);
         }
         if (stream != nullptr) {
             cudaStreamDestroy(stream);

@@ -88,24 +88,8 @@ void launch_scan(const ScanPlan& plan, ScanOp op, const float* rows,
                  cudaStream_t stream);
 
 // ---- certification
-// Sums partials per (query,row), applies the bound, writes certified results
-// and appends uncertified query ids to `ambiguous` (count in *ambiguous_count).
-// Scratch of the certified finalize/resolve pair (per-query merge state). It
-// must be zero when the workspace is created; finalize leaves its counters at
-// zero after every call.
-uint64_t finalize_scratch_bytes(uint64_t batch, uint64_t rows);
-// `capacity` is the batch capacity the scratch was sized for
-// (finalize_scratch_bytes); view.batch may be smaller.
-void launch_finalize_certified(PartialView view, Bound bound, Result* results,
-                               uint32_t* ambiguous, uint32_t* ambiguous_count,
-                               void* scratch, uint64_t capacity,
-                               cudaStream_t stream);
-// Binary32 norm identity (no certification), lowest index on ties.
-void launch_finalize_gemm(PartialView view, const float* row_norms,
-                          const float* query_norms, Result* results,
-                          cudaStream_t stream);
-// Replays the reference CPU arithmetic for every candidate row of each
-// ambiguous query and writes the exact winner.
+// Everything the binary64 replay of a query needs: the reference CPU's
+// operation sequence (`op`) and the operands it reads.
 struct ReplayInputs {
     ReplayOp op;
     const float* rows;         // [rows][padded_dim]
@@ -118,10 +102,23 @@ struct ReplayInputs {
     const double* projection64 = nullptr;  // projected ops: [proj_dim][dim]
     uint64_t proj_dim = 0;
 };
-void launch_resolve(PartialView view, Bound bound, ReplayInputs in,
-                    const uint32_t* ambiguous, uint32_t ambiguous_count,
-                    void* scratch, uint64_t capacity, Result* results,
-                    double* exact_distances, cudaStream_t stream);
+
+// Scratch of the argmin (per-query merge state, layout fixed by the workspace
+// capacity). It must be zero when the workspace is created; the argmin leaves
+// its counters at zero after every call.
+uint64_t finalize_scratch_bytes(uint64_t batch, uint64_t rows);
+// Certified argmin with lowest-index tie-break of every query of the view;
+// uncertified queries are settled in the same kernel by the binary64 replay.
+// results[q] receives the row; exact_distances[q] the replayed distance or
+// NaN when the query was certified. *replay_count counts replayed queries.
+void launch_argmin(PartialView view, Bound bound, ReplayInputs in,
+                   Result* results, double* exact_distances, void* scratch,
+                   uint64_t capacity, uint32_t* replay_count,
+                   cudaStream_t stream);
+// Binary32 norm identity (no certification), lowest index on ties.
+void launch_finalize_gemm(PartialView view, const float* row_norms,
+                          const float* query_norms, Result* results,
+                          cudaStream_t stream);
 
 // Reference binary64 distance of every query's selected row (projected
 // replay ops only).

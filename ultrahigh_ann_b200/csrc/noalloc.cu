@@ -12,7 +12,7 @@
 //
 // The scratch every step of the pipeline writes (the prepared queries, the
 // per-chunk partial distances, the certified-argmin merge state, the results
-// before conversion and the status counters) lives in one file-scope
+// and replayed distances before conversion, and the status counters) lives in one file-scope
 // __device__ array of kNoAllocScratchBytes. Every GPU that loads the library
 // holds that array until the process exits. Host code never uses the array's
 // name as an address: on each device, the first call looks the address up
@@ -133,7 +133,6 @@ extern "C" uha_status uha_query_noalloc(const uha_index* index,
                                                   n, index->sm_count);
         Carver c{static_cast<unsigned char*>(scratch_address(index->device))};
         uint32_t* counters = c.take<uint32_t>(4);  // [0] replay count, [1] error flag
-        uint32_t* ambiguous = c.take<uint32_t>(n);
         uha::Result* results = c.take<uha::Result>(n);
         double* replayed = c.take<double>(n);
         float* prepared = c.take<float>(n * index->padded_dim);
@@ -147,15 +146,12 @@ extern "C" uha_status uha_query_noalloc(const uha_index* index,
         }
 
         // The scratch keeps the previous call's contents: clear the counters
-        // and the merge state that must start at zero, and mark every
-        // replayed distance as absent (all-ones bytes are a NaN).
+        // and the merge state that must start at zero.
         uha::check_cuda(cudaMemsetAsync(counters, 0, 4 * sizeof(uint32_t), s),
                         "cannot clear query counters");
         uha::check_cuda(cudaMemsetAsync(finalize, 0,
                                         uha::finalize_scratch_bytes(n, index->rows), s),
                         "cannot clear merge state");
-        uha::check_cuda(cudaMemsetAsync(replayed, 0xff, n * sizeof(double), s),
-                        "cannot clear replayed distances");
 
         int* error_flag = reinterpret_cast<int*>(counters + 1);
         if (index->kind == uha::IndexKind::sampled) {
@@ -179,8 +175,22 @@ extern "C" uha_status uha_query_noalloc(const uha_index* index,
                                     static_cast<uint32_t>(index->rows)};
         const uha::Bound bound = uha::make_bound(
             plan.depth, index->scan_dim, op == uha::ScanOp::l1 ? 1 : 2);
-        uha::launch_finalize_certified(view, bound, results, ambiguous, counters,
-                                       finalize, n, s);
+        uha::ReplayInputs in{};
+        in.rows = index->scan_rows.get();
+        in.queries = prepared;
+        in.dim = index->scan_dim;
+        in.padded_dim = index->padded_dim;
+        in.weights64 = index->weights64.get();
+        in.op = index->metric == UHA_L2 ? uha::ReplayOp::l2_sequential
+                : index->weights64.size() != 0
+                    ? uha::ReplayOp::l1_weighted_sequential
+                    : uha::ReplayOp::l1_grouped4;
+        uha::launch_argmin(view, bound, in, results, replayed, finalize, n, counters,
+                           s);
+        write_outputs_kernel<<<1, 32, 0, s>>>(results, replayed,
+                                              static_cast<uint32_t>(n), out_indices,
+                                              out_distances);
+        uha::check_cuda(cudaGetLastError(), "cannot launch output kernel");
         uint32_t host_counters[2] = {0, 0};
         uha::check_cuda(cudaMemcpyAsync(host_counters, counters, sizeof(host_counters),
                                         cudaMemcpyDeviceToHost, s),
@@ -192,24 +202,5 @@ extern "C" uha_status uha_query_noalloc(const uha_index* index,
                      ? "sampled query coordinate must be finite"
                      : "queries must be finite");
         }
-        if (host_counters[0] != 0) {
-            uha::ReplayInputs in{};
-            in.rows = index->scan_rows.get();
-            in.queries = prepared;
-            in.dim = index->scan_dim;
-            in.padded_dim = index->padded_dim;
-            in.weights64 = index->weights64.get();
-            in.op = index->metric == UHA_L2 ? uha::ReplayOp::l2_sequential
-                    : index->weights64.size() != 0
-                        ? uha::ReplayOp::l1_weighted_sequential
-                        : uha::ReplayOp::l1_grouped4;
-            uha::launch_resolve(view, bound, in, ambiguous, host_counters[0],
-                                finalize, n, results, replayed, s);
-        }
-        write_outputs_kernel<<<1, 32, 0, s>>>(results, replayed,
-                                              static_cast<uint32_t>(n), out_indices,
-                                              out_distances);
-        uha::check_cuda(cudaGetLastError(), "cannot launch output kernel");
-        uha::check_cuda(cudaStreamSynchronize(s), "query failed");
     });
 }
