@@ -49,6 +49,10 @@ def parse_args():
     p.add_argument("--no-suite", action="store_true",
                    help="skip the secondary configurations")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--precision-only", action="store_true",
+                   help="only the precision-strategy table (one JSON line)")
+    p.add_argument("--precision-batch", type=int, default=0,
+                   help="with --precision-only: one batch size (2048 queries)")
     return p.parse_args()
 
 
@@ -257,6 +261,7 @@ def run_engine(args):
         del qdev
         torch.cuda.empty_cache()
         line["suite"] = suite(ds, index)
+        line["precision"] = precision(ds, index)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -347,6 +352,70 @@ def suite(ds, exact_index):
     return out
 
 
+def precision(ds, exact_index, batches=((1, 256), (64, 2048), (1024, 2048))):
+    """Precision strategies on the same data: BF16 and FP8-E4M3 tensor-core
+    scores, top-k (k = 8, 32), certified binary32 re-score. For each batch:
+    queries/s against the plain certified path at the same batch, agreement of
+    the answers with the binary64 exact argmin (the plain path's answers, which
+    are the reference CPU's), the relative distance excess over the exact
+    minimum, and the score kernel's tensor throughput."""
+    import torch
+
+    import ultrahigh_ann_b200 as uha
+
+    peaks = measured_peaks()
+    nq = max(n for _, n in batches)
+    qdev = torch.from_numpy(ds.queries[:nq]).cuda()
+    rows, dim = ds.rows.shape
+
+    def timed(B, n, strategy, k=None):
+        ws = exact_index.make_query_workspace(B)
+        if k is not None:
+            ws.set_candidates(k)
+        ws.set_timing(True)
+        res = np.zeros(n, np.uint64)
+        dist = np.zeros(n, np.float64)
+        w = min(B, n)
+        # warm-up (first use builds the low-precision rows)
+        exact_index.query_many(qdev.data_ptr(), w, B, res[:w], ws, strategy, dist[:w],
+                               on_device=True)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        exact_index.query_many(qdev.data_ptr(), n, B, res, ws, strategy, dist,
+                               on_device=True)
+        secs = time.perf_counter() - t
+        return res, dist, n / secs, ws.last_stats()
+
+    out = []
+    for B, n in batches:
+        ref, ref_dist, plain_qps, _ = timed(B, n, uha.QueryStrategy.direct)
+        out.append({"strategy": "direct", "batch": B, "queries": n,
+                    "queries_per_s": round(plain_qps, 1)})
+        for strategy, name, elem in ((uha.QueryStrategy.gemm_bf16_rerank, "bf16_rerank", 2),
+                                     (uha.QueryStrategy.gemm_fp8_rerank, "fp8_rerank", 1)):
+            for k in (8, 32):
+                res, dist, qps, st = timed(B, n, strategy, k)
+                excess = (dist - ref_dist) / np.maximum(ref_dist, 1e-300)
+                launches = (n + B - 1) // B
+                ms = st["scan_ms"] / launches
+                pitch = -(-dim // (64 if elem == 2 else 128)) * (64 if elem == 2 else 128)
+                tflops = 2.0 * rows * dim * min(B, n) / (ms * 1e-3) / 1e12
+                out.append({
+                    "strategy": name, "k": k, "batch": B, "queries": n,
+                    "queries_per_s": round(qps, 1),
+                    "speedup_vs_direct": round(qps / plain_qps, 2),
+                    "agreement_vs_fp64_exact": round(float(np.mean(res == ref)), 4),
+                    "distance_excess": {"mean": float(np.mean(excess)),
+                                        "max": float(np.max(excess))},
+                    "replayed": st["replayed_queries"],
+                    "score_kernel": {
+                        "ms_per_launch": round(ms, 4),
+                        "tflops": round(tflops, 1),
+                        "frac_of_measured_bf16": round(tflops / peaks["bf16_tflops"], 3),
+                        "row_bytes_gbs": round(rows * pitch * elem / (ms * 1e-3) / 1e9, 1)}})
+    return out
+
+
 # ------------------------------------------------------------ reference arm
 def run_reference(args):
     world, rank, _ = dist_env()
@@ -400,8 +469,24 @@ def main():
     args = parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.precision_only:
+        run_precision_only(args)
     else:
         run_engine(args)
+
+
+def run_precision_only(args):
+    """The precision table alone on one GPU (development runs)."""
+    import ultrahigh_ann_b200 as uha
+    from ultrahigh_ann_b200 import synthetic
+
+    ds = synthetic.row_dataset(rows=ROWS, classes=33, queries=2048, d=DIM, seed=1,
+                               query_stream=0)
+    index = uha.CudaExactL2Index(ds.rows)
+    batches = ((args.precision_batch, 2048),) if args.precision_batch else None
+    table = precision(ds, index, batches) if batches else precision(ds, index)
+    print(json.dumps({"workload": "exact_l2_r7028_d60660", "precision": table}),
+          flush=True)
 
 
 if __name__ == "__main__":

@@ -49,16 +49,28 @@ typedef enum uha_metric {
 /* Query strategies. The first two keep the reference enumerator values of
  * CudaDenseL2QueryStrategy / CudaSampledCoordinateL2QueryStrategy /
  * CudaHierarchicalL{1,2}QueryStrategy (include/ultrahigh_ann/core/
- * cuda_dense_l2_scan_index.hpp:17-23).
+ * cuda_dense_l2_scan_index.hpp:17-23); the precision forms are appended.
  *   UHA_DIRECT: binary32 scan on CUDA cores with a certified error bound per
  *     distance; queries whose winner is not certified are re-scored by
  *     replaying the reference CPU's binary64 operation sequence, so the
  *     returned index equals the reference CPU index on every query.
  *   UHA_GEMM: the reference's unrefined binary32 norm identity
- *     ||r||^2 + ||q||^2 - 2 r.q (L2 only; L1 treats it as DIRECT). */
+ *     ||r||^2 + ||q||^2 - 2 r.q (L2 only; L1 treats it as DIRECT).
+ *   UHA_GEMM_BF16_RERANK, UHA_GEMM_FP8_RERANK (exact and flat L2 indexes):
+ *     rows and queries rounded to BF16, or to FP8-E4M3 with one scale per
+ *     row and per query; the score matrix runs on the tensor cores with FP32
+ *     accumulation; the k rows with the smallest estimate ||r~||^2 - 2 r~.q~
+ *     (uha_workspace_set_candidates) are re-scored from the original rows
+ *     (the reference CPU's binary64 terms, added in parallel, with a
+ *     certified bound; near-ties replay the CPU's order). The answer equals
+ *     the reference CPU index whenever that row is among the k candidates.
+ *     The low-precision copy of the rows is built on the first query that
+ *     needs it. */
 typedef enum uha_strategy {
     UHA_DIRECT = 0,
-    UHA_GEMM = 1
+    UHA_GEMM = 1,
+    UHA_GEMM_BF16_RERANK = 2,
+    UHA_GEMM_FP8_RERANK = 3
 } uha_strategy;
 
 typedef struct uha_index uha_index;
@@ -269,6 +281,21 @@ void* uha_workspace_stream(const uha_workspace* workspace);
  * the workspace stream around the scan kernel and around the whole device
  * pipeline, reported in uha_query_stats.scan_ms / device_ms. */
 uha_status uha_workspace_set_timing(uha_workspace* workspace, int enabled);
+
+/* Candidates per query of the precision strategies (1 to 64; default 32).
+ * No reference counterpart. */
+uha_status uha_workspace_set_candidates(uha_workspace* workspace,
+                                        uint32_t candidates);
+
+/* Diagnostic of the precision strategies (no reference counterpart): for
+ * query_count host queries (at most the workspace capacity), out_scores
+ * (host, query_count x row_count, query-major) receives the tensor-core
+ * scores r~.q~ of every row (FP8: times both scales), and out_norms (host,
+ * row_count, nullable) the squared norms ||r~||^2 of the rounded rows. */
+uha_status uha_precision_scores(const uha_index* index, uha_workspace* workspace,
+                                const float* queries, uint64_t query_count,
+                                uha_strategy strategy, float* out_scores,
+                                float* out_norms);
 
 /* ---------------------------------------------------------- index build */
 

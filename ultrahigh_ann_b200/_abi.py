@@ -6,7 +6,7 @@ is no fallback: when the library is missing or fails to load, every call raises.
 from __future__ import annotations
 
 import ctypes
-from ctypes import (POINTER, c_char, c_char_p, c_double, c_int, c_uint64,
+from ctypes import (POINTER, c_char, c_char_p, c_double, c_int, c_uint32, c_uint64,
                     c_void_p)
 from pathlib import Path
 
@@ -33,6 +33,8 @@ PAIRS_GRAM = 1
 # uha_strategy
 DIRECT = 0
 GEMM = 1
+GEMM_BF16_RERANK = 2
+GEMM_FP8_RERANK = 3
 
 
 class SpaceUsage(ctypes.Structure):
@@ -105,6 +107,9 @@ SIGNATURES = {
     "uha_workspace_last_stats": (c_int, [c_void_p, POINTER(QueryStats)]),
     "uha_workspace_set_timing": (c_int, [c_void_p, c_int]),
     "uha_workspace_stream": (c_void_p, [c_void_p]),
+    "uha_workspace_set_candidates": (c_int, [c_void_p, c_uint32]),
+    "uha_precision_scores": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_int,
+                                      c_void_p, c_void_p]),
     "uha_importance_probabilities": (c_int, [c_int, c_int, c_void_p, c_uint64, c_uint64,
                                               c_int, c_uint64, c_void_p,
                                               POINTER(ProbabilityReport)]),

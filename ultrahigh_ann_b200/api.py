@@ -78,6 +78,11 @@ class QueryStrategy(enum.IntEnum):
 
     direct = _abi.DIRECT
     gemm = _abi.GEMM
+    # precision forms (appended; exact and flat L2 indexes): tensor-core
+    # scores of rounded rows/queries, then a certified binary32 re-score of
+    # the best candidates per query (QueryWorkspace.set_candidates)
+    gemm_bf16_rerank = _abi.GEMM_BF16_RERANK
+    gemm_fp8_rerank = _abi.GEMM_FP8_RERANK
 
 
 CudaDenseL2QueryStrategy = QueryStrategy
@@ -364,14 +369,22 @@ class QueryWorkspace:
         of every query on this workspace (see last_stats())."""
         _check(_abi.load().uha_workspace_set_timing(self._handle, int(enabled)))
 
+    def set_candidates(self, candidates: int) -> None:
+        """Candidates per query re-scored by the precision strategies (1-64)."""
+        if not 1 <= int(candidates) <= 64:
+            raise InvalidArgument("candidate count must be between 1 and 64")
+        _check(_abi.load().uha_workspace_set_candidates(self._handle,
+                                                        ctypes.c_uint32(int(candidates))))
+
 
 class _CudaIndex:
     _handle: ctypes.c_void_p = None
     _dimension: int = 0
 
-    def _adopt(self, handle: ctypes.c_void_p, dimension: int) -> None:
+    def _adopt(self, handle: ctypes.c_void_p, dimension: int, rows: int) -> None:
         self._handle = handle
         self._dimension = dimension
+        self._rows = rows
 
     def __del__(self):
         if getattr(self, "_handle", None):
@@ -381,6 +394,10 @@ class _CudaIndex:
     @property
     def dimension(self) -> int:
         return self._dimension
+
+    @property
+    def row_count(self) -> int:
+        return self._rows
 
     def make_query_workspace(self, maximum_batch_size: int) -> QueryWorkspace:
         return QueryWorkspace(self, maximum_batch_size)
@@ -450,6 +467,25 @@ class _CudaIndex:
                                           dist_ptr))
         return out
 
+    def precision_scores(self, queries, query_count: int, workspace: QueryWorkspace,
+                         strategy=QueryStrategy.gemm_bf16_rerank):
+        """Tensor-core scores of a precision strategy: (scores, norms) with
+        scores[q][row] = r~.q~ (FP8: times both scales) and norms[row] =
+        ||r~||^2 of the rounded rows."""
+        if not isinstance(workspace, QueryWorkspace):
+            raise InvalidArgument("CUDA workspace belongs to a different index")
+        q = np.ascontiguousarray(queries, dtype=np.float32).reshape(-1)
+        if q.size != query_count * self._dimension:
+            raise InvalidArgument("query batch dimensions do not match index dimension")
+        rows = self.row_count
+        scores = np.zeros((query_count, rows), dtype=np.float32)
+        norms = np.zeros(rows, dtype=np.float32)
+        _check(_abi.load().uha_precision_scores(
+            self._handle, workspace._handle, ctypes.c_void_p(q.ctypes.data if q.size else 0),
+            ctypes.c_uint64(query_count), int(strategy),
+            ctypes.c_void_p(scores.ctypes.data), ctypes.c_void_p(norms.ctypes.data)))
+        return scores, norms
+
     def query(self, query, workspace: QueryWorkspace,
               strategy=QueryStrategy.direct) -> int:
         q = np.ascontiguousarray(query, dtype=np.float32).reshape(-1)
@@ -492,7 +528,7 @@ class CudaDenseL2ScanIndex(_CudaIndex):
         _check(_abi.load().uha_exact_index_create(device, _abi.L2, _ptr(rows),
                                                   rows.shape[0], rows.shape[1],
                                                   ctypes.byref(handle)))
-        self._adopt(handle, rows.shape[1])
+        self._adopt(handle, rows.shape[1], rows.shape[0])
 
 
 class CudaExactL2Index(CudaDenseL2ScanIndex):
@@ -518,7 +554,7 @@ class CudaDenseL1ScanIndex(_CudaIndex):
             _check(lib.uha_weighted_l1_index_create(device, _ptr(rows), rows.shape[0],
                                                     rows.shape[1], _ptr(w),
                                                     ctypes.byref(handle)))
-        self._adopt(handle, rows.shape[1])
+        self._adopt(handle, rows.shape[1], rows.shape[0])
 
     def query_batch(self, queries, query_count, output, workspace,
                     strategy=QueryStrategy.direct, distances=None):
@@ -558,7 +594,7 @@ class _CudaSampledIndex(_CudaIndex):
             device, self._metric, _ptr(rows), rows.shape[0], rows.shape[1],
             _ptr(sample.source_columns), _ptr(sample.multiplicities),
             _ptr(sample.inverse_probabilities), len(sample), ctypes.byref(handle)))
-        self._adopt(handle, rows.shape[1])
+        self._adopt(handle, rows.shape[1], rows.shape[0])
         self.coordinate_sample = sample
 
 
@@ -694,7 +730,7 @@ class _CudaHierarchicalIndex(_CudaIndex):
             _ptr(sample.source_columns), _ptr(sample.multiplicities),
             _ptr(sample.inverse_probabilities), len(sample), _ptr(matrix), p,
             ctypes.byref(handle)))
-        self._adopt(handle, rows.shape[1])
+        self._adopt(handle, rows.shape[1], rows.shape[0])
         self.coordinate_sample = sample
         self.projection = matrix
 

@@ -507,6 +507,201 @@ __global__ void __launch_bounds__(kFinalizeThreads)
     }
 }
 
+constexpr uint32_t kMaxCandidates = 64;
+constexpr int kRescoreUnroll = 4;
+
+// Reference binary64 squared distance of one row, summed in parallel by the
+// whole block: the terms are the reference CPU's own
+// (t_j = (double(q_j) - double(r_j))^2, l2_distance.cpp:9-25), only the order
+// of the additions differs. Thread t folds the float4 groups t, t + 256, ...
+// into four accumulators (one per component); then (a0 + a1) + (a2 + a3), a
+// warp butterfly (every lane ends with the same value) and a fixed tree over
+// the eight warps. Longest chain of additions: rescore_depth().
+__device__ double block_l2_64(const float* q, const float* r, uint64_t padded_dim,
+                              double* scratch)
+{
+    const uint64_t groups = padded_dim / 4;
+    const float4* q4 = reinterpret_cast<const float4*>(q);
+    const float4* r4 = reinterpret_cast<const float4*>(r);
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    uint64_t g = threadIdx.x;
+    for (; g + (kRescoreUnroll - 1) * kFinalizeThreads < groups;
+         g += kRescoreUnroll * kFinalizeThreads) {
+        float4 x[kRescoreUnroll];
+        float4 y[kRescoreUnroll];
+#pragma unroll
+        for (int u = 0; u < kRescoreUnroll; ++u) {
+            x[u] = q4[g + u * kFinalizeThreads];
+            y[u] = __ldg(r4 + g + u * kFinalizeThreads);
+        }
+#pragma unroll
+        for (int u = 0; u < kRescoreUnroll; ++u) {
+            const double d0 = __dsub_rn(x[u].x, y[u].x);
+            const double d1 = __dsub_rn(x[u].y, y[u].y);
+            const double d2 = __dsub_rn(x[u].z, y[u].z);
+            const double d3 = __dsub_rn(x[u].w, y[u].w);
+            a0 = __dadd_rn(a0, __dmul_rn(d0, d0));
+            a1 = __dadd_rn(a1, __dmul_rn(d1, d1));
+            a2 = __dadd_rn(a2, __dmul_rn(d2, d2));
+            a3 = __dadd_rn(a3, __dmul_rn(d3, d3));
+        }
+    }
+    for (; g < groups; g += kFinalizeThreads) {
+        const float4 x = q4[g];
+        const float4 y = __ldg(r4 + g);
+        const double d0 = __dsub_rn(x.x, y.x);
+        const double d1 = __dsub_rn(x.y, y.y);
+        const double d2 = __dsub_rn(x.z, y.z);
+        const double d3 = __dsub_rn(x.w, y.w);
+        a0 = __dadd_rn(a0, __dmul_rn(d0, d0));
+        a1 = __dadd_rn(a1, __dmul_rn(d1, d1));
+        a2 = __dadd_rn(a2, __dmul_rn(d2, d2));
+        a3 = __dadd_rn(a3, __dmul_rn(d3, d3));
+    }
+    double t = __dadd_rn(__dadd_rn(a0, a1), __dadd_rn(a2, a3));
+    for (int o = 16; o > 0; o /= 2) {
+        t = __dadd_rn(t, __shfl_xor_sync(0xffffffffu, t, o));
+    }
+    if (threadIdx.x % 32 == 0) {
+        scratch[threadIdx.x / 32] = t;
+    }
+    __syncthreads();
+    static_assert(kFinalizeThreads / 32 == 8, "tree over eight warps");
+    return __dadd_rn(__dadd_rn(__dadd_rn(scratch[0], scratch[1]),
+                               __dadd_rn(scratch[2], scratch[3])),
+                     __dadd_rn(__dadd_rn(scratch[4], scratch[5]),
+                               __dadd_rn(scratch[6], scratch[7])));
+}
+
+struct Interval64 {
+    double lower;
+    double upper;
+};
+
+// [S (1 - rel) - abs, S (1 + rel) + abs], directed roundings; an overflowed
+// sum keeps every candidate below it.
+__device__ __forceinline__ Interval64 interval64(double s, const Bound64& b)
+{
+    if (!(s <= DBL_MAX)) {
+        return {0.0, __longlong_as_double(0x7ff0000000000000ll)};
+    }
+    const double lo = __dsub_rd(__dmul_rd(s, __dsub_rd(1.0, b.rel)), b.abs);
+    const double hi = __dadd_ru(__dmul_ru(s, __dadd_ru(1.0, b.rel)), b.abs);
+    return {lo > 0.0 ? lo : 0.0, hi};
+}
+
+// Certified argmin of each query over its candidate rows (the precision
+// form). grid = (k, batch): CTA (c, q) computes the binary64 distance of
+// candidate c; the last CTA of the query to finish decides. One candidate
+// whose interval can hold the reference minimum is the answer; otherwise the
+// candidates that can are replayed in the reference CPU's order (one warp
+// each) and the lexicographic minimum of (distance, row) wins. exact[q] is
+// the binary64 distance of the answer (the replayed one when replayed).
+__global__ void __launch_bounds__(kFinalizeThreads)
+    rescore_kernel(Bound64 bound, ReplayInputs in, const uint32_t* candidates,
+                   uint32_t k, uint32_t row_count, double* cand_dist,
+                   uint32_t* done, Result* results, double* exact_distances,
+                   uint32_t* replay_count)
+{
+    const uint32_t c = blockIdx.x;
+    const uint32_t q = blockIdx.y;
+    const double inf = __longlong_as_double(0x7ff0000000000000ll);
+    __shared__ double scratch[kFinalizeThreads / 32];
+    __shared__ bool is_last;
+    const float* qrow = in.queries + static_cast<uint64_t>(q) * in.padded_dim;
+    const uint32_t row = candidates[static_cast<uint64_t>(q) * k + c];
+    double d = inf;
+    if (row < row_count) {
+        d = block_l2_64(qrow, in.rows + static_cast<uint64_t>(row) * in.padded_dim,
+                        in.padded_dim, scratch);
+    }
+    if (threadIdx.x == 0) {
+        cand_dist[static_cast<uint64_t>(q) * k + c] = d;
+        __threadfence();
+        is_last = atomicAdd(done + q, 1u) == k - 1;
+    }
+    __syncthreads();
+    if (!is_last) {
+        return;
+    }
+    __threadfence();
+    __shared__ double dist[kMaxCandidates];
+    __shared__ uint32_t cand[kMaxCandidates];
+    for (uint32_t i = threadIdx.x; i < k; i += kFinalizeThreads) {
+        dist[i] = static_cast<volatile double*>(cand_dist)[static_cast<uint64_t>(q) * k + i];
+        cand[i] = candidates[static_cast<uint64_t>(q) * k + i];
+    }
+    __syncthreads();
+    __shared__ bool certified;
+    __shared__ double min_upper;
+    if (threadIdx.x == 0) {
+        done[q] = 0;
+        double first = inf, second = inf, upper = inf;
+        uint32_t first_i = 0xffffffffu;
+        for (uint32_t i = 0; i < k; ++i) {
+            if (cand[i] >= row_count) {
+                continue;
+            }
+            const Interval64 b = interval64(dist[i], bound);
+            upper = fmin(upper, b.upper);
+            if (first_i == 0xffffffffu || b.lower < first ||
+                (b.lower == first && cand[i] < cand[first_i])) {
+                second = first;
+                first = b.lower;
+                first_i = i;
+            } else if (b.lower < second) {
+                second = b.lower;
+            }
+        }
+        certified = first_i != 0xffffffffu && second > upper;
+        min_upper = upper;
+        if (certified) {
+            results[q] = Result{cand[first_i], static_cast<float>(dist[first_i])};
+            exact_distances[q] = dist[first_i];
+        } else {
+            atomicAdd(replay_count, 1u);
+        }
+    }
+    __syncthreads();
+    if (certified) {
+        return;
+    }
+    constexpr int warps = kFinalizeThreads / 32;
+    const int warp = threadIdx.x / 32;
+    const int lane = threadIdx.x % 32;
+    double best = inf;
+    uint32_t best_row = 0xffffffffu;
+    for (uint32_t i = warp; i < k; i += warps) {
+        const uint32_t r = cand[i];
+        if (r >= row_count || interval64(dist[i], bound).lower > min_upper) {
+            continue;
+        }
+        const double v = replay_row(in, qrow, in.rows + static_cast<uint64_t>(r) * in.padded_dim,
+                                    lane);
+        if (lex_less(v, r, best, best_row)) {
+            best = v;
+            best_row = r;
+        }
+    }
+    __shared__ double warp_best[warps];
+    __shared__ uint32_t warp_best_row[warps];
+    if (lane == 0) {
+        warp_best[warp] = best;
+        warp_best_row[warp] = best_row;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 0; w < warps; ++w) {
+            if (lex_less(warp_best[w], warp_best_row[w], best, best_row)) {
+                best = warp_best[w];
+                best_row = warp_best_row[w];
+            }
+        }
+        results[q] = Result{best_row, static_cast<float>(best)};
+        exact_distances[q] = best;
+    }
+}
+
 void set_dynamic_smem(const void* kernel, size_t smem)
 {
     if (smem > 48 * 1024) {
@@ -574,6 +769,31 @@ void launch_argmin(PartialView view, Bound bound, ReplayInputs in,
         view, bound, in, results, exact_distances, fs.summaries, fs.done,
         replay_count);
     check_cuda(cudaGetLastError(), "cannot launch argmin kernel");
+}
+
+uint32_t rescore_depth(uint64_t padded_dim)
+{
+    const uint64_t groups = padded_dim / 4;
+    return static_cast<uint32_t>((groups + kFinalizeThreads - 1) / kFinalizeThreads) + 10;
+}
+
+uint32_t max_rerank_candidates()
+{
+    return kMaxCandidates;
+}
+
+void launch_rescore(Bound64 bound, ReplayInputs in, const uint32_t* candidates,
+                    uint32_t k, uint32_t batch, uint32_t rows, double* cand_dist,
+                    uint32_t* done, Result* results, double* exact_distances,
+                    uint32_t* replay_count, cudaStream_t stream)
+{
+    if (batch == 0 || k == 0) {
+        return;
+    }
+    rescore_kernel<<<dim3(k, batch), kFinalizeThreads, 0, stream>>>(
+        bound, in, candidates, k, rows, cand_dist, done, results, exact_distances,
+        replay_count);
+    check_cuda(cudaGetLastError(), "cannot launch re-score kernel");
 }
 
 void launch_finalize_gemm(PartialView view, const float* row_norms,

@@ -167,6 +167,21 @@ Bound make_bound(uint32_t depth, uint64_t terms, int term_roundings)
     };
 }
 
+// Bound of a parallel binary64 sum (longest addition chain `depth`) of the
+// same `terms` rounded terms that the CPU adds sequentially:
+// |S_gpu - S_cpu| <= (g(depth) + g(terms)) / (1 - g(depth)) * S_gpu, plus an
+// absolute term for subnormal roundings.
+Bound64 make_bound64(uint32_t depth, uint64_t terms)
+{
+    const double u = std::ldexp(1.0, -53);
+    const double nd = static_cast<double>(depth) + 1;
+    const double nt = static_cast<double>(terms) + 1;
+    const double gd = nd * u / (1.0 - nd * u);
+    const double gt = nt * u / (1.0 - nt * u);
+    return Bound64{1.01 * (gd + gt) / (1.0 - gd) + 4 * u,
+                   std::ldexp(nd + nt + 4, -1074) * 4};
+}
+
 }  // namespace uha
 
 using uha::make_bound;
@@ -751,6 +766,106 @@ extern "C" uha_status uha_workspace_last_stats(const uha_workspace* workspace,
 
 namespace {
 
+bool precision_strategy(uha_strategy s)
+{
+    return s == UHA_GEMM_BF16_RERANK || s == UHA_GEMM_FP8_RERANK;
+}
+
+uha::LowpType lowp_type(uha_strategy s)
+{
+    return s == UHA_GEMM_FP8_RERANK ? uha::LowpType::fp8_e4m3 : uha::LowpType::bf16;
+}
+
+// The index's low-precision rows of `type`, rounded from the scanned binary32
+// rows on first use (on `stream`, synchronised before it is published).
+const uha::LowpRows& lowp_rows(const uha_index* index, uha::LowpType type,
+                               cudaStream_t stream)
+{
+    std::lock_guard<std::mutex> lock(index->lowp_mutex);
+    uha::LowpRows& lp = index->lowp[static_cast<int>(type)];
+    if (lp.ready) {
+        return lp;
+    }
+    lp.pitch = uha::lowp_pitch(type, index->scan_dim);
+    const uint64_t vectors = uha::lowp_padded_count(index->rows);
+    lp.data.allocate(checked_mul(checked_mul(vectors, lp.pitch, "low-precision rows"),
+                                 uha::lowp_element_bytes(type), "low-precision rows"));
+    lp.scales.allocate(vectors);
+    lp.norms.allocate(index->rows);
+    check_cuda(cudaMemsetAsync(lp.data.get(), 0, lp.data.bytes(), stream),
+               "cannot clear low-precision rows");
+    uha::launch_lowp_convert(type, index->scan_rows.get(), index->rows, index->padded_dim,
+                             index->scan_dim, lp.data.get(), lp.pitch, lp.scales.get(),
+                             lp.norms.get(), stream);
+    check_cuda(cudaStreamSynchronize(stream), "cannot build low-precision rows");
+    lp.ready = true;
+    return lp;
+}
+
+// Workspace buffers of the precision strategies for batches up to max_batch.
+void ensure_lowp_workspace(uha_workspace* ws, const uha_index* index,
+                           cudaStream_t stream)
+{
+    const uint64_t bytes = checked_mul(
+        checked_mul(uha::lowp_padded_count(ws->max_batch),
+                    uha::lowp_pitch(uha::LowpType::bf16, index->scan_dim), "query buffer"),
+        2, "query buffer");
+    if (ws->queries_lp.size() < bytes) {
+        check_cuda(cudaStreamSynchronize(stream), "CUDA query failed");
+        ws->queries_lp.allocate(bytes);
+        // vectors past a batch are read by the score kernel (and not stored)
+        check_cuda(cudaMemsetAsync(ws->queries_lp.get(), 0, bytes, stream),
+                   "cannot clear the query buffer");
+        ws->query_scales.allocate(uha::lowp_padded_count(ws->max_batch));
+        ws->query_amax.allocate(uha::lowp_padded_count(ws->max_batch));
+    }
+    const uint64_t cand = checked_mul(ws->max_batch, uha::max_rerank_candidates(),
+                                      "candidates");
+    if (ws->candidates.size() < cand) {
+        check_cuda(cudaStreamSynchronize(stream), "CUDA query failed");
+        ws->candidates.allocate(cand);
+        ws->cand_dist.allocate(cand);
+        ws->rescore_done.allocate(ws->max_batch);
+        check_cuda(cudaMemsetAsync(ws->rescore_done.get(), 0, ws->rescore_done.bytes(),
+                                   stream),
+                   "cannot clear re-score counters");
+    }
+}
+
+// Rounds the prepared queries and runs the tensor-core scores; returns the
+// plan (the partial-score slabs are in ws->partials).
+uha::LowpPlan enqueue_lowp_scores(const uha_index* index, uha_workspace* ws,
+                                  uha_strategy strategy, uint64_t n, bool time_scan,
+                                  cudaEvent_t scan_start, cudaEvent_t scan_stop)
+{
+    cudaStream_t stream = ws->stream;
+    const uha::LowpType type = lowp_type(strategy);
+    const uha::LowpRows& lp = lowp_rows(index, type, stream);
+    ensure_lowp_workspace(ws, index, stream);
+    uha::launch_lowp_queries(type, ws->prepared.get(), n, index->padded_dim,
+                             ws->queries_lp.get(), lp.pitch, ws->query_scales.get(),
+                             ws->query_amax.get(), stream);
+    const uha::LowpPlan plan =
+        uha::plan_lowp(type, index->rows, lp.pitch, n, index->sm_count);
+    const uint64_t partial_count =
+        checked_mul(checked_mul(plan.splits, n, "partials"), index->rows, "partials");
+    if (ws->partials.size() < partial_count) {
+        check_cuda(cudaStreamSynchronize(stream), "CUDA query failed");
+        ws->partials.allocate(partial_count);
+    }
+    if (time_scan) {
+        check_cuda(cudaEventRecord(scan_start, stream), "event");
+    }
+    uha::launch_lowp_scores(plan, type, lp.data.get(), lp.scales.get(), index->rows,
+                            ws->queries_lp.get(), ws->query_scales.get(), n, lp.pitch,
+                            ws->partials.get(),
+                            reinterpret_cast<int*>(ws->counters.get() + 1), stream);
+    if (time_scan) {
+        check_cuda(cudaEventRecord(scan_stop, stream), "event");
+    }
+    return plan;
+}
+
 // One query batch's kernels on the workspace stream: gather / copy with
 // validation, (projection), scan, certified argmin with in-kernel replay (or
 // the norm identity), (the replayed distance of each selected row of a
@@ -799,6 +914,29 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
         uha::launch_prepare_dense(source, n, index->dimension, ws->prepared.get(),
                                   index->padded_dim, error_flag, stream);
         ++launches;
+    }
+
+    if (precision_strategy(c.strategy)) {
+        const uha::LowpPlan plan = enqueue_lowp_scores(index, ws, c.strategy, n, time_scan,
+                                                       scan_start, scan_stop);
+        const uint32_t k = static_cast<uint32_t>(
+            std::min<uint64_t>(ws->candidates_per_query, index->rows));
+        uha::launch_lowp_topk(ws->partials.get(), plan.splits, static_cast<uint32_t>(n),
+                              static_cast<uint32_t>(index->rows),
+                              index->lowp[static_cast<int>(lowp_type(c.strategy))].norms.get(),
+                              k, ws->candidates.get(), stream);
+        const uha::Bound64 bound =
+            uha::make_bound64(uha::rescore_depth(index->padded_dim), index->scan_dim);
+        uha::ReplayInputs in{};
+        in.op = uha::ReplayOp::l2_sequential;
+        in.rows = index->scan_rows.get();
+        in.queries = ws->prepared.get();
+        in.dim = index->scan_dim;
+        in.padded_dim = index->padded_dim;
+        uha::launch_rescore(bound, in, ws->candidates.get(), k, static_cast<uint32_t>(n),
+                            static_cast<uint32_t>(index->rows), ws->cand_dist.get(),
+                            ws->rescore_done.get(), results, exact, replay_count, stream);
+        return launches + 4;
     }
 
     const bool gemm = c.strategy == UHA_GEMM && index->metric == UHA_L2;
@@ -917,6 +1055,9 @@ void finish_call(const uha_index* index, uha_workspace* ws, uint64_t n,
                  uint64_t* out_indices, double* out_distances)
 {
     const uint32_t flag = ws->host_counters.get()[1];
+    if (flag & 8u) {
+        fail(UHA_RUNTIME_ERROR, "tensor-core pipeline wait timed out");
+    }
     if (flag != 0) {
         if ((flag & 1u) && index->kind == IndexKind::hierarchical) {
             fail(UHA_INVALID_ARGUMENT, "sampled query coordinate must be finite");
@@ -952,8 +1093,13 @@ void validate_query_call(const uha_index* index, uha_workspace* ws,
             "CUDA workspace belongs to a different index");
     require(batch <= ws->max_batch, UHA_INVALID_ARGUMENT,
             "query count exceeds CUDA workspace capacity");
-    require(strategy == UHA_DIRECT || strategy == UHA_GEMM, UHA_INVALID_ARGUMENT,
-            "unknown CUDA query strategy");
+    require(strategy == UHA_DIRECT || strategy == UHA_GEMM || precision_strategy(strategy),
+            UHA_INVALID_ARGUMENT, "unknown CUDA query strategy");
+    require(!precision_strategy(strategy) ||
+                (index->metric == UHA_L2 && (index->kind == IndexKind::exact ||
+                                             index->kind == IndexKind::sampled)),
+            UHA_INVALID_ARGUMENT,
+            "precision strategies serve exact and flat L2 indexes");
     if (count != 0) {
         require(out_indices != nullptr, UHA_INVALID_ARGUMENT, "output must not be null");
         require(queries != nullptr || index->dimension == 0, UHA_INVALID_ARGUMENT,
@@ -1074,6 +1220,88 @@ extern "C" uha_status uha_query_many(const uha_index* index, uha_workspace* ws,
         ws->last.kernel_launches = launches;
         finish_call(index, ws, n, ws->host_results.get(), ws->host_exact.get(),
                     out_indices, out_distances);
+    });
+}
+
+extern "C" uha_status uha_workspace_set_candidates(uha_workspace* workspace,
+                                                   uint32_t candidates)
+{
+    return guarded([&] {
+        require(workspace != nullptr, UHA_INVALID_ARGUMENT,
+                "workspace must not be null");
+        require(candidates >= 1 && candidates <= uha::max_rerank_candidates(),
+                UHA_INVALID_ARGUMENT, "candidate count must be between 1 and 64");
+        workspace->candidates_per_query = candidates;
+    });
+}
+
+extern "C" uha_status uha_precision_scores(const uha_index* index, uha_workspace* ws,
+                                           const float* queries, uint64_t query_count,
+                                           uha_strategy strategy, float* out_scores,
+                                           float* out_norms)
+{
+    return guarded([&] {
+        require(precision_strategy(strategy), UHA_INVALID_ARGUMENT,
+                "not a precision strategy");
+        validate_query_call(index, ws, queries, query_count, query_count, strategy,
+                            reinterpret_cast<const uint64_t*>(out_scores));
+        if (query_count == 0 || index->padded_dim == 0) {
+            return;
+        }
+        DeviceGuard guard(index->device);
+        uha::clear_stale_cuda_error();
+        cudaStream_t stream = ws->stream;
+        const uint64_t n = query_count;
+        check_cuda(cudaMemsetAsync(ws->counters.get(), 0, ws->counters.bytes(), stream),
+                   "cannot clear query counters");
+        check_cuda(cudaMemcpyAsync(ws->raw_queries.get(), queries,
+                                   n * index->dimension * sizeof(float),
+                                   cudaMemcpyHostToDevice, stream),
+                   "cannot copy queries to the CUDA device");
+        int* error_flag = reinterpret_cast<int*>(ws->counters.get() + 1);
+        if (index->kind == IndexKind::sampled) {
+            uha::launch_prepare_sampled(ws->raw_queries.get(), n, index->dimension,
+                                        index->columns.get(), index->scales.get(),
+                                        index->sample_size, ws->prepared.get(),
+                                        index->padded_dim, error_flag, stream);
+        } else {
+            uha::launch_prepare_dense(ws->raw_queries.get(), n, index->dimension,
+                                      ws->prepared.get(), index->padded_dim, error_flag,
+                                      stream);
+        }
+        const uha::LowpPlan plan =
+            enqueue_lowp_scores(index, ws, strategy, n, false, nullptr, nullptr);
+        const uint64_t per_split = n * index->rows;
+        std::vector<float> slabs(plan.splits * per_split);
+        check_cuda(cudaMemcpyAsync(slabs.data(), ws->partials.get(),
+                                   slabs.size() * sizeof(float), cudaMemcpyDeviceToHost,
+                                   stream),
+                   "cannot copy scores from the CUDA device");
+        if (out_norms != nullptr) {
+            check_cuda(cudaMemcpyAsync(out_norms,
+                                       index->lowp[static_cast<int>(lowp_type(strategy))]
+                                           .norms.get(),
+                                       index->rows * sizeof(float), cudaMemcpyDeviceToHost,
+                                       stream),
+                       "cannot copy norms from the CUDA device");
+        }
+        check_cuda(cudaMemcpyAsync(ws->host_counters.get(), ws->counters.get(),
+                                   ws->counters.bytes(), cudaMemcpyDeviceToHost, stream),
+                   "cannot copy query counters from the CUDA device");
+        check_cuda(cudaStreamSynchronize(stream), "CUDA query failed");
+        const uint32_t flag = ws->host_counters.get()[1];
+        if (flag & 8u) {
+            fail(UHA_RUNTIME_ERROR, "tensor-core pipeline wait timed out");
+        }
+        require(flag == 0, UHA_INVALID_ARGUMENT, "queries must be finite");
+        // split slabs summed in split order, as the candidate selection does
+        for (uint64_t i = 0; i < per_split; ++i) {
+            float acc = 0.f;
+            for (uint32_t sp = 0; sp < plan.splits; ++sp) {
+                acc += slabs[sp * per_split + i];
+            }
+            out_scores[i] = acc;
+        }
     });
 }
 

@@ -6,6 +6,7 @@
 #include "kernels.h"
 
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -16,9 +17,23 @@ enum class IndexKind { exact, weighted, sampled, hierarchical };
 constexpr uint64_t kColumnAlign = 4;  // padded row length: 16-byte multiple
 constexpr uint64_t kMaxExtent = 0x7fffffffull;
 
+// Low-precision copy of an index's scanned rows for the precision
+// strategies: lowp_padded_count(rows) vectors of `pitch` elements (zero past
+// the scanned columns and past the last row), per-row scales (FP8) and the
+// squared norms of the rounded rows.
+struct LowpRows {
+    DeviceBuffer<unsigned char> data;
+    DeviceBuffer<float> scales;
+    DeviceBuffer<float> norms;
+    uint64_t pitch = 0;
+    bool ready = false;
+};
+
 // Relative and absolute certification bound for a binary32 distance (defined
 // in engine.cu).
 Bound make_bound(uint32_t depth, uint64_t terms, int term_roundings);
+// The same for a parallel binary64 sum of the CPU's terms.
+Bound64 make_bound64(uint32_t depth, uint64_t terms);
 
 }  // namespace uha
 
@@ -48,6 +63,9 @@ struct uha_index {
     uha::DeviceBuffer<float> projection32;  // p x padded_sample
     uha::DeviceBuffer<float> row_err;       // rows
     uha_space_usage usage{};
+    // precision strategies: built on first use (index_bf16 / index_fp8)
+    mutable std::mutex lowp_mutex;
+    mutable uha::LowpRows lowp[2];
 };
 
 struct uha_workspace {
@@ -66,6 +84,14 @@ struct uha_workspace {
     uha::DeviceBuffer<double> call_exact;         // replayed distances (NaN: none)
     uha::DeviceBuffer<uint32_t> counters;  // [0] replayed queries, [1] error flag
     uha::DeviceBuffer<unsigned char> finalize_scratch;
+    // precision strategies (allocated on first use)
+    uha::DeviceBuffer<unsigned char> queries_lp;  // lowp_padded_count(max_batch) vectors
+    uha::DeviceBuffer<float> query_scales;        // FP8 scale per query
+    uha::DeviceBuffer<unsigned int> query_amax;   // FP8 max |x| bits per query
+    uha::DeviceBuffer<uint32_t> candidates;       // [batch][candidates_per_query]
+    uha::DeviceBuffer<double> cand_dist;          // [batch][candidates_per_query]
+    uha::DeviceBuffer<uint32_t> rescore_done;     // per query, zero between calls
+    uint32_t candidates_per_query = 32;
     uha::PinnedBuffer<uha::Result> host_results;
     uha::PinnedBuffer<double> host_exact;
     uha::PinnedBuffer<uint32_t> host_counters;

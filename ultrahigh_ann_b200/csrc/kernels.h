@@ -126,6 +126,67 @@ void launch_refine_winners(ReplayInputs in, const Result* results,
                            uint32_t batch, double* exact_distances,
                            cudaStream_t stream);
 
+// ---- precision form: low-precision scores on the tensor cores, top-k,
+// binary32 re-score of the candidates
+enum class LowpType : int { bf16 = 0, fp8_e4m3 = 1 };
+// Elements per stored low-precision vector (a multiple of one 128-byte K
+// slice; zero past the scanned columns).
+uint64_t lowp_pitch(LowpType type, uint64_t dim);
+// Vectors a low-precision buffer holds for `count` rows or queries.
+uint64_t lowp_padded_count(uint64_t count);
+uint64_t lowp_element_bytes(LowpType type);
+// Rounds `count` binary32 vectors (src_pitch apart, `dim` used) into `out`
+// (pitch apart): BF16, or E4M3 with scales[i] = max|x| / 448. norms[i]
+// (nullable) = squared norm of the rounded (dequantized) vector.
+void launch_lowp_convert(LowpType type, const float* src, uint64_t count,
+                         uint64_t src_pitch, uint64_t dim, void* out,
+                         uint64_t pitch, float* scales, float* norms,
+                         cudaStream_t stream);
+// Rounds `count` zero-padded binary32 query vectors (src_pitch apart, a
+// multiple of 4) like launch_lowp_convert, without norms, with many blocks
+// per vector. amax_scratch: `count` words (FP8).
+void launch_lowp_queries(LowpType type, const float* src, uint64_t count,
+                         uint64_t src_pitch, void* out, uint64_t pitch,
+                         float* scales, unsigned int* amax_scratch,
+                         cudaStream_t stream);
+struct LowpPlan {
+    int bn;                      // queries per tile (UMMA N)
+    uint32_t splits;             // K splits (partial-score slabs)
+    uint32_t kblocks;            // 128-byte K slices per vector
+    uint32_t kblocks_per_split;
+};
+LowpPlan plan_lowp(LowpType type, uint64_t rows, uint64_t pitch, uint64_t batch,
+                   int sm_count);
+// partials[split][q][row] = q~ . v~ over the split's K slices (FP8: times the
+// row and query scales). error_flag |= 8 when a pipeline wait ran out.
+void launch_lowp_scores(const LowpPlan& plan, LowpType type, const void* rows_lp,
+                        const float* row_scale, uint64_t row_count,
+                        const void* queries_lp, const float* query_scale,
+                        uint64_t batch, uint64_t pitch, float* partials,
+                        int* error_flag, cudaStream_t stream);
+// candidates[q * k + i]: the k rows with the smallest ||v~||^2 - 2 S
+// (ascending, lowest row on ties; 0xffffffff past the index's rows).
+void launch_lowp_topk(const float* partials, uint32_t splits, uint32_t batch,
+                      uint32_t rows, const float* norms, uint32_t k,
+                      uint32_t* candidates, cudaStream_t stream);
+// Binary64 certification interval [S (1 - rel) - abs, S (1 + rel) + abs] of
+// a parallel binary64 sum S of the reference CPU's own terms.
+struct Bound64 {
+    double rel;
+    double abs;
+};
+// Accumulation depth of the re-score's binary64 distances (for the bound).
+uint32_t rescore_depth(uint64_t padded_dim);
+uint32_t max_rerank_candidates();
+// Certified argmin of each query over its k candidates (ReplayInputs as for
+// the plain L2 scan): cand_dist holds batch x k doubles, done batch counters
+// that are zero before and after the launch. results / exact distances /
+// replay count as launch_argmin; exact[q] is the answer's binary64 distance.
+void launch_rescore(Bound64 bound, ReplayInputs in, const uint32_t* candidates,
+                    uint32_t k, uint32_t batch, uint32_t rows, double* cand_dist,
+                    uint32_t* done, Result* results, double* exact_distances,
+                    uint32_t* replay_count, cudaStream_t stream);
+
 // ---- hierarchical index (projection)
 // Binary64 projected rows reps[row][j] = sum_i double(sampled[row][i]) *
 // projection[j][i] in i order; `bad` is set when a result is not finite.
