@@ -53,6 +53,9 @@ def parse_args():
                    help="only the precision-strategy table (one JSON line)")
     p.add_argument("--precision-batch", type=int, default=0,
                    help="with --precision-only: one batch size (2048 queries)")
+    p.add_argument("--precision-shape", default="",
+                   help="with --precision-only: ROWS,DIM of a smaller index "
+                        "(profiling captures)")
     return p.parse_args()
 
 
@@ -480,12 +483,15 @@ def run_precision_only(args):
     import ultrahigh_ann_b200 as uha
     from ultrahigh_ann_b200 import synthetic
 
-    ds = synthetic.row_dataset(rows=ROWS, classes=33, queries=2048, d=DIM, seed=1,
+    rows, dim = ROWS, DIM
+    if args.precision_shape:
+        rows, dim = (int(x) for x in args.precision_shape.split(","))
+    ds = synthetic.row_dataset(rows=rows, classes=33, queries=2048, d=dim, seed=1,
                                query_stream=0)
     index = uha.CudaExactL2Index(ds.rows)
     batches = ((args.precision_batch, 2048),) if args.precision_batch else None
     table = precision(ds, index, batches) if batches else precision(ds, index)
-    print(json.dumps({"workload": "exact_l2_r7028_d60660", "precision": table}),
+    print(json.dumps({"workload": f"exact_l2_r{rows}_d{dim}", "precision": table}),
           flush=True)
 
 
