@@ -297,6 +297,67 @@ uha_status uha_precision_scores(const uha_index* index, uha_workspace* workspace
                                 uha_strategy strategy, float* out_scores,
                                 float* out_norms);
 
+/* ------------------------------------------- autotuning and batches
+ * (no reference counterparts) */
+
+/* The scan shape the autotuner chose: kernel 0 = streaming scan
+ * (queries_per_pass queries per pass over the rows), 1 = register-tiled scan
+ * (64 queries per tile), 2 = tensor-core score kernel (tile_queries per
+ * tile); `splits` column / K splits. best_ms is its median event-timed
+ * duration, default_ms that of the built-in heuristic's shape. */
+typedef struct uha_tune_report {
+    uint32_t candidates;
+    uint32_t kernel;
+    uint32_t queries_per_pass;
+    uint32_t tile_queries;
+    uint32_t splits;
+    double best_ms;
+    double default_ms;
+} uha_tune_report;
+
+/* Times every candidate scan shape for batches of exactly `batch` queries with
+ * `strategy` on this workspace (CUDA events, median of 3 launches) and keeps
+ * the fastest: later queries of that batch size on this workspace use it.
+ * Answers do not change (the certification bound follows the shape).
+ * Indexes with a single shape (median hierarchies, trivial indexes) report
+ * zero candidates. report may be NULL. */
+uha_status uha_workspace_autotune(uha_workspace* workspace, uint64_t batch,
+                                  uha_strategy strategy, uha_tune_report* report);
+
+/* Many (index, query count, strategy) pairs on one device answered by one
+ * CUDA graph launch: every pair's pipeline (preparation, projection, scan,
+ * argmin or re-score, result copies) is captured once on its own graph branch.
+ * With autotune != 0 each pair's scan shape is autotuned first. Each pair's
+ * answers equal a uha_query of the same queries on that index. */
+typedef struct uha_batch uha_batch;
+typedef struct uha_batch_stats {
+    uint64_t pairs;
+    uint64_t queries;
+    uint64_t graph_nodes;
+    uint64_t kernel_launches;  /* kernels per run, all pairs */
+    uint64_t replayed_queries;
+    double device_ms;          /* graph launch to completion, last run */
+} uha_batch_stats;
+
+uha_status uha_batch_create(const uha_index* const* indexes,
+                            const uint64_t* query_counts,
+                            const uha_strategy* strategies, uint64_t count,
+                            int autotune, uha_batch** out);
+/* Device buffer (query_counts[pair] x dimension floats) that the graph reads
+ * pair `pair`'s queries from; NULL for an unknown pair. */
+float* uha_batch_query_buffer(uha_batch* batch, uint64_t pair);
+/* queries: NULL (use the query buffers as they are) or one pointer per pair,
+ * host or device (queries_on_device), copied into the query buffers before
+ * the graph launch. out_indices / out_distances (nullable): the pairs'
+ * answers concatenated in pair order. */
+uha_status uha_batch_run(uha_batch* batch, const float* const* queries,
+                         int queries_on_device, uint64_t* out_indices,
+                         double* out_distances);
+uha_status uha_batch_stats_get(const uha_batch* batch, uha_batch_stats* out);
+uha_status uha_batch_tuning(const uha_batch* batch, uint64_t pair,
+                            uha_tune_report* out);
+void uha_batch_destroy(uha_batch* batch);
+
 /* ---------------------------------------------------------- index build */
 
 /* Pair-distance method of the device probability build. DIRECT sums squared

@@ -37,6 +37,19 @@ GEMM_BF16_RERANK = 2
 GEMM_FP8_RERANK = 3
 
 
+class TuneReport(ctypes.Structure):
+    _fields_ = [("candidates", ctypes.c_uint32), ("kernel", ctypes.c_uint32),
+                ("queries_per_pass", ctypes.c_uint32), ("tile_queries", ctypes.c_uint32),
+                ("splits", ctypes.c_uint32), ("best_ms", c_double),
+                ("default_ms", c_double)]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [("pairs", c_uint64), ("queries", c_uint64), ("graph_nodes", c_uint64),
+                ("kernel_launches", c_uint64), ("replayed_queries", c_uint64),
+                ("device_ms", c_double)]
+
+
 class SpaceUsage(ctypes.Structure):
     _fields_ = [("index_payload_bytes", c_uint64),
                 ("query_workspace_payload_bytes", c_uint64),
@@ -108,6 +121,13 @@ SIGNATURES = {
     "uha_workspace_set_timing": (c_int, [c_void_p, c_int]),
     "uha_workspace_stream": (c_void_p, [c_void_p]),
     "uha_workspace_set_candidates": (c_int, [c_void_p, c_uint32]),
+    "uha_workspace_autotune": (c_int, [c_void_p, c_uint64, c_int, POINTER(TuneReport)]),
+    "uha_batch_create": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_int, _H]),
+    "uha_batch_query_buffer": (c_void_p, [c_void_p, c_uint64]),
+    "uha_batch_run": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
+    "uha_batch_stats_get": (c_int, [c_void_p, POINTER(BatchStats)]),
+    "uha_batch_tuning": (c_int, [c_void_p, c_uint64, POINTER(TuneReport)]),
+    "uha_batch_destroy": (None, [c_void_p]),
     "uha_precision_scores": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_int,
                                       c_void_p, c_void_p]),
     "uha_importance_probabilities": (c_int, [c_int, c_int, c_void_p, c_uint64, c_uint64,

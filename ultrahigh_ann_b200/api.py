@@ -323,6 +323,13 @@ def compute_l1_importance_probabilities_gpu(representatives, device: int = 0,
     return _probabilities_gpu(_abi.L1, representatives, device, pair_chunks=pair_chunks)
 
 
+def _tune_dict(r) -> dict:
+    kernel = ("stream", "tile", "tensor")[r.kernel] if r.candidates else "fixed"
+    return {"candidates": r.candidates, "kernel": kernel,
+            "queries_per_pass": r.queries_per_pass, "tile_queries": r.tile_queries,
+            "splits": r.splits, "best_ms": r.best_ms, "default_ms": r.default_ms}
+
+
 class QueryWorkspace:
     """Per-caller device buffers sized for a maximum batch
     (e.g. include/ultrahigh_ann/core/cuda_dense_l2_scan_index.hpp:28-45)."""
@@ -368,6 +375,14 @@ class QueryWorkspace:
         """Records CUDA events around the scan kernel and the device pipeline
         of every query on this workspace (see last_stats())."""
         _check(_abi.load().uha_workspace_set_timing(self._handle, int(enabled)))
+
+    def autotune(self, batch: int, strategy=QueryStrategy.direct) -> dict:
+        """Times every candidate scan shape for batches of exactly `batch`
+        queries and keeps the fastest for this workspace."""
+        r = _abi.TuneReport()
+        _check(_abi.load().uha_workspace_autotune(self._handle, ctypes.c_uint64(batch),
+                                                  int(strategy), ctypes.byref(r)))
+        return _tune_dict(r)
 
     def set_candidates(self, candidates: int) -> None:
         """Candidates per query re-scored by the precision strategies (1-64)."""
@@ -756,3 +771,80 @@ class CudaHierarchicalL1AnnIndex(_CudaHierarchicalIndex):
                     strategy=QueryStrategy.direct, distances=None):
         return super().query_batch(queries, query_count, output, workspace,
                                    QueryStrategy.direct, distances)
+
+
+class QueryBatch:
+    """Many (index, query count, strategy) pairs on one device answered by one
+    CUDA graph launch (uha_batch_*): each pair's pipeline is captured on its
+    own graph branch; with autotune each pair's scan shape is tuned first.
+    Each pair's answers equal a query_batch of the same queries."""
+
+    def __init__(self, pairs, autotune: bool = True):
+        pairs = list(pairs)
+        if not pairs:
+            raise InvalidArgument("a batch needs at least one index")
+        self._indexes = [p[0] for p in pairs]
+        self._counts = [int(p[1]) for p in pairs]
+        strategies = [int(p[2]) if len(p) > 2 else int(QueryStrategy.direct) for p in pairs]
+        n = len(pairs)
+        handles = (ctypes.c_void_p * n)(*[ix._handle for ix in self._indexes])
+        counts = (ctypes.c_uint64 * n)(*self._counts)
+        strat = (ctypes.c_int * n)(*strategies)
+        handle = ctypes.c_void_p()
+        _check(_abi.load().uha_batch_create(handles, counts, strat, ctypes.c_uint64(n),
+                                            int(bool(autotune)), ctypes.byref(handle)))
+        self._handle = handle
+        self.total = sum(self._counts)
+
+    def __del__(self):
+        if getattr(self, "_handle", None):
+            _abi.load().uha_batch_destroy(self._handle)
+            self._handle = None
+
+    def query_buffer(self, pair: int) -> int:
+        """Device pointer the graph reads pair `pair`'s queries from."""
+        return int(_abi.load().uha_batch_query_buffer(self._handle, ctypes.c_uint64(pair)) or 0)
+
+    def run(self, queries=None, on_device: bool = False):
+        """queries: None (use the query buffers) or one array (host) / device
+        pointer (on_device) per pair. Returns (indices, distances) per pair."""
+        n = len(self._counts)
+        keep = []
+        ptrs = None
+        if queries is not None:
+            if len(queries) != n:
+                raise InvalidArgument("one query set per batch pair")
+            arr = []
+            for q, ix, c in zip(queries, self._indexes, self._counts):
+                if on_device:
+                    arr.append(int(q))
+                else:
+                    a = np.ascontiguousarray(q, dtype=np.float32).reshape(-1)
+                    if a.size != c * ix.dimension:
+                        raise InvalidArgument("query batch dimensions do not match index dimension")
+                    keep.append(a)
+                    arr.append(a.ctypes.data)
+            ptrs = (ctypes.c_void_p * n)(*arr)
+        idx = np.zeros(self.total, np.uint64)
+        dist = np.zeros(self.total, np.float64)
+        _check(_abi.load().uha_batch_run(self._handle, ptrs, int(on_device),
+                                         ctypes.c_void_p(idx.ctypes.data),
+                                         ctypes.c_void_p(dist.ctypes.data)))
+        out, o = [], 0
+        for c in self._counts:
+            out.append((idx[o:o + c], dist[o:o + c]))
+            o += c
+        return out
+
+    def stats(self) -> dict:
+        st = _abi.BatchStats()
+        _check(_abi.load().uha_batch_stats_get(self._handle, ctypes.byref(st)))
+        return {"pairs": st.pairs, "queries": st.queries, "graph_nodes": st.graph_nodes,
+                "kernel_launches": st.kernel_launches,
+                "replayed_queries": st.replayed_queries, "device_ms": st.device_ms}
+
+    def tuning(self, pair: int) -> dict:
+        r = _abi.TuneReport()
+        _check(_abi.load().uha_batch_tuning(self._handle, ctypes.c_uint64(pair),
+                                            ctypes.byref(r)))
+        return _tune_dict(r)

@@ -9,6 +9,7 @@
 // finalize kernel reported uncertified queries.
 #include "common.h"
 #include "index_types.h"
+#include "engine_internal.h"
 #include "kernels.h"
 
 #include <algorithm>
@@ -764,7 +765,7 @@ extern "C" uha_status uha_workspace_last_stats(const uha_workspace* workspace,
 
 // ------------------------------------------------------------------ query
 
-namespace {
+namespace uha_engine {
 
 bool precision_strategy(uha_strategy s)
 {
@@ -845,8 +846,11 @@ uha::LowpPlan enqueue_lowp_scores(const uha_index* index, uha_workspace* ws,
     uha::launch_lowp_queries(type, ws->prepared.get(), n, index->padded_dim,
                              ws->queries_lp.get(), lp.pitch, ws->query_scales.get(),
                              ws->query_amax.get(), stream);
-    const uha::LowpPlan plan =
-        uha::plan_lowp(type, index->rows, lp.pitch, n, index->sm_count);
+    const TunedPlan* tuned = ws->find_tuned(n, static_cast<int>(strategy));
+    const uha::LowpPlan plan = tuned != nullptr && tuned->lowp
+                                   ? tuned->lowp_plan
+                                   : uha::plan_lowp(type, index->rows, lp.pitch, n,
+                                                    index->sm_count);
     const uint64_t partial_count =
         checked_mul(checked_mul(plan.splits, n, "partials"), index->rows, "partials");
     if (ws->partials.size() < partial_count) {
@@ -871,12 +875,6 @@ uha::LowpPlan enqueue_lowp_scores(const uha_index* index, uha_workspace* ws,
 // the norm identity), (the replayed distance of each selected row of a
 // hierarchy). `results` / `exact` receive this batch's answers; flags and the
 // replay count accumulate in ws.counters.
-struct BatchContext {
-    const uha_index* index;
-    uha_workspace* ws;
-    uha_strategy strategy;
-    bool want_distances;
-};
 
 uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
                        uha::Result* results, double* exact, bool time_scan,
@@ -947,8 +945,11 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
         op = index->weights32.size() != 0 ? uha::ScanOp::l1_weighted : uha::ScanOp::l1;
     }
     const bool median = hierarchical && index->metric == UHA_L1;
-    uha::ScanPlan plan = uha::plan_scan(index->rows, index->padded_dim, n,
-                                        index->sm_count);
+    const TunedPlan* tuned = ws->find_tuned(n, static_cast<int>(c.strategy));
+    uha::ScanPlan plan = tuned != nullptr && !tuned->lowp
+                             ? tuned->scan
+                             : uha::plan_scan(index->rows, index->padded_dim, n,
+                                              index->sm_count);
     if (median) {
         plan.chunks = 1;
         plan.depth = 0;
@@ -1117,7 +1118,9 @@ void ensure_scan_events(uha_workspace* ws, uint64_t batches)
     }
 }
 
-}  // namespace
+}  // namespace uha_engine
+
+using namespace uha_engine;
 
 extern "C" uha_status uha_query(const uha_index* index, uha_workspace* ws,
                                 const float* queries, uint64_t query_count,

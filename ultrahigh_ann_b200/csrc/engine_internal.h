@@ -1,0 +1,49 @@
+// Query pipeline pieces shared by the engine's host translation units
+// (engine.cu: single calls; batch.cu: captured multi-index batches, the
+// autotuner and the request loop).
+#pragma once
+
+#include "common.h"
+#include "index_types.h"
+#include "kernels.h"
+
+namespace uha_engine {
+
+bool precision_strategy(uha_strategy s);
+uha::LowpType lowp_type(uha_strategy s);
+
+// The index's low-precision rows of `type` (built on first use) and the
+// workspace buffers of the precision strategies.
+const uha::LowpRows& lowp_rows(const uha_index* index, uha::LowpType type,
+                               cudaStream_t stream);
+void ensure_lowp_workspace(uha_workspace* ws, const uha_index* index,
+                           cudaStream_t stream);
+
+struct BatchContext {
+    const uha_index* index;
+    uha_workspace* ws;
+    uha_strategy strategy;
+    bool want_distances;
+};
+
+// Enqueues one batch of n queries (`source`: device, n x dimension floats) on
+// ws->stream; returns the number of kernel launches. Buffers grow (with a
+// stream synchronisation) only when n needs more than an earlier call did.
+uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
+                       uha::Result* results, double* exact, bool time_scan,
+                       cudaEvent_t scan_start, cudaEvent_t scan_stop);
+
+// Answers of a call whose queries need no device work (row 0, distance 0).
+void fill_trivial(uint64_t n, uint64_t* out_indices, double* out_distances);
+
+// Reads the status words copied to ws->host_counters and converts the host
+// copies of results / exact distances into the caller's arrays.
+void finish_call(const uha_index* index, uha_workspace* ws, uint64_t n,
+                 const uha::Result* results, const double* exact,
+                 uint64_t* out_indices, double* out_distances);
+
+void validate_query_call(const uha_index* index, uha_workspace* ws,
+                         const float* queries, uint64_t count, uint64_t batch,
+                         uha_strategy strategy, const uint64_t* out_indices);
+
+}  // namespace uha_engine

@@ -68,6 +68,18 @@ struct uha_index {
     mutable uha::LowpRows lowp[2];
 };
 
+// A scan shape chosen by the autotuner for one (batch size, strategy) of a
+// workspace, with the device time it measured.
+struct TunedPlan {
+    uint64_t batch = 0;
+    int strategy = 0;
+    bool lowp = false;
+    uha::ScanPlan scan{};
+    uha::LowpPlan lowp_plan{};
+    double ms = 0.0;
+    int candidates = 0;
+};
+
 struct uha_workspace {
     const uha_index* owner = nullptr;
     int device = 0;  // the owner's device, kept so destruction never reads the owner
@@ -92,6 +104,17 @@ struct uha_workspace {
     uha::DeviceBuffer<double> cand_dist;          // [batch][candidates_per_query]
     uha::DeviceBuffer<uint32_t> rescore_done;     // per query, zero between calls
     uint32_t candidates_per_query = 32;
+    std::vector<TunedPlan> tuned;  // autotuned shapes (uha_workspace_autotune)
+
+    const TunedPlan* find_tuned(uint64_t batch, int strategy) const
+    {
+        for (const TunedPlan& t : tuned) {
+            if (t.batch == batch && t.strategy == strategy) {
+                return &t;
+            }
+        }
+        return nullptr;
+    }
     uha::PinnedBuffer<uha::Result> host_results;
     uha::PinnedBuffer<double> host_exact;
     uha::PinnedBuffer<uint32_t> host_counters;

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <vector>
 
 namespace uha {
 
@@ -82,6 +83,13 @@ struct ScanPlan {
 };
 ScanPlan plan_scan(uint64_t rows, uint64_t padded_dim, uint64_t batch,
                    int sm_count);
+// The stream kernel with `queries_per_pass` (1, 2, 4, 8) queries per pass; the
+// tile kernel with about `splits` column splits.
+ScanPlan stream_plan(uint64_t padded_dim, int queries_per_pass);
+ScanPlan tile_plan(uint64_t padded_dim, uint64_t splits);
+// Plans the autotuner times for one (index, batch): the heuristic plan first.
+std::vector<ScanPlan> scan_candidates(uint64_t rows, uint64_t padded_dim,
+                                      uint64_t batch, int sm_count);
 void launch_scan(const ScanPlan& plan, ScanOp op, const float* rows,
                  uint64_t row_count, uint64_t padded_dim, const float* weights,
                  const float* queries, uint64_t batch, float* partials,
@@ -157,6 +165,11 @@ struct LowpPlan {
 };
 LowpPlan plan_lowp(LowpType type, uint64_t rows, uint64_t pitch, uint64_t batch,
                    int sm_count);
+// Query tile width `bn` (16, 32, 64, 128, 256) and about `splits` K splits.
+LowpPlan lowp_plan(LowpType type, uint64_t pitch, int bn, uint64_t splits);
+// Plans the autotuner times for one (index, batch): the heuristic plan first.
+std::vector<LowpPlan> lowp_candidates(LowpType type, uint64_t rows, uint64_t pitch,
+                                      uint64_t batch, int sm_count);
 // partials[split][q][row] = q~ . v~ over the split's K slices (FP8: times the
 // row and query scales). error_flag |= 8 when a pipeline wait ran out.
 void launch_lowp_scores(const LowpPlan& plan, LowpType type, const void* rows_lp,

@@ -867,6 +867,47 @@ LowpPlan plan_lowp(LowpType type, uint64_t rows, uint64_t pitch, uint64_t batch,
     return plan;
 }
 
+LowpPlan lowp_plan(LowpType type, uint64_t pitch, int bn, uint64_t splits)
+{
+    LowpPlan plan{};
+    plan.bn = bn;
+    plan.kblocks = static_cast<uint32_t>(pitch / (type == LowpType::fp8_e4m3 ? 128 : 64));
+    splits = std::max<uint64_t>(1, std::min<uint64_t>(splits, plan.kblocks));
+    plan.kblocks_per_split = static_cast<uint32_t>((plan.kblocks + splits - 1) / splits);
+    plan.splits = (plan.kblocks + plan.kblocks_per_split - 1) / plan.kblocks_per_split;
+    return plan;
+}
+
+std::vector<LowpPlan> lowp_candidates(LowpType type, uint64_t rows, uint64_t pitch,
+                                      uint64_t batch, int sm_count)
+{
+    std::vector<LowpPlan> out;
+    out.push_back(plan_lowp(type, rows, pitch, batch, sm_count));
+    const uint64_t kblocks = pitch / (type == LowpType::fp8_e4m3 ? 128 : 64);
+    for (int bn : {16, 32, 64, 128, 256}) {
+        if (bn > 16 && static_cast<uint64_t>(bn) / 2 >= batch) {
+            continue;  // wider than twice the batch: only padding
+        }
+        for (uint64_t splits : {1, 2, 3, 4, 6, 8, 12, 16}) {
+            if (splits <= std::max<uint64_t>(1, kblocks / 4)) {
+                out.push_back(lowp_plan(type, pitch, bn, splits));
+            }
+        }
+    }
+    std::vector<LowpPlan> unique;
+    for (const LowpPlan& p : out) {
+        bool seen = false;
+        for (const LowpPlan& u : unique) {
+            seen = seen || (u.bn == p.bn && u.splits == p.splits &&
+                            u.kblocks_per_split == p.kblocks_per_split);
+        }
+        if (!seen) {
+            unique.push_back(p);
+        }
+    }
+    return unique;
+}
+
 void launch_lowp_scores(const LowpPlan& plan, LowpType type, const void* rows_lp,
                         const float* row_scale, uint64_t row_count,
                         const void* queries_lp, const float* query_scale,

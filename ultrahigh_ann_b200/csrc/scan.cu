@@ -16,6 +16,8 @@
 #include "common.h"
 #include "kernels.h"
 
+#include <vector>
+
 #include <algorithm>
 
 namespace uha {
@@ -379,34 +381,23 @@ void launch_tile_op(dim3 grid, cudaStream_t stream, const float* rows,
 
 }  // namespace
 
-ScanPlan plan_scan(uint64_t rows, uint64_t padded_dim, uint64_t batch,
-                   int sm_count)
+ScanPlan stream_plan(uint64_t padded_dim, int queries_per_pass)
 {
     ScanPlan plan{};
-    if (batch <= 8) {
-        plan.kernel = 0;
-        plan.queries_per_pass = 1;
-        while (plan.queries_per_pass < static_cast<int>(batch)) {
-            plan.queries_per_pass *= 2;
-        }
-        plan.chunks = static_cast<uint32_t>(
-            (padded_dim + kStreamChunk - 1) / kStreamChunk);
-        // per lane: 4 additions per float4, kStreamChunk / 128 float4s per
-        // lane; then 5 shuffle levels; then the chunk sum in finalize.
-        plan.depth = 4 * (kStreamChunk / 128) + 5 + plan.chunks;
-        return plan;
-    }
+    plan.kernel = 0;
+    plan.queries_per_pass = queries_per_pass;
+    plan.chunks = static_cast<uint32_t>((padded_dim + kStreamChunk - 1) / kStreamChunk);
+    // per lane: 4 additions per float4, kStreamChunk / 128 float4s per lane;
+    // then 5 shuffle levels; then the chunk sum in the argmin.
+    plan.depth = 4 * (kStreamChunk / 128) + 5 + plan.chunks;
+    return plan;
+}
+
+ScanPlan tile_plan(uint64_t padded_dim, uint64_t splits)
+{
+    ScanPlan plan{};
     plan.kernel = 1;
-    const uint64_t row_tiles = (rows + kTileRows - 1) / kTileRows;
-    const uint64_t query_tiles = (batch + kTileQueries - 1) / kTileQueries;
-    const uint64_t ctas = row_tiles * query_tiles;
-    const uint64_t target = 2ull * static_cast<uint64_t>(sm_count);
-    uint64_t splits = 1;
-    if (ctas < target) {
-        splits = (target + ctas - 1) / ctas;
-    }
-    const uint64_t max_splits = std::max<uint64_t>(1, padded_dim / 512);
-    splits = std::min(splits, max_splits);
+    splits = std::max<uint64_t>(1, std::min(splits, std::max<uint64_t>(1, padded_dim / 512)));
     uint64_t k_per_split = round_up((padded_dim + splits - 1) / splits, kTileK);
     if (k_per_split == 0) {
         k_per_split = kTileK;
@@ -415,10 +406,63 @@ ScanPlan plan_scan(uint64_t rows, uint64_t padded_dim, uint64_t batch,
     plan.k_per_split = static_cast<uint32_t>(k_per_split);
     plan.chunks = static_cast<uint32_t>(std::max<uint64_t>(1, splits));
     // 32 sequential additions inside a stage, one per stage into the total,
-    // then the split sum in finalize.
-    plan.depth = static_cast<uint32_t>(kTileK + (k_per_split / kTileK) +
-                                       plan.chunks);
+    // then the split sum in the argmin.
+    plan.depth = static_cast<uint32_t>(kTileK + (k_per_split / kTileK) + plan.chunks);
     return plan;
+}
+
+ScanPlan plan_scan(uint64_t rows, uint64_t padded_dim, uint64_t batch,
+                   int sm_count)
+{
+    if (batch <= 8) {
+        int nq = 1;
+        while (nq < static_cast<int>(batch)) {
+            nq *= 2;
+        }
+        return stream_plan(padded_dim, nq);
+    }
+    const uint64_t row_tiles = (rows + kTileRows - 1) / kTileRows;
+    const uint64_t query_tiles = (batch + kTileQueries - 1) / kTileQueries;
+    const uint64_t ctas = row_tiles * query_tiles;
+    const uint64_t target = 2ull * static_cast<uint64_t>(sm_count);
+    uint64_t splits = 1;
+    if (ctas < target) {
+        splits = (target + ctas - 1) / ctas;
+    }
+    return tile_plan(padded_dim, splits);
+}
+
+std::vector<ScanPlan> scan_candidates(uint64_t rows, uint64_t padded_dim,
+                                      uint64_t batch, int sm_count)
+{
+    std::vector<ScanPlan> out;
+    out.push_back(plan_scan(rows, padded_dim, batch, sm_count));
+    if (batch <= 64) {
+        // the stream kernel re-reads the rows once per pass of 8 queries
+        for (int nq : {1, 2, 4, 8}) {
+            if (nq <= static_cast<int>(2 * batch)) {
+                out.push_back(stream_plan(padded_dim, nq));
+            }
+        }
+    }
+    if (batch > 1) {
+        for (uint64_t splits : {1, 2, 3, 4, 6, 8, 12, 16}) {
+            out.push_back(tile_plan(padded_dim, splits));
+        }
+    }
+    // drop duplicates (same kernel, pass width and split)
+    std::vector<ScanPlan> unique;
+    for (const ScanPlan& p : out) {
+        bool seen = false;
+        for (const ScanPlan& u : unique) {
+            seen = seen || (u.kernel == p.kernel && u.queries_per_pass == p.queries_per_pass &&
+                            u.chunks == p.chunks && u.k_per_split == p.k_per_split);
+        }
+        if (!seen) {
+            unique.push_back(p);
+        }
+    }
+    return unique;
 }
 
 void launch_scan(const ScanPlan& plan, ScanOp op, const float* rows,
