@@ -358,6 +358,83 @@ uha_status uha_batch_tuning(const uha_batch* batch, uint64_t pair,
                             uha_tune_report* out);
 void uha_batch_destroy(uha_batch* batch);
 
+/* ------------------------------------------------------- request loop
+ * (no reference counterpart)
+ *
+ * A serving loop over device-resident indexes on one GPU. Requests (one
+ * query each, tagged with an index) are queued per index; a dispatcher thread
+ * forms a batch from an index's queue as soon as one of `slots` in-flight
+ * batches is free (continuous batching: queries that arrive while others are
+ * on the GPU go into the next batch), so batches of different indexes overlap
+ * on the device. Every in-flight batch holds a pooled query workspace of its
+ * index; a new workspace is admitted only while the pooled workspaces' device
+ * bytes stay within hbm_budget_bytes (idle workspaces of other indexes are
+ * released to make room; otherwise the batch waits for one to finish). Each
+ * answer equals a uha_query of that query alone on its index. */
+typedef struct uha_server uha_server;
+
+typedef struct uha_server_config {
+    uint64_t hbm_budget_bytes;  /* device bytes of pooled workspaces, at most */
+    uint32_t max_batch;         /* queries per batch, at most */
+    uint32_t slots;             /* batches in flight, at most */
+    int queries_on_device;      /* request query pointers are device pointers */
+} uha_server_config;
+
+typedef struct uha_server_result {
+    uint64_t tag;
+    uint32_t index_id;
+    uint32_t status;     /* uha_status of this query */
+    uint64_t row;
+    double distance;
+    double latency_us;   /* submission to completion seen by the loop */
+} uha_server_result;
+
+typedef struct uha_server_stats {
+    uint64_t submitted;
+    uint64_t completed;
+    uint64_t failed;
+    uint64_t batches;
+    double mean_batch;
+    double p50_us;
+    double p99_us;
+    double max_us;
+    double throughput_qps;        /* completed / (last completion - first submission) */
+    uint64_t workspace_bytes;     /* pooled workspaces now */
+    uint64_t peak_workspace_bytes;
+    uint64_t admission_waits;     /* dispatches deferred by the budget */
+    uint64_t evictions;           /* idle workspaces released for another index */
+    uint32_t peak_in_flight;
+} uha_server_stats;
+
+uha_status uha_server_create(int device, const uha_server_config* config,
+                             uha_server** out);
+/* Registers an index (its workspace is sized and warmed at max_batch here);
+ * fails with UHA_LENGTH_ERROR when one workspace exceeds the budget. The
+ * index must outlive the server. */
+uha_status uha_server_add_index(uha_server* server, const uha_index* index,
+                                uha_strategy strategy, uint32_t* out_id);
+/* Queues one query (dimension floats at `query`, host or device per the
+ * config; the memory must stay valid until its result is polled).
+ * Thread-safe. */
+uha_status uha_server_submit(uha_server* server, uint32_t index_id,
+                             const float* query, uint64_t tag);
+/* Open-loop load: submits request i at arrival_us[i] microseconds after the
+ * call (ascending), from the calling thread. */
+uha_status uha_server_replay(uha_server* server, uint64_t count,
+                             const uint32_t* index_ids,
+                             const float* const* queries,
+                             const double* arrival_us, const uint64_t* tags);
+/* Waits until every submitted request has completed. */
+uha_status uha_server_drain(uha_server* server);
+/* Moves up to `capacity` completed results into `out`; *count receives how
+ * many. */
+uha_status uha_server_poll(uha_server* server, uha_server_result* out,
+                           uint64_t capacity, uint64_t* count);
+uha_status uha_server_stats_get(uha_server* server, uha_server_stats* out);
+/* Clears the latency record and counters (the pool stays). */
+uha_status uha_server_reset_stats(uha_server* server);
+void uha_server_destroy(uha_server* server);
+
 /* ---------------------------------------------------------- index build */
 
 /* Pair-distance method of the device probability build. DIRECT sums squared

@@ -50,6 +50,26 @@ class BatchStats(ctypes.Structure):
                 ("device_ms", c_double)]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", c_uint64), ("max_batch", ctypes.c_uint32),
+                ("slots", ctypes.c_uint32), ("queries_on_device", c_int)]
+
+
+class ServerResult(ctypes.Structure):
+    _fields_ = [("tag", c_uint64), ("index_id", ctypes.c_uint32),
+                ("status", ctypes.c_uint32), ("row", c_uint64), ("distance", c_double),
+                ("latency_us", c_double)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", c_uint64), ("completed", c_uint64), ("failed", c_uint64),
+                ("batches", c_uint64), ("mean_batch", c_double), ("p50_us", c_double),
+                ("p99_us", c_double), ("max_us", c_double), ("throughput_qps", c_double),
+                ("workspace_bytes", c_uint64), ("peak_workspace_bytes", c_uint64),
+                ("admission_waits", c_uint64), ("evictions", c_uint64),
+                ("peak_in_flight", ctypes.c_uint32)]
+
+
 class SpaceUsage(ctypes.Structure):
     _fields_ = [("index_payload_bytes", c_uint64),
                 ("query_workspace_payload_bytes", c_uint64),
@@ -128,6 +148,16 @@ SIGNATURES = {
     "uha_batch_stats_get": (c_int, [c_void_p, POINTER(BatchStats)]),
     "uha_batch_tuning": (c_int, [c_void_p, c_uint64, POINTER(TuneReport)]),
     "uha_batch_destroy": (None, [c_void_p]),
+    "uha_server_create": (c_int, [c_int, POINTER(ServerConfig), _H]),
+    "uha_server_add_index": (c_int, [c_void_p, c_void_p, c_int, POINTER(ctypes.c_uint32)]),
+    "uha_server_submit": (c_int, [c_void_p, ctypes.c_uint32, c_void_p, c_uint64]),
+    "uha_server_replay": (c_int, [c_void_p, c_uint64, c_void_p, c_void_p, c_void_p,
+                                   c_void_p]),
+    "uha_server_drain": (c_int, [c_void_p]),
+    "uha_server_poll": (c_int, [c_void_p, c_void_p, c_uint64, _U]),
+    "uha_server_stats_get": (c_int, [c_void_p, POINTER(ServerStats)]),
+    "uha_server_reset_stats": (c_int, [c_void_p]),
+    "uha_server_destroy": (None, [c_void_p]),
     "uha_precision_scores": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_int,
                                       c_void_p, c_void_p]),
     "uha_importance_probabilities": (c_int, [c_int, c_int, c_void_p, c_uint64, c_uint64,

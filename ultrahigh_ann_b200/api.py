@@ -848,3 +848,86 @@ class QueryBatch:
         _check(_abi.load().uha_batch_tuning(self._handle, ctypes.c_uint64(pair),
                                             ctypes.byref(r)))
         return _tune_dict(r)
+
+
+class Server:
+    """Request loop over device-resident indexes on one GPU (uha_server_*):
+    per-index queues, continuous batching into up to `slots` in-flight
+    batches, workspaces admitted by an HBM budget, latency per request.
+    Query memory (host arrays or device pointers with queries_on_device) must
+    stay valid until the request has completed; the wrapper keeps the host
+    arrays it was given alive until drain()."""
+
+    RESULT_DTYPE = np.dtype([("tag", np.uint64), ("index_id", np.uint32),
+                             ("status", np.uint32), ("row", np.uint64),
+                             ("distance", np.float64), ("latency_us", np.float64)])
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 8 << 30,
+                 max_batch: int = 256, slots: int = 4, queries_on_device: bool = False):
+        cfg = _abi.ServerConfig(int(hbm_budget_bytes), int(max_batch), int(slots),
+                                int(bool(queries_on_device)))
+        handle = ctypes.c_void_p()
+        _check(_abi.load().uha_server_create(int(device), ctypes.byref(cfg),
+                                             ctypes.byref(handle)))
+        self._handle = handle
+        self._on_device = bool(queries_on_device)
+        self._indexes = []
+        self._keep = []
+
+    def __del__(self):
+        if getattr(self, "_handle", None):
+            _abi.load().uha_server_destroy(self._handle)
+            self._handle = None
+
+    def add_index(self, index: "_CudaIndex", strategy=QueryStrategy.direct) -> int:
+        out = ctypes.c_uint32()
+        _check(_abi.load().uha_server_add_index(self._handle, index._handle, int(strategy),
+                                                ctypes.byref(out)))
+        self._indexes.append(index)
+        return out.value
+
+    def _pointer(self, query) -> int:
+        if self._on_device:
+            return int(query)
+        a = np.ascontiguousarray(query, dtype=np.float32)
+        self._keep.append(a)
+        return a.ctypes.data
+
+    def submit(self, index_id: int, query, tag: int) -> None:
+        _check(_abi.load().uha_server_submit(self._handle, ctypes.c_uint32(index_id),
+                                             ctypes.c_void_p(self._pointer(query)),
+                                             ctypes.c_uint64(tag)))
+
+    def replay(self, index_ids, queries, arrival_us, tags=None) -> None:
+        """Open-loop load: request i arrives arrival_us[i] microseconds after
+        the call; queries[i] is a host array or a device pointer."""
+        n = len(index_ids)
+        ids = np.ascontiguousarray(index_ids, dtype=np.uint32)
+        ptrs = np.array([self._pointer(q) for q in queries], dtype=np.uint64)
+        arr = np.ascontiguousarray(arrival_us, dtype=np.float64)
+        tg = None if tags is None else np.ascontiguousarray(tags, dtype=np.uint64)
+        _check(_abi.load().uha_server_replay(
+            self._handle, ctypes.c_uint64(n), ctypes.c_void_p(ids.ctypes.data),
+            ctypes.c_void_p(ptrs.ctypes.data), ctypes.c_void_p(arr.ctypes.data),
+            ctypes.c_void_p(tg.ctypes.data) if tg is not None else None))
+
+    def drain(self) -> None:
+        """Waits for every submitted request; their host queries are then
+        released by the wrapper."""
+        _check(_abi.load().uha_server_drain(self._handle))
+        self._keep.clear()
+
+    def poll(self, capacity: int = 1 << 20) -> np.ndarray:
+        buf = np.zeros(capacity, dtype=self.RESULT_DTYPE)
+        got = ctypes.c_uint64()
+        _check(_abi.load().uha_server_poll(self._handle, ctypes.c_void_p(buf.ctypes.data),
+                                           ctypes.c_uint64(capacity), ctypes.byref(got)))
+        return buf[:got.value]
+
+    def stats(self) -> dict:
+        st = _abi.ServerStats()
+        _check(_abi.load().uha_server_stats_get(self._handle, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in _abi.ServerStats._fields_}
+
+    def reset_stats(self) -> None:
+        _check(_abi.load().uha_server_reset_stats(self._handle))

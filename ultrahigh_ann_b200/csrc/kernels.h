@@ -68,6 +68,10 @@ void launch_prepare_sampled(const float* queries, uint64_t batch, uint64_t dim,
                             uint64_t sample_size, float* out,
                             uint64_t padded_dim, int* error_flag,
                             cudaStream_t stream);
+// out[q] = sources[q] (count device vectors of dim floats, gathered into
+// one contiguous batch).
+void launch_gather_vectors(const float* const* sources, uint64_t count, uint64_t dim,
+                           float* out, cudaStream_t stream);
 void launch_query_norms(const float* prepared, uint64_t batch,
                         uint64_t padded_dim, float* norms, cudaStream_t stream);
 

@@ -17,6 +17,8 @@
 #include "common.h"
 #include "kernels.h"
 
+#include <algorithm>
+
 namespace uha {
 namespace {
 
@@ -132,7 +134,33 @@ uint32_t grid_for(uint64_t total)
                                                       : 148ull * 64);
 }
 
+// out[q][j] = sources[q][j] for j < dim: the queries of one batch gathered
+// from individually addressed device vectors (grid: column chunks x queries).
+__global__ void gather_vectors_kernel(const float* const* __restrict__ sources,
+                                      uint64_t dim, float* __restrict__ out)
+{
+    const uint64_t q = blockIdx.y;
+    const float* src = sources[q];
+    float* dst = out + q * dim;
+    for (uint64_t j = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; j < dim;
+         j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        dst[j] = src[j];
+    }
+}
+
 }  // namespace
+
+void launch_gather_vectors(const float* const* sources, uint64_t count, uint64_t dim,
+                           float* out, cudaStream_t stream)
+{
+    if (count == 0 || dim == 0) {
+        return;
+    }
+    const uint64_t chunks = std::min<uint64_t>((dim + kThreads - 1) / kThreads, 64);
+    gather_vectors_kernel<<<dim3(static_cast<uint32_t>(chunks), static_cast<uint32_t>(count)),
+                            kThreads, 0, stream>>>(sources, dim, out);
+    check_cuda(cudaGetLastError(), "cannot launch query gather kernel");
+}
 
 void launch_prepare_dense(const float* queries, uint64_t batch, uint64_t dim,
                           float* out, uint64_t padded_dim, int* error_flag,
