@@ -51,6 +51,8 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--precision-only", action="store_true",
                    help="only the precision-strategy table (one JSON line)")
+    p.add_argument("--only", default="", choices=["", "precision", "batched", "serving"],
+                   help="only this section of the bench (one JSON line)")
     p.add_argument("--precision-batch", type=int, default=0,
                    help="with --precision-only: one batch size (2048 queries)")
     p.add_argument("--precision-shape", default="",
@@ -265,6 +267,10 @@ def run_engine(args):
         torch.cuda.empty_cache()
         line["suite"] = suite(ds, index)
         line["precision"] = precision(ds, index)
+        torch.cuda.empty_cache()
+        line["batched"] = batched(ds)
+        torch.cuda.empty_cache()
+        line["serving"] = serving(ds)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -419,6 +425,169 @@ def precision(ds, exact_index, batches=((1, 256), (64, 2048), (1024, 2048))):
     return out
 
 
+_PROBS: dict = {}
+
+
+def _probabilities(metric: str, rows):
+    """GPU importance probabilities of the bench rows, computed once per metric."""
+    import ultrahigh_ann_b200 as uha
+
+    if metric not in _PROBS:
+        fn = (uha.compute_l2_importance_probabilities_gpu if metric == "l2"
+              else uha.compute_l1_importance_probabilities_gpu)
+        _PROBS[metric] = fn(rows).probabilities
+    return _PROBS[metric]
+
+
+def batched(ds, per_index=4096, reps=3):
+    """16 hierarchical indexes of uneven (rows, |I|, p), L2 (JL) and L1
+    (Cauchy, median), 4,096 queries each, answered by one captured CUDA graph
+    per run with autotuned scan shapes; against the same queries answered
+    index by index (uha_query_many, built-in shapes, one stream). The indexes
+    take row subsets of the r = 7,028, d = 60,660 data and the probabilities
+    of the full matrix."""
+    import torch
+
+    import ultrahigh_ann_b200 as uha
+
+    rows_choice = (1024, 2048, 4096, 7028)
+    p_choice = (16, 64, 256)
+    t_choice = (16, 32, 64)
+    specs, indexes = [], []
+    for i in range(16):
+        metric = "l2" if i % 2 == 0 else "l1"
+        r, p, T = rows_choice[i % 4], p_choice[i % 3], t_choice[(i // 3) % 3]
+        cls = (uha.CudaHierarchicalL2AnnIndex if metric == "l2"
+               else uha.CudaHierarchicalL1AnnIndex)
+        ix = cls(ds.rows[:r], T, p, uha.MT19937_64(100 + i),
+                 importance_probabilities=_probabilities(metric, ds.rows))
+        indexes.append(ix)
+        specs.append({"metric": metric, "rows": r, "T": T, "k": len(ix.coordinate_sample),
+                      "p": p})
+    qdev = torch.from_numpy(ds.queries[:per_index]).cuda()
+    t = time.perf_counter()
+    batch = uha.QueryBatch([(ix, per_index, uha.QueryStrategy.direct) for ix in indexes],
+                           autotune=True)
+    setup_s = time.perf_counter() - t
+    batch.run([qdev.data_ptr()] * len(indexes), on_device=True)  # queries into its buffers
+    ms = []
+    for _ in range(reps):
+        res = batch.run(None)
+        ms.append(batch.stats()["device_ms"])
+    st = batch.stats()
+    tuned = [batch.tuning(i) for i in range(len(indexes))]
+    # the same work index by index
+    ws = [ix.make_query_workspace(per_index) for ix in indexes]
+    out = np.zeros(per_index, np.uint64)
+    for ix, w, i in zip(indexes, ws, range(len(indexes))):
+        ix.query_many(batch.query_buffer(i), per_index, per_index, out, w, on_device=True)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    agree = []
+    for ix, w, i in zip(indexes, ws, range(len(indexes))):
+        ix.query_many(batch.query_buffer(i), per_index, per_index, out, w, on_device=True)
+        agree.append(bool(np.array_equal(out, res[i][0])))
+    seq_s = time.perf_counter() - t
+    total = per_index * len(indexes)
+    best = min(ms)
+    return {"indexes": specs, "queries_per_index": per_index,
+            "graph": {"queries_per_s": round(total / (best * 1e-3), 1),
+                      "device_ms": round(best, 3), "graph_nodes": st["graph_nodes"],
+                      "kernels_per_run": st["kernel_launches"],
+                      "replayed": st["replayed_queries"],
+                      "setup_s_with_autotune": round(setup_s, 2)},
+            "index_by_index": {"queries_per_s": round(total / seq_s, 1),
+                               "wall_ms": round(seq_s * 1e3, 3)},
+            "answers_equal": all(agree),
+            "autotune": {"pairs_changed": sum(1 for t_ in tuned
+                                               if t_["candidates"] and t_["best_ms"] < t_["default_ms"]),
+                         "default_scan_ms": round(sum(t_["default_ms"] for t_ in tuned), 3),
+                         "tuned_scan_ms": round(sum(t_["best_ms"] for t_ in tuned), 3)}}
+
+
+def serving(ds, rates=(10_000, 100_000, 1_000_000), seconds=0.5, pool=2048):
+    """Request loop over 8 device-resident indexes (exact, flat and
+    hierarchical, L1 and L2; r from 33 to 7,028, d = 60,660), Poisson arrivals
+    with a uniformly chosen index per request, queries from a device-resident
+    pool. Plain strategies, then BF16 + re-score on the exact and flat L2
+    indexes; agreement of the exact L2 answers with the binary64 exact argmin."""
+    import torch
+
+    import ultrahigh_ann_b200 as uha
+
+    S = uha.QueryStrategy
+    pl2, pl1 = _probabilities("l2", ds.rows), _probabilities("l1", ds.rows)
+    r33 = ds.rows[:33]
+    build = [
+        ("exact_l2_r33", lambda: uha.CudaExactL2Index(r33), True),
+        ("flat_l2_r33_T8", lambda: uha.CudaSampledCoordinateL2AnnIndex(
+            r33, pl2, 8, uha.MT19937_64(1)), True),
+        ("exact_l2_r7028", lambda: uha.CudaExactL2Index(ds.rows), True),
+        ("flat_l2_r7028_T32", lambda: uha.CudaSampledCoordinateL2AnnIndex(
+            ds.rows, pl2, 32, uha.MT19937_64(2)), True),
+        ("flat_l1_r7028_T32", lambda: uha.CudaSampledCoordinateL1AnnIndex(
+            ds.rows, pl1, 32, uha.MT19937_64(3)), False),
+        ("hier_l2_r7028_p64", lambda: uha.CudaHierarchicalL2AnnIndex(
+            ds.rows, 32, 64, uha.MT19937_64(4), importance_probabilities=pl2), False),
+        ("hier_l1_r2048_p16", lambda: uha.CudaHierarchicalL1AnnIndex(
+            ds.rows[:2048], 32, 16, uha.MT19937_64(5), importance_probabilities=pl1), False),
+        ("exact_l1_r1024", lambda: uha.CudaExactL1Index(ds.rows[:1024]), False),
+    ]
+    names = [b[0] for b in build]
+    indexes = [b[1]() for b in build]
+    qdev = torch.from_numpy(ds.queries[:pool]).cuda()
+    base, stride = qdev.data_ptr(), ds.rows.shape[1] * 4
+    # binary64 exact answers of the pool on the exact L2 index
+    ws = indexes[2].make_query_workspace(256)
+    exact = np.zeros(pool, np.uint64)
+    indexes[2].query_many(qdev.data_ptr(), pool, 256, exact, ws, on_device=True)
+    rng = np.random.default_rng(7)
+    out = {"indexes": names, "pool_queries": pool, "seconds_per_rate": seconds, "modes": []}
+    for mode in ("plain", "bf16_rerank"):
+        server = uha.Server(hbm_budget_bytes=16 << 30, max_batch=256, slots=8,
+                            queries_on_device=True)
+        for (name, _, l2_exact_or_flat), ix in zip(build, indexes):
+            st = S.gemm_bf16_rerank if (mode == "bf16_rerank" and l2_exact_or_flat) else S.direct
+            server.add_index(ix, st)
+        # warm-up load, then the measured rates
+        n = 2000
+        server.replay(rng.integers(0, 8, n), [base + int(j) * stride
+                                             for j in rng.integers(0, pool, n)],
+                      np.arange(n) * 50.0)
+        server.drain()
+        server.poll()
+        rows = []
+        for rate in rates:
+            n = int(rate * seconds)
+            ids = rng.integers(0, 8, n).astype(np.uint32)
+            qi = rng.integers(0, pool, n)
+            arrival = np.cumsum(rng.exponential(1e6 / rate, n))
+            server.reset_stats()
+            t = time.perf_counter()
+            server.replay(ids, (base + qi.astype(np.uint64) * stride).tolist(), arrival,
+                          np.arange(n))
+            server.drain()
+            wall = time.perf_counter() - t
+            res = server.poll(n)
+            st = server.stats()
+            order = np.argsort(res["tag"])
+            res = res[order]
+            sel = ids == 2
+            agreement = float(np.mean(res["row"][sel] == exact[qi[sel]])) if sel.any() else None
+            rows.append({"offered_qps": rate, "requests": n,
+                         "throughput_qps": round(st["throughput_qps"], 1),
+                         "p50_ms": round(st["p50_us"] / 1e3, 4),
+                         "p99_ms": round(st["p99_us"] / 1e3, 4),
+                         "mean_batch": round(st["mean_batch"], 2),
+                         "failed": st["failed"], "peak_in_flight": st["peak_in_flight"],
+                         "peak_workspace_gb": round(st["peak_workspace_bytes"] / 2**30, 3),
+                         "exact_l2_agreement_vs_fp64": agreement,
+                         "wall_s": round(wall, 2)})
+        out["modes"].append({"mode": mode, "rates": rows})
+        del server
+    return out
+
+
 # ------------------------------------------------------------ reference arm
 def run_reference(args):
     world, rank, _ = dist_env()
@@ -472,10 +641,23 @@ def main():
     args = parse_args()
     if args.impl == "reference":
         run_reference(args)
-    elif args.precision_only:
+    elif args.precision_only or args.only == "precision":
         run_precision_only(args)
+    elif args.only:
+        run_section(args)
     else:
         run_engine(args)
+
+
+def run_section(args):
+    """One section (batched or serving) alone on one GPU."""
+    from ultrahigh_ann_b200 import synthetic
+
+    ds = synthetic.row_dataset(rows=ROWS, classes=33, queries=4096, d=DIM, seed=1,
+                               query_stream=0)
+    fn = batched if args.only == "batched" else serving
+    print(json.dumps({"workload": f"{args.only}_r{ROWS}_d{DIM}", args.only: fn(ds)}),
+          flush=True)
 
 
 def run_precision_only(args):
