@@ -43,6 +43,12 @@ __device__ __forceinline__ Bounds2 bound_of(float d, const Bound& b,
     }
     const float e = __fadd_ru(b.row_err[row], b.query_err[q]);
     if (b.mode == BoundMode::median) {
+        if (d < 0.f) {
+            // a row the median scan set aside: binary32 median at least -d
+            const float t = -d;
+            const float err = __fadd_ru(__fadd_ru(__fmul_ru(b.rel, t), e), b.abs);
+            return {fmaxf(0.f, __fsub_rd(t, err)), inf};
+        }
         const float err = __fadd_ru(__fadd_ru(__fmul_ru(b.rel, d), e), b.abs);
         return {fmaxf(0.f, __fsub_rd(d, err)), __fadd_ru(d, err)};
     }

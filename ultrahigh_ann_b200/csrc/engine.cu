@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <string>
 #include <vector>
@@ -590,6 +591,17 @@ extern "C" uha_status uha_hierarchical_index_create(
         check_cuda(cudaMemcpy(&host_bad, bad.get(), sizeof(int),
                               cudaMemcpyDeviceToHost),
                    "row projection failed");
+        {
+            std::vector<float> err(row_count);
+            check_cuda(cudaMemcpy(err.data(), index->row_err.get(), row_count * sizeof(float),
+                                  cudaMemcpyDeviceToHost),
+                       "row projection failed");
+            index->row_err_max = 0.f;
+            for (float e : err) {
+                index->row_err_max = std::isnan(e) ? std::numeric_limits<float>::infinity()
+                                                   : std::max(index->row_err_max, e);
+            }
+        }
         if (host_bad & 1) {
             fail(UHA_OVERFLOW_ERROR, "projected representatives is not finite");
         }
@@ -965,10 +977,19 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
     if (time_scan) {
         check_cuda(cudaEventRecord(scan_start, stream), "event");
     }
+    // median bound: binary32 |diff| and midpoint roundings; the binary64 ones
+    const float median_rel = std::ldexp(6.0f, -24);
+    const float median_abs = std::ldexp(1.0f, -126);
     if (median) {
+        if (ws->median_min.size() < n) {
+            check_cuda(cudaStreamSynchronize(stream), "CUDA query failed");
+            ws->median_min.allocate(std::max<uint64_t>(n, ws->max_batch));
+        }
         uha::launch_median_scan(index->scan_rows.get(), index->rows, index->padded_dim,
                                 index->projection_dimension, scan_queries, n,
-                                ws->partials.get(), stream);
+                                ws->query_err.get(), index->row_err_max, median_rel,
+                                median_abs, ws->median_min.get(), ws->partials.get(),
+                                stream);
     } else {
         uha::launch_scan(plan, op, index->scan_rows.get(), index->rows,
                          index->padded_dim, index->weights32.get(), scan_queries, n,
@@ -1004,10 +1025,9 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
         bound.row_err = index->row_err.get();
         bound.query_err = ws->query_err.get();
         if (median) {
-            // binary32 |diff| and midpoint roundings; the binary64 ones
             bound.mode = uha::BoundMode::median;
-            bound.rel = std::ldexp(6.0f, -24);
-            bound.abs = std::ldexp(1.0f, -126);
+            bound.rel = median_rel;
+            bound.abs = median_abs;
         } else {
             bound.mode = uha::BoundMode::projected_l2;
             const double n64 = static_cast<double>(index->scan_dim) + 3;

@@ -200,26 +200,12 @@ __device__ float warp_select(const float (&v)[PER_LANE], int count_valid,
     return __uint_as_float(prefix);
 }
 
-// One warp per (query, row): |r_j - y_j| for j < p held in registers
-// (PER_LANE * 32 >= p), median by two warp selections for even p.
+// |r_j - y_j| for j < p into the lane's registers (lane + 32 i); +inf for a
+// binary32 overflow, 0 past p.
 template <int PER_LANE>
-__global__ void __launch_bounds__(kThreads)
-    median_scan_kernel(const float* __restrict__ rows, uint32_t row_count,
-                       uint32_t padded_p, uint32_t p,
-                       const float* __restrict__ queries, uint32_t batch,
-                       float* __restrict__ partials)
+__device__ __forceinline__ int load_abs_diffs(const float* r, const float* y, uint32_t p,
+                                              int lane, float (&v)[PER_LANE])
 {
-    const uint64_t warp_id =
-        (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) / 32;
-    const int lane = threadIdx.x % 32;
-    if (warp_id >= static_cast<uint64_t>(row_count) * batch) {
-        return;
-    }
-    const uint32_t q = static_cast<uint32_t>(warp_id / row_count);
-    const uint32_t row = static_cast<uint32_t>(warp_id - uint64_t(q) * row_count);
-    const float* r = rows + static_cast<uint64_t>(row) * padded_p;
-    const float* y = queries + static_cast<uint64_t>(q) * padded_p;
-    float v[PER_LANE];
     int valid = 0;
 #pragma unroll
     for (int i = 0; i < PER_LANE; ++i) {
@@ -234,13 +220,123 @@ __global__ void __launch_bounds__(kThreads)
             valid = i + 1;
         }
     }
+    return valid;
+}
+
+// Binary32 median of the warp's p values: the (p/2)-th smallest, and for
+// even p the midpoint with the (p/2 - 1)-th, which is the upper middle itself
+// when it occurs twice there, else the largest value below it.
+template <int PER_LANE>
+__device__ __forceinline__ float warp_median(const float (&v)[PER_LANE], int valid,
+                                             uint32_t p)
+{
     const uint32_t mid = p / 2;
     const float upper = warp_select<PER_LANE>(v, valid, mid);
-    float median = upper;
-    if (p % 2 == 0) {
-        const float lower = warp_select<PER_LANE>(v, valid, mid - 1);
-        median = lower + (upper - lower) * 0.5f;
+    if (p % 2 != 0) {
+        return upper;
     }
+    const uint32_t ub = __float_as_uint(upper);
+    uint32_t below = 0;
+    uint32_t largest_below = 0;
+#pragma unroll
+    for (int i = 0; i < PER_LANE; ++i) {
+        const uint32_t b = __float_as_uint(v[i]);
+        if (i < valid && b < ub) {
+            ++below;
+            largest_below = b > largest_below ? b : largest_below;
+        }
+    }
+    below = __reduce_add_sync(0xffffffffu, below);
+    largest_below = __reduce_max_sync(0xffffffffu, largest_below);
+    const float lower = below < mid ? upper : __uint_as_float(largest_below);
+    return lower + (upper - lower) * 0.5f;
+}
+
+// Stage 1 of the median scan: exact binary32 medians of `samples` rows spread
+// over the index (row s * rows / samples) for every query; their minimum per
+// query goes to min_bits[q] (binary32 bits; nonnegative values order like
+// them; the slots hold 0xffffffff before the launch).
+template <int PER_LANE>
+__global__ void __launch_bounds__(kThreads)
+    median_sample_kernel(const float* __restrict__ rows, uint32_t row_count,
+                         uint32_t padded_p, uint32_t p, const float* __restrict__ queries,
+                         uint32_t batch, uint32_t samples, float* __restrict__ partials,
+                         unsigned int* __restrict__ min_bits)
+{
+    const uint64_t warp_id =
+        (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) / 32;
+    const int lane = threadIdx.x % 32;
+    if (warp_id >= static_cast<uint64_t>(samples) * batch) {
+        return;
+    }
+    const uint32_t q = static_cast<uint32_t>(warp_id / samples);
+    const uint32_t s = static_cast<uint32_t>(warp_id - uint64_t(q) * samples);
+    const uint32_t row = static_cast<uint32_t>(uint64_t(s) * row_count / samples);
+    float v[PER_LANE];
+    const int valid = load_abs_diffs<PER_LANE>(rows + uint64_t(row) * padded_p,
+                                               queries + uint64_t(q) * padded_p, p, lane, v);
+    const float median = warp_median<PER_LANE>(v, valid, p);
+    if (lane == 0) {
+        partials[static_cast<uint64_t>(q) * row_count + row] = median;
+        atomicMin(min_bits + q, __float_as_uint(median));
+    }
+}
+
+// Stage 2, one warp per (query, row). With U the sampled minimum, E the
+// largest row error plus the query's error and (rel, abs) the median bound,
+//   T = (U (1 + rel) + 2 E + 2 abs) / (1 - rel)   (rounded up)
+// exceeds every upper bound the sampled rows give, so a row whose binary32
+// median is above T has a lower bound above the query's smallest upper bound
+// and cannot be the argmin. One count decides it: fewer than p/2 + 1 values
+// <= T (odd p), fewer than p/2 (even p: the lower middle is above T). Such a
+// row stores -T (a negative distance: "at least T, no upper bound"); every
+// other row stores its binary32 median.
+template <int PER_LANE>
+__global__ void __launch_bounds__(kThreads)
+    median_scan_kernel(const float* __restrict__ rows, uint32_t row_count,
+                       uint32_t padded_p, uint32_t p,
+                       const float* __restrict__ queries, uint32_t batch,
+                       const unsigned int* __restrict__ min_bits,
+                       const float* __restrict__ query_err, float row_err_max,
+                       float rel, float abs_err, float* __restrict__ partials)
+{
+    const uint64_t warp_id =
+        (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) / 32;
+    const int lane = threadIdx.x % 32;
+    if (warp_id >= static_cast<uint64_t>(row_count) * batch) {
+        return;
+    }
+    const uint32_t q = static_cast<uint32_t>(warp_id / row_count);
+    const uint32_t row = static_cast<uint32_t>(warp_id - uint64_t(q) * row_count);
+    float v[PER_LANE];
+    const int valid = load_abs_diffs<PER_LANE>(rows + uint64_t(row) * padded_p,
+                                               queries + uint64_t(q) * padded_p, p, lane, v);
+    const float u = __uint_as_float(min_bits[q]);
+    float t = __int_as_float(0x7f800000);
+    if (u <= FLT_MAX) {
+        const float e = __fadd_ru(row_err_max, query_err[q]);
+        const float num = __fadd_ru(__fadd_ru(__fmul_ru(u, __fadd_ru(1.f, rel)),
+                                              __fmul_ru(2.f, e)),
+                                    __fmul_ru(2.f, abs_err));
+        t = __fmul_ru(__fdiv_ru(num, __fsub_rd(1.f, rel)), 1.0000005f);
+    }
+    if (t <= FLT_MAX) {
+        const uint32_t tb = __float_as_uint(t);
+        uint32_t at_most = 0;
+#pragma unroll
+        for (int i = 0; i < PER_LANE; ++i) {
+            at_most += (i < valid && __float_as_uint(v[i]) <= tb) ? 1u : 0u;
+        }
+        at_most = __reduce_add_sync(0xffffffffu, at_most);
+        const uint32_t needed = p % 2 != 0 ? p / 2 + 1 : p / 2;
+        if (at_most < needed) {
+            if (lane == 0) {
+                partials[static_cast<uint64_t>(q) * row_count + row] = -t;
+            }
+            return;
+        }
+    }
+    const float median = warp_median<PER_LANE>(v, valid, p);
     if (lane == 0) {
         partials[static_cast<uint64_t>(q) * row_count + row] = median;
     }
@@ -295,28 +391,63 @@ void launch_project_queries(const float* gathered, uint64_t batch,
     check_cuda(cudaGetLastError(), "cannot launch projection error kernel");
 }
 
-void launch_median_scan(const float* rows, uint64_t row_count,
-                        uint64_t padded_p, uint64_t p, const float* queries,
-                        uint64_t batch, float* partials, cudaStream_t stream)
+namespace {
+
+uint32_t median_samples(uint64_t row_count)
 {
-    const uint64_t threads = row_count * batch * 32;
-    const uint32_t blocks = static_cast<uint32_t>((threads + kThreads - 1) / kThreads);
+    return static_cast<uint32_t>(row_count < 32 ? row_count : 32);
+}
+
+template <int PER_LANE>
+void launch_median_pair(const float* rows, uint32_t rc, uint32_t pp, uint32_t pv,
+                        const float* queries, uint32_t b, const float* query_err,
+                        float row_err_max, float rel, float abs_err,
+                        unsigned int* min_bits, float* partials, cudaStream_t stream)
+{
+    const uint32_t samples = median_samples(rc);
+    const uint64_t sample_threads = static_cast<uint64_t>(samples) * b * 32;
+    median_sample_kernel<PER_LANE>
+        <<<static_cast<uint32_t>((sample_threads + kThreads - 1) / kThreads), kThreads, 0,
+           stream>>>(rows, rc, pp, pv, queries, b, samples, partials, min_bits);
+    const uint64_t threads = static_cast<uint64_t>(rc) * b * 32;
+    median_scan_kernel<PER_LANE>
+        <<<static_cast<uint32_t>((threads + kThreads - 1) / kThreads), kThreads, 0, stream>>>(
+            rows, rc, pp, pv, queries, b, min_bits, query_err, row_err_max, rel, abs_err,
+            partials);
+}
+
+}  // namespace
+
+void launch_median_scan(const float* rows, uint64_t row_count, uint64_t padded_p,
+                        uint64_t p, const float* queries, uint64_t batch,
+                        const float* query_err, float row_err_max, float rel,
+                        float abs_err, unsigned int* min_bits, float* partials,
+                        cudaStream_t stream)
+{
     const uint32_t rc = static_cast<uint32_t>(row_count);
     const uint32_t pp = static_cast<uint32_t>(padded_p);
     const uint32_t pv = static_cast<uint32_t>(p);
     const uint32_t b = static_cast<uint32_t>(batch);
+    check_cuda(cudaMemsetAsync(min_bits, 0xff, batch * sizeof(unsigned int), stream),
+               "cannot clear median thresholds");
     if (p <= 32) {
-        median_scan_kernel<1><<<blocks, kThreads, 0, stream>>>(rows, rc, pp, pv, queries, b, partials);
+        launch_median_pair<1>(rows, rc, pp, pv, queries, b, query_err, row_err_max, rel,
+                              abs_err, min_bits, partials, stream);
     } else if (p <= 64) {
-        median_scan_kernel<2><<<blocks, kThreads, 0, stream>>>(rows, rc, pp, pv, queries, b, partials);
+        launch_median_pair<2>(rows, rc, pp, pv, queries, b, query_err, row_err_max, rel,
+                              abs_err, min_bits, partials, stream);
     } else if (p <= 128) {
-        median_scan_kernel<4><<<blocks, kThreads, 0, stream>>>(rows, rc, pp, pv, queries, b, partials);
+        launch_median_pair<4>(rows, rc, pp, pv, queries, b, query_err, row_err_max, rel,
+                              abs_err, min_bits, partials, stream);
     } else if (p <= 256) {
-        median_scan_kernel<8><<<blocks, kThreads, 0, stream>>>(rows, rc, pp, pv, queries, b, partials);
+        launch_median_pair<8>(rows, rc, pp, pv, queries, b, query_err, row_err_max, rel,
+                              abs_err, min_bits, partials, stream);
     } else if (p <= 512) {
-        median_scan_kernel<16><<<blocks, kThreads, 0, stream>>>(rows, rc, pp, pv, queries, b, partials);
+        launch_median_pair<16>(rows, rc, pp, pv, queries, b, query_err, row_err_max, rel,
+                               abs_err, min_bits, partials, stream);
     } else if (p <= 1024) {
-        median_scan_kernel<32><<<blocks, kThreads, 0, stream>>>(rows, rc, pp, pv, queries, b, partials);
+        launch_median_pair<32>(rows, rc, pp, pv, queries, b, query_err, row_err_max, rel,
+                               abs_err, min_bits, partials, stream);
     } else {
         fail(UHA_LENGTH_ERROR,
              "the L1 hierarchy supports projection dimensions up to 1024");

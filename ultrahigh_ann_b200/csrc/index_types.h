@@ -62,6 +62,7 @@ struct uha_index {
     uha::DeviceBuffer<double> projection64; // p x sample_size
     uha::DeviceBuffer<float> projection32;  // p x padded_sample
     uha::DeviceBuffer<float> row_err;       // rows
+    float row_err_max = 0.f;                // largest row_err
     uha_space_usage usage{};
     // precision strategies: built on first use (index_bf16 / index_fp8)
     mutable std::mutex lowp_mutex;
@@ -103,6 +104,7 @@ struct uha_workspace {
     uha::DeviceBuffer<uint32_t> candidates;       // [batch][candidates_per_query]
     uha::DeviceBuffer<double> cand_dist;          // [batch][candidates_per_query]
     uha::DeviceBuffer<uint32_t> rescore_done;     // per query, zero between calls
+    uha::DeviceBuffer<unsigned int> median_min;   // L1 hierarchy: sampled minimum per query
     uint32_t candidates_per_query = 32;
     std::vector<TunedPlan> tuned;  // autotuned shapes (uha_workspace_autotune)
 

@@ -227,10 +227,16 @@ void launch_project_queries(const float* gathered, uint64_t batch,
                             double err_per_abs, bool euclidean,
                             int* error_flag, cudaStream_t stream);
 // Median of |rows[row][j] - queries[q][j]| over j < p per (query, row),
-// written as one chunk of partials.
-void launch_median_scan(const float* rows, uint64_t row_count,
-                        uint64_t padded_p, uint64_t p, const float* queries,
-                        uint64_t batch, float* partials, cudaStream_t stream);
+// written as one chunk of partials. Rows that provably cannot be a query's
+// argmin (their median is above a threshold derived from the exact medians of
+// 32 spread rows and the median bound: relative `rel`, absolute `abs_err`,
+// row errors up to row_err_max, query_err[q]) store minus that threshold:
+// a lower bound with no upper bound. min_bits: one word per query.
+void launch_median_scan(const float* rows, uint64_t row_count, uint64_t padded_p,
+                        uint64_t p, const float* queries, uint64_t batch,
+                        const float* query_err, float row_err_max, float rel,
+                        float abs_err, unsigned int* min_bits, float* partials,
+                        cudaStream_t stream);
 
 // ---- build-time helpers
 void launch_gather_rows(const float* source, uint64_t row_count, uint64_t dim,
