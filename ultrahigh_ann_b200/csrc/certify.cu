@@ -383,14 +383,15 @@ __device__ double replay_candidate(const ReplayInputs& in, const float* qrow,
 __global__ void __launch_bounds__(kFinalizeThreads)
     argmin_kernel(PartialView view, Bound bound, ReplayInputs in, Result* results,
                   double* exact_distances, Summary* block_summaries,
-                  uint32_t* done, uint32_t* replay_count)
+                  uint32_t* done, uint32_t* replay_count, uint32_t span)
 {
     const uint32_t q = blockIdx.y;
     const uint32_t blocks = gridDim.x;
     const float inf = __int_as_float(0x7f800000);
     Summary s{inf, inf, inf, 0xffffffffu, inf};
-    const uint32_t row = blockIdx.x * kFinalizeThreads + threadIdx.x;
-    if (row < view.rows) {
+    const uint32_t first_row = blockIdx.x * span;
+    const uint32_t end_row = min(view.rows, first_row + span);
+    for (uint32_t row = first_row + threadIdx.x; row < end_row; row += kFinalizeThreads) {
         const float d = row_distance(view, q, row);
         const Bounds2 b = bound_of(d, bound, row, q);
         summary_insert(s, b.lower, b.upper, row, d);
@@ -496,9 +497,21 @@ __global__ void __launch_bounds__(kFinalizeThreads)
 // replayed). One CTA per query: the binary64 projected query, then one warp
 // replays the selected row.
 __global__ void __launch_bounds__(kFinalizeThreads)
-    refine_kernel(ReplayInputs in, const Result* results, double* exact_distances)
+    refine_kernel(ReplayInputs in, Bound bound, const Result* results,
+                  double* exact_distances)
 {
     const uint32_t q = blockIdx.x;
+    // replayed by the argmin already, or the certified interval is within the
+    // 1e-5 relative tolerance: the binary32 distance stands
+    const double known = exact_distances[q];
+    if (known == known) {
+        return;
+    }
+    const Result res = results[q];
+    const Bounds2 b = bound_of(res.distance, bound, res.row, q);
+    if (__fsub_ru(b.upper, b.lower) <= __fmul_rd(0.999e-5f, b.lower)) {
+        return;
+    }
     extern __shared__ double projected_query[];
     const float* qrow = in.queries + static_cast<uint64_t>(q) * in.padded_dim;
     project_query64(in, qrow, projected_query);
@@ -745,13 +758,13 @@ FinalizeScratch finalize_scratch(void* base, uint32_t capacity, uint32_t rows)
 
 }  // namespace
 
-void launch_refine_winners(ReplayInputs in, const Result* results,
+void launch_refine_winners(ReplayInputs in, Bound bound, const Result* results,
                            uint32_t batch, double* exact_distances,
                            cudaStream_t stream)
 {
     const size_t smem = replay_smem(in);
     set_dynamic_smem(reinterpret_cast<const void*>(refine_kernel), smem);
-    refine_kernel<<<batch, kFinalizeThreads, smem, stream>>>(in, results,
+    refine_kernel<<<batch, kFinalizeThreads, smem, stream>>>(in, bound, results,
                                                              exact_distances);
     check_cuda(cudaGetLastError(), "cannot launch refine kernel");
 }
@@ -766,14 +779,22 @@ void launch_argmin(PartialView view, Bound bound, ReplayInputs in,
                    Result* results, double* exact_distances, void* scratch,
                    uint64_t capacity, uint32_t* replay_count, cudaStream_t stream)
 {
-    const uint32_t blocks = (view.rows + kFinalizeThreads - 1) / kFinalizeThreads;
+    // Rows per CTA: one block of kFinalizeThreads rows, or several when the
+    // grid would exceed about 32 CTAs per SM (the scratch layout stays that of
+    // one block per kFinalizeThreads rows, so the counters keep their place).
+    const uint32_t min_span_blocks = (view.rows + kFinalizeThreads - 1) / kFinalizeThreads;
+    const uint64_t cap = 148ull * 32;
+    const uint64_t want = static_cast<uint64_t>(min_span_blocks) * view.batch;
+    const uint32_t factor = want > cap ? static_cast<uint32_t>((want + cap - 1) / cap) : 1u;
+    const uint32_t span = kFinalizeThreads * factor;
+    const uint32_t blocks = (view.rows + span - 1) / span;
     FinalizeScratch fs = finalize_scratch(scratch, static_cast<uint32_t>(capacity),
                                           view.rows);
     const size_t smem = replay_smem(in);
     set_dynamic_smem(reinterpret_cast<const void*>(argmin_kernel), smem);
     argmin_kernel<<<dim3(blocks, view.batch), kFinalizeThreads, smem, stream>>>(
         view, bound, in, results, exact_distances, fs.summaries, fs.done,
-        replay_count);
+        replay_count, span);
     check_cuda(cudaGetLastError(), "cannot launch argmin kernel");
 }
 

@@ -1053,7 +1053,8 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
     if (hierarchical && c.want_distances) {
         // reported distances of a hierarchy: the reference's binary64 value of
         // each selected row
-        uha::launch_refine_winners(in, results, static_cast<uint32_t>(n), exact, stream);
+        uha::launch_refine_winners(in, bound, results, static_cast<uint32_t>(n), exact,
+                                   stream);
         ++launches;
     }
     return launches;

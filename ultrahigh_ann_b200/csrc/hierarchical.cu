@@ -16,6 +16,7 @@
 #include "common.h"
 #include "kernels.h"
 
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 
@@ -263,22 +264,23 @@ __global__ void __launch_bounds__(kThreads)
                          uint32_t batch, uint32_t samples, float* __restrict__ partials,
                          unsigned int* __restrict__ min_bits)
 {
-    const uint64_t warp_id =
-        (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) / 32;
     const int lane = threadIdx.x % 32;
-    if (warp_id >= static_cast<uint64_t>(samples) * batch) {
-        return;
-    }
-    const uint32_t q = static_cast<uint32_t>(warp_id / samples);
-    const uint32_t s = static_cast<uint32_t>(warp_id - uint64_t(q) * samples);
-    const uint32_t row = static_cast<uint32_t>(uint64_t(s) * row_count / samples);
-    float v[PER_LANE];
-    const int valid = load_abs_diffs<PER_LANE>(rows + uint64_t(row) * padded_p,
-                                               queries + uint64_t(q) * padded_p, p, lane, v);
-    const float median = warp_median<PER_LANE>(v, valid, p);
-    if (lane == 0) {
-        partials[static_cast<uint64_t>(q) * row_count + row] = median;
-        atomicMin(min_bits + q, __float_as_uint(median));
+    const uint64_t total = static_cast<uint64_t>(samples) * batch;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * (blockDim.x / 32);
+    for (uint64_t w = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) / 32;
+         w < total; w += stride) {
+        const uint32_t q = static_cast<uint32_t>(w / samples);
+        const uint32_t s = static_cast<uint32_t>(w - uint64_t(q) * samples);
+        const uint32_t row = static_cast<uint32_t>(uint64_t(s) * row_count / samples);
+        float v[PER_LANE];
+        const int valid = load_abs_diffs<PER_LANE>(rows + uint64_t(row) * padded_p,
+                                                   queries + uint64_t(q) * padded_p, p, lane,
+                                                   v);
+        const float median = warp_median<PER_LANE>(v, valid, p);
+        if (lane == 0) {
+            partials[static_cast<uint64_t>(q) * row_count + row] = median;
+            atomicMin(min_bits + q, __float_as_uint(median));
+        }
     }
 }
 
@@ -300,45 +302,52 @@ __global__ void __launch_bounds__(kThreads)
                        const float* __restrict__ query_err, float row_err_max,
                        float rel, float abs_err, float* __restrict__ partials)
 {
-    const uint64_t warp_id =
-        (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) / 32;
     const int lane = threadIdx.x % 32;
-    if (warp_id >= static_cast<uint64_t>(row_count) * batch) {
-        return;
-    }
-    const uint32_t q = static_cast<uint32_t>(warp_id / row_count);
-    const uint32_t row = static_cast<uint32_t>(warp_id - uint64_t(q) * row_count);
-    float v[PER_LANE];
-    const int valid = load_abs_diffs<PER_LANE>(rows + uint64_t(row) * padded_p,
-                                               queries + uint64_t(q) * padded_p, p, lane, v);
-    const float u = __uint_as_float(min_bits[q]);
-    float t = __int_as_float(0x7f800000);
-    if (u <= FLT_MAX) {
-        const float e = __fadd_ru(row_err_max, query_err[q]);
-        const float num = __fadd_ru(__fadd_ru(__fmul_ru(u, __fadd_ru(1.f, rel)),
-                                              __fmul_ru(2.f, e)),
-                                    __fmul_ru(2.f, abs_err));
-        t = __fmul_ru(__fdiv_ru(num, __fsub_rd(1.f, rel)), 1.0000005f);
-    }
-    if (t <= FLT_MAX) {
-        const uint32_t tb = __float_as_uint(t);
-        uint32_t at_most = 0;
-#pragma unroll
-        for (int i = 0; i < PER_LANE; ++i) {
-            at_most += (i < valid && __float_as_uint(v[i]) <= tb) ? 1u : 0u;
-        }
-        at_most = __reduce_add_sync(0xffffffffu, at_most);
-        const uint32_t needed = p % 2 != 0 ? p / 2 + 1 : p / 2;
-        if (at_most < needed) {
-            if (lane == 0) {
-                partials[static_cast<uint64_t>(q) * row_count + row] = -t;
+    const uint64_t total = static_cast<uint64_t>(row_count) * batch;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * (blockDim.x / 32);
+    const uint32_t needed = p % 2 != 0 ? p / 2 + 1 : p / 2;
+    uint32_t cached_q = 0xffffffffu;
+    float t = 0.f;
+    for (uint64_t w = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) / 32;
+         w < total; w += stride) {
+        const uint32_t q = static_cast<uint32_t>(w / row_count);
+        const uint32_t row = static_cast<uint32_t>(w - uint64_t(q) * row_count);
+        if (q != cached_q) {
+            cached_q = q;
+            const float u = __uint_as_float(min_bits[q]);
+            t = __int_as_float(0x7f800000);
+            if (u <= FLT_MAX) {
+                const float e = __fadd_ru(row_err_max, query_err[q]);
+                const float num = __fadd_ru(__fadd_ru(__fmul_ru(u, __fadd_ru(1.f, rel)),
+                                                      __fmul_ru(2.f, e)),
+                                            __fmul_ru(2.f, abs_err));
+                t = __fmul_ru(__fdiv_ru(num, __fsub_rd(1.f, rel)), 1.0000005f);
             }
-            return;
         }
-    }
-    const float median = warp_median<PER_LANE>(v, valid, p);
-    if (lane == 0) {
-        partials[static_cast<uint64_t>(q) * row_count + row] = median;
+        float v[PER_LANE];
+        const int valid = load_abs_diffs<PER_LANE>(rows + uint64_t(row) * padded_p,
+                                                   queries + uint64_t(q) * padded_p, p, lane,
+                                                   v);
+        float* out = partials + static_cast<uint64_t>(q) * row_count + row;
+        if (t <= FLT_MAX) {
+            const uint32_t tb = __float_as_uint(t);
+            uint32_t at_most = 0;
+#pragma unroll
+            for (int i = 0; i < PER_LANE; ++i) {
+                at_most += (i < valid && __float_as_uint(v[i]) <= tb) ? 1u : 0u;
+            }
+            at_most = __reduce_add_sync(0xffffffffu, at_most);
+            if (at_most < needed) {
+                if (lane == 0) {
+                    *out = -t;
+                }
+                continue;
+            }
+        }
+        const float median = warp_median<PER_LANE>(v, valid, p);
+        if (lane == 0) {
+            *out = median;
+        }
     }
 }
 
@@ -404,14 +413,17 @@ void launch_median_pair(const float* rows, uint32_t rc, uint32_t pp, uint32_t pv
                         float row_err_max, float rel, float abs_err,
                         unsigned int* min_bits, float* partials, cudaStream_t stream)
 {
+    // grid-stride warps over the pairs: at most 16 resident CTAs' worth per SM
+    const uint64_t cap = 148ull * 16;
     const uint32_t samples = median_samples(rc);
-    const uint64_t sample_threads = static_cast<uint64_t>(samples) * b * 32;
+    const uint64_t sample_blocks =
+        (static_cast<uint64_t>(samples) * b * 32 + kThreads - 1) / kThreads;
     median_sample_kernel<PER_LANE>
-        <<<static_cast<uint32_t>((sample_threads + kThreads - 1) / kThreads), kThreads, 0,
-           stream>>>(rows, rc, pp, pv, queries, b, samples, partials, min_bits);
-    const uint64_t threads = static_cast<uint64_t>(rc) * b * 32;
+        <<<static_cast<uint32_t>(std::min(sample_blocks, cap)), kThreads, 0, stream>>>(
+            rows, rc, pp, pv, queries, b, samples, partials, min_bits);
+    const uint64_t blocks = (static_cast<uint64_t>(rc) * b * 32 + kThreads - 1) / kThreads;
     median_scan_kernel<PER_LANE>
-        <<<static_cast<uint32_t>((threads + kThreads - 1) / kThreads), kThreads, 0, stream>>>(
+        <<<static_cast<uint32_t>(std::min(blocks, cap)), kThreads, 0, stream>>>(
             rows, rc, pp, pv, queries, b, min_bits, query_err, row_err_max, rel, abs_err,
             partials);
 }

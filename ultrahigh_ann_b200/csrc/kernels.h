@@ -132,9 +132,10 @@ void launch_finalize_gemm(PartialView view, const float* row_norms,
                           const float* query_norms, Result* results,
                           cudaStream_t stream);
 
-// Reference binary64 distance of every query's selected row (projected
-// replay ops only).
-void launch_refine_winners(ReplayInputs in, const Result* results,
+// Reference binary64 distance of each query's selected row (projected replay
+// ops only), for the queries that the argmin did not replay and whose
+// certified interval is wider than 1e-5 relative.
+void launch_refine_winners(ReplayInputs in, Bound bound, const Result* results,
                            uint32_t batch, double* exact_distances,
                            cudaStream_t stream);
 
