@@ -51,7 +51,8 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--precision-only", action="store_true",
                    help="only the precision-strategy table (one JSON line)")
-    p.add_argument("--only", default="", choices=["", "precision", "batched", "serving"],
+    p.add_argument("--only", default="",
+                   choices=["", "precision", "batched", "serving", "centroids"],
                    help="only this section of the bench (one JSON line)")
     p.add_argument("--precision-batch", type=int, default=0,
                    help="with --precision-only: one batch size (2048 queries)")
@@ -266,6 +267,7 @@ def run_engine(args):
         del qdev
         torch.cuda.empty_cache()
         line["suite"] = suite(ds, index)
+        line["centroids_flat"] = centroids_flat()
         line["precision"] = precision(ds, index)
         torch.cuda.empty_cache()
         line["batched"] = batched(ds)
@@ -425,6 +427,61 @@ def precision(ds, exact_index, batches=((1, 256), (64, 2048), (1024, 2048))):
     return out
 
 
+def centroids_flat(queries=3013):
+    """The reference's own CPU-runnable case: 33 class centroids, d = 60,660,
+    flat L2 importance-sampling index with T = 8 and seed 0 (probabilities by
+    the reference CPU policy's arithmetic), 3,013 queries answered one at a
+    time. Reported in microseconds per query and kernels per query (the index
+    is 33 x |I| floats: launch-latency bound, not a %HBM case), with the
+    answers checked against the reference's own CPU flat index (oracle/_ref)
+    and the agreement with the binary64 exact argmin."""
+    import torch
+
+    import ultrahigh_ann_b200 as uha
+    from oracle import oracle as O
+    from ultrahigh_ann_b200 import synthetic
+
+    ds = synthetic.centroid_dataset(classes=33, queries=queries, seed=0)
+    probs = uha.compute_importance_probabilities_host("l2", ds.rows)
+    index = uha.CudaSampledCoordinateL2AnnIndex(ds.rows, probs, 8, uha.MT19937_64(0))
+    s = index.coordinate_sample
+    ws = index.make_query_workspace(1)
+    ws.set_timing(True)
+    qdev = torch.from_numpy(ds.queries).cuda()
+    out = np.zeros(queries, np.uint64)
+    index.query_many(qdev.data_ptr(), 64, 1, out[:64], ws, on_device=True)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    index.query_many(qdev.data_ptr(), queries, 1, out, ws, on_device=True)
+    dev_s = time.perf_counter() - t
+    launches = ws.last_stats()["kernel_launches"]
+    host = np.ascontiguousarray(ds.queries)
+    out_h = np.zeros(queries, np.uint64)
+    t = time.perf_counter()
+    index.query_many(host, queries, 1, out_h, ws)
+    e2e_s = time.perf_counter() - t
+    lat = []
+    for i in range(512):
+        t = time.perf_counter()
+        index.query(host[i], ws)
+        lat.append((time.perf_counter() - t) * 1e6)
+    entry = {"workload": "flat_l2_centroids_r33_d60660_T8_seed0", "queries": queries,
+             "k": len(s), "device_us_per_query": round(dev_s / queries * 1e6, 2),
+             "e2e_us_per_query": round(e2e_s / queries * 1e6, 2),
+             "single_call_us": {"p50": round(float(np.percentile(lat, 50)), 2),
+                                "p99": round(float(np.percentile(lat, 99)), 2)},
+             "kernels_per_query": round(launches / queries, 2),
+             "answers_equal_host_api": bool(np.array_equal(out, out_h))}
+    exact = uha.CudaExactL2Index(ds.rows)
+    ex = exact.query_many(host, queries, 1024, None, exact.make_query_workspace(1024))
+    entry["agreement_vs_fp64_exact"] = round(float(np.mean(out == ex)), 4)
+    if O.ref_available():
+        ref = O.ref_sampled("l2", ds.rows, s.source_columns, s.multiplicities,
+                            s.inverse_probabilities, ds.queries)
+        entry["equal_to_reference_cpu_flat"] = round(float(np.mean(out == ref)), 4)
+    return entry
+
+
 _PROBS: dict = {}
 
 
@@ -548,7 +605,8 @@ def serving(ds, rates=(10_000, 100_000, 1_000_000), seconds=0.5, pool=2048):
                             queries_on_device=True)
         for (name, _, l2_exact_or_flat), ix in zip(build, indexes):
             st = S.gemm_bf16_rerank if (mode == "bf16_rerank" and l2_exact_or_flat) else S.direct
-            server.add_index(ix, st)
+            sid = server.add_index(ix, st)
+            server.reserve(sid, 2)
         # warm-up load, then the measured rates
         n = 2000
         server.replay(rng.integers(0, 8, n), [base + int(j) * stride
@@ -650,9 +708,12 @@ def main():
 
 
 def run_section(args):
-    """One section (batched or serving) alone on one GPU."""
+    """One section (batched, serving or centroids) alone on one GPU."""
     from ultrahigh_ann_b200 import synthetic
 
+    if args.only == "centroids":
+        print(json.dumps({"centroids_flat": centroids_flat()}), flush=True)
+        return
     ds = synthetic.row_dataset(rows=ROWS, classes=33, queries=4096, d=DIM, seed=1,
                                query_stream=0)
     fn = batched if args.only == "batched" else serving

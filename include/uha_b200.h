@@ -413,6 +413,11 @@ uha_status uha_server_create(int device, const uha_server_config* config,
  * index must outlive the server. */
 uha_status uha_server_add_index(uha_server* server, const uha_index* index,
                                 uha_strategy strategy, uint32_t* out_id);
+/* Creates pooled workspaces of index `index_id` until it holds `count` (within
+ * the budget; *held receives how many it holds), so that a later burst does
+ * not wait for workspace creation. */
+uha_status uha_server_reserve(uha_server* server, uint32_t index_id, uint32_t count,
+                              uint32_t* held);
 /* Queues one query (dimension floats at `query`, host or device per the
  * config; the memory must stay valid until its result is polled).
  * Thread-safe. */

@@ -79,6 +79,7 @@ def test_same_result_alone_and_in_the_mix(on_device):
                         queries_on_device=on_device)
     sid = [server.add_index(ix, st) for ix, st in pairs]
     assert sid == list(range(len(pairs)))
+    assert server.reserve(0, 2) == 2
     alone = _alone(server, ids, handles)
     assert np.all(alone["status"] == 0)
     server.reset_stats()

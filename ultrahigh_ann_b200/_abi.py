@@ -150,6 +150,8 @@ SIGNATURES = {
     "uha_batch_destroy": (None, [c_void_p]),
     "uha_server_create": (c_int, [c_int, POINTER(ServerConfig), _H]),
     "uha_server_add_index": (c_int, [c_void_p, c_void_p, c_int, POINTER(ctypes.c_uint32)]),
+    "uha_server_reserve": (c_int, [c_void_p, ctypes.c_uint32, ctypes.c_uint32,
+                                    POINTER(ctypes.c_uint32)]),
     "uha_server_submit": (c_int, [c_void_p, ctypes.c_uint32, c_void_p, c_uint64]),
     "uha_server_replay": (c_int, [c_void_p, c_uint64, c_void_p, c_void_p, c_void_p,
                                    c_void_p]),

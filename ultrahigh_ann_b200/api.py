@@ -886,6 +886,14 @@ class Server:
         self._indexes.append(index)
         return out.value
 
+    def reserve(self, index_id: int, count: int) -> int:
+        """Pre-creates pooled workspaces of an index (within the budget);
+        returns how many it holds."""
+        held = ctypes.c_uint32()
+        _check(_abi.load().uha_server_reserve(self._handle, ctypes.c_uint32(index_id),
+                                              ctypes.c_uint32(count), ctypes.byref(held)))
+        return held.value
+
     def _pointer(self, query) -> int:
         if self._on_device:
             return int(query)

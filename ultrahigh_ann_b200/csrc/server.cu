@@ -587,6 +587,34 @@ extern "C" uha_status uha_server_add_index(uha_server* server, const uha_index* 
     });
 }
 
+extern "C" uha_status uha_server_reserve(uha_server* server, uint32_t index_id,
+                                         uint32_t count, uint32_t* held)
+{
+    return guarded([&] {
+        require(server != nullptr, UHA_INVALID_ARGUMENT, "server must not be null");
+        DeviceGuard guard(server->device);
+        std::lock_guard<std::mutex> lock(server->mu);
+        require(index_id < server->entries.size(), UHA_INVALID_ARGUMENT,
+                "unknown server index");
+        uha_server::Entry& e = *server->entries[index_id];
+        uint32_t have = 0;
+        for (const auto& p : server->pool) {
+            have += p->index_id == index_id ? 1u : 0u;
+        }
+        while (have < count && server->pool_bytes + e.ws_bytes <= server->cfg.hbm_budget_bytes) {
+            std::unique_ptr<uha_server::Pooled> fresh = server->make_pooled(index_id);
+            server->pool_bytes += fresh->bytes;
+            server->peak_pool_bytes = std::max(server->peak_pool_bytes, server->pool_bytes);
+            e.idle.push_back(fresh.get());
+            server->pool.push_back(std::move(fresh));
+            ++have;
+        }
+        if (held != nullptr) {
+            *held = have;
+        }
+    });
+}
+
 namespace {
 
 void push_request(uha_server* server, uint32_t index_id, const float* query, uint64_t tag,
