@@ -479,6 +479,42 @@ uha_status uha_importance_probabilities_host(uha_metric metric,
                                              uint64_t dimension, int threads,
                                              double* out_probabilities);
 
+/* ------------------------------------------------------------ data files */
+
+/* SHA-256 (FIPS 180-4) of a buffer or of a file's bytes, 32 bytes out.
+ * Replaces ultrahigh_ann::io::sha256_file (include/ultrahigh_ann/io/
+ * sha256.hpp:14). */
+uha_status uha_sha256(const void* data, uint64_t size, uint8_t* out);
+uha_status uha_sha256_file(const char* path, uint8_t* out);
+
+/* Versioned importance-probability file ("UHANNPR2", kind, representative
+ * count, SHA-256 of the representative-matrix file, binary64 probabilities),
+ * bound to the matrix it was computed from. Replaces
+ * save_importance_probabilities / load_importance_probabilities
+ * (include/ultrahigh_ann/io/importance_probability_io.hpp:27-35); malformed
+ * files fail with UHA_RUNTIME_ERROR and the reference's messages. load: with
+ * probabilities NULL only the header fields and *count are returned;
+ * otherwise capacity must hold *count values (UHA_LENGTH_ERROR). */
+uha_status uha_probabilities_save(const char* path, uha_metric kind,
+                                  uint64_t representative_count,
+                                  const uint8_t* representatives_sha256,
+                                  const double* probabilities, uint64_t count);
+uha_status uha_probabilities_load(const char* path, uha_metric* kind,
+                                  uint64_t* representative_count,
+                                  uint8_t* representatives_sha256,
+                                  double* probabilities, uint64_t capacity,
+                                  uint64_t* count);
+
+/* Little-endian NPY files of the transformed datasets: a two-dimensional
+ * C-order float32 matrix (finite values) and a one-dimensional uint16 label
+ * vector. Replace load_float_matrix_npy / load_label_vector_npy
+ * (include/ultrahigh_ann/datasets/representative_query_dataset.hpp:19-25);
+ * with out NULL only the shape is returned. */
+uha_status uha_npy_load_f32(const char* path, float* out, uint64_t capacity,
+                            uint64_t* rows, uint64_t* cols);
+uha_status uha_npy_load_u16(const char* path, uint64_t* out, uint64_t capacity,
+                            uint64_t* count);
+
 /* std::mt19937_64 engine shared by the host-side draws below, so that one
  * engine passes through sampling and projection in the reference order. */
 uha_status uha_rng_create(uint64_t seed, uha_rng** out);

@@ -118,6 +118,18 @@ def ref_lib() -> ctypes.CDLL:
         lib.ref_exact_destroy.argtypes = [c_void_p]
         lib.ref_exact_query.restype = c_int
         lib.ref_exact_query.argtypes = [c_void_p, c_void_p, c_uint64, c_int, c_void_p]
+        lib.ref_sha256_file.restype = c_int
+        lib.ref_sha256_file.argtypes = [c_char_p, c_void_p]
+        lib.ref_probabilities_save.restype = c_int
+        lib.ref_probabilities_save.argtypes = [c_char_p, c_int, c_uint64, c_void_p,
+                                               c_void_p, c_uint64]
+        lib.ref_probabilities_load.restype = c_int
+        lib.ref_probabilities_load.argtypes = [c_char_p, c_void_p, c_void_p, c_void_p,
+                                               c_void_p, c_uint64, c_void_p]
+        lib.ref_npy_f32.restype = c_int
+        lib.ref_npy_f32.argtypes = [c_char_p, c_void_p, c_uint64, c_void_p, c_void_p]
+        lib.ref_npy_u16.restype = c_int
+        lib.ref_npy_u16.argtypes = [c_char_p, c_void_p, c_uint64, c_void_p]
         _ref = lib
     return _ref
 
@@ -351,3 +363,53 @@ def ref_projection(metric: str, rows, cols, mult, invp, p: int, state: str | Non
                                         state.encode() if state else None, seed,
                                         _p(mat), _p(reps)))
     return mat, reps
+
+
+# ------------------------------------------------- reference data-file code
+
+def ref_sha256_file(path) -> bytes:
+    out = (ctypes.c_uint8 * 32)()
+    _ref_check(ref_lib().ref_sha256_file(str(path).encode(), out))
+    return bytes(out)
+
+
+def ref_probabilities_save(path, kind: int, reps: int, sha: bytes, probs) -> None:
+    """kind: 0 = L2, 1 = L1."""
+    p = np.ascontiguousarray(probs, np.float64)
+    d = (ctypes.c_uint8 * 32)(*sha)
+    _ref_check(ref_lib().ref_probabilities_save(str(path).encode(), kind, reps, d, _p(p),
+                                                p.size))
+
+
+def ref_probabilities_load(path):
+    kind = ctypes.c_int()
+    reps = ctypes.c_uint64()
+    n = ctypes.c_uint64()
+    d = (ctypes.c_uint8 * 32)()
+    _ref_check(ref_lib().ref_probabilities_load(str(path).encode(), ctypes.byref(kind),
+                                                ctypes.byref(reps), d, None, 0,
+                                                ctypes.byref(n)))
+    out = np.zeros(n.value, np.float64)
+    _ref_check(ref_lib().ref_probabilities_load(str(path).encode(), ctypes.byref(kind),
+                                                ctypes.byref(reps), d, _p(out), out.size,
+                                                ctypes.byref(n)))
+    return kind.value, reps.value, bytes(d), out
+
+
+def ref_npy_f32(path) -> np.ndarray:
+    r = ctypes.c_uint64()
+    c = ctypes.c_uint64()
+    _ref_check(ref_lib().ref_npy_f32(str(path).encode(), None, 0, ctypes.byref(r),
+                                     ctypes.byref(c)))
+    out = np.zeros((r.value, c.value), np.float32)
+    _ref_check(ref_lib().ref_npy_f32(str(path).encode(), _p(out), out.size, ctypes.byref(r),
+                                     ctypes.byref(c)))
+    return out
+
+
+def ref_npy_u16(path) -> np.ndarray:
+    n = ctypes.c_uint64()
+    _ref_check(ref_lib().ref_npy_u16(str(path).encode(), None, 0, ctypes.byref(n)))
+    out = np.zeros(n.value, np.uint64)
+    _ref_check(ref_lib().ref_npy_u16(str(path).encode(), _p(out), out.size, ctypes.byref(n)))
+    return out

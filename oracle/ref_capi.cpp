@@ -15,6 +15,9 @@
 #include "ultrahigh_ann/hnsvw25/l2/importance_sampling.hpp"
 #include "hnsvw25/l1/hierarchical/l1_hierarchical_projection.hpp"
 #include "hnsvw25/l2/hierarchical/l2_hierarchical_projection.hpp"
+#include "ultrahigh_ann/datasets/representative_query_dataset.hpp"
+#include "ultrahigh_ann/io/importance_probability_io.hpp"
+#include "ultrahigh_ann/io/sha256.hpp"
 
 #include <omp.h>
 
@@ -355,6 +358,82 @@ int ref_projection(int metric, const float* rows, uint64_t r, uint64_t d,
                       proj.cauchy_matrix.values().end(), matrix_out);
             std::copy(proj.projected_representatives.values().begin(),
                       proj.projected_representatives.values().end(), reps_out);
+        }
+    });
+}
+
+// ---- data files (src/io/*.cpp, src/datasets/representative_query_dataset.cpp)
+
+int ref_sha256_file(const char* path, uint8_t* out)
+{
+    return guarded([&] {
+        const auto d = ultrahigh_ann::io::sha256_file(path);
+        std::memcpy(out, d.data(), d.size());
+    });
+}
+
+// kind: 0 = L2, 1 = L1 (the engine's uha_metric values)
+int ref_probabilities_save(const char* path, int kind, uint64_t reps, const uint8_t* sha,
+                           const double* probs, uint64_t n)
+{
+    return guarded([&] {
+        ultrahigh_ann::io::Sha256Digest d{};
+        std::memcpy(d.data(), sha, d.size());
+        ultrahigh_ann::io::save_importance_probabilities(
+            path,
+            kind == 1 ? ultrahigh_ann::io::ImportanceProbabilityKind::l1
+                      : ultrahigh_ann::io::ImportanceProbabilityKind::l2,
+            reps, d, std::span<const double>(probs, n));
+    });
+}
+
+int ref_probabilities_load(const char* path, int* kind, uint64_t* reps, uint8_t* sha,
+                           double* probs, uint64_t capacity, uint64_t* n)
+{
+    return guarded([&] {
+        const auto f = ultrahigh_ann::io::load_importance_probabilities(path);
+        *kind = f.kind == ultrahigh_ann::io::ImportanceProbabilityKind::l1 ? 1 : 0;
+        *reps = f.representative_count;
+        std::memcpy(sha, f.representatives_sha256.data(), 32);
+        *n = f.probabilities.size();
+        if (probs != nullptr) {
+            if (capacity < f.probabilities.size()) {
+                throw std::length_error("capacity");
+            }
+            std::memcpy(probs, f.probabilities.data(), f.probabilities.size() * sizeof(double));
+        }
+    });
+}
+
+int ref_npy_f32(const char* path, float* out, uint64_t capacity, uint64_t* rows,
+                uint64_t* cols)
+{
+    return guarded([&] {
+        const DenseMatrix m = ultrahigh_ann::load_float_matrix_npy(path);
+        *rows = m.rows();
+        *cols = m.cols();
+        if (out != nullptr) {
+            if (capacity < m.rows() * m.cols()) {
+                throw std::length_error("capacity");
+            }
+            const auto v = m.values();
+            std::copy(v.begin(), v.end(), out);
+        }
+    });
+}
+
+int ref_npy_u16(const char* path, uint64_t* out, uint64_t capacity, uint64_t* count)
+{
+    return guarded([&] {
+        const auto v = ultrahigh_ann::load_label_vector_npy(path);
+        *count = v.size();
+        if (out != nullptr) {
+            if (capacity < v.size()) {
+                throw std::length_error("capacity");
+            }
+            for (size_t i = 0; i < v.size(); ++i) {
+                out[i] = v[i];
+            }
         }
     });
 }

@@ -167,6 +167,14 @@ SIGNATURES = {
                                               POINTER(ProbabilityReport)]),
     "uha_importance_probabilities_host": (c_int, [c_int, c_void_p, c_uint64, c_uint64,
                                                    c_int, c_void_p]),
+    "uha_sha256": (c_int, [c_void_p, c_uint64, c_void_p]),
+    "uha_sha256_file": (c_int, [c_char_p, c_void_p]),
+    "uha_probabilities_save": (c_int, [c_char_p, c_int, c_uint64, c_void_p, c_void_p,
+                                        c_uint64]),
+    "uha_probabilities_load": (c_int, [c_char_p, POINTER(c_int), _U, c_void_p, c_void_p,
+                                        c_uint64, _U]),
+    "uha_npy_load_f32": (c_int, [c_char_p, c_void_p, c_uint64, _U, _U]),
+    "uha_npy_load_u16": (c_int, [c_char_p, c_void_p, c_uint64, _U]),
     "uha_rng_create": (c_int, [c_uint64, _H]),
     "uha_rng_destroy": (None, [c_void_p]),
     "uha_rng_state": (c_int, [c_void_p, c_char_p, c_uint64, _U]),
