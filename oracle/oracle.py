@@ -80,6 +80,16 @@ def ref_available() -> bool:
     return REF_LIB.exists()
 
 
+def reference_dir():
+    """The reference source tree the _ref library was built from (recorded by
+    the Makefile), or None when it is not present on this machine."""
+    marker = REF_LIB.parent / "reference_dir"
+    if not marker.exists():
+        return None
+    d = Path(marker.read_text().strip())
+    return d if d.is_dir() else None
+
+
 def ref_lib() -> ctypes.CDLL:
     global _ref
     if _ref is None:
@@ -128,6 +138,8 @@ def ref_lib() -> ctypes.CDLL:
                                                c_void_p, c_uint64, c_void_p]
         lib.ref_npy_f32.restype = c_int
         lib.ref_npy_f32.argtypes = [c_char_p, c_void_p, c_uint64, c_void_p, c_void_p]
+        lib.ref_parse_setup.restype = c_int
+        lib.ref_parse_setup.argtypes = [c_char_p, c_void_p, c_uint64, c_void_p]
         lib.ref_npy_u16.restype = c_int
         lib.ref_npy_u16.argtypes = [c_char_p, c_void_p, c_uint64, c_void_p]
         _ref = lib
@@ -413,3 +425,14 @@ def ref_npy_u16(path) -> np.ndarray:
     out = np.zeros(n.value, np.uint64)
     _ref_check(ref_lib().ref_npy_u16(str(path).encode(), _p(out), out.size, ctypes.byref(n)))
     return out
+
+
+def ref_parse_setup(path) -> dict:
+    """The reference's load_benchmark_setup of a setup file, as a dict."""
+    import json
+    n = ctypes.c_uint64()
+    _ref_check(ref_lib().ref_parse_setup(str(path).encode(), None, 0, ctypes.byref(n)))
+    buf = ctypes.create_string_buffer(n.value + 1)
+    _ref_check(ref_lib().ref_parse_setup(str(path).encode(), buf, n.value + 1,
+                                         ctypes.byref(n)))
+    return json.loads(buf.value.decode())

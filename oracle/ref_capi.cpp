@@ -18,6 +18,7 @@
 #include "ultrahigh_ann/datasets/representative_query_dataset.hpp"
 #include "ultrahigh_ann/io/importance_probability_io.hpp"
 #include "ultrahigh_ann/io/sha256.hpp"
+#include "benchmarks/benchmark_setup.hpp"
 
 #include <omp.h>
 
@@ -434,6 +435,74 @@ int ref_npy_u16(const char* path, uint64_t* out, uint64_t capacity, uint64_t* co
             for (size_t i = 0; i < v.size(); ++i) {
                 out[i] = v[i];
             }
+        }
+    });
+}
+
+// ---- benchmark setup v2 (src/benchmarks/benchmark_setup.cpp): the parsed
+// setup as JSON text
+namespace {
+std::string json_str(const std::string& v)
+{
+    std::string o = "\"";
+    for (char c : v) {
+        if (c == '"' || c == '\\') {
+            o.push_back('\\');
+        }
+        o.push_back(c);
+    }
+    return o + "\"";
+}
+}  // namespace
+
+int ref_parse_setup(const char* path, char* out, uint64_t capacity, uint64_t* length)
+{
+    return guarded([&] {
+        namespace b = ultrahigh_ann::benchmark;
+        const b::BenchmarkSetup s = b::load_benchmark_setup(path);
+        std::ostringstream o;
+        o << "{\"setup_path\":" << json_str(s.setup_path.string())
+          << ",\"dataset_directory\":" << json_str(s.dataset_directory.string())
+          << ",\"representatives_path\":" << json_str(s.representatives_path.string())
+          << ",\"representative_labels_path\":"
+          << json_str(s.representative_labels_path.string())
+          << ",\"queries_path\":" << json_str(s.queries_path.string())
+          << ",\"query_labels_path\":" << json_str(s.query_labels_path.string())
+          << ",\"json_output_path\":" << json_str(s.json_output_path.string())
+          << ",\"csv_output_path\":" << json_str(s.csv_output_path.string())
+          << ",\"probabilities_path\":"
+          << (s.probabilities_path ? json_str(s.probabilities_path->string()) : "null")
+          << ",\"distance\":" << json_str(std::string(b::distance_name(s.distance)))
+          << ",\"probability_policy\":"
+          << json_str(std::string(b::probability_policy_name(s.probability_policy)))
+          << ",\"diagnostics\":"
+          << json_str(std::string(b::diagnostic_mode_name(s.diagnostics)))
+          << ",\"maximum_queries\":" << s.maximum_queries << ",\"warmups\":" << s.warmups
+          << ",\"trials\":" << s.trials << ",\"batch_sizes\":[";
+        for (size_t i = 0; i < s.batch_sizes.size(); ++i) {
+            o << (i ? "," : "") << s.batch_sizes[i];
+        }
+        o << "],\"device\":" << s.device << ",\"reference_run\":" << json_str(s.reference_run)
+          << ",\"runs\":[";
+        for (size_t r = 0; r < s.runs.size(); ++r) {
+            const b::BenchmarkRun& run = s.runs[r];
+            o << (r ? "," : "") << "{\"name\":" << json_str(run.name)
+              << ",\"index\":" << json_str(std::string(b::index_name(run.index)))
+              << ",\"backend\":" << json_str(std::string(b::backend_name(run.backend)))
+              << ",\"strategy\":" << json_str(std::string(b::strategy_name(run.strategy)))
+              << ",\"repetitions\":" << run.repetitions << ",\"seed\":" << run.seed
+              << ",\"projection_dimension\":" << run.projection_dimension
+              << ",\"batch_sizes\":[";
+            for (size_t i = 0; i < run.batch_sizes.size(); ++i) {
+                o << (i ? "," : "") << run.batch_sizes[i];
+            }
+            o << "],\"warmups\":" << run.warmups << ",\"trials\":" << run.trials << "}";
+        }
+        o << "]}";
+        const std::string text = o.str();
+        *length = text.size();
+        if (out != nullptr && capacity > text.size()) {
+            std::memcpy(out, text.c_str(), text.size() + 1);
         }
     });
 }
