@@ -900,7 +900,8 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
     uint64_t launches = 0;
 
     const bool hierarchical = index->kind == IndexKind::hierarchical;
-    const float* scan_queries = ws->prepared.get();
+    float* prepared = c.prepared != nullptr ? c.prepared : ws->prepared.get();
+    const float* scan_queries = prepared;
     if (hierarchical) {
         uha::launch_prepare_sampled(source, n, index->dimension, index->columns.get(),
                                     nullptr, index->sample_size, ws->prepared.get(),
@@ -917,11 +918,10 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
         uha::launch_prepare_sampled(
             source, n, index->dimension, index->columns.get(),
             index->metric == UHA_L2 ? index->scales.get() : nullptr,
-            index->sample_size, ws->prepared.get(), index->padded_dim, error_flag,
-            stream);
+            index->sample_size, prepared, index->padded_dim, error_flag, stream);
         ++launches;
     } else {
-        uha::launch_prepare_dense(source, n, index->dimension, ws->prepared.get(),
+        uha::launch_prepare_dense(source, n, index->dimension, prepared,
                                   index->padded_dim, error_flag, stream);
         ++launches;
     }
@@ -968,7 +968,7 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
     }
     const uint64_t partial_count =
         checked_mul(checked_mul(plan.chunks, n, "partials"), index->rows, "partials");
-    if (ws->partials.size() < partial_count) {
+    if (c.partials == nullptr && ws->partials.size() < partial_count) {
         // Grows to the largest plan used so far; the previous contents are not
         // needed (stream order: earlier kernels have consumed them).
         check_cuda(cudaStreamSynchronize(stream), "CUDA query failed");
@@ -993,14 +993,21 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
     } else {
         uha::launch_scan(plan, op, index->scan_rows.get(), index->rows,
                          index->padded_dim, index->weights32.get(), scan_queries, n,
-                         ws->partials.get(), stream);
+                         c.partials != nullptr ? c.partials : ws->partials.get(), stream);
     }
     if (time_scan) {
         check_cuda(cudaEventRecord(scan_stop, stream), "event");
     }
     ++launches;
+    if (c.finish_stream != nullptr) {
+        // the argmin of this batch runs on the finish stream, behind the scan
+        check_cuda(cudaEventRecord(c.handoff, stream), "event");
+        check_cuda(cudaStreamWaitEvent(c.finish_stream, c.handoff, 0), "event");
+        stream = c.finish_stream;
+    }
 
-    const uha::PartialView view{ws->partials.get(), plan.chunks,
+    const uha::PartialView view{c.partials != nullptr ? c.partials : ws->partials.get(),
+                                plan.chunks,
                                 static_cast<uint32_t>(n),
                                 static_cast<uint32_t>(index->rows)};
     if (gemm) {
@@ -1017,7 +1024,7 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
     uha::Bound bound = make_bound(plan.depth, index->scan_dim, term_roundings);
     uha::ReplayInputs in{};
     in.rows = index->scan_rows.get();
-    in.queries = ws->prepared.get();
+    in.queries = prepared;
     in.dim = index->scan_dim;
     in.padded_dim = index->padded_dim;
     in.weights64 = index->weights64.get();
@@ -1129,6 +1136,53 @@ void validate_query_call(const uha_index* index, uha_workspace* ws,
     }
 }
 
+// Calls of many small batches on exact and flat indexes with the certified or
+// norm-identity strategy run as a two-stage pipeline: batch b's preparation
+// and scan (workspace stream) overlap the argmin of batch b - 1 (a second
+// stream), with two slots of prepared queries and partial sums.
+bool pipeline_applies(const uha_index* index, uha_strategy strategy, uint64_t batch,
+                      uint64_t batches)
+{
+    return batches >= 2 && batch <= 8 && index->kind != IndexKind::hierarchical &&
+           (strategy == UHA_DIRECT || strategy == UHA_GEMM);
+}
+
+void prepare_pipeline(const uha_index* index, uha_workspace* ws, uha_strategy strategy,
+                      uint64_t batch)
+{
+    cudaStream_t stream = ws->stream;
+    if (ws->finish_stream == nullptr) {
+        check_cuda(cudaStreamCreateWithFlags(&ws->finish_stream, cudaStreamNonBlocking),
+                   "cannot create CUDA stream");
+        for (cudaEvent_t& e : ws->pipe_events) {
+            check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming),
+                       "cannot create CUDA event");
+        }
+    }
+    // the largest plan any batch size up to `batch` uses
+    uint64_t per_slot = 0;
+    for (uint64_t n = 1; n <= batch; ++n) {
+        const TunedPlan* tuned = ws->find_tuned(n, static_cast<int>(strategy));
+        const uha::ScanPlan plan = tuned != nullptr && !tuned->lowp
+                                       ? tuned->scan
+                                       : uha::plan_scan(index->rows, index->padded_dim, n,
+                                                        index->sm_count);
+        per_slot = std::max(per_slot, checked_mul(checked_mul(plan.chunks, n, "partials"),
+                                                  index->rows, "partials"));
+    }
+    const uint64_t prepared = checked_mul(batch, index->padded_dim, "prepared queries");
+    if (ws->pipe_partials.size() < 2 * per_slot ||
+        ws->pipe_prepared.size() < 2 * prepared) {
+        check_cuda(cudaStreamSynchronize(stream), "CUDA query failed");
+        check_cuda(cudaStreamSynchronize(ws->finish_stream), "CUDA query failed");
+        ws->pipe_partials.allocate(2 * per_slot);
+        ws->pipe_prepared.allocate(2 * prepared);
+    }
+    // the argmin stream starts behind everything already on the workspace stream
+    check_cuda(cudaEventRecord(ws->pipe_events[4], stream), "event");
+    check_cuda(cudaStreamWaitEvent(ws->finish_stream, ws->pipe_events[4], 0), "event");
+}
+
 // Event pairs for timing the scan of every batch of a call.
 void ensure_scan_events(uha_workspace* ws, uint64_t batches)
 {
@@ -1197,11 +1251,28 @@ extern "C" uha_status uha_query_many(const uha_index* index, uha_workspace* ws,
         check_cuda(cudaMemsetAsync(ws->counters.get(), 0, ws->counters.bytes(), stream),
                    "cannot clear query counters");
         const BatchContext ctx{index, ws, strategy, out_distances != nullptr};
+        const bool pipelined = pipeline_applies(index, strategy, batch, batches);
+        if (pipelined) {
+            prepare_pipeline(index, ws, strategy, batch);
+        }
         uint64_t launches = 0;
         for (uint64_t b = 0; b < batches; ++b) {
             const uint64_t start = b * batch;
             const uint64_t count = std::min(batch, n - start);
             const float* source = queries + start * index->dimension;
+            BatchContext bc = ctx;
+            if (pipelined) {
+                // slot b % 2 is free once the argmin of batch b - 2 is done
+                const uint64_t slot = b % 2;
+                if (b >= 2) {
+                    check_cuda(cudaStreamWaitEvent(stream, ws->pipe_events[2 + slot], 0),
+                               "event");
+                }
+                bc.prepared = ws->pipe_prepared.get() + slot * batch * index->padded_dim;
+                bc.partials = ws->pipe_partials.get() + slot * (ws->pipe_partials.size() / 2);
+                bc.finish_stream = ws->finish_stream;
+                bc.handoff = ws->pipe_events[slot];
+            }
             if (!queries_on_device) {
                 check_cuda(cudaMemcpyAsync(ws->raw_queries.get(), source,
                                            count * index->dimension * sizeof(float),
@@ -1209,10 +1280,18 @@ extern "C" uha_status uha_query_many(const uha_index* index, uha_workspace* ws,
                            "cannot copy queries to the CUDA device");
                 source = ws->raw_queries.get();
             }
-            launches += enqueue_batch(ctx, source, count, ws->call_results.get() + start,
+            launches += enqueue_batch(bc, source, count, ws->call_results.get() + start,
                                       ws->call_exact.get() + start, ws->timing,
                                       ws->timing ? ws->scan_events[2 * b] : nullptr,
                                       ws->timing ? ws->scan_events[2 * b + 1] : nullptr);
+            if (pipelined) {
+                check_cuda(cudaEventRecord(ws->pipe_events[2 + b % 2], ws->finish_stream),
+                           "event");
+            }
+        }
+        if (pipelined) {
+            check_cuda(cudaEventRecord(ws->pipe_events[4], ws->finish_stream), "event");
+            check_cuda(cudaStreamWaitEvent(stream, ws->pipe_events[4], 0), "event");
         }
         check_cuda(cudaMemcpyAsync(ws->host_results.get(), ws->call_results.get(),
                                    n * sizeof(uha::Result), cudaMemcpyDeviceToHost,

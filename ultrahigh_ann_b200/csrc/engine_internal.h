@@ -24,6 +24,14 @@ struct BatchContext {
     uha_workspace* ws;
     uha_strategy strategy;
     bool want_distances;
+    // Pipelined calls (exact and flat indexes, direct / gemm): this batch's
+    // prepared queries and partial sums (sized by the caller), and the stream
+    // its argmin runs on after `handoff` is recorded behind the scan. Null:
+    // the workspace's own buffers and stream.
+    float* prepared = nullptr;
+    float* partials = nullptr;
+    cudaStream_t finish_stream = nullptr;
+    cudaEvent_t handoff = nullptr;
 };
 
 // Enqueues one batch of n queries (`source`: device, n x dimension floats) on

@@ -124,6 +124,12 @@ struct uha_workspace {
     bool timing = false;
     cudaEvent_t events[4] = {nullptr, nullptr, nullptr, nullptr};
     std::vector<cudaEvent_t> scan_events;  // start/stop of each batch's scan
+    // pipelined small batches: a second stream for the argmins, two slots of
+    // prepared queries and partial sums, hand-off / slot-free / join events
+    cudaStream_t finish_stream = nullptr;
+    cudaEvent_t pipe_events[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    uha::DeviceBuffer<float> pipe_prepared;
+    uha::DeviceBuffer<float> pipe_partials;
 
     ~uha_workspace()
     {
@@ -134,6 +140,14 @@ struct uha_workspace {
         }
         for (cudaEvent_t e : scan_events) {
             cudaEventDestroy(e);
+        }
+        for (cudaEvent_t e : pipe_events) {
+            if (e != nullptr) {
+                cudaEventDestroy(e);
+            }
+        }
+        if (finish_stream != nullptr) {
+            cudaStreamDestroy(finish_stream);
         }
         if (stream != nullptr) {
             cudaStreamDestroy(stream);
