@@ -431,8 +431,9 @@ def centroids_flat(queries=3013):
     """The reference's own CPU-runnable case: 33 class centroids, d = 60,660,
     flat L2 importance-sampling index with T = 8 and seed 0 (probabilities by
     the reference CPU policy's arithmetic), 3,013 queries answered one at a
-    time. Reported in microseconds per query and kernels per query (the index
-    is 33 x |I| floats: launch-latency bound, not a %HBM case), with the
+    time (one launch each: gather, scan and certified argmin fused for small
+    indexes). Reported in microseconds per query and kernels per query (the
+    index is 33 x |I| floats: launch-latency bound, not a %HBM case), with the
     answers checked against the reference's own CPU flat index (oracle/_ref)
     and the agreement with the binary64 exact argmin."""
     import torch
@@ -446,7 +447,6 @@ def centroids_flat(queries=3013):
     index = uha.CudaSampledCoordinateL2AnnIndex(ds.rows, probs, 8, uha.MT19937_64(0))
     s = index.coordinate_sample
     ws = index.make_query_workspace(1)
-    ws.set_timing(True)
     qdev = torch.from_numpy(ds.queries).cuda()
     out = np.zeros(queries, np.uint64)
     index.query_many(qdev.data_ptr(), 64, 1, out[:64], ws, on_device=True)

@@ -526,6 +526,159 @@ __global__ void __launch_bounds__(kFinalizeThreads)
     }
 }
 
+// ------------------------------------------------ small indexes, one launch
+
+// One CTA per query for indexes small enough that a single CTA scans all of
+// them (rows x padded columns <= kSmallCells): the query's sampled (or all)
+// coordinates are gathered into shared memory with the preparation kernels'
+// finiteness flags, one warp per row computes the binary32 distance (lane
+// partial sums in column order, then a warp butterfly), and the block
+// certifies the argmin, replaying the candidates in binary64 when needed.
+// Answers are those of the three-kernel path; only the accumulation depth
+// (and with it the bound) differs.
+__global__ void __launch_bounds__(kFinalizeThreads)
+    small_query_kernel(SmallQuery sq, Bound bound, ReplayInputs in, Result* results,
+                       double* exact_distances, uint32_t* replay_count, int* error_flag)
+{
+    extern __shared__ float small_smem[];
+    float* qv = small_smem;                      // padded_dim
+    float* dist = small_smem + sq.padded_dim;    // row_count
+    __shared__ int bad;
+    const uint32_t q = blockIdx.x;
+    if (threadIdx.x == 0) {
+        bad = 0;
+    }
+    __syncthreads();
+    const float* src = sq.queries + static_cast<uint64_t>(q) * sq.dim;
+    for (uint64_t i = threadIdx.x; i < sq.padded_dim; i += kFinalizeThreads) {
+        float v = 0.f;
+        if (sq.columns == nullptr) {
+            if (i < sq.dim) {
+                v = src[i];
+                if (!isfinite(v)) {
+                    atomicOr(error_flag, 1);
+                    bad = 1;
+                }
+            }
+        } else if (i < sq.sample_size) {
+            v = src[sq.columns[i]];
+            if (!isfinite(v)) {
+                atomicOr(error_flag, 1);
+                bad = 1;
+            }
+            if (sq.scales != nullptr) {
+                v = __fmul_rn(v, sq.scales[i]);
+                if (!isfinite(v)) {
+                    atomicOr(error_flag, 2);
+                    bad = 1;
+                }
+            }
+        }
+        qv[i] = v;
+    }
+    __syncthreads();
+    if (bad) {
+        // the call fails on the flag; nothing to certify
+        if (threadIdx.x == 0) {
+            results[q] = Result{0, 0.f};
+            exact_distances[q] = __longlong_as_double(0x7ff8000000000000ll);
+        }
+        return;
+    }
+    constexpr int warps = kFinalizeThreads / 32;
+    const int warp = threadIdx.x / 32;
+    const int lane = threadIdx.x % 32;
+    const uint64_t groups = sq.padded_dim / 4;
+    const float4* q4 = reinterpret_cast<const float4*>(qv);
+    for (uint32_t row = warp; row < sq.row_count; row += warps) {
+        const float4* r4 =
+            reinterpret_cast<const float4*>(sq.rows + static_cast<uint64_t>(row) * sq.padded_dim);
+        const float4* w4 = reinterpret_cast<const float4*>(sq.weights32);
+        float acc = 0.f;
+        for (uint64_t g = lane; g < groups; g += 32) {
+            const float4 a = q4[g];
+            const float4 b = __ldg(r4 + g);
+            if (sq.op == static_cast<int>(ScanOp::l2)) {
+                float d = a.x - b.x; acc = fmaf(d, d, acc);
+                d = a.y - b.y; acc = fmaf(d, d, acc);
+                d = a.z - b.z; acc = fmaf(d, d, acc);
+                d = a.w - b.w; acc = fmaf(d, d, acc);
+            } else if (sq.op == static_cast<int>(ScanOp::l1)) {
+                acc += fabsf(a.x - b.x);
+                acc += fabsf(a.y - b.y);
+                acc += fabsf(a.z - b.z);
+                acc += fabsf(a.w - b.w);
+            } else {
+                const float4 w = __ldg(w4 + g);
+                acc = fmaf(fabsf(a.x - b.x), w.x, acc);
+                acc = fmaf(fabsf(a.y - b.y), w.y, acc);
+                acc = fmaf(fabsf(a.z - b.z), w.z, acc);
+                acc = fmaf(fabsf(a.w - b.w), w.w, acc);
+            }
+        }
+        for (int o = 16; o > 0; o /= 2) {
+            acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        }
+        if (lane == 0) {
+            dist[row] = acc;
+        }
+    }
+    __syncthreads();
+    const float inf = __int_as_float(0x7f800000);
+    Summary s{inf, inf, inf, 0xffffffffu, inf};
+    for (uint32_t row = threadIdx.x; row < sq.row_count; row += kFinalizeThreads) {
+        const Bounds2 b = bound_of(dist[row], bound, row, q);
+        summary_insert(s, b.lower, b.upper, row, dist[row]);
+    }
+    s = block_reduce_summary(s);
+    __shared__ bool certified;
+    __shared__ float min_upper;
+    if (threadIdx.x == 0) {
+        certified = s.second > s.min_upper;
+        min_upper = s.min_upper;
+        if (certified) {
+            results[q] = Result{s.first_row, s.first_distance};
+            exact_distances[q] = __longlong_as_double(0x7ff8000000000000ll);
+        } else {
+            atomicAdd(replay_count, 1u);
+        }
+    }
+    __syncthreads();
+    if (certified) {
+        return;
+    }
+    double best = __longlong_as_double(0x7ff0000000000000ll);
+    uint32_t best_row = 0xffffffffu;
+    for (uint32_t row = warp; row < sq.row_count; row += warps) {
+        if (bound_of(dist[row], bound, row, q).lower > min_upper) {
+            continue;
+        }
+        const double d = replay_row(in, qv, in.rows + static_cast<uint64_t>(row) * in.padded_dim,
+                                    lane);
+        if (lex_less(d, row, best, best_row)) {
+            best = d;
+            best_row = row;
+        }
+    }
+    __shared__ double warp_best[warps];
+    __shared__ uint32_t warp_best_row[warps];
+    if (lane == 0) {
+        warp_best[warp] = best;
+        warp_best_row[warp] = best_row;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 0; w < warps; ++w) {
+            if (lex_less(warp_best[w], warp_best_row[w], best, best_row)) {
+                best = warp_best[w];
+                best_row = warp_best_row[w];
+            }
+        }
+        results[q] = Result{best_row, static_cast<float>(best)};
+        exact_distances[q] = best;
+    }
+}
+
 constexpr uint32_t kMaxCandidates = 64;
 constexpr int kRescoreUnroll = 4;
 
@@ -821,6 +974,31 @@ void launch_rescore(Bound64 bound, ReplayInputs in, const uint32_t* candidates,
         bound, in, candidates, k, rows, cand_dist, done, results, exact_distances,
         replay_count);
     check_cuda(cudaGetLastError(), "cannot launch re-score kernel");
+}
+
+bool small_query_fits(uint64_t rows, uint64_t padded_dim)
+{
+    return rows >= 1 && rows <= kSmallRows && padded_dim <= kSmallColumns &&
+           rows * padded_dim <= kSmallCells;
+}
+
+uint32_t small_query_depth(uint64_t padded_dim)
+{
+    const uint64_t groups = padded_dim / 4;
+    return static_cast<uint32_t>(4 * ((groups + 31) / 32) + 5);
+}
+
+void launch_small_query(const SmallQuery& sq, uint32_t batch, Bound bound, ReplayInputs in,
+                        Result* results, double* exact_distances, uint32_t* replay_count,
+                        int* error_flag, cudaStream_t stream)
+{
+    if (batch == 0) {
+        return;
+    }
+    const size_t smem = (sq.padded_dim + sq.row_count) * sizeof(float);
+    small_query_kernel<<<batch, kFinalizeThreads, smem, stream>>>(
+        sq, bound, in, results, exact_distances, replay_count, error_flag);
+    check_cuda(cudaGetLastError(), "cannot launch small-index query kernel");
 }
 
 void launch_finalize_gemm(PartialView view, const float* row_norms,

@@ -779,6 +779,14 @@ extern "C" uha_status uha_workspace_last_stats(const uha_workspace* workspace,
 
 namespace uha_engine {
 
+// Certified queries on exact and flat indexes small enough for one CTA per
+// query run as one fused launch.
+bool small_path_applies(const uha_index* index, uha_strategy strategy)
+{
+    return strategy == UHA_DIRECT && index->kind != IndexKind::hierarchical &&
+           uha::small_query_fits(index->rows, index->padded_dim);
+}
+
 bool precision_strategy(uha_strategy s)
 {
     return s == UHA_GEMM_BF16_RERANK || s == UHA_GEMM_FP8_RERANK;
@@ -900,6 +908,45 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
     uint64_t launches = 0;
 
     const bool hierarchical = index->kind == IndexKind::hierarchical;
+    if (small_path_applies(index, c.strategy)) {
+        uha::SmallQuery sq{};
+        sq.queries = source;
+        sq.dim = index->dimension;
+        sq.columns = index->kind == IndexKind::sampled ? index->columns.get() : nullptr;
+        sq.scales = index->kind == IndexKind::sampled && index->metric == UHA_L2
+                        ? index->scales.get()
+                        : nullptr;
+        sq.sample_size = index->sample_size;
+        sq.rows = index->scan_rows.get();
+        sq.row_count = static_cast<uint32_t>(index->rows);
+        sq.padded_dim = index->padded_dim;
+        sq.weights32 = index->weights32.get();
+        uha::ScanOp op = uha::ScanOp::l2;
+        if (index->metric == UHA_L1) {
+            op = index->weights32.size() != 0 ? uha::ScanOp::l1_weighted : uha::ScanOp::l1;
+        }
+        sq.op = static_cast<int>(op);
+        const uha::Bound bound = make_bound(uha::small_query_depth(index->padded_dim),
+                                            index->scan_dim,
+                                            op == uha::ScanOp::l1 ? 1 : 2);
+        uha::ReplayInputs in{};
+        in.op = index->metric == UHA_L2 ? uha::ReplayOp::l2_sequential
+                : index->weights64.size() != 0 ? uha::ReplayOp::l1_weighted_sequential
+                                               : uha::ReplayOp::l1_grouped4;
+        in.rows = index->scan_rows.get();
+        in.dim = index->scan_dim;
+        in.padded_dim = index->padded_dim;
+        in.weights64 = index->weights64.get();
+        if (time_scan) {
+            check_cuda(cudaEventRecord(scan_start, stream), "event");
+        }
+        uha::launch_small_query(sq, static_cast<uint32_t>(n), bound, in, results, exact,
+                                replay_count, error_flag, stream);
+        if (time_scan) {
+            check_cuda(cudaEventRecord(scan_stop, stream), "event");
+        }
+        return 1;
+    }
     float* prepared = c.prepared != nullptr ? c.prepared : ws->prepared.get();
     const float* scan_queries = prepared;
     if (hierarchical) {
@@ -1144,7 +1191,8 @@ bool pipeline_applies(const uha_index* index, uha_strategy strategy, uint64_t ba
                       uint64_t batches)
 {
     return batches >= 2 && batch <= 8 && index->kind != IndexKind::hierarchical &&
-           (strategy == UHA_DIRECT || strategy == UHA_GEMM);
+           (strategy == UHA_DIRECT || strategy == UHA_GEMM) &&
+           !small_path_applies(index, strategy);
 }
 
 void prepare_pipeline(const uha_index* index, uha_workspace* ws, uha_strategy strategy,

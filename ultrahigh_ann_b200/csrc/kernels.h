@@ -127,6 +127,29 @@ void launch_argmin(PartialView view, Bound bound, ReplayInputs in,
                    Result* results, double* exact_distances, void* scratch,
                    uint64_t capacity, uint32_t* replay_count,
                    cudaStream_t stream);
+// Indexes small enough for one CTA per query (rows <= 4096, padded columns
+// <= 8192, rows x padded columns <= 65536): gather, scan and certified argmin
+// (with replay) in one launch.
+constexpr uint64_t kSmallRows = 4096;
+constexpr uint64_t kSmallColumns = 8192;
+constexpr uint64_t kSmallCells = 65536;
+struct SmallQuery {
+    const float* queries;     // [batch][dim] raw queries
+    uint64_t dim;
+    const uint32_t* columns;  // sampled columns (null: all columns)
+    const float* scales;      // sampled L2 scales (nullable)
+    uint64_t sample_size;
+    const float* rows;        // [row_count][padded_dim]
+    uint32_t row_count;
+    uint64_t padded_dim;
+    const float* weights32;   // weighted L1
+    int op;                   // ScanOp: l2, l1 or l1_weighted
+};
+bool small_query_fits(uint64_t rows, uint64_t padded_dim);
+uint32_t small_query_depth(uint64_t padded_dim);
+void launch_small_query(const SmallQuery& sq, uint32_t batch, Bound bound, ReplayInputs in,
+                        Result* results, double* exact_distances, uint32_t* replay_count,
+                        int* error_flag, cudaStream_t stream);
 // Binary32 norm identity (no certification), lowest index on ties.
 void launch_finalize_gemm(PartialView view, const float* row_norms,
                           const float* query_norms, Result* results,
