@@ -423,11 +423,25 @@ ScanPlan plan_scan(uint64_t rows, uint64_t padded_dim, uint64_t batch,
     }
     const uint64_t row_tiles = (rows + kTileRows - 1) / kTileRows;
     const uint64_t query_tiles = (batch + kTileQueries - 1) / kTileQueries;
-    const uint64_t ctas = row_tiles * query_tiles;
-    const uint64_t target = 2ull * static_cast<uint64_t>(sm_count);
+    const uint64_t tiles = row_tiles * query_tiles;
+    // Two CTAs of the tile kernel fit an SM (registers). Pick the column split
+    // count whose CTA count fills its last wave best, within four waves unless
+    // one split already exceeds that; ties go to fewer splits.
+    const uint64_t slots = 2ull * static_cast<uint64_t>(sm_count > 0 ? sm_count : 148);
+    const uint64_t most = std::max<uint64_t>(1, padded_dim / 512);
     uint64_t splits = 1;
-    if (ctas < target) {
-        splits = (target + ctas - 1) / ctas;
+    double best = -1.0;
+    for (uint64_t s = 1; s <= most; ++s) {
+        const uint64_t ctas = tiles * s;
+        if (s > 1 && ctas > 4 * slots) {
+            break;
+        }
+        const uint64_t waves = (ctas + slots - 1) / slots;
+        const double fill = static_cast<double>(ctas) / static_cast<double>(waves * slots);
+        if (fill > best + 1e-9) {
+            best = fill;
+            splits = s;
+        }
     }
     return tile_plan(padded_dim, splits);
 }
