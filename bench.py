@@ -606,7 +606,9 @@ def serving(ds, rates=(10_000, 100_000, 1_000_000), seconds=0.5, pool=2048):
         for (name, _, l2_exact_or_flat), ix in zip(build, indexes):
             st = S.gemm_bf16_rerank if (mode == "bf16_rerank" and l2_exact_or_flat) else S.direct
             sid = server.add_index(ix, st)
-            server.reserve(sid, 2)
+            # one workspace per slot up front: creating one mid-run would stop
+            # the dispatcher for a warm-up batch
+            server.reserve(sid, 8)
         # warm-up load, then the measured rates
         n = 2000
         server.replay(rng.integers(0, 8, n), [base + int(j) * stride

@@ -284,8 +284,8 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
-// Stage 2, one warp per (query, row). With U the sampled minimum, E the
-// largest row error plus the query's error and (rel, abs) the median bound,
+// Stage 2. With U the sampled minimum, E the largest row error plus the
+// query's error and (rel, abs) the median bound,
 //   T = (U (1 + rel) + 2 E + 2 abs) / (1 - rel)   (rounded up)
 // exceeds every upper bound the sampled rows give, so a row whose binary32
 // median is above T has a lower bound above the query's smallest upper bound
@@ -293,6 +293,34 @@ __global__ void __launch_bounds__(kThreads)
 // <= T (odd p), fewer than p/2 (even p: the lower middle is above T). Such a
 // row stores -T (a negative distance: "at least T, no upper bound"); every
 // other row stores its binary32 median.
+// Each warp takes a contiguous run of (query, row) pairs in query-major
+// order, so the query's values and threshold stay in registers across rows
+// and the next row's values are loaded while the current one is decided.
+template <int PER_LANE>
+__device__ __forceinline__ void load_lane_values(const float* v, uint32_t p, int lane,
+                                                 float (&out)[PER_LANE])
+{
+#pragma unroll
+    for (int i = 0; i < PER_LANE; ++i) {
+        const uint32_t j = lane + 32u * i;
+        out[i] = j < p ? v[j] : 0.f;
+    }
+}
+
+__device__ __forceinline__ float median_threshold(const unsigned int* min_bits,
+                                                  const float* query_err, uint32_t q,
+                                                  float row_err_max, float rel, float abs_err)
+{
+    const float u = __uint_as_float(min_bits[q]);
+    if (!(u <= FLT_MAX)) {
+        return __int_as_float(0x7f800000);
+    }
+    const float e = __fadd_ru(row_err_max, query_err[q]);
+    const float num = __fadd_ru(__fadd_ru(__fmul_ru(u, __fadd_ru(1.f, rel)), __fmul_ru(2.f, e)),
+                                __fmul_ru(2.f, abs_err));
+    return __fmul_ru(__fdiv_ru(num, __fsub_rd(1.f, rel)), 1.0000005f);
+}
+
 template <int PER_LANE>
 __global__ void __launch_bounds__(kThreads)
     median_scan_kernel(const float* __restrict__ rows, uint32_t row_count,
@@ -304,33 +332,56 @@ __global__ void __launch_bounds__(kThreads)
 {
     const int lane = threadIdx.x % 32;
     const uint64_t total = static_cast<uint64_t>(row_count) * batch;
-    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * (blockDim.x / 32);
+    const uint64_t warps = static_cast<uint64_t>(gridDim.x) * (blockDim.x / 32);
+    const uint64_t warp_id = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) / 32;
+    const uint64_t per_warp = (total + warps - 1) / warps;
+    const uint64_t begin = warp_id * per_warp;
+    const uint64_t end = begin + per_warp < total ? begin + per_warp : total;
+    if (begin >= end) {
+        return;
+    }
     const uint32_t needed = p % 2 != 0 ? p / 2 + 1 : p / 2;
-    uint32_t cached_q = 0xffffffffu;
-    float t = 0.f;
-    for (uint64_t w = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) / 32;
-         w < total; w += stride) {
-        const uint32_t q = static_cast<uint32_t>(w / row_count);
-        const uint32_t row = static_cast<uint32_t>(w - uint64_t(q) * row_count);
-        if (q != cached_q) {
-            cached_q = q;
-            const float u = __uint_as_float(min_bits[q]);
-            t = __int_as_float(0x7f800000);
-            if (u <= FLT_MAX) {
-                const float e = __fadd_ru(row_err_max, query_err[q]);
-                const float num = __fadd_ru(__fadd_ru(__fmul_ru(u, __fadd_ru(1.f, rel)),
-                                                      __fmul_ru(2.f, e)),
-                                            __fmul_ru(2.f, abs_err));
-                t = __fmul_ru(__fdiv_ru(num, __fsub_rd(1.f, rel)), 1.0000005f);
+    uint32_t q = static_cast<uint32_t>(begin / row_count);
+    uint32_t row = static_cast<uint32_t>(begin - uint64_t(q) * row_count);
+    float y[PER_LANE];
+    load_lane_values<PER_LANE>(queries + uint64_t(q) * padded_p, p, lane, y);
+    float t = median_threshold(min_bits, query_err, q, row_err_max, rel, abs_err);
+    float next[PER_LANE];
+    load_lane_values<PER_LANE>(rows + uint64_t(row) * padded_p, p, lane, next);
+    for (uint64_t w = begin; w < end; ++w) {
+        float v[PER_LANE];
+        int valid = 0;
+#pragma unroll
+        for (int i = 0; i < PER_LANE; ++i) {
+            const uint32_t j = lane + 32u * i;
+            v[i] = 0.f;
+            if (j < p) {
+                float d = fabsf(next[i] - y[i]);
+                if (!(d <= FLT_MAX)) {
+                    d = __int_as_float(0x7f800000);
+                }
+                v[i] = d;
+                valid = i + 1;
             }
         }
-        float v[PER_LANE];
-        const int valid = load_abs_diffs<PER_LANE>(rows + uint64_t(row) * padded_p,
-                                                   queries + uint64_t(q) * padded_p, p, lane,
-                                                   v);
-        float* out = partials + static_cast<uint64_t>(q) * row_count + row;
-        if (t <= FLT_MAX) {
-            const uint32_t tb = __float_as_uint(t);
+        const uint32_t cur_q = q;
+        const uint32_t cur_row = row;
+        const float cur_t = t;
+        // advance to the next pair and start its loads
+        if (++row == row_count) {
+            row = 0;
+            ++q;
+        }
+        if (w + 1 < end) {
+            if (q != cur_q) {
+                load_lane_values<PER_LANE>(queries + uint64_t(q) * padded_p, p, lane, y);
+                t = median_threshold(min_bits, query_err, q, row_err_max, rel, abs_err);
+            }
+            load_lane_values<PER_LANE>(rows + uint64_t(row) * padded_p, p, lane, next);
+        }
+        float* out = partials + static_cast<uint64_t>(cur_q) * row_count + cur_row;
+        if (cur_t <= FLT_MAX) {
+            const uint32_t tb = __float_as_uint(cur_t);
             uint32_t at_most = 0;
 #pragma unroll
             for (int i = 0; i < PER_LANE; ++i) {
@@ -339,7 +390,7 @@ __global__ void __launch_bounds__(kThreads)
             at_most = __reduce_add_sync(0xffffffffu, at_most);
             if (at_most < needed) {
                 if (lane == 0) {
-                    *out = -t;
+                    *out = -cur_t;
                 }
                 continue;
             }
