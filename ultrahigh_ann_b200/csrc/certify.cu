@@ -17,6 +17,9 @@
 #include "kernels.h"
 
 #include <cfloat>
+#include <map>
+#include <mutex>
+#include <utility>
 
 namespace uha {
 namespace {
@@ -526,6 +529,91 @@ __global__ void __launch_bounds__(kFinalizeThreads)
     }
 }
 
+// The same for groups of kRefineGroup consecutive queries per CTA: thread j
+// projects every query of the group that needs it (each coefficient of row j
+// of the binary64 projection is read once for the group; each query's sum
+// keeps the reference order), then one warp per such query replays its row.
+constexpr int kRefineGroup = 8;
+
+__global__ void __launch_bounds__(kFinalizeThreads)
+    refine_group_kernel(ReplayInputs in, Bound bound, const Result* results,
+                        double* exact_distances, uint32_t batch)
+{
+    extern __shared__ unsigned char refine_smem[];
+    double* y = reinterpret_cast<double*>(refine_smem);           // group x proj_dim
+    float* x = reinterpret_cast<float*>(y + kRefineGroup * in.proj_dim);  // group x dim
+    __shared__ uint32_t members[kRefineGroup];
+    __shared__ int count;
+    const uint32_t q0 = blockIdx.x * kRefineGroup;
+    if (threadIdx.x == 0) {
+        int c = 0;
+        for (int g = 0; g < kRefineGroup; ++g) {
+            const uint32_t q = q0 + g;
+            if (q >= batch) {
+                break;
+            }
+            const double known = exact_distances[q];
+            if (known == known) {
+                continue;
+            }
+            const Result res = results[q];
+            const Bounds2 b = bound_of(res.distance, bound, res.row, q);
+            if (__fsub_ru(b.upper, b.lower) <= __fmul_rd(0.999e-5f, b.lower)) {
+                continue;
+            }
+            members[c++] = q;
+        }
+        count = c;
+    }
+    __syncthreads();
+    const int n = count;
+    if (n == 0) {
+        return;
+    }
+    const uint64_t dim = in.dim;
+    for (uint64_t idx = threadIdx.x; idx < static_cast<uint64_t>(n) * dim;
+         idx += kFinalizeThreads) {
+        const uint64_t m = idx / dim;
+        const uint64_t i = idx - m * dim;
+        x[idx] = in.queries[static_cast<uint64_t>(members[m]) * in.padded_dim + i];
+    }
+    __syncthreads();
+    for (uint64_t j = threadIdx.x; j < in.proj_dim; j += kFinalizeThreads) {
+        const double* coeff = in.projection64 + j * dim;
+        double acc[kRefineGroup];
+#pragma unroll
+        for (int m = 0; m < kRefineGroup; ++m) {
+            acc[m] = 0.0;
+        }
+        for (uint64_t i = 0; i < dim; ++i) {
+            const double c = coeff[i];
+#pragma unroll
+            for (int m = 0; m < kRefineGroup; ++m) {
+                if (m < n) {
+                    acc[m] = __dadd_rn(acc[m], __dmul_rn(static_cast<double>(x[m * dim + i]), c));
+                }
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < kRefineGroup; ++m) {
+            if (m < n) {
+                y[m * in.proj_dim + j] = acc[m];
+            }
+        }
+    }
+    __syncthreads();
+    const int warp = threadIdx.x / 32;
+    const int lane = threadIdx.x % 32;
+    if (warp < n) {
+        const uint32_t q = members[warp];
+        const float* qrow = in.queries + static_cast<uint64_t>(q) * in.padded_dim;
+        const double d = replay_candidate(in, qrow, y + warp * in.proj_dim, results[q].row, lane);
+        if (lane == 0) {
+            exact_distances[q] = d;
+        }
+    }
+}
+
 // ------------------------------------------------ small indexes, one launch
 
 // One CTA per query for indexes small enough that a single CTA scans all of
@@ -874,14 +962,27 @@ __global__ void __launch_bounds__(kFinalizeThreads)
     }
 }
 
+// Raises a kernel's dynamic shared-memory limit when a launch needs more than
+// 48 KB and more than it was configured for on this device (a call that needs
+// no more makes no runtime call, so captured launches after a warm-up make
+// none).
 void set_dynamic_smem(const void* kernel, size_t smem)
 {
-    if (smem > 48 * 1024) {
-        check_cuda(cudaFuncSetAttribute(kernel,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(smem)),
-                   "cannot configure replay shared memory");
+    if (smem <= 48 * 1024) {
+        return;
     }
+    static std::mutex mutex;
+    static std::map<std::pair<int, const void*>, size_t> configured;
+    const int device = current_device();
+    std::lock_guard<std::mutex> lock(mutex);
+    size_t& have = configured[{device, kernel}];
+    if (smem <= have) {
+        return;
+    }
+    check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(smem)),
+               "cannot configure replay shared memory");
+    have = smem;
 }
 
 size_t replay_smem(const ReplayInputs& in)
@@ -915,10 +1016,20 @@ void launch_refine_winners(ReplayInputs in, Bound bound, const Result* results,
                            uint32_t batch, double* exact_distances,
                            cudaStream_t stream)
 {
-    const size_t smem = replay_smem(in);
-    set_dynamic_smem(reinterpret_cast<const void*>(refine_kernel), smem);
-    refine_kernel<<<batch, kFinalizeThreads, smem, stream>>>(in, bound, results,
-                                                             exact_distances);
+    static_assert(kRefineGroup <= kFinalizeThreads / 32, "one warp per group member");
+    const size_t group_smem =
+        kRefineGroup * (in.proj_dim * sizeof(double) + in.dim * sizeof(float));
+    if (group_smem <= 200 * 1024) {
+        set_dynamic_smem(reinterpret_cast<const void*>(refine_group_kernel), group_smem);
+        refine_group_kernel<<<(batch + kRefineGroup - 1) / kRefineGroup, kFinalizeThreads,
+                              group_smem, stream>>>(in, bound, results, exact_distances,
+                                                    batch);
+    } else {
+        const size_t smem = replay_smem(in);
+        set_dynamic_smem(reinterpret_cast<const void*>(refine_kernel), smem);
+        refine_kernel<<<batch, kFinalizeThreads, smem, stream>>>(in, bound, results,
+                                                                 exact_distances);
+    }
     check_cuda(cudaGetLastError(), "cannot launch refine kernel");
 }
 
