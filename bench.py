@@ -386,9 +386,9 @@ def precision(ds, exact_index, batches=((1, 256), (64, 2048), (1024, 2048))):
         ws.set_timing(True)
         res = np.zeros(n, np.uint64)
         dist = np.zeros(n, np.float64)
-        w = min(B, n)
-        # warm-up (first use builds the low-precision rows)
-        exact_index.query_many(qdev.data_ptr(), w, B, res[:w], ws, strategy, dist[:w],
+        # warm-up: the same call (first use builds the low-precision rows and
+        # the workspace's pipeline buffers)
+        exact_index.query_many(qdev.data_ptr(), n, B, res, ws, strategy, dist,
                                on_device=True)
         torch.cuda.synchronize()
         t = time.perf_counter()

@@ -857,13 +857,15 @@ void ensure_lowp_workspace(uha_workspace* ws, const uha_index* index,
 // plan (the partial-score slabs are in ws->partials).
 uha::LowpPlan enqueue_lowp_scores(const uha_index* index, uha_workspace* ws,
                                   uha_strategy strategy, uint64_t n, bool time_scan,
-                                  cudaEvent_t scan_start, cudaEvent_t scan_stop)
+                                  cudaEvent_t scan_start, cudaEvent_t scan_stop,
+                                  const float* prepared = nullptr)
 {
     cudaStream_t stream = ws->stream;
     const uha::LowpType type = lowp_type(strategy);
     const uha::LowpRows& lp = lowp_rows(index, type, stream);
     ensure_lowp_workspace(ws, index, stream);
-    uha::launch_lowp_queries(type, ws->prepared.get(), n, index->padded_dim,
+    uha::launch_lowp_queries(type, prepared != nullptr ? prepared : ws->prepared.get(), n,
+                             index->padded_dim,
                              ws->queries_lp.get(), lp.pitch, ws->query_scales.get(),
                              ws->query_amax.get(), stream);
     const TunedPlan* tuned = ws->find_tuned(n, static_cast<int>(strategy));
@@ -975,24 +977,35 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
 
     if (precision_strategy(c.strategy)) {
         const uha::LowpPlan plan = enqueue_lowp_scores(index, ws, c.strategy, n, time_scan,
-                                                       scan_start, scan_stop);
+                                                       scan_start, scan_stop, prepared);
         const uint32_t k = static_cast<uint32_t>(
             std::min<uint64_t>(ws->candidates_per_query, index->rows));
+        uint32_t* candidates = c.candidates != nullptr ? c.candidates : ws->candidates.get();
         uha::launch_lowp_topk(ws->partials.get(), plan.splits, static_cast<uint32_t>(n),
                               static_cast<uint32_t>(index->rows),
                               index->lowp[static_cast<int>(lowp_type(c.strategy))].norms.get(),
-                              k, ws->candidates.get(), stream);
+                              k, candidates, stream);
+        if (c.finish_stream != nullptr) {
+            // the re-score of this batch runs on the finish stream, behind the
+            // candidate selection (it overlaps the next batch's scores)
+            check_cuda(cudaEventRecord(c.handoff, stream), "event");
+            check_cuda(cudaStreamWaitEvent(c.finish_stream, c.handoff, 0), "event");
+            stream = c.finish_stream;
+        }
         const uha::Bound64 bound =
             uha::make_bound64(uha::rescore_depth(index->padded_dim), index->scan_dim);
         uha::ReplayInputs in{};
         in.op = uha::ReplayOp::l2_sequential;
         in.rows = index->scan_rows.get();
-        in.queries = ws->prepared.get();
+        in.queries = prepared;
         in.dim = index->scan_dim;
         in.padded_dim = index->padded_dim;
-        uha::launch_rescore(bound, in, ws->candidates.get(), k, static_cast<uint32_t>(n),
-                            static_cast<uint32_t>(index->rows), ws->cand_dist.get(),
-                            ws->rescore_done.get(), results, exact, replay_count, stream);
+        uha::launch_rescore(bound, in, candidates, k, static_cast<uint32_t>(n),
+                            static_cast<uint32_t>(index->rows),
+                            c.cand_dist != nullptr ? c.cand_dist : ws->cand_dist.get(),
+                            c.rescore_done != nullptr ? c.rescore_done
+                                                      : ws->rescore_done.get(),
+                            results, exact, replay_count, stream);
         return launches + 4;
     }
 
@@ -1190,8 +1203,13 @@ void validate_query_call(const uha_index* index, uha_workspace* ws,
 bool pipeline_applies(const uha_index* index, uha_strategy strategy, uint64_t batch,
                       uint64_t batches)
 {
-    return batches >= 2 && batch <= 8 && index->kind != IndexKind::hierarchical &&
-           (strategy == UHA_DIRECT || strategy == UHA_GEMM) &&
+    if (batches < 2 || index->kind == IndexKind::hierarchical) {
+        return false;
+    }
+    if (precision_strategy(strategy)) {
+        return true;  // scores of batch b overlap the re-score of batch b - 1
+    }
+    return batch <= 8 && (strategy == UHA_DIRECT || strategy == UHA_GEMM) &&
            !small_path_applies(index, strategy);
 }
 
@@ -1207,6 +1225,24 @@ void prepare_pipeline(const uha_index* index, uha_workspace* ws, uha_strategy st
                        "cannot create CUDA event");
         }
     }
+    const uint64_t prepared_slot = checked_mul(batch, index->padded_dim, "prepared queries");
+    if (precision_strategy(strategy)) {
+        const uint64_t cand = checked_mul(batch, uha::max_rerank_candidates(), "candidates");
+        if (ws->pipe_prepared.size() < 2 * prepared_slot || ws->pipe_candidates.size() < 2 * cand) {
+            check_cuda(cudaStreamSynchronize(stream), "CUDA query failed");
+            check_cuda(cudaStreamSynchronize(ws->finish_stream), "CUDA query failed");
+            ws->pipe_prepared.allocate(2 * prepared_slot);
+            ws->pipe_candidates.allocate(2 * cand);
+            ws->pipe_cand_dist.allocate(2 * cand);
+            ws->pipe_rescore_done.allocate(2 * batch);
+            check_cuda(cudaMemsetAsync(ws->pipe_rescore_done.get(), 0,
+                                       ws->pipe_rescore_done.bytes(), stream),
+                       "cannot clear re-score counters");
+        }
+        check_cuda(cudaEventRecord(ws->pipe_events[4], stream), "event");
+        check_cuda(cudaStreamWaitEvent(ws->finish_stream, ws->pipe_events[4], 0), "event");
+        return;
+    }
     // the largest plan any batch size up to `batch` uses
     uint64_t per_slot = 0;
     for (uint64_t n = 1; n <= batch; ++n) {
@@ -1218,7 +1254,7 @@ void prepare_pipeline(const uha_index* index, uha_workspace* ws, uha_strategy st
         per_slot = std::max(per_slot, checked_mul(checked_mul(plan.chunks, n, "partials"),
                                                   index->rows, "partials"));
     }
-    const uint64_t prepared = checked_mul(batch, index->padded_dim, "prepared queries");
+    const uint64_t prepared = prepared_slot;
     if (ws->pipe_partials.size() < 2 * per_slot ||
         ws->pipe_prepared.size() < 2 * prepared) {
         check_cuda(cudaStreamSynchronize(stream), "CUDA query failed");
@@ -1317,7 +1353,15 @@ extern "C" uha_status uha_query_many(const uha_index* index, uha_workspace* ws,
                                "event");
                 }
                 bc.prepared = ws->pipe_prepared.get() + slot * batch * index->padded_dim;
-                bc.partials = ws->pipe_partials.get() + slot * (ws->pipe_partials.size() / 2);
+                if (precision_strategy(strategy)) {
+                    const uint64_t cand = batch * uha::max_rerank_candidates();
+                    bc.candidates = ws->pipe_candidates.get() + slot * cand;
+                    bc.cand_dist = ws->pipe_cand_dist.get() + slot * cand;
+                    bc.rescore_done = ws->pipe_rescore_done.get() + slot * batch;
+                } else {
+                    bc.partials =
+                        ws->pipe_partials.get() + slot * (ws->pipe_partials.size() / 2);
+                }
                 bc.finish_stream = ws->finish_stream;
                 bc.handoff = ws->pipe_events[slot];
             }

@@ -25,12 +25,16 @@ struct BatchContext {
     uha_workspace* ws;
     uha_strategy strategy;
     bool want_distances;
-    // Pipelined calls (exact and flat indexes, direct / gemm): this batch's
-    // prepared queries and partial sums (sized by the caller), and the stream
-    // its argmin runs on after `handoff` is recorded behind the scan. Null:
-    // the workspace's own buffers and stream.
+    // Pipelined calls (exact and flat indexes): this batch's prepared queries
+    // and partial sums (direct / gemm) or candidate buffers (precision),
+    // sized by the caller, and the stream its argmin / re-score runs on after
+    // `handoff` is recorded behind the scan. Null: the workspace's own buffers
+    // and stream.
     float* prepared = nullptr;
     float* partials = nullptr;
+    uint32_t* candidates = nullptr;   // precision: this batch's candidate slot
+    double* cand_dist = nullptr;
+    uint32_t* rescore_done = nullptr;
     cudaStream_t finish_stream = nullptr;
     cudaEvent_t handoff = nullptr;
 };

@@ -130,6 +130,9 @@ struct uha_workspace {
     cudaEvent_t pipe_events[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     uha::DeviceBuffer<float> pipe_prepared;
     uha::DeviceBuffer<float> pipe_partials;
+    uha::DeviceBuffer<uint32_t> pipe_candidates;   // precision pipeline slots
+    uha::DeviceBuffer<double> pipe_cand_dist;
+    uha::DeviceBuffer<uint32_t> pipe_rescore_done;
 
     ~uha_workspace()
     {
