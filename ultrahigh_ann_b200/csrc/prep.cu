@@ -48,6 +48,28 @@ __global__ void prepare_dense_kernel(const float* __restrict__ queries,
     }
 }
 
+// The same for rows of a multiple of 4 floats starting on 16-byte
+// boundaries: grid (column groups of 4 x kThreads, queries).
+__global__ void prepare_dense_vec_kernel(const float* __restrict__ queries, uint64_t dim,
+                                         float* __restrict__ out, uint64_t padded_dim,
+                                         int* error_flag)
+{
+    const uint64_t b = blockIdx.y;
+    const uint64_t g = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    const uint64_t i = 4 * g;
+    if (i >= padded_dim) {
+        return;
+    }
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (i < dim) {
+        v = __ldg(reinterpret_cast<const float4*>(queries + b * dim + i));
+        if (!(isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && isfinite(v.w))) {
+            atomicOr(error_flag, 1);
+        }
+    }
+    *reinterpret_cast<float4*>(out + b * padded_dim + i) = v;
+}
+
 __global__ void prepare_sampled_kernel(const float* __restrict__ queries,
                                        uint64_t batch, uint64_t dim,
                                        const uint32_t* __restrict__ columns,
@@ -166,8 +188,21 @@ void launch_prepare_dense(const float* queries, uint64_t batch, uint64_t dim,
                           float* out, uint64_t padded_dim, int* error_flag,
                           cudaStream_t stream)
 {
-    prepare_dense_kernel<<<grid_for(batch * padded_dim), kThreads, 0, stream>>>(
-        queries, batch, dim, out, padded_dim, error_flag);
+    if (batch == 0 || padded_dim == 0) {
+        return;
+    }
+    const bool aligned = dim % 4 == 0 && (reinterpret_cast<uintptr_t>(queries) % 16) == 0;
+    if (aligned && batch <= 65535) {
+        // one thread per 4 columns, 16-byte loads and stores
+        const uint64_t groups = padded_dim / 4;
+        const dim3 grid(static_cast<uint32_t>((groups + kThreads - 1) / kThreads),
+                        static_cast<uint32_t>(batch));
+        prepare_dense_vec_kernel<<<grid, kThreads, 0, stream>>>(queries, dim, out, padded_dim,
+                                                                 error_flag);
+    } else {
+        prepare_dense_kernel<<<grid_for(batch * padded_dim), kThreads, 0, stream>>>(
+            queries, batch, dim, out, padded_dim, error_flag);
+    }
     check_cuda(cudaGetLastError(), "cannot launch query preparation kernel");
 }
 
