@@ -429,11 +429,15 @@ ScanPlan plan_scan(uint64_t rows, uint64_t padded_dim, uint64_t batch,
     // one split already exceeds that; ties go to fewer splits.
     const uint64_t slots = 2ull * static_cast<uint64_t>(sm_count > 0 ? sm_count : 148);
     const uint64_t most = std::max<uint64_t>(1, padded_dim / 512);
-    uint64_t splits = 1;
+    // at most 8192 columns per split: the accumulation depth (and with it the
+    // certification bound, and the share of queries that need the binary64
+    // replay) stays small
+    const uint64_t least = std::min<uint64_t>(most, (padded_dim + 8191) / 8192);
+    uint64_t splits = least;
     double best = -1.0;
-    for (uint64_t s = 1; s <= most; ++s) {
+    for (uint64_t s = least; s <= most; ++s) {
         const uint64_t ctas = tiles * s;
-        if (s > 1 && ctas > 4 * slots) {
+        if (s > least && ctas > 4 * slots) {
             break;
         }
         const uint64_t waves = (ctas + slots - 1) / slots;
