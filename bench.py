@@ -52,7 +52,7 @@ def parse_args():
     p.add_argument("--precision-only", action="store_true",
                    help="only the precision-strategy table (one JSON line)")
     p.add_argument("--only", default="",
-                   choices=["", "precision", "batched", "serving", "centroids"],
+                   choices=["", "precision", "batched", "serving", "centroids", "wide"],
                    help="only this section of the bench (one JSON line)")
     p.add_argument("--precision-batch", type=int, default=0,
                    help="with --precision-only: one batch size (2048 queries)")
@@ -273,6 +273,8 @@ def run_engine(args):
         line["batched"] = batched(ds)
         torch.cuda.empty_cache()
         line["serving"] = serving(ds)
+        torch.cuda.empty_cache()
+        line["wide"] = wide()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -562,6 +564,68 @@ def batched(ds, per_index=4096, reps=3):
                          "tuned_scan_ms": round(sum(t_["best_ms"] for t_ in tuned), 3)}}
 
 
+def _bf16_values(a: np.ndarray) -> np.ndarray:
+    """The binary32 values a BF16 store decodes to (round to nearest even)."""
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) >> 16
+    return (u.astype(np.uint32) << 16).view(np.float32)
+
+
+def wide(per_index=1024, dim=262_144):
+    """Hierarchical indexes at d = 262,144 with BF16-stored values (binary32
+    values that BF16 represents exactly): L2 (JL) and L1 (Cauchy / median),
+    rows 1,024 and 2,048, p = 16 and 64, T = 32, 1,024 queries each, in one
+    captured batch; the probabilities are those of the first 1,024 rows."""
+    import torch
+
+    import ultrahigh_ann_b200 as uha
+    from ultrahigh_ann_b200 import synthetic
+
+    t = time.perf_counter()
+    ds = synthetic.row_dataset(rows=2048, classes=33, queries=per_index, d=dim, seed=3)
+    rows = _bf16_values(ds.rows)
+    queries = _bf16_values(ds.queries)
+    gen_s = time.perf_counter() - t
+    t = time.perf_counter()
+    p2 = uha.compute_l2_importance_probabilities_gpu(rows[:1024]).probabilities
+    p1 = uha.compute_l1_importance_probabilities_gpu(rows[:1024]).probabilities
+    prob_s = time.perf_counter() - t
+    specs = [("l2", 1024, 16), ("l1", 1024, 64), ("l2", 2048, 64), ("l1", 2048, 16)]
+    indexes = []
+    t = time.perf_counter()
+    for i, (metric, r, p) in enumerate(specs):
+        cls = (uha.CudaHierarchicalL2AnnIndex if metric == "l2"
+               else uha.CudaHierarchicalL1AnnIndex)
+        indexes.append(cls(rows[:r], 32, p, uha.MT19937_64(200 + i),
+                           importance_probabilities=p2 if metric == "l2" else p1))
+    build_s = time.perf_counter() - t
+    qdev = torch.from_numpy(queries).cuda()
+    batch = uha.QueryBatch([(ix, per_index, uha.QueryStrategy.direct) for ix in indexes],
+                           autotune=True)
+    batch.run([qdev.data_ptr()] * len(indexes), on_device=True)
+    ms = []
+    for _ in range(3):
+        res = batch.run(None)
+        ms.append(batch.stats()["device_ms"])
+    # the same answers index by index
+    same = True
+    for ix, (got, _) in zip(indexes, res):
+        ws = ix.make_query_workspace(per_index)
+        want = ix.query_many(qdev.data_ptr(), per_index, per_index, None, ws, on_device=True)
+        same = same and bool(np.array_equal(want, got))
+    total = per_index * len(indexes)
+    return {"dimension": dim, "storage": "bf16 values",
+            "indexes": [{"metric": m, "rows": r, "p": p, "T": 32,
+                         "k": len(ix.coordinate_sample)} for (m, r, p), ix in
+                        zip(specs, indexes)],
+            "queries_per_index": per_index,
+            "queries_per_s": round(total / (min(ms) * 1e-3), 1),
+            "device_ms": round(min(ms), 3), "replayed": batch.stats()["replayed_queries"],
+            "answers_equal_index_by_index": same,
+            "setup_s": {"generate": round(gen_s, 1), "probabilities": round(prob_s, 1),
+                        "build": round(build_s, 1)}}
+
+
 def serving(ds, rates=(10_000, 100_000, 1_000_000), seconds=0.5, pool=2048):
     """Request loop over 8 device-resident indexes (exact, flat and
     hierarchical, L1 and L2; r from 33 to 7,028, d = 60,660), Poisson arrivals
@@ -715,6 +779,9 @@ def run_section(args):
 
     if args.only == "centroids":
         print(json.dumps({"centroids_flat": centroids_flat()}), flush=True)
+        return
+    if args.only == "wide":
+        print(json.dumps({"wide": wide()}), flush=True)
         return
     ds = synthetic.row_dataset(rows=ROWS, classes=33, queries=4096, d=DIM, seed=1,
                                query_stream=0)

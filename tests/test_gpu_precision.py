@@ -165,3 +165,28 @@ def test_precision_errors():
     wsh = hier.make_query_workspace(2)
     with pytest.raises(uha.InvalidArgument):
         hier.query_batch(queries[:2], 2, None, wsh, BF16)
+
+
+@pytest.mark.parametrize("strategy", [BF16, FP8])
+def test_query_many_pipeline_equals_per_batch_calls(strategy):
+    """Calls of several batches overlap each batch's re-score with the next
+    batch's scores (two candidate slots): the answers equal batch-by-batch
+    calls, and a failing call leaves the workspace usable."""
+    ds = synthetic.row_dataset(rows=700, classes=9, queries=50, d=2500, seed=6)
+    index = uha.CudaExactL2Index(ds.rows)
+    for batch in (1, 7, 16):
+        ws = index.make_query_workspace(batch)
+        ws.set_candidates(16)
+        dist = np.zeros(50, np.float64)
+        many = index.query_many(ds.queries, 50, batch, None, ws, strategy, dist)
+        single, sdist = run(index, ds.queries, batch, strategy, candidates=16)
+        assert np.array_equal(many, single), batch
+        assert np.array_equal(dist, sdist), batch
+    bad = ds.queries.copy()
+    bad[23, 5] = np.inf
+    ws = index.make_query_workspace(8)
+    with pytest.raises(uha.InvalidArgument):
+        index.query_many(bad, 50, 8, None, ws, strategy)
+    again = index.query_many(ds.queries, 50, 8, None, ws, strategy)
+    ref, _ = run(index, ds.queries, 8, strategy, candidates=32)
+    assert np.array_equal(again, ref)
