@@ -626,7 +626,7 @@ def wide(per_index=1024, dim=262_144):
                         "build": round(build_s, 1)}}
 
 
-def serving(ds, rates=(10_000, 100_000, 1_000_000), seconds=0.5, pool=2048):
+def serving(ds, rates=(10_000, 100_000, 1_000_000, 2_000_000), seconds=0.5, pool=2048):
     """Request loop over 8 device-resident indexes (exact, flat and
     hierarchical, L1 and L2; r from 33 to 7,028, d = 60,660), Poisson arrivals
     with a uniformly chosen index per request, queries from a device-resident

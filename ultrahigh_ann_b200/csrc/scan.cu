@@ -455,8 +455,10 @@ std::vector<ScanPlan> scan_candidates(uint64_t rows, uint64_t padded_dim,
 {
     std::vector<ScanPlan> out;
     out.push_back(plan_scan(rows, padded_dim, batch, sm_count));
-    if (batch <= 64) {
-        // the stream kernel re-reads the rows once per pass of 8 queries
+    if (batch <= 64 || padded_dim <= 2048) {
+        // the stream kernel re-reads the rows once per pass of up to 8
+        // queries: a candidate for small batches, and for narrow rows (the
+        // projected rows of hierarchies) whose re-reads stay in L2
         for (int nq : {1, 2, 4, 8}) {
             if (nq <= static_cast<int>(2 * batch)) {
                 out.push_back(stream_plan(padded_dim, nq));
