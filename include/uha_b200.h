@@ -103,8 +103,9 @@ typedef struct uha_query_stats {
     uint64_t certified_queries;   /* winner certified by the binary32 bound */
     uint64_t replayed_queries;    /* winner settled by the binary64 replay */
     uint64_t kernel_launches;     /* kernels this library launched for the call */
-    double scan_ms;               /* device time of the scan kernel (timing on) */
+    double scan_ms;               /* device time of the timed scan kernels */
     double device_ms;             /* device time from first enqueue to results */
+    uint64_t timed_scans;         /* scan launches scan_ms covers */
 } uha_query_stats;
 
 /* GPU probability-build report (include/ultrahigh_ann/hnsvw25/l2/
@@ -277,9 +278,11 @@ uha_status uha_workspace_last_stats(const uha_workspace* workspace,
  * caller can order its own work or record timing events against it. */
 void* uha_workspace_stream(const uha_workspace* workspace);
 
-/* With enabled != 0, every uha_query on this workspace records CUDA events on
- * the workspace stream around the scan kernel and around the whole device
- * pipeline, reported in uha_query_stats.scan_ms / device_ms. */
+/* With enabled != 0, queries on this workspace record CUDA events on the
+ * workspace stream around the whole device pipeline (device_ms) and around
+ * the scan kernel of every enabled-th batch of a call (scan_ms, summed over
+ * timed_scans launches): 1 times every batch, larger values sample batches
+ * so that the events cost less in long calls of small batches. */
 uha_status uha_workspace_set_timing(uha_workspace* workspace, int enabled);
 
 /* Candidates per query of the precision strategies (1 to 64; default 32).

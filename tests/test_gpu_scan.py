@@ -322,3 +322,21 @@ def test_query_many_equals_per_batch_calls(oracle_module, kind):
     bad[30, :] = np.nan
     with pytest.raises(uha.InvalidArgument):
         index.query_many(bad, 45, 4, None, index.make_query_workspace(4))
+
+
+def test_timing_samples_every_stride_batch():
+    ds = synthetic.row_dataset(rows=300, classes=5, queries=20, d=4000, seed=2)
+    index = uha.CudaExactL2Index(ds.rows)
+    ws = index.make_query_workspace(1)
+    ws.set_timing(True, stride=8)
+    got = index.query_many(ds.queries, 20, 1, None, ws)
+    st = ws.last_stats()
+    assert st["timed_scans"] == 3 and st["scan_ms"] > 0 and st["device_ms"] > 0
+    ws.set_timing(True)
+    assert np.array_equal(index.query_many(ds.queries, 20, 1, None, ws), got)
+    assert ws.last_stats()["timed_scans"] == 20
+    ws.set_timing(False)
+    index.query_many(ds.queries, 20, 1, None, ws)
+    assert ws.last_stats()["timed_scans"] == 0
+    with pytest.raises(uha.InvalidArgument):
+        ws.set_timing(True, stride=0)

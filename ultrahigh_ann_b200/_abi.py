@@ -94,7 +94,8 @@ class QueryStats(ctypes.Structure):
                 ("replayed_queries", c_uint64),
                 ("kernel_launches", c_uint64),
                 ("scan_ms", c_double),
-                ("device_ms", c_double)]
+                ("device_ms", c_double),
+                ("timed_scans", c_uint64)]
 
 
 class ProbabilityReport(ctypes.Structure):

@@ -154,9 +154,13 @@ class MT19937_64:
         self._handle = handle
 
     def __del__(self):
-        if getattr(self, "_handle", None):
-            _abi.load().uha_rng_destroy(self._handle)
+        handle = getattr(self, "_handle", None)
+        if handle:
             self._handle = None
+            try:
+                _abi.load().uha_rng_destroy(handle)
+            except Exception:  # interpreter shutdown: the module is gone
+                pass
 
     @property
     def handle(self) -> ctypes.c_void_p:
@@ -345,9 +349,13 @@ class QueryWorkspace:
         self._index = index  # keeps the index alive while the workspace lives
 
     def __del__(self):
-        if getattr(self, "_handle", None):
-            _abi.load().uha_workspace_destroy(self._handle)
+        handle = getattr(self, "_handle", None)
+        if handle:
             self._handle = None
+            try:
+                _abi.load().uha_workspace_destroy(handle)
+            except Exception:  # interpreter shutdown: the module is gone
+                pass
 
     def maximum_batch_size(self) -> int:
         b = ctypes.c_uint64()
@@ -365,16 +373,20 @@ class QueryWorkspace:
         return {"query_count": s.query_count, "certified_queries": s.certified_queries,
                 "replayed_queries": s.replayed_queries,
                 "kernel_launches": s.kernel_launches, "scan_ms": s.scan_ms,
-                "device_ms": s.device_ms}
+                "device_ms": s.device_ms, "timed_scans": s.timed_scans}
 
     def stream_handle(self) -> int:
         """cudaStream_t of the workspace as an integer."""
         return int(_abi.load().uha_workspace_stream(self._handle) or 0)
 
-    def set_timing(self, enabled: bool) -> None:
-        """Records CUDA events around the scan kernel and the device pipeline
-        of every query on this workspace (see last_stats())."""
-        _check(_abi.load().uha_workspace_set_timing(self._handle, int(enabled)))
+    def set_timing(self, enabled, stride: int = 1) -> None:
+        """Records CUDA events around the device pipeline of every call and
+        around the scan kernel of every stride-th batch (see last_stats():
+        scan_ms covers timed_scans launches)."""
+        value = int(stride) if enabled else 0
+        if enabled and value < 1:
+            raise InvalidArgument("timing stride must be positive")
+        _check(_abi.load().uha_workspace_set_timing(self._handle, value))
 
     def autotune(self, batch: int, strategy=QueryStrategy.direct) -> dict:
         """Times every candidate scan shape for batches of exactly `batch`
@@ -402,9 +414,13 @@ class _CudaIndex:
         self._rows = rows
 
     def __del__(self):
-        if getattr(self, "_handle", None):
-            _abi.load().uha_index_destroy(self._handle)
+        handle = getattr(self, "_handle", None)
+        if handle:
             self._handle = None
+            try:
+                _abi.load().uha_index_destroy(handle)
+            except Exception:  # interpreter shutdown: the module is gone
+                pass
 
     @property
     def dimension(self) -> int:
@@ -797,9 +813,13 @@ class QueryBatch:
         self.total = sum(self._counts)
 
     def __del__(self):
-        if getattr(self, "_handle", None):
-            _abi.load().uha_batch_destroy(self._handle)
+        handle = getattr(self, "_handle", None)
+        if handle:
             self._handle = None
+            try:
+                _abi.load().uha_batch_destroy(handle)
+            except Exception:  # interpreter shutdown: the module is gone
+                pass
 
     def query_buffer(self, pair: int) -> int:
         """Device pointer the graph reads pair `pair`'s queries from."""
@@ -875,9 +895,13 @@ class Server:
         self._keep = []
 
     def __del__(self):
-        if getattr(self, "_handle", None):
-            _abi.load().uha_server_destroy(self._handle)
+        handle = getattr(self, "_handle", None)
+        if handle:
             self._handle = None
+            try:
+                _abi.load().uha_server_destroy(handle)
+            except Exception:  # interpreter shutdown: the module is gone
+                pass
 
     def add_index(self, index: "_CudaIndex", strategy=QueryStrategy.direct) -> int:
         out = ctypes.c_uint32()

@@ -761,7 +761,9 @@ extern "C" uha_status uha_workspace_set_timing(uha_workspace* workspace,
     return guarded([&] {
         require(workspace != nullptr, UHA_INVALID_ARGUMENT,
                 "workspace must not be null");
+        require(enabled >= 0, UHA_INVALID_ARGUMENT, "timing must be 0 or a positive stride");
         workspace->timing = enabled != 0;
+        workspace->timing_stride = enabled > 0 ? static_cast<uint32_t>(enabled) : 1u;
     });
 }
 
@@ -1372,10 +1374,11 @@ extern "C" uha_status uha_query_many(const uha_index* index, uha_workspace* ws,
                            "cannot copy queries to the CUDA device");
                 source = ws->raw_queries.get();
             }
+            const bool timed = ws->timing && b % ws->timing_stride == 0;
             launches += enqueue_batch(bc, source, count, ws->call_results.get() + start,
-                                      ws->call_exact.get() + start, ws->timing,
-                                      ws->timing ? ws->scan_events[2 * b] : nullptr,
-                                      ws->timing ? ws->scan_events[2 * b + 1] : nullptr);
+                                      ws->call_exact.get() + start, timed,
+                                      timed ? ws->scan_events[2 * b] : nullptr,
+                                      timed ? ws->scan_events[2 * b + 1] : nullptr);
             if (pipelined) {
                 check_cuda(cudaEventRecord(ws->pipe_events[2 + b % 2], ws->finish_stream),
                            "event");
@@ -1402,13 +1405,16 @@ extern "C" uha_status uha_query_many(const uha_index* index, uha_workspace* ws,
         if (ws->timing) {
             float ms = 0.f;
             double scan = 0.0;
-            for (uint64_t b = 0; b < batches; ++b) {
+            uint64_t timed = 0;
+            for (uint64_t b = 0; b < batches; b += ws->timing_stride) {
                 check_cuda(cudaEventElapsedTime(&ms, ws->scan_events[2 * b],
                                                 ws->scan_events[2 * b + 1]),
                            "event");
                 scan += ms;
+                ++timed;
             }
             ws->last.scan_ms = scan;
+            ws->last.timed_scans = timed;
             check_cuda(cudaEventElapsedTime(&ms, ws->events[0], ws->events[3]), "event");
             ws->last.device_ms = ms;
         }

@@ -122,6 +122,7 @@ struct uha_workspace {
     uha::PinnedBuffer<uint32_t> host_counters;
     uha_query_stats last{};
     bool timing = false;
+    uint32_t timing_stride = 1;  // scan events on every timing_stride-th batch
     cudaEvent_t events[4] = {nullptr, nullptr, nullptr, nullptr};
     std::vector<cudaEvent_t> scan_events;  // start/stop of each batch's scan
     // pipelined small batches: a second stream for the argmins, two slots of
