@@ -19,6 +19,7 @@ oracle/_ref) on the host cores, on rank 0 only.
 from __future__ import annotations
 
 import argparse
+import functools
 import json
 import os
 import statistics
@@ -325,21 +326,21 @@ def suite(ds, exact_index):
     qdev = torch.from_numpy(ds.queries[:nq]).cuda()
 
     def timeit(index, B, n):
+        # One uha_query_many call answers the n device-resident queries in
+        # batches of B (each batch as one query_batch call); the first,
+        # identical call warms the workspace and its pipeline buffers.
         ws = index.make_query_workspace(B)
         res = np.zeros(n, np.uint64)
-        index.query_device_batch(qdev.data_ptr(), min(B, n), res[:min(B, n)], ws)
+        index.query_many(qdev.data_ptr(), n, B, res, ws, on_device=True)
         torch.cuda.synchronize()
         t = time.perf_counter()
-        repl = 0
-        for s in range(0, n, B):
-            e = min(n, s + B)
-            index.query_device_batch(qdev.data_ptr() + s * DIM * 4, e - s, res[s:e], ws)
-            repl += ws.last_stats()["replayed_queries"]
-        return res, n / (time.perf_counter() - t), repl
+        index.query_many(qdev.data_ptr(), n, B, res, ws, on_device=True)
+        qps = n / (time.perf_counter() - t)
+        return res, qps, ws.last_stats()["replayed_queries"]
 
     exact_ans = {}
     for metric, index in (("l2", exact_index), ("l1", uha.CudaExactL1Index(ds.rows))):
-        for B, n in ((1, 64), (64, 512), (1024, 2048)):
+        for B, n in ((1, 512), (64, 2048), (1024, 2048)):
             res, qps, repl = timeit(index, B, n)
             if B == 1024:
                 exact_ans[metric] = res
@@ -353,7 +354,7 @@ def suite(ds, exact_index):
         probs = prob_fn(ds.rows)
         for T in (32, 128):
             index = cls(ds.rows, probs.probabilities, T, uha.MT19937_64(0))
-            for B, n in ((1, 512), (64, 2048), (1024, 2048)):
+            for B, n in ((1, 2048), (64, 2048), (1024, 2048)):
                 res, qps, repl = timeit(index, B, n)
                 entry = {"index": "flat", "metric": metric, "T": T,
                          "k": len(index.coordinate_sample), "batch": B,
@@ -571,6 +572,25 @@ def _bf16_values(a: np.ndarray) -> np.ndarray:
     return (u.astype(np.uint32) << 16).view(np.float32)
 
 
+@functools.lru_cache(maxsize=1)
+def _wide_data(queries=1024, dim=262_144):
+    """2,048 rows and `queries` queries at d = dim with BF16-stored values
+    (the config-0 generator, 33 latent classes), and the L2 / L1 importance
+    probabilities of the first 1,024 rows; built once per run."""
+    import ultrahigh_ann_b200 as uha
+    from ultrahigh_ann_b200 import synthetic
+
+    t = time.perf_counter()
+    ds = synthetic.row_dataset(rows=2048, classes=33, queries=queries, d=dim, seed=3)
+    rows = _bf16_values(ds.rows)
+    qs = _bf16_values(ds.queries)
+    gen_s = time.perf_counter() - t
+    t = time.perf_counter()
+    p2 = uha.compute_l2_importance_probabilities_gpu(rows[:1024]).probabilities
+    p1 = uha.compute_l1_importance_probabilities_gpu(rows[:1024]).probabilities
+    return rows, qs, p2, p1, gen_s, time.perf_counter() - t
+
+
 def wide(per_index=1024, dim=262_144):
     """Hierarchical indexes at d = 262,144 with BF16-stored values (binary32
     values that BF16 represents exactly): L2 (JL) and L1 (Cauchy / median),
@@ -579,17 +599,8 @@ def wide(per_index=1024, dim=262_144):
     import torch
 
     import ultrahigh_ann_b200 as uha
-    from ultrahigh_ann_b200 import synthetic
 
-    t = time.perf_counter()
-    ds = synthetic.row_dataset(rows=2048, classes=33, queries=per_index, d=dim, seed=3)
-    rows = _bf16_values(ds.rows)
-    queries = _bf16_values(ds.queries)
-    gen_s = time.perf_counter() - t
-    t = time.perf_counter()
-    p2 = uha.compute_l2_importance_probabilities_gpu(rows[:1024]).probabilities
-    p1 = uha.compute_l1_importance_probabilities_gpu(rows[:1024]).probabilities
-    prob_s = time.perf_counter() - t
+    rows, queries, p2, p1, gen_s, prob_s = _wide_data(per_index, dim)
     specs = [("l2", 1024, 16), ("l1", 1024, 64), ("l2", 2048, 64), ("l1", 2048, 16)]
     indexes = []
     t = time.perf_counter()
@@ -628,10 +639,12 @@ def wide(per_index=1024, dim=262_144):
 
 def serving(ds, rates=(10_000, 100_000, 1_000_000, 2_000_000), seconds=0.5, pool=2048):
     """Request loop over 8 device-resident indexes (exact, flat and
-    hierarchical, L1 and L2; r from 33 to 7,028, d = 60,660), Poisson arrivals
-    with a uniformly chosen index per request, queries from a device-resident
-    pool. Plain strategies, then BF16 + re-score on the exact and flat L2
-    indexes; agreement of the exact L2 answers with the binary64 exact argmin."""
+    hierarchical, L1 and L2; r from 33 to 7,028; six at d = 60,660 and two
+    hierarchies at d = 262,144 with BF16-stored values), Poisson arrivals with
+    a uniformly chosen index per request, queries from a device-resident pool
+    of each dimension. Plain strategies, then BF16 + re-score on the exact and
+    flat L2 indexes; agreement of the exact L2 answers with the binary64 exact
+    argmin."""
     import torch
 
     import ultrahigh_ann_b200 as uha
@@ -650,14 +663,27 @@ def serving(ds, rates=(10_000, 100_000, 1_000_000, 2_000_000), seconds=0.5, pool
             ds.rows, pl1, 32, uha.MT19937_64(3)), False),
         ("hier_l2_r7028_p64", lambda: uha.CudaHierarchicalL2AnnIndex(
             ds.rows, 32, 64, uha.MT19937_64(4), importance_probabilities=pl2), False),
-        ("hier_l1_r2048_p16", lambda: uha.CudaHierarchicalL1AnnIndex(
-            ds.rows[:2048], 32, 16, uha.MT19937_64(5), importance_probabilities=pl1), False),
-        ("exact_l1_r1024", lambda: uha.CudaExactL1Index(ds.rows[:1024]), False),
+        ("hier_l2_r2048_p64_d262144", lambda: uha.CudaHierarchicalL2AnnIndex(
+            wrows, 32, 64, uha.MT19937_64(5), importance_probabilities=wp2), False),
+        ("hier_l1_r1024_p16_d262144", lambda: uha.CudaHierarchicalL1AnnIndex(
+            wrows[:1024], 32, 16, uha.MT19937_64(6), importance_probabilities=wp1), False),
     ]
+    wrows, wqueries, wp2, wp1, _, _ = _wide_data()
     names = [b[0] for b in build]
     indexes = [b[1]() for b in build]
     qdev = torch.from_numpy(ds.queries[:pool]).cuda()
-    base, stride = qdev.data_ptr(), ds.rows.shape[1] * 4
+    wdev = torch.from_numpy(wqueries).cuda()
+    # per index: the query pool's base pointer, its row stride and its size
+    pools = [(qdev.data_ptr(), ds.rows.shape[1] * 4, pool)] * 6 + \
+        [(wdev.data_ptr(), wrows.shape[1] * 4, wqueries.shape[0])] * 2
+    base_of = np.array([p[0] for p in pools], np.uint64)
+    stride_of = np.array([p[1] for p in pools], np.uint64)
+    size_of = np.array([p[2] for p in pools], np.int64)
+
+    def pointers(ids, draws):
+        # a uniform query of each request's own pool
+        qi = (draws * size_of[ids]).astype(np.int64)
+        return qi, (base_of[ids] + qi.astype(np.uint64) * stride_of[ids]).tolist()
     # binary64 exact answers of the pool on the exact L2 index
     ws = indexes[2].make_query_workspace(256)
     exact = np.zeros(pool, np.uint64)
@@ -675,21 +701,19 @@ def serving(ds, rates=(10_000, 100_000, 1_000_000, 2_000_000), seconds=0.5, pool
             server.reserve(sid, 8)
         # warm-up load, then the measured rates
         n = 2000
-        server.replay(rng.integers(0, 8, n), [base + int(j) * stride
-                                             for j in rng.integers(0, pool, n)],
-                      np.arange(n) * 50.0)
+        ids = rng.integers(0, 8, n)
+        server.replay(ids, pointers(ids, rng.random(n))[1], np.arange(n) * 50.0)
         server.drain()
         server.poll()
         rows = []
         for rate in rates:
             n = int(rate * seconds)
             ids = rng.integers(0, 8, n).astype(np.uint32)
-            qi = rng.integers(0, pool, n)
+            qi, ptrs = pointers(ids, rng.random(n))
             arrival = np.cumsum(rng.exponential(1e6 / rate, n))
             server.reset_stats()
             t = time.perf_counter()
-            server.replay(ids, (base + qi.astype(np.uint64) * stride).tolist(), arrival,
-                          np.arange(n))
+            server.replay(ids, ptrs, arrival, np.arange(n))
             server.drain()
             wall = time.perf_counter() - t
             res = server.poll(n)
