@@ -53,7 +53,8 @@ def parse_args():
     p.add_argument("--precision-only", action="store_true",
                    help="only the precision-strategy table (one JSON line)")
     p.add_argument("--only", default="",
-                   choices=["", "precision", "batched", "serving", "centroids", "wide"],
+                   choices=["", "precision", "batched", "serving", "centroids", "wide",
+                            "hierarchies"],
                    help="only this section of the bench (one JSON line)")
     p.add_argument("--precision-batch", type=int, default=0,
                    help="with --precision-only: one batch size (2048 queries)")
@@ -637,6 +638,113 @@ def wide(per_index=1024, dim=262_144):
                         "build": round(build_s, 1)}}
 
 
+def _projected_check(ix, metric, sampled64, queries64, got):
+    """Binary64 check of a hierarchy's answers on the host: for each query
+    (sampled coordinates, binary64) the returned row's projected distance
+    (squared L2, or the median |diff| with the mean of the two middle values
+    for even p) must equal the minimum over all rows within 1e-9 relative (the
+    numpy evaluation order differs from the reference's sequential one)."""
+    P = np.asarray(ix.projection, np.float64).reshape(-1, sampled64.shape[1])
+    reps = sampled64 @ P.T
+    ok = 0
+    for q, row in zip(queries64, got):
+        diff = reps - q @ P.T
+        d = (np.einsum("ij,ij->i", diff, diff) if metric == "l2"
+             else np.median(np.abs(diff), axis=1))
+        ok += int(d[int(row)] <= d.min() * (1 + 1e-9) + 1e-300)
+    return ok
+
+
+def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=16):
+    """16 hierarchical indexes at the full size of the hierarchical batched
+    configuration: rows 1,024 / 7,028 / 65,536 (row subsets of one
+    65,536 x 262,144 BF16 matrix generated on the device), T = 32,
+    p = 16 / 64 / 256, L2 (JL) and L1 (Cauchy, median), 4,096 queries each,
+    in one captured CUDA graph launch with autotuned scan shapes. The indexes
+    are built from the device-resident matrix (no host copy of it); the
+    importance probabilities are those of the first 1,024 rows (the pair
+    computation over all 65,536 rows is ~1e15 binary64 operations). Checks:
+    the same answers index by index, and a binary64 host check of `checked`
+    queries per index."""
+    import torch
+
+    import ultrahigh_ann_b200 as uha
+    from ultrahigh_ann_b200 import synthetic
+
+    t = time.perf_counter()
+    data = synthetic.device_row_dataset(rows=rows, classes=33, queries=per_index, d=dim,
+                                        seed=4, storage="bfloat16")
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t
+    t = time.perf_counter()
+    head = data.rows[:1024].float().cpu().numpy()
+    probs = {"l2": uha.compute_l2_importance_probabilities_gpu(head).probabilities,
+             "l1": uha.compute_l1_importance_probabilities_gpu(head).probabilities}
+    prob_s = time.perf_counter() - t
+    specs, indexes = [], []
+    t = time.perf_counter()
+    i = 0
+    for r in (1024, 7028, rows):
+        for p in (16, 64, 256):
+            for metric in ("l2", "l1"):
+                if r == 1024 and p == 256:
+                    continue
+                cls = (uha.CudaHierarchicalL2AnnIndex if metric == "l2"
+                       else uha.CudaHierarchicalL1AnnIndex)
+                ix = cls(uha.DeviceMatrix.from_torch(data.rows[:r]), 32, p,
+                         uha.MT19937_64(300 + i), importance_probabilities=probs[metric])
+                indexes.append(ix)
+                specs.append({"metric": metric, "rows": r, "T": 32, "p": p,
+                              "k": len(ix.coordinate_sample)})
+                i += 1
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t
+    # host copies of the sampled columns for the binary64 check, then the
+    # matrix is released
+    sampled = []
+    for ix, spec in zip(indexes, specs):
+        cols = torch.from_numpy(ix.coordinate_sample.source_columns.astype(np.int64)).cuda()
+        sampled.append(data.rows[:spec["rows"]].index_select(1, cols).double().cpu().numpy())
+    data.rows = None
+    torch.cuda.empty_cache()
+    qdev = data.queries
+    t = time.perf_counter()
+    batch = uha.QueryBatch([(ix, per_index, uha.QueryStrategy.direct) for ix in indexes],
+                           autotune=True)
+    setup_s = time.perf_counter() - t
+    batch.run([qdev.data_ptr()] * len(indexes), on_device=True)
+    ms = []
+    for _ in range(reps):
+        res = batch.run(None)
+        ms.append(batch.stats()["device_ms"])
+    st = batch.stats()
+    same = True
+    for k, ix in enumerate(indexes):
+        ws = ix.make_query_workspace(per_index)
+        want = ix.query_many(qdev.data_ptr(), per_index, per_index, None, ws, on_device=True)
+        same = same and bool(np.array_equal(want, res[k][0]))
+        del ws
+    picks = np.random.default_rng(9).choice(per_index, checked, replace=False)
+    q_host = qdev.index_select(0, torch.from_numpy(picks).cuda()).double().cpu().numpy()
+    ok = 0
+    for k, (ix, spec) in enumerate(zip(indexes, specs)):
+        cols = ix.coordinate_sample.source_columns.astype(np.int64)
+        ok += _projected_check(ix, spec["metric"], sampled[k], q_host[:, cols],
+                               res[k][0][picks])
+    total = per_index * len(indexes)
+    best = min(ms)
+    return {"workload": f"hierarchical_16_indexes_r{rows}_d{dim}_bf16",
+            "indexes": specs, "queries_per_index": per_index,
+            "queries_per_s": round(total / (best * 1e-3), 1),
+            "device_ms": round(best, 3), "device_ms_runs": [round(m, 3) for m in ms],
+            "graph_nodes": st["graph_nodes"], "kernels_per_run": st["kernel_launches"],
+            "replayed": st["replayed_queries"], "answers_equal_index_by_index": same,
+            "binary64_checked": {"queries": checked * len(indexes), "distance_optimal": ok},
+            "setup_s": {"generate_on_device": round(gen_s, 1),
+                        "probabilities": round(prob_s, 1), "build": round(build_s, 1),
+                        "autotune_and_capture": round(setup_s, 1)}}
+
+
 def serving(ds, rates=(10_000, 100_000, 1_000_000, 2_000_000), seconds=0.5, pool=2048):
     """Request loop over 8 device-resident indexes (exact, flat and
     hierarchical, L1 and L2; r from 33 to 7,028; six at d = 60,660 and two
@@ -806,6 +914,9 @@ def run_section(args):
         return
     if args.only == "wide":
         print(json.dumps({"wide": wide()}), flush=True)
+        return
+    if args.only == "hierarchies":
+        print(json.dumps({"hierarchies_full": hierarchies_full()}), flush=True)
         return
     ds = synthetic.row_dataset(rows=ROWS, classes=33, queries=4096, d=DIM, seed=1,
                                query_stream=0)

@@ -192,6 +192,46 @@ uha_status uha_hierarchical_index_create(int device, uha_metric metric,
                                          uint64_t projection_dimension,
                                          uha_index** out);
 
+/* A row-major matrix already resident on the index's device: row i starts
+ * at element i * row_stride of `data` (row_stride >= columns). BF16 values
+ * are decoded exactly to binary32, so an index built from them equals one
+ * built from the host binary32 matrix of the decoded values. */
+typedef enum uha_value_type {
+    UHA_VALUES_F32 = 0,
+    UHA_VALUES_BF16 = 1
+} uha_value_type;
+
+typedef struct uha_device_matrix {
+    const void* data;
+    uha_value_type type;
+    uint64_t rows;
+    uint64_t columns;
+    uint64_t row_stride;
+} uha_device_matrix;
+
+/* The three index constructors above with the representative matrix read
+ * on the device (no host copy of it is made or needed): only the sampled
+ * columns are read for sampled and hierarchical indexes. Same validation,
+ * errors and resulting index as the host forms; in addition `data` must be
+ * device memory of `device`, aligned to its element size. No reference
+ * counterpart (the reference's constructors take a host DenseMatrix); it
+ * builds indexes whose host matrix would not fit host memory (for example
+ * 65,536 x 262,144 values). */
+uha_status uha_exact_index_create_device(int device, uha_metric metric,
+                                         const uha_device_matrix* rows,
+                                         uha_index** out);
+uha_status uha_sampled_index_create_device(int device, uha_metric metric,
+                                           const uha_device_matrix* rows,
+                                           const uint64_t* columns,
+                                           const uint64_t* multiplicities,
+                                           const double* inverse_probabilities,
+                                           uint64_t sample_size, uha_index** out);
+uha_status uha_hierarchical_index_create_device(
+    int device, uha_metric metric, const uha_device_matrix* rows,
+    const uint64_t* columns, const uint64_t* multiplicities,
+    const double* inverse_probabilities, uint64_t sample_size,
+    const double* projection, uint64_t projection_dimension, uha_index** out);
+
 void uha_index_destroy(uha_index* index);
 
 /* Replaces space_usage() of every CUDA index class, with the reference byte

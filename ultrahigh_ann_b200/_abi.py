@@ -70,6 +70,15 @@ class ServerStats(ctypes.Structure):
                 ("peak_in_flight", ctypes.c_uint32)]
 
 
+VALUES_F32 = 0
+VALUES_BF16 = 1
+
+
+class DeviceMatrix(ctypes.Structure):
+    _fields_ = [("data", c_void_p), ("type", c_int), ("rows", c_uint64),
+                ("columns", c_uint64), ("row_stride", c_uint64)]
+
+
 class SpaceUsage(ctypes.Structure):
     _fields_ = [("index_payload_bytes", c_uint64),
                 ("query_workspace_payload_bytes", c_uint64),
@@ -126,6 +135,13 @@ SIGNATURES = {
     "uha_hierarchical_index_create": (c_int, [c_int, c_int, c_void_p, c_uint64, c_uint64,
                                                c_void_p, c_void_p, c_void_p, c_uint64,
                                                c_void_p, c_uint64, _H]),
+    "uha_exact_index_create_device": (c_int, [c_int, c_int, POINTER(DeviceMatrix), _H]),
+    "uha_sampled_index_create_device": (c_int, [c_int, c_int, POINTER(DeviceMatrix),
+                                                 c_void_p, c_void_p, c_void_p, c_uint64,
+                                                 _H]),
+    "uha_hierarchical_index_create_device": (c_int, [c_int, c_int, POINTER(DeviceMatrix),
+                                                      c_void_p, c_void_p, c_void_p,
+                                                      c_uint64, c_void_p, c_uint64, _H]),
     "uha_index_destroy": (None, [c_void_p]),
     "uha_index_space_usage": (c_int, [c_void_p, POINTER(SpaceUsage)]),
     "uha_index_device": (c_int, [c_void_p, POINTER(c_int), c_char_p, c_uint64]),

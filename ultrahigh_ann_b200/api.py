@@ -282,10 +282,67 @@ class ProbabilityResult:
 
 
 def _matrix(values) -> np.ndarray:
+    if isinstance(values, DeviceMatrix) or _is_cuda_tensor(values):
+        raise InvalidArgument("this operation needs a host representative matrix")
     m = np.ascontiguousarray(values, dtype=np.float32)
     if m.ndim != 2:
         raise InvalidArgument("representative matrix must be two-dimensional")
     return m
+
+
+def _is_cuda_tensor(values) -> bool:
+    return type(values).__module__.startswith("torch") and \
+        getattr(getattr(values, "device", None), "type", None) == "cuda"
+
+
+@dataclass(frozen=True)
+class DeviceMatrix:
+    """A row-major representative matrix already on a CUDA device: row i
+    starts at element i * row_stride of `pointer`; values binary32 or BF16
+    (decoded exactly). Index constructors given one read it on the device
+    (uha_*_index_create_device) instead of copying a host matrix; only the
+    sampled columns are read by sampled and hierarchical indexes. The memory
+    must stay valid while the constructor runs."""
+    pointer: int
+    rows: int
+    columns: int
+    dtype: str = "float32"
+    row_stride: Optional[int] = None
+
+    @classmethod
+    def from_torch(cls, tensor) -> "DeviceMatrix":
+        import torch
+        if tensor.dim() != 2 or tensor.device.type != "cuda":
+            raise InvalidArgument("a device matrix is a two-dimensional CUDA tensor")
+        if tensor.dtype not in (torch.float32, torch.bfloat16) or tensor.stride(1) != 1:
+            raise InvalidArgument("a device matrix holds float32 or bfloat16 rows "
+                                  "with unit column stride")
+        return cls(tensor.data_ptr(), tensor.shape[0], tensor.shape[1],
+                   "bfloat16" if tensor.dtype == torch.bfloat16 else "float32",
+                   tensor.stride(0))
+
+    @property
+    def shape(self) -> tuple:
+        return (self.rows, self.columns)
+
+    def _struct(self) -> "_abi.DeviceMatrix":
+        if self.dtype not in ("float32", "bfloat16"):
+            raise InvalidArgument("a device matrix holds float32 or bfloat16 values")
+        return _abi.DeviceMatrix(ctypes.c_void_p(int(self.pointer)),
+                                 _abi.VALUES_BF16 if self.dtype == "bfloat16"
+                                 else _abi.VALUES_F32,
+                                 int(self.rows), int(self.columns),
+                                 int(self.columns if self.row_stride is None
+                                     else self.row_stride))
+
+
+def _rows_input(values):
+    """A host matrix (as binary32 numpy) or a DeviceMatrix."""
+    if isinstance(values, DeviceMatrix):
+        return values
+    if _is_cuda_tensor(values):
+        return DeviceMatrix.from_torch(values)
+    return _matrix(values)
 
 
 def _probabilities_gpu(metric: int, representatives, device: int,
@@ -554,11 +611,15 @@ class CudaDenseL2ScanIndex(_CudaIndex):
     """include/ultrahigh_ann/core/cuda_dense_l2_scan_index.hpp:27-91."""
 
     def __init__(self, representatives, device: int = 0):
-        rows = _matrix(representatives)
+        rows = _rows_input(representatives)
         handle = ctypes.c_void_p()
-        _check(_abi.load().uha_exact_index_create(device, _abi.L2, _ptr(rows),
-                                                  rows.shape[0], rows.shape[1],
-                                                  ctypes.byref(handle)))
+        if isinstance(rows, DeviceMatrix):
+            _check(_abi.load().uha_exact_index_create_device(
+                device, _abi.L2, ctypes.byref(rows._struct()), ctypes.byref(handle)))
+        else:
+            _check(_abi.load().uha_exact_index_create(device, _abi.L2, _ptr(rows),
+                                                      rows.shape[0], rows.shape[1],
+                                                      ctypes.byref(handle)))
         self._adopt(handle, rows.shape[1], rows.shape[0])
 
 
@@ -571,10 +632,16 @@ class CudaDenseL1ScanIndex(_CudaIndex):
     weighted form evaluates sum_j w_j |r_j - q_j|."""
 
     def __init__(self, representatives, coordinate_weights=None, device: int = 0):
-        rows = _matrix(representatives)
+        rows = _rows_input(representatives)
         handle = ctypes.c_void_p()
         lib = _abi.load()
-        if coordinate_weights is None:
+        if isinstance(rows, DeviceMatrix):
+            if coordinate_weights is not None:
+                raise InvalidArgument("coordinate weights need a host representative matrix")
+            _check(lib.uha_exact_index_create_device(device, _abi.L1,
+                                                     ctypes.byref(rows._struct()),
+                                                     ctypes.byref(handle)))
+        elif coordinate_weights is None:
             _check(lib.uha_exact_index_create(device, _abi.L1, _ptr(rows),
                                               rows.shape[0], rows.shape[1],
                                               ctypes.byref(handle)))
@@ -600,7 +667,7 @@ class CudaExactL1Index(CudaDenseL1ScanIndex):
         super().__init__(representatives, None, device)
 
 
-def _resolve_sample(input_rows: np.ndarray, probabilities, repetitions,
+def _resolve_sample(input_rows, probabilities, repetitions,
                     random_engine, coordinate_sample) -> CoordinateSample:
     if coordinate_sample is not None:
         if isinstance(coordinate_sample, CoordinateSample):
@@ -617,14 +684,20 @@ class _CudaSampledIndex(_CudaIndex):
 
     def __init__(self, input, probabilities=None, repetitions=None,
                  random_engine=None, device: int = 0, *, coordinate_sample=None):
-        rows = _matrix(input)
+        rows = _rows_input(input)
         sample = _resolve_sample(rows, probabilities, repetitions, random_engine,
                                  coordinate_sample)
         handle = ctypes.c_void_p()
-        _check(_abi.load().uha_sampled_index_create(
-            device, self._metric, _ptr(rows), rows.shape[0], rows.shape[1],
-            _ptr(sample.source_columns), _ptr(sample.multiplicities),
-            _ptr(sample.inverse_probabilities), len(sample), ctypes.byref(handle)))
+        sample_args = (_ptr(sample.source_columns), _ptr(sample.multiplicities),
+                       _ptr(sample.inverse_probabilities), len(sample),
+                       ctypes.byref(handle))
+        if isinstance(rows, DeviceMatrix):
+            _check(_abi.load().uha_sampled_index_create_device(
+                device, self._metric, ctypes.byref(rows._struct()), *sample_args))
+        else:
+            _check(_abi.load().uha_sampled_index_create(
+                device, self._metric, _ptr(rows), rows.shape[0], rows.shape[1],
+                *sample_args))
         self._adopt(handle, rows.shape[1], rows.shape[0])
         self.coordinate_sample = sample
 
@@ -699,10 +772,10 @@ class CudaFlatL2AnnIndex(CudaSampledCoordinateL2AnnIndex):
                  device: int = 0,
                  probability_execution_policy: ExecutionPolicy = ExecutionPolicy.gpu_fp32,
                  *, importance_probabilities=None):
-        rows = _matrix(input)
+        rows = _rows_input(input)
         if importance_probabilities is None:
             importance_probabilities = _probabilities_for(
-                _abi.L2, rows, probability_execution_policy, device)
+                _abi.L2, _matrix(rows), probability_execution_policy, device)
         super().__init__(rows, importance_probabilities, repetitions, random_engine,
                          device)
 
@@ -716,10 +789,10 @@ class CudaFlatL1AnnIndex(CudaSampledCoordinateL1AnnIndex):
                  device: int = 0,
                  probability_execution_policy: ExecutionPolicy = ExecutionPolicy.sequential,
                  *, importance_probabilities=None):
-        rows = _matrix(input)
+        rows = _rows_input(input)
         if importance_probabilities is None:
             importance_probabilities = _probabilities_for(
-                _abi.L1, rows, probability_execution_policy, device)
+                _abi.L1, _matrix(rows), probability_execution_policy, device)
         super().__init__(rows, importance_probabilities, repetitions, random_engine,
                          device)
 
@@ -731,7 +804,7 @@ class _CudaHierarchicalIndex(_CudaIndex):
                  random_engine=None, device: int = 0,
                  probability_execution_policy: Optional[ExecutionPolicy] = None, *,
                  importance_probabilities=None, coordinate_sample=None):
-        rows = _matrix(input)
+        rows = _rows_input(input)
         if rows.shape[0] == 0:
             raise InvalidArgument(
                 "hierarchical index expects at least one representative")
@@ -746,7 +819,7 @@ class _CudaHierarchicalIndex(_CudaIndex):
         else:
             if importance_probabilities is None:
                 policy = probability_execution_policy or self._default_policy
-                importance_probabilities = _probabilities_for(self._metric, rows,
+                importance_probabilities = _probabilities_for(self._metric, _matrix(rows),
                                                               policy, device)
             sample = _resolve_sample(rows, importance_probabilities, repetitions,
                                      random_engine, None)
@@ -756,11 +829,16 @@ class _CudaHierarchicalIndex(_CudaIndex):
         draw = build_jl_matrix if self._metric == _abi.L2 else build_cauchy_matrix
         matrix = draw(sample, p, random_engine)
         handle = ctypes.c_void_p()
-        _check(_abi.load().uha_hierarchical_index_create(
-            device, self._metric, _ptr(rows), rows.shape[0], rows.shape[1],
-            _ptr(sample.source_columns), _ptr(sample.multiplicities),
-            _ptr(sample.inverse_probabilities), len(sample), _ptr(matrix), p,
-            ctypes.byref(handle)))
+        sample_args = (_ptr(sample.source_columns), _ptr(sample.multiplicities),
+                       _ptr(sample.inverse_probabilities), len(sample), _ptr(matrix), p,
+                       ctypes.byref(handle))
+        if isinstance(rows, DeviceMatrix):
+            _check(_abi.load().uha_hierarchical_index_create_device(
+                device, self._metric, ctypes.byref(rows._struct()), *sample_args))
+        else:
+            _check(_abi.load().uha_hierarchical_index_create(
+                device, self._metric, _ptr(rows), rows.shape[0], rows.shape[1],
+                *sample_args))
         self._adopt(handle, rows.shape[1], rows.shape[0])
         self.coordinate_sample = sample
         self.projection = matrix

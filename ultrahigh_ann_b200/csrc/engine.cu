@@ -71,6 +71,70 @@ void validate_rows(const float* rows, uint64_t r, uint64_t d)
             "representative matrix must not be null");
 }
 
+// Where an index's representative matrix comes from: a host binary32 r x d
+// matrix, or a matrix already on the index's device.
+struct RowSource {
+    const float* host = nullptr;
+    const uha_device_matrix* device = nullptr;
+};
+
+void validate_device_matrix(const uha_device_matrix* m)
+{
+    require(m != nullptr, UHA_INVALID_ARGUMENT, "device matrix must not be null");
+    require(m->type == UHA_VALUES_F32 || m->type == UHA_VALUES_BF16,
+            UHA_INVALID_ARGUMENT, "unknown device matrix value type");
+    require(m->rows != 0, UHA_INVALID_ARGUMENT,
+            "CUDA index expects at least one representative");
+    require(m->rows <= kMaxExtent && m->columns <= kMaxExtent, UHA_LENGTH_ERROR,
+            "CUDA index dimensions exceed the device grid limits");
+    require(m->row_stride >= m->columns, UHA_INVALID_ARGUMENT,
+            "device matrix row stride is shorter than a row");
+    checked_mul(m->rows, m->row_stride, "representative matrix");
+    require(m->data != nullptr || m->columns == 0, UHA_INVALID_ARGUMENT,
+            "representative matrix must not be null");
+    const uint64_t element = m->type == UHA_VALUES_BF16 ? 2 : 4;
+    require(reinterpret_cast<uintptr_t>(m->data) % element == 0, UHA_INVALID_ARGUMENT,
+            "device matrix is not aligned to its element size");
+}
+
+// After select_device: the matrix must be memory of that device.
+void require_on_device(const uha_device_matrix* m, int device)
+{
+    if (m->data == nullptr) {
+        return;
+    }
+    cudaPointerAttributes a{};
+    const cudaError_t e = cudaPointerGetAttributes(&a, m->data);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+    }
+    require(e == cudaSuccess &&
+                (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) &&
+                a.device == device,
+            UHA_INVALID_ARGUMENT, "device matrix is not memory of the index's device");
+}
+
+// Gathers columns (nullptr: 0..k-1) of a device-resident source into the
+// r x padded layout `out`, times `scales` when given; returns the first
+// non-finite source / scaled value's r * k + i (~0 when none).
+std::pair<uint64_t, uint64_t> gather_device_source(const uha_device_matrix* m,
+                                                   const uint32_t* columns,
+                                                   const float* scales, uint64_t k,
+                                                   float* out, uint64_t padded)
+{
+    DeviceBuffer<unsigned long long> bad(2);
+    check_cuda(cudaMemset(bad.get(), 0xFF, bad.bytes()), "cannot clear flag");
+    if (m->rows * padded != 0) {
+        uha::launch_gather_device_rows(m->data, m->type == UHA_VALUES_BF16, m->row_stride,
+                                       m->rows, columns, scales, k, out, padded, bad.get(),
+                                       nullptr);
+    }
+    unsigned long long host[2] = {0, 0};
+    check_cuda(cudaMemcpy(host, bad.get(), sizeof(host), cudaMemcpyDeviceToHost),
+               "device row gather kernel failed");
+    return {host[0], host[1]};
+}
+
 // Uploads a host r x d matrix into the padded r x pd device layout.
 void upload_padded(DeviceBuffer<float>& dst, const float* src, uint64_t r,
                    uint64_t d, uint64_t pd)
@@ -230,17 +294,17 @@ extern "C" uha_status uha_device_info_get(int device, uha_device_info* out)
 
 // ----------------------------------------------------------------- indexes
 
-extern "C" uha_status uha_exact_index_create(int device, uha_metric metric,
-                                             const float* rows,
-                                             uint64_t row_count,
-                                             uint64_t dimension,
-                                             uha_index** out)
+namespace {
+
+void create_exact_index(int device, uha_metric metric, const RowSource& src,
+                        uint64_t row_count, uint64_t dimension, uha_index** out)
 {
-    return guarded([&] {
-        require(out != nullptr, UHA_INVALID_ARGUMENT,
-                "output pointer must not be null");
-        require(metric == UHA_L2 || metric == UHA_L1, UHA_INVALID_ARGUMENT,
-                "unknown metric");
+    require(out != nullptr, UHA_INVALID_ARGUMENT,
+            "output pointer must not be null");
+    require(metric == UHA_L2 || metric == UHA_L1, UHA_INVALID_ARGUMENT,
+            "unknown metric");
+    if (src.host != nullptr || src.device == nullptr) {
+        const float* rows = src.host;
         validate_rows(rows, row_count, dimension);
         const uint64_t total = row_count * dimension;
         for (uint64_t i = 0; i < total; ++i) {
@@ -248,31 +312,69 @@ extern "C" uha_status uha_exact_index_create(int device, uha_metric metric,
                 fail(UHA_INVALID_ARGUMENT, "representatives must be finite");
             }
         }
-        auto index = std::make_unique<uha_index>();
-        select_device(*index, device);
-        DeviceGuard guard(device);
-        index->kind = IndexKind::exact;
-        index->metric = metric;
-        index->rows = row_count;
-        index->dimension = dimension;
-        index->scan_dim = dimension;
-        index->padded_dim = uha::round_up(dimension, kColumnAlign);
-        require(index->padded_dim <= kMaxExtent, UHA_LENGTH_ERROR,
-                "CUDA index dimensions exceed the device grid limits");
-        upload_padded(index->scan_rows, rows, row_count, dimension,
+    } else {
+        validate_device_matrix(src.device);
+    }
+    auto index = std::make_unique<uha_index>();
+    select_device(*index, device);
+    DeviceGuard guard(device);
+    index->kind = IndexKind::exact;
+    index->metric = metric;
+    index->rows = row_count;
+    index->dimension = dimension;
+    index->scan_dim = dimension;
+    index->padded_dim = uha::round_up(dimension, kColumnAlign);
+    require(index->padded_dim <= kMaxExtent, UHA_LENGTH_ERROR,
+            "CUDA index dimensions exceed the device grid limits");
+    if (src.device == nullptr) {
+        upload_padded(index->scan_rows, src.host, row_count, dimension,
                       index->padded_dim);
-        const uint64_t f = sizeof(float);
-        if (metric == UHA_L2) {
-            compute_row_norms(*index);
-            index->usage.index_payload_bytes =
-                row_count * dimension * f + row_count * f;
-        } else {
-            index->usage.index_payload_bytes = row_count * dimension * f;
+    } else {
+        require_on_device(src.device, device);
+        index->scan_rows.allocate(
+            checked_mul(row_count, index->padded_dim, "padded representative matrix"));
+        if (gather_device_source(src.device, nullptr, nullptr, dimension,
+                                 index->scan_rows.get(), index->padded_dim)
+                .first != ~0ull) {
+            fail(UHA_INVALID_ARGUMENT, "representatives must be finite");
         }
-        index->usage.query_workspace_payload_bytes = 0;
-        index->usage.unique_query_coordinates = dimension;
-        index->usage.sampled_multiplicity = dimension;
-        *out = index.release();
+    }
+    const uint64_t f = sizeof(float);
+    if (metric == UHA_L2) {
+        compute_row_norms(*index);
+        index->usage.index_payload_bytes =
+            row_count * dimension * f + row_count * f;
+    } else {
+        index->usage.index_payload_bytes = row_count * dimension * f;
+    }
+    index->usage.query_workspace_payload_bytes = 0;
+    index->usage.unique_query_coordinates = dimension;
+    index->usage.sampled_multiplicity = dimension;
+    *out = index.release();
+}
+
+}  // namespace
+
+extern "C" uha_status uha_exact_index_create(int device, uha_metric metric,
+                                             const float* rows,
+                                             uint64_t row_count,
+                                             uint64_t dimension,
+                                             uha_index** out)
+{
+    return guarded([&] {
+        create_exact_index(device, metric, RowSource{rows, nullptr}, row_count, dimension,
+                           out);
+    });
+}
+
+extern "C" uha_status uha_exact_index_create_device(int device, uha_metric metric,
+                                                    const uha_device_matrix* rows,
+                                                    uha_index** out)
+{
+    return guarded([&] {
+        require(rows != nullptr, UHA_INVALID_ARGUMENT, "device matrix must not be null");
+        create_exact_index(device, metric, RowSource{nullptr, rows}, rows->rows,
+                           rows->columns, out);
     });
 }
 
@@ -328,134 +430,180 @@ extern "C" uha_status uha_weighted_l1_index_create(int device,
     });
 }
 
+namespace {
+
+void create_sampled_index(int device, uha_metric metric, const RowSource& src,
+                          uint64_t row_count, uint64_t dimension,
+                          const uint64_t* columns, const uint64_t* multiplicities,
+                          const double* inverse_probabilities, uint64_t sample_size,
+                          uha_index** out)
+{
+    const float* rows = src.host;
+    require(out != nullptr, UHA_INVALID_ARGUMENT,
+            "output pointer must not be null");
+    require(metric == UHA_L2 || metric == UHA_L1, UHA_INVALID_ARGUMENT,
+            "unknown metric");
+    if (src.device == nullptr) {
+        validate_rows(rows, row_count, dimension);
+    } else {
+        validate_device_matrix(src.device);
+    }
+    require(sample_size == 0 ||
+                (columns != nullptr && multiplicities != nullptr &&
+                 inverse_probabilities != nullptr),
+            UHA_INVALID_ARGUMENT, "coordinate sample must not be null");
+    require(sample_size <= kMaxExtent, UHA_LENGTH_ERROR,
+            "coordinate sample exceeds the device grid limits");
+    uint64_t multiplicity_sum = 0;
+    std::vector<uint32_t> cols(sample_size);
+    std::vector<float> scales(sample_size);
+    std::vector<float> w32(uha::round_up(sample_size, kColumnAlign), 0.0f);
+    std::vector<double> w64(sample_size);
+    for (uint64_t i = 0; i < sample_size; ++i) {
+        if (columns[i] >= dimension) {
+            fail(UHA_OUT_OF_RANGE, "sampled column index out of range");
+        }
+        if (multiplicities[i] == 0 ||
+            !std::isfinite(inverse_probabilities[i]) ||
+            inverse_probabilities[i] <= 0.0) {
+            fail(UHA_INVALID_ARGUMENT,
+                 "sampled columns require positive finite weights");
+        }
+        if (multiplicity_sum > UINT64_MAX - multiplicities[i]) {
+            fail(UHA_LENGTH_ERROR, "sampled multiplicity overflows");
+        }
+        multiplicity_sum += multiplicities[i];
+        // weight = double(multiplicity) * (1/p), as in
+        // l2_coordinate_embedding.cpp:56-57 and l1_coordinate_embedding.cpp:53-54
+        const double weight = static_cast<double>(multiplicities[i]) *
+                              inverse_probabilities[i];
+        if (metric == UHA_L2) {
+            const float scale = static_cast<float>(std::sqrt(weight));
+            if (!std::isfinite(weight) || weight <= 0.0 ||
+                !std::isfinite(scale) || scale <= 0.0f) {
+                fail(UHA_INVALID_ARGUMENT,
+                     "sampled coordinate weight is not representable in "
+                     "float32");
+            }
+            scales[i] = scale;
+        } else {
+            const float fw = static_cast<float>(weight);
+            if (!std::isfinite(weight) || weight <= 0.0 ||
+                !std::isfinite(fw) || fw <= 0.0f) {
+                fail(UHA_INVALID_ARGUMENT,
+                     "sampled coordinate weight is not representable in "
+                     "float32");
+            }
+            w32[i] = fw;
+            w64[i] = weight;
+        }
+        cols[i] = static_cast<uint32_t>(columns[i]);
+    }
+    // Validate the sampled representative values (only sampled columns
+    // are part of the index) and, for L2, their scaled binary32 values;
+    // a device-resident matrix is validated by its gather below.
+    for (uint64_t r = 0; src.device == nullptr && r < row_count; ++r) {
+        const float* row = rows + r * dimension;
+        for (uint64_t i = 0; i < sample_size; ++i) {
+            const float v = row[cols[i]];
+            if (!std::isfinite(v)) {
+                fail(UHA_INVALID_ARGUMENT,
+                     "sampled representatives must be finite");
+            }
+            if (metric == UHA_L2 && !std::isfinite(v * scales[i])) {
+                fail(UHA_INVALID_ARGUMENT,
+                     "transformed representatives must be finite");
+            }
+        }
+    }
+
+    auto index = std::make_unique<uha_index>();
+    select_device(*index, device);
+    DeviceGuard guard(device);
+    index->kind = IndexKind::sampled;
+    index->metric = metric;
+    index->rows = row_count;
+    index->dimension = dimension;
+    index->scan_dim = sample_size;
+    index->sample_size = sample_size;
+    index->sampled_multiplicity = multiplicity_sum;
+    index->padded_dim = uha::round_up(sample_size, kColumnAlign);
+    upload(index->columns, cols.data(), cols.size());
+    if (metric == UHA_L2) {
+        upload(index->scales, scales.data(), scales.size());
+    } else {
+        upload(index->weights32, w32.data(), w32.size());
+        upload(index->weights64, w64.data(), w64.size());
+    }
+    // Gather (and scale) the sampled columns of the rows on the device.
+    if (src.device != nullptr) {
+        require_on_device(src.device, device);
+        index->scan_rows.allocate(row_count * index->padded_dim);
+        const auto bad = gather_device_source(
+            src.device, index->columns.get(),
+            metric == UHA_L2 ? index->scales.get() : nullptr, sample_size,
+            index->scan_rows.get(), index->padded_dim);
+        if (bad.first != ~0ull || bad.second != ~0ull) {
+            fail(UHA_INVALID_ARGUMENT, bad.first <= bad.second
+                                           ? "sampled representatives must be finite"
+                                           : "transformed representatives must be finite");
+        }
+    } else if (index->padded_dim != 0) {
+        DeviceBuffer<float> source(checked_mul(row_count, dimension,
+                                               "representative matrix"));
+        check_cuda(cudaMemcpy(source.get(), rows, source.bytes(),
+                              cudaMemcpyHostToDevice),
+                   "cannot copy representatives to the CUDA device");
+        index->scan_rows.allocate(row_count * index->padded_dim);
+        uha::launch_gather_rows(source.get(), row_count, dimension,
+                                index->columns.get(),
+                                metric == UHA_L2 ? index->scales.get()
+                                                 : nullptr,
+                                sample_size, index->scan_rows.get(),
+                                index->padded_dim, nullptr);
+        check_cuda(cudaDeviceSynchronize(), "row gather kernel failed");
+    }
+    const uint64_t f = sizeof(float);
+    const uint64_t k = sample_size;
+    if (metric == UHA_L2) {
+        compute_row_norms(*index);
+        index->usage.index_payload_bytes = row_count * k * f +
+                                           row_count * f +
+                                           k * sizeof(std::size_t) + k * f;
+    } else {
+        index->usage.index_payload_bytes =
+            row_count * k * f + k * f + k * sizeof(std::size_t);
+    }
+    index->usage.query_workspace_payload_bytes = 0;
+    index->usage.unique_query_coordinates = k;
+    index->usage.sampled_multiplicity = multiplicity_sum;
+    *out = index.release();
+}
+
+}  // namespace
+
 extern "C" uha_status uha_sampled_index_create(
     int device, uha_metric metric, const float* rows, uint64_t row_count,
     uint64_t dimension, const uint64_t* columns, const uint64_t* multiplicities,
     const double* inverse_probabilities, uint64_t sample_size, uha_index** out)
 {
     return guarded([&] {
-        require(out != nullptr, UHA_INVALID_ARGUMENT,
-                "output pointer must not be null");
-        require(metric == UHA_L2 || metric == UHA_L1, UHA_INVALID_ARGUMENT,
-                "unknown metric");
-        validate_rows(rows, row_count, dimension);
-        require(sample_size == 0 ||
-                    (columns != nullptr && multiplicities != nullptr &&
-                     inverse_probabilities != nullptr),
-                UHA_INVALID_ARGUMENT, "coordinate sample must not be null");
-        require(sample_size <= kMaxExtent, UHA_LENGTH_ERROR,
-                "coordinate sample exceeds the device grid limits");
-        uint64_t multiplicity_sum = 0;
-        std::vector<uint32_t> cols(sample_size);
-        std::vector<float> scales(sample_size);
-        std::vector<float> w32(uha::round_up(sample_size, kColumnAlign), 0.0f);
-        std::vector<double> w64(sample_size);
-        for (uint64_t i = 0; i < sample_size; ++i) {
-            if (columns[i] >= dimension) {
-                fail(UHA_OUT_OF_RANGE, "sampled column index out of range");
-            }
-            if (multiplicities[i] == 0 ||
-                !std::isfinite(inverse_probabilities[i]) ||
-                inverse_probabilities[i] <= 0.0) {
-                fail(UHA_INVALID_ARGUMENT,
-                     "sampled columns require positive finite weights");
-            }
-            if (multiplicity_sum > UINT64_MAX - multiplicities[i]) {
-                fail(UHA_LENGTH_ERROR, "sampled multiplicity overflows");
-            }
-            multiplicity_sum += multiplicities[i];
-            // weight = double(multiplicity) * (1/p), as in
-            // l2_coordinate_embedding.cpp:56-57 and l1_coordinate_embedding.cpp:53-54
-            const double weight = static_cast<double>(multiplicities[i]) *
-                                  inverse_probabilities[i];
-            if (metric == UHA_L2) {
-                const float scale = static_cast<float>(std::sqrt(weight));
-                if (!std::isfinite(weight) || weight <= 0.0 ||
-                    !std::isfinite(scale) || scale <= 0.0f) {
-                    fail(UHA_INVALID_ARGUMENT,
-                         "sampled coordinate weight is not representable in "
-                         "float32");
-                }
-                scales[i] = scale;
-            } else {
-                const float fw = static_cast<float>(weight);
-                if (!std::isfinite(weight) || weight <= 0.0 ||
-                    !std::isfinite(fw) || fw <= 0.0f) {
-                    fail(UHA_INVALID_ARGUMENT,
-                         "sampled coordinate weight is not representable in "
-                         "float32");
-                }
-                w32[i] = fw;
-                w64[i] = weight;
-            }
-            cols[i] = static_cast<uint32_t>(columns[i]);
-        }
-        // Validate the sampled representative values (only sampled columns
-        // are part of the index) and, for L2, their scaled binary32 values.
-        for (uint64_t r = 0; r < row_count; ++r) {
-            const float* row = rows + r * dimension;
-            for (uint64_t i = 0; i < sample_size; ++i) {
-                const float v = row[cols[i]];
-                if (!std::isfinite(v)) {
-                    fail(UHA_INVALID_ARGUMENT,
-                         "sampled representatives must be finite");
-                }
-                if (metric == UHA_L2 && !std::isfinite(v * scales[i])) {
-                    fail(UHA_INVALID_ARGUMENT,
-                         "transformed representatives must be finite");
-                }
-            }
-        }
+        create_sampled_index(device, metric, RowSource{rows, nullptr}, row_count, dimension,
+                             columns, multiplicities, inverse_probabilities, sample_size,
+                             out);
+    });
+}
 
-        auto index = std::make_unique<uha_index>();
-        select_device(*index, device);
-        DeviceGuard guard(device);
-        index->kind = IndexKind::sampled;
-        index->metric = metric;
-        index->rows = row_count;
-        index->dimension = dimension;
-        index->scan_dim = sample_size;
-        index->sample_size = sample_size;
-        index->sampled_multiplicity = multiplicity_sum;
-        index->padded_dim = uha::round_up(sample_size, kColumnAlign);
-        upload(index->columns, cols.data(), cols.size());
-        if (metric == UHA_L2) {
-            upload(index->scales, scales.data(), scales.size());
-        } else {
-            upload(index->weights32, w32.data(), w32.size());
-            upload(index->weights64, w64.data(), w64.size());
-        }
-        // Gather (and scale) the sampled columns of the rows on the device.
-        if (index->padded_dim != 0) {
-            DeviceBuffer<float> source(checked_mul(row_count, dimension,
-                                                   "representative matrix"));
-            check_cuda(cudaMemcpy(source.get(), rows, source.bytes(),
-                                  cudaMemcpyHostToDevice),
-                       "cannot copy representatives to the CUDA device");
-            index->scan_rows.allocate(row_count * index->padded_dim);
-            uha::launch_gather_rows(source.get(), row_count, dimension,
-                                    index->columns.get(),
-                                    metric == UHA_L2 ? index->scales.get()
-                                                     : nullptr,
-                                    sample_size, index->scan_rows.get(),
-                                    index->padded_dim, nullptr);
-            check_cuda(cudaDeviceSynchronize(), "row gather kernel failed");
-        }
-        const uint64_t f = sizeof(float);
-        const uint64_t k = sample_size;
-        if (metric == UHA_L2) {
-            compute_row_norms(*index);
-            index->usage.index_payload_bytes = row_count * k * f +
-                                               row_count * f +
-                                               k * sizeof(std::size_t) + k * f;
-        } else {
-            index->usage.index_payload_bytes =
-                row_count * k * f + k * f + k * sizeof(std::size_t);
-        }
-        index->usage.query_workspace_payload_bytes = 0;
-        index->usage.unique_query_coordinates = k;
-        index->usage.sampled_multiplicity = multiplicity_sum;
-        *out = index.release();
+extern "C" uha_status uha_sampled_index_create_device(
+    int device, uha_metric metric, const uha_device_matrix* rows, const uint64_t* columns,
+    const uint64_t* multiplicities, const double* inverse_probabilities,
+    uint64_t sample_size, uha_index** out)
+{
+    return guarded([&] {
+        require(rows != nullptr, UHA_INVALID_ARGUMENT, "device matrix must not be null");
+        create_sampled_index(device, metric, RowSource{nullptr, rows}, rows->rows,
+                             rows->columns, columns, multiplicities, inverse_probabilities,
+                             sample_size, out);
     });
 }
 
@@ -479,6 +627,161 @@ double projection_error_per_abs(uint64_t k)
            (1 - g32b);
 }
 
+void create_hierarchical_index(int device, uha_metric metric, const RowSource& src,
+                               uint64_t row_count, uint64_t dimension,
+                               const uint64_t* columns, const uint64_t* multiplicities,
+                               const double* inverse_probabilities, uint64_t sample_size,
+                               const double* projection, uint64_t projection_dimension,
+                               uha_index** out)
+{
+    const float* rows = src.host;
+    require(out != nullptr, UHA_INVALID_ARGUMENT,
+            "output pointer must not be null");
+    require(metric == UHA_L2 || metric == UHA_L1, UHA_INVALID_ARGUMENT,
+            "unknown metric");
+    if (src.device == nullptr) {
+        validate_rows(rows, row_count, dimension);
+    } else {
+        validate_device_matrix(src.device);
+    }
+    const uint64_t k = sample_size;
+    const uint64_t p = projection_dimension;
+    require(p != 0, UHA_INVALID_ARGUMENT,
+            "projection_dimension has to be a positive integer");
+    if (k == 0 && row_count > 1) {
+        fail(UHA_RUNTIME_ERROR, "importance sampling selected no coordinates");
+    }
+    require(k == 0 || (columns != nullptr && multiplicities != nullptr &&
+                       inverse_probabilities != nullptr &&
+                       projection != nullptr),
+            UHA_INVALID_ARGUMENT, "coordinate sample must not be null");
+    require(k <= kMaxExtent, UHA_LENGTH_ERROR,
+            "coordinate sample exceeds the device grid limits");
+    require(p <= (metric == UHA_L2 ? 16384u : 1024u), UHA_LENGTH_ERROR,
+            "projection dimension exceeds the supported maximum "
+            "(16384 for L2, 1024 for L1)");
+    checked_mul(p, k, "projection matrix");
+    uint64_t multiplicity_sum = 0;
+    std::vector<uint32_t> cols(k);
+    for (uint64_t i = 0; i < k; ++i) {
+        if (columns[i] >= dimension) {
+            fail(UHA_OUT_OF_RANGE, "sampled column index out of range");
+        }
+        if (multiplicities[i] == 0 ||
+            !std::isfinite(inverse_probabilities[i]) ||
+            inverse_probabilities[i] <= 0.0) {
+            fail(UHA_INVALID_ARGUMENT,
+                 "sampled columns require positive finite weights");
+        }
+        if (multiplicity_sum > UINT64_MAX - multiplicities[i]) {
+            fail(UHA_LENGTH_ERROR, "sampled multiplicity overflows");
+        }
+        multiplicity_sum += multiplicities[i];
+        cols[i] = static_cast<uint32_t>(columns[i]);
+    }
+    const uint64_t kp = uha::round_up(k, kColumnAlign);
+    const uint64_t pp = uha::round_up(p, kColumnAlign);
+    std::vector<float> proj32(p * kp, 0.0f);
+    for (uint64_t j = 0; j < p; ++j) {
+        for (uint64_t i = 0; i < k; ++i) {
+            const double c = projection[j * k + i];
+            const float f = static_cast<float>(c);
+            if (!std::isfinite(c)) {
+                fail(UHA_OVERFLOW_ERROR, "projection coefficient is not finite");
+            }
+            if (!std::isfinite(f)) {
+                fail(UHA_OVERFLOW_ERROR,
+                     "binary32 projection coefficient is not finite");
+            }
+            proj32[j * kp + i] = f;
+        }
+    }
+
+    auto index = std::make_unique<uha_index>();
+    select_device(*index, device);
+    DeviceGuard guard(device);
+    index->kind = IndexKind::hierarchical;
+    index->metric = metric;
+    index->rows = row_count;
+    index->dimension = dimension;
+    index->sample_size = k;
+    index->padded_sample = kp;
+    index->sampled_multiplicity = multiplicity_sum;
+    index->projection_dimension = p;
+    index->scan_dim = p;
+    index->padded_dim = pp;
+    upload(index->columns, cols.data(), cols.size());
+    upload(index->projection64, projection, p * k);
+    upload(index->projection32, proj32.data(), proj32.size());
+
+    DeviceBuffer<int> bad(1);
+    check_cuda(cudaMemset(bad.get(), 0, sizeof(int)), "cannot clear flag");
+    DeviceBuffer<float> sampled(std::max<uint64_t>(1, row_count * kp));
+    check_cuda(cudaMemset(sampled.get(), 0, sampled.bytes()),
+               "cannot clear sampled rows");
+    if (k != 0 && src.device != nullptr) {
+        // the reference does not validate the sampled values of a
+        // hierarchy; a non-finite one fails as a non-finite projection
+        require_on_device(src.device, device);
+        gather_device_source(src.device, index->columns.get(), nullptr, k,
+                             sampled.get(), kp);
+    } else if (k != 0) {
+        DeviceBuffer<float> source(checked_mul(row_count, dimension,
+                                               "representative matrix"));
+        check_cuda(cudaMemcpy(source.get(), rows, source.bytes(),
+                              cudaMemcpyHostToDevice),
+                   "cannot copy representatives to the CUDA device");
+        uha::launch_gather_rows(source.get(), row_count, dimension,
+                                index->columns.get(), nullptr, k,
+                                sampled.get(), kp, nullptr);
+    }
+    index->rows64.allocate(row_count * p);
+    uha::launch_project_rows64(sampled.get(), row_count, kp, k,
+                               index->projection64.get(), p,
+                               index->rows64.get(), bad.get(), nullptr);
+    index->scan_rows.allocate(row_count * pp);
+    index->row_err.allocate(row_count);
+    uha::launch_narrow_rows(index->rows64.get(), row_count, p,
+                            index->scan_rows.get(), pp, index->row_err.get(),
+                            metric == UHA_L2, bad.get(), nullptr);
+    int host_bad = 0;
+    check_cuda(cudaMemcpy(&host_bad, bad.get(), sizeof(int),
+                          cudaMemcpyDeviceToHost),
+               "row projection failed");
+    {
+        std::vector<float> err(row_count);
+        check_cuda(cudaMemcpy(err.data(), index->row_err.get(), row_count * sizeof(float),
+                              cudaMemcpyDeviceToHost),
+                   "row projection failed");
+        index->row_err_max = 0.f;
+        for (float e : err) {
+            index->row_err_max = std::isnan(e) ? std::numeric_limits<float>::infinity()
+                                               : std::max(index->row_err_max, e);
+        }
+    }
+    if (host_bad & 1) {
+        fail(UHA_OVERFLOW_ERROR, "projected representatives is not finite");
+    }
+    if (host_bad & 2) {
+        fail(UHA_OVERFLOW_ERROR,
+             "binary32 projected representative is not finite");
+    }
+    const uint64_t f = sizeof(float);
+    const uint64_t column_bytes = 2 * sizeof(uint64_t) + sizeof(double);
+    if (metric == UHA_L2) {
+        compute_row_norms(*index);
+        index->usage.index_payload_bytes = row_count * p * f + row_count * f +
+                                           k * column_bytes + p * k * f;
+    } else {
+        index->usage.index_payload_bytes =
+            k * column_bytes + p * k * f + row_count * p * f;
+    }
+    index->usage.query_workspace_payload_bytes = 0;
+    index->usage.unique_query_coordinates = k;
+    index->usage.sampled_multiplicity = multiplicity_sum;
+    *out = index.release();
+}
+
 }  // namespace
 
 extern "C" uha_status uha_hierarchical_index_create(
@@ -488,141 +791,25 @@ extern "C" uha_status uha_hierarchical_index_create(
     const double* projection, uint64_t projection_dimension, uha_index** out)
 {
     return guarded([&] {
-        require(out != nullptr, UHA_INVALID_ARGUMENT,
-                "output pointer must not be null");
-        require(metric == UHA_L2 || metric == UHA_L1, UHA_INVALID_ARGUMENT,
-                "unknown metric");
-        validate_rows(rows, row_count, dimension);
-        const uint64_t k = sample_size;
-        const uint64_t p = projection_dimension;
-        require(p != 0, UHA_INVALID_ARGUMENT,
-                "projection_dimension has to be a positive integer");
-        if (k == 0 && row_count > 1) {
-            fail(UHA_RUNTIME_ERROR, "importance sampling selected no coordinates");
-        }
-        require(k == 0 || (columns != nullptr && multiplicities != nullptr &&
-                           inverse_probabilities != nullptr &&
-                           projection != nullptr),
-                UHA_INVALID_ARGUMENT, "coordinate sample must not be null");
-        require(k <= kMaxExtent, UHA_LENGTH_ERROR,
-                "coordinate sample exceeds the device grid limits");
-        require(p <= (metric == UHA_L2 ? 16384u : 1024u), UHA_LENGTH_ERROR,
-                "projection dimension exceeds the supported maximum "
-                "(16384 for L2, 1024 for L1)");
-        checked_mul(p, k, "projection matrix");
-        uint64_t multiplicity_sum = 0;
-        std::vector<uint32_t> cols(k);
-        for (uint64_t i = 0; i < k; ++i) {
-            if (columns[i] >= dimension) {
-                fail(UHA_OUT_OF_RANGE, "sampled column index out of range");
-            }
-            if (multiplicities[i] == 0 ||
-                !std::isfinite(inverse_probabilities[i]) ||
-                inverse_probabilities[i] <= 0.0) {
-                fail(UHA_INVALID_ARGUMENT,
-                     "sampled columns require positive finite weights");
-            }
-            if (multiplicity_sum > UINT64_MAX - multiplicities[i]) {
-                fail(UHA_LENGTH_ERROR, "sampled multiplicity overflows");
-            }
-            multiplicity_sum += multiplicities[i];
-            cols[i] = static_cast<uint32_t>(columns[i]);
-        }
-        const uint64_t kp = uha::round_up(k, kColumnAlign);
-        const uint64_t pp = uha::round_up(p, kColumnAlign);
-        std::vector<float> proj32(p * kp, 0.0f);
-        for (uint64_t j = 0; j < p; ++j) {
-            for (uint64_t i = 0; i < k; ++i) {
-                const double c = projection[j * k + i];
-                const float f = static_cast<float>(c);
-                if (!std::isfinite(c)) {
-                    fail(UHA_OVERFLOW_ERROR, "projection coefficient is not finite");
-                }
-                if (!std::isfinite(f)) {
-                    fail(UHA_OVERFLOW_ERROR,
-                         "binary32 projection coefficient is not finite");
-                }
-                proj32[j * kp + i] = f;
-            }
-        }
+        create_hierarchical_index(device, metric, RowSource{rows, nullptr}, row_count,
+                                  dimension, columns, multiplicities,
+                                  inverse_probabilities, sample_size, projection,
+                                  projection_dimension, out);
+    });
+}
 
-        auto index = std::make_unique<uha_index>();
-        select_device(*index, device);
-        DeviceGuard guard(device);
-        index->kind = IndexKind::hierarchical;
-        index->metric = metric;
-        index->rows = row_count;
-        index->dimension = dimension;
-        index->sample_size = k;
-        index->padded_sample = kp;
-        index->sampled_multiplicity = multiplicity_sum;
-        index->projection_dimension = p;
-        index->scan_dim = p;
-        index->padded_dim = pp;
-        upload(index->columns, cols.data(), cols.size());
-        upload(index->projection64, projection, p * k);
-        upload(index->projection32, proj32.data(), proj32.size());
-
-        DeviceBuffer<int> bad(1);
-        check_cuda(cudaMemset(bad.get(), 0, sizeof(int)), "cannot clear flag");
-        DeviceBuffer<float> sampled(std::max<uint64_t>(1, row_count * kp));
-        check_cuda(cudaMemset(sampled.get(), 0, sampled.bytes()),
-                   "cannot clear sampled rows");
-        if (k != 0) {
-            DeviceBuffer<float> source(checked_mul(row_count, dimension,
-                                                   "representative matrix"));
-            check_cuda(cudaMemcpy(source.get(), rows, source.bytes(),
-                                  cudaMemcpyHostToDevice),
-                       "cannot copy representatives to the CUDA device");
-            uha::launch_gather_rows(source.get(), row_count, dimension,
-                                    index->columns.get(), nullptr, k,
-                                    sampled.get(), kp, nullptr);
-        }
-        index->rows64.allocate(row_count * p);
-        uha::launch_project_rows64(sampled.get(), row_count, kp, k,
-                                   index->projection64.get(), p,
-                                   index->rows64.get(), bad.get(), nullptr);
-        index->scan_rows.allocate(row_count * pp);
-        index->row_err.allocate(row_count);
-        uha::launch_narrow_rows(index->rows64.get(), row_count, p,
-                                index->scan_rows.get(), pp, index->row_err.get(),
-                                metric == UHA_L2, bad.get(), nullptr);
-        int host_bad = 0;
-        check_cuda(cudaMemcpy(&host_bad, bad.get(), sizeof(int),
-                              cudaMemcpyDeviceToHost),
-                   "row projection failed");
-        {
-            std::vector<float> err(row_count);
-            check_cuda(cudaMemcpy(err.data(), index->row_err.get(), row_count * sizeof(float),
-                                  cudaMemcpyDeviceToHost),
-                       "row projection failed");
-            index->row_err_max = 0.f;
-            for (float e : err) {
-                index->row_err_max = std::isnan(e) ? std::numeric_limits<float>::infinity()
-                                                   : std::max(index->row_err_max, e);
-            }
-        }
-        if (host_bad & 1) {
-            fail(UHA_OVERFLOW_ERROR, "projected representatives is not finite");
-        }
-        if (host_bad & 2) {
-            fail(UHA_OVERFLOW_ERROR,
-                 "binary32 projected representative is not finite");
-        }
-        const uint64_t f = sizeof(float);
-        const uint64_t column_bytes = 2 * sizeof(uint64_t) + sizeof(double);
-        if (metric == UHA_L2) {
-            compute_row_norms(*index);
-            index->usage.index_payload_bytes = row_count * p * f + row_count * f +
-                                               k * column_bytes + p * k * f;
-        } else {
-            index->usage.index_payload_bytes =
-                k * column_bytes + p * k * f + row_count * p * f;
-        }
-        index->usage.query_workspace_payload_bytes = 0;
-        index->usage.unique_query_coordinates = k;
-        index->usage.sampled_multiplicity = multiplicity_sum;
-        *out = index.release();
+extern "C" uha_status uha_hierarchical_index_create_device(
+    int device, uha_metric metric, const uha_device_matrix* rows, const uint64_t* columns,
+    const uint64_t* multiplicities, const double* inverse_probabilities,
+    uint64_t sample_size, const double* projection, uint64_t projection_dimension,
+    uha_index** out)
+{
+    return guarded([&] {
+        require(rows != nullptr, UHA_INVALID_ARGUMENT, "device matrix must not be null");
+        create_hierarchical_index(device, metric, RowSource{nullptr, rows}, rows->rows,
+                                  rows->columns, columns, multiplicities,
+                                  inverse_probabilities, sample_size, projection,
+                                  projection_dimension, out);
     });
 }
 

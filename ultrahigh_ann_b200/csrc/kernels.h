@@ -267,6 +267,14 @@ void launch_gather_rows(const float* source, uint64_t row_count, uint64_t dim,
                         const uint32_t* columns, const float* scales,
                         uint64_t sample_size, float* out, uint64_t padded_dim,
                         cudaStream_t stream);
+// Gather from a device-resident binary32 or BF16 matrix with a row stride
+// (columns == nullptr: column i); first_bad (nullable, two entries preset to
+// ~0) receives the first non-finite source / scaled value's r * k + i.
+void launch_gather_device_rows(const void* source, bool bf16, uint64_t stride,
+                               uint64_t row_count, const uint32_t* columns,
+                               const float* scales, uint64_t sample_size,
+                               float* out, uint64_t padded_dim,
+                               unsigned long long* first_bad, cudaStream_t stream);
 void launch_row_norms(const float* rows, uint64_t row_count,
                       uint64_t padded_dim, float* norms, cudaStream_t stream);
 

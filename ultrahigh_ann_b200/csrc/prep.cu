@@ -149,6 +149,51 @@ __global__ void gather_rows_kernel(const float* __restrict__ source,
     }
 }
 
+// Build-time gather from a device-resident matrix (binary32, or BF16 decoded
+// exactly to binary32) with a row stride: out[r][i] = source[r][column i]
+// (times scales[i] when given; columns == nullptr reads column i). When
+// first_bad is given, first_bad[0] / [1] receive the smallest r * k + i whose
+// source value / scaled value is not finite (the host validation's order).
+template <bool BF16>
+__global__ void gather_device_rows_kernel(const void* __restrict__ source,
+                                          uint64_t stride, uint64_t row_count,
+                                          const uint32_t* __restrict__ columns,
+                                          const float* __restrict__ scales,
+                                          uint64_t sample_size,
+                                          float* __restrict__ out,
+                                          uint64_t padded_dim,
+                                          unsigned long long* first_bad)
+{
+    const uint64_t total = row_count * padded_dim;
+    for (uint64_t idx = blockIdx.x * static_cast<uint64_t>(blockDim.x) +
+                        threadIdx.x;
+         idx < total; idx += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t r = idx / padded_dim;
+        const uint64_t i = idx - r * padded_dim;
+        float v = 0.f;
+        if (i < sample_size) {
+            const uint64_t at = r * stride + (columns != nullptr ? columns[i] : i);
+            if constexpr (BF16) {
+                const uint32_t bits = static_cast<const uint16_t*>(source)[at];
+                v = __uint_as_float(bits << 16);
+            } else {
+                v = static_cast<const float*>(source)[at];
+            }
+            const unsigned long long linear = r * sample_size + i;
+            if (first_bad != nullptr && !isfinite(v)) {
+                atomicMin(first_bad, linear);
+            }
+            if (scales != nullptr) {
+                v = __fmul_rn(v, scales[i]);
+                if (first_bad != nullptr && !isfinite(v)) {
+                    atomicMin(first_bad + 1, linear);
+                }
+            }
+        }
+        out[idx] = v;
+    }
+}
+
 uint32_t grid_for(uint64_t total)
 {
     const uint64_t blocks = (total + kThreads - 1) / kThreads;
@@ -239,6 +284,25 @@ void launch_gather_rows(const float* source, uint64_t row_count, uint64_t dim,
                          stream>>>(source, row_count, dim, columns, scales,
                                    sample_size, out, padded_dim);
     check_cuda(cudaGetLastError(), "cannot launch row gather kernel");
+}
+
+void launch_gather_device_rows(const void* source, bool bf16, uint64_t stride,
+                               uint64_t row_count, const uint32_t* columns,
+                               const float* scales, uint64_t sample_size,
+                               float* out, uint64_t padded_dim,
+                               unsigned long long* first_bad, cudaStream_t stream)
+{
+    const uint32_t grid = grid_for(row_count * padded_dim);
+    if (bf16) {
+        gather_device_rows_kernel<true><<<grid, kThreads, 0, stream>>>(
+            source, stride, row_count, columns, scales, sample_size, out, padded_dim,
+            first_bad);
+    } else {
+        gather_device_rows_kernel<false><<<grid, kThreads, 0, stream>>>(
+            source, stride, row_count, columns, scales, sample_size, out, padded_dim,
+            first_bad);
+    }
+    check_cuda(cudaGetLastError(), "cannot launch device row gather kernel");
 }
 
 void launch_row_norms(const float* rows, uint64_t row_count,

@@ -75,3 +75,54 @@ def row_dataset(rows: int = 7028, classes: int = 33, queries: int = 8192,
     q_labels = qrng.integers(0, classes, size=queries)
     q = _noisy(qrng, cent, q_labels, sigma)
     return Dataset(r, q, q_labels, row_labels)
+
+
+@dataclass
+class DeviceDataset:
+    rows: "object"          # r x d torch tensor on the device (float32 or bfloat16)
+    queries: "object"       # n x d float32 torch tensor on the device
+    query_class: np.ndarray
+    row_class: np.ndarray
+
+
+def device_row_dataset(rows: int, classes: int = 33, queries: int = 4096,
+                       d: int = TCGA_DIMENSION, sigma: float = 0.8,
+                       zero_fraction: float = 0.4, seed: int = 1,
+                       storage: str = "bfloat16", device: int = 0,
+                       chunk: int = 1024) -> DeviceDataset:
+    """The row-level workload generated on the device, for sizes whose host
+    matrix would not fit host memory (65,536 x 262,144 values): the same law
+    as row_dataset (class centroids drawn on the host with numpy, per-value
+    N(0, sigma^2) noise from torch's device generator, clipped at 0, masked
+    columns zero in the rows). Rows are stored as `storage` (BF16 rounds to nearest
+    even); queries hold the binary32 values of the same storage type, so
+    queries and rows share one value grid. Different random streams than
+    row_dataset: the values are not the same as a host dataset's."""
+    import torch
+
+    rng = np.random.default_rng([seed, 0])
+    cent, mask = _centroids(rng, classes, d, zero_fraction)
+    row_labels = rng.integers(0, classes, size=rows)
+    q_labels = np.random.default_rng([seed, 1]).integers(0, classes, size=queries)
+    dev = torch.device("cuda", device)
+    cent_t = torch.from_numpy(cent).to(dev)
+    keep = torch.from_numpy(~mask).to(dev)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    dtype = torch.bfloat16 if storage == "bfloat16" else torch.float32
+
+    def fill(out, labels, store_dtype, masked):
+        for s in range(0, labels.size, chunk):
+            e = min(labels.size, s + chunk)
+            lab = torch.from_numpy(labels[s:e]).to(dev)
+            block = torch.randn((e - s, d), generator=gen, device=dev)
+            block.mul_(sigma).add_(cent_t[lab]).clamp_(min=0.0)
+            if masked:
+                block.mul_(keep)
+            out[s:e] = block.to(store_dtype).to(out.dtype)
+        return out
+
+    r = fill(torch.empty((rows, d), dtype=dtype, device=dev), row_labels, dtype, True)
+    q = fill(torch.empty((queries, d), dtype=torch.float32, device=dev), q_labels, dtype,
+             False)
+    return DeviceDataset(r, q, q_labels, row_labels)
