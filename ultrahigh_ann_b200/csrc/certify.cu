@@ -25,26 +25,23 @@ namespace uha {
 namespace {
 
 constexpr int kFinalizeThreads = 256;
+constexpr int kArgminUnroll = 8;
 
 struct Bounds2 {
     float lower;
     float upper;
 };
 
-__device__ __forceinline__ Bounds2 bound_of(float d, const Bound& b,
-                                            uint32_t row, uint32_t q)
+// Bounds of a finite binary32 distance d given the row's error term e (row
+// plus query error; median: the pair's own error for a computed median;
+// unused in plain mode). Monotone: nondecreasing in d, nonincreasing in e.
+__device__ __forceinline__ Bounds2 bound_with(float d, const Bound& b, float e)
 {
     const float inf = __int_as_float(0x7f800000);
-    if (!(d <= FLT_MAX)) {
-        // binary32 overflow: no finite upper bound; every row below stays a
-        // candidate and the replay decides
-        return {0.f, inf};
-    }
     if (b.mode == BoundMode::plain) {
         const float err = __fadd_ru(__fmul_ru(b.rel, d), b.abs);
         return {fmaxf(0.f, __fsub_rd(d, err)), __fadd_ru(d, err)};
     }
-    const float e = __fadd_ru(b.row_err[row], b.query_err[q]);
     if (b.mode == BoundMode::median) {
         if (d < 0.f) {
             // a row the median scan set aside: binary32 median at least -d
@@ -64,6 +61,34 @@ __device__ __forceinline__ Bounds2 bound_of(float d, const Bound& b,
     const float lo = __fmul_rd(__fmul_rd(lo_root, lo_root), __fsub_rd(1.f, b.cpu_rel));
     const float hi = __fmul_ru(__fmul_ru(hi_root, hi_root), __fadd_ru(1.f, b.cpu_rel));
     return {fmaxf(0.f, __fsub_rd(lo, b.abs)), __fadd_ru(hi, b.abs)};
+}
+
+__device__ __forceinline__ Bounds2 bound_of(float d, const Bound& b,
+                                            uint32_t row, uint32_t q)
+{
+    if (!(d <= FLT_MAX)) {
+        // binary32 overflow: no finite upper bound; every row below stays a
+        // candidate and the replay decides
+        return {0.f, __int_as_float(0x7f800000)};
+    }
+    if (b.mode == BoundMode::plain) {
+        return bound_with(d, b, 0.f);
+    }
+    float e = __fadd_ru(b.row_err[row], b.query_err[q]);
+    if (b.mode == BoundMode::median && d >= 0.f && b.pair_err != nullptr) {
+        // a computed median: its own error bound
+        e = b.pair_err[static_cast<uint64_t>(q) * b.pair_rows + row];
+    }
+    return bound_with(d, b, e);
+}
+
+// A lower bound valid for every row of query q whose binary32 distance is at
+// least d (finite): the largest row error in place of the row's own.
+__device__ __forceinline__ float lower_any(float d, const Bound& b, uint32_t q)
+{
+    const float e =
+        b.mode == BoundMode::plain ? 0.f : __fadd_ru(b.row_err_max, b.query_err[q]);
+    return bound_with(d, b, e).lower;
 }
 
 // Sum of the chunk partials of one (query, row) in chunk order. The loads are
@@ -377,6 +402,68 @@ __device__ double replay_candidate(const ReplayInputs& in, const float* qrow,
     return replay_row(in, qrow, in.rows + uint64_t(row) * in.padded_dim, lane);
 }
 
+// One thread's pass over its rows of a query in the argmin kernel.
+struct RowScan {
+    float k1 = __builtin_huge_valf();  // smallest distance
+    float k2 = __builtin_huge_valf();  // second smallest
+    uint32_t r1 = 0xffffffffu;              // row of k1 (lowest on ties)
+    float set_aside = __builtin_huge_valf();  // median: smallest -d < 0
+    bool overflow = false;
+};
+
+template <bool kSingleChunk>
+__device__ __forceinline__ float load_distance(const PartialView& v, uint32_t q, uint32_t row)
+{
+    if constexpr (kSingleChunk) {
+        return v.partials[static_cast<uint64_t>(q) * v.rows + row];
+    } else {
+        return row_distance(v, q, row);
+    }
+}
+
+// kArgminUnroll rows per thread per step, their loads issued together (with
+// one partial slab the load is a single instruction the compiler can batch).
+template <bool kSingleChunk>
+__device__ __forceinline__ void scan_rows(const PartialView& view, const Bound& bound,
+                                          uint32_t q, uint32_t first_row, uint32_t end_row,
+                                          RowScan& scan, Summary& s)
+{
+    const bool keyed = bound.mode != BoundMode::median;
+    for (uint32_t base = first_row + threadIdx.x; base < end_row;
+         base += kFinalizeThreads * kArgminUnroll) {
+        float d[kArgminUnroll];
+#pragma unroll
+        for (int u = 0; u < kArgminUnroll; ++u) {
+            const uint32_t row = base + u * kFinalizeThreads;
+            d[u] = row < end_row ? load_distance<kSingleChunk>(view, q, row) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < kArgminUnroll; ++u) {
+            const uint32_t row = base + u * kFinalizeThreads;
+            if (row >= end_row) {
+                continue;
+            }
+            const float x = d[u];
+            if (!(x <= FLT_MAX)) {
+                scan.overflow = true;
+            } else if (keyed) {
+                if (x < scan.k1) {
+                    scan.k2 = scan.k1;
+                    scan.k1 = x;
+                    scan.r1 = row;
+                } else if (x < scan.k2) {
+                    scan.k2 = x;
+                }
+            } else if (x < 0.f) {
+                scan.set_aside = fminf(scan.set_aside, -x);
+            } else {
+                const Bounds2 b = bound_of(x, bound, row, q);
+                summary_insert(s, b.lower, b.upper, row, x);
+            }
+        }
+    }
+}
+
 // grid = (row blocks, batch). Every CTA summarises kFinalizeThreads rows of
 // one query; the last CTA of the query to finish merges the summaries. A
 // certified query is answered there; otherwise the same CTA replays every
@@ -394,10 +481,30 @@ __global__ void __launch_bounds__(kFinalizeThreads)
     Summary s{inf, inf, inf, 0xffffffffu, inf};
     const uint32_t first_row = blockIdx.x * span;
     const uint32_t end_row = min(view.rows, first_row + span);
-    for (uint32_t row = first_row + threadIdx.x; row < end_row; row += kFinalizeThreads) {
-        const float d = row_distance(view, q, row);
-        const Bounds2 b = bound_of(d, bound, row, q);
-        summary_insert(s, b.lower, b.upper, row, d);
+    // Plain and projected_l2 bounds are monotone in d, so a thread keeps only
+    // its smallest distance (lowest row on ties) and its second smallest; the
+    // bounds are formed once, from the best row's own error and, for all its
+    // other rows, the largest row error. Median rows set aside by the scan
+    // share one lower bound; computed medians (few) are inserted with their
+    // own bounds. Binary32 overflows enter as a lower bound of 0.
+    RowScan scan;
+    if (view.chunks == 1) {
+        scan_rows<true>(view, bound, q, first_row, end_row, scan, s);
+    } else {
+        scan_rows<false>(view, bound, q, first_row, end_row, scan, s);
+    }
+    if (bound.mode != BoundMode::median && scan.r1 != 0xffffffffu) {
+        const Bounds2 b1 = bound_of(scan.k1, bound, scan.r1, q);
+        s = Summary{b1.upper, b1.lower,
+                    scan.k2 <= FLT_MAX ? lower_any(scan.k2, bound, q) : inf, scan.r1,
+                    scan.k1};
+    }
+    if (scan.set_aside <= FLT_MAX) {
+        summary_insert(s, lower_any(-scan.set_aside, bound, q), inf, 0xffffffffu,
+                       -scan.set_aside);
+    }
+    if (scan.overflow) {
+        summary_insert(s, 0.f, inf, 0xffffffffu, inf);
     }
     s = block_reduce_summary(s);
     __shared__ bool is_last;
@@ -432,7 +539,7 @@ __global__ void __launch_bounds__(kFinalizeThreads)
     __shared__ bool certified;
     __shared__ float min_upper;
     if (threadIdx.x == 0) {
-        certified = s.second > s.min_upper;
+        certified = s.second > s.min_upper && s.first_row != 0xffffffffu;
         min_upper = s.min_upper;
         if (certified) {
             results[q] = Result{s.first_row, s.first_distance};
@@ -457,21 +564,31 @@ __global__ void __launch_bounds__(kFinalizeThreads)
     const int lane = threadIdx.x % 32;
     double best = __longlong_as_double(0x7ff0000000000000ll);
     uint32_t best_row = 0xffffffffu;
-    for (uint32_t base = warp * 32; base < view.rows; base += warps * 32) {
-        const uint32_t r = base + lane;
-        bool candidate = false;
-        if (r < view.rows) {
-            candidate = bound_of(row_distance(view, q, r), bound, r, q).lower <= min_upper;
+    // candidate flags for kArgminUnroll runs of 32 rows per warp step (loads
+    // in flight together), then the replays of the step's candidates in one
+    // rolled loop (a single copy of the replay code)
+    for (uint32_t base = warp * 32; base < view.rows; base += warps * 32 * kArgminUnroll) {
+        unsigned int masks[kArgminUnroll];
+#pragma unroll
+        for (int u = 0; u < kArgminUnroll; ++u) {
+            const uint32_t r = base + u * warps * 32 + lane;
+            masks[u] = __ballot_sync(
+                0xffffffffu,
+                r < view.rows &&
+                    bound_of(row_distance(view, q, r), bound, r, q).lower <= min_upper);
         }
-        unsigned int mask = __ballot_sync(0xffffffffu, candidate);
-        while (mask != 0u) {
-            const int bit = __ffs(mask) - 1;
-            mask &= mask - 1u;
-            const uint32_t crow = base + bit;
-            const double d = replay_candidate(in, qrow, projected_query, crow, lane);
-            if (lex_less(d, crow, best, best_row)) {
-                best = d;
-                best_row = crow;
+#pragma unroll 1
+        for (int u = 0; u < kArgminUnroll; ++u) {
+            unsigned int mask = masks[u];
+            while (mask != 0u) {
+                const int bit = __ffs(mask) - 1;
+                mask &= mask - 1u;
+                const uint32_t crow = base + u * warps * 32 + bit;
+                const double d = replay_candidate(in, qrow, projected_query, crow, lane);
+                if (lex_less(d, crow, best, best_row)) {
+                    best = d;
+                    best_row = crow;
+                }
             }
         }
     }

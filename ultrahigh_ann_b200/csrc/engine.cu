@@ -775,6 +775,12 @@ void create_hierarchical_index(int device, uha_metric metric, const RowSource& s
     } else {
         index->usage.index_payload_bytes =
             k * column_bytes + p * k * f + row_count * p * f;
+        // the median scan's pruning count reads the rows transposed
+        index->rows_pitch = uha::round_up(row_count, 32);
+        index->scan_rows_t.allocate(checked_mul(pp, index->rows_pitch, "transposed rows"));
+        uha::launch_transpose_rows(index->scan_rows.get(), row_count, pp,
+                                   index->scan_rows_t.get(), index->rows_pitch, nullptr);
+        check_cuda(cudaDeviceSynchronize(), "row transpose kernel failed");
     }
     index->usage.query_workspace_payload_bytes = 0;
     index->usage.unique_query_coordinates = k;
@@ -884,6 +890,10 @@ extern "C" uha_status uha_workspace_create(const uha_index* index,
             ws->prepared.allocate(b * index->padded_sample);
             ws->projected.allocate(b * index->padded_dim);
             ws->query_err.allocate(b);
+            if (index->metric == UHA_L1) {
+                ws->coord_err.allocate(b * index->padded_dim);
+                ws->pair_err.allocate(checked_mul(b, index->rows, "median errors"));
+            }
         } else {
             ws->prepared.allocate(b * index->padded_dim);
         }
@@ -1148,6 +1158,7 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
             ws->prepared.get(), n, index->padded_sample, index->sample_size,
             index->projection32.get(), index->projection_dimension,
             ws->projected.get(), index->padded_dim, ws->query_err.get(),
+            index->metric == UHA_L1 ? ws->coord_err.get() : nullptr,
             projection_error_per_abs(index->sample_size), index->metric == UHA_L2,
             error_flag, stream);
         scan_queries = ws->projected.get();
@@ -1234,11 +1245,13 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
             check_cuda(cudaStreamSynchronize(stream), "CUDA query failed");
             ws->median_min.allocate(std::max<uint64_t>(n, ws->max_batch));
         }
-        uha::launch_median_scan(index->scan_rows.get(), index->rows, index->padded_dim,
+        uha::launch_median_scan(index->scan_rows.get(), index->scan_rows_t.get(),
+                                index->rows_pitch, index->rows, index->padded_dim,
                                 index->projection_dimension, scan_queries, n,
-                                ws->query_err.get(), index->row_err_max, median_rel,
-                                median_abs, ws->median_min.get(), ws->partials.get(),
-                                stream);
+                                ws->query_err.get(), ws->coord_err.get(),
+                                index->row_err_max, median_rel, median_abs,
+                                ws->median_min.get(), ws->partials.get(),
+                                ws->pair_err.get(), stream);
     } else {
         uha::launch_scan(plan, op, index->scan_rows.get(), index->rows,
                          index->padded_dim, index->weights32.get(), scan_queries, n,
@@ -1280,10 +1293,13 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
     if (hierarchical) {
         bound.row_err = index->row_err.get();
         bound.query_err = ws->query_err.get();
+        bound.row_err_max = index->row_err_max;
         if (median) {
             bound.mode = uha::BoundMode::median;
             bound.rel = median_rel;
             bound.abs = median_abs;
+            bound.pair_err = ws->pair_err.get();
+            bound.pair_rows = static_cast<uint32_t>(index->rows);
         } else {
             bound.mode = uha::BoundMode::projected_l2;
             const double n64 = static_cast<double>(index->scan_dim) + 3;

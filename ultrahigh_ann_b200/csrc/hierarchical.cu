@@ -107,8 +107,8 @@ __global__ void __launch_bounds__(kProjQueries * kProjCols)
                            uint64_t padded_k, uint64_t k,
                            const float* __restrict__ proj, uint64_t p,
                            float* __restrict__ y, uint64_t padded_p,
-                           float* __restrict__ err_acc, double err_per_abs,
-                           bool euclidean, int* error_flag)
+                           float* __restrict__ err_acc, float* __restrict__ coord_err,
+                           double err_per_abs, bool euclidean, int* error_flag)
 {
     __shared__ float sx[kProjQueries][kProjK];
     __shared__ float sp[kProjCols][kProjK + 1];
@@ -149,6 +149,9 @@ __global__ void __launch_bounds__(kProjQueries * kProjCols)
     }
     if (j >= p) {
         y[b * padded_p + j] = 0.f;
+        if (coord_err != nullptr) {
+            coord_err[b * padded_p + j] = 0.f;
+        }
         return;
     }
     if (!isfinite(total)) {
@@ -159,6 +162,9 @@ __global__ void __launch_bounds__(kProjQueries * kProjCols)
     // per-coordinate error
     const double e = err_per_abs * static_cast<double>(total_abs) +
                      static_cast<double>(k + 2) * 1.0e-44;
+    if (coord_err != nullptr) {
+        coord_err[b * padded_p + j] = __double2float_ru(e);
+    }
     if (euclidean) {
         atomicAdd(err_acc + b, __double2float_ru(e * e));
     } else {
@@ -228,13 +234,15 @@ __device__ __forceinline__ int load_abs_diffs(const float* r, const float* y, ui
 // even p the midpoint with the (p/2 - 1)-th, which is the upper middle itself
 // when it occurs twice there, else the largest value below it.
 template <int PER_LANE>
-__device__ __forceinline__ float warp_median(const float (&v)[PER_LANE], int valid,
-                                             uint32_t p)
+__device__ __forceinline__ void warp_middles(const float (&v)[PER_LANE], int valid,
+                                             uint32_t p, float& lower_out, float& upper_out)
 {
     const uint32_t mid = p / 2;
     const float upper = warp_select<PER_LANE>(v, valid, mid);
+    upper_out = upper;
+    lower_out = upper;
     if (p % 2 != 0) {
-        return upper;
+        return;
     }
     const uint32_t ub = __float_as_uint(upper);
     uint32_t below = 0;
@@ -249,8 +257,46 @@ __device__ __forceinline__ float warp_median(const float (&v)[PER_LANE], int val
     }
     below = __reduce_add_sync(0xffffffffu, below);
     largest_below = __reduce_max_sync(0xffffffffu, largest_below);
-    const float lower = below < mid ? upper : __uint_as_float(largest_below);
-    return lower + (upper - lower) * 0.5f;
+    lower_out = below < mid ? upper : __uint_as_float(largest_below);
+}
+
+template <int PER_LANE>
+__device__ __forceinline__ float warp_median(const float (&v)[PER_LANE], int valid,
+                                             uint32_t p)
+{
+    float lower, upper;
+    warp_middles<PER_LANE>(v, valid, p, lower, upper);
+    return p % 2 != 0 ? upper : lower + (upper - lower) * 0.5f;
+}
+
+// Bound on |m - m64| for an order statistic m of the lane values v (binary32
+// |r - y|) against the same order statistic of the reference values, which
+// lie within eps_j of v_j: the k-th smallest of the perturbed values is at
+// least min(m, min over v_j >= m of v_j - eps_j) and at most
+// max(m, max over v_j <= m of v_j + eps_j), so only coordinates within eps_j
+// of m contribute. Returns the larger side, over the lower and upper middle.
+template <int PER_LANE>
+__device__ __forceinline__ float warp_middle_error(const float (&v)[PER_LANE],
+                                                   const float (&eps)[PER_LANE], int valid,
+                                                   float m_lower, float m_upper)
+{
+    if (!(m_upper <= 1.0e37f)) {
+        return __int_as_float(0x7f800000);
+    }
+    float e = 0.f;
+#pragma unroll
+    for (int i = 0; i < PER_LANE; ++i) {
+        // an overflowed |diff| lies far above either middle
+        if (i < valid && v[i] <= FLT_MAX) {
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                const float m = side == 0 ? m_lower : m_upper;
+                const float gap = v[i] >= m ? __fsub_rd(v[i], m) : __fsub_rd(m, v[i]);
+                e = fmaxf(e, __fsub_ru(eps[i], gap));
+            }
+        }
+    }
+    return __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(e)));
 }
 
 // Stage 1 of the median scan: exact binary32 medians of `samples` rows spread
@@ -292,21 +338,7 @@ __global__ void __launch_bounds__(kThreads)
 // and cannot be the argmin. One count decides it: fewer than p/2 + 1 values
 // <= T (odd p), fewer than p/2 (even p: the lower middle is above T). Such a
 // row stores -T (a negative distance: "at least T, no upper bound"); every
-// other row stores its binary32 median.
-// Each warp takes a contiguous run of (query, row) pairs in query-major
-// order, so the query's values and threshold stay in registers across rows
-// and the next row's values are loaded while the current one is decided.
-template <int PER_LANE>
-__device__ __forceinline__ void load_lane_values(const float* v, uint32_t p, int lane,
-                                                 float (&out)[PER_LANE])
-{
-#pragma unroll
-    for (int i = 0; i < PER_LANE; ++i) {
-        const uint32_t j = lane + 32u * i;
-        out[i] = j < p ? v[j] : 0.f;
-    }
-}
-
+// other row gets its binary32 median in stage 3.
 __device__ __forceinline__ float median_threshold(const unsigned int* min_bits,
                                                   const float* query_err, uint32_t q,
                                                   float row_err_max, float rel, float abs_err)
@@ -321,84 +353,175 @@ __device__ __forceinline__ float median_threshold(const unsigned int* min_bits,
     return __fmul_ru(__fdiv_ru(num, __fsub_rd(1.f, rel)), 1.0000005f);
 }
 
+// The stage-2 count over the transposed rows (rows_t[j][row], row pitch
+// r_pitch): two rows per thread and Q queries per CTA, so each row value
+// read from L2 serves Q queries and each query value broadcast from shared
+// memory serves two rows. A pruned pair stores -T, any other pair the survivor mark (bits
+// 0xffffffff, a NaN no distance takes) for median_survivor_kernel. Values
+// above T are counted from the sign bit of T - |r_j - y_j|: a rounded
+// difference of binary32 values has the sign of the exact one (and is +0
+// when they are equal), so the count is that of |r_j - y_j| > T exactly.
+constexpr int kCountRows = 128;
+constexpr int kCountRowsPerThread = 2;
+constexpr uint32_t kSurvivorMark = 0xffffffffu;
+
+template <int Q>
+__global__ void __launch_bounds__(kCountRows)
+    median_count_kernel(const float* __restrict__ rows_t, uint32_t r_pitch,
+                        uint32_t row_count, uint32_t padded_p, uint32_t p,
+                        const float* __restrict__ queries, uint32_t batch,
+                        uint32_t q_begin, const unsigned int* __restrict__ min_bits,
+                        const float* __restrict__ query_err, float row_err_max, float rel,
+                        float abs_err, float* __restrict__ partials)
+{
+    extern __shared__ float4 ys4[];  // [Q][padded_p / 4]
+    float* ys = reinterpret_cast<float*>(ys4);
+    const uint32_t q0 = q_begin + blockIdx.y * Q;
+    for (uint32_t i = threadIdx.x; i < Q * padded_p; i += blockDim.x) {
+        const uint32_t qq = i / padded_p;
+        const uint32_t j = i - qq * padded_p;
+        ys[i] = (q0 + qq < batch && j < p) ? queries[uint64_t(q0 + qq) * padded_p + j] : 0.f;
+    }
+    float t[Q];
+    uint32_t over[Q][kCountRowsPerThread];
+#pragma unroll
+    for (int qq = 0; qq < Q; ++qq) {
+        t[qq] = q0 + qq < batch
+                    ? median_threshold(min_bits, query_err, q0 + qq, row_err_max, rel, abs_err)
+                    : 0.f;
+#pragma unroll
+        for (int k = 0; k < kCountRowsPerThread; ++k) {
+            over[qq][k] = 0;
+        }
+    }
+    __syncthreads();
+    // rows row0 + k * kCountRows (k < kCountRowsPerThread): each broadcast
+    // query value serves them all
+    const uint32_t row0 = blockIdx.x * (kCountRows * kCountRowsPerThread) + threadIdx.x;
+    const float* col[kCountRowsPerThread];
+#pragma unroll
+    for (int k = 0; k < kCountRowsPerThread; ++k) {
+        const uint32_t row = row0 + k * kCountRows;
+        col[k] = rows_t + (row < row_count ? row : 0);
+    }
+    const uint32_t p4 = p & ~3u;
+    const uint32_t pitch4 = padded_p / 4;
+    for (uint32_t j = 0; j < p4; j += 4) {
+        float r[kCountRowsPerThread][4];
+#pragma unroll
+        for (int k = 0; k < kCountRowsPerThread; ++k) {
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                r[k][m] = col[k][uint64_t(j + m) * r_pitch];
+            }
+        }
+#pragma unroll
+        for (int qq = 0; qq < Q; ++qq) {
+            const float4 y4 = ys4[qq * pitch4 + j / 4];
+            const float y[4] = {y4.x, y4.y, y4.z, y4.w};
+#pragma unroll
+            for (int k = 0; k < kCountRowsPerThread; ++k) {
+#pragma unroll
+                for (int m = 0; m < 4; ++m) {
+                    over[qq][k] +=
+                        __float_as_uint(__fsub_rn(t[qq], fabsf(__fsub_rn(r[k][m], y[m])))) >> 31;
+                }
+            }
+        }
+    }
+    for (uint32_t j = p4; j < p; ++j) {
+#pragma unroll
+        for (int k = 0; k < kCountRowsPerThread; ++k) {
+            const float rv = col[k][uint64_t(j) * r_pitch];
+#pragma unroll
+            for (int qq = 0; qq < Q; ++qq) {
+                over[qq][k] += __float_as_uint(__fsub_rn(
+                                   t[qq], fabsf(__fsub_rn(rv, ys[qq * padded_p + j])))) >>
+                               31;
+            }
+        }
+    }
+    const uint32_t needed = p % 2 != 0 ? p / 2 + 1 : p / 2;
+#pragma unroll
+    for (int k = 0; k < kCountRowsPerThread; ++k) {
+        const uint32_t row = row0 + k * kCountRows;
+        if (row >= row_count) {
+            continue;
+        }
+#pragma unroll
+        for (int qq = 0; qq < Q; ++qq) {
+            if (q0 + qq < batch) {
+                const bool pruned = t[qq] <= FLT_MAX && p - over[qq][k] < needed;
+                partials[uint64_t(q0 + qq) * row_count + row] =
+                    pruned ? -t[qq] : __uint_as_float(kSurvivorMark);
+            }
+        }
+    }
+}
+
+// Stage 3: the binary32 median of every pair marked by the count, one warp
+// per marked pair; warps take runs of 32 pairs and vote on their marks.
 template <int PER_LANE>
 __global__ void __launch_bounds__(kThreads)
-    median_scan_kernel(const float* __restrict__ rows, uint32_t row_count,
-                       uint32_t padded_p, uint32_t p,
-                       const float* __restrict__ queries, uint32_t batch,
-                       const unsigned int* __restrict__ min_bits,
-                       const float* __restrict__ query_err, float row_err_max,
-                       float rel, float abs_err, float* __restrict__ partials)
+    median_survivor_kernel(const float* __restrict__ rows, uint32_t row_count,
+                           uint32_t padded_p, uint32_t p,
+                           const float* __restrict__ queries, uint32_t batch,
+                           const float* __restrict__ coord_err,
+                           float* __restrict__ partials, float* __restrict__ pair_err)
 {
     const int lane = threadIdx.x % 32;
     const uint64_t total = static_cast<uint64_t>(row_count) * batch;
-    const uint64_t warps = static_cast<uint64_t>(gridDim.x) * (blockDim.x / 32);
-    const uint64_t warp_id = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) / 32;
-    const uint64_t per_warp = (total + warps - 1) / warps;
-    const uint64_t begin = warp_id * per_warp;
-    const uint64_t end = begin + per_warp < total ? begin + per_warp : total;
-    if (begin >= end) {
-        return;
-    }
-    const uint32_t needed = p % 2 != 0 ? p / 2 + 1 : p / 2;
-    uint32_t q = static_cast<uint32_t>(begin / row_count);
-    uint32_t row = static_cast<uint32_t>(begin - uint64_t(q) * row_count);
-    float y[PER_LANE];
-    load_lane_values<PER_LANE>(queries + uint64_t(q) * padded_p, p, lane, y);
-    float t = median_threshold(min_bits, query_err, q, row_err_max, rel, abs_err);
-    float next[PER_LANE];
-    load_lane_values<PER_LANE>(rows + uint64_t(row) * padded_p, p, lane, next);
-    for (uint64_t w = begin; w < end; ++w) {
-        float v[PER_LANE];
-        int valid = 0;
-#pragma unroll
-        for (int i = 0; i < PER_LANE; ++i) {
-            const uint32_t j = lane + 32u * i;
-            v[i] = 0.f;
-            if (j < p) {
-                float d = fabsf(next[i] - y[i]);
-                if (!(d <= FLT_MAX)) {
-                    d = __int_as_float(0x7f800000);
-                }
-                v[i] = d;
-                valid = i + 1;
-            }
-        }
-        const uint32_t cur_q = q;
-        const uint32_t cur_row = row;
-        const float cur_t = t;
-        // advance to the next pair and start its loads
-        if (++row == row_count) {
-            row = 0;
-            ++q;
-        }
-        if (w + 1 < end) {
-            if (q != cur_q) {
-                load_lane_values<PER_LANE>(queries + uint64_t(q) * padded_p, p, lane, y);
-                t = median_threshold(min_bits, query_err, q, row_err_max, rel, abs_err);
-            }
-            load_lane_values<PER_LANE>(rows + uint64_t(row) * padded_p, p, lane, next);
-        }
-        float* out = partials + static_cast<uint64_t>(cur_q) * row_count + cur_row;
-        if (cur_t <= FLT_MAX) {
-            const uint32_t tb = __float_as_uint(cur_t);
-            uint32_t at_most = 0;
+    const uint64_t runs = (total + 31) / 32;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * (blockDim.x / 32);
+    for (uint64_t run = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) / 32;
+         run < runs; run += stride) {
+        const uint64_t mine = run * 32 + lane;
+        const bool marked =
+            mine < total && __float_as_uint(partials[mine]) == kSurvivorMark;
+        uint32_t mask = __ballot_sync(0xffffffffu, marked);
+        while (mask != 0) {
+            const int bit = __ffs(mask) - 1;
+            mask &= mask - 1;
+            const uint64_t pair = run * 32 + bit;
+            const uint32_t q = static_cast<uint32_t>(pair / row_count);
+            const uint32_t row = static_cast<uint32_t>(pair - uint64_t(q) * row_count);
+            const float* r = rows + uint64_t(row) * padded_p;
+            const float* y = queries + uint64_t(q) * padded_p;
+            const float* ye = coord_err + uint64_t(q) * padded_p;
+            float v[PER_LANE];
+            float eps[PER_LANE];
+            const int valid = load_abs_diffs<PER_LANE>(r, y, p, lane, v);
+            // per coordinate: the row's binary32 rounding (at most 2^-24 |r|),
+            // the query's projection error and the rounding of r - y
 #pragma unroll
             for (int i = 0; i < PER_LANE; ++i) {
-                at_most += (i < valid && __float_as_uint(v[i]) <= tb) ? 1u : 0u;
+                const uint32_t j = lane + 32u * i;
+                eps[i] = j < p ? __fadd_ru(__fadd_ru(__fmul_ru(fabsf(r[j]), 0x1p-24f), ye[j]),
+                                           __fmul_ru(v[i], 0x1p-24f))
+                               : 0.f;
             }
-            at_most = __reduce_add_sync(0xffffffffu, at_most);
-            if (at_most < needed) {
-                if (lane == 0) {
-                    *out = -cur_t;
-                }
-                continue;
+            float lower, upper;
+            warp_middles<PER_LANE>(v, valid, p, lower, upper);
+            const float median = p % 2 != 0 ? upper : lower + (upper - lower) * 0.5f;
+            const float err = warp_middle_error<PER_LANE>(v, eps, valid, lower, upper);
+            if (lane == 0) {
+                partials[pair] = median;
+                pair_err[pair] = err;
             }
         }
-        const float median = warp_median<PER_LANE>(v, valid, p);
-        if (lane == 0) {
-            *out = median;
-        }
+    }
+}
+
+__global__ void transpose_rows_kernel(const float* __restrict__ rows, uint64_t row_count,
+                                      uint64_t padded_p, float* __restrict__ out,
+                                      uint64_t r_pitch)
+{
+    const uint64_t total = padded_p * r_pitch;
+    for (uint64_t idx = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+         idx < total; idx += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t j = idx / r_pitch;
+        const uint64_t row = idx - j * r_pitch;
+        out[idx] = row < row_count ? rows[row * padded_p + j] : 0.f;
     }
 }
 
@@ -420,6 +543,14 @@ void launch_project_rows64(const float* sampled, uint64_t row_count,
     check_cuda(cudaGetLastError(), "cannot launch row projection kernel");
 }
 
+void launch_transpose_rows(const float* rows, uint64_t row_count, uint64_t padded_p,
+                           float* out, uint64_t r_pitch, cudaStream_t stream)
+{
+    transpose_rows_kernel<<<grid_for(padded_p * r_pitch), kThreads, 0, stream>>>(
+        rows, row_count, padded_p, out, r_pitch);
+    check_cuda(cudaGetLastError(), "cannot launch row transpose kernel");
+}
+
 void launch_narrow_rows(const double* reps, uint64_t row_count, uint64_t p,
                         float* out, uint64_t padded_p, float* row_err,
                         bool euclidean, int* bad, cudaStream_t stream)
@@ -434,7 +565,7 @@ void launch_narrow_rows(const double* reps, uint64_t row_count, uint64_t p,
 void launch_project_queries(const float* gathered, uint64_t batch,
                             uint64_t padded_k, uint64_t k,
                             const float* proj32, uint64_t p, float* out,
-                            uint64_t padded_p, float* query_err,
+                            uint64_t padded_p, float* query_err, float* coord_err,
                             double err_per_abs, bool euclidean,
                             int* error_flag, cudaStream_t stream)
 {
@@ -443,7 +574,7 @@ void launch_project_queries(const float* gathered, uint64_t batch,
     const dim3 grid(static_cast<uint32_t>((padded_p + kProjCols - 1) / kProjCols),
                     static_cast<uint32_t>((batch + kProjQueries - 1) / kProjQueries));
     project_queries_kernel<<<grid, kProjQueries * kProjCols, 0, stream>>>(
-        gathered, batch, padded_k, k, proj32, p, out, padded_p, query_err,
+        gathered, batch, padded_k, k, proj32, p, out, padded_p, query_err, coord_err,
         err_per_abs, euclidean, error_flag);
     check_cuda(cudaGetLastError(), "cannot launch query projection kernel");
     finish_query_err_kernel<<<static_cast<uint32_t>((batch + kThreads - 1) / kThreads),
@@ -453,16 +584,46 @@ void launch_project_queries(const float* gathered, uint64_t batch,
 
 namespace {
 
+// Rows whose exact medians set the pruning threshold: about sqrt(rows)
+// (balancing these medians against the ~rows / samples survivors per
+// query), in [32, 256] and at most the row count.
 uint32_t median_samples(uint64_t row_count)
 {
-    return static_cast<uint32_t>(row_count < 32 ? row_count : 32);
+    uint64_t s = 32;
+    while (s < 256 && s * s < row_count) {
+        s += 32;
+    }
+    return static_cast<uint32_t>(row_count < s ? row_count : s);
+}
+
+template <int Q>
+void launch_median_count(const float* rows_t, uint32_t r_pitch, uint32_t rc, uint32_t pp,
+                         uint32_t pv, const float* queries, uint32_t b,
+                         const unsigned int* min_bits, const float* query_err,
+                         float row_err_max, float rel, float abs_err, float* partials,
+                         cudaStream_t stream)
+{
+    // at most 8 x 1024 binary32 values: within the default 48 KB
+    const size_t smem = static_cast<size_t>(Q) * pp * sizeof(float);
+    // grid.y is limited to 65,535 query groups per launch
+    const uint64_t groups = (static_cast<uint64_t>(b) + Q - 1) / Q;
+    for (uint64_t g = 0; g < groups; g += 65535) {
+        const dim3 grid((rc + kCountRows * kCountRowsPerThread - 1) /
+                            (kCountRows * kCountRowsPerThread),
+                        static_cast<uint32_t>(std::min<uint64_t>(65535, groups - g)));
+        median_count_kernel<Q><<<grid, kCountRows, smem, stream>>>(
+            rows_t, r_pitch, rc, pp, pv, queries, b, static_cast<uint32_t>(g * Q), min_bits,
+            query_err, row_err_max, rel, abs_err, partials);
+    }
 }
 
 template <int PER_LANE>
-void launch_median_pair(const float* rows, uint32_t rc, uint32_t pp, uint32_t pv,
-                        const float* queries, uint32_t b, const float* query_err,
+void launch_median_pair(const float* rows, const float* rows_t, uint32_t r_pitch,
+                        uint32_t rc, uint32_t pp, uint32_t pv, const float* queries,
+                        uint32_t b, const float* query_err, const float* coord_err,
                         float row_err_max, float rel, float abs_err,
-                        unsigned int* min_bits, float* partials, cudaStream_t stream)
+                        unsigned int* min_bits, float* partials, float* pair_err,
+                        cudaStream_t stream)
 {
     // grid-stride warps over the pairs: at most 16 resident CTAs' worth per SM
     const uint64_t cap = 148ull * 16;
@@ -472,21 +633,37 @@ void launch_median_pair(const float* rows, uint32_t rc, uint32_t pp, uint32_t pv
     median_sample_kernel<PER_LANE>
         <<<static_cast<uint32_t>(std::min(sample_blocks, cap)), kThreads, 0, stream>>>(
             rows, rc, pp, pv, queries, b, samples, partials, min_bits);
-    const uint64_t blocks = (static_cast<uint64_t>(rc) * b * 32 + kThreads - 1) / kThreads;
-    median_scan_kernel<PER_LANE>
+    if (b >= 8) {
+        launch_median_count<8>(rows_t, r_pitch, rc, pp, pv, queries, b, min_bits, query_err,
+                               row_err_max, rel, abs_err, partials, stream);
+    } else if (b >= 4) {
+        launch_median_count<4>(rows_t, r_pitch, rc, pp, pv, queries, b, min_bits, query_err,
+                               row_err_max, rel, abs_err, partials, stream);
+    } else if (b >= 2) {
+        launch_median_count<2>(rows_t, r_pitch, rc, pp, pv, queries, b, min_bits, query_err,
+                               row_err_max, rel, abs_err, partials, stream);
+    } else {
+        launch_median_count<1>(rows_t, r_pitch, rc, pp, pv, queries, b, min_bits, query_err,
+                               row_err_max, rel, abs_err, partials, stream);
+    }
+    const uint64_t runs = (static_cast<uint64_t>(rc) * b + 31) / 32;
+    const uint64_t blocks = (runs * 32 + kThreads - 1) / kThreads;
+    median_survivor_kernel<PER_LANE>
         <<<static_cast<uint32_t>(std::min(blocks, cap)), kThreads, 0, stream>>>(
-            rows, rc, pp, pv, queries, b, min_bits, query_err, row_err_max, rel, abs_err,
-            partials);
+            rows, rc, pp, pv, queries, b, coord_err, partials, pair_err);
 }
 
 }  // namespace
 
-void launch_median_scan(const float* rows, uint64_t row_count, uint64_t padded_p,
+void launch_median_scan(const float* rows, const float* rows_t, uint64_t r_pitch,
+                        uint64_t row_count, uint64_t padded_p,
                         uint64_t p, const float* queries, uint64_t batch,
-                        const float* query_err, float row_err_max, float rel,
+                        const float* query_err, const float* coord_err,
+                        float row_err_max, float rel,
                         float abs_err, unsigned int* min_bits, float* partials,
-                        cudaStream_t stream)
+                        float* pair_err, cudaStream_t stream)
 {
+    const uint32_t rp = static_cast<uint32_t>(r_pitch);
     const uint32_t rc = static_cast<uint32_t>(row_count);
     const uint32_t pp = static_cast<uint32_t>(padded_p);
     const uint32_t pv = static_cast<uint32_t>(p);
@@ -494,23 +671,29 @@ void launch_median_scan(const float* rows, uint64_t row_count, uint64_t padded_p
     check_cuda(cudaMemsetAsync(min_bits, 0xff, batch * sizeof(unsigned int), stream),
                "cannot clear median thresholds");
     if (p <= 32) {
-        launch_median_pair<1>(rows, rc, pp, pv, queries, b, query_err, row_err_max, rel,
-                              abs_err, min_bits, partials, stream);
+        launch_median_pair<1>(rows, rows_t, rp, rc, pp, pv, queries, b, query_err,
+                               coord_err, row_err_max, rel, abs_err, min_bits, partials,
+                               pair_err, stream);
     } else if (p <= 64) {
-        launch_median_pair<2>(rows, rc, pp, pv, queries, b, query_err, row_err_max, rel,
-                              abs_err, min_bits, partials, stream);
+        launch_median_pair<2>(rows, rows_t, rp, rc, pp, pv, queries, b, query_err,
+                               coord_err, row_err_max, rel, abs_err, min_bits, partials,
+                               pair_err, stream);
     } else if (p <= 128) {
-        launch_median_pair<4>(rows, rc, pp, pv, queries, b, query_err, row_err_max, rel,
-                              abs_err, min_bits, partials, stream);
+        launch_median_pair<4>(rows, rows_t, rp, rc, pp, pv, queries, b, query_err,
+                               coord_err, row_err_max, rel, abs_err, min_bits, partials,
+                               pair_err, stream);
     } else if (p <= 256) {
-        launch_median_pair<8>(rows, rc, pp, pv, queries, b, query_err, row_err_max, rel,
-                              abs_err, min_bits, partials, stream);
+        launch_median_pair<8>(rows, rows_t, rp, rc, pp, pv, queries, b, query_err,
+                               coord_err, row_err_max, rel, abs_err, min_bits, partials,
+                               pair_err, stream);
     } else if (p <= 512) {
-        launch_median_pair<16>(rows, rc, pp, pv, queries, b, query_err, row_err_max, rel,
-                               abs_err, min_bits, partials, stream);
+        launch_median_pair<16>(rows, rows_t, rp, rc, pp, pv, queries, b, query_err,
+                               coord_err, row_err_max, rel, abs_err, min_bits, partials,
+                               pair_err, stream);
     } else if (p <= 1024) {
-        launch_median_pair<32>(rows, rc, pp, pv, queries, b, query_err, row_err_max, rel,
-                               abs_err, min_bits, partials, stream);
+        launch_median_pair<32>(rows, rows_t, rp, rc, pp, pv, queries, b, query_err,
+                               coord_err, row_err_max, rel, abs_err, min_bits, partials,
+                               pair_err, stream);
     } else {
         fail(UHA_LENGTH_ERROR,
              "the L1 hierarchy supports projection dimensions up to 1024");

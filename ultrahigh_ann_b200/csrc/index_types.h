@@ -63,6 +63,9 @@ struct uha_index {
     uha::DeviceBuffer<float> projection32;  // p x padded_sample
     uha::DeviceBuffer<float> row_err;       // rows
     float row_err_max = 0.f;                // largest row_err
+    // L1 hierarchy: scan_rows transposed, padded_dim x rows_pitch
+    uha::DeviceBuffer<float> scan_rows_t;
+    uint64_t rows_pitch = 0;
     uha_space_usage usage{};
     // precision strategies: built on first use (index_bf16 / index_fp8)
     mutable std::mutex lowp_mutex;
@@ -105,6 +108,8 @@ struct uha_workspace {
     uha::DeviceBuffer<double> cand_dist;          // [batch][candidates_per_query]
     uha::DeviceBuffer<uint32_t> rescore_done;     // per query, zero between calls
     uha::DeviceBuffer<unsigned int> median_min;   // L1 hierarchy: sampled minimum per query
+    uha::DeviceBuffer<float> coord_err;   // L1 hierarchy: batch x padded p query errors
+    uha::DeviceBuffer<float> pair_err;    // L1 hierarchy: batch x rows median errors
     uint32_t candidates_per_query = 32;
     std::vector<TunedPlan> tuned;  // autotuned shapes (uha_workspace_autotune)
 

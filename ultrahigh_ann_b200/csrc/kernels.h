@@ -52,6 +52,11 @@ struct Bound {
     const float* row_err = nullptr;
     const float* query_err = nullptr;
     float cpu_rel = 0.f;
+    // median mode (nullable): per (query, row) error of a computed median,
+    // pair_err[q * pair_rows + row], used in place of row_err + query_err
+    const float* pair_err = nullptr;
+    uint32_t pair_rows = 0;
+    float row_err_max = 0.f;  // largest row_err (hierarchical modes)
 };
 
 struct Result {
@@ -243,24 +248,36 @@ void launch_narrow_rows(const double* reps, uint64_t row_count, uint64_t p,
 // Binary32 projection of gathered queries with its certified error norm:
 // y[b][j] = sum_i x[b][i] proj32[j][i]; query_err[b] bounds the distance
 // between y[b] and the reference's binary64 projection (2-norm if
-// euclidean, else max-norm). error_flag |= 4 for a non-finite projection.
+// euclidean, else max-norm); coord_err (nullable) receives the bound of each
+// coordinate, [batch][padded_p]. error_flag |= 4 for a non-finite projection.
 void launch_project_queries(const float* gathered, uint64_t batch,
                             uint64_t padded_k, uint64_t k,
                             const float* proj32, uint64_t p, float* out,
-                            uint64_t padded_p, float* query_err,
+                            uint64_t padded_p, float* query_err, float* coord_err,
                             double err_per_abs, bool euclidean,
                             int* error_flag, cudaStream_t stream);
 // Median of |rows[row][j] - queries[q][j]| over j < p per (query, row),
 // written as one chunk of partials. Rows that provably cannot be a query's
 // argmin (their median is above a threshold derived from the exact medians of
-// 32 spread rows and the median bound: relative `rel`, absolute `abs_err`,
-// row errors up to row_err_max, query_err[q]) store minus that threshold:
-// a lower bound with no upper bound. min_bits: one word per query.
-void launch_median_scan(const float* rows, uint64_t row_count, uint64_t padded_p,
+// 32-256 spread rows and the median bound: relative `rel`, absolute
+// `abs_err`, row errors up to row_err_max, query_err[q]) store minus that
+// threshold: a lower bound with no upper bound. min_bits: one word per query.
+// rows_t (nullable): the same rows transposed, [padded_p][r_pitch], for the
+// register-tiled pruning count.
+// Every pair whose median is computed also gets pair_err[q][row]: a bound on
+// |median - reference median| from the coordinates near the median only
+// (coord_err[q][j]: the projected query's per-coordinate error; rows carry
+// their binary32 rounding), in place of the max-norm errors.
+void launch_median_scan(const float* rows, const float* rows_t, uint64_t r_pitch,
+                        uint64_t row_count, uint64_t padded_p,
                         uint64_t p, const float* queries, uint64_t batch,
-                        const float* query_err, float row_err_max, float rel,
+                        const float* query_err, const float* coord_err,
+                        float row_err_max, float rel,
                         float abs_err, unsigned int* min_bits, float* partials,
-                        cudaStream_t stream);
+                        float* pair_err, cudaStream_t stream);
+// out[j][row] = rows[row][j] for j < padded_p (build time).
+void launch_transpose_rows(const float* rows, uint64_t row_count, uint64_t padded_p,
+                           float* out, uint64_t r_pitch, cudaStream_t stream);
 
 // ---- build-time helpers
 void launch_gather_rows(const float* source, uint64_t row_count, uint64_t dim,
