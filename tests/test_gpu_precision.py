@@ -11,7 +11,7 @@ What is checked:
   * with fewer candidates, the answer is the reference CPU argmin among the
     k rows with the smallest estimate ||r~||^2 - 2 r~.q~ (recomputed here from
     the engine's own scores), lowest row on ties;
-  * errors: L1 / hierarchical indexes, candidate counts, non-finite queries.
+  * errors: L1 indexes, candidate counts, non-finite queries.
 """
 from __future__ import annotations
 
@@ -161,10 +161,10 @@ def test_precision_errors():
     # the workspace stays usable
     got = index.query_batch(queries[:2], 2, None, ws, BF16)
     assert np.array_equal(got, golden("exact_l2")["indices"][:2])
-    hier = uha.CudaHierarchicalL2AnnIndex(rows, 32, 16, random_engine=uha.MT19937_64(3))
+    hier = uha.CudaHierarchicalL1AnnIndex(rows, 32, 16, random_engine=uha.MT19937_64(3))
     wsh = hier.make_query_workspace(2)
     with pytest.raises(uha.InvalidArgument):
-        hier.query_batch(queries[:2], 2, None, wsh, BF16)
+        _CudaIndex.query_batch(hier, queries[:2], 2, None, wsh, BF16)
 
 
 @pytest.mark.parametrize("strategy", [BF16, FP8])

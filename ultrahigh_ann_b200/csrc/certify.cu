@@ -402,6 +402,53 @@ __device__ double replay_candidate(const ReplayInputs& in, const float* qrow,
     return replay_row(in, qrow, in.rows + uint64_t(row) * in.padded_dim, lane);
 }
 
+// One block per query: each warp re-scores candidates by the reference's
+// binary64 squared distance in the projected space (j order); the block keeps
+// the lexicographic minimum of (distance, row).
+__global__ void __launch_bounds__(kFinalizeThreads)
+    rescore_projected_kernel(const uint32_t* __restrict__ candidates, uint32_t k,
+                             const double* __restrict__ rows64,
+                             const double* __restrict__ y64, uint32_t p, Result* results,
+                             double* exact_distances)
+{
+    constexpr int warps = kFinalizeThreads / 32;
+    const uint32_t q = blockIdx.x;
+    const int warp = threadIdx.x / 32;
+    const int lane = threadIdx.x % 32;
+    const double* y = y64 + static_cast<uint64_t>(q) * p;
+    double best = __longlong_as_double(0x7ff0000000000000ll);
+    uint32_t best_row = 0xffffffffu;
+    for (uint32_t i = warp; i < k; i += warps) {
+        const uint32_t row = candidates[static_cast<uint64_t>(q) * k + i];
+        if (row == 0xffffffffu) {
+            continue;
+        }
+        const double d = replay_projected_l2(rows64 + static_cast<uint64_t>(row) * p, y, p,
+                                             lane);
+        if (lex_less(d, row, best, best_row)) {
+            best = d;
+            best_row = row;
+        }
+    }
+    __shared__ double warp_best[warps];
+    __shared__ uint32_t warp_row[warps];
+    if (lane == 0) {
+        warp_best[warp] = best;
+        warp_row[warp] = best_row;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 0; w < warps; ++w) {
+            if (lex_less(warp_best[w], warp_row[w], best, best_row)) {
+                best = warp_best[w];
+                best_row = warp_row[w];
+            }
+        }
+        results[q] = Result{best_row, static_cast<float>(best)};
+        exact_distances[q] = best;
+    }
+}
+
 // One thread's pass over its rows of a query in the argmin kernel.
 struct RowScan {
     float k1 = __builtin_huge_valf();  // smallest distance
@@ -1177,6 +1224,16 @@ void launch_argmin(PartialView view, Bound bound, ReplayInputs in,
         view, bound, in, results, exact_distances, fs.summaries, fs.done,
         replay_count, span);
     check_cuda(cudaGetLastError(), "cannot launch argmin kernel");
+}
+
+void launch_rescore_projected(const uint32_t* candidates, uint32_t k, uint32_t batch,
+                              const double* rows64, const double* y64, uint32_t p,
+                              Result* results, double* exact_distances,
+                              cudaStream_t stream)
+{
+    rescore_projected_kernel<<<batch, kFinalizeThreads, 0, stream>>>(
+        candidates, k, rows64, y64, p, results, exact_distances);
+    check_cuda(cudaGetLastError(), "cannot launch projected re-score kernel");
 }
 
 uint32_t rescore_depth(uint64_t padded_dim)

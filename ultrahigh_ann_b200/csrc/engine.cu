@@ -769,6 +769,14 @@ void create_hierarchical_index(int device, uha_metric metric, const RowSource& s
     const uint64_t f = sizeof(float);
     const uint64_t column_bytes = 2 * sizeof(uint64_t) + sizeof(double);
     if (metric == UHA_L2) {
+        // the precision strategies' binary64 query projection reads it
+        std::vector<double> proj_t(p * k);
+        for (uint64_t j = 0; j < p; ++j) {
+            for (uint64_t i = 0; i < k; ++i) {
+                proj_t[i * p + j] = projection[j * k + i];
+            }
+        }
+        upload(index->projection64_t, proj_t.data(), proj_t.size());
         compute_row_norms(*index);
         index->usage.index_payload_bytes = row_count * p * f + row_count * f +
                                            k * column_bytes + p * k * f;
@@ -1052,6 +1060,80 @@ void ensure_lowp_workspace(uha_workspace* ws, const uha_index* index,
     }
 }
 
+// The p x k projection of an L2 hierarchy rounded like index rows (built on
+// first use).
+const uha::LowpRows& lowp_projection(const uha_index* index, uha::LowpType type,
+                                     cudaStream_t stream)
+{
+    std::lock_guard<std::mutex> lock(index->lowp_mutex);
+    uha::LowpRows& lp = index->lowp_projection[static_cast<int>(type)];
+    if (lp.ready) {
+        return lp;
+    }
+    const uint64_t p = index->projection_dimension;
+    lp.pitch = uha::lowp_pitch(type, index->sample_size);
+    const uint64_t vectors = uha::lowp_padded_count(p);
+    lp.data.allocate(checked_mul(checked_mul(vectors, lp.pitch, "low-precision projection"),
+                                 uha::lowp_element_bytes(type), "low-precision projection"));
+    lp.scales.allocate(vectors);
+    lp.norms.allocate(p);
+    check_cuda(cudaMemsetAsync(lp.data.get(), 0, lp.data.bytes(), stream),
+               "cannot clear low-precision projection");
+    uha::launch_lowp_convert(type, index->projection32.get(), p, index->padded_sample,
+                             index->sample_size, lp.data.get(), lp.pitch, lp.scales.get(),
+                             lp.norms.get(), stream);
+    check_cuda(cudaStreamSynchronize(stream), "cannot build low-precision projection");
+    lp.ready = true;
+    return lp;
+}
+
+// Precision form of the L2 hierarchy, before the scores: the gathered
+// queries are rounded and projected on the tensor cores (the projection as
+// a GEMM of the rounded p x k matrix with the batch) into ws->projected, the
+// approximate queries of the score GEMM; the reference's binary64 projection
+// goes to ws->projected64 for the re-score.
+void enqueue_hierarchical_projection(const uha_index* index, uha_workspace* ws,
+                                     uha_strategy strategy, uint64_t n, int* error_flag,
+                                     cudaStream_t stream)
+{
+    const uha::LowpType type = lowp_type(strategy);
+    const uha::LowpRows& lp = lowp_projection(index, type, stream);
+    const uint64_t p = index->projection_dimension;
+    const uint64_t bytes = checked_mul(
+        checked_mul(uha::lowp_padded_count(ws->max_batch),
+                    uha::lowp_pitch(uha::LowpType::bf16, index->sample_size),
+                    "query buffer"),
+        2, "query buffer");
+    if (ws->gathered_lp.size() < bytes) {
+        check_cuda(cudaStreamSynchronize(stream), "CUDA query failed");
+        ws->gathered_lp.allocate(bytes);
+        // vectors past a batch are read by the score kernel (and not stored)
+        check_cuda(cudaMemsetAsync(ws->gathered_lp.get(), 0, bytes, stream),
+                   "cannot clear the query buffer");
+        ws->gathered_scales.allocate(uha::lowp_padded_count(ws->max_batch));
+        ws->gathered_amax.allocate(uha::lowp_padded_count(ws->max_batch));
+        ws->projected64.allocate(checked_mul(ws->max_batch, p, "projected queries"));
+    }
+    uha::launch_lowp_queries(type, ws->prepared.get(), n, index->padded_sample,
+                             ws->gathered_lp.get(), lp.pitch, ws->gathered_scales.get(),
+                             ws->gathered_amax.get(), stream);
+    const uha::LowpPlan plan = uha::plan_lowp(type, p, lp.pitch, n, index->sm_count);
+    const uint64_t partial_count =
+        checked_mul(checked_mul(plan.splits, n, "partials"), p, "partials");
+    if (ws->partials.size() < partial_count) {
+        check_cuda(cudaStreamSynchronize(stream), "CUDA query failed");
+        ws->partials.allocate(partial_count);
+    }
+    uha::launch_lowp_scores(plan, type, lp.data.get(), lp.scales.get(), p,
+                            ws->gathered_lp.get(), ws->gathered_scales.get(), n, lp.pitch,
+                            ws->partials.get(), error_flag, stream);
+    uha::launch_sum_slabs(ws->partials.get(), plan.splits, n, p, ws->projected.get(),
+                          index->padded_dim, stream);
+    uha::launch_project_queries64(ws->prepared.get(), n, index->padded_sample,
+                                  index->sample_size, index->projection64_t.get(), p,
+                                  ws->projected64.get(), error_flag, stream);
+}
+
 // Rounds the prepared queries and runs the tensor-core scores; returns the
 // plan (the partial-score slabs are in ws->partials).
 uha::LowpPlan enqueue_lowp_scores(const uha_index* index, uha_workspace* ws,
@@ -1150,7 +1232,14 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
     }
     float* prepared = c.prepared != nullptr ? c.prepared : ws->prepared.get();
     const float* scan_queries = prepared;
-    if (hierarchical) {
+    if (hierarchical && precision_strategy(c.strategy)) {
+        uha::launch_prepare_sampled(source, n, index->dimension, index->columns.get(),
+                                    nullptr, index->sample_size, ws->prepared.get(),
+                                    index->padded_sample, error_flag, stream);
+        enqueue_hierarchical_projection(index, ws, c.strategy, n, error_flag, stream);
+        scan_queries = ws->projected.get();
+        launches += 6;
+    } else if (hierarchical) {
         uha::launch_prepare_sampled(source, n, index->dimension, index->columns.get(),
                                     nullptr, index->sample_size, ws->prepared.get(),
                                     index->padded_sample, error_flag, stream);
@@ -1176,8 +1265,9 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
     }
 
     if (precision_strategy(c.strategy)) {
-        const uha::LowpPlan plan = enqueue_lowp_scores(index, ws, c.strategy, n, time_scan,
-                                                       scan_start, scan_stop, prepared);
+        const uha::LowpPlan plan =
+            enqueue_lowp_scores(index, ws, c.strategy, n, time_scan, scan_start, scan_stop,
+                                hierarchical ? scan_queries : prepared);
         const uint32_t k = static_cast<uint32_t>(
             std::min<uint64_t>(ws->candidates_per_query, index->rows));
         uint32_t* candidates = c.candidates != nullptr ? c.candidates : ws->candidates.get();
@@ -1185,6 +1275,15 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
                               static_cast<uint32_t>(index->rows),
                               index->lowp[static_cast<int>(lowp_type(c.strategy))].norms.get(),
                               k, candidates, stream);
+        if (hierarchical) {
+            // the reference's binary64 distance of every candidate, in the
+            // projected space; the smallest (lowest row on ties) is the answer
+            uha::launch_rescore_projected(candidates, k, static_cast<uint32_t>(n),
+                                          index->rows64.get(), ws->projected64.get(),
+                                          static_cast<uint32_t>(index->projection_dimension),
+                                          results, exact, stream);
+            return launches + 3;
+        }
         if (c.finish_stream != nullptr) {
             // the re-score of this batch runs on the finish stream, behind the
             // candidate selection (it overlaps the next batch's scores)
@@ -1389,11 +1488,8 @@ void validate_query_call(const uha_index* index, uha_workspace* ws,
             "query count exceeds CUDA workspace capacity");
     require(strategy == UHA_DIRECT || strategy == UHA_GEMM || precision_strategy(strategy),
             UHA_INVALID_ARGUMENT, "unknown CUDA query strategy");
-    require(!precision_strategy(strategy) ||
-                (index->metric == UHA_L2 && (index->kind == IndexKind::exact ||
-                                             index->kind == IndexKind::sampled)),
-            UHA_INVALID_ARGUMENT,
-            "precision strategies serve exact and flat L2 indexes");
+    require(!precision_strategy(strategy) || index->metric == UHA_L2, UHA_INVALID_ARGUMENT,
+            "precision strategies serve L2 indexes");
     if (count != 0) {
         require(out_indices != nullptr, UHA_INVALID_ARGUMENT, "output must not be null");
         require(queries != nullptr || index->dimension == 0, UHA_INVALID_ARGUMENT,
@@ -1647,6 +1743,8 @@ extern "C" uha_status uha_precision_scores(const uha_index* index, uha_workspace
     return guarded([&] {
         require(precision_strategy(strategy), UHA_INVALID_ARGUMENT,
                 "not a precision strategy");
+        require(index == nullptr || index->kind != IndexKind::hierarchical,
+                UHA_INVALID_ARGUMENT, "precision scores serve exact and flat L2 indexes");
         validate_query_call(index, ws, queries, query_count, query_count, strategy,
                             reinterpret_cast<const uint64_t*>(out_scores));
         if (query_count == 0 || index->padded_dim == 0) {

@@ -512,6 +512,50 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
+__global__ void sum_slabs_kernel(const float* __restrict__ partials, uint32_t splits,
+                                 uint64_t batch, uint64_t rows, float* __restrict__ out,
+                                 uint64_t out_pitch)
+{
+    const uint64_t total = batch * out_pitch;
+    const uint64_t slab = batch * rows;
+    for (uint64_t idx = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+         idx < total; idx += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t q = idx / out_pitch;
+        const uint64_t j = idx - q * out_pitch;
+        float v = 0.f;
+        if (j < rows) {
+            for (uint32_t sp = 0; sp < splits; ++sp) {
+                v += partials[sp * slab + q * rows + j];
+            }
+        }
+        out[idx] = v;
+    }
+}
+
+// One thread per (query, j), j fastest: the warp reads 32 consecutive
+// coefficients of one transposed row and broadcasts the query value.
+__global__ void project_queries64_kernel(const float* __restrict__ x, uint64_t batch,
+                                         uint64_t padded_k, uint64_t k,
+                                         const double* __restrict__ proj_t, uint64_t p,
+                                         double* __restrict__ y, int* error_flag)
+{
+    const uint64_t idx = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (idx >= batch * p) {
+        return;
+    }
+    const uint64_t q = idx / p;
+    const uint64_t j = idx - q * p;
+    const float* xq = x + q * padded_k;
+    double acc = 0.0;
+    for (uint64_t i = 0; i < k; ++i) {
+        acc = __dadd_rn(acc, __dmul_rn(static_cast<double>(xq[i]), proj_t[i * p + j]));
+    }
+    if (!isfinite(acc)) {
+        atomicOr(error_flag, 4);
+    }
+    y[idx] = acc;
+}
+
 __global__ void transpose_rows_kernel(const float* __restrict__ rows, uint64_t row_count,
                                       uint64_t padded_p, float* __restrict__ out,
                                       uint64_t r_pitch)
@@ -541,6 +585,25 @@ void launch_project_rows64(const float* sampled, uint64_t row_count,
     project_rows64_kernel<<<grid_for(row_count * p), kThreads, 0, stream>>>(
         sampled, row_count, padded_k, k, projection, p, reps, bad);
     check_cuda(cudaGetLastError(), "cannot launch row projection kernel");
+}
+
+void launch_sum_slabs(const float* partials, uint32_t splits, uint64_t batch,
+                      uint64_t rows, float* out, uint64_t out_pitch, cudaStream_t stream)
+{
+    sum_slabs_kernel<<<grid_for(batch * out_pitch), kThreads, 0, stream>>>(
+        partials, splits, batch, rows, out, out_pitch);
+    check_cuda(cudaGetLastError(), "cannot launch slab sum kernel");
+}
+
+void launch_project_queries64(const float* x, uint64_t batch, uint64_t padded_k,
+                              uint64_t k, const double* proj_t, uint64_t p, double* y,
+                              int* error_flag, cudaStream_t stream)
+{
+    const uint64_t threads = batch * p;
+    project_queries64_kernel<<<static_cast<uint32_t>((threads + kThreads - 1) / kThreads),
+                               kThreads, 0, stream>>>(x, batch, padded_k, k, proj_t, p, y,
+                                                      error_flag);
+    check_cuda(cudaGetLastError(), "cannot launch binary64 query projection kernel");
 }
 
 void launch_transpose_rows(const float* rows, uint64_t row_count, uint64_t padded_p,

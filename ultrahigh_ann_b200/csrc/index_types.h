@@ -66,10 +66,13 @@ struct uha_index {
     // L1 hierarchy: scan_rows transposed, padded_dim x rows_pitch
     uha::DeviceBuffer<float> scan_rows_t;
     uint64_t rows_pitch = 0;
+    // L2 hierarchy: projection64 transposed, sample_size x p
+    uha::DeviceBuffer<double> projection64_t;
     uha_space_usage usage{};
     // precision strategies: built on first use (index_bf16 / index_fp8)
     mutable std::mutex lowp_mutex;
     mutable uha::LowpRows lowp[2];
+    mutable uha::LowpRows lowp_projection[2];  // L2 hierarchy: the p x k projection
 };
 
 // A scan shape chosen by the autotuner for one (batch size, strategy) of a
@@ -110,6 +113,12 @@ struct uha_workspace {
     uha::DeviceBuffer<unsigned int> median_min;   // L1 hierarchy: sampled minimum per query
     uha::DeviceBuffer<float> coord_err;   // L1 hierarchy: batch x padded p query errors
     uha::DeviceBuffer<float> pair_err;    // L1 hierarchy: batch x rows median errors
+    // precision form of the L2 hierarchy: rounded gathered queries, their
+    // scales, and the reference's binary64 projection of each query
+    uha::DeviceBuffer<unsigned char> gathered_lp;
+    uha::DeviceBuffer<float> gathered_scales;
+    uha::DeviceBuffer<unsigned int> gathered_amax;
+    uha::DeviceBuffer<double> projected64;
     uint32_t candidates_per_query = 32;
     std::vector<TunedPlan> tuned;  // autotuned shapes (uha_workspace_autotune)
 

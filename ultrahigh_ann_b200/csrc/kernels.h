@@ -215,6 +215,23 @@ void launch_lowp_scores(const LowpPlan& plan, LowpType type, const void* rows_lp
 void launch_lowp_topk(const float* partials, uint32_t splits, uint32_t batch,
                       uint32_t rows, const float* norms, uint32_t k,
                       uint32_t* candidates, cudaStream_t stream);
+// Precision form of the L2 hierarchy: out[q][j] = sum over the slabs of
+// partials[s][q][j] for j < rows, zeros up to out_pitch.
+void launch_sum_slabs(const float* partials, uint32_t splits, uint64_t batch,
+                      uint64_t rows, float* out, uint64_t out_pitch, cudaStream_t stream);
+// The reference's binary64 projection of gathered queries, y[q][j] =
+// sum_i double(x[q][i]) * P[j][i] in i order (proj_t = P transposed,
+// [k][p]); error_flag |= 4 for a non-finite result.
+void launch_project_queries64(const float* x, uint64_t batch, uint64_t padded_k,
+                              uint64_t k, const double* proj_t, uint64_t p, double* y,
+                              int* error_flag, cudaStream_t stream);
+// Per query, the candidate with the smallest (reference binary64 squared
+// distance of the projected row rows64[row] to y64[q], row): results[q] and
+// exact_distances[q]. Candidates 0xffffffff are skipped.
+void launch_rescore_projected(const uint32_t* candidates, uint32_t k, uint32_t batch,
+                              const double* rows64, const double* y64, uint32_t p,
+                              Result* results, double* exact_distances,
+                              cudaStream_t stream);
 // Binary64 certification interval [S (1 - rel) - abs, S (1 + rel) + abs] of
 // a parallel binary64 sum S of the reference CPU's own terms.
 struct Bound64 {

@@ -67,7 +67,8 @@ uint64_t workspace_device_bytes(const uha_workspace* ws)
            ws->finalize_scratch.bytes() + ws->queries_lp.bytes() + ws->query_scales.bytes() +
            ws->query_amax.bytes() + ws->candidates.bytes() + ws->cand_dist.bytes() +
            ws->rescore_done.bytes() + ws->median_min.bytes() + ws->coord_err.bytes() +
-           ws->pair_err.bytes();
+           ws->pair_err.bytes() + ws->gathered_lp.bytes() + ws->gathered_scales.bytes() +
+           ws->gathered_amax.bytes() + ws->projected64.bytes();
 }
 
 bool trivial_index(const uha_index* index)
