@@ -733,6 +733,31 @@ def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=1
         specs[k]["replayed"] = ls["replayed_queries"]
         specs[k]["tuned_scan_ms"] = round(batch.tuning(k)["best_ms"], 3)
         del ws
+    # the same batch with the L2 hierarchies on the BF16 precision strategy
+    # (tensor-core projection and scores, 32 candidates, binary64 re-score)
+    bf16 = uha.QueryStrategy.gemm_bf16_rerank
+    mixed = uha.QueryBatch([(ix, per_index, bf16 if spec["metric"] == "l2"
+                             else uha.QueryStrategy.direct)
+                            for ix, spec in zip(indexes, specs)], autotune=True)
+    mixed.run([qdev.data_ptr()] * len(indexes), on_device=True)
+    mixed_ms = []
+    torch.cuda.nvtx.range_push("timed_mixed_graph")
+    for _ in range(reps):
+        mres = mixed.run(None)
+        mixed_ms.append(mixed.stats()["device_ms"])
+    torch.cuda.nvtx.range_pop()
+    precision = []
+    for k, spec in enumerate(specs):
+        if spec["metric"] != "l2":
+            continue
+        want_rows, want_dist = res[k]
+        got_rows, got_dist = mres[k]
+        excess = (got_dist - want_dist) / np.maximum(want_dist, 1e-300)
+        precision.append({"rows": spec["rows"], "p": spec["p"],
+                          "agreement_vs_direct": round(float(np.mean(got_rows == want_rows)), 4),
+                          "distance_excess_mean": float(excess.mean()),
+                          "distance_excess_max": float(excess.max())})
+    del mixed
     picks = np.random.default_rng(9).choice(per_index, checked, replace=False)
     q_host = qdev.index_select(0, torch.from_numpy(picks).cuda()).double().cpu().numpy()
     ok = 0
@@ -749,6 +774,11 @@ def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=1
             "graph_nodes": st["graph_nodes"], "kernels_per_run": st["kernel_launches"],
             "replayed": st["replayed_queries"], "answers_equal_index_by_index": same,
             "binary64_checked": {"queries": checked * len(indexes), "distance_optimal": ok},
+            "l2_bf16_rerank": {"queries_per_s": round(total / (min(mixed_ms) * 1e-3), 1),
+                               "device_ms": round(min(mixed_ms), 3),
+                               "strategy": "L2 hierarchies gemm_bf16_rerank (k = 32), "
+                                           "L1 hierarchies direct",
+                               "indexes": precision},
             "setup_s": {"generate_on_device": round(gen_s, 1),
                         "probabilities": round(prob_s, 1), "build": round(build_s, 1),
                         "autotune_and_capture": round(setup_s, 1)}}

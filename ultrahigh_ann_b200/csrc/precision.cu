@@ -662,6 +662,127 @@ __global__ void __launch_bounds__(kTopkThreads)
     }
 }
 
+// Top-k for k <= 32 as a warp-wide sorted list (one key per lane, ascending
+// by lane) with a two-slot queue per lane (the warp-select scheme of Johnson,
+// Douze and Jegou, "Billion-scale similarity search with GPUs", 2017): a key
+// below the list's largest enters the lane's queue; when a queue fills, the
+// warp sorts each queue slot across its lanes (bitonic network over the 32
+// lanes) and merges it into the list. Most keys cost a load, an FMA and one
+// comparison.
+__device__ __forceinline__ unsigned long long warp_sort32(unsigned long long v, int lane)
+{
+#pragma unroll
+    for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+        for (int stride = size / 2; stride > 0; stride /= 2) {
+            const unsigned long long o = __shfl_xor_sync(0xffffffffu, v, stride);
+            const bool ascending = (lane & size) == 0;
+            const bool low = (lane & stride) == 0;
+            v = (low == ascending) ? (o < v ? o : v) : (o < v ? v : o);
+        }
+    }
+    return v;
+}
+
+// The 32 smallest of two ascending warp lists, ascending: min(w_i, e_{31-i})
+// is bitonic and holds them; one bitonic merge sorts it.
+__device__ __forceinline__ unsigned long long warp_merge32(unsigned long long w,
+                                                           unsigned long long e, int lane)
+{
+    const unsigned long long er = __shfl_sync(0xffffffffu, e, 31 - lane);
+    unsigned long long m = er < w ? er : w;
+#pragma unroll
+    for (int stride = 16; stride > 0; stride /= 2) {
+        const unsigned long long o = __shfl_xor_sync(0xffffffffu, m, stride);
+        const bool low = (lane & stride) == 0;
+        m = low ? (o < m ? o : m) : (o < m ? m : o);
+    }
+    return m;
+}
+
+template <bool kSingleSlab>
+__global__ void __launch_bounds__(kTopkThreads)
+    warp_topk_kernel(const float* __restrict__ partials, uint32_t splits, uint32_t batch,
+                     uint32_t row_count, const float* __restrict__ norms, uint32_t k,
+                     uint32_t* __restrict__ candidates)
+{
+    constexpr int kWarps = kTopkThreads / 32;
+    constexpr int U = 8;  // rows per lane whose loads are in flight together
+    __shared__ unsigned long long lists[kWarps][32];
+    const uint32_t q = blockIdx.x;
+    const int warp = threadIdx.x / 32;
+    const int lane = threadIdx.x % 32;
+    const uint64_t split_stride = static_cast<uint64_t>(batch) * row_count;
+    const float* base = partials + static_cast<uint64_t>(q) * row_count;
+    unsigned long long list = ~0ull;
+    unsigned long long largest = ~0ull;
+    unsigned long long slot0 = ~0ull;
+    unsigned long long slot1 = ~0ull;
+    int queued = 0;
+    auto flush = [&]() {
+        list = warp_merge32(list, warp_sort32(slot0, lane), lane);
+        list = warp_merge32(list, warp_sort32(slot1, lane), lane);
+        slot0 = ~0ull;
+        slot1 = ~0ull;
+        queued = 0;
+        largest = __shfl_sync(0xffffffffu, list, 31);
+    };
+    for (uint32_t first = warp * 32; first < row_count; first += kTopkThreads * U) {
+        float e[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint32_t row = first + lane + u * kTopkThreads;
+            float dot = 0.f;
+            if (row < row_count) {
+                if constexpr (kSingleSlab) {
+                    dot = base[row];
+                } else {
+                    for (uint32_t sp = 0; sp < splits; ++sp) {
+                        dot += base[sp * split_stride + row];
+                    }
+                }
+            }
+            e[u] = dot;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint32_t row = first + lane + u * kTopkThreads;
+            if (row < row_count) {
+                const float est = __fmaf_rn(-2.f, e[u], norms[row]);
+                const unsigned long long key =
+                    (static_cast<unsigned long long>(ordered_key_bits(est)) << 32) | row;
+                if (key < largest) {
+                    if (queued == 0) {
+                        slot0 = key;
+                    } else {
+                        slot1 = key;
+                    }
+                    ++queued;
+                }
+            }
+            if (__any_sync(0xffffffffu, queued == 2)) {
+                flush();
+            }
+        }
+    }
+    if (__any_sync(0xffffffffu, queued != 0)) {
+        flush();
+    }
+    lists[warp][lane] = list;
+    __syncthreads();
+    if (warp == 0) {
+        list = lists[0][lane];
+#pragma unroll 1
+        for (int w = 1; w < kWarps; ++w) {
+            list = warp_merge32(list, lists[w][lane], lane);
+        }
+        if (static_cast<uint32_t>(lane) < k) {
+            candidates[static_cast<uint64_t>(q) * k + lane] =
+                list == ~0ull ? 0xffffffffu : static_cast<uint32_t>(list & 0xffffffffu);
+        }
+    }
+}
+
 // ------------------------------------------------------------ host side
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
@@ -939,15 +1060,19 @@ void launch_lowp_topk(const float* partials, uint32_t splits, uint32_t batch,
     if (batch == 0) {
         return;
     }
+    // up to 16 candidates: short per-thread lists; up to 32: the warp list
     if (k <= 8) {
         topk_kernel<8><<<batch, kTopkThreads, 0, stream>>>(partials, splits, batch, rows,
                                                            norms, k, candidates);
     } else if (k <= 16) {
         topk_kernel<16><<<batch, kTopkThreads, 0, stream>>>(partials, splits, batch, rows,
                                                             norms, k, candidates);
+    } else if (k <= 32 && splits == 1) {
+        warp_topk_kernel<true><<<batch, kTopkThreads, 0, stream>>>(partials, splits, batch,
+                                                                   rows, norms, k, candidates);
     } else if (k <= 32) {
-        topk_kernel<32><<<batch, kTopkThreads, 0, stream>>>(partials, splits, batch, rows,
-                                                            norms, k, candidates);
+        warp_topk_kernel<false><<<batch, kTopkThreads, 0, stream>>>(partials, splits, batch,
+                                                                    rows, norms, k, candidates);
     } else {
         topk_kernel<64><<<batch, kTopkThreads, 0, stream>>>(partials, splits, batch, rows,
                                                             norms, k, candidates);
