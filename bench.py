@@ -278,6 +278,8 @@ def run_engine(args):
         line["serving"] = serving(ds)
         torch.cuda.empty_cache()
         line["wide"] = wide()
+        torch.cuda.empty_cache()
+        line["hierarchies_full"] = hierarchies_full()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -786,21 +788,34 @@ def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=1
 
 def serving(ds, rates=(10_000, 100_000, 1_000_000, 2_000_000), seconds=0.5, pool=2048):
     """Request loop over 8 device-resident indexes (exact, flat and
-    hierarchical, L1 and L2; r from 33 to 7,028; six at d = 60,660 and two
+    hierarchical, L1 and L2; r from 33 to 65,536; six at d = 60,660 and two
     hierarchies at d = 262,144 with BF16-stored values), Poisson arrivals with
     a uniformly chosen index per request, queries from a device-resident pool
-    of each dimension. Plain strategies, then BF16 + re-score on the exact and
-    flat L2 indexes; agreement of the exact L2 answers with the binary64 exact
-    argmin."""
+    of each dimension. The 65,536-row flat index is built from a BF16 matrix
+    generated on the device (same law, 33 latent classes) with the
+    probabilities of the 7,028-row matrix. Plain strategies, then BF16 +
+    re-score on the exact and flat L2 indexes; agreement of the exact L2
+    answers with the binary64 exact argmin."""
     import torch
 
     import ultrahigh_ann_b200 as uha
+    from ultrahigh_ann_b200 import synthetic
 
     S = uha.QueryStrategy
     pl2, pl1 = _probabilities("l2", ds.rows), _probabilities("l1", ds.rows)
     r33 = ds.rows[:33]
+
+    def flat_65536():
+        big = synthetic.device_row_dataset(rows=65_536, classes=33, queries=1,
+                                           d=ds.rows.shape[1], seed=5, storage="bfloat16")
+        ix = uha.CudaSampledCoordinateL2AnnIndex(uha.DeviceMatrix.from_torch(big.rows), pl2,
+                                                 32, uha.MT19937_64(7))
+        del big
+        torch.cuda.empty_cache()
+        return ix
+
     build = [
-        ("exact_l2_r33", lambda: uha.CudaExactL2Index(r33), True),
+        ("flat_l2_r65536_T32", flat_65536, True),
         ("flat_l2_r33_T8", lambda: uha.CudaSampledCoordinateL2AnnIndex(
             r33, pl2, 8, uha.MT19937_64(1)), True),
         ("exact_l2_r7028", lambda: uha.CudaExactL2Index(ds.rows), True),
