@@ -56,16 +56,18 @@ typedef enum uha_metric {
  *     returned index equals the reference CPU index on every query.
  *   UHA_GEMM: the reference's unrefined binary32 norm identity
  *     ||r||^2 + ||q||^2 - 2 r.q (L2 only; L1 treats it as DIRECT).
- *   UHA_GEMM_BF16_RERANK, UHA_GEMM_FP8_RERANK (exact and flat L2 indexes):
- *     rows and queries rounded to BF16, or to FP8-E4M3 with one scale per
- *     row and per query; the score matrix runs on the tensor cores with FP32
- *     accumulation; the k rows with the smallest estimate ||r~||^2 - 2 r~.q~
- *     (uha_workspace_set_candidates) are re-scored from the original rows
- *     (the reference CPU's binary64 terms, added in parallel, with a
- *     certified bound; near-ties replay the CPU's order). The answer equals
- *     the reference CPU index whenever that row is among the k candidates.
- *     The low-precision copy of the rows is built on the first query that
- *     needs it. */
+ *   UHA_GEMM_BF16_RERANK, UHA_GEMM_FP8_RERANK (exact, flat and
+ *     hierarchical L2 indexes): rows and queries rounded to BF16, or to
+ *     FP8-E4M3 with one scale per row and per query; the score matrix runs
+ *     on the tensor cores with FP32 accumulation; the k rows with the
+ *     smallest estimate ||r~||^2 - 2 r~.q~ (uha_workspace_set_candidates) are
+ *     re-scored from the original rows (the reference CPU's binary64 terms,
+ *     added in parallel, with a certified bound; near-ties replay the CPU's
+ *     order). Hierarchies also project the queries on the tensor cores (the
+ *     rounded p x k projection times the batch) and re-score by the
+ *     reference's binary64 projected distance. The answer equals the
+ *     reference CPU index whenever that row is among the k candidates. The
+ *     low-precision copies are built on the first query that needs them. */
 typedef enum uha_strategy {
     UHA_DIRECT = 0,
     UHA_GEMM = 1,

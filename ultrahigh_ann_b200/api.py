@@ -78,9 +78,10 @@ class QueryStrategy(enum.IntEnum):
 
     direct = _abi.DIRECT
     gemm = _abi.GEMM
-    # precision forms (appended; exact and flat L2 indexes): tensor-core
-    # scores of rounded rows/queries, then a certified binary32 re-score of
-    # the best candidates per query (QueryWorkspace.set_candidates)
+    # precision forms (appended; exact, flat and hierarchical L2 indexes):
+    # tensor-core scores of rounded rows/queries (hierarchies: and of the
+    # projection), then a binary64 re-score of the best candidates per query
+    # (QueryWorkspace.set_candidates)
     gemm_bf16_rerank = _abi.GEMM_BF16_RERANK
     gemm_fp8_rerank = _abi.GEMM_FP8_RERANK
 
