@@ -56,6 +56,9 @@ def parse_args():
                    choices=["", "precision", "batched", "serving", "centroids", "wide",
                             "hierarchies"],
                    help="only this section of the bench (one JSON line)")
+    p.add_argument("--hier-shape", default="",
+                   help="ROWS,DIM,QUERIES of the full-size hierarchical batch "
+                        "(--only hierarchies; smaller shapes for profiler captures)")
     p.add_argument("--precision-batch", type=int, default=0,
                    help="with --precision-only: one batch size (2048 queries)")
     p.add_argument("--precision-shape", default="",
@@ -686,7 +689,7 @@ def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=1
     specs, indexes = [], []
     t = time.perf_counter()
     i = 0
-    for r in (1024, 7028, rows):
+    for r in sorted({min(1024, rows), min(7028, rows), rows}):
         for p in (16, 64, 256):
             for metric in ("l2", "l1"):
                 if r == 1024 and p == 256:
@@ -970,7 +973,11 @@ def run_section(args):
         print(json.dumps({"wide": wide()}), flush=True)
         return
     if args.only == "hierarchies":
-        print(json.dumps({"hierarchies_full": hierarchies_full()}), flush=True)
+        shape = {}
+        if args.hier_shape:
+            rows, dim, queries = (int(x) for x in args.hier_shape.split(","))
+            shape = {"rows": rows, "dim": dim, "per_index": queries}
+        print(json.dumps({"hierarchies_full": hierarchies_full(**shape)}), flush=True)
         return
     ds = synthetic.row_dataset(rows=ROWS, classes=33, queries=4096, d=DIM, seed=1,
                                query_stream=0)
