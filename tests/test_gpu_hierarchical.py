@@ -164,3 +164,27 @@ def test_hierarchical_edge_cases(metric):
             coordinate_sample=uha.CoordinateSample([0], [1], [1.0]))
     with pytest.raises(uha.CudaRuntimeError):
         cls(two, None, 3, uha.MT19937_64(1), coordinate_sample=uha.CoordinateSample())
+
+
+@pytest.mark.parametrize("metric", ["l2", "l1"])
+def test_hierarchical_near_ties_match_reference(oracle_module, metric):
+    """Groups of six rows equal up to relative 1e-6 noise: their projected
+    distances differ far below the binary32 bounds, so most queries take the
+    binary64 replay (and, for L1, the per-pair median bounds must not
+    exclude the reference's row)."""
+    rng = np.random.default_rng(3)
+    base = (np.abs(rng.standard_normal((20, 500))) * 10).astype(np.float32)
+    rows = np.repeat(base, 6, axis=0)
+    rows = (rows * (1 + 1e-6 * rng.standard_normal(rows.shape))).astype(np.float32)
+    queries = (base[:12] + 0.05 * rng.standard_normal((12, 500))).astype(np.float32)
+    sample = uha.CoordinateSample(np.arange(0, 500, 2), np.ones(250, np.uint64),
+                                  np.full(250, 2.0))
+    for p in (16, 64, 255):
+        index = CLASSES[metric](rows, None, p, uha.MT19937_64(p),
+                                coordinate_sample=sample)
+        expected, edist = oracle_module.hierarchical(metric, rows, sample.source_columns,
+                                                     index.projection, queries)
+        for batch in (1, 12):
+            got, dist = run(index, queries, batch)
+            assert np.array_equal(got, expected), (p, batch)
+            assert np.allclose(dist, edist, rtol=DIST_RTOL, atol=1e-30)

@@ -340,3 +340,24 @@ def test_timing_samples_every_stride_batch():
     assert ws.last_stats()["timed_scans"] == 0
     with pytest.raises(uha.InvalidArgument):
         ws.set_timing(True, stride=0)
+
+
+@pytest.mark.parametrize("metric", ["l2", "l1"])
+def test_binary32_overflowing_distances_match_reference(oracle_module, metric):
+    """Distances above the binary32 range (finite in the CPU's binary64) have
+    no finite upper bound: the query is replayed and the CPU's row returned,
+    both when one row overflows and when every row does."""
+    rng = np.random.default_rng(5)
+    rows = rng.standard_normal((50, 64)).astype(np.float32)
+    queries = rng.standard_normal((12, 64)).astype(np.float32)
+    scale = np.float32(4e18 if metric == "l2" else 1e37)
+    one = rows.copy()
+    one[7] *= scale
+    everything = rows * scale
+    cls = uha.CudaExactL2Index if metric == "l2" else uha.CudaExactL1Index
+    for r, q in ((one, queries), (everything, queries * scale)):
+        expected, edist = oracle_module.exact(metric, r, q)
+        assert np.all(np.isfinite(edist))
+        for batch in (1, 12):
+            got, _ = run(cls(r), q, batch)
+            assert np.array_equal(got, expected), batch
