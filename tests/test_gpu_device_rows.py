@@ -15,14 +15,14 @@ pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
 
-def _answers(index, queries, batch=16):
+def _answers(index, queries, batch=16, strategy=uha.QueryStrategy.direct):
     ws = index.make_query_workspace(batch)
     n = queries.shape[0]
     out = np.zeros(n, np.uint64)
     dist = np.zeros(n, np.float64)
     for s in range(0, n, batch):
         e = min(n, s + batch)
-        index.query_batch(queries[s:e], e - s, out[s:e], ws, distances=dist[s:e])
+        index.query_batch(queries[s:e], e - s, out[s:e], ws, strategy, distances=dist[s:e])
     return out, dist
 
 
@@ -90,6 +90,11 @@ def test_hierarchical_from_device_rows(data, metric, p):
         a, da = _answers(want, ds.queries)
         b, db = _answers(got, ds.queries)
         assert np.array_equal(a, b) and np.array_equal(da, db)
+        if metric == "l2":
+            bf16 = uha.QueryStrategy.gemm_bf16_rerank
+            a, da = _answers(want, ds.queries, strategy=bf16)
+            b, db = _answers(got, ds.queries, strategy=bf16)
+            assert np.array_equal(a, b) and np.array_equal(da, db)
 
 
 def test_device_rows_need_probabilities(data):

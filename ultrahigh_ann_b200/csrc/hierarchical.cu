@@ -354,16 +354,24 @@ __device__ __forceinline__ float median_threshold(const unsigned int* min_bits,
 }
 
 // The stage-2 count over the transposed rows (rows_t[j][row], row pitch
-// r_pitch): two rows per thread and Q queries per CTA, so each row value
-// read from L2 serves Q queries and each query value broadcast from shared
-// memory serves two rows. A pruned pair stores -T, any other pair the survivor mark (bits
+// r_pitch): R rows per thread and Q queries per CTA, so each row value read
+// from L2 serves Q queries and each query value broadcast from shared memory
+// serves R rows. A pruned pair stores -T, any other pair the survivor mark (bits
 // 0xffffffff, a NaN no distance takes) for median_survivor_kernel. Values
 // above T are counted from the sign bit of T - |r_j - y_j|: a rounded
 // difference of binary32 values has the sign of the exact one (and is +0
 // when they are equal), so the count is that of |r_j - y_j| > T exactly.
 constexpr int kCountRows = 128;
-constexpr int kCountRowsPerThread = 2;
 constexpr uint32_t kSurvivorMark = 0xffffffffu;
+
+// Rows per thread: 2 with 4 or 8 queries per CTA (4 rows measured no faster:
+// 128 registers), 1 for the smallest batches so that the grid still spreads
+// over the SMs.
+template <int Q>
+__host__ __device__ constexpr int count_rows_per_thread()
+{
+    return Q >= 4 ? 2 : 1;
+}
 
 template <int Q>
 __global__ void __launch_bounds__(kCountRows)
@@ -374,6 +382,7 @@ __global__ void __launch_bounds__(kCountRows)
                         const float* __restrict__ query_err, float row_err_max, float rel,
                         float abs_err, float* __restrict__ partials)
 {
+    constexpr int R = count_rows_per_thread<Q>();
     extern __shared__ float4 ys4[];  // [Q][padded_p / 4]
     float* ys = reinterpret_cast<float*>(ys4);
     const uint32_t q0 = q_begin + blockIdx.y * Q;
@@ -383,33 +392,33 @@ __global__ void __launch_bounds__(kCountRows)
         ys[i] = (q0 + qq < batch && j < p) ? queries[uint64_t(q0 + qq) * padded_p + j] : 0.f;
     }
     float t[Q];
-    uint32_t over[Q][kCountRowsPerThread];
+    uint32_t over[Q][R];
 #pragma unroll
     for (int qq = 0; qq < Q; ++qq) {
         t[qq] = q0 + qq < batch
                     ? median_threshold(min_bits, query_err, q0 + qq, row_err_max, rel, abs_err)
                     : 0.f;
 #pragma unroll
-        for (int k = 0; k < kCountRowsPerThread; ++k) {
+        for (int k = 0; k < R; ++k) {
             over[qq][k] = 0;
         }
     }
     __syncthreads();
-    // rows row0 + k * kCountRows (k < kCountRowsPerThread): each broadcast
+    // rows row0 + k * kCountRows (k < R): each broadcast
     // query value serves them all
-    const uint32_t row0 = blockIdx.x * (kCountRows * kCountRowsPerThread) + threadIdx.x;
-    const float* col[kCountRowsPerThread];
+    const uint32_t row0 = blockIdx.x * (kCountRows * R) + threadIdx.x;
+    const float* col[R];
 #pragma unroll
-    for (int k = 0; k < kCountRowsPerThread; ++k) {
+    for (int k = 0; k < R; ++k) {
         const uint32_t row = row0 + k * kCountRows;
         col[k] = rows_t + (row < row_count ? row : 0);
     }
     const uint32_t p4 = p & ~3u;
     const uint32_t pitch4 = padded_p / 4;
     for (uint32_t j = 0; j < p4; j += 4) {
-        float r[kCountRowsPerThread][4];
+        float r[R][4];
 #pragma unroll
-        for (int k = 0; k < kCountRowsPerThread; ++k) {
+        for (int k = 0; k < R; ++k) {
 #pragma unroll
             for (int m = 0; m < 4; ++m) {
                 r[k][m] = col[k][uint64_t(j + m) * r_pitch];
@@ -420,7 +429,7 @@ __global__ void __launch_bounds__(kCountRows)
             const float4 y4 = ys4[qq * pitch4 + j / 4];
             const float y[4] = {y4.x, y4.y, y4.z, y4.w};
 #pragma unroll
-            for (int k = 0; k < kCountRowsPerThread; ++k) {
+            for (int k = 0; k < R; ++k) {
 #pragma unroll
                 for (int m = 0; m < 4; ++m) {
                     over[qq][k] +=
@@ -431,7 +440,7 @@ __global__ void __launch_bounds__(kCountRows)
     }
     for (uint32_t j = p4; j < p; ++j) {
 #pragma unroll
-        for (int k = 0; k < kCountRowsPerThread; ++k) {
+        for (int k = 0; k < R; ++k) {
             const float rv = col[k][uint64_t(j) * r_pitch];
 #pragma unroll
             for (int qq = 0; qq < Q; ++qq) {
@@ -443,7 +452,7 @@ __global__ void __launch_bounds__(kCountRows)
     }
     const uint32_t needed = p % 2 != 0 ? p / 2 + 1 : p / 2;
 #pragma unroll
-    for (int k = 0; k < kCountRowsPerThread; ++k) {
+    for (int k = 0; k < R; ++k) {
         const uint32_t row = row0 + k * kCountRows;
         if (row >= row_count) {
             continue;
@@ -671,8 +680,8 @@ void launch_median_count(const float* rows_t, uint32_t r_pitch, uint32_t rc, uin
     // grid.y is limited to 65,535 query groups per launch
     const uint64_t groups = (static_cast<uint64_t>(b) + Q - 1) / Q;
     for (uint64_t g = 0; g < groups; g += 65535) {
-        const dim3 grid((rc + kCountRows * kCountRowsPerThread - 1) /
-                            (kCountRows * kCountRowsPerThread),
+        constexpr uint32_t per_cta = kCountRows * count_rows_per_thread<Q>();
+        const dim3 grid((rc + per_cta - 1) / per_cta,
                         static_cast<uint32_t>(std::min<uint64_t>(65535, groups - g)));
         median_count_kernel<Q><<<grid, kCountRows, smem, stream>>>(
             rows_t, r_pitch, rc, pp, pv, queries, b, static_cast<uint32_t>(g * Q), min_bits,
