@@ -35,8 +35,25 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_library_is_built_for_sm100a():
-    data = _abi.LIBRARY_PATH.read_bytes()
-    assert b"sm_100a" in data
+    from ultrahigh_ann_b200 import build
+    assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+    assert _abi.LIBRARY_PATH.exists()
+
+
+def test_device_matrix_descriptor_needs_no_device():
+    m = uha.DeviceMatrix(4096, 3, 5, "bfloat16", row_stride=8)
+    st = m._struct()
+    assert (st.data, st.type, st.rows, st.columns, st.row_stride) == (4096, _abi.VALUES_BF16,
+                                                                      3, 5, 8)
+    assert uha.DeviceMatrix(64, 2, 7)._struct().row_stride == 7
+    with pytest.raises(uha.InvalidArgument):
+        uha.DeviceMatrix(64, 2, 7, "float16")._struct()
+    torch = pytest.importorskip("torch")
+    with pytest.raises(uha.InvalidArgument):
+        uha.DeviceMatrix.from_torch(torch.zeros((2, 3)))
+    # a host-side operation on a device matrix names what it needs
+    with pytest.raises(uha.InvalidArgument, match="host representative matrix"):
+        uha.compute_importance_probabilities_host("l2", m)
 
 
 def test_no_device_is_reported_as_runtime_error_or_none():
