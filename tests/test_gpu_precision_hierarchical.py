@@ -74,7 +74,7 @@ def _projected_distances(index, rows, queries, picked):
 
 
 @pytest.mark.parametrize("strategy", [BF16, FP8])
-@pytest.mark.parametrize("p,k", [(16, 1), (16, 8), (64, 32), (256, 8)])
+@pytest.mark.parametrize("p,k", [(1, 4), (2, 8), (16, 1), (16, 8), (64, 32), (256, 8)])
 def test_reported_distance_is_reference_distance_of_answer(oracle_module, strategy, p, k):
     ds = synthetic.row_dataset(rows=700, classes=9, queries=60, d=2500, seed=p + k)
     probs = oracle_module.probabilities("l2", ds.rows)
