@@ -10,6 +10,7 @@ The engine never imports this module.
 from __future__ import annotations
 
 import ctypes
+import os
 import subprocess
 from ctypes import c_char_p, c_double, c_int, c_int64, c_uint64, c_void_p
 from pathlib import Path
@@ -24,9 +25,20 @@ _oracle = None
 _ref = None
 
 
+REFERENCE_TREE_ENV = "UHA_REFERENCE_DIR"
+DEFAULT_REFERENCE_TREE = "/root/reference"
+
+
 def build() -> None:
-    """Builds liboracle.so and, when the reference sources exist, _ref/."""
-    subprocess.run(["make", "-s", "-C", str(HERE), "-j8"], check=True)
+    """Builds liboracle.so and, when the reference sources exist, _ref/.
+
+    The reference tree is UHA_REFERENCE_DIR when set, else the container's
+    read-only checkout; the Makefile itself has no default for it."""
+    tree = os.environ.get(REFERENCE_TREE_ENV, DEFAULT_REFERENCE_TREE)
+    cmd = ["make", "-s", "-C", str(HERE), "-j8"]
+    if (Path(tree) / "src").is_dir():
+        cmd.append(f"REF={tree}")
+    subprocess.run(cmd, check=True)
 
 
 def _p(a):
@@ -128,6 +140,9 @@ def ref_lib() -> ctypes.CDLL:
         lib.ref_exact_destroy.argtypes = [c_void_p]
         lib.ref_exact_query.restype = c_int
         lib.ref_exact_query.argtypes = [c_void_p, c_void_p, c_uint64, c_int, c_void_p]
+        lib.ref_exact_query_batched.restype = c_int
+        lib.ref_exact_query_batched.argtypes = [c_void_p, c_void_p, c_uint64, c_uint64,
+                                                c_int, c_void_p]
         lib.ref_sha256_file.restype = c_int
         lib.ref_sha256_file.argtypes = [c_char_p, c_void_p]
         lib.ref_probabilities_save.restype = c_int
@@ -324,6 +339,15 @@ class RefExactIndex:
         out = np.zeros(q.shape[0], np.uint64)
         _ref_check(ref_lib().ref_exact_query(self._h, _p(q), q.shape[0], threads,
                                              _p(out)))
+        return out
+
+    def query_in_batches(self, queries, batch: int, threads: int) -> np.ndarray:
+        """L2: query_batch calls of `batch` queries with the reference's
+        automatic strategy (parallel over rows for one query)."""
+        q = _f32(queries).reshape(-1, self.dimension)
+        out = np.zeros(q.shape[0], np.uint64)
+        _ref_check(ref_lib().ref_exact_query_batched(self._h, _p(q), q.shape[0], batch,
+                                                     threads, _p(out)))
         return out
 
     def __del__(self):

@@ -185,6 +185,33 @@ int ref_exact_query(void* handle, const float* queries, uint64_t n,
     });
 }
 
+// L2 only: the queries in calls of `batch` queries each, every call a
+// query_batch with CpuDenseL2QueryStrategy::automatic on `threads` OpenMP
+// threads -- the reference's own choice of parallel dimension for that batch
+// size (src/core/dense_l2_scan_index.cpp:82-101: parallel_representatives for
+// one query, parallel_queries once the batch reaches half the threads).
+int ref_exact_query_batched(void* handle, const float* queries, uint64_t n,
+                            uint64_t batch, int threads, uint64_t* out)
+{
+    return guarded([&] {
+        auto* h = static_cast<RefExact*>(handle);
+        if (!h->l2) {
+            throw std::invalid_argument("ref_exact_query_batched serves L2 indexes");
+        }
+        const uint64_t d = h->matrix.cols();
+        omp_set_num_threads(std::max(1, threads));
+        const uint64_t b = std::max<uint64_t>(1, batch);
+        std::vector<std::size_t> o(b);
+        for (uint64_t s = 0; s < n; s += b) {
+            const uint64_t m = std::min(b, n - s);
+            h->l2->query_batch(std::span<const float>(queries + s * d, m * d), m,
+                               std::span<std::size_t>(o.data(), m),
+                               CpuDenseL2QueryStrategy::automatic);
+            std::copy(o.begin(), o.begin() + m, out + s);
+        }
+    });
+}
+
 // build_coordinate_sample; engine state after sampling is written to state_out.
 int ref_sample(const double* probs, uint64_t d, uint64_t repetitions,
                uint64_t seed, uint64_t* cols, uint64_t* mult, double* invp,

@@ -41,11 +41,16 @@ def workspace_query(index, queries, n):
     return out, dist
 
 
-@pytest.mark.parametrize("kind", ["exact_l2", "exact_l1", "flat_l2", "flat_l1"])
+@pytest.mark.parametrize("kind", ["exact_l2", "exact_l1", "weighted_l1", "flat_l2",
+                                  "flat_l1"])
 def test_noalloc_matches_workspace_query_on_two_calls(kind):
     torch = pytest.importorskip("torch")
     ds = synthetic.row_dataset(rows=700, classes=9, queries=16, d=6001, seed=4)
-    if kind.startswith("exact"):
+    if kind == "weighted_l1":
+        # the dense L1 scan with per-coordinate binary32 weights
+        weights = np.random.default_rng(5).uniform(0.25, 4.0, ds.rows.shape[1])
+        index = uha.CudaDenseL1ScanIndex(ds.rows, weights.astype(np.float32))
+    elif kind.startswith("exact"):
         cls = uha.CudaExactL2Index if kind == "exact_l2" else uha.CudaExactL1Index
         index = cls(ds.rows)
     else:
