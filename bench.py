@@ -290,10 +290,45 @@ def run_engine(args):
         line["wide"] = wide()
         torch.cuda.empty_cache()
         line["hierarchies_full"] = hierarchies_full()
+        # last key of the line: the figures the sections above are quoted by
+        line["summary"] = summarize(line)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def summarize(line: dict) -> dict:
+    """One short dict of the sections' headline figures (printed last)."""
+    out = {"queries_per_s": line["value"], "e2e_queries_per_s": line["e2e"]["value"],
+           "roofline_frac": line["roofline"]["frac"]}
+    suite_ = line.get("suite") or {}
+    eq = [e["equal_to_reference"] for e in suite_.get("lines", [])
+          if e.get("equal_to_reference") is not None]
+    parity = {"headline_sample": line.get("agreement_vs_fp64_exact"),
+              "r7028_exact_flat_min": min(eq) if eq else None,
+              "r7028_lines_checked": len(eq),
+              "probabilities_bit_identical": suite_.get("probabilities")}
+    cent = line.get("centroids_flat") or {}
+    parity["r33_flat_t8"] = cent.get("equal_to_reference_cpu_flat")
+    hf = line.get("hierarchies_full") or {}
+    ref = hf.get("reference") or {}
+    parity["hierarchical_16"] = ref.get("equal_to_reference")
+    out["equal_to_reference"] = parity
+    out["flat_batch1_queries_per_s"] = {
+        f"{e['metric']}_T{e['T']}": e["queries_per_s"] for e in suite_.get("lines", [])
+        if e["index"] == "flat" and e["batch"] == 1}
+    prec = [e for e in line.get("precision") or [] if e.get("strategy") != "direct"
+            and e["batch"] == 1024]
+    out["precision_b1024"] = {f"{e['strategy']}_k{e['k']}": {
+        "speedup_vs_direct": e["speedup_vs_direct"],
+        "agreement": e["agreement_vs_fp64_exact"]} for e in prec}
+    if hf:
+        out["hierarchical_16"] = {"device_ms": hf.get("device_ms"),
+                                  "kernels_per_run": hf.get("kernels_per_run"),
+                                  "l2_bf16_device_ms":
+                                      (hf.get("l2_bf16_rerank") or {}).get("device_ms")}
+    return out
 
 
 def cpu_baseline(ds, index, ws, batch):
@@ -329,18 +364,27 @@ def cpu_baseline(ds, index, ws, batch):
                        f"({secs:.1f} s)"}, agree)
 
 
-def suite(ds, exact_index):
-    """Secondary configurations of the same data: batches 64 and 1024, L1, and
-    the flat (importance-sampled) indexes with their agreement against the
-    exact argmin (the engine's exact index, itself bit-exact to the reference's
-    binary64 scan)."""
+def suite(ds, exact_index, nq=1024):
+    """Secondary configurations of the same data (r = 7,028, d = 60,660): exact
+    and flat (importance-sampled, T = 32 and 128) indexes, L1 and L2, at
+    batches 1, 64 and 1,024 over the same `nq` queries. Every line states
+    `equal_to_reference`: the fraction of answers equal to the reference's own
+    CPU index (oracle/_ref: ExactL2Index / ExactL1Index, and the reference's
+    SampledCoordinateL{2,1}AnnIndex given the engine's coordinate sample), and
+    the flat lines their agreement with the binary64 exact argmin. The flat
+    indexes sample from GPU probabilities, which equal the reference CPU's bit
+    for bit (checked here on a 512-row subset, and the sample drawn from them
+    against the reference sampler)."""
     import torch
 
     import ultrahigh_ann_b200 as uha
+    from oracle import oracle as O
 
     out = []
-    nq = 2048
-    qdev = torch.from_numpy(ds.queries[:nq]).cuda()
+    threads = os.cpu_count() or 1
+    queries = np.ascontiguousarray(ds.queries[:nq])
+    qdev = torch.from_numpy(queries).cuda()
+    have_ref = O.ref_available()
 
     def timeit(index, B, n):
         # One uha_query_many call answers the n device-resident queries in
@@ -355,33 +399,69 @@ def suite(ds, exact_index):
         qps = n / (time.perf_counter() - t)
         return res, qps, ws.last_stats()["replayed_queries"]
 
+    def equal(res, ref):
+        return None if ref is None else round(float(np.mean(res == ref)), 4)
+
     exact_ans = {}
+    ref_seconds = 0.0
     for metric, index in (("l2", exact_index), ("l1", uha.CudaExactL1Index(ds.rows))):
-        for B, n in ((1, 512), (64, 2048), (1024, 2048)):
-            res, qps, repl = timeit(index, B, n)
+        ref = None
+        if have_ref:
+            t = time.perf_counter()
+            ref = O.ref_exact(metric, ds.rows, queries, threads)
+            ref_seconds += time.perf_counter() - t
+        for B in (1, 64, 1024):
+            res, qps, repl = timeit(index, B, nq)
             if B == 1024:
                 exact_ans[metric] = res
-            out.append({"index": "exact", "metric": metric, "batch": B,
-                        "queries_per_s": round(qps, 1), "replayed": repl})
-    for metric, prob_fn, cls in (
-            ("l2", uha.compute_l2_importance_probabilities_gpu,
-             uha.CudaSampledCoordinateL2AnnIndex),
-            ("l1", uha.compute_l1_importance_probabilities_gpu,
-             uha.CudaSampledCoordinateL1AnnIndex)):
-        probs = prob_fn(ds.rows)
+            out.append({"index": "exact", "metric": metric, "batch": B, "queries": nq,
+                        "queries_per_s": round(qps, 1), "replayed": repl,
+                        "equal_to_reference": equal(res, ref)})
+    for metric, cls in (("l2", uha.CudaSampledCoordinateL2AnnIndex),
+                        ("l1", uha.CudaSampledCoordinateL1AnnIndex)):
+        probs = _probabilities(metric, ds.rows)
         for T in (32, 128):
-            index = cls(ds.rows, probs.probabilities, T, uha.MT19937_64(0))
-            for B, n in ((1, 2048), (64, 2048), (1024, 2048)):
-                res, qps, repl = timeit(index, B, n)
-                entry = {"index": "flat", "metric": metric, "T": T,
-                         "k": len(index.coordinate_sample), "batch": B,
-                         "queries_per_s": round(qps, 1), "replayed": repl}
-                if B == 1024:
-                    entry["agreement_vs_fp64_exact"] = round(
-                        float(np.mean(res == exact_ans[metric])), 4)
-                out.append(entry)
-            out[-1]["probability_build_ms"] = round(probs.total_ms, 1)
-    return out
+            index = cls(ds.rows, probs, T, uha.MT19937_64(0))
+            cs = index.coordinate_sample
+            ref = None
+            sample_equal = None
+            if have_ref:
+                t = time.perf_counter()
+                cols, mult, invp, _ = O.ref_sample(probs, T, 0)
+                sample_equal = bool(np.array_equal(cols, cs.source_columns) and
+                                    np.array_equal(mult, cs.multiplicities) and
+                                    invp.tobytes() == cs.inverse_probabilities.tobytes())
+                ref = O.ref_sampled(metric, ds.rows, cols, mult, invp, queries, threads)
+                ref_seconds += time.perf_counter() - t
+            for B in (1, 64, 1024):
+                res, qps, repl = timeit(index, B, nq)
+                out.append({"index": "flat", "metric": metric, "T": T, "k": len(cs),
+                            "batch": B, "queries": nq, "queries_per_s": round(qps, 1),
+                            "replayed": repl, "equal_to_reference": equal(res, ref),
+                            "sample_equal_to_reference_sampler": sample_equal,
+                            "agreement_vs_fp64_exact": round(
+                                float(np.mean(res == exact_ans[metric])), 4)})
+    return {"lines": out, "probabilities": probability_parity(ds),
+            "reference_cpu_seconds": round(ref_seconds, 1)}
+
+
+def probability_parity(ds, rows=512):
+    """GPU importance probabilities (direct pair backend) against the
+    reference CPU's (oracle/_ref, cpu_parallel policy) on the first `rows`
+    rows at full dimension: bit-identical or not."""
+    import ultrahigh_ann_b200 as uha
+    from oracle import oracle as O
+
+    if not O.ref_available():
+        return None
+    sub = np.ascontiguousarray(ds.rows[:rows])
+    res = {"rows": rows, "dimension": sub.shape[1]}
+    for metric, fn in (("l2", uha.compute_l2_importance_probabilities_gpu),
+                       ("l1", uha.compute_l1_importance_probabilities_gpu)):
+        got = fn(sub).probabilities
+        want = O.ref_probabilities(metric, sub)
+        res[f"{metric}_bit_identical"] = got.tobytes() == want.tobytes()
+    return res
 
 
 def precision(ds, exact_index, batches=((1, 256), (64, 2048), (1024, 2048))):
@@ -671,7 +751,8 @@ def _projected_check(ix, metric, sampled64, queries64, got):
     return ok
 
 
-def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=16):
+def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=16,
+                     ref_queries=64):
     """16 hierarchical indexes at the full size of the hierarchical batched
     configuration: rows 1,024 / 7,028 / 65,536 (row subsets of one
     65,536 x 262,144 BF16 matrix generated on the device), T = 32,
@@ -697,7 +778,7 @@ def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=1
     probs = {"l2": uha.compute_l2_importance_probabilities_gpu(head).probabilities,
              "l1": uha.compute_l1_importance_probabilities_gpu(head).probabilities}
     prob_s = time.perf_counter() - t
-    specs, indexes = [], []
+    specs, indexes, seeds = [], [], []
     t = time.perf_counter()
     i = 0
     for r in sorted({min(1024, rows), min(7028, rows), rows}):
@@ -709,18 +790,33 @@ def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=1
                        else uha.CudaHierarchicalL1AnnIndex)
                 ix = cls(uha.DeviceMatrix.from_torch(data.rows[:r]), 32, p,
                          uha.MT19937_64(300 + i), importance_probabilities=probs[metric])
+                seeds.append(300 + i)
                 indexes.append(ix)
                 specs.append({"metric": metric, "rows": r, "T": 32, "p": p,
                               "k": len(ix.coordinate_sample)})
                 i += 1
     torch.cuda.synchronize()
     build_s = time.perf_counter() - t
-    # host copies of the sampled columns for the binary64 check, then the
-    # matrix is released
+    # host copies of the sampled columns (binary32 holds the BF16 values
+    # exactly) for the reference check, then the matrix is released
     sampled = []
     for ix, spec in zip(indexes, specs):
         cols = torch.from_numpy(ix.coordinate_sample.source_columns.astype(np.int64)).cuda()
-        sampled.append(data.rows[:spec["rows"]].index_select(1, cols).double().cpu().numpy())
+        sampled.append(data.rows[:spec["rows"]].index_select(1, cols).float().cpu().numpy())
+    # the picked queries (reference and binary64 checks) and their binary64
+    # exact L2 distances to every row over the full dimension; a Gaussian-JL
+    # twin of every L2 hierarchy (same seed, so the same sample) from the same
+    # device matrix
+    picks = np.random.default_rng(9).choice(per_index, max(checked, ref_queries),
+                                            replace=False)
+    exact_d2 = exact_l2_distances(data.rows, data.queries, picks[:ref_queries])
+    gaussian = []
+    for k, spec in enumerate(specs):
+        if spec["metric"] == "l2":
+            gaussian.append((k, uha.CudaHierarchicalL2AnnIndex(
+                uha.DeviceMatrix.from_torch(data.rows[:spec["rows"]]), 32, spec["p"],
+                uha.MT19937_64(seeds[k]), importance_probabilities=probs["l2"],
+                projection="gaussian")))
     data.rows = None
     torch.cuda.empty_cache()
     qdev = data.queries
@@ -774,13 +870,18 @@ def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=1
                           "distance_excess_mean": float(excess.mean()),
                           "distance_excess_max": float(excess.max())})
     del mixed
-    picks = np.random.default_rng(9).choice(per_index, checked, replace=False)
-    q_host = qdev.index_select(0, torch.from_numpy(picks).cuda()).double().cpu().numpy()
+    q_host = qdev.index_select(0, torch.from_numpy(picks).cuda()).float().cpu().numpy()
     ok = 0
     for k, (ix, spec) in enumerate(zip(indexes, specs)):
         cols = ix.coordinate_sample.source_columns.astype(np.int64)
-        ok += _projected_check(ix, spec["metric"], sampled[k], q_host[:, cols],
-                               res[k][0][picks])
+        ok += _projected_check(ix, spec["metric"], sampled[k].astype(np.float64),
+                               q_host[:checked, cols].astype(np.float64),
+                               res[k][0][picks[:checked]])
+    reference = hierarchy_reference_parity(indexes, specs, seeds, probs, sampled,
+                                           q_host[:ref_queries], picks[:ref_queries],
+                                           [r[0] for r in res])
+    projections = gaussian_vs_rademacher(gaussian, specs, res, qdev, per_index,
+                                         picks[:ref_queries], exact_d2)
     total = per_index * len(indexes)
     best = min(ms)
     return {"workload": f"hierarchical_16_indexes_r{rows}_d{dim}_bf16",
@@ -790,6 +891,8 @@ def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=1
             "graph_nodes": st["graph_nodes"], "kernels_per_run": st["kernel_launches"],
             "replayed": st["replayed_queries"], "answers_equal_index_by_index": same,
             "binary64_checked": {"queries": checked * len(indexes), "distance_optimal": ok},
+            "reference": reference,
+            "l2_projection_modes": projections,
             "l2_bf16_rerank": {"queries_per_s": round(total / (min(mixed_ms) * 1e-3), 1),
                                "device_ms": round(min(mixed_ms), 3),
                                "strategy": "L2 hierarchies gemm_bf16_rerank (k = 32), "
@@ -798,6 +901,101 @@ def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=1
             "setup_s": {"generate_on_device": round(gen_s, 1),
                         "probabilities": round(prob_s, 1), "build": round(build_s, 1),
                         "autotune_and_capture": round(setup_s, 1)}}
+
+
+def exact_l2_distances(rows_dev, queries_dev, picks, chunk=4096):
+    """Binary64 squared L2 distances of the picked queries to every row over
+    the full dimension (host array, queries x rows), in row chunks on the
+    device: ||x||^2 - 2 x.q + ||q||^2 with binary64 products (relative error
+    near 1e-14 here, far below the gaps the agreement figures resolve)."""
+    import torch
+
+    q = queries_dev.index_select(0, torch.from_numpy(picks).to(queries_dev.device))
+    q = q.double()
+    qn = (q * q).sum(1)
+    out = []
+    for s in range(0, rows_dev.shape[0], chunk):
+        x = rows_dev[s:s + chunk].double()
+        d = (x * x).sum(1)[None, :] - 2.0 * (q @ x.T) + qn[:, None]
+        out.append(d.clamp_min(0.0).cpu().numpy())
+        del x, d
+    torch.cuda.empty_cache()
+    return np.concatenate(out, axis=1)
+
+
+def gaussian_vs_rademacher(gaussian, specs, res, qdev, per_index, picks, exact_d2):
+    """Agreement with the binary64 exact L2 argmin over the full dimension and
+    the relative distance excess of the returned row, for each L2 hierarchy
+    with the reference's Rademacher projection and with the seeded Gaussian
+    one (same sample), on the picked queries; plus the Gaussian twins' device
+    time in one captured batch."""
+    import ultrahigh_ann_b200 as uha
+
+    if not gaussian:
+        return None
+    batch = uha.QueryBatch([(ix, per_index, uha.QueryStrategy.direct)
+                            for _, ix in gaussian], autotune=True)
+    batch.run([qdev.data_ptr()] * len(gaussian), on_device=True)
+    ms = []
+    for _ in range(3):
+        gres = batch.run(None)
+        ms.append(batch.stats()["device_ms"])
+    rows_out = []
+    for (k, _), (got_rows, _) in zip(gaussian, gres):
+        r = specs[k]["rows"]
+        d2 = exact_d2[:, :r]
+        best = d2.min(axis=1)
+        exact_rows = d2.argmin(axis=1)
+
+        def stats(answer):
+            a = answer[picks].astype(np.int64)
+            excess = d2[np.arange(len(picks)), a] / np.maximum(best, 1e-300) - 1.0
+            return {"agreement_vs_fp64_exact": round(float(np.mean(a == exact_rows)), 4),
+                    "distance_excess_mean": float(excess.mean()),
+                    "distance_excess_max": float(excess.max())}
+        rows_out.append({"rows": r, "p": specs[k]["p"], "k": specs[k]["k"],
+                         "rademacher": stats(res[k][0]), "gaussian": stats(got_rows)})
+    return {"queries_per_index": len(picks), "indexes": rows_out,
+            "gaussian_batch_device_ms": round(min(ms), 3),
+            "exact": "binary64 squared L2 over all 262,144 coordinates"}
+
+
+def hierarchy_reference_parity(indexes, specs, seeds, probs, sampled, q_host, picks,
+                               answers):
+    """Each hierarchy's answers on the picked queries against the reference's
+    own HierarchicalL{2,1}AnnIndex (oracle/_ref) built over the same sampled
+    columns, with the sample renumbered (the same index: it reads only those
+    columns). The reference sampler is run on the same probabilities and seed;
+    its sample must equal the engine's and its engine state after sampling
+    seeds the reference's projection draws."""
+    from oracle import oracle as O
+
+    if not O.ref_available():
+        return None
+    threads = os.cpu_count() or 1
+    t = time.perf_counter()
+    equal, samples_equal, total = 0, 0, 0
+    per_index = []
+    for ix, spec, seed, rows_k, want in zip(indexes, specs, seeds, sampled, answers):
+        cols, mult, invp, state = O.ref_sample(probs[spec["metric"]], spec["T"], seed)
+        cs = ix.coordinate_sample
+        same_sample = bool(np.array_equal(cols, cs.source_columns) and
+                           np.array_equal(mult, cs.multiplicities) and
+                           invp.tobytes() == cs.inverse_probabilities.tobytes())
+        got = O.ref_hierarchical_sampled(spec["metric"], rows_k, mult, invp, spec["p"],
+                                         state, q_host[:, cols.astype(np.int64)], threads)
+        e = int(np.sum(got == want[picks]))
+        equal += e
+        total += len(picks)
+        samples_equal += int(same_sample)
+        per_index.append(e)
+    return {"queries_per_index": len(picks), "queries": total,
+            "equal_to_reference": round(equal / max(1, total), 4),
+            "equal_per_index": per_index,
+            "samples_equal_to_reference_sampler": samples_equal,
+            "reference": "HierarchicalL{2,1}AnnIndex::query on the sampled columns, "
+                         f"{threads} threads",
+            "seconds": round(time.perf_counter() - t, 1)}
 
 
 def serving(ds, rates=(10_000, 100_000, 1_000_000, 2_000_000), seconds=0.5, pool=2048):

@@ -598,6 +598,21 @@ uha_status uha_cauchy_matrix(const uint64_t* multiplicities,
                              uint64_t projection_dimension, uha_rng* rng,
                              double* out);
 
+/* Row-major p x k Gaussian JL matrix, a seeded binary32 matrix for L2
+ * hierarchies (passed to uha_hierarchical_index_create like the Rademacher
+ * one): entry (row, i) = float(Z * sqrt(m_i * (1/p_i) / p)) with Z a standard
+ * normal draw (std::normal_distribution<double> on the engine, row-major
+ * order). The variance per entry, m_i (1/p_i) / p, is that of the
+ * aggregated Rademacher entry it replaces (a sum of m_i independent
+ * N(0, 1) is N(0, m_i)), so both estimate the same squared distance.
+ * No counterpart in the reference, whose L2 hierarchy is Rademacher-only
+ * (src/hnsvw25/l2/hierarchical/l2_hierarchical_projection.cpp:53-77). */
+uha_status uha_gaussian_jl_matrix(const uint64_t* multiplicities,
+                                  const double* inverse_probabilities,
+                                  uint64_t sample_size,
+                                  uint64_t projection_dimension, uha_rng* rng,
+                                  double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -401,6 +401,33 @@ def ref_projection(metric: str, rows, cols, mult, invp, p: int, state: str | Non
     return mat, reps
 
 
+def ref_hierarchical_sampled(metric: str, sampled_rows, mult, invp, p: int, state: str,
+                             sampled_queries, threads: int = 1) -> np.ndarray:
+    """The reference's hierarchical index (its own constructor and query())
+    over the r x k sampled columns with the sample renumbered 0..k-1; equal to
+    the index over the full matrix (ref_hier_capi.cpp)."""
+    lib = ref_lib()
+    if not getattr(lib, "_hier_typed", False):
+        lib.ref_hier_last_error.restype = c_char_p
+        lib.ref_hierarchical_sampled.restype = c_int
+        lib.ref_hierarchical_sampled.argtypes = [c_int, c_void_p, c_uint64, c_uint64,
+                                                 c_void_p, c_void_p, c_uint64, c_char_p,
+                                                 c_void_p, c_uint64, c_int, c_void_p]
+        lib._hier_typed = True
+    rows = _f32(sampled_rows)
+    q = _f32(sampled_queries).reshape(-1, rows.shape[1])
+    mult = np.ascontiguousarray(mult, np.uint64)
+    invp = np.ascontiguousarray(invp, np.float64)
+    out = np.zeros(q.shape[0], np.uint64)
+    code = lib.ref_hierarchical_sampled(0 if metric == "l2" else 1, _p(rows),
+                                        rows.shape[0], rows.shape[1], _p(mult), _p(invp),
+                                        p, state.encode(), _p(q), q.shape[0], threads,
+                                        _p(out))
+    if code != 0:
+        raise ReferenceError_(code, lib.ref_hier_last_error().decode())
+    return out
+
+
 # ------------------------------------------------- reference data-file code
 
 def ref_sha256_file(path) -> bytes:

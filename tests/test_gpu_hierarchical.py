@@ -188,3 +188,29 @@ def test_hierarchical_near_ties_match_reference(oracle_module, metric):
             got, dist = run(index, queries, batch)
             assert np.array_equal(got, expected), (p, batch)
             assert np.allclose(dist, edist, rtol=DIST_RTOL, atol=1e-30)
+
+
+@pytest.mark.parametrize("p", [1, 16, 64, 256])
+def test_gaussian_jl_hierarchy_matches_oracle(oracle_module, p):
+    """The seeded Gaussian JL mode (not in the reference) runs the same
+    certified path as the Rademacher one: its answers are the binary64
+    projected argmin of the oracle given the same matrix, on every query and
+    with every strategy, lowest row on ties."""
+    ds = synthetic.row_dataset(rows=300, classes=6, queries=70, d=2500, seed=p + 40)
+    probs = oracle_module.probabilities("l2", ds.rows)
+    index = uha.CudaHierarchicalL2AnnIndex(ds.rows, 16, p, uha.MT19937_64(p),
+                                           importance_probabilities=probs,
+                                           projection="gaussian")
+    assert index.projection_kind == "gaussian"
+    cs = index.coordinate_sample
+    expected, edist = oracle_module.hierarchical("l2", ds.rows, cs.source_columns,
+                                                 index.projection, ds.queries)
+    for batch in (1, 8, 70):
+        got, dist = run(index, ds.queries, batch)
+        assert np.array_equal(got, expected), f"batch {batch}"
+        assert np.allclose(dist, edist, rtol=DIST_RTOL, atol=1e-30)
+    ws = index.make_query_workspace(70)
+    ws.set_candidates(64)
+    got = index.query_batch(ds.queries, 70, None, ws, uha.QueryStrategy.gemm_bf16_rerank)
+    # with 64 candidates per query every near row is re-scored in binary64
+    assert np.mean(got == expected) >= 0.98

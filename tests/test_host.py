@@ -150,3 +150,22 @@ def test_host_probabilities_edge_cases():
     with pytest.raises(uha.InvalidArgument):
         uha.compute_importance_probabilities_host(
             "l2", np.array([[np.nan, 0.0], [1.0, 1.0]], np.float32))
+
+
+def test_gaussian_jl_matrix_is_seeded_binary32_with_rademacher_variance():
+    s = uha.CoordinateSample([0, 5, 9], [1, 4, 9], [2.0, 0.5, 1.25])
+    p = 4096
+    a = uha.build_gaussian_jl_matrix(s, p, uha.MT19937_64(3))
+    b = uha.build_gaussian_jl_matrix(s, p, uha.MT19937_64(3))
+    assert a.shape == (p, 3) and np.array_equal(a, b)
+    assert np.array_equal(a, a.astype(np.float32).astype(np.float64))
+    assert not np.array_equal(a, uha.build_gaussian_jl_matrix(s, p, uha.MT19937_64(4)))
+    # the aggregated Rademacher entry's variance m (1/p_j) / p
+    want = np.array([1 * 2.0, 4 * 0.5, 9 * 1.25]) / p
+    assert np.allclose(a.var(axis=0), want, rtol=0.1)
+    assert np.allclose(a.mean(axis=0), 0.0, atol=4 * np.sqrt(want / p))
+    with pytest.raises(uha.InvalidArgument):
+        uha.build_gaussian_jl_matrix(s, 0, uha.MT19937_64(1))
+    with pytest.raises(uha.InvalidArgument):
+        uha.CudaHierarchicalL1AnnIndex(np.ones((2, 3), np.float32), 4, 2,
+                                       uha.MT19937_64(1), projection="gaussian")

@@ -106,3 +106,24 @@ def test_l1_grouped_summation_differs_from_sequential(oracle_module):
     sequential = ((big + 100.0) + 100.0) + 100.0
     assert grouped != sequential
     assert dist[0] == grouped
+
+
+@pytest.mark.parametrize("metric", ["l2", "l1"])
+def test_reference_hierarchy_on_sampled_columns_equals_full_matrix(oracle_module, metric):
+    """The full-size parity check runs the reference's hierarchical index over
+    the sampled columns only (the full 65,536 x 262,144 matrix does not fit host
+    memory). That index must answer exactly as the reference index over the
+    full matrix, whatever the thread count of its row-block projection."""
+    O = oracle_module
+    if not O.ref_available():
+        pytest.skip("reference library oracle/_ref is not built")
+    ds = synthetic.row_dataset(rows=230, classes=6, queries=40, d=3001, seed=15)
+    probs = O.ref_probabilities(metric, ds.rows)
+    for reps, p, seed in ((8, 15, 3), (32, 16, 4), (16, 64, 5)):
+        full, _ = O.ref_hierarchical(metric, ds.rows, probs, reps, p, seed, ds.queries)
+        cols, mult, invp, state = O.ref_sample(probs, reps, seed)
+        cols = cols.astype(np.int64)
+        for threads in (1, 3, 8):
+            got = O.ref_hierarchical_sampled(metric, ds.rows[:, cols], mult, invp, p,
+                                             state, ds.queries[:, cols], threads)
+            assert np.array_equal(got, full), (reps, p, threads)

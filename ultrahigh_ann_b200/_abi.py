@@ -200,6 +200,8 @@ SIGNATURES = {
                                         c_void_p, c_void_p, c_void_p, _U]),
     "uha_jl_matrix": (c_int, [c_void_p, c_void_p, c_uint64, c_uint64, c_void_p, c_void_p]),
     "uha_cauchy_matrix": (c_int, [c_void_p, c_void_p, c_uint64, c_uint64, c_void_p, c_void_p]),
+    "uha_gaussian_jl_matrix": (c_int, [c_void_p, c_void_p, c_uint64, c_uint64, c_void_p,
+                                       c_void_p]),
 }
 
 _lib: ctypes.CDLL | None = None

@@ -253,6 +253,18 @@ def build_jl_matrix(sample: CoordinateSample, projection_dimension: int,
     return out
 
 
+def build_gaussian_jl_matrix(sample: CoordinateSample, projection_dimension: int,
+                             random_engine: MT19937_64) -> np.ndarray:
+    """p x k Gaussian JL matrix with binary32 entries Z * sqrt(m (1/p) / p),
+    the variance of the aggregated Rademacher entry (uha_gaussian_jl_matrix);
+    an extra projection mode, not in the reference."""
+    out = np.empty((projection_dimension, len(sample)), dtype=np.float64)
+    _check(_abi.load().uha_gaussian_jl_matrix(
+        _ptr(sample.multiplicities), _ptr(sample.inverse_probabilities),
+        len(sample), projection_dimension, random_engine.handle, _ptr(out)))
+    return out
+
+
 def build_cauchy_matrix(sample: CoordinateSample, projection_dimension: int,
                         random_engine: MT19937_64) -> np.ndarray:
     """p x k Cauchy matrix in the reference's draw order
@@ -804,8 +816,11 @@ class _CudaHierarchicalIndex(_CudaIndex):
     def __init__(self, input, repetitions=None, projection_dimension=None,
                  random_engine=None, device: int = 0,
                  probability_execution_policy: Optional[ExecutionPolicy] = None, *,
-                 importance_probabilities=None, coordinate_sample=None):
+                 importance_probabilities=None, coordinate_sample=None,
+                 projection: str = "default"):
         rows = _rows_input(input)
+        if projection not in self._projections:
+            raise InvalidArgument(f"unknown projection {projection!r}")
         if rows.shape[0] == 0:
             raise InvalidArgument(
                 "hierarchical index expects at least one representative")
@@ -827,8 +842,7 @@ class _CudaHierarchicalIndex(_CudaIndex):
         if len(sample) == 0 and rows.shape[0] > 1:
             raise CudaRuntimeError("importance sampling selected no coordinates")
         p = int(projection_dimension)
-        draw = build_jl_matrix if self._metric == _abi.L2 else build_cauchy_matrix
-        matrix = draw(sample, p, random_engine)
+        matrix = self._projections[projection](sample, p, random_engine)
         handle = ctypes.c_void_p()
         sample_args = (_ptr(sample.source_columns), _ptr(sample.multiplicities),
                        _ptr(sample.inverse_probabilities), len(sample), _ptr(matrix), p,
@@ -843,15 +857,22 @@ class _CudaHierarchicalIndex(_CudaIndex):
         self._adopt(handle, rows.shape[1], rows.shape[0])
         self.coordinate_sample = sample
         self.projection = matrix
+        self.projection_kind = projection
 
 
 class CudaHierarchicalL2AnnIndex(_CudaHierarchicalIndex):
     """include/ultrahigh_ann/hnsvw25/l2/hierarchical/cuda_hierarchical_l2_ann_index.hpp:33-104:
     sampled coordinates, Rademacher-JL projection to p coordinates, squared-L2
-    scan of the projected rows. Default probability policy gpu_fp32."""
+    scan of the projected rows. Default probability policy gpu_fp32.
+
+    projection="gaussian" (keyword only; not in the reference) draws a seeded
+    Gaussian JL matrix with binary32 entries from the same engine instead of
+    the Rademacher one; everything after the matrix is the same path."""
 
     _metric = _abi.L2
     _default_policy = ExecutionPolicy.gpu_fp32
+    _projections = {"default": build_jl_matrix, "rademacher": build_jl_matrix,
+                    "gaussian": build_gaussian_jl_matrix}
 
 
 class CudaHierarchicalL1AnnIndex(_CudaHierarchicalIndex):
@@ -861,6 +882,7 @@ class CudaHierarchicalL1AnnIndex(_CudaHierarchicalIndex):
 
     _metric = _abi.L1
     _default_policy = ExecutionPolicy.sequential
+    _projections = {"default": build_cauchy_matrix, "cauchy": build_cauchy_matrix}
 
     def query_batch(self, queries, query_count, output, workspace,
                     strategy=QueryStrategy.direct, distances=None):

@@ -235,6 +235,51 @@ extern "C" uha_status uha_cauchy_matrix(const uint64_t* multiplicities,
     });
 }
 
+// Gaussian JL entries with the variance of the aggregated Rademacher entries,
+// rounded to binary32 (the matrix is a binary32 matrix held in binary64, so the
+// binary64 projection path is exact with respect to it).
+extern "C" uha_status uha_gaussian_jl_matrix(const uint64_t* multiplicities,
+                                             const double* inverse_probabilities,
+                                             uint64_t sample_size,
+                                             uint64_t projection_dimension,
+                                             uha_rng* rng, double* out)
+{
+    return guarded([&] {
+        if (rng == nullptr ||
+            (sample_size != 0 && projection_dimension != 0 &&
+             (multiplicities == nullptr || inverse_probabilities == nullptr ||
+              out == nullptr))) {
+            fail(UHA_INVALID_ARGUMENT, "projection arguments must not be null");
+        }
+        if (projection_dimension == 0) {
+            fail(UHA_INVALID_ARGUMENT,
+                 "projection_dimension has to be a positive integer");
+        }
+        uha::checked_mul(projection_dimension, sample_size, "Gaussian JL matrix");
+        validate_sample_weights(multiplicities, inverse_probabilities,
+                                sample_size);
+        std::vector<double> scale(sample_size);
+        for (uint64_t i = 0; i < sample_size; ++i) {
+            scale[i] = std::sqrt(static_cast<double>(multiplicities[i]) *
+                                 inverse_probabilities[i] /
+                                 static_cast<double>(projection_dimension));
+        }
+        std::normal_distribution<double> normal(0.0, 1.0);
+        uint64_t index = 0;
+        for (uint64_t row = 0; row < projection_dimension; ++row) {
+            for (uint64_t i = 0; i < sample_size; ++i) {
+                const float coefficient =
+                    static_cast<float>(normal(rng->engine) * scale[i]);
+                if (!std::isfinite(coefficient)) {
+                    fail(UHA_OVERFLOW_ERROR,
+                         "Gaussian JL projection coefficient is not finite");
+                }
+                out[index++] = coefficient;
+            }
+        }
+    });
+}
+
 // Importance probabilities on the host cores with the reference CPU policies'
 // arithmetic (src/hnsvw25/l2/importance_sampling.cpp:19-45,
 // src/hnsvw25/l1/importance_sampling.cpp:19-47): binary64 pair distances (L2

@@ -5,8 +5,12 @@
 // with nonzero distance, L2 contributes min(1, (a_j - b_j)^2 / ||a - b||^2) and
 // L1 contributes |a_j - b_j| / ||a - b||_1 to column j; p_j is the maximum
 // contribution. Pair distances and the per-column maxima use binary64 (the
-// normalisation of the probabilities), so the result agrees with the CPU's
-// binary64 loop to a few ulps.
+// normalisation of the probabilities). The direct backend performs the CPU's
+// own operations in the CPU's order (sequential squared differences for L2,
+// libstdc++'s transform_reduce grouping for L1, one IEEE division per pair,
+// the same two roundings per contribution) and the maximum is exact, so its
+// probabilities equal the reference CPU's bit for bit. The Gram backend
+// agrees to a few ulps.
 //
 // Stage 1 (pair kernel): a 32 x 32 block of pairs per CTA, columns staged
 // through shared memory in 64-column slabs; each thread accumulates four
@@ -64,16 +68,46 @@ __global__ void __launch_bounds__(256)
             sb[r][c] = vb;
         }
         __syncthreads();
+        if (metric == 0) {
+            // squared_l2_dist: sequential binary64 sum of separately rounded
+            // squares, column order (src/core/l2_distance.cpp:17-23)
 #pragma unroll 4
-        for (int c = 0; c < kPairSlab; ++c) {
-            const double va = sa[ty][c];
+            for (int c = 0; c < kPairSlab; ++c) {
+                const double va = sa[ty][c];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const double d = va - static_cast<double>(sb[tx + 8 * j][c]);
-                if (metric == 0) {
-                    acc[j] = fma(d, d, acc[j]);
+                for (int j = 0; j < 4; ++j) {
+                    const double d =
+                        __dsub_rn(va, static_cast<double>(sb[tx + 8 * j][c]));
+                    acc[j] = __dadd_rn(acc[j], __dmul_rn(d, d));
+                }
+            }
+        } else {
+            // l1_dist: std::transform_reduce as libstdc++ 13 evaluates it
+            // (src/core/l1_distance.cpp:17-26): init + ((t0 + t1) + (t2 + t3))
+            // per group of four from column 0, then the last dim % 4 columns
+            // one by one. Slabs are 64 columns, so groups never straddle one.
+            const uint64_t grouped_end = dim & ~uint64_t(3);
+            for (int c = 0; c < kPairSlab; c += 4) {
+                if (c0 + c + 4 <= grouped_end) {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const float* vb = &sb[tx + 8 * j][c];
+                        const double t0 = fabs(__dsub_rn(sa[ty][c], vb[0]));
+                        const double t1 = fabs(__dsub_rn(sa[ty][c + 1], vb[1]));
+                        const double t2 = fabs(__dsub_rn(sa[ty][c + 2], vb[2]));
+                        const double t3 = fabs(__dsub_rn(sa[ty][c + 3], vb[3]));
+                        acc[j] = __dadd_rn(acc[j], __dadd_rn(__dadd_rn(t0, t1),
+                                                             __dadd_rn(t2, t3)));
+                    }
                 } else {
-                    acc[j] += fabs(d);
+                    for (int e = 0; e < 4 && c0 + c + e < dim; ++e) {
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            acc[j] = __dadd_rn(
+                                acc[j], fabs(__dsub_rn(sa[ty][c + e],
+                                                       sb[tx + 8 * j][c + e])));
+                        }
+                    }
                 }
             }
         }
@@ -240,9 +274,13 @@ __global__ void __launch_bounds__(kColumns)
             const double va = sa[ra * kColumns + threadIdx.x];
 #pragma unroll 8
             for (int rb = 0; rb < kPairBlock; ++rb) {
-                const double d = va - static_cast<double>(sb[rb * kColumns + threadIdx.x]);
+                const double d =
+                    __dsub_rn(va, static_cast<double>(sb[rb * kColumns + threadIdx.x]));
                 const double w = sinv[ra * kPairBlock + rb];
-                const double c = metric == 0 ? (d * d) * w : fabs(d) * w;
+                // (d * d) * inverse or |d| * inverse, each product rounded as
+                // the CPU rounds it (importance_sampling.cpp:36-41 of l2, :26-30 of l1)
+                const double c = metric == 0 ? __dmul_rn(__dmul_rn(d, d), w)
+                                             : __dmul_rn(fabs(d), w);
                 m = fmax(m, c);
             }
         }
