@@ -16,6 +16,7 @@
 #include "common.h"
 #include "kernels.h"
 
+#include <algorithm>
 #include <cfloat>
 #include <map>
 #include <mutex>
@@ -931,6 +932,258 @@ __global__ void __launch_bounds__(kFinalizeThreads)
     }
 }
 
+// ------------------------------------- flat indexes at small batches, one launch
+
+// Programmatic dependent launch: a grid launched with programmatic stream
+// serialization may start while the previous kernel of the stream runs;
+// griddepcontrol.wait returns once that kernel has completed and its memory
+// is visible (immediately when the launch had no programmatic edge), and
+// griddepcontrol.launch_dependents lets the next such grid start.
+__device__ __forceinline__ void wait_for_previous_grid()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+__device__ __forceinline__ void allow_next_grid()
+{
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Per-row accumulation of one lane: binary32, column order, four terms per
+// float4 group (the same arithmetic as small_query_kernel).
+__device__ __forceinline__ float flat_terms(int op, float acc, const float4 a,
+                                            const float4 b, const float4* w4, uint64_t g)
+{
+    if (op == static_cast<int>(ScanOp::l2)) {
+        float d = a.x - b.x; acc = fmaf(d, d, acc);
+        d = a.y - b.y; acc = fmaf(d, d, acc);
+        d = a.z - b.z; acc = fmaf(d, d, acc);
+        d = a.w - b.w; acc = fmaf(d, d, acc);
+    } else if (op == static_cast<int>(ScanOp::l1)) {
+        acc += fabsf(a.x - b.x);
+        acc += fabsf(a.y - b.y);
+        acc += fabsf(a.z - b.z);
+        acc += fabsf(a.w - b.w);
+    } else {
+        const float4 w = __ldg(w4 + g);
+        acc = fmaf(fabsf(a.x - b.x), w.x, acc);
+        acc = fmaf(fabsf(a.y - b.y), w.y, acc);
+        acc = fmaf(fabsf(a.z - b.z), w.z, acc);
+        acc = fmaf(fabsf(a.w - b.w), w.w, acc);
+    }
+    return acc;
+}
+
+// grid = (row blocks, batch), kFinalizeThreads threads. Every CTA gathers its
+// query's sampled (or all) coordinates into shared memory with the
+// preparation kernels' finiteness flags, then computes the binary32 distance
+// of each of its rows with kLanes lanes per row (each lane sums its float4
+// groups g = lane, lane + kLanes, ... in column order; a butterfly within the
+// lane group adds the kLanes partial sums), stores it in the query's distance
+// slab and keeps its two smallest. The last CTA of the query to finish merges
+// the CTA summaries and certifies the argmin, replaying the candidates in
+// binary64 when the bounds overlap, exactly as argmin_kernel does. Every CTA
+// passes wait_for_previous_grid() before it writes anything, so a grid that
+// starts early (programmatic serialization) only overlaps its launch and its
+// gather with the previous kernel.
+template <int kLanes>
+__global__ void __launch_bounds__(kFinalizeThreads)
+    flat_query_kernel(SmallQuery sq, Bound bound, ReplayInputs in, float* distances,
+                      Summary* block_summaries, uint32_t* done, uint32_t summary_stride,
+                      uint32_t span, Result* results, double* exact_distances,
+                      uint32_t* replay_count, int* error_flag)
+{
+    extern __shared__ float flat_smem[];
+    float* qv = flat_smem;  // padded_dim
+    __shared__ int bad;
+    const uint32_t q = blockIdx.y;
+    const uint32_t blocks = gridDim.x;
+    if (threadIdx.x == 0) {
+        bad = 0;
+    }
+    __syncthreads();
+    const float* src = sq.queries + static_cast<uint64_t>(q) * sq.dim;
+    int local_bad = 0;
+    for (uint64_t i = threadIdx.x; i < sq.padded_dim; i += kFinalizeThreads) {
+        float v = 0.f;
+        if (sq.columns == nullptr) {
+            if (i < sq.dim) {
+                v = src[i];
+                local_bad |= isfinite(v) ? 0 : 1;
+            }
+        } else if (i < sq.sample_size) {
+            v = src[sq.columns[i]];
+            local_bad |= isfinite(v) ? 0 : 1;
+            if (sq.scales != nullptr) {
+                v = __fmul_rn(v, sq.scales[i]);
+                local_bad |= isfinite(v) ? 0 : 2;
+            }
+        }
+        qv[i] = v;
+    }
+    if (local_bad != 0) {
+        bad = 1;
+    }
+    __syncthreads();
+    wait_for_previous_grid();
+    allow_next_grid();
+    if (bad) {
+        // the call fails on the flag; nothing to certify
+        if (local_bad != 0) {
+            atomicOr(error_flag, local_bad);
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            results[q] = Result{0, 0.f};
+            exact_distances[q] = __longlong_as_double(0x7ff8000000000000ll);
+        }
+        return;
+    }
+
+    constexpr int kRowsPerStep = kFinalizeThreads / kLanes;
+    const int lane = threadIdx.x % 32;
+    const int sub = threadIdx.x % kLanes;
+    const int group = threadIdx.x / kLanes;
+    const uint64_t groups = sq.padded_dim / 4;
+    const float4* q4 = reinterpret_cast<const float4*>(qv);
+    const float4* w4 = reinterpret_cast<const float4*>(sq.weights32);
+    const uint32_t first_row = blockIdx.x * span;
+    const uint32_t end_row = min(sq.row_count, first_row + span);
+    float* dist = distances + static_cast<uint64_t>(q) * sq.row_count;
+    RowScan scan;
+    for (uint32_t base = first_row; base < end_row; base += kRowsPerStep) {
+        const uint32_t row = base + group;
+        const bool valid = row < end_row;
+        const float4* r4 = reinterpret_cast<const float4*>(
+            sq.rows + static_cast<uint64_t>(valid ? row : first_row) * sq.padded_dim);
+        float acc = 0.f;
+        uint64_t g = sub;
+        for (; g + 3 * kLanes < groups; g += 4 * kLanes) {
+            const float4 b0 = __ldg(r4 + g);
+            const float4 b1 = __ldg(r4 + g + kLanes);
+            const float4 b2 = __ldg(r4 + g + 2 * kLanes);
+            const float4 b3 = __ldg(r4 + g + 3 * kLanes);
+            acc = flat_terms(sq.op, acc, q4[g], b0, w4, g);
+            acc = flat_terms(sq.op, acc, q4[g + kLanes], b1, w4, g + kLanes);
+            acc = flat_terms(sq.op, acc, q4[g + 2 * kLanes], b2, w4, g + 2 * kLanes);
+            acc = flat_terms(sq.op, acc, q4[g + 3 * kLanes], b3, w4, g + 3 * kLanes);
+        }
+        for (; g < groups; g += kLanes) {
+            acc = flat_terms(sq.op, acc, q4[g], __ldg(r4 + g), w4, g);
+        }
+#pragma unroll
+        for (int o = kLanes / 2; o > 0; o /= 2) {
+            acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        }
+        if (valid && sub == 0) {
+            dist[row] = acc;
+            if (!(acc <= FLT_MAX)) {
+                scan.overflow = true;
+            } else if (acc < scan.k1) {
+                scan.k2 = scan.k1;
+                scan.k1 = acc;
+                scan.r1 = row;
+            } else if (acc < scan.k2) {
+                scan.k2 = acc;
+            }
+        }
+    }
+    const float inf = __int_as_float(0x7f800000);
+    Summary s{inf, inf, inf, 0xffffffffu, inf};
+    if (scan.r1 != 0xffffffffu) {
+        const Bounds2 b1 = bound_of(scan.k1, bound, scan.r1, q);
+        s = Summary{b1.upper, b1.lower,
+                    scan.k2 <= FLT_MAX ? lower_any(scan.k2, bound, q) : inf, scan.r1,
+                    scan.k1};
+    }
+    if (scan.overflow) {
+        summary_insert(s, 0.f, inf, 0xffffffffu, inf);
+    }
+    s = block_reduce_summary(s);
+    __shared__ bool is_last;
+    if (blocks > 1) {
+        if (threadIdx.x == 0) {
+            block_summaries[static_cast<uint64_t>(q) * summary_stride + blockIdx.x] = s;
+            __threadfence();
+            is_last = atomicAdd(done + q, 1u) == blocks - 1;
+        }
+        __syncthreads();
+        if (!is_last) {
+            return;
+        }
+        __threadfence();
+        Summary m{inf, inf, inf, 0xffffffffu, inf};
+        for (uint32_t i = threadIdx.x; i < blocks; i += kFinalizeThreads) {
+            const volatile Summary* src_s =
+                block_summaries + static_cast<uint64_t>(q) * summary_stride + i;
+            Summary b;
+            b.min_upper = src_s->min_upper;
+            b.first = src_s->first;
+            b.second = src_s->second;
+            b.first_row = src_s->first_row;
+            b.first_distance = src_s->first_distance;
+            m = summary_merge(m, b);
+        }
+        s = block_reduce_summary(m);
+        if (threadIdx.x == 0) {
+            done[q] = 0;
+        }
+    }
+    __shared__ bool certified;
+    __shared__ float min_upper;
+    if (threadIdx.x == 0) {
+        certified = s.second > s.min_upper && s.first_row != 0xffffffffu;
+        min_upper = s.min_upper;
+        if (certified) {
+            results[q] = Result{s.first_row, s.first_distance};
+            exact_distances[q] = __longlong_as_double(0x7ff8000000000000ll);
+        } else {
+            atomicAdd(replay_count, 1u);
+        }
+    }
+    __syncthreads();
+    if (certified) {
+        return;
+    }
+    constexpr int warps = kFinalizeThreads / 32;
+    const int warp = threadIdx.x / 32;
+    double best = __longlong_as_double(0x7ff0000000000000ll);
+    uint32_t best_row = 0xffffffffu;
+    for (uint32_t base = warp * 32; base < sq.row_count; base += warps * 32) {
+        const uint32_t r = base + lane;
+        unsigned int mask = __ballot_sync(
+            0xffffffffu,
+            r < sq.row_count && bound_of(__ldcg(dist + r), bound, r, q).lower <= min_upper);
+        while (mask != 0u) {
+            const int bit = __ffs(mask) - 1;
+            mask &= mask - 1u;
+            const uint32_t crow = base + bit;
+            const double d = replay_row(
+                in, qv, in.rows + static_cast<uint64_t>(crow) * in.padded_dim, lane);
+            if (lex_less(d, crow, best, best_row)) {
+                best = d;
+                best_row = crow;
+            }
+        }
+    }
+    __shared__ double warp_best[warps];
+    __shared__ uint32_t warp_best_row[warps];
+    if (lane == 0) {
+        warp_best[warp] = best;
+        warp_best_row[warp] = best_row;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 0; w < warps; ++w) {
+            if (lex_less(warp_best[w], warp_best_row[w], best, best_row)) {
+                best = warp_best[w];
+                best_row = warp_best_row[w];
+            }
+        }
+        results[q] = Result{best_row, static_cast<float>(best)};
+        exact_distances[q] = best;
+    }
+}
+
 constexpr uint32_t kMaxCandidates = 64;
 constexpr int kRescoreUnroll = 4;
 
@@ -1284,6 +1537,128 @@ void launch_small_query(const SmallQuery& sq, uint32_t batch, Bound bound, Repla
     small_query_kernel<<<batch, kFinalizeThreads, smem, stream>>>(
         sq, bound, in, results, exact_distances, replay_count, error_flag);
     check_cuda(cudaGetLastError(), "cannot launch small-index query kernel");
+}
+
+bool flat_query_fits(uint64_t rows, uint64_t padded_dim, uint64_t batch)
+{
+    return rows >= 1 && rows <= 0x7fffffffull && padded_dim >= 4 &&
+           padded_dim <= kFlatColumns && batch >= 1 && batch <= kFlatBatch;
+}
+
+FlatPlan plan_flat_query(uint64_t rows, uint64_t padded_dim, uint64_t batch,
+                         int sm_count)
+{
+    const uint64_t groups = padded_dim / 4;
+    // lanes per row: enough float4 groups per lane (about four or more) to
+    // keep several loads in flight, at least 8 lanes
+    uint32_t lanes = 32;
+    if (groups < 32 * 4) {
+        lanes = groups < 16 * 4 ? 8 : 16;
+    }
+    const uint32_t step = kFinalizeThreads / lanes;  // rows per CTA pass
+    // about four CTAs per SM over the whole launch
+    const uint64_t target = static_cast<uint64_t>(sm_count) * 4;
+    const uint64_t per_query = std::max<uint64_t>(1, target / batch);
+    uint64_t span = (rows + per_query - 1) / per_query;
+    span = std::max<uint64_t>(step, (span + step - 1) / step * step);
+    FlatPlan plan;
+    plan.lanes = lanes;
+    plan.span = static_cast<uint32_t>(span);
+    plan.blocks = static_cast<uint32_t>((rows + span - 1) / span);
+    uint32_t log_lanes = 0;
+    while ((1u << log_lanes) < lanes) {
+        ++log_lanes;
+    }
+    plan.depth = static_cast<uint32_t>(4 * ((groups + lanes - 1) / lanes) + log_lanes);
+    return plan;
+}
+
+namespace {
+
+// Scratch of the fused flat query for a workspace of `capacity` queries:
+// distance slabs, CTA summaries (room for the most CTAs any plan uses) and
+// per-query completion counters at a fixed place (zero between launches).
+struct FlatScratch {
+    float* distances;
+    Summary* summaries;
+    uint32_t* done;
+    uint32_t summary_stride;
+};
+
+FlatScratch flat_scratch(void* base, uint64_t capacity, uint64_t rows)
+{
+    const uint64_t max_blocks = (rows + 7) / 8;  // span >= 8 rows
+    char* p = static_cast<char*>(base);
+    FlatScratch fs;
+    fs.distances = reinterpret_cast<float*>(p);
+    p += capacity * rows * sizeof(float);
+    p = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
+    fs.summaries = reinterpret_cast<Summary*>(p);
+    p += capacity * max_blocks * sizeof(Summary);
+    p = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
+    fs.done = reinterpret_cast<uint32_t*>(p);
+    fs.summary_stride = static_cast<uint32_t>(max_blocks);
+    return fs;
+}
+
+template <int kLanes>
+void launch_flat_lanes(const SmallQuery& sq, const FlatPlan& plan, uint32_t batch,
+                       Bound bound, ReplayInputs in, const FlatScratch& fs,
+                       Result* results, double* exact_distances, uint32_t* replay_count,
+                       int* error_flag, cudaStream_t stream)
+{
+    const size_t smem = sq.padded_dim * sizeof(float);
+    auto kernel = flat_query_kernel<kLanes>;
+    set_dynamic_smem(reinterpret_cast<const void*>(kernel), smem);
+    cudaLaunchConfig_t config{};
+    config.gridDim = dim3(plan.blocks, batch);
+    config.blockDim = dim3(kFinalizeThreads);
+    config.dynamicSmemBytes = smem;
+    config.stream = stream;
+    cudaLaunchAttribute attr[1];
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    check_cuda(cudaStreamIsCapturing(stream, &capture), "cannot query stream capture");
+    if (capture == cudaStreamCaptureStatusNone) {
+        // the next query's launch and gather overlap this kernel
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        config.attrs = attr;
+        config.numAttrs = 1;
+    }
+    check_cuda(cudaLaunchKernelEx(&config, kernel, sq, bound, in, fs.distances,
+                                  fs.summaries, fs.done, fs.summary_stride, plan.span,
+                                  results, exact_distances, replay_count, error_flag),
+               "cannot launch flat query kernel");
+}
+
+}  // namespace
+
+uint64_t flat_query_scratch_bytes(uint64_t capacity, uint64_t rows)
+{
+    const uint64_t max_blocks = (rows + 7) / 8;
+    return capacity * rows * sizeof(float) + 16 + capacity * max_blocks * sizeof(Summary) +
+           16 + capacity * sizeof(uint32_t) + 64;
+}
+
+void launch_flat_query(const SmallQuery& sq, const FlatPlan& plan, uint32_t batch,
+                       Bound bound, ReplayInputs in, void* scratch, uint64_t capacity,
+                       Result* results, double* exact_distances, uint32_t* replay_count,
+                       int* error_flag, cudaStream_t stream)
+{
+    if (batch == 0) {
+        return;
+    }
+    const FlatScratch fs = flat_scratch(scratch, capacity, sq.row_count);
+    if (plan.lanes == 8) {
+        launch_flat_lanes<8>(sq, plan, batch, bound, in, fs, results, exact_distances,
+                             replay_count, error_flag, stream);
+    } else if (plan.lanes == 16) {
+        launch_flat_lanes<16>(sq, plan, batch, bound, in, fs, results, exact_distances,
+                              replay_count, error_flag, stream);
+    } else {
+        launch_flat_lanes<32>(sq, plan, batch, bound, in, fs, results, exact_distances,
+                              replay_count, error_flag, stream);
+    }
 }
 
 void launch_finalize_gemm(PartialView view, const float* row_norms,

@@ -994,6 +994,16 @@ bool small_path_applies(const uha_index* index, uha_strategy strategy)
            uha::small_query_fits(index->rows, index->padded_dim);
 }
 
+// Certified queries of at most uha::kFlatBatch on flat (and small exact)
+// indexes too large for one CTA run as one fused launch with many CTAs per
+// query.
+bool flat_path_applies(const uha_index* index, uha_strategy strategy, uint64_t batch)
+{
+    return strategy == UHA_DIRECT && index->kind != IndexKind::hierarchical &&
+           !uha::small_query_fits(index->rows, index->padded_dim) &&
+           uha::flat_query_fits(index->rows, index->padded_dim, batch);
+}
+
 bool precision_strategy(uha_strategy s)
 {
     return s == UHA_GEMM_BF16_RERANK || s == UHA_GEMM_FP8_RERANK;
@@ -1191,7 +1201,8 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
     uint64_t launches = 0;
 
     const bool hierarchical = index->kind == IndexKind::hierarchical;
-    if (small_path_applies(index, c.strategy)) {
+    const bool flat = flat_path_applies(index, c.strategy, n);
+    if (small_path_applies(index, c.strategy) || flat) {
         uha::SmallQuery sq{};
         sq.queries = source;
         sq.dim = index->dimension;
@@ -1209,9 +1220,12 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
             op = index->weights32.size() != 0 ? uha::ScanOp::l1_weighted : uha::ScanOp::l1;
         }
         sq.op = static_cast<int>(op);
-        const uha::Bound bound = make_bound(uha::small_query_depth(index->padded_dim),
-                                            index->scan_dim,
-                                            op == uha::ScanOp::l1 ? 1 : 2);
+        const uha::FlatPlan flat_plan =
+            flat ? uha::plan_flat_query(index->rows, index->padded_dim, n, index->sm_count)
+                 : uha::FlatPlan{};
+        const uha::Bound bound =
+            make_bound(flat ? flat_plan.depth : uha::small_query_depth(index->padded_dim),
+                       index->scan_dim, op == uha::ScanOp::l1 ? 1 : 2);
         uha::ReplayInputs in{};
         in.op = index->metric == UHA_L2 ? uha::ReplayOp::l2_sequential
                 : index->weights64.size() != 0 ? uha::ReplayOp::l1_weighted_sequential
@@ -1220,11 +1234,25 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
         in.dim = index->scan_dim;
         in.padded_dim = index->padded_dim;
         in.weights64 = index->weights64.get();
+        if (flat && ws->flat_scratch.size() == 0) {
+            // zero once: the kernel leaves its completion counters at zero
+            ws->flat_scratch.allocate(
+                uha::flat_query_scratch_bytes(ws->max_batch, index->rows));
+            check_cuda(cudaMemsetAsync(ws->flat_scratch.get(), 0,
+                                       ws->flat_scratch.bytes(), stream),
+                       "cannot clear flat query scratch");
+        }
         if (time_scan) {
             check_cuda(cudaEventRecord(scan_start, stream), "event");
         }
-        uha::launch_small_query(sq, static_cast<uint32_t>(n), bound, in, results, exact,
-                                replay_count, error_flag, stream);
+        if (flat) {
+            uha::launch_flat_query(sq, flat_plan, static_cast<uint32_t>(n), bound, in,
+                                   ws->flat_scratch.get(), ws->max_batch, results, exact,
+                                   replay_count, error_flag, stream);
+        } else {
+            uha::launch_small_query(sq, static_cast<uint32_t>(n), bound, in, results,
+                                    exact, replay_count, error_flag, stream);
+        }
         if (time_scan) {
             check_cuda(cudaEventRecord(scan_stop, stream), "event");
         }
@@ -1511,7 +1539,7 @@ bool pipeline_applies(const uha_index* index, uha_strategy strategy, uint64_t ba
         return true;  // scores of batch b overlap the re-score of batch b - 1
     }
     return batch <= 8 && (strategy == UHA_DIRECT || strategy == UHA_GEMM) &&
-           !small_path_applies(index, strategy);
+           !small_path_applies(index, strategy) && !flat_path_applies(index, strategy, batch);
 }
 
 void prepare_pipeline(const uha_index* index, uha_workspace* ws, uha_strategy strategy,

@@ -103,6 +103,8 @@ struct uha_workspace {
     uha::DeviceBuffer<double> call_exact;         // replayed distances (NaN: none)
     uha::DeviceBuffer<uint32_t> counters;  // [0] replayed queries, [1] error flag
     uha::DeviceBuffer<unsigned char> finalize_scratch;
+    // fused flat query (allocated and zeroed on first use)
+    uha::DeviceBuffer<unsigned char> flat_scratch;
     // precision strategies (allocated on first use)
     uha::DeviceBuffer<unsigned char> queries_lp;  // lowp_padded_count(max_batch) vectors
     uha::DeviceBuffer<float> query_scales;        // FP8 scale per query

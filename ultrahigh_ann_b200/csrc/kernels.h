@@ -155,6 +155,29 @@ uint32_t small_query_depth(uint64_t padded_dim);
 void launch_small_query(const SmallQuery& sq, uint32_t batch, Bound bound, ReplayInputs in,
                         Result* results, double* exact_distances, uint32_t* replay_count,
                         int* error_flag, cudaStream_t stream);
+// Flat and small exact indexes (padded columns <= kFlatColumns) at batches of
+// at most kFlatBatch queries: gather, scan and certified argmin (with replay)
+// in one launch with many CTAs per query, the last CTA of a query merging.
+// Launched with programmatic stream serialization outside stream capture: the
+// next kernel's launch and gather overlap this one.
+constexpr uint64_t kFlatColumns = 8192;
+constexpr uint64_t kFlatBatch = 8;
+struct FlatPlan {
+    uint32_t lanes;   // lanes per row: 8, 16 or 32
+    uint32_t span;    // rows per CTA
+    uint32_t blocks;  // CTAs per query
+    uint32_t depth;   // longest chain of binary32 additions per distance
+};
+bool flat_query_fits(uint64_t rows, uint64_t padded_dim, uint64_t batch);
+FlatPlan plan_flat_query(uint64_t rows, uint64_t padded_dim, uint64_t batch,
+                         int sm_count);
+// Scratch for a workspace of `capacity` queries; zero when created, left with
+// its counters at zero by every launch.
+uint64_t flat_query_scratch_bytes(uint64_t capacity, uint64_t rows);
+void launch_flat_query(const SmallQuery& sq, const FlatPlan& plan, uint32_t batch,
+                       Bound bound, ReplayInputs in, void* scratch, uint64_t capacity,
+                       Result* results, double* exact_distances, uint32_t* replay_count,
+                       int* error_flag, cudaStream_t stream);
 // Binary32 norm identity (no certification), lowest index on ties.
 void launch_finalize_gemm(PartialView view, const float* row_norms,
                           const float* query_norms, Result* results,
