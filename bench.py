@@ -315,9 +315,10 @@ def summarize(line: dict) -> dict:
     ref = hf.get("reference") or {}
     parity["hierarchical_16"] = ref.get("equal_to_reference")
     out["equal_to_reference"] = parity
-    out["flat_batch1_queries_per_s"] = {
-        f"{e['metric']}_T{e['T']}": e["queries_per_s"] for e in suite_.get("lines", [])
-        if e["index"] == "flat" and e["batch"] == 1}
+    out["flat_batch1"] = {
+        f"{e['metric']}_T{e['T']}": {"queries_per_s": e["queries_per_s"],
+                                     "one_read_frac_of_hbm": e.get("one_read_frac_of_hbm")}
+        for e in suite_.get("lines", []) if e["index"] == "flat" and e["batch"] == 1}
     prec = [e for e in line.get("precision") or [] if e.get("strategy") != "direct"
             and e["batch"] == 1024]
     out["precision_b1024"] = {f"{e['strategy']}_k{e['k']}": {
@@ -386,11 +387,12 @@ def suite(ds, exact_index, nq=1024):
     qdev = torch.from_numpy(queries).cuda()
     have_ref = O.ref_available()
 
-    def timeit(index, B, n):
+    def timeit(index, B, n, emulated=False):
         # One uha_query_many call answers the n device-resident queries in
         # batches of B (each batch as one query_batch call); the first,
         # identical call warms the workspace and its pipeline buffers.
         ws = index.make_query_workspace(B)
+        ws.set_replay(emulated)
         res = np.zeros(n, np.uint64)
         index.query_many(qdev.data_ptr(), n, B, res, ws, on_device=True)
         torch.cuda.synchronize()
@@ -417,6 +419,12 @@ def suite(ds, exact_index, nq=1024):
             out.append({"index": "exact", "metric": metric, "batch": B, "queries": nq,
                         "queries_per_s": round(qps, 1), "replayed": repl,
                         "equal_to_reference": equal(res, ref)})
+        # the replay of uncertified queries without FP64 instructions
+        res, qps, repl = timeit(index, 1, nq, emulated=True)
+        out.append({"index": "exact", "metric": metric, "batch": 1, "queries": nq,
+                    "replay": "emulated (float-float, emulated binary64)",
+                    "queries_per_s": round(qps, 1), "replayed": repl,
+                    "equal_to_reference": equal(res, ref)})
     for metric, cls in (("l2", uha.CudaSampledCoordinateL2AnnIndex),
                         ("l1", uha.CudaSampledCoordinateL1AnnIndex)):
         probs = _probabilities(metric, ds.rows)
@@ -435,12 +443,19 @@ def suite(ds, exact_index, nq=1024):
                 ref_seconds += time.perf_counter() - t
             for B in (1, 64, 1024):
                 res, qps, repl = timeit(index, B, nq)
-                out.append({"index": "flat", "metric": metric, "T": T, "k": len(cs),
-                            "batch": B, "queries": nq, "queries_per_s": round(qps, 1),
-                            "replayed": repl, "equal_to_reference": equal(res, ref),
-                            "sample_equal_to_reference_sampler": sample_equal,
-                            "agreement_vs_fp64_exact": round(
-                                float(np.mean(res == exact_ans[metric])), 4)})
+                entry = {"index": "flat", "metric": metric, "T": T, "k": len(cs),
+                         "batch": B, "queries": nq, "queries_per_s": round(qps, 1),
+                         "replayed": repl, "equal_to_reference": equal(res, ref),
+                         "sample_equal_to_reference_sampler": sample_equal,
+                         "agreement_vs_fp64_exact": round(
+                             float(np.mean(res == exact_ans[metric])), 4)}
+                if B == 1:
+                    # the index's rows read once per query at the measured HBM
+                    # bandwidth (they also fit the 126 MB L2)
+                    row_bytes = ds.rows.shape[0] * (-(-len(cs) // 4) * 4) * 4
+                    entry["one_read_frac_of_hbm"] = round(
+                        row_bytes * qps / (measured_peaks()["hbm_gbs"] * 1e9), 3)
+                out.append(entry)
     return {"lines": out, "probabilities": probability_parity(ds),
             "reference_cpu_seconds": round(ref_seconds, 1)}
 
@@ -466,7 +481,9 @@ def probability_parity(ds, rows=512):
 
 def precision(ds, exact_index, batches=((1, 256), (64, 2048), (1024, 2048))):
     """Precision strategies on the same data: BF16 and FP8-E4M3 tensor-core
-    scores, top-k (k = 8, 32), certified binary32 re-score. For each batch:
+    scores, top-k (k = 8, 32), then a certified re-score of the candidates
+    from the original rows -- binary64 terms (`*_rerank`) or binary32 with
+    near-ties settled without FP64 instructions (`*_rerank_fp32`). For each batch:
     queries/s against the plain certified path at the same batch, agreement of
     the answers with the binary64 exact argmin (the plain path's answers, which
     are the reference CPU's), the relative distance excess over the exact
@@ -503,8 +520,11 @@ def precision(ds, exact_index, batches=((1, 256), (64, 2048), (1024, 2048))):
         ref, ref_dist, plain_qps, _ = timed(B, n, uha.QueryStrategy.direct)
         out.append({"strategy": "direct", "batch": B, "queries": n,
                     "queries_per_s": round(plain_qps, 1)})
-        for strategy, name, elem in ((uha.QueryStrategy.gemm_bf16_rerank, "bf16_rerank", 2),
-                                     (uha.QueryStrategy.gemm_fp8_rerank, "fp8_rerank", 1)):
+        for strategy, name, elem in (
+                (uha.QueryStrategy.gemm_bf16_rerank, "bf16_rerank", 2),
+                (uha.QueryStrategy.gemm_fp8_rerank, "fp8_rerank", 1),
+                (uha.QueryStrategy.gemm_bf16_rerank_fp32, "bf16_rerank_fp32", 2),
+                (uha.QueryStrategy.gemm_fp8_rerank_fp32, "fp8_rerank_fp32", 1)):
             for k in (8, 32):
                 res, dist, qps, st = timed(B, n, strategy, k)
                 excess = (dist - ref_dist) / np.maximum(ref_dist, 1e-300)

@@ -67,12 +67,21 @@ typedef enum uha_metric {
  *     rounded p x k projection times the batch) and re-score by the
  *     reference's binary64 projected distance. The answer equals the
  *     reference CPU index whenever that row is among the k candidates. The
- *     low-precision copies are built on the first query that needs them. */
+ *     low-precision copies are built on the first query that needs them.
+ *   UHA_GEMM_BF16_RERANK_FP32, UHA_GEMM_FP8_RERANK_FP32 (exact and flat L2
+ *     indexes): the same scores and candidates, re-scored in binary32 from
+ *     the original rows with a certified bound; a query whose candidates'
+ *     bounds overlap is settled without FP64 instructions (float-float
+ *     distances, then emulated binary64 for the candidates they cannot
+ *     separate), so the answer is again the reference CPU's whenever its
+ *     row is among the candidates. */
 typedef enum uha_strategy {
     UHA_DIRECT = 0,
     UHA_GEMM = 1,
     UHA_GEMM_BF16_RERANK = 2,
-    UHA_GEMM_FP8_RERANK = 3
+    UHA_GEMM_FP8_RERANK = 3,
+    UHA_GEMM_BF16_RERANK_FP32 = 4,
+    UHA_GEMM_FP8_RERANK_FP32 = 5
 } uha_strategy;
 
 typedef struct uha_index uha_index;
@@ -331,6 +340,20 @@ uha_status uha_workspace_set_timing(uha_workspace* workspace, int enabled);
  * No reference counterpart. */
 uha_status uha_workspace_set_candidates(uha_workspace* workspace,
                                         uint32_t candidates);
+
+/* Arithmetic of the replay that settles uncertified queries of the certified
+ * (UHA_DIRECT) path on exact and flat indexes: UHA_REPLAY_BINARY64 (default)
+ * replays the reference CPU's operations on the FP64 units;
+ * UHA_REPLAY_EMULATED uses no FP64 instruction (float-float distances with a
+ * stated bound, then emulated binary64 for candidates they cannot separate).
+ * Both return the reference CPU's row. Hierarchical indexes always replay in
+ * binary64. No reference counterpart. */
+typedef enum uha_replay_arithmetic {
+    UHA_REPLAY_BINARY64 = 0,
+    UHA_REPLAY_EMULATED = 1
+} uha_replay_arithmetic;
+uha_status uha_workspace_set_replay(uha_workspace* workspace,
+                                    uha_replay_arithmetic arithmetic);
 
 /* Diagnostic of the precision strategies (no reference counterpart): for
  * query_count host queries (at most the workspace capacity), out_scores

@@ -35,6 +35,10 @@ DIRECT = 0
 GEMM = 1
 GEMM_BF16_RERANK = 2
 GEMM_FP8_RERANK = 3
+GEMM_BF16_RERANK_FP32 = 4
+GEMM_FP8_RERANK_FP32 = 5
+REPLAY_BINARY64 = 0
+REPLAY_EMULATED = 1
 
 
 class TuneReport(ctypes.Structure):
@@ -158,6 +162,7 @@ SIGNATURES = {
     "uha_workspace_set_timing": (c_int, [c_void_p, c_int]),
     "uha_workspace_stream": (c_void_p, [c_void_p]),
     "uha_workspace_set_candidates": (c_int, [c_void_p, c_uint32]),
+    "uha_workspace_set_replay": (c_int, [c_void_p, c_int]),
     "uha_workspace_autotune": (c_int, [c_void_p, c_uint64, c_int, POINTER(TuneReport)]),
     "uha_batch_create": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_int, _H]),
     "uha_batch_query_buffer": (c_void_p, [c_void_p, c_uint64]),

@@ -84,6 +84,10 @@ class QueryStrategy(enum.IntEnum):
     # (QueryWorkspace.set_candidates)
     gemm_bf16_rerank = _abi.GEMM_BF16_RERANK
     gemm_fp8_rerank = _abi.GEMM_FP8_RERANK
+    # the same scores and candidates re-scored in binary32 with a certified
+    # bound, near-ties settled without FP64 instructions (exact and flat L2)
+    gemm_bf16_rerank_fp32 = _abi.GEMM_BF16_RERANK_FP32
+    gemm_fp8_rerank_fp32 = _abi.GEMM_FP8_RERANK_FP32
 
 
 CudaDenseL2QueryStrategy = QueryStrategy
@@ -465,6 +469,14 @@ class QueryWorkspace:
         _check(_abi.load().uha_workspace_autotune(self._handle, ctypes.c_uint64(batch),
                                                   int(strategy), ctypes.byref(r)))
         return _tune_dict(r)
+
+    def set_replay(self, emulated: bool) -> None:
+        """Arithmetic of the certified path's replay on exact and flat
+        indexes: binary64 on the FP64 units (default) or, with emulated=True,
+        no FP64 instruction (float-float, then emulated binary64). Both give
+        the reference CPU's row."""
+        _check(_abi.load().uha_workspace_set_replay(
+            self._handle, _abi.REPLAY_EMULATED if emulated else _abi.REPLAY_BINARY64))
 
     def set_candidates(self, candidates: int) -> None:
         """Candidates per query re-scored by the precision strategies (1-64)."""

@@ -14,10 +14,12 @@
 // kernel, in the block that merges the query's summaries, so a query batch
 // needs no host decision between its kernels.
 #include "common.h"
+#include "exact64.h"
 #include "kernels.h"
 
 #include <algorithm>
 #include <cfloat>
+#include <cmath>
 #include <map>
 #include <mutex>
 #include <utility>
@@ -403,6 +405,262 @@ __device__ double replay_candidate(const ReplayInputs& in, const float* qrow,
     return replay_row(in, qrow, in.rows + uint64_t(row) * in.padded_dim, lane);
 }
 
+// ------------------------------------------ replay without the FP64 units
+
+// Float-float distance of one candidate row, evaluated by one warp: each
+// lane forms the terms i = lane, lane + 32, ... (the L2 and weighted-L1 terms
+// within 2^-45 relative, the L1 terms exactly) and adds them in float-float,
+// then a butterfly adds the lanes (ff_add is commutative, so every lane ends
+// with the same value).
+__device__ x64::FF ff_row(const ReplayInputs& in, const float* qrow, const float* rrow,
+                          int lane)
+{
+    x64::FF s{0.f, 0.f};
+    for (uint64_t i = lane; i < in.dim; i += 32) {
+        x64::FF d = x64::two_sum(qrow[i], -rrow[i]);  // q - r exactly
+        x64::FF t;
+        if (in.op == ReplayOp::l2_sequential) {
+            const x64::FF p = x64::two_prod(d.hi, d.hi);
+            const float cross = __fmul_rn(__fmul_rn(2.f, d.hi), d.lo);
+            t = x64::two_sum(p.hi, __fadd_rn(p.lo, cross));
+        } else {
+            if (d.hi < 0.f) {
+                d = x64::FF{-d.hi, -d.lo};
+            }
+            t = d;
+            if (in.op == ReplayOp::l1_weighted_sequential) {
+                const float wh = in.weights_ff[2 * i];
+                const float wl = in.weights_ff[2 * i + 1];
+                const x64::FF p = x64::two_prod(wh, d.hi);
+                const float c = __fmaf_rn(wh, d.lo, __fmul_rn(wl, d.hi));
+                t = x64::two_sum(p.hi, __fadd_rn(p.lo, c));
+            }
+        }
+        s = x64::ff_add(s, t);
+    }
+    for (int o = 16; o > 0; o /= 2) {
+        const x64::FF other{__shfl_xor_sync(0xffffffffu, s.hi, o),
+                            __shfl_xor_sync(0xffffffffu, s.lo, o)};
+        s = x64::ff_add(s, other);
+    }
+    return s;
+}
+
+// The reference CPU's binary64 distance of one row, bit for bit, in emulated
+// binary64 (the operations and order of replay_row). Every lane returns it.
+__device__ uint64_t x64_row(const ReplayInputs& in, const float* qrow, const float* rrow,
+                            int lane)
+{
+    uint64_t s = 0;
+    if (in.op == ReplayOp::l1_grouped4) {
+        const uint64_t groups = in.dim / 4;
+        for (uint64_t base = 0; base < groups; base += 32) {
+            const uint64_t g = base + lane;
+            uint64_t v3 = 0;
+            if (g < groups) {
+                const uint64_t i = 4 * g;
+                uint64_t t[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    t[e] = x64::sub(x64::from_float(qrow[i + e]), x64::from_float(rrow[i + e])) &
+                           ~x64::kSignBit;
+                }
+                v3 = x64::add(x64::add(t[0], t[1]), x64::add(t[2], t[3]));
+            }
+            const uint64_t n = groups - base < 32 ? groups - base : 32;
+            for (uint64_t j = 0; j < n; ++j) {
+                s = x64::add(s, __shfl_sync(0xffffffffu, v3, static_cast<int>(j)));
+            }
+        }
+        for (uint64_t i = 4 * groups; i < in.dim; ++i) {
+            s = x64::add(s, x64::sub(x64::from_float(qrow[i]), x64::from_float(rrow[i])) &
+                                ~x64::kSignBit);
+        }
+        return s;
+    }
+    const uint64_t* w64 = reinterpret_cast<const uint64_t*>(in.weights64);
+    for (uint64_t base = 0; base < in.dim; base += 32) {
+        const uint64_t i = base + lane;
+        uint64_t t = 0;
+        if (i < in.dim) {
+            const uint64_t d = x64::sub(x64::from_float(qrow[i]), x64::from_float(rrow[i]));
+            t = in.op == ReplayOp::l2_sequential ? x64::mul(d, d)
+                                                 : x64::mul(w64[i], d & ~x64::kSignBit);
+        }
+        const uint64_t n = in.dim - base < 32 ? in.dim - base : 32;
+        for (uint64_t j = 0; j < n; ++j) {
+            s = x64::add(s, __shfl_sync(0xffffffffu, t, static_cast<int>(j)));
+        }
+    }
+    return s;
+}
+
+constexpr uint32_t kResolveCap = 512;
+
+struct ResolveSmem {
+    uint32_t row[kResolveCap];
+    float hi[kResolveCap];
+    float lo[kResolveCap];
+    float delta[kResolveCap];
+    unsigned char replay[kResolveCap];
+    uint32_t count;
+    uint32_t winner;
+    uint32_t unseparated;
+};
+
+__device__ __forceinline__ void resolve_begin(ResolveSmem& sm)
+{
+    if (threadIdx.x == 0) {
+        sm.count = 0;
+    }
+    __syncthreads();
+}
+
+// Appends a candidate row (any thread); false when the list is full.
+__device__ __forceinline__ bool resolve_push(ResolveSmem& sm, uint32_t row)
+{
+    const uint32_t slot = atomicAdd(&sm.count, 1u);
+    if (slot < kResolveCap) {
+        sm.row[slot] = row;
+        return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void lex_update_bits(unsigned long long& best, uint32_t& best_row,
+                                                unsigned long long bits, uint32_t row)
+{
+    if (bits < best || (bits == best && row < best_row)) {
+        best = bits;
+        best_row = row;
+    }
+}
+
+// The block's lexicographic minimum of the warps' (binary64 bits, row), all
+// distances nonnegative (their bits order like the values), into the result.
+__device__ void resolve_finish(unsigned long long best, uint32_t best_row, Result* result,
+                               double* exact_distance)
+{
+    constexpr int warps = kFinalizeThreads / 32;
+    __shared__ unsigned long long warp_bits[warps];
+    __shared__ uint32_t warp_rows[warps];
+    if (threadIdx.x % 32 == 0) {
+        warp_bits[threadIdx.x / 32] = best;
+        warp_rows[threadIdx.x / 32] = best_row;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int v = 0; v < warps; ++v) {
+            lex_update_bits(best, best_row, warp_bits[v], warp_rows[v]);
+        }
+        *result = Result{best_row, x64::to_float(best)};
+        *exact_distance = __longlong_as_double(static_cast<long long>(best));
+    }
+}
+
+// Block-wide: the reference CPU's argmin among the listed candidate rows of
+// one query (every one of which may hold the minimum), without FP64
+// instructions. (1) Float-float distance S_i of every candidate; the
+// reference's value lies within delta_i = ff_rel S_i + ff_abs of it. (2) The
+// candidate i* with the smallest S_i + delta_i wins outright when every other
+// candidate j is separated: a lower bound of S_j - S_i* exceeds
+// delta_j + delta_i*, so the reference's distance of j is larger. (3)
+// Otherwise i* and the candidates not separated from it are replayed in
+// emulated binary64 and the lexicographic minimum of (distance, row) wins.
+// When the list overflowed (more than kResolveCap candidates), every row for
+// which `is_candidate` holds is replayed in emulated binary64 instead.
+// Writes results[q] / exact_distances[q] (binary64 bits of the distance).
+template <typename IsCandidate>
+__device__ void resolve_without_fp64(const ReplayInputs& in, const float* qrow,
+                                     ResolveSmem& sm, uint32_t row_count,
+                                     IsCandidate is_candidate, Result* result,
+                                     double* exact_distance)
+{
+    constexpr int warps = kFinalizeThreads / 32;
+    const int warp = threadIdx.x / 32;
+    const int lane = threadIdx.x % 32;
+    __syncthreads();
+    const uint32_t n = sm.count;
+    unsigned long long best = ~0ull;
+    uint32_t best_row = 0xffffffffu;
+    if (n > kResolveCap) {
+        for (uint32_t base = warp * 32; base < row_count; base += warps * 32) {
+            const uint32_t r = base + lane;
+            unsigned int mask = __ballot_sync(0xffffffffu, r < row_count && is_candidate(r));
+            while (mask != 0u) {
+                const int bit = __ffs(mask) - 1;
+                mask &= mask - 1u;
+                const uint32_t crow = base + bit;
+                lex_update_bits(best, best_row,
+                                x64_row(in, qrow, in.rows + uint64_t(crow) * in.padded_dim,
+                                        lane),
+                                crow);
+            }
+        }
+        resolve_finish(best, best_row, result, exact_distance);
+        return;
+    }
+    for (uint32_t i = warp; i < n; i += warps) {
+        const x64::FF s = ff_row(in, qrow, in.rows + uint64_t(sm.row[i]) * in.padded_dim, lane);
+        if (lane == 0) {
+            sm.hi[i] = s.hi;
+            sm.lo[i] = s.lo;
+            sm.delta[i] = __fadd_ru(__fmul_ru(in.ff_rel, __fmul_ru(fabsf(s.hi), 1.0000002f)),
+                                    in.ff_abs);
+            sm.replay[i] = 0;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        // any choice of i* is valid; the smallest approximate upper end makes
+        // separation likely
+        uint32_t w = 0;
+        for (uint32_t i = 1; i < n; ++i) {
+            const float ui = __fadd_ru(sm.hi[i], sm.delta[i]);
+            const float uw = __fadd_ru(sm.hi[w], sm.delta[w]);
+            if (ui < uw || (ui == uw && sm.row[i] < sm.row[w])) {
+                w = i;
+            }
+        }
+        sm.winner = w;
+        sm.unseparated = 0;
+        sm.replay[w] = 1;
+    }
+    __syncthreads();
+    const uint32_t w = sm.winner;
+    for (uint32_t j = threadIdx.x; j < n; j += kFinalizeThreads) {
+        if (j == w) {
+            continue;
+        }
+        // lower bound of S_j - S_w: exact difference of the high parts, the
+        // rest rounded down (a NaN from overflowed sums fails the test)
+        const x64::FF a = x64::two_sum(sm.hi[j], -sm.hi[w]);
+        const float lower =
+            __fadd_rd(a.hi, __fadd_rd(a.lo, __fsub_rd(sm.lo[j], sm.lo[w])));
+        if (!(lower > __fadd_ru(sm.delta[j], sm.delta[w]))) {
+            sm.replay[j] = 1;
+            atomicAdd(&sm.unseparated, 1u);
+        }
+    }
+    __syncthreads();
+    if (sm.unseparated == 0) {
+        if (threadIdx.x == 0) {
+            const uint64_t bits = x64::add(x64::from_float(sm.hi[w]), x64::from_float(sm.lo[w]));
+            *result = Result{sm.row[w], x64::to_float(bits)};
+            *exact_distance = __longlong_as_double(static_cast<long long>(bits));
+        }
+        return;
+    }
+    for (uint32_t i = warp; i < n; i += warps) {
+        if (sm.replay[i]) {
+            const uint32_t r = sm.row[i];
+            lex_update_bits(best, best_row,
+                            x64_row(in, qrow, in.rows + uint64_t(r) * in.padded_dim, lane), r);
+        }
+    }
+    resolve_finish(best, best_row, result, exact_distance);
+}
+
 // One block per query: each warp re-scores candidates by the reference's
 // binary64 squared distance in the projected space (j order); the block keeps
 // the lexicographic minimum of (distance, row).
@@ -518,6 +776,7 @@ __device__ __forceinline__ void scan_rows(const PartialView& view, const Bound& 
 // candidate row (D - err <= U*) in binary64, one warp per candidate, and keeps
 // the lexicographic minimum of (distance, row). exact_distances[q] is the
 // replayed distance, or NaN when the query was certified.
+template <bool kEmulated>
 __global__ void __launch_bounds__(kFinalizeThreads)
     argmin_kernel(PartialView view, Bound bound, ReplayInputs in, Result* results,
                   double* exact_distances, Summary* block_summaries,
@@ -602,6 +861,22 @@ __global__ void __launch_bounds__(kFinalizeThreads)
     }
 
     const float* qrow = in.queries + static_cast<uint64_t>(q) * in.padded_dim;
+    if constexpr (kEmulated) {
+        // exact and flat ops only: settled without FP64 instructions
+        __shared__ ResolveSmem rs;
+        auto is_candidate = [&](uint32_t r) {
+            return bound_of(row_distance(view, q, r), bound, r, q).lower <= min_upper;
+        };
+        resolve_begin(rs);
+        for (uint32_t r = threadIdx.x; r < view.rows; r += kFinalizeThreads) {
+            if (is_candidate(r)) {
+                resolve_push(rs, r);
+            }
+        }
+        resolve_without_fp64(in, qrow, rs, view.rows, is_candidate, results + q,
+                             exact_distances + q);
+        return;
+    }
     extern __shared__ double projected_query[];
     if (projected_op(in.op)) {
         project_query64(in, qrow, projected_query);
@@ -789,6 +1064,7 @@ __global__ void __launch_bounds__(kFinalizeThreads)
 // certifies the argmin, replaying the candidates in binary64 when needed.
 // Answers are those of the three-kernel path; only the accumulation depth
 // (and with it the bound) differs.
+template <bool kEmulated>
 __global__ void __launch_bounds__(kFinalizeThreads)
     small_query_kernel(SmallQuery sq, Bound bound, ReplayInputs in, Result* results,
                        double* exact_distances, uint32_t* replay_count, int* error_flag)
@@ -900,6 +1176,21 @@ __global__ void __launch_bounds__(kFinalizeThreads)
     if (certified) {
         return;
     }
+    if constexpr (kEmulated) {
+        __shared__ ResolveSmem rs;
+        auto is_candidate = [&](uint32_t r) {
+            return bound_of(dist[r], bound, r, q).lower <= min_upper;
+        };
+        resolve_begin(rs);
+        for (uint32_t r = threadIdx.x; r < sq.row_count; r += kFinalizeThreads) {
+            if (is_candidate(r)) {
+                resolve_push(rs, r);
+            }
+        }
+        resolve_without_fp64(in, qv, rs, sq.row_count, is_candidate, results + q,
+                             exact_distances + q);
+        return;
+    }
     double best = __longlong_as_double(0x7ff0000000000000ll);
     uint32_t best_row = 0xffffffffu;
     for (uint32_t row = warp; row < sq.row_count; row += warps) {
@@ -986,7 +1277,7 @@ __device__ __forceinline__ float flat_terms(int op, float acc, const float4 a,
 // passes wait_for_previous_grid() before it writes anything, so a grid that
 // starts early (programmatic serialization) only overlaps its launch and its
 // gather with the previous kernel.
-template <int kLanes>
+template <int kLanes, bool kEmulated>
 __global__ void __launch_bounds__(kFinalizeThreads)
     flat_query_kernel(SmallQuery sq, Bound bound, ReplayInputs in, float* distances,
                       Summary* block_summaries, uint32_t* done, uint32_t summary_stride,
@@ -1142,6 +1433,21 @@ __global__ void __launch_bounds__(kFinalizeThreads)
     }
     __syncthreads();
     if (certified) {
+        return;
+    }
+    if constexpr (kEmulated) {
+        __shared__ ResolveSmem rs;
+        auto is_candidate = [&](uint32_t r) {
+            return bound_of(__ldcg(dist + r), bound, r, q).lower <= min_upper;
+        };
+        resolve_begin(rs);
+        for (uint32_t r = threadIdx.x; r < sq.row_count; r += kFinalizeThreads) {
+            if (is_candidate(r)) {
+                resolve_push(rs, r);
+            }
+        }
+        resolve_without_fp64(in, qv, rs, sq.row_count, is_candidate, results + q,
+                             exact_distances + q);
         return;
     }
     constexpr int warps = kFinalizeThreads / 32;
@@ -1379,6 +1685,153 @@ __global__ void __launch_bounds__(kFinalizeThreads)
     }
 }
 
+// Binary32 squared distance of one row summed by the whole block with the
+// structure of block_l2_64 (four accumulators per thread over its float4
+// groups, pairwise, warp butterfly, fixed tree over the eight warps), so its
+// longest addition chain is rescore_depth() as well.
+__device__ float block_l2_32(const float* q, const float* r, uint64_t padded_dim,
+                             float* scratch)
+{
+    const uint64_t groups = padded_dim / 4;
+    const float4* q4 = reinterpret_cast<const float4*>(q);
+    const float4* r4 = reinterpret_cast<const float4*>(r);
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+    uint64_t g = threadIdx.x;
+    for (; g + (kRescoreUnroll - 1) * kFinalizeThreads < groups;
+         g += kRescoreUnroll * kFinalizeThreads) {
+        float4 x[kRescoreUnroll];
+        float4 y[kRescoreUnroll];
+#pragma unroll
+        for (int u = 0; u < kRescoreUnroll; ++u) {
+            x[u] = q4[g + u * kFinalizeThreads];
+            y[u] = __ldg(r4 + g + u * kFinalizeThreads);
+        }
+#pragma unroll
+        for (int u = 0; u < kRescoreUnroll; ++u) {
+            const float d0 = __fsub_rn(x[u].x, y[u].x);
+            const float d1 = __fsub_rn(x[u].y, y[u].y);
+            const float d2 = __fsub_rn(x[u].z, y[u].z);
+            const float d3 = __fsub_rn(x[u].w, y[u].w);
+            a0 = __fmaf_rn(d0, d0, a0);
+            a1 = __fmaf_rn(d1, d1, a1);
+            a2 = __fmaf_rn(d2, d2, a2);
+            a3 = __fmaf_rn(d3, d3, a3);
+        }
+    }
+    for (; g < groups; g += kFinalizeThreads) {
+        const float4 x = q4[g];
+        const float4 y = __ldg(r4 + g);
+        const float d0 = __fsub_rn(x.x, y.x);
+        const float d1 = __fsub_rn(x.y, y.y);
+        const float d2 = __fsub_rn(x.z, y.z);
+        const float d3 = __fsub_rn(x.w, y.w);
+        a0 = __fmaf_rn(d0, d0, a0);
+        a1 = __fmaf_rn(d1, d1, a1);
+        a2 = __fmaf_rn(d2, d2, a2);
+        a3 = __fmaf_rn(d3, d3, a3);
+    }
+    float t = __fadd_rn(__fadd_rn(a0, a1), __fadd_rn(a2, a3));
+    for (int o = 16; o > 0; o /= 2) {
+        t = __fadd_rn(t, __shfl_xor_sync(0xffffffffu, t, o));
+    }
+    if (threadIdx.x % 32 == 0) {
+        scratch[threadIdx.x / 32] = t;
+    }
+    __syncthreads();
+    return __fadd_rn(__fadd_rn(__fadd_rn(scratch[0], scratch[1]),
+                               __fadd_rn(scratch[2], scratch[3])),
+                     __fadd_rn(__fadd_rn(scratch[4], scratch[5]),
+                               __fadd_rn(scratch[6], scratch[7])));
+}
+
+// The FP32 re-score of the precision strategies, without FP64 instructions.
+// grid = (k, batch): CTA (c, q) computes candidate c's binary32 distance from
+// the original rows; the last CTA of the query certifies: one candidate whose
+// bound can hold the reference minimum is the answer (its binary32 distance
+// reported); otherwise the candidates that can are settled by
+// resolve_without_fp64 (float-float, then emulated binary64 for unseparated
+// ones).
+__global__ void __launch_bounds__(kFinalizeThreads)
+    rescore32_kernel(Bound bound, ReplayInputs in, const uint32_t* candidates,
+                     uint32_t k, uint32_t row_count, float* cand_dist, uint32_t* done,
+                     Result* results, double* exact_distances, uint32_t* replay_count)
+{
+    const uint32_t c = blockIdx.x;
+    const uint32_t q = blockIdx.y;
+    const float inf = __int_as_float(0x7f800000);
+    __shared__ float scratch[kFinalizeThreads / 32];
+    __shared__ bool is_last;
+    const float* qrow = in.queries + static_cast<uint64_t>(q) * in.padded_dim;
+    const uint32_t row = candidates[static_cast<uint64_t>(q) * k + c];
+    float d = inf;
+    if (row < row_count) {
+        d = block_l2_32(qrow, in.rows + static_cast<uint64_t>(row) * in.padded_dim,
+                        in.padded_dim, scratch);
+    }
+    if (threadIdx.x == 0) {
+        cand_dist[static_cast<uint64_t>(q) * k + c] = d;
+        __threadfence();
+        is_last = atomicAdd(done + q, 1u) == k - 1;
+    }
+    __syncthreads();
+    if (!is_last) {
+        return;
+    }
+    __threadfence();
+    __shared__ float dist[kMaxCandidates];
+    __shared__ uint32_t cand[kMaxCandidates];
+    for (uint32_t i = threadIdx.x; i < k; i += kFinalizeThreads) {
+        dist[i] = static_cast<volatile float*>(cand_dist)[static_cast<uint64_t>(q) * k + i];
+        cand[i] = candidates[static_cast<uint64_t>(q) * k + i];
+    }
+    __syncthreads();
+    __shared__ bool certified;
+    __shared__ float min_upper;
+    if (threadIdx.x == 0) {
+        done[q] = 0;
+        float first = inf, second = inf, upper = inf;
+        uint32_t first_i = 0xffffffffu;
+        for (uint32_t i = 0; i < k; ++i) {
+            if (cand[i] >= row_count) {
+                continue;
+            }
+            const Bounds2 b = bound_of(dist[i], bound, cand[i], q);
+            upper = fminf(upper, b.upper);
+            if (first_i == 0xffffffffu || b.lower < first ||
+                (b.lower == first && cand[i] < cand[first_i])) {
+                second = first;
+                first = b.lower;
+                first_i = i;
+            } else if (b.lower < second) {
+                second = b.lower;
+            }
+        }
+        certified = first_i != 0xffffffffu && second > upper;
+        min_upper = upper;
+        if (certified) {
+            results[q] = Result{cand[first_i], dist[first_i]};
+            exact_distances[q] = __longlong_as_double(
+                static_cast<long long>(x64::from_float(dist[first_i])));
+        } else {
+            atomicAdd(replay_count, 1u);
+        }
+    }
+    __syncthreads();
+    if (certified) {
+        return;
+    }
+    __shared__ ResolveSmem rs;
+    resolve_begin(rs);
+    for (uint32_t i = threadIdx.x; i < k; i += kFinalizeThreads) {
+        if (cand[i] < row_count && bound_of(dist[i], bound, cand[i], q).lower <= min_upper) {
+            resolve_push(rs, cand[i]);
+        }
+    }
+    // k <= kMaxCandidates < kResolveCap: the list never overflows
+    resolve_without_fp64(in, qrow, rs, row_count, [](uint32_t) { return false; },
+                         results + q, exact_distances + q);
+}
+
 // Raises a kernel's dynamic shared-memory limit when a launch needs more than
 // 48 KB and more than it was configured for on this device (a call that needs
 // no more makes no runtime call, so captured launches after a warm-up make
@@ -1472,8 +1925,9 @@ void launch_argmin(PartialView view, Bound bound, ReplayInputs in,
     FinalizeScratch fs = finalize_scratch(scratch, static_cast<uint32_t>(capacity),
                                           view.rows);
     const size_t smem = replay_smem(in);
-    set_dynamic_smem(reinterpret_cast<const void*>(argmin_kernel), smem);
-    argmin_kernel<<<dim3(blocks, view.batch), kFinalizeThreads, smem, stream>>>(
+    const auto kernel = in.emulated ? argmin_kernel<true> : argmin_kernel<false>;
+    set_dynamic_smem(reinterpret_cast<const void*>(kernel), smem);
+    kernel<<<dim3(blocks, view.batch), kFinalizeThreads, smem, stream>>>(
         view, bound, in, results, exact_distances, fs.summaries, fs.done,
         replay_count, span);
     check_cuda(cudaGetLastError(), "cannot launch argmin kernel");
@@ -1514,6 +1968,35 @@ void launch_rescore(Bound64 bound, ReplayInputs in, const uint32_t* candidates,
     check_cuda(cudaGetLastError(), "cannot launch re-score kernel");
 }
 
+void launch_rescore32(Bound bound, ReplayInputs in, const uint32_t* candidates,
+                      uint32_t k, uint32_t batch, uint32_t rows, float* cand_dist,
+                      uint32_t* done, Result* results, double* exact_distances,
+                      uint32_t* replay_count, cudaStream_t stream)
+{
+    if (batch == 0 || k == 0) {
+        return;
+    }
+    rescore32_kernel<<<dim3(k, batch), kFinalizeThreads, 0, stream>>>(
+        bound, in, candidates, k, rows, cand_dist, done, results, exact_distances,
+        replay_count);
+    check_cuda(cudaGetLastError(), "cannot launch FP32 re-score kernel");
+}
+
+void emulated_replay_bound(uint64_t dim, float* rel, float* abs)
+{
+    // float-float: terms within 2^-45, each lane's chain of ceil(dim / 32)
+    // additions and five butterfly levels at 2^-45 each; the reference CPU's
+    // own binary64 rounding, gamma(dim + 3); binary32 underflow of tiny terms
+    // as an absolute term
+    const double u = std::ldexp(1.0, -53);
+    const double n64 = static_cast<double>(dim) + 3;
+    const double chain = static_cast<double>((dim + 31) / 32) + 7;
+    const double r = 1.01 * (chain * std::ldexp(1.0, -45) + n64 * u / (1.0 - n64 * u)) +
+                     std::ldexp(1.0, -40);
+    *rel = std::nextafter(static_cast<float>(r), 1.0f);
+    *abs = static_cast<float>((2.0 * static_cast<double>(dim) + 16.0) * std::ldexp(1.0, -148));
+}
+
 bool small_query_fits(uint64_t rows, uint64_t padded_dim)
 {
     return rows >= 1 && rows <= kSmallRows && padded_dim <= kSmallColumns &&
@@ -1534,7 +2017,8 @@ void launch_small_query(const SmallQuery& sq, uint32_t batch, Bound bound, Repla
         return;
     }
     const size_t smem = (sq.padded_dim + sq.row_count) * sizeof(float);
-    small_query_kernel<<<batch, kFinalizeThreads, smem, stream>>>(
+    const auto kernel = in.emulated ? small_query_kernel<true> : small_query_kernel<false>;
+    kernel<<<batch, kFinalizeThreads, smem, stream>>>(
         sq, bound, in, results, exact_distances, replay_count, error_flag);
     check_cuda(cudaGetLastError(), "cannot launch small-index query kernel");
 }
@@ -1608,7 +2092,8 @@ void launch_flat_lanes(const SmallQuery& sq, const FlatPlan& plan, uint32_t batc
                        int* error_flag, cudaStream_t stream)
 {
     const size_t smem = sq.padded_dim * sizeof(float);
-    auto kernel = flat_query_kernel<kLanes>;
+    const auto kernel =
+        in.emulated ? flat_query_kernel<kLanes, true> : flat_query_kernel<kLanes, false>;
     set_dynamic_smem(reinterpret_cast<const void*>(kernel), smem);
     cudaLaunchConfig_t config{};
     config.gridDim = dim3(plan.blocks, batch);

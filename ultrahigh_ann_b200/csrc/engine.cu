@@ -164,6 +164,19 @@ void upload(DeviceBuffer<T>& dst, const T* src, uint64_t count)
     }
 }
 
+// The binary64 weights as float pairs (hi = nearest binary32, lo = the
+// nearest binary32 to the rest) for the emulated replay's float-float terms.
+void upload_weights_ff(uha_index& index, const std::vector<double>& w64)
+{
+    std::vector<float> ff(2 * w64.size());
+    for (size_t i = 0; i < w64.size(); ++i) {
+        const float hi = static_cast<float>(w64[i]);
+        ff[2 * i] = hi;
+        ff[2 * i + 1] = static_cast<float>(w64[i] - static_cast<double>(hi));
+    }
+    upload(index.weights_ff, ff.data(), ff.size());
+}
+
 void compute_row_norms(uha_index& index)
 {
     index.row_norms.allocate(index.rows);
@@ -421,6 +434,7 @@ extern "C" uha_status uha_weighted_l1_index_create(int device,
         }
         upload(index->weights32, w32.data(), w32.size());
         upload(index->weights64, w64.data(), w64.size());
+        upload_weights_ff(*index, w64);
         const uint64_t f = sizeof(float);
         index->usage.index_payload_bytes =
             row_count * dimension * f + dimension * f;
@@ -534,6 +548,7 @@ void create_sampled_index(int device, uha_metric metric, const RowSource& src,
     } else {
         upload(index->weights32, w32.data(), w32.size());
         upload(index->weights64, w64.data(), w64.size());
+        upload_weights_ff(*index, w64);
     }
     // Gather (and scale) the sampled columns of the rows on the device.
     if (src.device != nullptr) {
@@ -1006,12 +1021,29 @@ bool flat_path_applies(const uha_index* index, uha_strategy strategy, uint64_t b
 
 bool precision_strategy(uha_strategy s)
 {
-    return s == UHA_GEMM_BF16_RERANK || s == UHA_GEMM_FP8_RERANK;
+    return s == UHA_GEMM_BF16_RERANK || s == UHA_GEMM_FP8_RERANK ||
+           s == UHA_GEMM_BF16_RERANK_FP32 || s == UHA_GEMM_FP8_RERANK_FP32;
+}
+
+// The precision strategies that re-score in binary32 (no FP64 instructions).
+bool fp32_rescore_strategy(uha_strategy s)
+{
+    return s == UHA_GEMM_BF16_RERANK_FP32 || s == UHA_GEMM_FP8_RERANK_FP32;
+}
+
+// Replay inputs of the emulated (FP64-free) replay of exact and flat ops.
+void set_emulated(uha::ReplayInputs& in, const uha_index* index)
+{
+    in.emulated = true;
+    in.weights_ff = index->weights_ff.get();
+    uha::emulated_replay_bound(index->scan_dim, &in.ff_rel, &in.ff_abs);
 }
 
 uha::LowpType lowp_type(uha_strategy s)
 {
-    return s == UHA_GEMM_FP8_RERANK ? uha::LowpType::fp8_e4m3 : uha::LowpType::bf16;
+    return s == UHA_GEMM_FP8_RERANK || s == UHA_GEMM_FP8_RERANK_FP32
+               ? uha::LowpType::fp8_e4m3
+               : uha::LowpType::bf16;
 }
 
 // The index's low-precision rows of `type`, rounded from the scanned binary32
@@ -1234,6 +1266,9 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
         in.dim = index->scan_dim;
         in.padded_dim = index->padded_dim;
         in.weights64 = index->weights64.get();
+        if (ws->emulated_replay) {
+            set_emulated(in, index);
+        }
         if (flat && ws->flat_scratch.size() == 0) {
             // zero once: the kernel leaves its completion counters at zero
             ws->flat_scratch.allocate(
@@ -1319,14 +1354,27 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
             check_cuda(cudaStreamWaitEvent(c.finish_stream, c.handoff, 0), "event");
             stream = c.finish_stream;
         }
-        const uha::Bound64 bound =
-            uha::make_bound64(uha::rescore_depth(index->padded_dim), index->scan_dim);
         uha::ReplayInputs in{};
         in.op = uha::ReplayOp::l2_sequential;
         in.rows = index->scan_rows.get();
         in.queries = prepared;
         in.dim = index->scan_dim;
         in.padded_dim = index->padded_dim;
+        if (fp32_rescore_strategy(c.strategy)) {
+            set_emulated(in, index);
+            const uha::Bound bound32 =
+                make_bound(uha::rescore_depth(index->padded_dim), index->scan_dim, 2);
+            double* slot = c.cand_dist != nullptr ? c.cand_dist : ws->cand_dist.get();
+            uha::launch_rescore32(bound32, in, candidates, k, static_cast<uint32_t>(n),
+                                  static_cast<uint32_t>(index->rows),
+                                  reinterpret_cast<float*>(slot),
+                                  c.rescore_done != nullptr ? c.rescore_done
+                                                            : ws->rescore_done.get(),
+                                  results, exact, replay_count, stream);
+            return launches + 4;
+        }
+        const uha::Bound64 bound =
+            uha::make_bound64(uha::rescore_depth(index->padded_dim), index->scan_dim);
         uha::launch_rescore(bound, in, candidates, k, static_cast<uint32_t>(n),
                             static_cast<uint32_t>(index->rows),
                             c.cand_dist != nullptr ? c.cand_dist : ws->cand_dist.get(),
@@ -1446,6 +1494,9 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
     } else {
         in.op = uha::ReplayOp::l1_grouped4;
     }
+    if (!hierarchical && ws->emulated_replay) {
+        set_emulated(in, index);
+    }
     uha::launch_argmin(view, bound, in, results, exact, ws->finalize_scratch.get(),
                        ws->max_batch, replay_count, stream);
     ++launches;
@@ -1518,6 +1569,8 @@ void validate_query_call(const uha_index* index, uha_workspace* ws,
             UHA_INVALID_ARGUMENT, "unknown CUDA query strategy");
     require(!precision_strategy(strategy) || index->metric == UHA_L2, UHA_INVALID_ARGUMENT,
             "precision strategies serve L2 indexes");
+    require(!fp32_rescore_strategy(strategy) || index->kind != IndexKind::hierarchical,
+            UHA_INVALID_ARGUMENT, "FP32 re-score strategies serve exact and flat L2 indexes");
     if (count != 0) {
         require(out_indices != nullptr, UHA_INVALID_ARGUMENT, "output must not be null");
         require(queries != nullptr || index->dimension == 0, UHA_INVALID_ARGUMENT,
@@ -1748,6 +1801,18 @@ extern "C" uha_status uha_query_many(const uha_index* index, uha_workspace* ws,
         ws->last.kernel_launches = launches;
         finish_call(index, ws, n, ws->host_results.get(), ws->host_exact.get(),
                     out_indices, out_distances);
+    });
+}
+
+extern "C" uha_status uha_workspace_set_replay(uha_workspace* workspace,
+                                               uha_replay_arithmetic arithmetic)
+{
+    return guarded([&] {
+        require(workspace != nullptr, UHA_INVALID_ARGUMENT,
+                "workspace must not be null");
+        require(arithmetic == UHA_REPLAY_BINARY64 || arithmetic == UHA_REPLAY_EMULATED,
+                UHA_INVALID_ARGUMENT, "unknown replay arithmetic");
+        workspace->emulated_replay = arithmetic == UHA_REPLAY_EMULATED;
     });
 }
 

@@ -10,6 +10,7 @@
 namespace uha_engine {
 
 bool precision_strategy(uha_strategy s);
+bool fp32_rescore_strategy(uha_strategy s);
 bool small_path_applies(const uha_index* index, uha_strategy strategy);
 uha::LowpType lowp_type(uha_strategy s);
 

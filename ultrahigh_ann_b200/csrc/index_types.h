@@ -53,6 +53,7 @@ struct uha_index {
     uha::DeviceBuffer<float> row_norms;   // rows (L2, norm-identity strategy)
     uha::DeviceBuffer<float> weights32;   // padded_dim (weighted L1 scan)
     uha::DeviceBuffer<double> weights64;  // scan_dim (weighted L1 replay)
+    uha::DeviceBuffer<float> weights_ff;  // 2 x scan_dim: weights64 as hi, lo
     uha::DeviceBuffer<uint32_t> columns;  // sample_size (sampled)
     uha::DeviceBuffer<float> scales;      // sample_size (sampled L2)
     // hierarchical: scan_dim = p; scan_rows = binary32 projected rows
@@ -122,6 +123,7 @@ struct uha_workspace {
     uha::DeviceBuffer<unsigned int> gathered_amax;
     uha::DeviceBuffer<double> projected64;
     uint32_t candidates_per_query = 32;
+    bool emulated_replay = false;  // uha_workspace_set_replay
     std::vector<TunedPlan> tuned;  // autotuned shapes (uha_workspace_autotune)
 
     const TunedPlan* find_tuned(uint64_t batch, int strategy) const

@@ -118,7 +118,18 @@ struct ReplayInputs {
     const double* rows64 = nullptr;        // projected ops: [rows][proj_dim]
     const double* projection64 = nullptr;  // projected ops: [proj_dim][dim]
     uint64_t proj_dim = 0;
+    // Replay without the FP64 units (exact and flat ops): a float-float
+    // distance per candidate, within ff_rel * S + ff_abs of the reference
+    // CPU's binary64 value (its own rounding included), decides unless two
+    // candidates' intervals overlap; those are replayed in emulated binary64
+    // (exact64.h). weights_ff: the binary64 weights as float pairs hi, lo.
+    bool emulated = false;
+    float ff_rel = 0.f;
+    float ff_abs = 0.f;
+    const float* weights_ff = nullptr;
 };
+// ff_rel / ff_abs of the emulated replay of `dim` terms.
+void emulated_replay_bound(uint64_t dim, float* rel, float* abs);
 
 // Scratch of the argmin (per-query merge state, layout fixed by the workspace
 // capacity). It must be zero when the workspace is created; the argmin leaves
@@ -261,7 +272,8 @@ struct Bound64 {
     double rel;
     double abs;
 };
-// Accumulation depth of the re-score's binary64 distances (for the bound).
+// Accumulation depth of the re-score's binary64 distances (for the bound);
+// the binary32 re-score has the same structure and depth.
 uint32_t rescore_depth(uint64_t padded_dim);
 uint32_t max_rerank_candidates();
 // Certified argmin of each query over its k candidates (ReplayInputs as for
@@ -273,6 +285,14 @@ void launch_rescore(Bound64 bound, ReplayInputs in, const uint32_t* candidates,
                     uint32_t* done, Result* results, double* exact_distances,
                     uint32_t* replay_count, cudaStream_t stream);
 
+// The FP32 re-score of the precision strategies: each candidate's binary32
+// distance from the original rows (bound: make_bound(rescore_depth, k, 2)),
+// certified per query; uncertified queries are settled by the emulated replay
+// (in.emulated must be set). cand_dist: batch x k floats; done as above.
+void launch_rescore32(Bound bound, ReplayInputs in, const uint32_t* candidates,
+                      uint32_t k, uint32_t batch, uint32_t rows, float* cand_dist,
+                      uint32_t* done, Result* results, double* exact_distances,
+                      uint32_t* replay_count, cudaStream_t stream);
 // ---- hierarchical index (projection)
 // Binary64 projected rows reps[row][j] = sum_i double(sampled[row][i]) *
 // projection[j][i] in i order; `bad` is set when a result is not finite.
