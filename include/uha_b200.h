@@ -411,6 +411,20 @@ uha_status uha_batch_create(const uha_index* const* indexes,
                             const uint64_t* query_counts,
                             const uha_strategy* strategies, uint64_t count,
                             int autotune, uha_batch** out);
+/* The same batch run as ONE persistent, cooperative kernel launch (captured
+ * in the batch's graph with the result copies): every CTA drains, stage by
+ * stage, a work list of units from all pairs (gather, projection, L2 tile
+ * scan or median sample / count / survivor passes, certified argmin with
+ * replay, reported distances), separated by grid-wide barriers whose waits
+ * give up after about two seconds (the run then fails with
+ * UHA_RUNTIME_ERROR). Each unit runs the device code of the standalone
+ * kernel it replaces, so each pair's answers equal a uha_query of the same
+ * queries. Serves hierarchical indexes with the certified direct strategy
+ * (projection dimension up to 256; L2 hierarchies with more than 8 queries);
+ * other pairs fail with UHA_INVALID_ARGUMENT. No reference counterpart. */
+uha_status uha_batch_create_persistent(const uha_index* const* indexes,
+                                       const uint64_t* query_counts, uint64_t count,
+                                       int autotune, uha_batch** out);
 /* Device buffer (query_counts[pair] x dimension floats) that the graph reads
  * pair `pair`'s queries from; NULL for an unknown pair. */
 float* uha_batch_query_buffer(uha_batch* batch, uint64_t pair);

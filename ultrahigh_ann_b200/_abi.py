@@ -165,6 +165,7 @@ SIGNATURES = {
     "uha_workspace_set_replay": (c_int, [c_void_p, c_int]),
     "uha_workspace_autotune": (c_int, [c_void_p, c_uint64, c_int, POINTER(TuneReport)]),
     "uha_batch_create": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_int, _H]),
+    "uha_batch_create_persistent": (c_int, [c_void_p, c_void_p, c_uint64, c_int, _H]),
     "uha_batch_query_buffer": (c_void_p, [c_void_p, c_uint64]),
     "uha_batch_run": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
     "uha_batch_stats_get": (c_int, [c_void_p, POINTER(BatchStats)]),

@@ -906,9 +906,13 @@ class QueryBatch:
     """Many (index, query count, strategy) pairs on one device answered by one
     CUDA graph launch (uha_batch_*): each pair's pipeline is captured on its
     own graph branch; with autotune each pair's scan shape is tuned first.
-    Each pair's answers equal a query_batch of the same queries."""
+    With persistent=True (hierarchical indexes, direct strategy) the graph
+    holds one cooperative launch of the persistent batch kernel instead, which
+    drains every pair's stages from one work list
+    (uha_batch_create_persistent). Each pair's answers equal a query_batch of
+    the same queries."""
 
-    def __init__(self, pairs, autotune: bool = True):
+    def __init__(self, pairs, autotune: bool = True, persistent: bool = False):
         pairs = list(pairs)
         if not pairs:
             raise InvalidArgument("a batch needs at least one index")
@@ -920,8 +924,16 @@ class QueryBatch:
         counts = (ctypes.c_uint64 * n)(*self._counts)
         strat = (ctypes.c_int * n)(*strategies)
         handle = ctypes.c_void_p()
-        _check(_abi.load().uha_batch_create(handles, counts, strat, ctypes.c_uint64(n),
-                                            int(bool(autotune)), ctypes.byref(handle)))
+        if persistent:
+            if any(s != int(QueryStrategy.direct) for s in strategies):
+                raise InvalidArgument("the persistent batch runs the direct strategy")
+            _check(_abi.load().uha_batch_create_persistent(
+                handles, counts, ctypes.c_uint64(n), int(bool(autotune)),
+                ctypes.byref(handle)))
+        else:
+            _check(_abi.load().uha_batch_create(handles, counts, strat, ctypes.c_uint64(n),
+                                                int(bool(autotune)), ctypes.byref(handle)))
+        self.persistent = bool(persistent)
         self._handle = handle
         self.total = sum(self._counts)
 

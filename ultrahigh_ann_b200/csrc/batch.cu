@@ -13,7 +13,9 @@
 // into one CUDA graph: each pair's preparation, projection, scan, argmin /
 // re-score and result copies run on their own branch, forked from and joined
 // into one stream, so small indexes overlap on the device and the host issues
-// one launch per run.
+// one launch per run. uha_batch_create_persistent captures instead one
+// cooperative launch of the persistent batch kernel (stage_bodies.h) that
+// drains every pair's stages from one work list, plus the result copies.
 #include "common.h"
 #include "engine_internal.h"
 #include "index_types.h"
@@ -244,6 +246,14 @@ struct uha_batch {
     cudaEvent_t start = nullptr;
     cudaEvent_t stop = nullptr;
     uha_batch_stats last{};
+    // persistent form
+    bool persistent = false;
+    uha::DeviceBuffer<uha::PersistentPair> d_pairs;
+    uha::DeviceBuffer<uha::PersistentSegment> d_segments;
+    uha::DeviceBuffer<unsigned int> barrier;  // [0] arrivals [1] generation [2] status
+    uha::PinnedBuffer<int> host_status;
+    uha::PersistentPlan plan{};
+    uint32_t grid = 0;
 
     ~uha_batch()
     {
@@ -306,12 +316,56 @@ uint64_t enqueue_pair(uha_batch::Pair& p)
     return launches;
 }
 
-}  // namespace
+// Builds the persistent plan of a batch whose pairs are sized (after their
+// warm-up runs) and uploads it; fails when a pair has no persistent form.
+void build_persistent(uha_batch* batch)
+{
+    std::vector<uha::PersistentPair> pairs;
+    for (uha_batch::Pair& p : batch->pairs) {
+        if (p.trivial) {
+            continue;
+        }
+        uha::PersistentPair d{};
+        require(p.strategy == UHA_DIRECT && persistent_pair(p.index, p.ws, p.count, &d),
+                UHA_INVALID_ARGUMENT,
+                "the persistent batch serves hierarchical indexes with the certified "
+                "direct strategy, projection dimensions up to 256 and more than 8 "
+                "queries per L2 hierarchy");
+        pairs.push_back(d);
+    }
+    require(!pairs.empty(), UHA_INVALID_ARGUMENT, "the persistent batch has no work");
+    const uint32_t count = static_cast<uint32_t>(pairs.size());
+    std::vector<uha::PersistentSegment> segments(uha::persistent_segment_capacity(count));
+    uint32_t used = 0;
+    uha::plan_persistent_batch(pairs.data(), count, segments.data(), &used, &batch->plan);
+    batch->d_pairs.allocate(count);
+    batch->d_segments.allocate(used);
+    batch->barrier.allocate(3);
+    batch->host_status.allocate(1);
+    batch->host_status.get()[0] = 0;
+    check_cuda(cudaMemcpyAsync(batch->d_pairs.get(), pairs.data(), batch->d_pairs.bytes(),
+                               cudaMemcpyHostToDevice, batch->stream),
+               "cannot upload the persistent batch");
+    check_cuda(cudaMemcpyAsync(batch->d_segments.get(), segments.data(),
+                               used * sizeof(uha::PersistentSegment), cudaMemcpyHostToDevice,
+                               batch->stream),
+               "cannot upload the persistent batch");
+    check_cuda(cudaMemsetAsync(batch->barrier.get(), 0, batch->barrier.bytes(), batch->stream),
+               "cannot clear the persistent batch barrier");
+    check_cuda(cudaStreamSynchronize(batch->stream), "cannot upload the persistent batch");
+    batch->plan.pairs = batch->d_pairs.get();
+    batch->plan.segments = batch->d_segments.get();
+    batch->plan.barrier = batch->barrier.get();
+    batch->plan.status = reinterpret_cast<int*>(batch->barrier.get() + 2);
+    batch->grid = uha::persistent_grid(batch->plan.smem_bytes);
+    require(batch->grid != 0, UHA_RUNTIME_ERROR,
+            "the persistent batch kernel cannot be resident with its shared memory");
+    batch->persistent = true;
+}
 
-extern "C" uha_status uha_batch_create(const uha_index* const* indexes,
-                                       const uint64_t* query_counts,
-                                       const uha_strategy* strategies, uint64_t count,
-                                       int autotune_shapes, uha_batch** out)
+uha_status create_batch(const uha_index* const* indexes, const uint64_t* query_counts,
+                        const uha_strategy* strategies, uint64_t count, int autotune_shapes,
+                        bool persistent, uha_batch** out)
 {
     return guarded([&] {
         require(out != nullptr, UHA_INVALID_ARGUMENT, "output must not be null");
@@ -369,14 +423,43 @@ extern "C" uha_status uha_batch_create(const uha_index* const* indexes,
                 check_cuda(cudaStreamSynchronize(ws->stream), "CUDA batch warm-up failed");
             }
         }
-        // capture: fork every pair from the batch stream, join back
+        if (persistent) {
+            build_persistent(batch.get());
+        }
+        // capture: fork every pair from the batch stream, join back (or the
+        // persistent kernel and the result copies)
         check_cuda(cudaStreamBeginCapture(batch->stream, cudaStreamCaptureModeThreadLocal),
                    "cannot capture the batch");
         uint64_t launches = 0;
         try {
+            if (batch->persistent) {
+                uha::launch_persistent_batch(batch->plan, batch->grid, batch->stream);
+                launches = 1;
+                for (uha_batch::Pair& p : batch->pairs) {
+                    if (p.trivial) {
+                        continue;
+                    }
+                    uha_workspace* ws = p.ws;
+                    check_cuda(cudaMemcpyAsync(ws->host_results.get(), ws->call_results.get(),
+                                               p.count * sizeof(uha::Result),
+                                               cudaMemcpyDeviceToHost, batch->stream),
+                               "cannot copy query results from the CUDA device");
+                    check_cuda(cudaMemcpyAsync(ws->host_exact.get(), ws->call_exact.get(),
+                                               p.count * sizeof(double), cudaMemcpyDeviceToHost,
+                                               batch->stream),
+                               "cannot copy query distances from the CUDA device");
+                    check_cuda(cudaMemcpyAsync(ws->host_counters.get(), ws->counters.get(),
+                                               ws->counters.bytes(), cudaMemcpyDeviceToHost,
+                                               batch->stream),
+                               "cannot copy query counters from the CUDA device");
+                }
+                check_cuda(cudaMemcpyAsync(batch->host_status.get(), batch->plan.status,
+                                           sizeof(int), cudaMemcpyDeviceToHost, batch->stream),
+                           "cannot copy the persistent batch status");
+            }
             check_cuda(cudaEventRecord(batch->fork, batch->stream), "event");
             for (uha_batch::Pair& p : batch->pairs) {
-                if (p.trivial) {
+                if (p.trivial || batch->persistent) {
                     continue;
                 }
                 check_cuda(cudaStreamWaitEvent(p.ws->stream, batch->fork, 0), "event");
@@ -401,6 +484,25 @@ extern "C" uha_status uha_batch_create(const uha_index* const* indexes,
         batch->launches = launches;
         *out = batch.release();
     });
+}
+
+}  // namespace
+
+extern "C" uha_status uha_batch_create(const uha_index* const* indexes,
+                                       const uint64_t* query_counts,
+                                       const uha_strategy* strategies, uint64_t count,
+                                       int autotune_shapes, uha_batch** out)
+{
+    return create_batch(indexes, query_counts, strategies, count, autotune_shapes, false,
+                        out);
+}
+
+extern "C" uha_status uha_batch_create_persistent(const uha_index* const* indexes,
+                                                  const uint64_t* query_counts,
+                                                  uint64_t count, int autotune_shapes,
+                                                  uha_batch** out)
+{
+    return create_batch(indexes, query_counts, nullptr, count, autotune_shapes, true, out);
 }
 
 extern "C" float* uha_batch_query_buffer(uha_batch* batch, uint64_t pair)
@@ -439,6 +541,15 @@ extern "C" uha_status uha_batch_run(uha_batch* batch, const float* const* querie
         check_cuda(cudaGraphLaunch(batch->exec, batch->stream), "cannot launch the batch graph");
         check_cuda(cudaEventRecord(batch->stop, batch->stream), "event");
         check_cuda(cudaStreamSynchronize(batch->stream), "CUDA batch failed");
+        if (batch->persistent && batch->host_status.get()[0] != 0) {
+            // a grid barrier wait ran out: reset the barrier for the next run
+            check_cuda(cudaMemsetAsync(batch->barrier.get(), 0, batch->barrier.bytes(),
+                                       batch->stream),
+                       "cannot reset the persistent batch barrier");
+            check_cuda(cudaStreamSynchronize(batch->stream), "CUDA batch failed");
+            batch->host_status.get()[0] = 0;
+            fail(UHA_RUNTIME_ERROR, "persistent batch barrier wait timed out");
+        }
         float ms = 0.f;
         check_cuda(cudaEventElapsedTime(&ms, batch->start, batch->stop), "event");
         uha_batch_stats st{};

@@ -15,7 +15,10 @@
 // needs no host decision between its kernels.
 #include "common.h"
 #include "exact64.h"
+#include "hier_body.cuh"
 #include "kernels.h"
+#include "stage_bodies.h"
+#include "tile_body.cuh"
 
 #include <algorithm>
 #include <cfloat>
@@ -777,16 +780,19 @@ __device__ __forceinline__ void scan_rows(const PartialView& view, const Bound& 
 // the lexicographic minimum of (distance, row). exact_distances[q] is the
 // replayed distance, or NaN when the query was certified.
 template <bool kEmulated>
-__global__ void __launch_bounds__(kFinalizeThreads)
-    argmin_kernel(PartialView view, Bound bound, ReplayInputs in, Result* results,
-                  double* exact_distances, Summary* block_summaries,
-                  uint32_t* done, uint32_t* replay_count, uint32_t span)
+__device__ __forceinline__ void argmin_block(const PartialView& view, const Bound& bound,
+                                             const ReplayInputs& in, Result* results,
+                                             double* exact_distances,
+                                             Summary* block_summaries, uint32_t* done,
+                                             uint32_t* replay_count, uint32_t span,
+                                             uint32_t bx, uint32_t by, uint32_t gx,
+                                             double* projected_query)
 {
-    const uint32_t q = blockIdx.y;
-    const uint32_t blocks = gridDim.x;
+    const uint32_t q = by;
+    const uint32_t blocks = gx;
     const float inf = __int_as_float(0x7f800000);
     Summary s{inf, inf, inf, 0xffffffffu, inf};
-    const uint32_t first_row = blockIdx.x * span;
+    const uint32_t first_row = bx * span;
     const uint32_t end_row = min(view.rows, first_row + span);
     // Plain and projected_l2 bounds are monotone in d, so a thread keeps only
     // its smallest distance (lowest row on ties) and its second smallest; the
@@ -817,7 +823,7 @@ __global__ void __launch_bounds__(kFinalizeThreads)
     __shared__ bool is_last;
     if (blocks > 1) {
         if (threadIdx.x == 0) {
-            block_summaries[static_cast<uint64_t>(q) * blocks + blockIdx.x] = s;
+            block_summaries[static_cast<uint64_t>(q) * blocks + bx] = s;
             __threadfence();
             is_last = atomicAdd(done + q, 1u) == blocks - 1;
         }
@@ -877,7 +883,6 @@ __global__ void __launch_bounds__(kFinalizeThreads)
                              exact_distances + q);
         return;
     }
-    extern __shared__ double projected_query[];
     if (projected_op(in.op)) {
         project_query64(in, qrow, projected_query);
         __syncthreads();
@@ -934,6 +939,18 @@ __global__ void __launch_bounds__(kFinalizeThreads)
     }
 }
 
+template <bool kEmulated>
+__global__ void __launch_bounds__(kFinalizeThreads)
+    argmin_kernel(PartialView view, Bound bound, ReplayInputs in, Result* results,
+                  double* exact_distances, Summary* block_summaries,
+                  uint32_t* done, uint32_t* replay_count, uint32_t span)
+{
+    extern __shared__ double argmin_projected_query[];
+    argmin_block<kEmulated>(view, bound, in, results, exact_distances, block_summaries, done,
+                            replay_count, span, blockIdx.x, blockIdx.y, gridDim.x,
+                            argmin_projected_query);
+}
+
 // The reference binary64 distance of each query's selected row (hierarchical
 // indexes: their binary32 projected distances can differ from the reference's
 // by more than 1e-5 relative when rows are close, so the reported distance is
@@ -975,16 +992,16 @@ __global__ void __launch_bounds__(kFinalizeThreads)
 // keeps the reference order), then one warp per such query replays its row.
 constexpr int kRefineGroup = 8;
 
-__global__ void __launch_bounds__(kFinalizeThreads)
-    refine_group_kernel(ReplayInputs in, Bound bound, const Result* results,
-                        double* exact_distances, uint32_t batch)
+__device__ __forceinline__ void refine_group_block(const ReplayInputs& in, const Bound& bound,
+                                                   const Result* results,
+                                                   double* exact_distances, uint32_t batch,
+                                                   uint32_t bx, unsigned char* refine_smem)
 {
-    extern __shared__ unsigned char refine_smem[];
     double* y = reinterpret_cast<double*>(refine_smem);           // group x proj_dim
     float* x = reinterpret_cast<float*>(y + kRefineGroup * in.proj_dim);  // group x dim
     __shared__ uint32_t members[kRefineGroup];
     __shared__ int count;
-    const uint32_t q0 = blockIdx.x * kRefineGroup;
+    const uint32_t q0 = bx * kRefineGroup;
     if (threadIdx.x == 0) {
         int c = 0;
         for (int g = 0; g < kRefineGroup; ++g) {
@@ -1052,6 +1069,15 @@ __global__ void __launch_bounds__(kFinalizeThreads)
             exact_distances[q] = d;
         }
     }
+}
+
+__global__ void __launch_bounds__(kFinalizeThreads)
+    refine_group_kernel(ReplayInputs in, Bound bound, const Result* results,
+                        double* exact_distances, uint32_t batch)
+{
+    extern __shared__ unsigned char refine_group_smem[];
+    refine_group_block(in, bound, results, exact_distances, batch, blockIdx.x,
+                       refine_group_smem);
 }
 
 // ------------------------------------------------ small indexes, one launch
@@ -1832,6 +1858,233 @@ __global__ void __launch_bounds__(kFinalizeThreads)
                          results + q, exact_distances + q);
 }
 
+// ------------------------------------------ the persistent multi-index batch
+
+enum PersistentKind : uint32_t {
+    kUnitClear = 0,
+    kUnitGather,
+    kUnitProject,
+    kUnitFinishErr,
+    kUnitTile,
+    kUnitSample,
+    kUnitCount,
+    kUnitSurvivor,
+    kUnitArgmin,
+    kUnitRefine,
+};
+
+// about 2^23 polls of ~256 ns: seconds, far above any stage of a batch
+constexpr uint32_t kBarrierSpins = 1u << 23;
+
+// Grid-wide barrier of the cooperative persistent kernel (every CTA is
+// resident): thread 0 reads the generation, arrives, and the last arrival
+// resets the count and advances the generation; the others poll it with a
+// bounded wait. False (and the status set) when the wait ran out.
+__device__ bool persistent_barrier(unsigned int* bar, int* status)
+{
+    __shared__ int passed;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned int* generation = bar + 1;
+        const unsigned int gen = *generation;
+        __threadfence();
+        const unsigned int arrived = atomicAdd(bar, 1u);
+        if (arrived == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+            passed = 1;
+        } else {
+            passed = 0;
+            for (uint32_t i = 0; i < kBarrierSpins; ++i) {
+                if (*generation != gen) {
+                    passed = 1;
+                    break;
+                }
+                __nanosleep(256);
+            }
+            if (!passed) {
+                atomicOr(status, 1);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return passed != 0;
+}
+
+template <int PER_LANE>
+__device__ __forceinline__ void persistent_sample(const MedianArgs& a, uint32_t u,
+                                                  uint32_t units)
+{
+    hierbody::median_sample_loop<PER_LANE>(a.rows, a.row_count, a.padded_p, a.p, a.queries,
+                                           a.batch, a.samples, a.partials, a.min_bits, u,
+                                           units, kFinalizeThreads);
+}
+
+template <int PER_LANE>
+__device__ __forceinline__ void persistent_survivor(const MedianArgs& a, uint32_t u,
+                                                    uint32_t units)
+{
+    hierbody::median_survivor_loop<PER_LANE>(a.rows, a.row_count, a.padded_p, a.p, a.queries,
+                                             a.batch, a.coord_err, a.partials, a.pair_err, u,
+                                             units, kFinalizeThreads);
+}
+
+template <int Q>
+__device__ __forceinline__ void persistent_count(const MedianArgs& a, uint32_t b,
+                                                 uint32_t gx, float* smem, uint32_t half)
+{
+    hierbody::median_count_block<Q>(a.rows_t, a.r_pitch, a.row_count, a.padded_p, a.p,
+                                    a.queries, a.batch, 0, a.min_bits, a.query_err,
+                                    a.row_err_max, a.rel, a.abs_err, a.partials, b % gx,
+                                    b / gx, reinterpret_cast<float4*>(smem),
+                                    threadIdx.x % hierbody::kCountRows, 1 + half);
+}
+
+// Unit u (of `units`) of one kind for one pair: one block of the stage kernel
+// the standalone path launches for it.
+__device__ void persistent_unit(const PersistentPair& d, uint32_t kind, uint32_t u,
+                                uint32_t units, unsigned char* smem)
+{
+    int* error_flag = reinterpret_cast<int*>(d.counters + 1);
+    switch (kind) {
+    case kUnitClear: {
+        const uint64_t stride = static_cast<uint64_t>(units) * kFinalizeThreads;
+        for (uint64_t i = u * static_cast<uint64_t>(kFinalizeThreads) + threadIdx.x;
+             i < d.batch; i += stride) {
+            d.query_err[i] = 0.f;
+            if (!d.l2) {
+                d.median.min_bits[i] = 0xffffffffu;
+            }
+        }
+        if (u == 0) {
+            for (uint32_t i = threadIdx.x; i < d.counter_words; i += kFinalizeThreads) {
+                d.counters[i] = 0;
+            }
+        }
+        break;
+    }
+    case kUnitGather:
+        hierbody::prepare_sampled_loop(d.raw_queries, d.batch, d.dim, d.columns, nullptr,
+                                       d.sample_size, d.prepared, d.padded_sample, error_flag,
+                                       u, units, kFinalizeThreads);
+        break;
+    case kUnitProject:
+        hierbody::project_queries_block(
+            d.prepared, d.batch, d.padded_sample, d.sample_size, d.projection32, d.proj_dim,
+            d.projected, d.padded_p, d.query_err, d.l2 ? nullptr : d.coord_err, d.err_per_abs,
+            d.l2 != 0, error_flag, u % d.proj_gx, u / d.proj_gx,
+            *reinterpret_cast<hierbody::ProjShared*>(smem));
+        break;
+    case kUnitFinishErr:
+        hierbody::finish_query_err_loop(d.query_err, d.batch, true, u, units, kFinalizeThreads);
+        break;
+    case kUnitTile: {
+        const uint32_t plane = d.tile_gx * d.tile_gy;
+        tilebody::tile_scan_wide_tile<static_cast<int>(ScanOp::l2)>(
+            d.scan_rows, d.rows, static_cast<uint32_t>(d.padded_p), nullptr, d.projected,
+            d.batch, d.k_per_split, d.partials, u % d.tile_gx, (u % plane) / d.tile_gx,
+            u / plane, smem);
+        break;
+    }
+    case kUnitSample: {
+        const MedianArgs a = d.median;
+        if (a.p <= 32) {
+            persistent_sample<1>(a, u, units);
+        } else if (a.p <= 64) {
+            persistent_sample<2>(a, u, units);
+        } else if (a.p <= 128) {
+            persistent_sample<4>(a, u, units);
+        } else {
+            persistent_sample<8>(a, u, units);
+        }
+        break;
+    }
+    case kUnitCount: {
+        // two count blocks per unit, one per half of the CTA (own barrier and
+        // shared memory)
+        const MedianArgs a = d.median;
+        const uint32_t half = threadIdx.x / hierbody::kCountRows;
+        const uint32_t b = 2 * u + half;
+        if (b < d.count_gx * d.count_gy) {
+            const int q = a.batch >= 8 ? 8 : a.batch >= 4 ? 4 : a.batch >= 2 ? 2 : 1;
+            float* half_smem = reinterpret_cast<float*>(smem) + half * q * a.padded_p;
+            if (q == 8) {
+                persistent_count<8>(a, b, d.count_gx, half_smem, half);
+            } else if (q == 4) {
+                persistent_count<4>(a, b, d.count_gx, half_smem, half);
+            } else if (q == 2) {
+                persistent_count<2>(a, b, d.count_gx, half_smem, half);
+            } else {
+                persistent_count<1>(a, b, d.count_gx, half_smem, half);
+            }
+        }
+        break;
+    }
+    case kUnitSurvivor: {
+        const MedianArgs a = d.median;
+        if (a.p <= 32) {
+            persistent_survivor<1>(a, u, units);
+        } else if (a.p <= 64) {
+            persistent_survivor<2>(a, u, units);
+        } else if (a.p <= 128) {
+            persistent_survivor<4>(a, u, units);
+        } else {
+            persistent_survivor<8>(a, u, units);
+        }
+        break;
+    }
+    case kUnitArgmin: {
+        const PartialView view = d.view;
+        const Bound bound = d.bound;
+        const ReplayInputs in = d.replay;
+        argmin_block<false>(view, bound, in, d.results, d.exact_distances,
+                            static_cast<Summary*>(d.summaries), d.done, d.counters,
+                            d.argmin_span, u % d.argmin_gx, u / d.argmin_gx, d.argmin_gx,
+                            reinterpret_cast<double*>(smem));
+        break;
+    }
+    case kUnitRefine: {
+        const Bound bound = d.bound;
+        const ReplayInputs in = d.replay;
+        refine_group_block(in, bound, d.results, d.exact_distances, d.batch, u, smem);
+        break;
+    }
+    default:
+        break;
+    }
+}
+
+// The whole batch in one cooperative launch: stage after stage, every CTA
+// takes units blockIdx.x, blockIdx.x + gridDim.x, ... of the stage's list,
+// then waits at the grid barrier; a barrier that ran out ends the kernel.
+__global__ void __launch_bounds__(kFinalizeThreads, 2)
+    persistent_batch_kernel(PersistentPlan plan)
+{
+    extern __shared__ __align__(16) unsigned char persistent_smem[];
+    for (int stage = 0; stage < kPersistentStages; ++stage) {
+        const uint32_t units = plan.stage_units[stage];
+        const uint32_t seg_end = plan.stage_begin[stage + 1];
+        uint32_t seg = plan.stage_begin[stage];
+        for (uint32_t u = blockIdx.x; u < units; u += gridDim.x) {
+            while (seg + 1 < seg_end && plan.segments[seg + 1].first <= u) {
+                ++seg;
+            }
+            const PersistentSegment sg = plan.segments[seg];
+            persistent_unit(plan.pairs[sg.pair], sg.kind, u - sg.first, sg.units,
+                            persistent_smem);
+            __syncthreads();
+        }
+        if (stage + 1 < kPersistentStages) {
+            if (!persistent_barrier(plan.barrier, plan.status) ||
+                *static_cast<volatile int*>(plan.status) != 0) {
+                return;
+            }
+        }
+    }
+}
+
 // Raises a kernel's dynamic shared-memory limit when a launch needs more than
 // 48 KB and more than it was configured for on this device (a call that needs
 // no more makes no runtime call, so captured launches after a warm-up make
@@ -2153,6 +2406,176 @@ void launch_finalize_gemm(PartialView view, const float* row_norms,
     finalize_gemm_kernel<<<view.batch, kFinalizeThreads, 0, stream>>>(
         view, row_norms, query_norms, results);
     check_cuda(cudaGetLastError(), "cannot launch gemm finalize kernel");
+}
+
+// ------------------------------------ shapes for the persistent batch kernel
+
+void argmin_grid(uint32_t rows, uint32_t batch, uint32_t* gx, uint32_t* span)
+{
+    // launch_argmin's shape
+    const uint32_t min_span_blocks = (rows + kFinalizeThreads - 1) / kFinalizeThreads;
+    const uint64_t cap = 148ull * 32;
+    const uint64_t want = static_cast<uint64_t>(min_span_blocks) * batch;
+    const uint32_t factor = want > cap ? static_cast<uint32_t>((want + cap - 1) / cap) : 1u;
+    *span = kFinalizeThreads * factor;
+    *gx = (rows + *span - 1) / *span;
+}
+
+void argmin_scratch(void* scratch, uint64_t capacity, uint32_t rows, void** summaries,
+                    uint32_t** done)
+{
+    const FinalizeScratch fs = finalize_scratch(scratch, static_cast<uint32_t>(capacity), rows);
+    *summaries = fs.summaries;
+    *done = fs.done;
+}
+
+uint64_t replay_smem_bytes(const ReplayInputs& in)
+{
+    return replay_smem(in);
+}
+
+uint64_t refine_group_smem_bytes(const ReplayInputs& in)
+{
+    return kRefineGroup * (in.proj_dim * sizeof(double) + in.dim * sizeof(float));
+}
+
+uint32_t refine_group_blocks(uint32_t batch)
+{
+    return (batch + kRefineGroup - 1) / kRefineGroup;
+}
+
+// ------------------------------------------ the persistent batch (host side)
+
+uint32_t persistent_segment_capacity(uint32_t count)
+{
+    // at most two unit kinds per pair in any stage
+    return 2 * count * kPersistentStages + 1;
+}
+
+void plan_persistent_batch(const PersistentPair* pairs, uint32_t count,
+                           PersistentSegment* segments, uint32_t* segment_count,
+                           PersistentPlan* plan)
+{
+    uint32_t n = 0;
+    uint64_t smem = 0;
+    auto add = [&](int stage, uint32_t pair, uint32_t kind, uint64_t units) {
+        if (units == 0) {
+            return;
+        }
+        const uint64_t total = static_cast<uint64_t>(plan->stage_units[stage]) + units;
+        if (total > 0xffffffffull) {
+            fail(UHA_LENGTH_ERROR, "persistent batch stage exceeds 2^32 units");
+        }
+        PersistentSegment sg{};
+        sg.pair = pair;
+        sg.kind = kind;
+        sg.units = static_cast<uint32_t>(units);
+        sg.first = plan->stage_units[stage];
+        plan->stage_units[stage] = static_cast<uint32_t>(total);
+        segments[n++] = sg;
+    };
+    for (int stage = 0; stage < kPersistentStages; ++stage) {
+        plan->stage_units[stage] = 0;
+    }
+    for (int stage = 0; stage < kPersistentStages; ++stage) {
+        plan->stage_begin[stage] = n;
+        for (uint32_t i = 0; i < count; ++i) {
+            const PersistentPair& d = pairs[i];
+            const uint64_t per_query = (d.batch + kFinalizeThreads - 1) / kFinalizeThreads;
+            switch (stage) {
+            case 0:
+                add(0, i, kUnitClear, std::max<uint64_t>(1, per_query));
+                break;
+            case 1: {
+                const uint64_t total = d.batch * d.padded_sample;
+                const uint64_t blocks = (total + kFinalizeThreads - 1) / kFinalizeThreads;
+                add(1, i, kUnitGather,
+                    std::max<uint64_t>(1, std::min<uint64_t>(blocks, 148ull * 64)));
+                break;
+            }
+            case 2:
+                add(2, i, kUnitProject, static_cast<uint64_t>(d.proj_gx) * d.proj_gy);
+                smem = std::max<uint64_t>(smem, project_queries_smem_bytes());
+                break;
+            case 3:
+                if (d.l2) {
+                    add(3, i, kUnitFinishErr, std::max<uint64_t>(1, per_query));
+                    add(3, i, kUnitTile,
+                        static_cast<uint64_t>(d.tile_gx) * d.tile_gy * d.tile_gz);
+                    smem = std::max<uint64_t>(smem, tile_scan_smem_bytes());
+                } else {
+                    add(3, i, kUnitSample, d.sample_blocks);
+                }
+                break;
+            case 4:
+                if (!d.l2) {
+                    add(4, i, kUnitCount,
+                        (static_cast<uint64_t>(d.count_gx) * d.count_gy + 1) / 2);
+                    smem = std::max<uint64_t>(
+                        smem, 2ull * median_count_queries(d.batch) * d.padded_p * sizeof(float));
+                }
+                break;
+            case 5:
+                if (d.l2) {
+                    add(5, i, kUnitArgmin, static_cast<uint64_t>(d.argmin_gx) * d.batch);
+                    smem = std::max<uint64_t>(smem, replay_smem(d.replay));
+                } else {
+                    add(5, i, kUnitSurvivor, d.survivor_blocks);
+                }
+                break;
+            case 6:
+                if (d.l2) {
+                    add(6, i, kUnitRefine, d.refine_blocks);
+                    smem = std::max<uint64_t>(smem, refine_group_smem_bytes(d.replay));
+                } else {
+                    add(6, i, kUnitArgmin, static_cast<uint64_t>(d.argmin_gx) * d.batch);
+                    smem = std::max<uint64_t>(smem, replay_smem(d.replay));
+                }
+                break;
+            default:
+                if (!d.l2) {
+                    add(7, i, kUnitRefine, d.refine_blocks);
+                    smem = std::max<uint64_t>(smem, refine_group_smem_bytes(d.replay));
+                }
+                break;
+            }
+        }
+    }
+    plan->stage_begin[kPersistentStages] = n;
+    plan->smem_bytes = static_cast<uint32_t>((smem + 15) / 16 * 16);
+    *segment_count = n;
+}
+
+uint32_t persistent_grid(uint32_t smem_bytes)
+{
+    set_dynamic_smem(reinterpret_cast<const void*>(persistent_batch_kernel), smem_bytes);
+    int per_sm = 0;
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                   &per_sm, persistent_batch_kernel, kFinalizeThreads, smem_bytes),
+               "cannot size the persistent batch kernel");
+    int sms = 0;
+    check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, current_device()),
+               "cannot query the SM count");
+    return static_cast<uint32_t>(std::max(0, per_sm) * sms);
+}
+
+void launch_persistent_batch(const PersistentPlan& plan, uint32_t grid, cudaStream_t stream)
+{
+    set_dynamic_smem(reinterpret_cast<const void*>(persistent_batch_kernel), plan.smem_bytes);
+    cudaLaunchConfig_t config{};
+    config.gridDim = dim3(grid);
+    config.blockDim = dim3(kFinalizeThreads);
+    config.dynamicSmemBytes = plan.smem_bytes;
+    config.stream = stream;
+    cudaLaunchAttribute attr[1];
+    // every CTA resident at once: the grid barrier never waits for a CTA
+    // that has not started
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    config.attrs = attr;
+    config.numAttrs = 1;
+    check_cuda(cudaLaunchKernelEx(&config, persistent_batch_kernel, plan),
+               "cannot launch the persistent batch kernel");
 }
 
 }  // namespace uha

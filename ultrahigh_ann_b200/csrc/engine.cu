@@ -11,6 +11,7 @@
 #include "index_types.h"
 #include "engine_internal.h"
 #include "kernels.h"
+#include "stage_bodies.h"
 
 #include <algorithm>
 #include <cmath>
@@ -1031,6 +1032,11 @@ bool fp32_rescore_strategy(uha_strategy s)
     return s == UHA_GEMM_BF16_RERANK_FP32 || s == UHA_GEMM_FP8_RERANK_FP32;
 }
 
+// Median bound of the L1 hierarchy: the binary32 |diff| and midpoint
+// roundings (the binary64 ones are within them).
+const float kMedianRel = std::ldexp(6.0f, -24);
+const float kMedianAbs = std::ldexp(1.0f, -126);
+
 // Replay inputs of the emulated (FP64-free) replay of exact and flat ops.
 void set_emulated(uha::ReplayInputs& in, const uha_index* index)
 {
@@ -1220,6 +1226,147 @@ uha::LowpPlan enqueue_lowp_scores(const uha_index* index, uha_workspace* ws,
 // the norm identity), (the replayed distance of each selected row of a
 // hierarchy). `results` / `exact` receive this batch's answers; flags and the
 // replay count accumulate in ws.counters.
+
+// The certification bound and replay inputs of a scan of `plan` (operation
+// `op`) over `index`, the workspace holding the query-side buffers; shared by
+// the standalone pipeline and the persistent batch.
+void certification_inputs(const uha_index* index, const uha_workspace* ws,
+                          const uha::ScanPlan& plan, uha::ScanOp op, const float* prepared,
+                          uha::Bound* bound_out, uha::ReplayInputs* in_out)
+{
+    const bool hierarchical = index->kind == IndexKind::hierarchical;
+    const bool median = hierarchical && index->metric == UHA_L1;
+    const int term_roundings = op == uha::ScanOp::l1 ? 1 : 2;
+    uha::Bound bound = make_bound(plan.depth, index->scan_dim, term_roundings);
+    uha::ReplayInputs in{};
+    in.rows = index->scan_rows.get();
+    in.queries = prepared;
+    in.dim = index->scan_dim;
+    in.padded_dim = index->padded_dim;
+    in.weights64 = index->weights64.get();
+    if (hierarchical) {
+        bound.row_err = index->row_err.get();
+        bound.query_err = ws->query_err.get();
+        bound.row_err_max = index->row_err_max;
+        if (median) {
+            bound.mode = uha::BoundMode::median;
+            bound.rel = kMedianRel;
+            bound.abs = kMedianAbs;
+            bound.pair_err = ws->pair_err.get();
+            bound.pair_rows = static_cast<uint32_t>(index->rows);
+        } else {
+            bound.mode = uha::BoundMode::projected_l2;
+            const double n64 = static_cast<double>(index->scan_dim) + 3;
+            const double g64 = n64 * std::ldexp(1.0, -53);
+            bound.cpu_rel = std::nextafter(static_cast<float>(1.01 * g64), 1.0f);
+        }
+        in.op = median ? uha::ReplayOp::median_projected : uha::ReplayOp::l2_projected;
+        in.dim = index->sample_size;
+        in.padded_dim = index->padded_sample;
+        in.rows64 = index->rows64.get();
+        in.projection64 = index->projection64.get();
+        in.proj_dim = index->projection_dimension;
+    } else if (index->metric == UHA_L2) {
+        in.op = uha::ReplayOp::l2_sequential;
+    } else if (index->weights64.size() != 0) {
+        in.op = uha::ReplayOp::l1_weighted_sequential;
+    } else {
+        in.op = uha::ReplayOp::l1_grouped4;
+    }
+    if (!hierarchical && ws->emulated_replay) {
+        set_emulated(in, index);
+    }
+    *bound_out = bound;
+    *in_out = in;
+}
+
+bool persistent_pair(const uha_index* index, uha_workspace* ws, uint64_t n,
+                     uha::PersistentPair* d)
+{
+    if (index->kind != IndexKind::hierarchical || index->rows < 2 || index->padded_dim == 0 ||
+        index->projection_dimension > 256 || n == 0 || n > 0xffffffffull ||
+        index->rows > 0xffffffffull) {
+        return false;
+    }
+    const bool median = index->metric == UHA_L1;
+    const TunedPlan* tuned = ws->find_tuned(n, static_cast<int>(UHA_DIRECT));
+    uha::ScanPlan plan = tuned != nullptr && !tuned->lowp
+                             ? tuned->scan
+                             : uha::plan_scan(index->rows, index->padded_dim, n,
+                                              index->sm_count);
+    if (median) {
+        plan.chunks = 1;
+        plan.depth = 0;
+    } else if (plan.kernel != 1) {
+        return false;  // the streaming scan of batches up to 8 is not a unit kind
+    }
+    *d = uha::PersistentPair{};
+    const uint32_t rows = static_cast<uint32_t>(index->rows);
+    const uint32_t b = static_cast<uint32_t>(n);
+    d->l2 = median ? 0 : 1;
+    d->batch = b;
+    d->counters = ws->counters.get();
+    d->counter_words = static_cast<uint32_t>(ws->counters.size());
+    d->raw_queries = ws->raw_queries.get();
+    d->dim = index->dimension;
+    d->columns = index->columns.get();
+    d->sample_size = index->sample_size;
+    d->prepared = ws->prepared.get();
+    d->padded_sample = index->padded_sample;
+    d->projection32 = index->projection32.get();
+    d->proj_dim = index->projection_dimension;
+    d->projected = ws->projected.get();
+    d->padded_p = index->padded_dim;
+    d->query_err = ws->query_err.get();
+    d->coord_err = ws->coord_err.get();
+    d->err_per_abs = projection_error_per_abs(index->sample_size);
+    uha::project_queries_grid(n, index->padded_dim, &d->proj_gx, &d->proj_gy);
+    d->scan_rows = index->scan_rows.get();
+    d->rows = rows;
+    d->partials = ws->partials.get();
+    if (!median) {
+        d->k_per_split = plan.k_per_split;
+        uha::tile_scan_grid(index->rows, n, plan.chunks, &d->tile_gx, &d->tile_gy,
+                            &d->tile_gz);
+    } else {
+        if (ws->median_min.size() < n || ws->pair_err.size() < n * index->rows) {
+            return false;
+        }
+        uha::MedianArgs& m = d->median;
+        m.rows = index->scan_rows.get();
+        m.rows_t = index->scan_rows_t.get();
+        m.r_pitch = static_cast<uint32_t>(index->rows_pitch);
+        m.row_count = rows;
+        m.padded_p = static_cast<uint32_t>(index->padded_dim);
+        m.p = static_cast<uint32_t>(index->projection_dimension);
+        m.queries = ws->projected.get();
+        m.batch = b;
+        m.query_err = ws->query_err.get();
+        m.coord_err = ws->coord_err.get();
+        m.row_err_max = index->row_err_max;
+        m.rel = kMedianRel;
+        m.abs_err = kMedianAbs;
+        m.min_bits = ws->median_min.get();
+        m.partials = ws->partials.get();
+        m.pair_err = ws->pair_err.get();
+        m.samples = uha::median_sample_count(index->rows);
+        d->sample_blocks = uha::median_sample_blocks(rows, b);
+        uha::median_count_grid(rows, b, &d->count_gx, &d->count_gy);
+        d->survivor_blocks = uha::median_survivor_blocks(rows, b);
+    }
+    d->view = uha::PartialView{ws->partials.get(), plan.chunks, b, rows};
+    certification_inputs(index, ws, plan, median ? uha::ScanOp::l1 : uha::ScanOp::l2,
+                         ws->prepared.get(), &d->bound, &d->replay);
+    d->results = ws->call_results.get();
+    d->exact_distances = ws->call_exact.get();
+    uha::argmin_scratch(ws->finalize_scratch.get(), ws->max_batch, rows, &d->summaries,
+                        &d->done);
+    uha::argmin_grid(rows, b, &d->argmin_gx, &d->argmin_span);
+    d->refine_blocks = uha::refine_group_blocks(b);
+    // the grouped reported-distance pass must fit the kernel's shared memory
+    return uha::refine_group_smem_bytes(d->replay) <= 96 * 1024 &&
+           ws->partials.size() >= uint64_t(plan.chunks) * n * index->rows;
+}
 
 uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
                        uha::Result* results, double* exact, bool time_scan,
@@ -1412,9 +1559,6 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
     if (time_scan) {
         check_cuda(cudaEventRecord(scan_start, stream), "event");
     }
-    // median bound: binary32 |diff| and midpoint roundings; the binary64 ones
-    const float median_rel = std::ldexp(6.0f, -24);
-    const float median_abs = std::ldexp(1.0f, -126);
     if (median) {
         if (ws->median_min.size() < n) {
             check_cuda(cudaStreamSynchronize(stream), "CUDA query failed");
@@ -1424,7 +1568,7 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
                                 index->rows_pitch, index->rows, index->padded_dim,
                                 index->projection_dimension, scan_queries, n,
                                 ws->query_err.get(), ws->coord_err.get(),
-                                index->row_err_max, median_rel, median_abs,
+                                index->row_err_max, kMedianRel, kMedianAbs,
                                 ws->median_min.get(), ws->partials.get(),
                                 ws->pair_err.get(), stream);
     } else {
@@ -1457,46 +1601,9 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
         return launches + 2;
     }
 
-    const int term_roundings = op == uha::ScanOp::l1 ? 1 : 2;
-    uha::Bound bound = make_bound(plan.depth, index->scan_dim, term_roundings);
+    uha::Bound bound{};
     uha::ReplayInputs in{};
-    in.rows = index->scan_rows.get();
-    in.queries = prepared;
-    in.dim = index->scan_dim;
-    in.padded_dim = index->padded_dim;
-    in.weights64 = index->weights64.get();
-    if (hierarchical) {
-        bound.row_err = index->row_err.get();
-        bound.query_err = ws->query_err.get();
-        bound.row_err_max = index->row_err_max;
-        if (median) {
-            bound.mode = uha::BoundMode::median;
-            bound.rel = median_rel;
-            bound.abs = median_abs;
-            bound.pair_err = ws->pair_err.get();
-            bound.pair_rows = static_cast<uint32_t>(index->rows);
-        } else {
-            bound.mode = uha::BoundMode::projected_l2;
-            const double n64 = static_cast<double>(index->scan_dim) + 3;
-            const double g64 = n64 * std::ldexp(1.0, -53);
-            bound.cpu_rel = std::nextafter(static_cast<float>(1.01 * g64), 1.0f);
-        }
-        in.op = median ? uha::ReplayOp::median_projected : uha::ReplayOp::l2_projected;
-        in.dim = index->sample_size;
-        in.padded_dim = index->padded_sample;
-        in.rows64 = index->rows64.get();
-        in.projection64 = index->projection64.get();
-        in.proj_dim = index->projection_dimension;
-    } else if (index->metric == UHA_L2) {
-        in.op = uha::ReplayOp::l2_sequential;
-    } else if (index->weights64.size() != 0) {
-        in.op = uha::ReplayOp::l1_weighted_sequential;
-    } else {
-        in.op = uha::ReplayOp::l1_grouped4;
-    }
-    if (!hierarchical && ws->emulated_replay) {
-        set_emulated(in, index);
-    }
+    certification_inputs(index, ws, plan, op, prepared, &bound, &in);
     uha::launch_argmin(view, bound, in, results, exact, ws->finalize_scratch.get(),
                        ws->max_batch, replay_count, stream);
     ++launches;

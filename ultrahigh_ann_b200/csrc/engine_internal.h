@@ -6,6 +6,7 @@
 #include "common.h"
 #include "index_types.h"
 #include "kernels.h"
+#include "stage_bodies.h"
 
 namespace uha_engine {
 
@@ -46,6 +47,14 @@ struct BatchContext {
 uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
                        uha::Result* results, double* exact, bool time_scan,
                        cudaEvent_t scan_start, cudaEvent_t scan_stop);
+
+// The persistent batch's description of one pair (a hierarchical index and n
+// queries in ws->raw_queries, certified direct strategy), read from the
+// index and from workspace buffers that a standalone run of n queries has
+// sized; false when the pair has no persistent form (projection dimension
+// above 256, the streaming scan of batches up to 8, oversized shared memory).
+bool persistent_pair(const uha_index* index, uha_workspace* ws, uint64_t n,
+                     uha::PersistentPair* d);
 
 // Answers of a call whose queries need no device work (row 0, distance 0).
 void fill_trivial(uint64_t n, uint64_t* out_indices, double* out_distances);

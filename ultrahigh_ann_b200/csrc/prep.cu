@@ -15,12 +15,15 @@
 // (l2_coordinate_embedding.cpp:71-79, filter_columns.cpp:10-36) and the row
 // norms of the binary32 norm-identity strategy.
 #include "common.h"
+#include "hier_body.cuh"
 #include "kernels.h"
 
 #include <algorithm>
 
 namespace uha {
 namespace {
+
+using hierbody::prepare_sampled_loop;
 
 constexpr int kThreads = 256;
 
@@ -78,27 +81,8 @@ __global__ void prepare_sampled_kernel(const float* __restrict__ queries,
                                        float* __restrict__ out,
                                        uint64_t padded_dim, int* error_flag)
 {
-    const uint64_t total = batch * padded_dim;
-    for (uint64_t idx = blockIdx.x * static_cast<uint64_t>(blockDim.x) +
-                        threadIdx.x;
-         idx < total; idx += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint64_t b = idx / padded_dim;
-        const uint64_t i = idx - b * padded_dim;
-        float v = 0.f;
-        if (i < sample_size) {
-            v = queries[b * dim + columns[i]];
-            if (!isfinite(v)) {
-                atomicOr(error_flag, 1);
-            }
-            if (scales != nullptr) {
-                v = __fmul_rn(v, scales[i]);
-                if (!isfinite(v)) {
-                    atomicOr(error_flag, 2);
-                }
-            }
-        }
-        out[idx] = v;
-    }
+    prepare_sampled_loop(queries, batch, dim, columns, scales, sample_size, out, padded_dim,
+                         error_flag, blockIdx.x, gridDim.x, blockDim.x);
 }
 
 __global__ void query_norms_kernel(const float* __restrict__ prepared,

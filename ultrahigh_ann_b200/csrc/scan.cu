@@ -15,6 +15,8 @@
 //   may be split across CTAs (split-K) to fill the 148 SMs.
 #include "common.h"
 #include "kernels.h"
+#include "stage_bodies.h"
+#include "tile_body.cuh"
 
 #include <vector>
 
@@ -23,16 +25,13 @@
 namespace uha {
 namespace {
 
+using namespace tilebody;
+
 constexpr uint32_t kStreamChunk = 2048;  // columns per stream chunk
 constexpr uint32_t kStreamWarps = 8;
 constexpr uint32_t kRowsPerWarp = 2;
 constexpr uint32_t kStreamRows = kStreamWarps * kRowsPerWarp;
 
-constexpr uint32_t kTileRows = 128;
-constexpr uint32_t kTileQueries = 64;
-constexpr uint32_t kTileK = 32;
-constexpr uint32_t kTileStride = kTileK + 4;  // padded smem row (floats)
-constexpr uint32_t kTileThreads = 128;
 
 __device__ __forceinline__ float4 load_streaming(const float4* p)
 {
@@ -41,37 +40,6 @@ __device__ __forceinline__ float4 load_streaming(const float4* p)
                  : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
                  : "l"(p));
     return v;
-}
-
-// One accumulation step acc <- acc (+) f(q, r[, w]) per component, in the
-// fixed order x, y, z, w.
-template <int OP>
-__device__ __forceinline__ float accumulate4(float acc, const float4& q,
-                                             const float4& r, const float4& w)
-{
-    if constexpr (OP == static_cast<int>(ScanOp::l2)) {
-        float d;
-        d = q.x - r.x; acc = fmaf(d, d, acc);
-        d = q.y - r.y; acc = fmaf(d, d, acc);
-        d = q.z - r.z; acc = fmaf(d, d, acc);
-        d = q.w - r.w; acc = fmaf(d, d, acc);
-    } else if constexpr (OP == static_cast<int>(ScanOp::l1)) {
-        acc += fabsf(q.x - r.x);
-        acc += fabsf(q.y - r.y);
-        acc += fabsf(q.z - r.z);
-        acc += fabsf(q.w - r.w);
-    } else if constexpr (OP == static_cast<int>(ScanOp::l1_weighted)) {
-        acc = fmaf(fabsf(q.x - r.x), w.x, acc);
-        acc = fmaf(fabsf(q.y - r.y), w.y, acc);
-        acc = fmaf(fabsf(q.z - r.z), w.z, acc);
-        acc = fmaf(fabsf(q.w - r.w), w.w, acc);
-    } else {
-        acc = fmaf(q.x, r.x, acc);
-        acc = fmaf(q.y, r.y, acc);
-        acc = fmaf(q.z, r.z, acc);
-        acc = fmaf(q.w, r.w, acc);
-    }
-    return acc;
 }
 
 template <int NQ, int OP>
@@ -167,32 +135,6 @@ __global__ void __launch_bounds__(kStreamWarps * 32)
         }
     }
 }
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem,
-                                           bool in_range)
-{
-    const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
-    const int src_bytes = in_range ? 16 : 0;
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s),
-                 "l"(gmem), "r"(src_bytes));
-}
-
-__device__ __forceinline__ void cp_async_commit()
-{
-    asm volatile("cp.async.commit_group;");
-}
-
-template <int N>
-__device__ __forceinline__ void cp_async_wait()
-{
-    asm volatile("cp.async.wait_group %0;" ::"n"(N));
-}
-
-struct TileShared {
-    float rows[2][kTileRows][kTileStride];
-    float queries[2][kTileQueries][kTileStride];
-    float weights[2][kTileK];
-};
 
 template <int OP>
 __global__ void __launch_bounds__(kTileThreads)
@@ -380,6 +322,19 @@ void launch_tile_op(dim3 grid, cudaStream_t stream, const float* rows,
 }
 
 }  // namespace
+
+uint64_t tile_scan_smem_bytes()
+{
+    return sizeof(TileShared);
+}
+
+void tile_scan_grid(uint64_t row_count, uint64_t batch, uint32_t splits, uint32_t* gx,
+                    uint32_t* gy, uint32_t* gz)
+{
+    *gx = static_cast<uint32_t>((row_count + kTileRows - 1) / kTileRows);
+    *gy = static_cast<uint32_t>((batch + kTileQueries - 1) / kTileQueries);
+    *gz = splits;
+}
 
 ScanPlan stream_plan(uint64_t padded_dim, int queries_per_pass)
 {
