@@ -327,6 +327,9 @@ def summarize(line: dict) -> dict:
     if hf:
         out["hierarchical_16"] = {"device_ms": hf.get("device_ms"),
                                   "kernels_per_run": hf.get("kernels_per_run"),
+                                  "persistent": {k: (hf.get("persistent") or {}).get(k)
+                                                 for k in ("device_ms", "kernels_per_run",
+                                                           "answers_equal_graph")},
                                   "l2_bf16_device_ms":
                                       (hf.get("l2_bf16_rerank") or {}).get("device_ms")}
     return out
@@ -852,6 +855,31 @@ def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=1
         ms.append(batch.stats()["device_ms"])
     torch.cuda.nvtx.range_pop()
     st = batch.stats()
+    # the same pairs in one persistent cooperative launch per run
+    persistent = None
+    try:
+        t = time.perf_counter()
+        pbatch = uha.QueryBatch([(ix, per_index) for ix in indexes], autotune=True,
+                                persistent=True)
+        psetup = time.perf_counter() - t
+        pbatch.run([qdev.data_ptr()] * len(indexes), on_device=True)
+        pms = []
+        torch.cuda.nvtx.range_push("timed_persistent")
+        for _ in range(reps):
+            pres = pbatch.run(None)
+            pms.append(pbatch.stats()["device_ms"])
+        torch.cuda.nvtx.range_pop()
+        pst = pbatch.stats()
+        persistent = {
+            "queries_per_s": round(per_index * len(indexes) / (min(pms) * 1e-3), 1),
+            "device_ms": round(min(pms), 3), "device_ms_runs": [round(m, 3) for m in pms],
+            "kernels_per_run": pst["kernel_launches"], "graph_nodes": pst["graph_nodes"],
+            "answers_equal_graph": all(bool(np.array_equal(a[0], b[0]))
+                                       for a, b in zip(pres, res)),
+            "setup_s": round(psetup, 1)}
+        del pbatch
+    except (ValueError, RuntimeError) as e:  # reported, not fatal: the graph batch stands
+        persistent = {"error": str(e)}
     same = True
     for k, ix in enumerate(indexes):
         ws = ix.make_query_workspace(per_index)
@@ -910,6 +938,7 @@ def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=1
             "device_ms": round(best, 3), "device_ms_runs": [round(m, 3) for m in ms],
             "graph_nodes": st["graph_nodes"], "kernels_per_run": st["kernel_launches"],
             "replayed": st["replayed_queries"], "answers_equal_index_by_index": same,
+            "persistent": persistent,
             "binary64_checked": {"queries": checked * len(indexes), "distance_optimal": ok},
             "reference": reference,
             "l2_projection_modes": projections,
