@@ -876,6 +876,10 @@ def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=1
             "kernels_per_run": pst["kernel_launches"], "graph_nodes": pst["graph_nodes"],
             "answers_equal_graph": all(bool(np.array_equal(a[0], b[0]))
                                        for a, b in zip(pres, res)),
+            "stage_ms_last_run": dict(zip(
+                ["clear", "gather", "project", "tile_scan_or_median_sample",
+                 "median_count", "argmin_l2_or_median_survivor",
+                 "refine_l2_or_argmin_l1", "refine_l1"], pbatch.stage_ms())),
             "setup_s": round(psetup, 1)}
         del pbatch
     except (ValueError, RuntimeError) as e:  # reported, not fatal: the graph batch stands

@@ -371,7 +371,9 @@ uha_status uha_precision_scores(const uha_index* index, uha_workspace* workspace
 /* The scan shape the autotuner chose: kernel 0 = streaming scan
  * (queries_per_pass queries per pass over the rows), 1 = register-tiled scan
  * (64 queries per tile), 2 = tensor-core score kernel (tile_queries per
- * tile); `splits` column / K splits. best_ms is its median event-timed
+ * tile); `splits` column / K splits; 3 = the L1 hierarchy's median passes
+ * (queries_per_pass queries per pruning-count CTA, `splits` rows whose exact
+ * medians set the pruning threshold). best_ms is its median event-timed
  * duration, default_ms that of the built-in heuristic's shape. */
 typedef struct uha_tune_report {
     uint32_t candidates;
@@ -387,8 +389,11 @@ typedef struct uha_tune_report {
  * `strategy` on this workspace (CUDA events, median of 3 launches) and keeps
  * the fastest: later queries of that batch size on this workspace use it.
  * Answers do not change (the certification bound follows the shape).
- * Indexes with a single shape (median hierarchies, trivial indexes) report
- * zero candidates. report may be NULL. */
+ * L1 hierarchies time their median passes (sample, pruning count,
+ * survivors) on stand-in queries, midpoints of pairs of the index's own
+ * projected rows, since their cost depends on the data; the workspace's query
+ * buffers are overwritten. Trivial indexes report zero candidates. report
+ * may be NULL. */
 uha_status uha_workspace_autotune(uha_workspace* workspace, uint64_t batch,
                                   uha_strategy strategy, uha_tune_report* report);
 
@@ -436,6 +441,12 @@ uha_status uha_batch_run(uha_batch* batch, const float* const* queries,
                          int queries_on_device, uint64_t* out_indices,
                          double* out_distances);
 uha_status uha_batch_stats_get(const uha_batch* batch, uha_batch_stats* out);
+/* Stage durations of the last run of a persistent batch, in ms, as CTA 0 of
+ * the kernel saw them (between the grid barriers; %globaltimer): the first
+ * `count` of them into out_ms, zero past the last stage. *stages = number of
+ * stages (0 for a batch that is not persistent). No reference counterpart. */
+uha_status uha_batch_stage_times(const uha_batch* batch, double* out_ms, uint64_t count,
+                                 uint64_t* stages);
 uha_status uha_batch_tuning(const uha_batch* batch, uint64_t pair,
                             uha_tune_report* out);
 void uha_batch_destroy(uha_batch* batch);

@@ -143,3 +143,40 @@ def test_batch_rejects_bad_input():
         batch.run([bad])
     (got, _), = batch.run([queries[:2]])
     assert np.array_equal(got, golden("exact_l2")["indices"][:2])
+
+
+@pytest.mark.parametrize("batch", [1, 3, 8, 64])
+def test_autotune_median_passes_keeps_oracle_answers(oracle_module, batch):
+    """The L1 hierarchy's median passes are tuned (sampled rows for the
+    pruning threshold, queries per count CTA) on stand-in queries; every
+    candidate shape gives the oracle's answers, and the tuned workspace
+    answers as an untuned one."""
+    ds = synthetic.row_dataset(rows=3000, classes=9, queries=64, d=2049, seed=12)
+    probs = oracle_module.probabilities("l1", ds.rows)
+    index = uha.CudaHierarchicalL1AnnIndex(ds.rows, 16, 64, uha.MT19937_64(5),
+                                           importance_probabilities=probs)
+    cs = index.coordinate_sample
+    q = np.ascontiguousarray(ds.queries[:batch])
+    expected, _ = oracle_module.hierarchical("l1", ds.rows, cs.source_columns,
+                                             index.projection, q)
+    ws = index.make_query_workspace(batch)
+    rep = ws.autotune(batch)
+    assert rep["kernel"] == "median"
+    assert rep["candidates"] >= 3
+    assert rep["best_ms"] <= rep["default_ms"]
+    assert 32 <= rep["splits"] <= 1024  # sampled rows
+    assert rep["queries_per_pass"] in (1, 2, 4, 8)
+    tuned_dist = np.zeros(batch, np.float64)
+    got = index.query_batch(q, batch, None, ws, distances=tuned_dist)
+    assert np.array_equal(got, expected)
+    want, want_dist = _individual(index, q)
+    assert np.array_equal(got, want)
+    assert np.allclose(tuned_dist, want_dist, rtol=1e-5, atol=1e-30)
+    # a batch with autotune uses the tuned median shape in its graph and in
+    # the persistent form (more than 8 queries)
+    pair = [(index, batch)]
+    for persistent in ((False, True) if batch > 8 else (False,)):
+        b = uha.QueryBatch(pair, autotune=True, persistent=persistent)
+        assert b.tuning(0)["kernel"] == "median"
+        res = b.run([q])
+        assert np.array_equal(res[0][0], expected)

@@ -66,7 +66,10 @@ def test_emulated_replay_exact_matches_oracle(oracle_module, metric, shape):
         got, dist, replayed = run(index, queries, batch)
         assert np.array_equal(got, expected), f"batch {batch}"
         assert np.allclose(dist, edist, rtol=DIST_RTOL, atol=1e-30)
-        assert replayed >= 3  # the duplicates cannot be certified in binary32
+        # query 0 ties with exact duplicates of its row: no binary32 bound
+        # separates them, so it is always replayed (the one-ulp neighbour is
+        # separable in binary32 and need not be)
+        assert replayed >= 1
         assert got[0] == 5
 
 

@@ -169,6 +169,7 @@ SIGNATURES = {
     "uha_batch_query_buffer": (c_void_p, [c_void_p, c_uint64]),
     "uha_batch_run": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
     "uha_batch_stats_get": (c_int, [c_void_p, POINTER(BatchStats)]),
+    "uha_batch_stage_times": (c_int, [c_void_p, c_void_p, c_uint64, POINTER(c_uint64)]),
     "uha_batch_tuning": (c_int, [c_void_p, c_uint64, POINTER(TuneReport)]),
     "uha_batch_destroy": (None, [c_void_p]),
     "uha_server_create": (c_int, [c_int, POINTER(ServerConfig), _H]),

@@ -402,7 +402,7 @@ def compute_l1_importance_probabilities_gpu(representatives, device: int = 0,
 
 
 def _tune_dict(r) -> dict:
-    kernel = ("stream", "tile", "tensor")[r.kernel] if r.candidates else "fixed"
+    kernel = ("stream", "tile", "tensor", "median")[r.kernel] if r.candidates else "fixed"
     return {"candidates": r.candidates, "kernel": kernel,
             "queries_per_pass": r.queries_per_pass, "tile_queries": r.tile_queries,
             "splits": r.splits, "best_ms": r.best_ms, "default_ms": r.default_ms}
@@ -987,6 +987,15 @@ class QueryBatch:
         return {"pairs": st.pairs, "queries": st.queries, "graph_nodes": st.graph_nodes,
                 "kernel_launches": st.kernel_launches,
                 "replayed_queries": st.replayed_queries, "device_ms": st.device_ms}
+
+    def stage_ms(self) -> list[float]:
+        """Stage durations (ms) of the last run of a persistent batch, as the
+        kernel's first CTA saw them between its grid barriers; [] otherwise."""
+        out = np.zeros(16, np.float64)
+        stages = ctypes.c_uint64(0)
+        _check(_abi.load().uha_batch_stage_times(self._handle, out.ctypes.data, 16,
+                                                 ctypes.byref(stages)))
+        return [round(float(v), 4) for v in out[:stages.value]]
 
     def tuning(self, pair: int) -> dict:
         r = _abi.TuneReport()

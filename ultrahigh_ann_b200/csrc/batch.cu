@@ -92,7 +92,7 @@ void autotune(const uha_index* index, uha_workspace* ws, uint64_t batch,
     const bool trivial = (index->kind == IndexKind::hierarchical && index->rows == 1) ||
                          index->padded_dim == 0;
     const bool median = index->kind == IndexKind::hierarchical && index->metric == UHA_L1;
-    if (trivial || median || batch == 0) {
+    if (trivial || batch == 0) {
         // one shape only: nothing to choose
         if (report != nullptr) {
             *report = rep;
@@ -106,7 +106,58 @@ void autotune(const uha_index* index, uha_workspace* ws, uint64_t batch,
     best.strategy = static_cast<int>(strategy);
     best.ms = -1.0;
     const int reps = 3;
-    if (precision_strategy(strategy)) {
+    if (median) {
+        // The median passes' cost depends on the data (the pruning threshold,
+        // the survivors), so they are timed on stand-in queries like the
+        // index's own data: midpoints of row pairs, with zero projection
+        // errors. The passes' answers do not depend on the shape.
+        const uint64_t pp = index->padded_dim;
+        const uint64_t rows = index->rows;
+        require(ws->projected.size() >= batch * pp && ws->query_err.size() >= batch &&
+                    ws->coord_err.size() >= batch * pp &&
+                    ws->pair_err.size() >= batch * rows,
+                UHA_RUNTIME_ERROR, "the workspace has no room for tuning the median passes");
+        if (ws->median_min.size() < batch || ws->partials.size() < batch * rows) {
+            check_cuda(cudaStreamSynchronize(stream), "CUDA query failed");
+            if (ws->median_min.size() < batch) {
+                ws->median_min.allocate(std::max<uint64_t>(batch, ws->max_batch));
+            }
+            if (ws->partials.size() < batch * rows) {
+                ws->partials.allocate(batch * rows);
+            }
+        }
+        uha::launch_median_tuning_queries(index->scan_rows.get(), rows, pp,
+                                          index->projection_dimension, batch,
+                                          ws->projected.get(), stream);
+        check_cuda(cudaMemsetAsync(ws->query_err.get(), 0, batch * sizeof(float), stream),
+                   "cannot clear query errors");
+        check_cuda(cudaMemsetAsync(ws->coord_err.get(), 0, batch * pp * sizeof(float), stream),
+                   "cannot clear query errors");
+        const std::vector<uha::MedianPlan> cands = uha::median_candidates(rows, batch);
+        for (size_t i = 0; i < cands.size(); ++i) {
+            const double ms = time_launches(stream, reps, [&] {
+                uha::launch_median_scan(cands[i], index->scan_rows.get(),
+                                        index->scan_rows_t.get(), index->rows_pitch, rows, pp,
+                                        index->projection_dimension, ws->projected.get(),
+                                        batch, ws->query_err.get(), ws->coord_err.get(),
+                                        index->row_err_max, kMedianRel, kMedianAbs,
+                                        ws->median_min.get(), ws->partials.get(),
+                                        ws->pair_err.get(), stream);
+            });
+            if (i == 0) {
+                rep.default_ms = ms;
+            }
+            if (best.ms < 0 || ms < best.ms) {
+                best.ms = ms;
+                best.median = true;
+                best.median_plan = cands[i];
+            }
+        }
+        best.candidates = static_cast<int>(cands.size());
+        rep.kernel = 3;
+        rep.queries_per_pass = best.median_plan.count_queries;
+        rep.splits = best.median_plan.samples;
+    } else if (precision_strategy(strategy)) {
         const uha::LowpType type = lowp_type(strategy);
         const uha::LowpRows& lp = lowp_rows(index, type, stream);
         ensure_lowp_workspace(ws, index, stream);
@@ -252,6 +303,8 @@ struct uha_batch {
     uha::DeviceBuffer<uha::PersistentSegment> d_segments;
     uha::DeviceBuffer<unsigned int> barrier;  // [0] arrivals [1] generation [2] status
     uha::PinnedBuffer<int> host_status;
+    uha::DeviceBuffer<unsigned long long> clock;  // stage boundaries (ns)
+    uha::PinnedBuffer<unsigned long long> host_clock;
     uha::PersistentPlan plan{};
     uint32_t grid = 0;
 
@@ -343,6 +396,10 @@ void build_persistent(uha_batch* batch)
     batch->barrier.allocate(3);
     batch->host_status.allocate(1);
     batch->host_status.get()[0] = 0;
+    batch->clock.allocate(uha::kPersistentStages + 1);
+    batch->host_clock.allocate(uha::kPersistentStages + 1);
+    std::fill(batch->host_clock.get(), batch->host_clock.get() + uha::kPersistentStages + 1,
+              0ull);
     check_cuda(cudaMemcpyAsync(batch->d_pairs.get(), pairs.data(), batch->d_pairs.bytes(),
                                cudaMemcpyHostToDevice, batch->stream),
                "cannot upload the persistent batch");
@@ -357,6 +414,7 @@ void build_persistent(uha_batch* batch)
     batch->plan.segments = batch->d_segments.get();
     batch->plan.barrier = batch->barrier.get();
     batch->plan.status = reinterpret_cast<int*>(batch->barrier.get() + 2);
+    batch->plan.clock = batch->clock.get();
     batch->grid = uha::persistent_grid(batch->plan.smem_bytes);
     require(batch->grid != 0, UHA_RUNTIME_ERROR,
             "the persistent batch kernel cannot be resident with its shared memory");
@@ -456,6 +514,10 @@ uha_status create_batch(const uha_index* const* indexes, const uint64_t* query_c
                 check_cuda(cudaMemcpyAsync(batch->host_status.get(), batch->plan.status,
                                            sizeof(int), cudaMemcpyDeviceToHost, batch->stream),
                            "cannot copy the persistent batch status");
+                check_cuda(cudaMemcpyAsync(batch->host_clock.get(), batch->clock.get(),
+                                           batch->clock.bytes(), cudaMemcpyDeviceToHost,
+                                           batch->stream),
+                           "cannot copy the persistent batch stage clock");
             }
             check_cuda(cudaEventRecord(batch->fork, batch->stream), "event");
             for (uha_batch::Pair& p : batch->pairs) {
@@ -584,6 +646,22 @@ extern "C" uha_status uha_batch_stats_get(const uha_batch* batch, uha_batch_stat
             out->queries = batch->total;
             out->graph_nodes = batch->graph_nodes;
             out->kernel_launches = batch->launches;
+        }
+    });
+}
+
+extern "C" uha_status uha_batch_stage_times(const uha_batch* batch, double* out_ms,
+                                            uint64_t count, uint64_t* stages)
+{
+    return guarded([&] {
+        require(batch != nullptr && stages != nullptr && (out_ms != nullptr || count == 0),
+                UHA_INVALID_ARGUMENT, "batch and outputs must not be null");
+        *stages = batch->persistent ? uha::kPersistentStages : 0;
+        const unsigned long long* c = batch->host_clock.get();
+        for (uint64_t s = 0; s < count; ++s) {
+            const bool have = batch->persistent && s < uha::kPersistentStages &&
+                              c[s + 1] >= c[s] && c[0] != 0;
+            out_ms[s] = have ? static_cast<double>(c[s + 1] - c[s]) * 1e-6 : 0.0;
         }
     });
 }

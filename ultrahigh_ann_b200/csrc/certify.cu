@@ -1266,8 +1266,13 @@ __device__ __forceinline__ void allow_next_grid()
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// float4 groups of a row each lane of the flat query kernel loads before it
+// adds them (loads in flight per lane)
+constexpr int kFlatChunk = 8;
+
 // Per-row accumulation of one lane: binary32, column order, four terms per
-// float4 group (the same arithmetic as small_query_kernel).
+// float4 group (the same arithmetic as small_query_kernel); the query and the
+// weights are in shared memory.
 __device__ __forceinline__ float flat_terms(int op, float acc, const float4 a,
                                             const float4 b, const float4* w4, uint64_t g)
 {
@@ -1282,7 +1287,7 @@ __device__ __forceinline__ float flat_terms(int op, float acc, const float4 a,
         acc += fabsf(a.z - b.z);
         acc += fabsf(a.w - b.w);
     } else {
-        const float4 w = __ldg(w4 + g);
+        const float4 w = w4[g];
         acc = fmaf(fabsf(a.x - b.x), w.x, acc);
         acc = fmaf(fabsf(a.y - b.y), w.y, acc);
         acc = fmaf(fabsf(a.z - b.z), w.z, acc);
@@ -1293,28 +1298,38 @@ __device__ __forceinline__ float flat_terms(int op, float acc, const float4 a,
 
 // grid = (row blocks, batch), kFinalizeThreads threads. Every CTA gathers its
 // query's sampled (or all) coordinates into shared memory with the
-// preparation kernels' finiteness flags, then computes the binary32 distance
-// of each of its rows with kLanes lanes per row (each lane sums its float4
-// groups g = lane, lane + kLanes, ... in column order; a butterfly within the
-// lane group adds the kLanes partial sums), stores it in the query's distance
-// slab and keeps its two smallest. The last CTA of the query to finish merges
-// the CTA summaries and certifies the argmin, replaying the candidates in
-// binary64 when the bounds overlap, exactly as argmin_kernel does. Every CTA
-// passes wait_for_previous_grid() before it writes anything, so a grid that
-// starts early (programmatic serialization) only overlaps its launch and its
-// gather with the previous kernel.
+// preparation kernels' finiteness flags (and the column weights of a weighted
+// L1 index), then computes the binary32 distance of each of its rows with
+// kLanes lanes per row (each lane sums its float4 groups g = lane,
+// lane + kLanes, ... in column order, kFlatChunk loads in flight; a butterfly
+// within the lane group adds the kLanes partial sums), stores it in the
+// query's distance slab and keeps its two smallest. The last CTA of the query
+// to finish merges the CTA summaries and certifies the argmin, replaying the
+// candidates in binary64 when the bounds overlap, exactly as argmin_kernel
+// does.
+//
+// Consecutive launches alternate between two scratch slots (distance slabs,
+// summaries, completion counters), so a launch's gather and scan depend on
+// nothing the previous launch writes and run while it finishes (programmatic
+// serialization). Every CTA passes wait_for_previous_grid() -- the previous
+// grid has completed -- before it publishes its summary or writes a result,
+// and only then lets the next grid start; so at most two grids are in flight,
+// and the grid after next, which reuses this grid's slot, starts only once
+// this grid has completed.
 template <int kLanes, bool kEmulated>
-__global__ void __launch_bounds__(kFinalizeThreads)
+__global__ void __launch_bounds__(kFinalizeThreads, 4)
     flat_query_kernel(SmallQuery sq, Bound bound, ReplayInputs in, float* distances,
                       Summary* block_summaries, uint32_t* done, uint32_t summary_stride,
                       uint32_t span, Result* results, double* exact_distances,
                       uint32_t* replay_count, int* error_flag)
 {
     extern __shared__ float flat_smem[];
-    float* qv = flat_smem;  // padded_dim
+    float* qv = flat_smem;                  // padded_dim
+    float* wv = flat_smem + sq.padded_dim;  // padded_dim, weighted L1 only
     __shared__ int bad;
     const uint32_t q = blockIdx.y;
     const uint32_t blocks = gridDim.x;
+    const bool weighted = sq.op == static_cast<int>(ScanOp::l1_weighted);
     if (threadIdx.x == 0) {
         bad = 0;
     }
@@ -1337,11 +1352,79 @@ __global__ void __launch_bounds__(kFinalizeThreads)
             }
         }
         qv[i] = v;
+        if (weighted) {
+            wv[i] = sq.weights32[i];
+        }
     }
     if (local_bad != 0) {
         bad = 1;
     }
     __syncthreads();
+
+    const float inf = __int_as_float(0x7f800000);
+    Summary s{inf, inf, inf, 0xffffffffu, inf};
+    const int lane = threadIdx.x % 32;
+    float* dist = distances + static_cast<uint64_t>(q) * sq.row_count;
+    if (!bad) {
+        constexpr int kRowsPerStep = kFinalizeThreads / kLanes;
+        const int sub = threadIdx.x % kLanes;
+        const int group = threadIdx.x / kLanes;
+        const uint64_t groups = sq.padded_dim / 4;
+        const float4* q4 = reinterpret_cast<const float4*>(qv);
+        const float4* w4 = reinterpret_cast<const float4*>(wv);
+        const uint32_t first_row = blockIdx.x * span;
+        const uint32_t end_row = min(sq.row_count, first_row + span);
+        RowScan scan;
+        for (uint32_t base = first_row; base < end_row; base += kRowsPerStep) {
+            const uint32_t row = base + group;
+            const bool valid = row < end_row;
+            const float4* r4 = reinterpret_cast<const float4*>(
+                sq.rows + static_cast<uint64_t>(valid ? row : first_row) * sq.padded_dim);
+            float acc = 0.f;
+            for (uint64_t g0 = sub; g0 < groups; g0 += kFlatChunk * kLanes) {
+                float4 b[kFlatChunk];
+#pragma unroll
+                for (int j = 0; j < kFlatChunk; ++j) {
+                    const uint64_t g = g0 + j * kLanes;
+                    b[j] = g < groups ? __ldg(r4 + g) : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+#pragma unroll
+                for (int j = 0; j < kFlatChunk; ++j) {
+                    const uint64_t g = g0 + j * kLanes;
+                    if (g < groups) {
+                        acc = flat_terms(sq.op, acc, q4[g], b[j], w4, g);
+                    }
+                }
+            }
+#pragma unroll
+            for (int o = kLanes / 2; o > 0; o /= 2) {
+                acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            }
+            if (valid && sub == 0) {
+                dist[row] = acc;
+                if (!(acc <= FLT_MAX)) {
+                    scan.overflow = true;
+                } else if (acc < scan.k1) {
+                    scan.k2 = scan.k1;
+                    scan.k1 = acc;
+                    scan.r1 = row;
+                } else if (acc < scan.k2) {
+                    scan.k2 = acc;
+                }
+            }
+        }
+        if (scan.r1 != 0xffffffffu) {
+            const Bounds2 b1 = bound_of(scan.k1, bound, scan.r1, q);
+            s = Summary{b1.upper, b1.lower,
+                        scan.k2 <= FLT_MAX ? lower_any(scan.k2, bound, q) : inf, scan.r1,
+                        scan.k1};
+        }
+        if (scan.overflow) {
+            summary_insert(s, 0.f, inf, 0xffffffffu, inf);
+        }
+        s = block_reduce_summary(s);
+    }
+
     wait_for_previous_grid();
     allow_next_grid();
     if (bad) {
@@ -1355,67 +1438,6 @@ __global__ void __launch_bounds__(kFinalizeThreads)
         }
         return;
     }
-
-    constexpr int kRowsPerStep = kFinalizeThreads / kLanes;
-    const int lane = threadIdx.x % 32;
-    const int sub = threadIdx.x % kLanes;
-    const int group = threadIdx.x / kLanes;
-    const uint64_t groups = sq.padded_dim / 4;
-    const float4* q4 = reinterpret_cast<const float4*>(qv);
-    const float4* w4 = reinterpret_cast<const float4*>(sq.weights32);
-    const uint32_t first_row = blockIdx.x * span;
-    const uint32_t end_row = min(sq.row_count, first_row + span);
-    float* dist = distances + static_cast<uint64_t>(q) * sq.row_count;
-    RowScan scan;
-    for (uint32_t base = first_row; base < end_row; base += kRowsPerStep) {
-        const uint32_t row = base + group;
-        const bool valid = row < end_row;
-        const float4* r4 = reinterpret_cast<const float4*>(
-            sq.rows + static_cast<uint64_t>(valid ? row : first_row) * sq.padded_dim);
-        float acc = 0.f;
-        uint64_t g = sub;
-        for (; g + 3 * kLanes < groups; g += 4 * kLanes) {
-            const float4 b0 = __ldg(r4 + g);
-            const float4 b1 = __ldg(r4 + g + kLanes);
-            const float4 b2 = __ldg(r4 + g + 2 * kLanes);
-            const float4 b3 = __ldg(r4 + g + 3 * kLanes);
-            acc = flat_terms(sq.op, acc, q4[g], b0, w4, g);
-            acc = flat_terms(sq.op, acc, q4[g + kLanes], b1, w4, g + kLanes);
-            acc = flat_terms(sq.op, acc, q4[g + 2 * kLanes], b2, w4, g + 2 * kLanes);
-            acc = flat_terms(sq.op, acc, q4[g + 3 * kLanes], b3, w4, g + 3 * kLanes);
-        }
-        for (; g < groups; g += kLanes) {
-            acc = flat_terms(sq.op, acc, q4[g], __ldg(r4 + g), w4, g);
-        }
-#pragma unroll
-        for (int o = kLanes / 2; o > 0; o /= 2) {
-            acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        }
-        if (valid && sub == 0) {
-            dist[row] = acc;
-            if (!(acc <= FLT_MAX)) {
-                scan.overflow = true;
-            } else if (acc < scan.k1) {
-                scan.k2 = scan.k1;
-                scan.k1 = acc;
-                scan.r1 = row;
-            } else if (acc < scan.k2) {
-                scan.k2 = acc;
-            }
-        }
-    }
-    const float inf = __int_as_float(0x7f800000);
-    Summary s{inf, inf, inf, 0xffffffffu, inf};
-    if (scan.r1 != 0xffffffffu) {
-        const Bounds2 b1 = bound_of(scan.k1, bound, scan.r1, q);
-        s = Summary{b1.upper, b1.lower,
-                    scan.k2 <= FLT_MAX ? lower_any(scan.k2, bound, q) : inf, scan.r1,
-                    scan.k1};
-    }
-    if (scan.overflow) {
-        summary_insert(s, 0.f, inf, 0xffffffffu, inf);
-    }
-    s = block_reduce_summary(s);
     __shared__ bool is_last;
     if (blocks > 1) {
         if (threadIdx.x == 0) {
@@ -2008,7 +2030,7 @@ __device__ void persistent_unit(const PersistentPair& d, uint32_t kind, uint32_t
         const uint32_t half = threadIdx.x / hierbody::kCountRows;
         const uint32_t b = 2 * u + half;
         if (b < d.count_gx * d.count_gy) {
-            const int q = a.batch >= 8 ? 8 : a.batch >= 4 ? 4 : a.batch >= 2 ? 2 : 1;
+            const uint32_t q = a.count_queries;
             float* half_smem = reinterpret_cast<float*>(smem) + half * q * a.padded_p;
             if (q == 8) {
                 persistent_count<8>(a, b, d.count_gx, half_smem, half);
@@ -2059,10 +2081,21 @@ __device__ void persistent_unit(const PersistentPair& d, uint32_t kind, uint32_t
 // The whole batch in one cooperative launch: stage after stage, every CTA
 // takes units blockIdx.x, blockIdx.x + gridDim.x, ... of the stage's list,
 // then waits at the grid barrier; a barrier that ran out ends the kernel.
+__device__ __forceinline__ unsigned long long global_timer_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 __global__ void __launch_bounds__(kFinalizeThreads, 2)
     persistent_batch_kernel(PersistentPlan plan)
 {
     extern __shared__ __align__(16) unsigned char persistent_smem[];
+    const bool timer = blockIdx.x == 0 && threadIdx.x == 0 && plan.clock != nullptr;
+    if (timer) {
+        plan.clock[0] = global_timer_ns();
+    }
     for (int stage = 0; stage < kPersistentStages; ++stage) {
         const uint32_t units = plan.stage_units[stage];
         const uint32_t seg_end = plan.stage_begin[stage + 1];
@@ -2081,6 +2114,9 @@ __global__ void __launch_bounds__(kFinalizeThreads, 2)
                 *static_cast<volatile int*>(plan.status) != 0) {
                 return;
             }
+        }
+        if (timer) {
+            plan.clock[stage + 1] = global_timer_ns();
         }
     }
 }
@@ -2312,9 +2348,10 @@ FlatPlan plan_flat_query(uint64_t rows, uint64_t padded_dim, uint64_t batch,
 
 namespace {
 
-// Scratch of the fused flat query for a workspace of `capacity` queries:
-// distance slabs, CTA summaries (room for the most CTAs any plan uses) and
-// per-query completion counters at a fixed place (zero between launches).
+// Scratch of the fused flat query for a workspace of `capacity` queries: two
+// slots (consecutive launches alternate), each with the distance slabs, the
+// CTA summaries (room for the most CTAs any plan uses) and the per-query
+// completion counters at a fixed place (zero between launches).
 struct FlatScratch {
     float* distances;
     Summary* summaries;
@@ -2322,19 +2359,42 @@ struct FlatScratch {
     uint32_t summary_stride;
 };
 
-FlatScratch flat_scratch(void* base, uint64_t capacity, uint64_t rows)
+uint64_t round_up(uint64_t v, uint64_t to)
 {
-    const uint64_t max_blocks = (rows + 7) / 8;  // span >= 8 rows
-    char* p = static_cast<char*>(base);
+    return (v + to - 1) / to * to;
+}
+
+uint64_t flat_max_blocks(uint64_t rows)
+{
+    return (rows + 7) / 8;  // span >= 8 rows
+}
+
+// offsets within a slot (the scratch starts 256-byte aligned)
+uint64_t flat_summaries_offset(uint64_t capacity, uint64_t rows)
+{
+    return round_up(capacity * rows * sizeof(float), 16);
+}
+
+uint64_t flat_done_offset(uint64_t capacity, uint64_t rows)
+{
+    return round_up(flat_summaries_offset(capacity, rows) +
+                        capacity * flat_max_blocks(rows) * sizeof(Summary),
+                    16);
+}
+
+uint64_t flat_slot_bytes(uint64_t capacity, uint64_t rows)
+{
+    return round_up(flat_done_offset(capacity, rows) + capacity * sizeof(uint32_t), 256);
+}
+
+FlatScratch flat_scratch(void* base, uint64_t capacity, uint64_t rows, uint32_t slot)
+{
+    char* p = static_cast<char*>(base) + (slot & 1u) * flat_slot_bytes(capacity, rows);
     FlatScratch fs;
     fs.distances = reinterpret_cast<float*>(p);
-    p += capacity * rows * sizeof(float);
-    p = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
-    fs.summaries = reinterpret_cast<Summary*>(p);
-    p += capacity * max_blocks * sizeof(Summary);
-    p = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
-    fs.done = reinterpret_cast<uint32_t*>(p);
-    fs.summary_stride = static_cast<uint32_t>(max_blocks);
+    fs.summaries = reinterpret_cast<Summary*>(p + flat_summaries_offset(capacity, rows));
+    fs.done = reinterpret_cast<uint32_t*>(p + flat_done_offset(capacity, rows));
+    fs.summary_stride = static_cast<uint32_t>(flat_max_blocks(rows));
     return fs;
 }
 
@@ -2344,7 +2404,9 @@ void launch_flat_lanes(const SmallQuery& sq, const FlatPlan& plan, uint32_t batc
                        Result* results, double* exact_distances, uint32_t* replay_count,
                        int* error_flag, cudaStream_t stream)
 {
-    const size_t smem = sq.padded_dim * sizeof(float);
+    // the gathered query, and the column weights of a weighted L1 index
+    const size_t smem = sq.padded_dim * sizeof(float) *
+                        (sq.op == static_cast<int>(ScanOp::l1_weighted) ? 2 : 1);
     const auto kernel =
         in.emulated ? flat_query_kernel<kLanes, true> : flat_query_kernel<kLanes, false>;
     set_dynamic_smem(reinterpret_cast<const void*>(kernel), smem);
@@ -2357,7 +2419,7 @@ void launch_flat_lanes(const SmallQuery& sq, const FlatPlan& plan, uint32_t batc
     cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
     check_cuda(cudaStreamIsCapturing(stream, &capture), "cannot query stream capture");
     if (capture == cudaStreamCaptureStatusNone) {
-        // the next query's launch and gather overlap this kernel
+        // this grid's gather and scan overlap the end of the previous one
         attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
         attr[0].val.programmaticStreamSerializationAllowed = 1;
         config.attrs = attr;
@@ -2373,20 +2435,18 @@ void launch_flat_lanes(const SmallQuery& sq, const FlatPlan& plan, uint32_t batc
 
 uint64_t flat_query_scratch_bytes(uint64_t capacity, uint64_t rows)
 {
-    const uint64_t max_blocks = (rows + 7) / 8;
-    return capacity * rows * sizeof(float) + 16 + capacity * max_blocks * sizeof(Summary) +
-           16 + capacity * sizeof(uint32_t) + 64;
+    return 2 * flat_slot_bytes(capacity, rows);
 }
 
 void launch_flat_query(const SmallQuery& sq, const FlatPlan& plan, uint32_t batch,
                        Bound bound, ReplayInputs in, void* scratch, uint64_t capacity,
-                       Result* results, double* exact_distances, uint32_t* replay_count,
-                       int* error_flag, cudaStream_t stream)
+                       uint32_t slot, Result* results, double* exact_distances,
+                       uint32_t* replay_count, int* error_flag, cudaStream_t stream)
 {
     if (batch == 0) {
         return;
     }
-    const FlatScratch fs = flat_scratch(scratch, capacity, sq.row_count);
+    const FlatScratch fs = flat_scratch(scratch, capacity, sq.row_count, slot);
     if (plan.lanes == 8) {
         launch_flat_lanes<8>(sq, plan, batch, bound, in, fs, results, exact_distances,
                              replay_count, error_flag, stream);
@@ -2512,7 +2572,7 @@ void plan_persistent_batch(const PersistentPair* pairs, uint32_t count,
                     add(4, i, kUnitCount,
                         (static_cast<uint64_t>(d.count_gx) * d.count_gy + 1) / 2);
                     smem = std::max<uint64_t>(
-                        smem, 2ull * median_count_queries(d.batch) * d.padded_p * sizeof(float));
+                        smem, 2ull * d.median.count_queries * d.padded_p * sizeof(float));
                 }
                 break;
             case 5:

@@ -1032,11 +1032,6 @@ bool fp32_rescore_strategy(uha_strategy s)
     return s == UHA_GEMM_BF16_RERANK_FP32 || s == UHA_GEMM_FP8_RERANK_FP32;
 }
 
-// Median bound of the L1 hierarchy: the binary32 |diff| and midpoint
-// roundings (the binary64 ones are within them).
-const float kMedianRel = std::ldexp(6.0f, -24);
-const float kMedianAbs = std::ldexp(1.0f, -126);
-
 // Replay inputs of the emulated (FP64-free) replay of exact and flat ops.
 void set_emulated(uha::ReplayInputs& in, const uha_index* index)
 {
@@ -1280,6 +1275,16 @@ void certification_inputs(const uha_index* index, const uha_workspace* ws,
     *in_out = in;
 }
 
+uha::MedianPlan median_plan(const uha_index* index, const uha_workspace* ws, uint64_t n)
+{
+    for (const TunedPlan& t : ws->tuned) {
+        if (t.median && t.batch == n) {
+            return t.median_plan;
+        }
+    }
+    return uha::default_median_plan(index->rows, n);
+}
+
 bool persistent_pair(const uha_index* index, uha_workspace* ws, uint64_t n,
                      uha::PersistentPair* d)
 {
@@ -1289,11 +1294,14 @@ bool persistent_pair(const uha_index* index, uha_workspace* ws, uint64_t n,
         return false;
     }
     const bool median = index->metric == UHA_L1;
+    // the tuned plan when it is a tile scan (the tuner may pick the streaming
+    // scan, which has no unit kind), else the default plan
     const TunedPlan* tuned = ws->find_tuned(n, static_cast<int>(UHA_DIRECT));
-    uha::ScanPlan plan = tuned != nullptr && !tuned->lowp
-                             ? tuned->scan
-                             : uha::plan_scan(index->rows, index->padded_dim, n,
-                                              index->sm_count);
+    uha::ScanPlan plan = uha::plan_scan(index->rows, index->padded_dim, n, index->sm_count);
+    if (!median && tuned != nullptr && !tuned->lowp && !tuned->median &&
+        tuned->scan.kernel == 1) {
+        plan = tuned->scan;
+    }
     if (median) {
         plan.chunks = 1;
         plan.depth = 0;
@@ -1349,9 +1357,11 @@ bool persistent_pair(const uha_index* index, uha_workspace* ws, uint64_t n,
         m.min_bits = ws->median_min.get();
         m.partials = ws->partials.get();
         m.pair_err = ws->pair_err.get();
-        m.samples = uha::median_sample_count(index->rows);
-        d->sample_blocks = uha::median_sample_blocks(rows, b);
-        uha::median_count_grid(rows, b, &d->count_gx, &d->count_gy);
+        const uha::MedianPlan mp = median_plan(index, ws, n);
+        m.samples = mp.samples;
+        m.count_queries = mp.count_queries;
+        d->sample_blocks = uha::median_sample_blocks(mp.samples, b);
+        uha::median_count_grid(rows, b, mp.count_queries, &d->count_gx, &d->count_gy);
         d->survivor_blocks = uha::median_survivor_blocks(rows, b);
     }
     d->view = uha::PartialView{ws->partials.get(), plan.chunks, b, rows};
@@ -1429,8 +1439,9 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
         }
         if (flat) {
             uha::launch_flat_query(sq, flat_plan, static_cast<uint32_t>(n), bound, in,
-                                   ws->flat_scratch.get(), ws->max_batch, results, exact,
-                                   replay_count, error_flag, stream);
+                                   ws->flat_scratch.get(), ws->max_batch, ws->flat_slot,
+                                   results, exact, replay_count, error_flag, stream);
+            ws->flat_slot ^= 1u;
         } else {
             uha::launch_small_query(sq, static_cast<uint32_t>(n), bound, in, results,
                                     exact, replay_count, error_flag, stream);
@@ -1540,7 +1551,7 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
     }
     const bool median = hierarchical && index->metric == UHA_L1;
     const TunedPlan* tuned = ws->find_tuned(n, static_cast<int>(c.strategy));
-    uha::ScanPlan plan = tuned != nullptr && !tuned->lowp
+    uha::ScanPlan plan = tuned != nullptr && !tuned->lowp && !tuned->median
                              ? tuned->scan
                              : uha::plan_scan(index->rows, index->padded_dim, n,
                                               index->sm_count);
@@ -1564,7 +1575,8 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
             check_cuda(cudaStreamSynchronize(stream), "CUDA query failed");
             ws->median_min.allocate(std::max<uint64_t>(n, ws->max_batch));
         }
-        uha::launch_median_scan(index->scan_rows.get(), index->scan_rows_t.get(),
+        uha::launch_median_scan(median_plan(index, ws, n), index->scan_rows.get(),
+                                index->scan_rows_t.get(),
                                 index->rows_pitch, index->rows, index->padded_dim,
                                 index->projection_dimension, scan_queries, n,
                                 ws->query_err.get(), ws->coord_err.get(),
@@ -1736,7 +1748,7 @@ void prepare_pipeline(const uha_index* index, uha_workspace* ws, uha_strategy st
     uint64_t per_slot = 0;
     for (uint64_t n = 1; n <= batch; ++n) {
         const TunedPlan* tuned = ws->find_tuned(n, static_cast<int>(strategy));
-        const uha::ScanPlan plan = tuned != nullptr && !tuned->lowp
+        const uha::ScanPlan plan = tuned != nullptr && !tuned->lowp && !tuned->median
                                        ? tuned->scan
                                        : uha::plan_scan(index->rows, index->padded_dim, n,
                                                         index->sm_count);

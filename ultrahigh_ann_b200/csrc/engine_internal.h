@@ -53,6 +53,15 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
 // index and from workspace buffers that a standalone run of n queries has
 // sized; false when the pair has no persistent form (projection dimension
 // above 256, the streaming scan of batches up to 8, oversized shared memory).
+// Median bound of the L1 hierarchy: the binary32 |diff| and midpoint
+// roundings (the binary64 ones are within them): 6 * 2^-24 relative, 2^-126
+// absolute.
+constexpr float kMedianRel = 0x1.8p-22f;
+constexpr float kMedianAbs = 0x1p-126f;
+
+// The median passes' shape for batches of n on this workspace: the tuned
+// one, else the default.
+uha::MedianPlan median_plan(const uha_index* index, const uha_workspace* ws, uint64_t n);
 bool persistent_pair(const uha_index* index, uha_workspace* ws, uint64_t n,
                      uha::PersistentPair* d);
 

@@ -322,28 +322,29 @@ void launch_median_count(const float* rows_t, uint32_t r_pitch, uint32_t rc, uin
 }
 
 template <int PER_LANE>
-void launch_median_pair(const float* rows, const float* rows_t, uint32_t r_pitch,
-                        uint32_t rc, uint32_t pp, uint32_t pv, const float* queries,
-                        uint32_t b, const float* query_err, const float* coord_err,
-                        float row_err_max, float rel, float abs_err,
+void launch_median_pair(const MedianPlan& plan, const float* rows, const float* rows_t,
+                        uint32_t r_pitch, uint32_t rc, uint32_t pp, uint32_t pv,
+                        const float* queries, uint32_t b, const float* query_err,
+                        const float* coord_err, float row_err_max, float rel, float abs_err,
                         unsigned int* min_bits, float* partials, float* pair_err,
                         cudaStream_t stream)
 {
     // grid-stride warps over the pairs: at most 16 resident CTAs' worth per SM
     const uint64_t cap = 148ull * 16;
-    const uint32_t samples = median_samples(rc);
+    const uint32_t samples = plan.samples;
     const uint64_t sample_blocks =
         (static_cast<uint64_t>(samples) * b * 32 + kThreads - 1) / kThreads;
     median_sample_kernel<PER_LANE>
         <<<static_cast<uint32_t>(std::min(sample_blocks, cap)), kThreads, 0, stream>>>(
             rows, rc, pp, pv, queries, b, samples, partials, min_bits);
-    if (b >= 8) {
+    const uint32_t q = plan.count_queries;
+    if (q >= 8) {
         launch_median_count<8>(rows_t, r_pitch, rc, pp, pv, queries, b, min_bits, query_err,
                                row_err_max, rel, abs_err, partials, stream);
-    } else if (b >= 4) {
+    } else if (q >= 4) {
         launch_median_count<4>(rows_t, r_pitch, rc, pp, pv, queries, b, min_bits, query_err,
                                row_err_max, rel, abs_err, partials, stream);
-    } else if (b >= 2) {
+    } else if (q >= 2) {
         launch_median_count<2>(rows_t, r_pitch, rc, pp, pv, queries, b, min_bits, query_err,
                                row_err_max, rel, abs_err, partials, stream);
     } else {
@@ -357,10 +358,76 @@ void launch_median_pair(const float* rows, const float* rows_t, uint32_t r_pitch
             rows, rc, pp, pv, queries, b, coord_err, partials, pair_err);
 }
 
+__global__ void median_tuning_queries_kernel(const float* __restrict__ rows, uint32_t rc,
+                                             uint32_t pp, uint32_t pv, uint32_t batch,
+                                             float* __restrict__ queries)
+{
+    const uint64_t total = static_cast<uint64_t>(batch) * pp;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+         i < total; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t q = i / pp;
+        const uint32_t j = static_cast<uint32_t>(i % pp);
+        const uint64_t a = (7919ull * q + 1) % rc;
+        const uint64_t b = (104729ull * q + 3) % rc;
+        queries[i] = j < pv ? 0.5f * (rows[a * pp + j] + rows[b * pp + j]) : 0.f;
+    }
+}
+
 }  // namespace
 
-void launch_median_scan(const float* rows, const float* rows_t, uint64_t r_pitch,
-                        uint64_t row_count, uint64_t padded_p,
+MedianPlan default_median_plan(uint64_t row_count, uint64_t batch)
+{
+    return MedianPlan{median_samples(row_count),
+                      static_cast<uint32_t>(median_count_queries(
+                          static_cast<uint32_t>(std::min<uint64_t>(batch, 8))))};
+}
+
+std::vector<MedianPlan> median_candidates(uint64_t row_count, uint64_t batch)
+{
+    const MedianPlan base = default_median_plan(row_count, batch);
+    std::vector<MedianPlan> out{base};
+    // half and twice the sampled rows (32 to 1024, at most the row count)
+    std::vector<uint32_t> samples{base.samples};
+    for (uint64_t s : {static_cast<uint64_t>(base.samples) / 2,
+                       static_cast<uint64_t>(base.samples) * 2}) {
+        s = std::min<uint64_t>(std::max<uint64_t>(s, 32), std::min<uint64_t>(row_count, 1024));
+        if (std::find(samples.begin(), samples.end(), s) == samples.end()) {
+            samples.push_back(static_cast<uint32_t>(s));
+        }
+    }
+    // the count with the default's queries per CTA and with half as many
+    std::vector<uint32_t> widths{base.count_queries};
+    if (base.count_queries > 1) {
+        widths.push_back(base.count_queries / 2);
+    }
+    for (uint32_t s : samples) {
+        for (uint32_t q : widths) {
+            if (s != base.samples || q != base.count_queries) {
+                out.push_back(MedianPlan{s, q});
+            }
+        }
+    }
+    return out;
+}
+
+void launch_median_tuning_queries(const float* rows, uint64_t row_count, uint64_t padded_p,
+                                  uint64_t p, uint64_t batch, float* queries,
+                                  cudaStream_t stream)
+{
+    if (row_count == 0 || batch == 0 || padded_p == 0) {
+        return;
+    }
+    const uint64_t total = batch * padded_p;
+    const uint32_t blocks =
+        static_cast<uint32_t>(std::min<uint64_t>((total + kThreads - 1) / kThreads, 148 * 8));
+    median_tuning_queries_kernel<<<blocks, kThreads, 0, stream>>>(
+        rows, static_cast<uint32_t>(row_count), static_cast<uint32_t>(padded_p),
+        static_cast<uint32_t>(p), static_cast<uint32_t>(batch), queries);
+    check_cuda(cudaGetLastError(), "cannot launch tuning query kernel");
+}
+
+void launch_median_scan(const MedianPlan& plan, const float* rows, const float* rows_t,
+                        uint64_t r_pitch, uint64_t row_count, uint64_t padded_p,
                         uint64_t p, const float* queries, uint64_t batch,
                         const float* query_err, const float* coord_err,
                         float row_err_max, float rel,
@@ -375,27 +442,27 @@ void launch_median_scan(const float* rows, const float* rows_t, uint64_t r_pitch
     check_cuda(cudaMemsetAsync(min_bits, 0xff, batch * sizeof(unsigned int), stream),
                "cannot clear median thresholds");
     if (p <= 32) {
-        launch_median_pair<1>(rows, rows_t, rp, rc, pp, pv, queries, b, query_err,
+        launch_median_pair<1>(plan, rows, rows_t, rp, rc, pp, pv, queries, b, query_err,
                                coord_err, row_err_max, rel, abs_err, min_bits, partials,
                                pair_err, stream);
     } else if (p <= 64) {
-        launch_median_pair<2>(rows, rows_t, rp, rc, pp, pv, queries, b, query_err,
+        launch_median_pair<2>(plan, rows, rows_t, rp, rc, pp, pv, queries, b, query_err,
                                coord_err, row_err_max, rel, abs_err, min_bits, partials,
                                pair_err, stream);
     } else if (p <= 128) {
-        launch_median_pair<4>(rows, rows_t, rp, rc, pp, pv, queries, b, query_err,
+        launch_median_pair<4>(plan, rows, rows_t, rp, rc, pp, pv, queries, b, query_err,
                                coord_err, row_err_max, rel, abs_err, min_bits, partials,
                                pair_err, stream);
     } else if (p <= 256) {
-        launch_median_pair<8>(rows, rows_t, rp, rc, pp, pv, queries, b, query_err,
+        launch_median_pair<8>(plan, rows, rows_t, rp, rc, pp, pv, queries, b, query_err,
                                coord_err, row_err_max, rel, abs_err, min_bits, partials,
                                pair_err, stream);
     } else if (p <= 512) {
-        launch_median_pair<16>(rows, rows_t, rp, rc, pp, pv, queries, b, query_err,
+        launch_median_pair<16>(plan, rows, rows_t, rp, rc, pp, pv, queries, b, query_err,
                                coord_err, row_err_max, rel, abs_err, min_bits, partials,
                                pair_err, stream);
     } else if (p <= 1024) {
-        launch_median_pair<32>(rows, rows_t, rp, rc, pp, pv, queries, b, query_err,
+        launch_median_pair<32>(plan, rows, rows_t, rp, rc, pp, pv, queries, b, query_err,
                                coord_err, row_err_max, rel, abs_err, min_bits, partials,
                                pair_err, stream);
     } else {
@@ -418,17 +485,11 @@ void project_queries_grid(uint64_t batch, uint64_t padded_p, uint32_t* gx, uint3
     *gy = static_cast<uint32_t>((batch + kProjQueries - 1) / kProjQueries);
 }
 
-uint32_t median_sample_count(uint64_t row_count)
-{
-    return median_samples(row_count);
-}
-
-uint32_t median_sample_blocks(uint32_t row_count, uint32_t batch)
+uint32_t median_sample_blocks(uint32_t samples, uint32_t batch)
 {
     const uint64_t cap = 148ull * 16;
     const uint64_t blocks =
-        (static_cast<uint64_t>(median_samples(row_count)) * batch * 32 + kThreads - 1) /
-        kThreads;
+        (static_cast<uint64_t>(samples) * batch * 32 + kThreads - 1) / kThreads;
     return static_cast<uint32_t>(std::min(blocks, cap));
 }
 
@@ -437,9 +498,9 @@ int median_count_queries(uint32_t batch)
     return batch >= 8 ? 8 : batch >= 4 ? 4 : batch >= 2 ? 2 : 1;
 }
 
-void median_count_grid(uint32_t row_count, uint32_t batch, uint32_t* gx, uint32_t* gy)
+void median_count_grid(uint32_t row_count, uint32_t batch, uint32_t q, uint32_t* gx,
+                       uint32_t* gy)
 {
-    const int q = median_count_queries(batch);
     const uint32_t per_cta = kCountRows * (q >= 4 ? 2 : 1);
     *gx = (row_count + per_cta - 1) / per_cta;
     *gy = (batch + q - 1) / q;

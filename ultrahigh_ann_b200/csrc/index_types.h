@@ -82,8 +82,10 @@ struct TunedPlan {
     uint64_t batch = 0;
     int strategy = 0;
     bool lowp = false;
+    bool median = false;  // median_plan holds the L1 hierarchy's median passes
     uha::ScanPlan scan{};
     uha::LowpPlan lowp_plan{};
+    uha::MedianPlan median_plan{};
     double ms = 0.0;
     int candidates = 0;
 };
@@ -104,8 +106,10 @@ struct uha_workspace {
     uha::DeviceBuffer<double> call_exact;         // replayed distances (NaN: none)
     uha::DeviceBuffer<uint32_t> counters;  // [0] replayed queries, [1] error flag
     uha::DeviceBuffer<unsigned char> finalize_scratch;
-    // fused flat query (allocated and zeroed on first use)
+    // fused flat query (allocated and zeroed on first use) and the scratch
+    // slot its next launch uses
     uha::DeviceBuffer<unsigned char> flat_scratch;
+    uint32_t flat_slot = 0;
     // precision strategies (allocated on first use)
     uha::DeviceBuffer<unsigned char> queries_lp;  // lowp_padded_count(max_batch) vectors
     uha::DeviceBuffer<float> query_scales;        // FP8 scale per query

@@ -169,8 +169,10 @@ void launch_small_query(const SmallQuery& sq, uint32_t batch, Bound bound, Repla
 // Flat and small exact indexes (padded columns <= kFlatColumns) at batches of
 // at most kFlatBatch queries: gather, scan and certified argmin (with replay)
 // in one launch with many CTAs per query, the last CTA of a query merging.
-// Launched with programmatic stream serialization outside stream capture: the
-// next kernel's launch and gather overlap this one.
+// Launched with programmatic stream serialization outside stream capture:
+// consecutive launches alternate between the two slots of the scratch (pass
+// slot = 0, 1, 0, ...), and each one's gather and scan overlap the end of the
+// previous one.
 constexpr uint64_t kFlatColumns = 8192;
 constexpr uint64_t kFlatBatch = 8;
 struct FlatPlan {
@@ -187,8 +189,8 @@ FlatPlan plan_flat_query(uint64_t rows, uint64_t padded_dim, uint64_t batch,
 uint64_t flat_query_scratch_bytes(uint64_t capacity, uint64_t rows);
 void launch_flat_query(const SmallQuery& sq, const FlatPlan& plan, uint32_t batch,
                        Bound bound, ReplayInputs in, void* scratch, uint64_t capacity,
-                       Result* results, double* exact_distances, uint32_t* replay_count,
-                       int* error_flag, cudaStream_t stream);
+                       uint32_t slot, Result* results, double* exact_distances,
+                       uint32_t* replay_count, int* error_flag, cudaStream_t stream);
 // Binary32 norm identity (no certification), lowest index on ties.
 void launch_finalize_gemm(PartialView view, const float* row_norms,
                           const float* query_norms, Result* results,
@@ -328,13 +330,30 @@ void launch_project_queries(const float* gathered, uint64_t batch,
 // |median - reference median| from the coordinates near the median only
 // (coord_err[q][j]: the projected query's per-coordinate error; rows carry
 // their binary32 rounding), in place of the max-norm errors.
-void launch_median_scan(const float* rows, const float* rows_t, uint64_t r_pitch,
-                        uint64_t row_count, uint64_t padded_p,
+//
+// The shape of the three passes (answers do not depend on it): `samples` rows
+// whose exact medians set the threshold, `count_queries` queries per CTA of
+// the pruning count (1, 2, 4 or 8, at most the batch).
+struct MedianPlan {
+    uint32_t samples;
+    uint32_t count_queries;
+};
+MedianPlan default_median_plan(uint64_t row_count, uint64_t batch);
+// The default first, then the autotuner's other candidates.
+std::vector<MedianPlan> median_candidates(uint64_t row_count, uint64_t batch);
+void launch_median_scan(const MedianPlan& plan, const float* rows, const float* rows_t,
+                        uint64_t r_pitch, uint64_t row_count, uint64_t padded_p,
                         uint64_t p, const float* queries, uint64_t batch,
                         const float* query_err, const float* coord_err,
                         float row_err_max, float rel,
                         float abs_err, unsigned int* min_bits, float* partials,
                         float* pair_err, cudaStream_t stream);
+// Stand-in queries for timing the median passes: query q is the midpoint of
+// two rows of the index (rows a = (7919 q + 1) mod r, b = (104729 q + 3) mod r),
+// zero past column p; written as batch x padded_p.
+void launch_median_tuning_queries(const float* rows, uint64_t row_count, uint64_t padded_p,
+                                  uint64_t p, uint64_t batch, float* queries,
+                                  cudaStream_t stream);
 // out[j][row] = rows[row][j] for j < padded_p (build time).
 void launch_transpose_rows(const float* rows, uint64_t row_count, uint64_t padded_p,
                            float* out, uint64_t r_pitch, cudaStream_t stream);

@@ -44,12 +44,14 @@ struct MedianArgs {
     unsigned int* min_bits;  // 0xffffffff before the sample stage
     float* partials;
     float* pair_err;
-    uint32_t samples;  // median_sample_count(row_count)
+    uint32_t samples;        // MedianPlan::samples
+    uint32_t count_queries;  // MedianPlan::count_queries
 };
-uint32_t median_sample_count(uint64_t row_count);
-uint32_t median_sample_blocks(uint32_t row_count, uint32_t batch);
+uint32_t median_sample_blocks(uint32_t samples, uint32_t batch);
+// the default queries per count CTA for a batch
 int median_count_queries(uint32_t batch);
-void median_count_grid(uint32_t row_count, uint32_t batch, uint32_t* gx, uint32_t* gy);
+void median_count_grid(uint32_t row_count, uint32_t batch, uint32_t count_queries,
+                       uint32_t* gx, uint32_t* gy);
 uint32_t median_survivor_blocks(uint32_t row_count, uint32_t batch);
 // the binary32 L2 tile scan
 uint64_t tile_scan_smem_bytes();
@@ -131,6 +133,10 @@ struct PersistentPlan {
     uint32_t stage_units[kPersistentStages];
     unsigned int* barrier;  // device: [0] arrivals, [1] generation (zero at creation)
     int* status;            // device: nonzero when a barrier wait ran out
+    // device, kPersistentStages + 1 entries: %globaltimer (ns) at the start
+    // and at the end of each stage, as CTA 0 sees them (after each barrier;
+    // the last entry when CTA 0 finishes its units of the last stage)
+    unsigned long long* clock;
     uint32_t smem_bytes;
 };
 
