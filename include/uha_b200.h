@@ -416,8 +416,10 @@ uha_status uha_batch_create(const uha_index* const* indexes,
                             const uint64_t* query_counts,
                             const uha_strategy* strategies, uint64_t count,
                             int autotune, uha_batch** out);
-/* The same batch run as ONE persistent, cooperative kernel launch (captured
- * in the batch's graph with the result copies): every CTA drains, stage by
+/* The same batch run as two persistent, cooperative kernel launches (the
+ * early stages with the tile scan's register budget, then the late stages at
+ * twice the residency; captured in the batch's graph with the result
+ * copies): every CTA drains, stage by
  * stage, a work list of units from all pairs (gather, projection, L2 tile
  * scan or median sample / count / survivor passes, certified argmin with
  * replay, reported distances), separated by grid-wide barriers whose waits

@@ -55,8 +55,9 @@ def tied_rows(rng, r, d, anchor=5):
 @pytest.mark.parametrize("metric", ["l2", "l1"])
 @pytest.mark.parametrize("shape", [(40, 300), (5000, 700), (300, 20000)])
 def test_emulated_replay_exact_matches_oracle(oracle_module, metric, shape):
-    # (40, 300): one-CTA kernel; (5000, 700): fused flat kernel at batch <= 8,
-    # scan + argmin above; (300, 20000): scan + argmin
+    # (40, 300): fused flat kernel at batch <= 8, one-CTA kernel above;
+    # (5000, 700): fused flat kernel at batch <= 8, scan + argmin above;
+    # (300, 20000): scan + argmin
     r, d = shape
     rows, queries = tied_rows(np.random.default_rng(r + d), r, d)
     expected, edist = oracle_module.exact(metric, rows, queries)

@@ -29,7 +29,8 @@ def _sources() -> list[Path]:
 
 
 def _headers() -> list[Path]:
-    return sorted(list(CSRC.glob("*.h")) + list((ROOT / "include").glob("*.h")))
+    return sorted(list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) +
+                  list((ROOT / "include").glob("*.h")))
 
 
 def _stale(target: Path, deps: list[Path]) -> bool:

@@ -15,7 +15,8 @@
 // into one stream, so small indexes overlap on the device and the host issues
 // one launch per run. uha_batch_create_persistent captures instead one
 // cooperative launch of the persistent batch kernel (stage_bodies.h) that
-// drains every pair's stages from one work list, plus the result copies.
+// drains every pair's stages from one work list (two cooperative launches:
+// the early and the late stages), plus the result copies.
 #include "common.h"
 #include "engine_internal.h"
 #include "index_types.h"
@@ -306,7 +307,7 @@ struct uha_batch {
     uha::DeviceBuffer<unsigned long long> clock;  // stage boundaries (ns)
     uha::PinnedBuffer<unsigned long long> host_clock;
     uha::PersistentPlan plan{};
-    uint32_t grid = 0;
+    uint32_t grid[2] = {0, 0};  // CTAs of the two persistent kernels
 
     ~uha_batch()
     {
@@ -352,7 +353,8 @@ uint64_t enqueue_pair(uha_batch::Pair& p)
     uha_workspace* ws = p.ws;
     check_cuda(cudaMemsetAsync(ws->counters.get(), 0, ws->counters.bytes(), ws->stream),
                "cannot clear query counters");
-    const BatchContext ctx{p.index, ws, p.strategy, true};
+    BatchContext ctx{p.index, ws, p.strategy, true};
+    ctx.filter_candidates = true;
     const uint64_t launches =
         enqueue_batch(ctx, ws->raw_queries.get(), p.count, ws->call_results.get(),
                       ws->call_exact.get(), false, nullptr, nullptr);
@@ -415,9 +417,11 @@ void build_persistent(uha_batch* batch)
     batch->plan.barrier = batch->barrier.get();
     batch->plan.status = reinterpret_cast<int*>(batch->barrier.get() + 2);
     batch->plan.clock = batch->clock.get();
-    batch->grid = uha::persistent_grid(batch->plan.smem_bytes);
-    require(batch->grid != 0, UHA_RUNTIME_ERROR,
-            "the persistent batch kernel cannot be resident with its shared memory");
+    for (int part = 0; part < 2; ++part) {
+        batch->grid[part] = uha::persistent_grid(part, batch->plan.smem_bytes[part]);
+        require(batch->grid[part] != 0, UHA_RUNTIME_ERROR,
+                "the persistent batch kernel cannot be resident with its shared memory");
+    }
     batch->persistent = true;
 }
 
@@ -492,7 +496,7 @@ uha_status create_batch(const uha_index* const* indexes, const uint64_t* query_c
         try {
             if (batch->persistent) {
                 uha::launch_persistent_batch(batch->plan, batch->grid, batch->stream);
-                launches = 1;
+                launches = 2;
                 for (uha_batch::Pair& p : batch->pairs) {
                     if (p.trivial) {
                         continue;
@@ -626,6 +630,20 @@ extern "C" uha_status uha_batch_run(uha_batch* batch, const float* const* querie
             if (p.trivial) {
                 fill_trivial(p.count, idx, dist);
                 continue;
+            }
+            if ((p.ws->host_counters.get()[1] & uha::kCandidateOverflow) != 0u) {
+                // a filtered candidate list overflowed: this pair again,
+                // eagerly, with the slab selection (its queries are still in
+                // the workspace)
+                p.ws->filter_disabled = true;
+                try {
+                    enqueue_pair(p);
+                    check_cuda(cudaStreamSynchronize(p.ws->stream), "CUDA batch failed");
+                } catch (...) {
+                    p.ws->filter_disabled = false;
+                    throw;
+                }
+                p.ws->filter_disabled = false;
             }
             finish_call(p.index, p.ws, p.count, p.ws->host_results.get(),
                         p.ws->host_exact.get(), idx, dist);

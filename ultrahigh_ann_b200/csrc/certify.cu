@@ -13,6 +13,7 @@
 // of (distance, row) is the CPU's argmin. The replay runs inside the argmin
 // kernel, in the block that merges the query's summaries, so a query batch
 // needs no host decision between its kernels.
+#include "async_copy.cuh"
 #include "common.h"
 #include "exact64.h"
 #include "hier_body.cuh"
@@ -1266,9 +1267,12 @@ __device__ __forceinline__ void allow_next_grid()
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
-// float4 groups of a row each lane of the flat query kernel loads before it
-// adds them (loads in flight per lane)
-constexpr int kFlatChunk = 8;
+// Polls of a flat query copy wait before it gives up (well above any copy's
+// time), and the error bit it then sets.
+constexpr uint32_t kFlatCopySpins = 1u << 22;
+constexpr int kFlatCopyTimeout = 16;
+// bytes of rows per bulk copy of the flat query kernel (two buffers per CTA)
+constexpr uint64_t kFlatChunkBytes = 32 * 1024;
 
 // Per-row accumulation of one lane: binary32, column order, four terms per
 // float4 group (the same arithmetic as small_query_kernel); the query and the
@@ -1296,42 +1300,71 @@ __device__ __forceinline__ float flat_terms(int op, float acc, const float4 a,
     return acc;
 }
 
-// grid = (row blocks, batch), kFinalizeThreads threads. Every CTA gathers its
-// query's sampled (or all) coordinates into shared memory with the
-// preparation kernels' finiteness flags (and the column weights of a weighted
-// L1 index), then computes the binary32 distance of each of its rows with
-// kLanes lanes per row (each lane sums its float4 groups g = lane,
-// lane + kLanes, ... in column order, kFlatChunk loads in flight; a butterfly
-// within the lane group adds the kLanes partial sums), stores it in the
-// query's distance slab and keeps its two smallest. The last CTA of the query
-// to finish merges the CTA summaries and certifies the argmin, replaying the
-// candidates in binary64 when the bounds overlap, exactly as argmin_kernel
-// does.
+// grid = (row blocks, batch), kFinalizeThreads threads. At entry one thread
+// of every CTA starts bulk copies (the TMA engine, cp.async.bulk) of its row
+// block into shared memory: `chunk_rows` rows per copy, two buffers, the next
+// chunk copied while one is scanned. Meanwhile the CTA gathers its query's
+// sampled (or all) coordinates into shared memory with the preparation
+// kernels' finiteness flags (and the column weights of a weighted L1 index).
+// Then it computes the binary32 distance of each row with kLanes lanes per row
+// (each lane sums its float4 groups g = lane, lane + kLanes, ... in column
+// order; a butterfly within the lane group adds the kLanes partial sums),
+// stores it in the query's distance slab and keeps its two smallest. The last
+// CTA of the query to finish merges the CTA summaries and certifies the
+// argmin, replaying the candidates in binary64 when the bounds overlap,
+// exactly as argmin_kernel does.
 //
 // Consecutive launches alternate between two scratch slots (distance slabs,
-// summaries, completion counters), so a launch's gather and scan depend on
-// nothing the previous launch writes and run while it finishes (programmatic
-// serialization). Every CTA passes wait_for_previous_grid() -- the previous
-// grid has completed -- before it publishes its summary or writes a result,
-// and only then lets the next grid start; so at most two grids are in flight,
-// and the grid after next, which reuses this grid's slot, starts only once
-// this grid has completed.
+// summaries, completion counters), so a launch's copies, gather and scan
+// depend on nothing the previous launch writes and run while it finishes
+// (programmatic serialization). Every CTA passes wait_for_previous_grid() --
+// the previous grid has completed -- before it publishes its summary or
+// writes a result, and only then lets the next grid start; so at most two
+// grids are in flight, and the grid after next, which reuses this grid's
+// slot, starts only once this grid has completed.
+//
+// A copy wait gives up after kFlatCopySpins polls: the CTA sets error bit 16
+// (the call fails), waits (bounded) for the copies it issued, and still
+// takes part in the query's merge with an empty summary, so the completion
+// counters stay consistent.
 template <int kLanes, bool kEmulated>
-__global__ void __launch_bounds__(kFinalizeThreads, 4)
+__global__ void __launch_bounds__(kFinalizeThreads, 3)
     flat_query_kernel(SmallQuery sq, Bound bound, ReplayInputs in, float* distances,
                       Summary* block_summaries, uint32_t* done, uint32_t summary_stride,
-                      uint32_t span, Result* results, double* exact_distances,
-                      uint32_t* replay_count, int* error_flag)
+                      uint32_t span, uint32_t chunk_rows, Result* results,
+                      double* exact_distances, uint32_t* replay_count, int* error_flag)
 {
-    extern __shared__ float flat_smem[];
+    extern __shared__ __align__(16) float flat_smem[];
+    const bool weighted = sq.op == static_cast<int>(ScanOp::l1_weighted);
     float* qv = flat_smem;                  // padded_dim
     float* wv = flat_smem + sq.padded_dim;  // padded_dim, weighted L1 only
+    float* chunks = flat_smem + sq.padded_dim * (weighted ? 2 : 1);  // 2 x chunk rows
+    __shared__ uint64_t full[2];
     __shared__ int bad;
+    __shared__ int copy_failed;
     const uint32_t q = blockIdx.y;
     const uint32_t blocks = gridDim.x;
-    const bool weighted = sq.op == static_cast<int>(ScanOp::l1_weighted);
+    const uint32_t first_row = blockIdx.x * span;
+    const uint32_t end_row = min(sq.row_count, first_row + span);
+    const uint32_t row_words = static_cast<uint32_t>(sq.padded_dim);
+    const uint32_t nchunks = (end_row - first_row + chunk_rows - 1) / chunk_rows;
+    auto issue = [&](uint32_t c) {
+        const uint32_t r0 = first_row + c * chunk_rows;
+        const uint32_t bytes = min(chunk_rows, end_row - r0) * row_words * 4u;
+        uint64_t* bar = full + (c & 1u);
+        async::mbar_expect_tx(bar, bytes);
+        async::bulk_copy_g2s(chunks + (c & 1u) * chunk_rows * row_words,
+                             sq.rows + static_cast<uint64_t>(r0) * row_words, bytes, bar);
+    };
     if (threadIdx.x == 0) {
         bad = 0;
+        copy_failed = 0;
+        async::mbar_init(full, 1);
+        async::mbar_init(full + 1, 1);
+        async::mbar_init_fence();
+        for (uint32_t c = 0; c < nchunks && c < 2; ++c) {
+            issue(c);
+        }
     }
     __syncthreads();
     const float* src = sq.queries + static_cast<uint64_t>(q) * sq.dim;
@@ -1365,62 +1398,85 @@ __global__ void __launch_bounds__(kFinalizeThreads, 4)
     Summary s{inf, inf, inf, 0xffffffffu, inf};
     const int lane = threadIdx.x % 32;
     float* dist = distances + static_cast<uint64_t>(q) * sq.row_count;
-    if (!bad) {
+    {
         constexpr int kRowsPerStep = kFinalizeThreads / kLanes;
         const int sub = threadIdx.x % kLanes;
         const int group = threadIdx.x / kLanes;
         const uint64_t groups = sq.padded_dim / 4;
         const float4* q4 = reinterpret_cast<const float4*>(qv);
         const float4* w4 = reinterpret_cast<const float4*>(wv);
-        const uint32_t first_row = blockIdx.x * span;
-        const uint32_t end_row = min(sq.row_count, first_row + span);
         RowScan scan;
-        for (uint32_t base = first_row; base < end_row; base += kRowsPerStep) {
-            const uint32_t row = base + group;
-            const bool valid = row < end_row;
-            const float4* r4 = reinterpret_cast<const float4*>(
-                sq.rows + static_cast<uint64_t>(valid ? row : first_row) * sq.padded_dim);
-            float acc = 0.f;
-            for (uint64_t g0 = sub; g0 < groups; g0 += kFlatChunk * kLanes) {
-                float4 b[kFlatChunk];
+        uint32_t failed_chunk = nchunks;
+        for (uint32_t c = 0; c < nchunks; ++c) {
+            // every thread sees the chunk complete (or the copy given up)
+            if (!async::mbar_wait(full + (c & 1u), (c >> 1) & 1u, kFlatCopySpins)) {
+                copy_failed = 1;
+            }
+            __syncthreads();
+            if (copy_failed) {
+                failed_chunk = c;  // chunks c and c + 1 may still be in flight
+                break;
+            }
+            const uint32_t r0 = first_row + c * chunk_rows;
+            const uint32_t rows_here = min(chunk_rows, end_row - r0);
+            const float4* buf =
+                reinterpret_cast<const float4*>(chunks + (c & 1u) * chunk_rows * row_words);
+            if (!bad) {
+                // the same trip count on every lane (warp-wide shuffles below)
+                for (uint32_t base = 0; base < rows_here; base += kRowsPerStep) {
+                    const uint32_t lr = base + group;
+                    const bool valid = lr < rows_here;
+                    const float4* r4 =
+                        buf + static_cast<uint64_t>(valid ? lr : 0) * (row_words / 4);
+                    float acc = 0.f;
+#pragma unroll 4
+                    for (uint64_t g = sub; g < groups; g += kLanes) {
+                        acc = flat_terms(sq.op, acc, q4[g], r4[g], w4, g);
+                    }
 #pragma unroll
-                for (int j = 0; j < kFlatChunk; ++j) {
-                    const uint64_t g = g0 + j * kLanes;
-                    b[j] = g < groups ? __ldg(r4 + g) : make_float4(0.f, 0.f, 0.f, 0.f);
-                }
-#pragma unroll
-                for (int j = 0; j < kFlatChunk; ++j) {
-                    const uint64_t g = g0 + j * kLanes;
-                    if (g < groups) {
-                        acc = flat_terms(sq.op, acc, q4[g], b[j], w4, g);
+                    for (int o = kLanes / 2; o > 0; o /= 2) {
+                        acc += __shfl_xor_sync(0xffffffffu, acc, o);
+                    }
+                    const uint32_t row = r0 + lr;
+                    if (valid && sub == 0) {
+                        dist[row] = acc;
+                        if (!(acc <= FLT_MAX)) {
+                            scan.overflow = true;
+                        } else if (acc < scan.k1) {
+                            scan.k2 = scan.k1;
+                            scan.k1 = acc;
+                            scan.r1 = row;
+                        } else if (acc < scan.k2) {
+                            scan.k2 = acc;
+                        }
                     }
                 }
             }
-#pragma unroll
-            for (int o = kLanes / 2; o > 0; o /= 2) {
-                acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            // the buffer is free again: copy chunk c + 2 into it
+            __syncthreads();
+            if (threadIdx.x == 0 && c + 2 < nchunks) {
+                async::fence_proxy_async_smem();
+                issue(c + 2);
             }
-            if (valid && sub == 0) {
-                dist[row] = acc;
-                if (!(acc <= FLT_MAX)) {
-                    scan.overflow = true;
-                } else if (acc < scan.k1) {
-                    scan.k2 = scan.k1;
-                    scan.k1 = acc;
-                    scan.r1 = row;
-                } else if (acc < scan.k2) {
-                    scan.k2 = acc;
+        }
+        if (failed_chunk < nchunks) {
+            // wait (bounded) for the copies that may still be in flight
+            if (threadIdx.x == 0) {
+                for (uint32_t c = failed_chunk; c < nchunks && c < failed_chunk + 2; ++c) {
+                    async::mbar_wait(full + (c & 1u), (c >> 1) & 1u, kFlatCopySpins);
                 }
+                atomicOr(error_flag, kFlatCopyTimeout);
             }
-        }
-        if (scan.r1 != 0xffffffffu) {
-            const Bounds2 b1 = bound_of(scan.k1, bound, scan.r1, q);
-            s = Summary{b1.upper, b1.lower,
-                        scan.k2 <= FLT_MAX ? lower_any(scan.k2, bound, q) : inf, scan.r1,
-                        scan.k1};
-        }
-        if (scan.overflow) {
-            summary_insert(s, 0.f, inf, 0xffffffffu, inf);
+        } else if (!bad) {
+            if (scan.r1 != 0xffffffffu) {
+                const Bounds2 b1 = bound_of(scan.k1, bound, scan.r1, q);
+                s = Summary{b1.upper, b1.lower,
+                            scan.k2 <= FLT_MAX ? lower_any(scan.k2, bound, q) : inf, scan.r1,
+                            scan.k1};
+            }
+            if (scan.overflow) {
+                summary_insert(s, 0.f, inf, 0xffffffffu, inf);
+            }
         }
         s = block_reduce_summary(s);
     }
@@ -1966,9 +2022,16 @@ __device__ __forceinline__ void persistent_count(const MedianArgs& a, uint32_t b
 
 // Unit u (of `units`) of one kind for one pair: one block of the stage kernel
 // the standalone path launches for it.
+// Units of the early stages (0-3: clear, gather, projection, tile scan,
+// median samples) when !kLate, of the late stages (4-7: median counts and
+// survivors, argmin, reported distances) when kLate; each kernel compiles
+// only its own kinds, so the late kernel's register budget is not the tile
+// scan's.
+template <bool kLate>
 __device__ void persistent_unit(const PersistentPair& d, uint32_t kind, uint32_t u,
                                 uint32_t units, unsigned char* smem)
 {
+    if constexpr (!kLate) {
     int* error_flag = reinterpret_cast<int*>(d.counters + 1);
     switch (kind) {
     case kUnitClear: {
@@ -2023,6 +2086,11 @@ __device__ void persistent_unit(const PersistentPair& d, uint32_t kind, uint32_t
         }
         break;
     }
+    default:
+        break;
+    }
+    } else {
+    switch (kind) {
     case kUnitCount: {
         // two count blocks per unit, one per half of the CTA (own barrier and
         // shared memory)
@@ -2076,11 +2144,15 @@ __device__ void persistent_unit(const PersistentPair& d, uint32_t kind, uint32_t
     default:
         break;
     }
+    }
 }
 
-// The whole batch in one cooperative launch: stage after stage, every CTA
-// takes units blockIdx.x, blockIdx.x + gridDim.x, ... of the stage's list,
-// then waits at the grid barrier; a barrier that ran out ends the kernel.
+// The batch in two cooperative launches: the early stages [0, kPersistentSplit)
+// with the tile scan's register budget (2 CTAs per SM), then the late stages
+// [kPersistentSplit, kPersistentStages) at 4 CTAs per SM. Stage after stage,
+// every CTA takes units blockIdx.x, blockIdx.x + gridDim.x, ... of the
+// stage's list, then waits at the grid barrier; a barrier that ran out ends
+// the kernel (the status word stops the next kernel too).
 __device__ __forceinline__ unsigned long long global_timer_ns()
 {
     unsigned long long t;
@@ -2088,15 +2160,19 @@ __device__ __forceinline__ unsigned long long global_timer_ns()
     return t;
 }
 
-__global__ void __launch_bounds__(kFinalizeThreads, 2)
-    persistent_batch_kernel(PersistentPlan plan)
+template <int kFirst, int kEnd, int kMinBlocks>
+__global__ void __launch_bounds__(kFinalizeThreads, kMinBlocks)
+    persistent_stages_kernel(PersistentPlan plan)
 {
     extern __shared__ __align__(16) unsigned char persistent_smem[];
+    if (*static_cast<volatile int*>(plan.status) != 0) {
+        return;  // the earlier kernel of this run gave up
+    }
     const bool timer = blockIdx.x == 0 && threadIdx.x == 0 && plan.clock != nullptr;
     if (timer) {
-        plan.clock[0] = global_timer_ns();
+        plan.clock[kFirst] = global_timer_ns();
     }
-    for (int stage = 0; stage < kPersistentStages; ++stage) {
+    for (int stage = kFirst; stage < kEnd; ++stage) {
         const uint32_t units = plan.stage_units[stage];
         const uint32_t seg_end = plan.stage_begin[stage + 1];
         uint32_t seg = plan.stage_begin[stage];
@@ -2105,11 +2181,12 @@ __global__ void __launch_bounds__(kFinalizeThreads, 2)
                 ++seg;
             }
             const PersistentSegment sg = plan.segments[seg];
-            persistent_unit(plan.pairs[sg.pair], sg.kind, u - sg.first, sg.units,
-                            persistent_smem);
+            persistent_unit<(kFirst >= kPersistentSplit)>(plan.pairs[sg.pair], sg.kind,
+                                                          u - sg.first, sg.units,
+                                                          persistent_smem);
             __syncthreads();
         }
-        if (stage + 1 < kPersistentStages) {
+        if (stage + 1 < kEnd) {
             if (!persistent_barrier(plan.barrier, plan.status) ||
                 *static_cast<volatile int*>(plan.status) != 0) {
                 return;
@@ -2121,27 +2198,46 @@ __global__ void __launch_bounds__(kFinalizeThreads, 2)
     }
 }
 
+constexpr auto persistent_early_kernel = persistent_stages_kernel<0, kPersistentSplit, 2>;
+constexpr auto persistent_late_kernel =
+    persistent_stages_kernel<kPersistentSplit, kPersistentStages, 4>;
+
 // Raises a kernel's dynamic shared-memory limit when a launch needs more than
-// 48 KB and more than it was configured for on this device (a call that needs
-// no more makes no runtime call, so captured launches after a warm-up make
-// none).
+// the default allows: 48 KB less the kernel's static shared memory (read once
+// per kernel and device). A call that needs no more makes no runtime call
+// beyond reading the current device, so captured launches after a warm-up
+// make none.
 void set_dynamic_smem(const void* kernel, size_t smem)
 {
-    if (smem <= 48 * 1024) {
+    // the last kernel this thread configured
+    thread_local const void* last_kernel = nullptr;
+    thread_local int last_device = -1;
+    thread_local size_t last_ok = 0;
+    const int device = current_device();
+    if (kernel == last_kernel && device == last_device && smem <= last_ok) {
         return;
     }
     static std::mutex mutex;
-    static std::map<std::pair<int, const void*>, size_t> configured;
-    const int device = current_device();
+    // dynamic bytes a launch may use without raising the limit again
+    static std::map<std::pair<int, const void*>, size_t> launchable;
     std::lock_guard<std::mutex> lock(mutex);
-    size_t& have = configured[{device, kernel}];
-    if (smem <= have) {
-        return;
+    auto it = launchable.find({device, kernel});
+    if (it == launchable.end()) {
+        cudaFuncAttributes attr{};
+        check_cuda(cudaFuncGetAttributes(&attr, kernel), "cannot read kernel attributes");
+        const size_t base =
+            attr.sharedSizeBytes < 48 * 1024 ? 48 * 1024 - attr.sharedSizeBytes : 0;
+        it = launchable.emplace(std::make_pair(device, kernel), base).first;
     }
-    check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(smem)),
-               "cannot configure replay shared memory");
-    have = smem;
+    if (smem > it->second) {
+        check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(smem)),
+                   "cannot configure kernel shared memory");
+        it->second = smem;
+    }
+    last_kernel = kernel;
+    last_device = device;
+    last_ok = it->second;
 }
 
 size_t replay_smem(const ReplayInputs& in)
@@ -2329,8 +2425,8 @@ FlatPlan plan_flat_query(uint64_t rows, uint64_t padded_dim, uint64_t batch,
         lanes = groups < 16 * 4 ? 8 : 16;
     }
     const uint32_t step = kFinalizeThreads / lanes;  // rows per CTA pass
-    // about four CTAs per SM over the whole launch
-    const uint64_t target = static_cast<uint64_t>(sm_count) * 4;
+    // about three CTAs per SM over the whole launch (one wave)
+    const uint64_t target = static_cast<uint64_t>(sm_count) * 3;
     const uint64_t per_query = std::max<uint64_t>(1, target / batch);
     uint64_t span = (rows + per_query - 1) / per_query;
     span = std::max<uint64_t>(step, (span + step - 1) / step * step);
@@ -2338,6 +2434,15 @@ FlatPlan plan_flat_query(uint64_t rows, uint64_t padded_dim, uint64_t batch,
     plan.lanes = lanes;
     plan.span = static_cast<uint32_t>(span);
     plan.blocks = static_cast<uint32_t>((rows + span - 1) / span);
+    // rows per bulk copy: whole passes of the CTA up to kFlatChunkBytes, else
+    // as many rows as fit (at least one: a row is at most 32 KB)
+    const uint64_t row_bytes = padded_dim * sizeof(float);
+    uint64_t chunk = kFlatChunkBytes / row_bytes / step * step;
+    if (chunk == 0) {
+        chunk = std::max<uint64_t>(1, kFlatChunkBytes / row_bytes);
+    }
+    plan.chunk_rows = static_cast<uint32_t>(std::min<uint64_t>(chunk, span));
+    plan.buffers = plan.chunk_rows >= span ? 1u : 2u;
     uint32_t log_lanes = 0;
     while ((1u << log_lanes) < lanes) {
         ++log_lanes;
@@ -2404,9 +2509,12 @@ void launch_flat_lanes(const SmallQuery& sq, const FlatPlan& plan, uint32_t batc
                        Result* results, double* exact_distances, uint32_t* replay_count,
                        int* error_flag, cudaStream_t stream)
 {
-    // the gathered query, and the column weights of a weighted L1 index
-    const size_t smem = sq.padded_dim * sizeof(float) *
-                        (sq.op == static_cast<int>(ScanOp::l1_weighted) ? 2 : 1);
+    // the gathered query (and the column weights of a weighted L1 index),
+    // then the copy buffers of the rows
+    const size_t smem =
+        sq.padded_dim * sizeof(float) *
+        ((sq.op == static_cast<int>(ScanOp::l1_weighted) ? 2 : 1) +
+         static_cast<size_t>(plan.buffers) * plan.chunk_rows);
     const auto kernel =
         in.emulated ? flat_query_kernel<kLanes, true> : flat_query_kernel<kLanes, false>;
     set_dynamic_smem(reinterpret_cast<const void*>(kernel), smem);
@@ -2427,7 +2535,8 @@ void launch_flat_lanes(const SmallQuery& sq, const FlatPlan& plan, uint32_t batc
     }
     check_cuda(cudaLaunchKernelEx(&config, kernel, sq, bound, in, fs.distances,
                                   fs.summaries, fs.done, fs.summary_stride, plan.span,
-                                  results, exact_distances, replay_count, error_flag),
+                                  plan.chunk_rows, results, exact_distances, replay_count,
+                                  error_flag),
                "cannot launch flat query kernel");
 }
 
@@ -2517,6 +2626,7 @@ void plan_persistent_batch(const PersistentPair* pairs, uint32_t count,
                            PersistentPlan* plan)
 {
     uint32_t n = 0;
+    uint64_t smem_group[2] = {0, 0};
     uint64_t smem = 0;
     auto add = [&](int stage, uint32_t pair, uint32_t kind, uint64_t units) {
         if (units == 0) {
@@ -2539,6 +2649,7 @@ void plan_persistent_batch(const PersistentPair* pairs, uint32_t count,
     }
     for (int stage = 0; stage < kPersistentStages; ++stage) {
         plan->stage_begin[stage] = n;
+        smem = 0;
         for (uint32_t i = 0; i < count; ++i) {
             const PersistentPair& d = pairs[i];
             const uint64_t per_query = (d.batch + kFinalizeThreads - 1) / kFinalizeThreads;
@@ -2600,18 +2711,33 @@ void plan_persistent_batch(const PersistentPair* pairs, uint32_t count,
                 break;
             }
         }
+        uint64_t& group = smem_group[stage < kPersistentSplit ? 0 : 1];
+        group = std::max(group, smem);
     }
     plan->stage_begin[kPersistentStages] = n;
-    plan->smem_bytes = static_cast<uint32_t>((smem + 15) / 16 * 16);
+    for (int k = 0; k < 2; ++k) {
+        plan->smem_bytes[k] = static_cast<uint32_t>((smem_group[k] + 15) / 16 * 16);
+    }
     *segment_count = n;
 }
 
-uint32_t persistent_grid(uint32_t smem_bytes)
+namespace {
+
+const void* persistent_kernel(int part)
 {
-    set_dynamic_smem(reinterpret_cast<const void*>(persistent_batch_kernel), smem_bytes);
+    return part == 0 ? reinterpret_cast<const void*>(persistent_early_kernel)
+                     : reinterpret_cast<const void*>(persistent_late_kernel);
+}
+
+}  // namespace
+
+uint32_t persistent_grid(int part, uint32_t smem_bytes)
+{
+    const void* kernel = persistent_kernel(part);
+    set_dynamic_smem(kernel, smem_bytes);
     int per_sm = 0;
-    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                   &per_sm, persistent_batch_kernel, kFinalizeThreads, smem_bytes),
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kFinalizeThreads,
+                                                             smem_bytes),
                "cannot size the persistent batch kernel");
     int sms = 0;
     check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, current_device()),
@@ -2619,23 +2745,28 @@ uint32_t persistent_grid(uint32_t smem_bytes)
     return static_cast<uint32_t>(std::max(0, per_sm) * sms);
 }
 
-void launch_persistent_batch(const PersistentPlan& plan, uint32_t grid, cudaStream_t stream)
+void launch_persistent_batch(const PersistentPlan& plan, const uint32_t grid[2],
+                             cudaStream_t stream)
 {
-    set_dynamic_smem(reinterpret_cast<const void*>(persistent_batch_kernel), plan.smem_bytes);
-    cudaLaunchConfig_t config{};
-    config.gridDim = dim3(grid);
-    config.blockDim = dim3(kFinalizeThreads);
-    config.dynamicSmemBytes = plan.smem_bytes;
-    config.stream = stream;
-    cudaLaunchAttribute attr[1];
-    // every CTA resident at once: the grid barrier never waits for a CTA
-    // that has not started
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
-    config.attrs = attr;
-    config.numAttrs = 1;
-    check_cuda(cudaLaunchKernelEx(&config, persistent_batch_kernel, plan),
-               "cannot launch the persistent batch kernel");
+    for (int part = 0; part < 2; ++part) {
+        const void* kernel = persistent_kernel(part);
+        set_dynamic_smem(kernel, plan.smem_bytes[part]);
+        cudaLaunchConfig_t config{};
+        config.gridDim = dim3(grid[part]);
+        config.blockDim = dim3(kFinalizeThreads);
+        config.dynamicSmemBytes = plan.smem_bytes[part];
+        config.stream = stream;
+        cudaLaunchAttribute attr[1];
+        // every CTA resident at once: the grid barrier never waits for a CTA
+        // that has not started
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        config.attrs = attr;
+        config.numAttrs = 1;
+        void* args[] = {const_cast<PersistentPlan*>(&plan)};
+        check_cuda(cudaLaunchKernelExC(&config, kernel, args),
+                   "cannot launch the persistent batch kernel");
+    }
 }
 
 }  // namespace uha

@@ -1010,13 +1010,13 @@ bool small_path_applies(const uha_index* index, uha_strategy strategy)
            uha::small_query_fits(index->rows, index->padded_dim);
 }
 
-// Certified queries of at most uha::kFlatBatch on flat (and small exact)
-// indexes too large for one CTA run as one fused launch with many CTAs per
-// query.
+// Certified queries of at most uha::kFlatBatch on flat and small exact
+// indexes run as one fused launch with many CTAs per query (also the indexes
+// one CTA could scan: a CTA per query walks its rows one after another, which
+// at small batches leaves the GPU waiting on memory).
 bool flat_path_applies(const uha_index* index, uha_strategy strategy, uint64_t batch)
 {
     return strategy == UHA_DIRECT && index->kind != IndexKind::hierarchical &&
-           !uha::small_query_fits(index->rows, index->padded_dim) &&
            uha::flat_query_fits(index->rows, index->padded_dim, batch);
 }
 
@@ -1182,7 +1182,7 @@ void enqueue_hierarchical_projection(const uha_index* index, uha_workspace* ws,
 uha::LowpPlan enqueue_lowp_scores(const uha_index* index, uha_workspace* ws,
                                   uha_strategy strategy, uint64_t n, bool time_scan,
                                   cudaEvent_t scan_start, cudaEvent_t scan_stop,
-                                  const float* prepared = nullptr)
+                                  const float* prepared = nullptr, bool scores = true)
 {
     cudaStream_t stream = ws->stream;
     const uha::LowpType type = lowp_type(strategy);
@@ -1197,6 +1197,9 @@ uha::LowpPlan enqueue_lowp_scores(const uha_index* index, uha_workspace* ws,
                                    ? tuned->lowp_plan
                                    : uha::plan_lowp(type, index->rows, lp.pitch, n,
                                                     index->sm_count);
+    if (!scores) {
+        return plan;  // the caller sizes the partials for its selection
+    }
     const uint64_t partial_count =
         checked_mul(checked_mul(plan.splits, n, "partials"), index->rows, "partials");
     if (ws->partials.size() < partial_count) {
@@ -1214,6 +1217,94 @@ uha::LowpPlan enqueue_lowp_scores(const uha_index* index, uha_workspace* ws,
         check_cuda(cudaEventRecord(scan_stop, stream), "event");
     }
     return plan;
+}
+
+// Whether a batch of n takes the fused selection: plans of one K split on
+// indexes of at least kFilterMinRows rows, up to 64 candidates, on the
+// workspace stream (not pipelined), and not turned off for this call.
+bool filter_applies(const BatchContext& c, const uha::LowpPlan& plan, uint32_t k)
+{
+    return c.filter_candidates && !c.ws->filter_disabled && c.finish_stream == nullptr &&
+           plan.splits == 1 && c.index->rows >= uha::kFilterMinRows && k >= 1 && k <= 64;
+}
+
+// The k candidates per query of a precision strategy into `candidates`; the
+// rounded queries are in ws->queries_lp. The slab path stores every partial
+// score and selects from the slab. The fused path scores the first sample
+// rows the same way (bit-identical estimates: the same plan and tiles), takes
+// each query's k-th smallest estimate as its threshold, and scores all rows
+// with the filter epilogue, which keeps only the keys at or below the
+// threshold; the selection over those keys gives the slab path's candidates.
+// Returns the kernel launches.
+uint64_t enqueue_lowp_candidates(const BatchContext& c, uint64_t n, const uha::LowpPlan& plan,
+                                 uint32_t k, uint32_t* candidates, bool time_scan,
+                                 cudaEvent_t scan_start, cudaEvent_t scan_stop)
+{
+    const uha_index* index = c.index;
+    uha_workspace* ws = c.ws;
+    cudaStream_t stream = ws->stream;
+    const uha::LowpType type = lowp_type(c.strategy);
+    const uha::LowpRows& lp = lowp_rows(index, type, stream);
+    const float* norms = index->lowp[static_cast<int>(type)].norms.get();
+    int* error_flag = reinterpret_cast<int*>(ws->counters.get() + 1);
+    const uint32_t b = static_cast<uint32_t>(n);
+    const uint32_t rows = static_cast<uint32_t>(index->rows);
+    const bool fused = filter_applies(c, plan, k);
+    // the slab path's partial scores, or the fused path's sample slab
+    const uint64_t partial_count =
+        fused ? checked_mul(n, uha::filter_sample_rows(index->rows), "partials")
+              : checked_mul(checked_mul(plan.splits, n, "partials"), index->rows, "partials");
+    if (ws->partials.size() < partial_count) {
+        check_cuda(cudaStreamSynchronize(stream), "CUDA query failed");
+        ws->partials.allocate(partial_count);
+    }
+    if (!fused) {
+        if (time_scan) {
+            check_cuda(cudaEventRecord(scan_start, stream), "event");
+        }
+        uha::launch_lowp_scores(plan, type, lp.data.get(), lp.scales.get(), index->rows,
+                                ws->queries_lp.get(), ws->query_scales.get(), n, lp.pitch,
+                                ws->partials.get(), error_flag, stream);
+        if (time_scan) {
+            check_cuda(cudaEventRecord(scan_stop, stream), "event");
+        }
+        uha::launch_lowp_topk(ws->partials.get(), plan.splits, b, rows, norms, k, candidates,
+                              stream);
+        return 2;
+    }
+    const uint64_t sample = uha::filter_sample_rows(index->rows);
+    const uint32_t cap = uha::filter_capacity(index->rows, k);
+    if (ws->filter_keys.size() < ws->max_batch * cap) {
+        check_cuda(cudaStreamSynchronize(stream), "CUDA query failed");
+        ws->filter_keys.allocate(checked_mul(ws->max_batch, cap, "candidate lists"));
+        ws->filter_count.allocate(ws->max_batch);
+        ws->filter_tau.allocate(ws->max_batch);
+        ws->filter_sample.allocate(ws->max_batch * 64);
+    }
+    if (time_scan) {
+        check_cuda(cudaEventRecord(scan_start, stream), "event");
+    }
+    // the sample's one slab (fits the partials of the full plan)
+    uha::launch_lowp_scores(plan, type, lp.data.get(), lp.scales.get(), sample,
+                            ws->queries_lp.get(), ws->query_scales.get(), n, lp.pitch,
+                            ws->partials.get(), error_flag, stream);
+    uha::launch_lowp_topk(ws->partials.get(), 1, b, static_cast<uint32_t>(sample), norms, k,
+                          ws->filter_sample.get(), stream);
+    uha::launch_lowp_threshold(ws->partials.get(), b, static_cast<uint32_t>(sample), norms, k,
+                               ws->filter_sample.get(), ws->filter_tau.get(), stream);
+    check_cuda(cudaMemsetAsync(ws->filter_count.get(), 0, n * sizeof(uint32_t), stream),
+               "cannot clear candidate counts");
+    const uha::FilterArgs filter{norms, ws->filter_tau.get(), ws->filter_keys.get(),
+                                 ws->filter_count.get(), cap};
+    uha::launch_lowp_scores(plan, type, lp.data.get(), lp.scales.get(), index->rows,
+                            ws->queries_lp.get(), ws->query_scales.get(), n, lp.pitch,
+                            nullptr, error_flag, stream, &filter);
+    uha::launch_lowp_select(ws->filter_keys.get(), ws->filter_count.get(), cap, b, k,
+                            candidates, error_flag, stream);
+    if (time_scan) {
+        check_cuda(cudaEventRecord(scan_stop, stream), "event");
+    }
+    return 5;
 }
 
 // One query batch's kernels on the workspace stream: gather / copy with
@@ -1487,15 +1578,13 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
 
     if (precision_strategy(c.strategy)) {
         const uha::LowpPlan plan =
-            enqueue_lowp_scores(index, ws, c.strategy, n, time_scan, scan_start, scan_stop,
-                                hierarchical ? scan_queries : prepared);
+            enqueue_lowp_scores(index, ws, c.strategy, n, false, nullptr, nullptr,
+                                hierarchical ? scan_queries : prepared, false);
         const uint32_t k = static_cast<uint32_t>(
             std::min<uint64_t>(ws->candidates_per_query, index->rows));
         uint32_t* candidates = c.candidates != nullptr ? c.candidates : ws->candidates.get();
-        uha::launch_lowp_topk(ws->partials.get(), plan.splits, static_cast<uint32_t>(n),
-                              static_cast<uint32_t>(index->rows),
-                              index->lowp[static_cast<int>(lowp_type(c.strategy))].norms.get(),
-                              k, candidates, stream);
+        launches += enqueue_lowp_candidates(c, n, plan, k, candidates, time_scan, scan_start,
+                                            scan_stop) - 2;
         if (hierarchical) {
             // the reference's binary64 distance of every candidate, in the
             // projected space; the smallest (lowest row on ties) is the answer
@@ -1648,6 +1737,12 @@ void finish_call(const uha_index* index, uha_workspace* ws, uint64_t n,
     const uint32_t flag = ws->host_counters.get()[1];
     if (flag & 8u) {
         fail(UHA_RUNTIME_ERROR, "tensor-core pipeline wait timed out");
+    }
+    if (flag & 16u) {
+        fail(UHA_RUNTIME_ERROR, "flat query row copy wait timed out");
+    }
+    if (flag & static_cast<uint32_t>(uha::kCandidateOverflow)) {
+        fail(UHA_RUNTIME_ERROR, "filtered candidate list overflowed");
     }
     if (flag != 0) {
         if ((flag & 1u) && index->kind == IndexKind::hierarchical) {
@@ -1835,7 +1930,8 @@ extern "C" uha_status uha_query_many(const uha_index* index, uha_workspace* ws,
         }
         check_cuda(cudaMemsetAsync(ws->counters.get(), 0, ws->counters.bytes(), stream),
                    "cannot clear query counters");
-        const BatchContext ctx{index, ws, strategy, out_distances != nullptr};
+        BatchContext ctx{index, ws, strategy, out_distances != nullptr};
+        ctx.filter_candidates = true;
         const bool pipelined = pipeline_applies(index, strategy, batch, batches);
         if (pipelined) {
             prepare_pipeline(index, ws, strategy, batch);
@@ -1918,6 +2014,20 @@ extern "C" uha_status uha_query_many(const uha_index* index, uha_workspace* ws,
             ws->last.device_ms = ms;
         }
         ws->last.kernel_launches = launches;
+        if ((ws->host_counters.get()[1] & uha::kCandidateOverflow) != 0u &&
+            !ws->filter_disabled) {
+            // a query's filtered candidate list overflowed: answer the whole
+            // call again with the slab selection
+            ws->filter_disabled = true;
+            const uha_status again =
+                uha_query_many(index, ws, queries, query_count, batch, queries_on_device,
+                               strategy, out_indices, out_distances);
+            ws->filter_disabled = false;
+            if (again != UHA_OK) {
+                fail(again, uha_last_error());
+            }
+            return;
+        }
         finish_call(index, ws, n, ws->host_results.get(), ws->host_exact.get(),
                     out_indices, out_distances);
     });

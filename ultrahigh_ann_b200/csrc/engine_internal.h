@@ -39,6 +39,10 @@ struct BatchContext {
     uint32_t* rescore_done = nullptr;
     cudaStream_t finish_stream = nullptr;
     cudaEvent_t handoff = nullptr;
+    // The precision strategies may take the fused candidate selection: the
+    // caller answers the call again without it when a candidate list
+    // overflows (error bit uha::kCandidateOverflow).
+    bool filter_candidates = false;
 };
 
 // Enqueues one batch of n queries (`source`: device, n x dimension floats) on

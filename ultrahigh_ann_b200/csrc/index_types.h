@@ -114,6 +114,13 @@ struct uha_workspace {
     uha::DeviceBuffer<unsigned char> queries_lp;  // lowp_padded_count(max_batch) vectors
     uha::DeviceBuffer<float> query_scales;        // FP8 scale per query
     uha::DeviceBuffer<unsigned int> query_amax;   // FP8 max |x| bits per query
+    // fused candidate selection (allocated on first use): per-query key
+    // lists, their counts and thresholds, the sample's candidates
+    uha::DeviceBuffer<unsigned long long> filter_keys;
+    uha::DeviceBuffer<uint32_t> filter_count;
+    uha::DeviceBuffer<float> filter_tau;
+    uha::DeviceBuffer<uint32_t> filter_sample;
+    bool filter_disabled = false;  // answering again after an overflow
     uha::DeviceBuffer<uint32_t> candidates;       // [batch][candidates_per_query]
     uha::DeviceBuffer<double> cand_dist;          // [batch][candidates_per_query]
     uha::DeviceBuffer<uint32_t> rescore_done;     // per query, zero between calls

@@ -176,10 +176,12 @@ void launch_small_query(const SmallQuery& sq, uint32_t batch, Bound bound, Repla
 constexpr uint64_t kFlatColumns = 8192;
 constexpr uint64_t kFlatBatch = 8;
 struct FlatPlan {
-    uint32_t lanes;   // lanes per row: 8, 16 or 32
-    uint32_t span;    // rows per CTA
-    uint32_t blocks;  // CTAs per query
-    uint32_t depth;   // longest chain of binary32 additions per distance
+    uint32_t lanes;       // lanes per row: 8, 16 or 32
+    uint32_t span;        // rows per CTA
+    uint32_t blocks;      // CTAs per query
+    uint32_t depth;       // longest chain of binary32 additions per distance
+    uint32_t chunk_rows;  // rows per bulk copy into shared memory
+    uint32_t buffers;     // copy buffers per CTA (1 when a span is one chunk)
 };
 bool flat_query_fits(uint64_t rows, uint64_t padded_dim, uint64_t batch);
 FlatPlan plan_flat_query(uint64_t rows, uint64_t padded_dim, uint64_t batch,
@@ -239,13 +241,46 @@ LowpPlan lowp_plan(LowpType type, uint64_t pitch, int bn, uint64_t splits);
 // Plans the autotuner times for one (index, batch): the heuristic plan first.
 std::vector<LowpPlan> lowp_candidates(LowpType type, uint64_t rows, uint64_t pitch,
                                       uint64_t batch, int sm_count);
+// The candidate filter fused into the score kernel (plans of one K split):
+// keys (e, row) of the rows whose estimate e = ||v~||^2 - 2 S is at most
+// tau[q] are appended to keys[q][0 .. cap); count[q] (zero before) counts
+// them all.
+struct FilterArgs {
+    const float* norms;        // rounded-row norms ||v~||^2
+    const float* tau;          // per query
+    unsigned long long* keys;  // batch x cap
+    uint32_t* count;           // batch
+    uint32_t cap;
+};
 // partials[split][q][row] = q~ . v~ over the split's K slices (FP8: times the
-// row and query scales). error_flag |= 8 when a pipeline wait ran out.
+// row and query scales), or with `filter` (one K split) the filter's keys in
+// place of the slab. error_flag |= 8 when a pipeline wait ran out.
 void launch_lowp_scores(const LowpPlan& plan, LowpType type, const void* rows_lp,
                         const float* row_scale, uint64_t row_count,
                         const void* queries_lp, const float* query_scale,
                         uint64_t batch, uint64_t pitch, float* partials,
-                        int* error_flag, cudaStream_t stream);
+                        int* error_flag, cudaStream_t stream,
+                        const FilterArgs* filter = nullptr);
+// The fused selection: sample rows (the first ones, whole tiles) whose k-th
+// smallest estimate bounds each query's threshold, and the list capacity.
+// A query whose list overflows sets error bit kCandidateOverflow; the call
+// is then answered again by the slab path.
+constexpr uint64_t kFilterMinRows = 16384;
+constexpr int kCandidateOverflow = 32;
+uint64_t filter_sample_rows(uint64_t rows);
+uint32_t filter_capacity(uint64_t rows, uint32_t k);
+// tau[q] = the estimate of sample_candidates[q * k + k - 1] over the sample's
+// one-slab partials (+inf when the sample has fewer than k rows).
+void launch_lowp_threshold(const float* partials, uint32_t batch, uint32_t sample_rows,
+                           const float* norms, uint32_t k,
+                           const uint32_t* sample_candidates, float* tau,
+                           cudaStream_t stream);
+// candidates[q * k + i]: the k smallest keys of the query's list (the same
+// rows and order as launch_lowp_topk over the whole slab); count[q] > cap
+// sets error bit kCandidateOverflow.
+void launch_lowp_select(const unsigned long long* keys, const uint32_t* count, uint32_t cap,
+                        uint32_t batch, uint32_t k, uint32_t* candidates, int* error_flag,
+                        cudaStream_t stream);
 // candidates[q * k + i]: the k rows with the smallest ||v~||^2 - 2 S
 // (ascending, lowest row on ties; 0xffffffff past the index's rows).
 void launch_lowp_topk(const float* partials, uint32_t splits, uint32_t batch,

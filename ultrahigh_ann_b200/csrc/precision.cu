@@ -22,6 +22,7 @@
 //               scores [split][query][row]
 // Every mbarrier wait is bounded; a wait that runs out sets bit 8 of the
 // error flag and the CTA drains its pipeline (bounded) and returns.
+#include "async_copy.cuh"
 #include "common.h"
 #include "kernels.h"
 
@@ -45,48 +46,14 @@ constexpr int kPipelineTimeout = 8;   // error-flag bit
 
 // ------------------------------------------------------------ PTX helpers
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p)
-{
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)),
-                 "r"(count)
-                 : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
-                     smem_u32(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
-{
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return done != 0;
-}
+using async::mbar_expect_tx;
+using async::mbar_init;
+using async::smem_u32;
 
 // Waits for the phase of `parity` to complete; false after kSpinLimit tries.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
 {
-    for (uint32_t i = 0; i < kSpinLimit; ++i) {
-        if (mbar_try_wait(bar, parity)) {
-            return true;
-        }
-    }
-    return false;
+    return async::mbar_wait(bar, parity, kSpinLimit);
 }
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map,
@@ -185,6 +152,14 @@ __device__ __forceinline__ void tmem_load16(uint32_t addr, float (&v)[16])
     }
 }
 
+// Unsigned key bits that order like the binary32 value (negative values
+// below positive ones).
+__device__ __forceinline__ unsigned int ordered_key_bits(float f)
+{
+    const unsigned int u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
 template <int BN, int STAGES>
 struct GemmSmem {
     static constexpr uint32_t a_bytes = kTileRows * kSliceBytes;
@@ -198,13 +173,20 @@ struct GemmSmem {
 // Partial scores of one (row tile, query tile, K split):
 // partials[split][q][row] = sum over the split's K range of q~ . v~ (times
 // the row and query scales for FP8).
-template <int BN, int STAGES, bool FP8>
+//
+// With FILTER (one K split only) nothing is stored per score: the epilogue
+// forms the estimate e = ||v~||^2 - 2 S exactly as the candidate selection
+// does and appends the key (e, row) of every row with e <= f.tau[q] to the
+// query's list f.keys[q][0 .. f.cap) (f.count[q] counts them all, also past
+// the capacity).
+template <int BN, int STAGES, bool FP8, bool FILTER>
 __global__ void __launch_bounds__(kGemmThreads, 1)
     lowp_score_kernel(const __grid_constant__ CUtensorMap rows_map,
                       const __grid_constant__ CUtensorMap queries_map,
                       uint32_t kblocks, uint32_t kblocks_per_split,
                       uint32_t row_count, uint32_t batch, const float* row_scale,
-                      const float* query_scale, float* partials, int* error_flag)
+                      const float* query_scale, float* partials, FilterArgs f,
+                      int* error_flag)
 {
     using L = GemmSmem<BN, STAGES>;
     extern __shared__ unsigned char smem_raw[];
@@ -315,6 +297,47 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         if (!ready) {
             if (lane == 0) {
                 atomicOr(error_flag, kPipelineTimeout);
+            }
+        } else if (store && FILTER) {
+            const uint32_t row = static_cast<uint32_t>(row0) + quarter + lane;
+            const bool row_ok = row < row_count;
+            const float rs = FP8 && row_ok ? row_scale[row] : 1.f;
+            const float norm = row_ok ? f.norms[row] : 0.f;
+#pragma unroll 1
+            for (int c = 0; c < BN; c += 16) {
+                float v[16];
+                tmem_load16(tmem + (quarter << 16) + static_cast<uint32_t>(c), v);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const uint32_t q = static_cast<uint32_t>(q0 + c + j);
+                    bool pass = false;
+                    unsigned long long key = 0;
+                    if (row_ok && q < batch) {
+                        const float value =
+                            FP8 ? __fmul_rn(__fmul_rn(v[j], rs), query_scale[q]) : v[j];
+                        // the selection sums one slab from zero: 0 + value
+                        const float est = __fmaf_rn(-2.f, 0.f + value, norm);
+                        pass = est <= f.tau[q];
+                        key = (static_cast<unsigned long long>(ordered_key_bits(est)) << 32) |
+                              row;
+                    }
+                    const unsigned int mask = __ballot_sync(0xffffffffu, pass);
+                    if (mask != 0u) {
+                        const int leader = __ffs(mask) - 1;
+                        uint32_t base = 0;
+                        if (lane == leader) {
+                            base = atomicAdd(f.count + q, static_cast<uint32_t>(__popc(mask)));
+                        }
+                        base = __shfl_sync(0xffffffffu, base, leader);
+                        if (pass) {
+                            const uint32_t slot =
+                                base + static_cast<uint32_t>(__popc(mask & ((1u << lane) - 1u)));
+                            if (slot < f.cap) {
+                                f.keys[static_cast<uint64_t>(q) * f.cap + slot] = key;
+                            }
+                        }
+                    }
+                }
             }
         } else if (store) {
             const uint32_t row = static_cast<uint32_t>(row0) + quarter + lane;
@@ -530,12 +553,6 @@ __global__ void __launch_bounds__(kQueryThreads)
 }
 
 // ---------------------------------------------------------------- top-k
-
-__device__ __forceinline__ unsigned int ordered_key_bits(float f)
-{
-    const unsigned int u = __float_as_uint(f);
-    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-}
 
 template <int KCAP>
 __device__ __forceinline__ void keep_smallest(unsigned long long (&best)[KCAP],
@@ -783,6 +800,73 @@ __global__ void __launch_bounds__(kTopkThreads)
     }
 }
 
+// tau[q]: the estimate of the query's k-th candidate over the sample's one
+// slab (the selection's own arithmetic: 0 + S, then the FMA with the norm).
+__global__ void threshold_kernel(const float* __restrict__ partials, uint32_t batch,
+                                 uint32_t rows, const float* __restrict__ norms, uint32_t k,
+                                 const uint32_t* __restrict__ candidates,
+                                 float* __restrict__ tau)
+{
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= batch) {
+        return;
+    }
+    const uint32_t row = candidates[static_cast<uint64_t>(q) * k + k - 1];
+    float t = __int_as_float(0x7f800000);
+    if (row != 0xffffffffu) {
+        const float dot = 0.f + partials[static_cast<uint64_t>(q) * rows + row];
+        t = __fmaf_rn(-2.f, dot, norms[row]);
+    }
+    tau[q] = t;
+}
+
+// One block per query: the k smallest keys of the query's filtered list,
+// ascending (the keys order by estimate, then row, as the slab selection's).
+template <int KCAP>
+__global__ void __launch_bounds__(kTopkThreads)
+    select_kernel(const unsigned long long* __restrict__ keys,
+                  const uint32_t* __restrict__ count, uint32_t cap, uint32_t k,
+                  uint32_t* __restrict__ candidates, int* error_flag)
+{
+    __shared__ unsigned long long lists[kTopkThreads / 32][KCAP];
+    __shared__ unsigned long long final_list[KCAP];
+    const uint32_t q = blockIdx.x;
+    const int warp = threadIdx.x / 32;
+    const int lane = threadIdx.x % 32;
+    const uint32_t total = count[q];
+    if (total > cap && threadIdx.x == 0) {
+        atomicOr(error_flag, kCandidateOverflow);
+    }
+    const uint32_t n = min(total, cap);
+    unsigned long long best[KCAP];
+#pragma unroll
+    for (int i = 0; i < KCAP; ++i) {
+        best[i] = ~0ull;
+    }
+    const unsigned long long* list = keys + static_cast<uint64_t>(q) * cap;
+    for (uint32_t i = threadIdx.x; i < n; i += kTopkThreads) {
+        keep_smallest(best, list[i]);
+    }
+    warp_merge(best, lists[warp], lane);
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int i = 0; i < KCAP; ++i) {
+            best[i] = ~0ull;
+        }
+        for (int i = lane; i < (kTopkThreads / 32) * KCAP; i += 32) {
+            keep_smallest(best, lists[i / KCAP][i % KCAP]);
+        }
+        warp_merge(best, final_list, lane);
+        __syncwarp();
+        for (uint32_t i = lane; i < k; i += 32) {
+            const unsigned long long key = final_list[i];
+            candidates[static_cast<uint64_t>(q) * k + i] =
+                key == ~0ull ? 0xffffffffu : static_cast<uint32_t>(key & 0xffffffffu);
+        }
+    }
+}
+
 // ------------------------------------------------------------ host side
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
@@ -829,15 +913,15 @@ CUtensorMap make_map(const void* base, bool fp8, uint64_t pitch, uint64_t outer,
     return map;
 }
 
-template <int BN, int STAGES, bool FP8>
-void launch_gemm_instance(const LowpPlan& plan, const CUtensorMap& rows_map,
+template <int BN, int STAGES, bool FP8, bool FILTER>
+void launch_gemm_filtered(const LowpPlan& plan, const CUtensorMap& rows_map,
                           const CUtensorMap& queries_map, uint32_t row_count,
                           uint32_t batch, const float* row_scale,
-                          const float* query_scale, float* partials, int* error_flag,
-                          cudaStream_t stream)
+                          const float* query_scale, float* partials, const FilterArgs& f,
+                          int* error_flag, cudaStream_t stream)
 {
     using L = GemmSmem<BN, STAGES>;
-    auto kernel = lowp_score_kernel<BN, STAGES, FP8>;
+    auto kernel = lowp_score_kernel<BN, STAGES, FP8, FILTER>;
     static std::once_flag once[kMaxDevices];
     std::call_once(once[current_device()], [&] {
         check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -849,15 +933,34 @@ void launch_gemm_instance(const LowpPlan& plan, const CUtensorMap& rows_map,
     kernel<<<grid, kGemmThreads, L::total, stream>>>(rows_map, queries_map, plan.kblocks,
                                                       plan.kblocks_per_split, row_count,
                                                       batch, row_scale, query_scale,
-                                                      partials, error_flag);
+                                                      partials, f, error_flag);
     check_cuda(cudaGetLastError(), "cannot launch the tensor-core score kernel");
+}
+
+template <int BN, int STAGES, bool FP8>
+void launch_gemm_instance(const LowpPlan& plan, const CUtensorMap& rows_map,
+                          const CUtensorMap& queries_map, uint32_t row_count,
+                          uint32_t batch, const float* row_scale,
+                          const float* query_scale, float* partials,
+                          const FilterArgs* filter, int* error_flag, cudaStream_t stream)
+{
+    if (filter != nullptr) {
+        launch_gemm_filtered<BN, STAGES, FP8, true>(plan, rows_map, queries_map, row_count,
+                                                    batch, row_scale, query_scale, partials,
+                                                    *filter, error_flag, stream);
+    } else {
+        launch_gemm_filtered<BN, STAGES, FP8, false>(plan, rows_map, queries_map, row_count,
+                                                     batch, row_scale, query_scale, partials,
+                                                     FilterArgs{}, error_flag, stream);
+    }
 }
 
 template <bool FP8>
 void launch_gemm_typed(const LowpPlan& plan, const CUtensorMap& rows_map,
                        const void* queries, uint64_t pitch, uint32_t row_count,
                        uint32_t batch, const float* row_scale, const float* query_scale,
-                       float* partials, int* error_flag, cudaStream_t stream)
+                       float* partials, const FilterArgs* filter, int* error_flag,
+                       cudaStream_t stream)
 {
     // the query buffer holds lowp_padded_count(batch) vectors: every box is
     // inside it (the vectors past `batch` are computed and not stored)
@@ -867,28 +970,28 @@ void launch_gemm_typed(const LowpPlan& plan, const CUtensorMap& rows_map,
     switch (plan.bn) {
     case 16:
         launch_gemm_instance<16, 8, FP8>(plan, rows_map, queries_map, row_count, batch,
-                                         row_scale, query_scale, partials, error_flag,
-                                         stream);
+                                         row_scale, query_scale, partials, filter,
+                                         error_flag, stream);
         break;
     case 32:
         launch_gemm_instance<32, 8, FP8>(plan, rows_map, queries_map, row_count, batch,
-                                         row_scale, query_scale, partials, error_flag,
-                                         stream);
+                                         row_scale, query_scale, partials, filter,
+                                         error_flag, stream);
         break;
     case 64:
         launch_gemm_instance<64, 8, FP8>(plan, rows_map, queries_map, row_count, batch,
-                                         row_scale, query_scale, partials, error_flag,
-                                         stream);
+                                         row_scale, query_scale, partials, filter,
+                                         error_flag, stream);
         break;
     case 128:
         launch_gemm_instance<128, 6, FP8>(plan, rows_map, queries_map, row_count, batch,
-                                          row_scale, query_scale, partials, error_flag,
-                                          stream);
+                                          row_scale, query_scale, partials, filter,
+                                          error_flag, stream);
         break;
     default:
         launch_gemm_instance<256, 4, FP8>(plan, rows_map, queries_map, row_count, batch,
-                                          row_scale, query_scale, partials, error_flag,
-                                          stream);
+                                          row_scale, query_scale, partials, filter,
+                                          error_flag, stream);
         break;
     }
 }
@@ -1033,8 +1136,11 @@ void launch_lowp_scores(const LowpPlan& plan, LowpType type, const void* rows_lp
                         const float* row_scale, uint64_t row_count,
                         const void* queries_lp, const float* query_scale,
                         uint64_t batch, uint64_t pitch, float* partials,
-                        int* error_flag, cudaStream_t stream)
+                        int* error_flag, cudaStream_t stream, const FilterArgs* filter)
 {
+    if (filter != nullptr && plan.splits != 1) {
+        fail(UHA_LOGIC_ERROR, "the fused candidate filter needs one K split");
+    }
     const bool fp8 = type == LowpType::fp8_e4m3;
     // the row buffer holds lowp_padded_count(row_count) vectors (zero past
     // row_count), so no box leaves it
@@ -1044,12 +1150,12 @@ void launch_lowp_scores(const LowpPlan& plan, LowpType type, const void* rows_lp
         launch_gemm_typed<true>(plan, rows_map, queries_lp, pitch,
                                 static_cast<uint32_t>(row_count),
                                 static_cast<uint32_t>(batch), row_scale, query_scale,
-                                partials, error_flag, stream);
+                                partials, filter, error_flag, stream);
     } else {
         launch_gemm_typed<false>(plan, rows_map, queries_lp, pitch,
                                  static_cast<uint32_t>(row_count),
                                  static_cast<uint32_t>(batch), row_scale, query_scale,
-                                 partials, error_flag, stream);
+                                 partials, filter, error_flag, stream);
     }
 }
 
@@ -1078,6 +1184,59 @@ void launch_lowp_topk(const float* partials, uint32_t splits, uint32_t batch,
                                                             norms, k, candidates);
     }
     check_cuda(cudaGetLastError(), "cannot launch the candidate selection kernel");
+}
+
+uint64_t filter_sample_rows(uint64_t rows)
+{
+    // about a sixteenth of the rows in whole tiles: about 16 k keys per query
+    // pass the threshold
+    const uint64_t s = rows / 16 / kTileRows * kTileRows;
+    return std::min<uint64_t>(rows, std::max<uint64_t>(s, 1024));
+}
+
+uint32_t filter_capacity(uint64_t rows, uint32_t k)
+{
+    // four times the expected list length, at least 2,048
+    const uint64_t expected = static_cast<uint64_t>(k) *
+                              ((rows + filter_sample_rows(rows) - 1) / filter_sample_rows(rows));
+    return static_cast<uint32_t>(std::max<uint64_t>(2048, 4 * expected));
+}
+
+void launch_lowp_threshold(const float* partials, uint32_t batch, uint32_t sample_rows,
+                           const float* norms, uint32_t k,
+                           const uint32_t* sample_candidates, float* tau,
+                           cudaStream_t stream)
+{
+    if (batch == 0) {
+        return;
+    }
+    threshold_kernel<<<(batch + 255) / 256, 256, 0, stream>>>(partials, batch, sample_rows,
+                                                              norms, k, sample_candidates,
+                                                              tau);
+    check_cuda(cudaGetLastError(), "cannot launch the candidate threshold kernel");
+}
+
+void launch_lowp_select(const unsigned long long* keys, const uint32_t* count, uint32_t cap,
+                        uint32_t batch, uint32_t k, uint32_t* candidates, int* error_flag,
+                        cudaStream_t stream)
+{
+    if (batch == 0) {
+        return;
+    }
+    if (k <= 8) {
+        select_kernel<8><<<batch, kTopkThreads, 0, stream>>>(keys, count, cap, k, candidates,
+                                                            error_flag);
+    } else if (k <= 16) {
+        select_kernel<16><<<batch, kTopkThreads, 0, stream>>>(keys, count, cap, k,
+                                                             candidates, error_flag);
+    } else if (k <= 32) {
+        select_kernel<32><<<batch, kTopkThreads, 0, stream>>>(keys, count, cap, k,
+                                                             candidates, error_flag);
+    } else {
+        select_kernel<64><<<batch, kTopkThreads, 0, stream>>>(keys, count, cap, k,
+                                                             candidates, error_flag);
+    }
+    check_cuda(cudaGetLastError(), "cannot launch the filtered selection kernel");
 }
 
 }  // namespace uha

@@ -1,8 +1,8 @@
-// The persistent multi-index batch kernel (certify.cu, launch_persistent_batch)
-// and the shapes of the stage kernels it stands in for.
+// The persistent multi-index batch kernels (certify.cu, launch_persistent_batch)
+// and the shapes of the stage kernels they stand in for.
 //
-// The kernel answers many (hierarchical index, query batch) pairs in one
-// cooperative launch: every CTA drains, stage after stage, a work list of
+// Two kernels answer many (hierarchical index, query batch) pairs, one
+// cooperative launch each: every CTA drains, stage after stage, a work list of
 // units drawn from all pairs (a unit is one block of the stage kernel that the
 // standalone path would launch for that pair, run by the same device code from
 // tile_body.cuh, hier_body.cuh and certify.cu, so both paths compute the same
@@ -11,9 +11,11 @@
 //   1 gather of the sampled coordinates          5 median survivors (L1), argmin (L2)
 //   2 binary32 projection with its error bound   6 argmin (L1), reported distances (L2)
 //   3 L2 tile scan + error root, median samples  7 reported distances (L1)
-// A barrier wait gives up after about two seconds, sets the batch status and
-// ends the kernel (every CTA then does the same at its next barrier), so a
-// fault can never hold the GPU.
+// Stages 0-3 run in the first kernel (the tile scan's register budget, 2 CTAs
+// per SM), stages 4-7 in the second (4 CTAs per SM). A barrier wait gives up
+// after about two seconds, sets the batch status and ends the kernel (every
+// CTA then does the same at its next barrier, and the second kernel returns
+// at once), so a fault can never hold the GPU.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -67,6 +69,9 @@ uint32_t refine_group_blocks(uint32_t batch);
 
 // ---- the persistent batch
 constexpr int kPersistentStages = 8;
+// stages [0, kPersistentSplit) run in the first kernel of a run, the rest in
+// the second
+constexpr int kPersistentSplit = 4;
 
 // Everything one pair's stages read and write (device pointers into the
 // pair's workspace and index).
@@ -137,7 +142,7 @@ struct PersistentPlan {
     // and at the end of each stage, as CTA 0 sees them (after each barrier;
     // the last entry when CTA 0 finishes its units of the last stage)
     unsigned long long* clock;
-    uint32_t smem_bytes;
+    uint32_t smem_bytes[2];  // dynamic shared memory of the two kernels
 };
 
 // Builds the segment list of `pairs` (host copies) into `segments` (room for
@@ -147,10 +152,12 @@ void plan_persistent_batch(const PersistentPair* pairs, uint32_t count,
                            PersistentSegment* segments, uint32_t* segment_count,
                            PersistentPlan* plan);
 uint32_t persistent_segment_capacity(uint32_t count);
-// CTAs of one cooperative launch on the current device for `smem_bytes` of
-// dynamic shared memory (all resident at once); 0 if it cannot be launched.
-uint32_t persistent_grid(uint32_t smem_bytes);
-// One cooperative launch of the persistent kernel (capturable in a graph).
-void launch_persistent_batch(const PersistentPlan& plan, uint32_t grid, cudaStream_t stream);
+// CTAs of one cooperative launch of kernel `part` (0: early stages, 1: late
+// stages) on the current device for `smem_bytes` of dynamic shared memory
+// (all resident at once); 0 if it cannot be launched.
+uint32_t persistent_grid(int part, uint32_t smem_bytes);
+// The run's two cooperative launches (capturable in a graph).
+void launch_persistent_batch(const PersistentPlan& plan, const uint32_t grid[2],
+                             cudaStream_t stream);
 
 }  // namespace uha
