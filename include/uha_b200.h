@@ -427,7 +427,8 @@ uha_status uha_batch_create(const uha_index* const* indexes,
  * UHA_RUNTIME_ERROR). Each unit runs the device code of the standalone
  * kernel it replaces, so each pair's answers equal a uha_query of the same
  * queries. Serves hierarchical indexes with the certified direct strategy
- * (projection dimension up to 256; L2 hierarchies with more than 8 queries);
+ * (projection dimension up to 256; L2 hierarchies with more than 8 queries;
+ * up to 32 pairs);
  * other pairs fail with UHA_INVALID_ARGUMENT. No reference counterpart. */
 uha_status uha_batch_create_persistent(const uha_index* const* indexes,
                                        const uint64_t* query_counts, uint64_t count,

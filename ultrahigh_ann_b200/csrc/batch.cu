@@ -300,13 +300,11 @@ struct uha_batch {
     uha_batch_stats last{};
     // persistent form
     bool persistent = false;
-    uha::DeviceBuffer<uha::PersistentPair> d_pairs;
-    uha::DeviceBuffer<uha::PersistentSegment> d_segments;
     uha::DeviceBuffer<unsigned int> barrier;  // [0] arrivals [1] generation [2] status
     uha::PinnedBuffer<int> host_status;
     uha::DeviceBuffer<unsigned long long> clock;  // stage boundaries (ns)
     uha::PinnedBuffer<unsigned long long> host_clock;
-    uha::PersistentPlan plan{};
+    std::unique_ptr<uha::PersistentParams> params;  // the kernels' parameter
     uint32_t grid[2] = {0, 0};  // CTAs of the two persistent kernels
 
     ~uha_batch()
@@ -389,12 +387,14 @@ void build_persistent(uha_batch* batch)
         pairs.push_back(d);
     }
     require(!pairs.empty(), UHA_INVALID_ARGUMENT, "the persistent batch has no work");
+    require(pairs.size() <= uha::kPersistentMaxPairs, UHA_INVALID_ARGUMENT,
+            "the persistent batch serves up to 32 pairs");
     const uint32_t count = static_cast<uint32_t>(pairs.size());
-    std::vector<uha::PersistentSegment> segments(uha::persistent_segment_capacity(count));
+    batch->params = std::make_unique<uha::PersistentParams>();
+    uha::PersistentParams& params = *batch->params;
     uint32_t used = 0;
-    uha::plan_persistent_batch(pairs.data(), count, segments.data(), &used, &batch->plan);
-    batch->d_pairs.allocate(count);
-    batch->d_segments.allocate(used);
+    uha::plan_persistent_batch(pairs.data(), count, params.segments, &used, &params.plan);
+    std::copy(pairs.begin(), pairs.end(), params.pairs);
     batch->barrier.allocate(3);
     batch->host_status.allocate(1);
     batch->host_status.get()[0] = 0;
@@ -402,23 +402,14 @@ void build_persistent(uha_batch* batch)
     batch->host_clock.allocate(uha::kPersistentStages + 1);
     std::fill(batch->host_clock.get(), batch->host_clock.get() + uha::kPersistentStages + 1,
               0ull);
-    check_cuda(cudaMemcpyAsync(batch->d_pairs.get(), pairs.data(), batch->d_pairs.bytes(),
-                               cudaMemcpyHostToDevice, batch->stream),
-               "cannot upload the persistent batch");
-    check_cuda(cudaMemcpyAsync(batch->d_segments.get(), segments.data(),
-                               used * sizeof(uha::PersistentSegment), cudaMemcpyHostToDevice,
-                               batch->stream),
-               "cannot upload the persistent batch");
     check_cuda(cudaMemsetAsync(batch->barrier.get(), 0, batch->barrier.bytes(), batch->stream),
                "cannot clear the persistent batch barrier");
-    check_cuda(cudaStreamSynchronize(batch->stream), "cannot upload the persistent batch");
-    batch->plan.pairs = batch->d_pairs.get();
-    batch->plan.segments = batch->d_segments.get();
-    batch->plan.barrier = batch->barrier.get();
-    batch->plan.status = reinterpret_cast<int*>(batch->barrier.get() + 2);
-    batch->plan.clock = batch->clock.get();
+    check_cuda(cudaStreamSynchronize(batch->stream), "cannot clear the persistent batch");
+    params.plan.barrier = batch->barrier.get();
+    params.plan.status = reinterpret_cast<int*>(batch->barrier.get() + 2);
+    params.plan.clock = batch->clock.get();
     for (int part = 0; part < 2; ++part) {
-        batch->grid[part] = uha::persistent_grid(part, batch->plan.smem_bytes[part]);
+        batch->grid[part] = uha::persistent_grid(part, params.plan.smem_bytes[part]);
         require(batch->grid[part] != 0, UHA_RUNTIME_ERROR,
                 "the persistent batch kernel cannot be resident with its shared memory");
     }
@@ -495,7 +486,7 @@ uha_status create_batch(const uha_index* const* indexes, const uint64_t* query_c
         uint64_t launches = 0;
         try {
             if (batch->persistent) {
-                uha::launch_persistent_batch(batch->plan, batch->grid, batch->stream);
+                uha::launch_persistent_batch(*batch->params, batch->grid, batch->stream);
                 launches = 2;
                 for (uha_batch::Pair& p : batch->pairs) {
                     if (p.trivial) {
@@ -515,7 +506,7 @@ uha_status create_batch(const uha_index* const* indexes, const uint64_t* query_c
                                                batch->stream),
                                "cannot copy query counters from the CUDA device");
                 }
-                check_cuda(cudaMemcpyAsync(batch->host_status.get(), batch->plan.status,
+                check_cuda(cudaMemcpyAsync(batch->host_status.get(), batch->params->plan.status,
                                            sizeof(int), cudaMemcpyDeviceToHost, batch->stream),
                            "cannot copy the persistent batch status");
                 check_cuda(cudaMemcpyAsync(batch->host_clock.get(), batch->clock.get(),

@@ -1273,6 +1273,8 @@ constexpr uint32_t kFlatCopySpins = 1u << 22;
 constexpr int kFlatCopyTimeout = 16;
 // bytes of rows per bulk copy of the flat query kernel (two buffers per CTA)
 constexpr uint64_t kFlatChunkBytes = 32 * 1024;
+// query entries a flat query thread gathers at a time
+constexpr int kFlatGather = 8;
 
 // Per-row accumulation of one lane: binary32, column order, four terms per
 // float4 group (the same arithmetic as small_query_kernel); the query and the
@@ -1369,24 +1371,53 @@ __global__ void __launch_bounds__(kFinalizeThreads, 3)
     __syncthreads();
     const float* src = sq.queries + static_cast<uint64_t>(q) * sq.dim;
     int local_bad = 0;
-    for (uint64_t i = threadIdx.x; i < sq.padded_dim; i += kFinalizeThreads) {
-        float v = 0.f;
-        if (sq.columns == nullptr) {
-            if (i < sq.dim) {
-                v = src[i];
-                local_bad |= isfinite(v) ? 0 : 1;
-            }
-        } else if (i < sq.sample_size) {
-            v = src[sq.columns[i]];
-            local_bad |= isfinite(v) ? 0 : 1;
-            if (sq.scales != nullptr) {
-                v = __fmul_rn(v, sq.scales[i]);
-                local_bad |= isfinite(v) ? 0 : 2;
+    // kFlatGather entries per thread at a time: their column indices (and
+    // scales, weights) in flight together, then their query values together,
+    // so the gather costs two memory round trips, not two per entry
+    for (uint64_t base = threadIdx.x; base < sq.padded_dim;
+         base += static_cast<uint64_t>(kFinalizeThreads) * kFlatGather) {
+        uint32_t col[kFlatGather];
+        float scale[kFlatGather];
+        float weight[kFlatGather];
+#pragma unroll
+        for (int u = 0; u < kFlatGather; ++u) {
+            const uint64_t i = base + static_cast<uint64_t>(u) * kFinalizeThreads;
+            const bool sampled = sq.columns != nullptr && i < sq.sample_size;
+            col[u] = sampled ? sq.columns[i] : 0u;
+            scale[u] = sampled && sq.scales != nullptr ? sq.scales[i] : 1.f;
+            weight[u] = weighted && i < sq.padded_dim ? sq.weights32[i] : 0.f;
+        }
+        float value[kFlatGather];
+#pragma unroll
+        for (int u = 0; u < kFlatGather; ++u) {
+            const uint64_t i = base + static_cast<uint64_t>(u) * kFinalizeThreads;
+            value[u] = 0.f;
+            if (sq.columns == nullptr) {
+                if (i < sq.dim) {
+                    value[u] = src[i];
+                }
+            } else if (i < sq.sample_size) {
+                value[u] = src[col[u]];
             }
         }
-        qv[i] = v;
-        if (weighted) {
-            wv[i] = sq.weights32[i];
+#pragma unroll
+        for (int u = 0; u < kFlatGather; ++u) {
+            const uint64_t i = base + static_cast<uint64_t>(u) * kFinalizeThreads;
+            if (i >= sq.padded_dim) {
+                continue;
+            }
+            float v = value[u];
+            if (sq.columns == nullptr ? i < sq.dim : i < sq.sample_size) {
+                local_bad |= isfinite(v) ? 0 : 1;
+                if (sq.columns != nullptr && sq.scales != nullptr) {
+                    v = __fmul_rn(v, scale[u]);
+                    local_bad |= isfinite(v) ? 0 : 2;
+                }
+            }
+            qv[i] = v;
+            if (weighted) {
+                wv[i] = weight[u];
+            }
         }
     }
     if (local_bad != 0) {
@@ -1507,16 +1538,25 @@ __global__ void __launch_bounds__(kFinalizeThreads, 3)
         }
         __threadfence();
         Summary m{inf, inf, inf, 0xffffffffu, inf};
-        for (uint32_t i = threadIdx.x; i < blocks; i += kFinalizeThreads) {
-            const volatile Summary* src_s =
-                block_summaries + static_cast<uint64_t>(q) * summary_stride + i;
-            Summary b;
-            b.min_upper = src_s->min_upper;
-            b.first = src_s->first;
-            b.second = src_s->second;
-            b.first_row = src_s->first_row;
-            b.first_distance = src_s->first_distance;
-            m = summary_merge(m, b);
+        // two summaries per thread in flight together
+        for (uint32_t i0 = threadIdx.x; i0 < blocks; i0 += 2 * kFinalizeThreads) {
+            Summary b[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const uint32_t i = i0 + u * kFinalizeThreads;
+                b[u] = Summary{inf, inf, inf, 0xffffffffu, inf};
+                if (i < blocks) {
+                    const volatile Summary* src_s =
+                        block_summaries + static_cast<uint64_t>(q) * summary_stride + i;
+                    b[u].min_upper = src_s->min_upper;
+                    b[u].first = src_s->first;
+                    b[u].second = src_s->second;
+                    b[u].first_row = src_s->first_row;
+                    b[u].first_distance = src_s->first_distance;
+                }
+            }
+            m = summary_merge(m, b[0]);
+            m = summary_merge(m, b[1]);
         }
         s = block_reduce_summary(m);
         if (threadIdx.x == 0) {
@@ -2074,7 +2114,7 @@ __device__ void persistent_unit(const PersistentPair& d, uint32_t kind, uint32_t
         break;
     }
     case kUnitSample: {
-        const MedianArgs a = d.median;
+        const MedianArgs& a = d.median;
         if (a.p <= 32) {
             persistent_sample<1>(a, u, units);
         } else if (a.p <= 64) {
@@ -2094,7 +2134,7 @@ __device__ void persistent_unit(const PersistentPair& d, uint32_t kind, uint32_t
     case kUnitCount: {
         // two count blocks per unit, one per half of the CTA (own barrier and
         // shared memory)
-        const MedianArgs a = d.median;
+        const MedianArgs& a = d.median;
         const uint32_t half = threadIdx.x / hierbody::kCountRows;
         const uint32_t b = 2 * u + half;
         if (b < d.count_gx * d.count_gy) {
@@ -2113,7 +2153,7 @@ __device__ void persistent_unit(const PersistentPair& d, uint32_t kind, uint32_t
         break;
     }
     case kUnitSurvivor: {
-        const MedianArgs a = d.median;
+        const MedianArgs& a = d.median;
         if (a.p <= 32) {
             persistent_survivor<1>(a, u, units);
         } else if (a.p <= 64) {
@@ -2126,19 +2166,14 @@ __device__ void persistent_unit(const PersistentPair& d, uint32_t kind, uint32_t
         break;
     }
     case kUnitArgmin: {
-        const PartialView view = d.view;
-        const Bound bound = d.bound;
-        const ReplayInputs in = d.replay;
-        argmin_block<false>(view, bound, in, d.results, d.exact_distances,
+        argmin_block<false>(d.view, d.bound, d.replay, d.results, d.exact_distances,
                             static_cast<Summary*>(d.summaries), d.done, d.counters,
                             d.argmin_span, u % d.argmin_gx, u / d.argmin_gx, d.argmin_gx,
                             reinterpret_cast<double*>(smem));
         break;
     }
     case kUnitRefine: {
-        const Bound bound = d.bound;
-        const ReplayInputs in = d.replay;
-        refine_group_block(in, bound, d.results, d.exact_distances, d.batch, u, smem);
+        refine_group_block(d.replay, d.bound, d.results, d.exact_distances, d.batch, u, smem);
         break;
     }
     default:
@@ -2162,9 +2197,10 @@ __device__ __forceinline__ unsigned long long global_timer_ns()
 
 template <int kFirst, int kEnd, int kMinBlocks>
 __global__ void __launch_bounds__(kFinalizeThreads, kMinBlocks)
-    persistent_stages_kernel(PersistentPlan plan)
+    persistent_stages_kernel(const __grid_constant__ PersistentParams params)
 {
     extern __shared__ __align__(16) unsigned char persistent_smem[];
+    const PersistentPlan& plan = params.plan;
     if (*static_cast<volatile int*>(plan.status) != 0) {
         return;  // the earlier kernel of this run gave up
     }
@@ -2177,11 +2213,11 @@ __global__ void __launch_bounds__(kFinalizeThreads, kMinBlocks)
         const uint32_t seg_end = plan.stage_begin[stage + 1];
         uint32_t seg = plan.stage_begin[stage];
         for (uint32_t u = blockIdx.x; u < units; u += gridDim.x) {
-            while (seg + 1 < seg_end && plan.segments[seg + 1].first <= u) {
+            while (seg + 1 < seg_end && params.segments[seg + 1].first <= u) {
                 ++seg;
             }
-            const PersistentSegment sg = plan.segments[seg];
-            persistent_unit<(kFirst >= kPersistentSplit)>(plan.pairs[sg.pair], sg.kind,
+            const PersistentSegment sg = params.segments[seg];
+            persistent_unit<(kFirst >= kPersistentSplit)>(params.pairs[sg.pair], sg.kind,
                                                           u - sg.first, sg.units,
                                                           persistent_smem);
             __syncthreads();
@@ -2745,9 +2781,10 @@ uint32_t persistent_grid(int part, uint32_t smem_bytes)
     return static_cast<uint32_t>(std::max(0, per_sm) * sms);
 }
 
-void launch_persistent_batch(const PersistentPlan& plan, const uint32_t grid[2],
+void launch_persistent_batch(const PersistentParams& params, const uint32_t grid[2],
                              cudaStream_t stream)
 {
+    const PersistentPlan& plan = params.plan;
     for (int part = 0; part < 2; ++part) {
         const void* kernel = persistent_kernel(part);
         set_dynamic_smem(kernel, plan.smem_bytes[part]);
@@ -2763,7 +2800,7 @@ void launch_persistent_batch(const PersistentPlan& plan, const uint32_t grid[2],
         attr[0].val.cooperative = 1;
         config.attrs = attr;
         config.numAttrs = 1;
-        void* args[] = {const_cast<PersistentPlan*>(&plan)};
+        void* args[] = {const_cast<PersistentParams*>(&params)};
         check_cuda(cudaLaunchKernelExC(&config, kernel, args),
                    "cannot launch the persistent batch kernel");
     }

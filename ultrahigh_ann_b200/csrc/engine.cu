@@ -1281,17 +1281,24 @@ uint64_t enqueue_lowp_candidates(const BatchContext& c, uint64_t n, const uha::L
         ws->filter_tau.allocate(ws->max_batch);
         ws->filter_sample.allocate(ws->max_batch * 64);
     }
+    if (ws->filter_norms.size() < sample) {
+        ws->filter_norms.allocate(sample);
+    }
     if (time_scan) {
         check_cuda(cudaEventRecord(scan_start, stream), "event");
     }
-    // the sample's one slab (fits the partials of the full plan)
-    uha::launch_lowp_scores(plan, type, lp.data.get(), lp.scales.get(), sample,
+    // the sample's one slab: whole tiles spread over the index
+    uha::launch_lowp_scores(plan, type, lp.data.get(), lp.scales.get(), index->rows,
                             ws->queries_lp.get(), ws->query_scales.get(), n, lp.pitch,
-                            ws->partials.get(), error_flag, stream);
-    uha::launch_lowp_topk(ws->partials.get(), 1, b, static_cast<uint32_t>(sample), norms, k,
-                          ws->filter_sample.get(), stream);
-    uha::launch_lowp_threshold(ws->partials.get(), b, static_cast<uint32_t>(sample), norms, k,
-                               ws->filter_sample.get(), ws->filter_tau.get(), stream);
+                            ws->partials.get(), error_flag, stream, nullptr, sample);
+    // the sample rows' norms in sample order, for its selection and threshold
+    uha::launch_gather_sample_norms(norms, index->rows, static_cast<uint32_t>(sample),
+                                    ws->filter_norms.get(), stream);
+    uha::launch_lowp_topk(ws->partials.get(), 1, b, static_cast<uint32_t>(sample),
+                          ws->filter_norms.get(), k, ws->filter_sample.get(), stream);
+    uha::launch_lowp_threshold(ws->partials.get(), b, static_cast<uint32_t>(sample),
+                               ws->filter_norms.get(), k, ws->filter_sample.get(),
+                               ws->filter_tau.get(), stream);
     check_cuda(cudaMemsetAsync(ws->filter_count.get(), 0, n * sizeof(uint32_t), stream),
                "cannot clear candidate counts");
     const uha::FilterArgs filter{norms, ws->filter_tau.get(), ws->filter_keys.get(),
@@ -1304,7 +1311,7 @@ uint64_t enqueue_lowp_candidates(const BatchContext& c, uint64_t n, const uha::L
     if (time_scan) {
         check_cuda(cudaEventRecord(scan_stop, stream), "event");
     }
-    return 5;
+    return 6;
 }
 
 // One query batch's kernels on the workspace stream: gather / copy with

@@ -120,6 +120,7 @@ struct uha_workspace {
     uha::DeviceBuffer<uint32_t> filter_count;
     uha::DeviceBuffer<float> filter_tau;
     uha::DeviceBuffer<uint32_t> filter_sample;
+    uha::DeviceBuffer<float> filter_norms;  // the sample rows' norms
     bool filter_disabled = false;  // answering again after an overflow
     uha::DeviceBuffer<uint32_t> candidates;       // [batch][candidates_per_query]
     uha::DeviceBuffer<double> cand_dist;          // [batch][candidates_per_query]

@@ -255,24 +255,34 @@ struct FilterArgs {
 // partials[split][q][row] = q~ . v~ over the split's K slices (FP8: times the
 // row and query scales), or with `filter` (one K split) the filter's keys in
 // place of the slab. error_flag |= 8 when a pipeline wait ran out.
+// With sample_rows (a multiple of 128, below row_count) only that many rows
+// are scored: whole tiles spread evenly over the index (sample_tile_stride),
+// written as rows 0 .. sample_rows of the slab.
 void launch_lowp_scores(const LowpPlan& plan, LowpType type, const void* rows_lp,
                         const float* row_scale, uint64_t row_count,
                         const void* queries_lp, const float* query_scale,
                         uint64_t batch, uint64_t pitch, float* partials,
                         int* error_flag, cudaStream_t stream,
-                        const FilterArgs* filter = nullptr);
-// The fused selection: sample rows (the first ones, whole tiles) whose k-th
-// smallest estimate bounds each query's threshold, and the list capacity.
+                        const FilterArgs* filter = nullptr, uint64_t sample_rows = 0);
+uint32_t sample_tile_stride(uint64_t rows, uint64_t sample_rows);
+// The fused selection: sample rows (whole tiles spread over the index) whose
+// k-th smallest estimate bounds each query's threshold, and the list
+// capacity.
 // A query whose list overflows sets error bit kCandidateOverflow; the call
 // is then answered again by the slab path.
 constexpr uint64_t kFilterMinRows = 16384;
 constexpr int kCandidateOverflow = 32;
 uint64_t filter_sample_rows(uint64_t rows);
 uint32_t filter_capacity(uint64_t rows, uint32_t k);
+// out[i] = norms[the index row sample row i stands for] (a sample of
+// sample_rows over an index of `rows` rows, as launch_lowp_scores scores it).
+void launch_gather_sample_norms(const float* norms, uint64_t rows, uint32_t sample_rows,
+                                float* out, cudaStream_t stream);
 // tau[q] = the estimate of sample_candidates[q * k + k - 1] over the sample's
-// one-slab partials (+inf when the sample has fewer than k rows).
+// one-slab partials, with the sample's norms (+inf when the sample has fewer
+// than k rows).
 void launch_lowp_threshold(const float* partials, uint32_t batch, uint32_t sample_rows,
-                           const float* norms, uint32_t k,
+                           const float* sample_norms, uint32_t k,
                            const uint32_t* sample_candidates, float* tau,
                            cudaStream_t stream);
 // candidates[q * k + i]: the k smallest keys of the query's list (the same

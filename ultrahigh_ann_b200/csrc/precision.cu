@@ -179,6 +179,10 @@ struct GemmSmem {
 // does and appends the key (e, row) of every row with e <= f.tau[q] to the
 // query's list f.keys[q][0 .. f.cap) (f.count[q] counts them all, also past
 // the capacity).
+//
+// Row tile y reads the index's tile y * tile_stride (rows below source_rows);
+// its scores are row y * 128 + i of the output (rows below row_count). A
+// stride above 1 scores a sample of whole tiles spread over the index.
 template <int BN, int STAGES, bool FP8, bool FILTER>
 __global__ void __launch_bounds__(kGemmThreads, 1)
     lowp_score_kernel(const __grid_constant__ CUtensorMap rows_map,
@@ -186,7 +190,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
                       uint32_t kblocks, uint32_t kblocks_per_split,
                       uint32_t row_count, uint32_t batch, const float* row_scale,
                       const float* query_scale, float* partials, FilterArgs f,
-                      int* error_flag)
+                      uint32_t tile_stride, uint32_t source_rows, int* error_flag)
 {
     using L = GemmSmem<BN, STAGES>;
     extern __shared__ unsigned char smem_raw[];
@@ -206,7 +210,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     const uint32_t kb_begin = split * kblocks_per_split;
     const uint32_t kb_end = min(kblocks, kb_begin + kblocks_per_split);
     const uint32_t steps = kb_end > kb_begin ? kb_end - kb_begin : 0;
-    const int32_t row0 = static_cast<int32_t>(blockIdx.y) * kTileRows;
+    const int32_t row0 = static_cast<int32_t>(blockIdx.y) * kTileRows;  // output rows
+    const int32_t src0 = static_cast<int32_t>(blockIdx.y * tile_stride) * kTileRows;
     const int32_t q0 = static_cast<int32_t>(blockIdx.x) * BN;
 
     if (warp == 0 && lane == 0) {
@@ -249,7 +254,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
                 }
                 mbar_expect_tx(full + s, L::a_bytes + L::b_bytes);
                 const int32_t x = static_cast<int32_t>((kb_begin + i) * (FP8 ? 128u : 64u));
-                tma_load_2d(a_tiles + s * L::a_bytes, &rows_map, full + s, x, row0);
+                tma_load_2d(a_tiles + s * L::a_bytes, &rows_map, full + s, x, src0);
                 tma_load_2d(b_tiles + s * L::b_bytes, &queries_map, full + s, x, q0);
                 ++issued;
             }
@@ -299,8 +304,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
                 atomicOr(error_flag, kPipelineTimeout);
             }
         } else if (store && FILTER) {
-            const uint32_t row = static_cast<uint32_t>(row0) + quarter + lane;
-            const bool row_ok = row < row_count;
+            const uint32_t row = static_cast<uint32_t>(src0) + quarter + lane;
+            const bool row_ok = row < source_rows;
             const float rs = FP8 && row_ok ? row_scale[row] : 1.f;
             const float norm = row_ok ? f.norms[row] : 0.f;
 #pragma unroll 1
@@ -341,8 +346,9 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
             }
         } else if (store) {
             const uint32_t row = static_cast<uint32_t>(row0) + quarter + lane;
-            const bool row_ok = row < row_count;
-            const float rs = FP8 && row_ok ? row_scale[row] : 1.f;
+            const uint32_t src_row = static_cast<uint32_t>(src0) + quarter + lane;
+            const bool row_ok = row < row_count && src_row < source_rows;
+            const float rs = FP8 && row_ok ? row_scale[src_row] : 1.f;
             float* out = partials + static_cast<uint64_t>(split) * batch * row_count + row;
 #pragma unroll 1
             for (int c = 0; c < BN; c += 16) {
@@ -801,7 +807,8 @@ __global__ void __launch_bounds__(kTopkThreads)
 }
 
 // tau[q]: the estimate of the query's k-th candidate over the sample's one
-// slab (the selection's own arithmetic: 0 + S, then the FMA with the norm).
+// slab (the selection's own arithmetic: 0 + S, then the FMA with the norm;
+// norms in sample order).
 __global__ void threshold_kernel(const float* __restrict__ partials, uint32_t batch,
                                  uint32_t rows, const float* __restrict__ norms, uint32_t k,
                                  const uint32_t* __restrict__ candidates,
@@ -818,6 +825,17 @@ __global__ void threshold_kernel(const float* __restrict__ partials, uint32_t ba
         t = __fmaf_rn(-2.f, dot, norms[row]);
     }
     tau[q] = t;
+}
+
+// out[i] = norms of the index row that sample row i stands for (tile i / 128
+// is the index's tile (i / 128) * tile_stride).
+__global__ void sample_norms_kernel(const float* __restrict__ norms, uint32_t sample_rows,
+                                    uint32_t tile_stride, float* __restrict__ out)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < sample_rows) {
+        out[i] = norms[(i / kTileRows) * tile_stride * kTileRows + i % kTileRows];
+    }
 }
 
 // One block per query: the k smallest keys of the query's filtered list,
@@ -913,12 +931,19 @@ CUtensorMap make_map(const void* base, bool fp8, uint64_t pitch, uint64_t outer,
     return map;
 }
 
+// Row tiles a score launch reads: tile y of the output is the index's tile
+// y * stride (rows below source_rows).
+struct RowTiles {
+    uint32_t stride;
+    uint32_t source_rows;
+};
+
 template <int BN, int STAGES, bool FP8, bool FILTER>
 void launch_gemm_filtered(const LowpPlan& plan, const CUtensorMap& rows_map,
                           const CUtensorMap& queries_map, uint32_t row_count,
                           uint32_t batch, const float* row_scale,
                           const float* query_scale, float* partials, const FilterArgs& f,
-                          int* error_flag, cudaStream_t stream)
+                          const RowTiles& tiles, int* error_flag, cudaStream_t stream)
 {
     using L = GemmSmem<BN, STAGES>;
     auto kernel = lowp_score_kernel<BN, STAGES, FP8, FILTER>;
@@ -933,7 +958,8 @@ void launch_gemm_filtered(const LowpPlan& plan, const CUtensorMap& rows_map,
     kernel<<<grid, kGemmThreads, L::total, stream>>>(rows_map, queries_map, plan.kblocks,
                                                       plan.kblocks_per_split, row_count,
                                                       batch, row_scale, query_scale,
-                                                      partials, f, error_flag);
+                                                      partials, f, tiles.stride,
+                                                      tiles.source_rows, error_flag);
     check_cuda(cudaGetLastError(), "cannot launch the tensor-core score kernel");
 }
 
@@ -942,16 +968,17 @@ void launch_gemm_instance(const LowpPlan& plan, const CUtensorMap& rows_map,
                           const CUtensorMap& queries_map, uint32_t row_count,
                           uint32_t batch, const float* row_scale,
                           const float* query_scale, float* partials,
-                          const FilterArgs* filter, int* error_flag, cudaStream_t stream)
+                          const FilterArgs* filter, const RowTiles& tiles, int* error_flag,
+                          cudaStream_t stream)
 {
     if (filter != nullptr) {
         launch_gemm_filtered<BN, STAGES, FP8, true>(plan, rows_map, queries_map, row_count,
                                                     batch, row_scale, query_scale, partials,
-                                                    *filter, error_flag, stream);
+                                                    *filter, tiles, error_flag, stream);
     } else {
         launch_gemm_filtered<BN, STAGES, FP8, false>(plan, rows_map, queries_map, row_count,
                                                      batch, row_scale, query_scale, partials,
-                                                     FilterArgs{}, error_flag, stream);
+                                                     FilterArgs{}, tiles, error_flag, stream);
     }
 }
 
@@ -959,8 +986,8 @@ template <bool FP8>
 void launch_gemm_typed(const LowpPlan& plan, const CUtensorMap& rows_map,
                        const void* queries, uint64_t pitch, uint32_t row_count,
                        uint32_t batch, const float* row_scale, const float* query_scale,
-                       float* partials, const FilterArgs* filter, int* error_flag,
-                       cudaStream_t stream)
+                       float* partials, const FilterArgs* filter, const RowTiles& tiles,
+                       int* error_flag, cudaStream_t stream)
 {
     // the query buffer holds lowp_padded_count(batch) vectors: every box is
     // inside it (the vectors past `batch` are computed and not stored)
@@ -971,27 +998,27 @@ void launch_gemm_typed(const LowpPlan& plan, const CUtensorMap& rows_map,
     case 16:
         launch_gemm_instance<16, 8, FP8>(plan, rows_map, queries_map, row_count, batch,
                                          row_scale, query_scale, partials, filter,
-                                         error_flag, stream);
+                                         tiles, error_flag, stream);
         break;
     case 32:
         launch_gemm_instance<32, 8, FP8>(plan, rows_map, queries_map, row_count, batch,
                                          row_scale, query_scale, partials, filter,
-                                         error_flag, stream);
+                                         tiles, error_flag, stream);
         break;
     case 64:
         launch_gemm_instance<64, 8, FP8>(plan, rows_map, queries_map, row_count, batch,
                                          row_scale, query_scale, partials, filter,
-                                         error_flag, stream);
+                                         tiles, error_flag, stream);
         break;
     case 128:
         launch_gemm_instance<128, 6, FP8>(plan, rows_map, queries_map, row_count, batch,
                                           row_scale, query_scale, partials, filter,
-                                          error_flag, stream);
+                                          tiles, error_flag, stream);
         break;
     default:
         launch_gemm_instance<256, 4, FP8>(plan, rows_map, queries_map, row_count, batch,
                                           row_scale, query_scale, partials, filter,
-                                          error_flag, stream);
+                                          tiles, error_flag, stream);
         break;
     }
 }
@@ -1136,10 +1163,18 @@ void launch_lowp_scores(const LowpPlan& plan, LowpType type, const void* rows_lp
                         const float* row_scale, uint64_t row_count,
                         const void* queries_lp, const float* query_scale,
                         uint64_t batch, uint64_t pitch, float* partials,
-                        int* error_flag, cudaStream_t stream, const FilterArgs* filter)
+                        int* error_flag, cudaStream_t stream, const FilterArgs* filter,
+                        uint64_t sample_rows)
 {
     if (filter != nullptr && plan.splits != 1) {
         fail(UHA_LOGIC_ERROR, "the fused candidate filter needs one K split");
+    }
+    // every row, or a sample of whole tiles spread over the index
+    RowTiles tiles{1, static_cast<uint32_t>(row_count)};
+    uint64_t out_rows = row_count;
+    if (sample_rows != 0 && sample_rows < row_count) {
+        tiles.stride = sample_tile_stride(row_count, sample_rows);
+        out_rows = sample_rows;
     }
     const bool fp8 = type == LowpType::fp8_e4m3;
     // the row buffer holds lowp_padded_count(row_count) vectors (zero past
@@ -1148,14 +1183,14 @@ void launch_lowp_scores(const LowpPlan& plan, LowpType type, const void* rows_lp
         make_map(rows_lp, fp8, pitch, round_up(row_count, kTileRows), kTileRows);
     if (fp8) {
         launch_gemm_typed<true>(plan, rows_map, queries_lp, pitch,
-                                static_cast<uint32_t>(row_count),
+                                static_cast<uint32_t>(out_rows),
                                 static_cast<uint32_t>(batch), row_scale, query_scale,
-                                partials, filter, error_flag, stream);
+                                partials, filter, tiles, error_flag, stream);
     } else {
         launch_gemm_typed<false>(plan, rows_map, queries_lp, pitch,
-                                 static_cast<uint32_t>(row_count),
+                                 static_cast<uint32_t>(out_rows),
                                  static_cast<uint32_t>(batch), row_scale, query_scale,
-                                 partials, filter, error_flag, stream);
+                                 partials, filter, tiles, error_flag, stream);
     }
 }
 
@@ -1186,6 +1221,13 @@ void launch_lowp_topk(const float* partials, uint32_t splits, uint32_t batch,
     check_cuda(cudaGetLastError(), "cannot launch the candidate selection kernel");
 }
 
+uint32_t sample_tile_stride(uint64_t rows, uint64_t sample_rows)
+{
+    const uint64_t tiles = (rows + kTileRows - 1) / kTileRows;
+    const uint64_t sampled = std::max<uint64_t>(1, sample_rows / kTileRows);
+    return static_cast<uint32_t>(std::max<uint64_t>(1, tiles / sampled));
+}
+
 uint64_t filter_sample_rows(uint64_t rows)
 {
     // about a sixteenth of the rows in whole tiles: about 16 k keys per query
@@ -1203,7 +1245,7 @@ uint32_t filter_capacity(uint64_t rows, uint32_t k)
 }
 
 void launch_lowp_threshold(const float* partials, uint32_t batch, uint32_t sample_rows,
-                           const float* norms, uint32_t k,
+                           const float* sample_norms, uint32_t k,
                            const uint32_t* sample_candidates, float* tau,
                            cudaStream_t stream)
 {
@@ -1211,9 +1253,21 @@ void launch_lowp_threshold(const float* partials, uint32_t batch, uint32_t sampl
         return;
     }
     threshold_kernel<<<(batch + 255) / 256, 256, 0, stream>>>(partials, batch, sample_rows,
-                                                              norms, k, sample_candidates,
-                                                              tau);
+                                                              sample_norms, k,
+                                                              sample_candidates, tau);
     check_cuda(cudaGetLastError(), "cannot launch the candidate threshold kernel");
+}
+
+void launch_gather_sample_norms(const float* norms, uint64_t rows, uint32_t sample_rows,
+                                float* out, cudaStream_t stream)
+{
+    if (sample_rows == 0) {
+        return;
+    }
+    const uint32_t stride = sample_rows < rows ? sample_tile_stride(rows, sample_rows) : 1u;
+    sample_norms_kernel<<<(sample_rows + 255) / 256, 256, 0, stream>>>(norms, sample_rows,
+                                                                       stride, out);
+    check_cuda(cudaGetLastError(), "cannot launch the sample norm kernel");
 }
 
 void launch_lowp_select(const unsigned long long* keys, const uint32_t* count, uint32_t cap,

@@ -132,8 +132,6 @@ struct PersistentSegment {
 };
 
 struct PersistentPlan {
-    const PersistentPair* pairs;        // device
-    const PersistentSegment* segments;  // device, grouped by stage
     uint32_t stage_begin[kPersistentStages + 1];  // segment ranges per stage
     uint32_t stage_units[kPersistentStages];
     unsigned int* barrier;  // device: [0] arrivals, [1] generation (zero at creation)
@@ -143,6 +141,18 @@ struct PersistentPlan {
     // the last entry when CTA 0 finishes its units of the last stage)
     unsigned long long* clock;
     uint32_t smem_bytes[2];  // dynamic shared memory of the two kernels
+};
+
+// The kernels' one parameter (about 25 KB, read from the constant bank like
+// any kernel argument: the units address the pairs' fields in place instead
+// of copying them into registers): the plan, the pairs and the segments,
+// grouped by stage.
+constexpr uint32_t kPersistentMaxPairs = 32;
+constexpr uint32_t kPersistentMaxSegments = 2 * kPersistentMaxPairs * kPersistentStages + 1;
+struct PersistentParams {
+    PersistentPlan plan;
+    PersistentPair pairs[kPersistentMaxPairs];
+    PersistentSegment segments[kPersistentMaxSegments];
 };
 
 // Builds the segment list of `pairs` (host copies) into `segments` (room for
@@ -157,7 +167,7 @@ uint32_t persistent_segment_capacity(uint32_t count);
 // (all resident at once); 0 if it cannot be launched.
 uint32_t persistent_grid(int part, uint32_t smem_bytes);
 // The run's two cooperative launches (capturable in a graph).
-void launch_persistent_batch(const PersistentPlan& plan, const uint32_t grid[2],
+void launch_persistent_batch(const PersistentParams& params, const uint32_t grid[2],
                              cudaStream_t stream);
 
 }  // namespace uha
