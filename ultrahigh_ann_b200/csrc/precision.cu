@@ -304,42 +304,86 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
                 atomicOr(error_flag, kPipelineTimeout);
             }
         } else if (store && FILTER) {
+            // Three passes, so that a tile waits for one round of atomics:
+            // (1) the pass mask of every query column (warp ballot over the
+            // warp's 32 rows) into shared memory; (2) one atomic per column
+            // with passes, all of the warp's in flight together (lane l takes
+            // columns l, l + 32, ...); (3) the keys into their slots. The
+            // operand tiles are free once every MMA has completed.
+            // per warp: thresholds, query scales, masks, slot bases (BN words
+            // each; a warp that gave up never leaves another one waiting)
+            const uint32_t qi = static_cast<uint32_t>(warp % 4);
+            uint32_t* area = reinterpret_cast<uint32_t*>(a_tiles) + qi * 4 * BN;
+            float* tau_s = reinterpret_cast<float*>(area);
+            float* qscale_s = tau_s + BN;
+            uint32_t* masks = area + 2 * BN;
+            uint32_t* bases = area + 3 * BN;
+            for (int c = lane; c < BN; c += 32) {
+                const uint32_t q = static_cast<uint32_t>(q0 + c);
+                tau_s[c] = q < batch ? f.tau[q] : -__int_as_float(0x7f800000);
+                qscale_s[c] = FP8 && q < batch ? query_scale[q] : 1.f;
+            }
+            __syncwarp();
             const uint32_t row = static_cast<uint32_t>(src0) + quarter + lane;
             const bool row_ok = row < source_rows;
             const float rs = FP8 && row_ok ? row_scale[row] : 1.f;
             const float norm = row_ok ? f.norms[row] : 0.f;
+            auto estimate = [&](float v, int c) {
+                const float value = FP8 ? __fmul_rn(__fmul_rn(v, rs), qscale_s[c]) : v;
+                // the selection sums one slab from zero: 0 + value
+                return __fmaf_rn(-2.f, 0.f + value, norm);
+            };
 #pragma unroll 1
             for (int c = 0; c < BN; c += 16) {
                 float v[16];
                 tmem_load16(tmem + (quarter << 16) + static_cast<uint32_t>(c), v);
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
-                    const uint32_t q = static_cast<uint32_t>(q0 + c + j);
-                    bool pass = false;
-                    unsigned long long key = 0;
-                    if (row_ok && q < batch) {
-                        const float value =
-                            FP8 ? __fmul_rn(__fmul_rn(v[j], rs), query_scale[q]) : v[j];
-                        // the selection sums one slab from zero: 0 + value
-                        const float est = __fmaf_rn(-2.f, 0.f + value, norm);
-                        pass = est <= f.tau[q];
-                        key = (static_cast<unsigned long long>(ordered_key_bits(est)) << 32) |
-                              row;
-                    }
+                    const bool pass = row_ok && estimate(v[j], c + j) <= tau_s[c + j];
                     const unsigned int mask = __ballot_sync(0xffffffffu, pass);
-                    if (mask != 0u) {
-                        const int leader = __ffs(mask) - 1;
-                        uint32_t base = 0;
-                        if (lane == leader) {
-                            base = atomicAdd(f.count + q, static_cast<uint32_t>(__popc(mask)));
-                        }
-                        base = __shfl_sync(0xffffffffu, base, leader);
-                        if (pass) {
-                            const uint32_t slot =
-                                base + static_cast<uint32_t>(__popc(mask & ((1u << lane) - 1u)));
-                            if (slot < f.cap) {
-                                f.keys[static_cast<uint64_t>(q) * f.cap + slot] = key;
-                            }
+                    if (lane == 0) {
+                        masks[c + j] = mask;
+                    }
+                }
+            }
+            __syncwarp();
+#pragma unroll
+            for (int c0 = 0; c0 < BN; c0 += 32) {
+                const int c = c0 + lane;
+                const uint32_t mask = c < BN ? masks[c] : 0u;
+                uint32_t base = 0;
+                if (mask != 0u) {
+                    base = atomicAdd(f.count + q0 + c, static_cast<uint32_t>(__popc(mask)));
+                }
+                if (c < BN) {
+                    bases[c] = base;
+                }
+            }
+            __syncwarp();
+            const unsigned int below = (1u << lane) - 1u;
+#pragma unroll 1
+            for (int c = 0; c < BN; c += 16) {
+                bool any = false;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    any = any || masks[c + j] != 0u;
+                }
+                if (!any) {
+                    continue;  // warp-uniform: the masks are shared
+                }
+                float v[16];
+                tmem_load16(tmem + (quarter << 16) + static_cast<uint32_t>(c), v);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const unsigned int mask = masks[c + j];
+                    if ((mask >> lane) & 1u) {
+                        const uint32_t slot =
+                            bases[c + j] + static_cast<uint32_t>(__popc(mask & below));
+                        if (slot < f.cap) {
+                            const float est = estimate(v[j], c + j);
+                            f.keys[static_cast<uint64_t>(q0 + c + j) * f.cap + slot] =
+                                (static_cast<unsigned long long>(ordered_key_bits(est)) << 32) |
+                                row;
                         }
                     }
                 }
@@ -885,6 +929,59 @@ __global__ void __launch_bounds__(kTopkThreads)
     }
 }
 
+// One warp per query (k <= 32): the k smallest keys of the query's filtered
+// list with the warp list and two-slot lane queues of warp_topk_kernel.
+__global__ void __launch_bounds__(kTopkThreads)
+    warp_select_kernel(const unsigned long long* __restrict__ keys,
+                       const uint32_t* __restrict__ count, uint32_t cap, uint32_t batch,
+                       uint32_t k, uint32_t* __restrict__ candidates, int* error_flag)
+{
+    const uint32_t q = blockIdx.x * (kTopkThreads / 32) + threadIdx.x / 32;
+    const int lane = threadIdx.x % 32;
+    if (q >= batch) {
+        return;
+    }
+    const uint32_t total = count[q];
+    if (total > cap && lane == 0) {
+        atomicOr(error_flag, kCandidateOverflow);
+    }
+    const uint32_t n = min(total, cap);
+    const unsigned long long* list_in = keys + static_cast<uint64_t>(q) * cap;
+    unsigned long long list = ~0ull;
+    unsigned long long largest = ~0ull;
+    unsigned long long slot0 = ~0ull;
+    unsigned long long slot1 = ~0ull;
+    int queued = 0;
+    for (uint32_t first = 0; first < n; first += 32) {
+        const uint32_t i = first + lane;
+        const unsigned long long key = i < n ? list_in[i] : ~0ull;
+        if (key < largest) {
+            if (queued == 0) {
+                slot0 = key;
+            } else {
+                slot1 = key;
+            }
+            ++queued;
+        }
+        if (__any_sync(0xffffffffu, queued == 2)) {
+            list = warp_merge32(list, warp_sort32(slot0, lane), lane);
+            list = warp_merge32(list, warp_sort32(slot1, lane), lane);
+            slot0 = ~0ull;
+            slot1 = ~0ull;
+            queued = 0;
+            largest = __shfl_sync(0xffffffffu, list, 31);
+        }
+    }
+    if (__any_sync(0xffffffffu, queued != 0)) {
+        list = warp_merge32(list, warp_sort32(slot0, lane), lane);
+        list = warp_merge32(list, warp_sort32(slot1, lane), lane);
+    }
+    if (static_cast<uint32_t>(lane) < k) {
+        candidates[static_cast<uint64_t>(q) * k + lane] =
+            list == ~0ull ? 0xffffffffu : static_cast<uint32_t>(list & 0xffffffffu);
+    }
+}
+
 // ------------------------------------------------------------ host side
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
@@ -1277,15 +1374,10 @@ void launch_lowp_select(const unsigned long long* keys, const uint32_t* count, u
     if (batch == 0) {
         return;
     }
-    if (k <= 8) {
-        select_kernel<8><<<batch, kTopkThreads, 0, stream>>>(keys, count, cap, k, candidates,
-                                                            error_flag);
-    } else if (k <= 16) {
-        select_kernel<16><<<batch, kTopkThreads, 0, stream>>>(keys, count, cap, k,
-                                                             candidates, error_flag);
-    } else if (k <= 32) {
-        select_kernel<32><<<batch, kTopkThreads, 0, stream>>>(keys, count, cap, k,
-                                                             candidates, error_flag);
+    if (k <= 32) {
+        constexpr uint32_t per_cta = kTopkThreads / 32;
+        warp_select_kernel<<<(batch + per_cta - 1) / per_cta, kTopkThreads, 0, stream>>>(
+            keys, count, cap, batch, k, candidates, error_flag);
     } else {
         select_kernel<64><<<batch, kTopkThreads, 0, stream>>>(keys, count, cap, k,
                                                              candidates, error_flag);
