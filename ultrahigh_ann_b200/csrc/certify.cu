@@ -2489,8 +2489,9 @@ FlatPlan plan_flat_query(uint64_t rows, uint64_t padded_dim, uint64_t batch,
 
 namespace {
 
-// Scratch of the fused flat query for a workspace of `capacity` queries: two
-// slots (consecutive launches alternate), each with the distance slabs, the
+// Scratch of the fused flat query for a workspace of `capacity` queries:
+// slots (two per stream lane; consecutive launches on a stream alternate),
+// each with the distance slabs, the
 // CTA summaries (room for the most CTAs any plan uses) and the per-query
 // completion counters at a fixed place (zero between launches).
 struct FlatScratch {
@@ -2530,7 +2531,7 @@ uint64_t flat_slot_bytes(uint64_t capacity, uint64_t rows)
 
 FlatScratch flat_scratch(void* base, uint64_t capacity, uint64_t rows, uint32_t slot)
 {
-    char* p = static_cast<char*>(base) + (slot & 1u) * flat_slot_bytes(capacity, rows);
+    char* p = static_cast<char*>(base) + slot * flat_slot_bytes(capacity, rows);
     FlatScratch fs;
     fs.distances = reinterpret_cast<float*>(p);
     fs.summaries = reinterpret_cast<Summary*>(p + flat_summaries_offset(capacity, rows));
@@ -2578,9 +2579,9 @@ void launch_flat_lanes(const SmallQuery& sq, const FlatPlan& plan, uint32_t batc
 
 }  // namespace
 
-uint64_t flat_query_scratch_bytes(uint64_t capacity, uint64_t rows)
+uint64_t flat_query_scratch_bytes(uint64_t capacity, uint64_t rows, uint32_t slots)
 {
-    return 2 * flat_slot_bytes(capacity, rows);
+    return slots * flat_slot_bytes(capacity, rows);
 }
 
 void launch_flat_query(const SmallQuery& sq, const FlatPlan& plan, uint32_t batch,

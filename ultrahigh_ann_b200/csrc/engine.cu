@@ -1476,6 +1476,19 @@ bool persistent_pair(const uha_index* index, uha_workspace* ws, uint64_t n,
            ws->partials.size() >= uint64_t(plan.chunks) * n * index->rows;
 }
 
+void ensure_flat_scratch(const uha_index* index, uha_workspace* ws)
+{
+    if (ws->flat_scratch.size() != 0) {
+        return;
+    }
+    // zero once: the kernel leaves its completion counters at zero
+    ws->flat_scratch.allocate(
+        uha::flat_query_scratch_bytes(ws->max_batch, index->rows, 2 * uha::kFlatLanes));
+    check_cuda(cudaMemsetAsync(ws->flat_scratch.get(), 0, ws->flat_scratch.bytes(),
+                               ws->stream),
+               "cannot clear flat query scratch");
+}
+
 uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
                        uha::Result* results, double* exact, bool time_scan,
                        cudaEvent_t scan_start, cudaEvent_t scan_stop)
@@ -1524,22 +1537,20 @@ uint64_t enqueue_batch(const BatchContext& c, const float* source, uint64_t n,
         if (ws->emulated_replay) {
             set_emulated(in, index);
         }
-        if (flat && ws->flat_scratch.size() == 0) {
-            // zero once: the kernel leaves its completion counters at zero
-            ws->flat_scratch.allocate(
-                uha::flat_query_scratch_bytes(ws->max_batch, index->rows));
-            check_cuda(cudaMemsetAsync(ws->flat_scratch.get(), 0,
-                                       ws->flat_scratch.bytes(), stream),
-                       "cannot clear flat query scratch");
+        if (flat) {
+            ensure_flat_scratch(index, ws);
         }
         if (time_scan) {
             check_cuda(cudaEventRecord(scan_start, stream), "event");
         }
         if (flat) {
+            const int lane = c.flat_lane;
+            const cudaStream_t lane_stream = lane == 0 ? stream : ws->flat_streams[lane];
             uha::launch_flat_query(sq, flat_plan, static_cast<uint32_t>(n), bound, in,
-                                   ws->flat_scratch.get(), ws->max_batch, ws->flat_slot,
-                                   results, exact, replay_count, error_flag, stream);
-            ws->flat_slot ^= 1u;
+                                   ws->flat_scratch.get(), ws->max_batch,
+                                   2u * static_cast<uint32_t>(lane) + ws->flat_parity[lane],
+                                   results, exact, replay_count, error_flag, lane_stream);
+            ws->flat_parity[lane] ^= 1u;
         } else {
             uha::launch_small_query(sq, static_cast<uint32_t>(n), bound, in, results,
                                     exact, replay_count, error_flag, stream);
@@ -1943,6 +1954,34 @@ extern "C" uha_status uha_query_many(const uha_index* index, uha_workspace* ws,
         if (pipelined) {
             prepare_pipeline(index, ws, strategy, batch);
         }
+        // Fused flat batches of device-resident queries go round-robin over
+        // kFlatLanes streams: every launch still answers its own batch, and
+        // the lanes' launch chains run side by side.
+        const int lanes = !pipelined && queries_on_device && !ws->timing && batches > 1 &&
+                                  flat_path_applies(index, strategy, batch)
+                              ? uha::kFlatLanes
+                              : 1;
+        if (lanes > 1) {
+            ensure_flat_scratch(index, ws);
+            ws->flat_streams[0] = stream;
+            for (int i = 0; i < lanes; ++i) {
+                if (i > 0 && ws->flat_streams[i] == nullptr) {
+                    check_cuda(cudaStreamCreateWithFlags(&ws->flat_streams[i],
+                                                         cudaStreamNonBlocking),
+                               "cannot create CUDA stream");
+                }
+                if (ws->flat_events[i] == nullptr) {
+                    check_cuda(cudaEventCreateWithFlags(&ws->flat_events[i],
+                                                        cudaEventDisableTiming),
+                               "cannot create CUDA event");
+                }
+            }
+            check_cuda(cudaEventRecord(ws->flat_events[0], stream), "event");
+            for (int i = 1; i < lanes; ++i) {
+                check_cuda(cudaStreamWaitEvent(ws->flat_streams[i], ws->flat_events[0], 0),
+                           "event");
+            }
+        }
         uint64_t launches = 0;
         for (uint64_t b = 0; b < batches; ++b) {
             const uint64_t start = b * batch;
@@ -1977,6 +2016,7 @@ extern "C" uha_status uha_query_many(const uha_index* index, uha_workspace* ws,
                 source = ws->raw_queries.get();
             }
             const bool timed = ws->timing && b % ws->timing_stride == 0;
+            bc.flat_lane = static_cast<int>(b % static_cast<uint64_t>(lanes));
             launches += enqueue_batch(bc, source, count, ws->call_results.get() + start,
                                       ws->call_exact.get() + start, timed,
                                       timed ? ws->scan_events[2 * b] : nullptr,
@@ -1989,6 +2029,10 @@ extern "C" uha_status uha_query_many(const uha_index* index, uha_workspace* ws,
         if (pipelined) {
             check_cuda(cudaEventRecord(ws->pipe_events[4], ws->finish_stream), "event");
             check_cuda(cudaStreamWaitEvent(stream, ws->pipe_events[4], 0), "event");
+        }
+        for (int i = 1; i < lanes; ++i) {
+            check_cuda(cudaEventRecord(ws->flat_events[i], ws->flat_streams[i]), "event");
+            check_cuda(cudaStreamWaitEvent(stream, ws->flat_events[i], 0), "event");
         }
         check_cuda(cudaMemcpyAsync(ws->host_results.get(), ws->call_results.get(),
                                    n * sizeof(uha::Result), cudaMemcpyDeviceToHost,

@@ -43,7 +43,15 @@ struct BatchContext {
     // caller answers the call again without it when a candidate list
     // overflows (error bit uha::kCandidateOverflow).
     bool filter_candidates = false;
+    // The fused flat query of this batch runs on stream lane `flat_lane`
+    // (0: ws->stream; others: ws->flat_streams, forked and joined by the
+    // caller) with that lane's scratch slots.
+    int flat_lane = 0;
 };
+
+// Allocates and clears (on ws->stream) the fused flat query's scratch of
+// every stream lane, if it does not exist yet.
+void ensure_flat_scratch(const uha_index* index, uha_workspace* ws);
 
 // Enqueues one batch of n queries (`source`: device, n x dimension floats) on
 // ws->stream; returns the number of kernel launches. Buffers grow (with a

@@ -106,10 +106,14 @@ struct uha_workspace {
     uha::DeviceBuffer<double> call_exact;         // replayed distances (NaN: none)
     uha::DeviceBuffer<uint32_t> counters;  // [0] replayed queries, [1] error flag
     uha::DeviceBuffer<unsigned char> finalize_scratch;
-    // fused flat query (allocated and zeroed on first use) and the scratch
-    // slot its next launch uses
+    // fused flat query (allocated and zeroed on first use): two scratch slots
+    // per stream lane (uha::kFlatLanes lanes; lane 0 is `stream`), the slot
+    // parity each lane's next launch uses, the lanes' other streams and the
+    // fork / join events of a call that spreads its batches over them
     uha::DeviceBuffer<unsigned char> flat_scratch;
-    uint32_t flat_slot = 0;
+    uint32_t flat_parity[uha::kFlatLanes] = {};
+    cudaStream_t flat_streams[uha::kFlatLanes] = {};
+    cudaEvent_t flat_events[uha::kFlatLanes] = {};
     // precision strategies (allocated on first use)
     uha::DeviceBuffer<unsigned char> queries_lp;  // lowp_padded_count(max_batch) vectors
     uha::DeviceBuffer<float> query_scales;        // FP8 scale per query
@@ -178,6 +182,14 @@ struct uha_workspace {
         for (cudaEvent_t e : pipe_events) {
             if (e != nullptr) {
                 cudaEventDestroy(e);
+            }
+        }
+        for (int i = 0; i < uha::kFlatLanes; ++i) {
+            if (flat_events[i] != nullptr) {
+                cudaEventDestroy(flat_events[i]);
+            }
+            if (i > 0 && flat_streams[i] != nullptr) {
+                cudaStreamDestroy(flat_streams[i]);
             }
         }
         if (finish_stream != nullptr) {

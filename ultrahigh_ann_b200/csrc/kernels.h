@@ -170,11 +170,13 @@ void launch_small_query(const SmallQuery& sq, uint32_t batch, Bound bound, Repla
 // at most kFlatBatch queries: gather, scan and certified argmin (with replay)
 // in one launch with many CTAs per query, the last CTA of a query merging.
 // Launched with programmatic stream serialization outside stream capture:
-// consecutive launches alternate between the two slots of the scratch (pass
-// slot = 0, 1, 0, ...), and each one's gather and scan overlap the end of the
-// previous one.
+// consecutive launches on one stream alternate between that stream's two
+// slots of the scratch (slot = 2 lane + 0, 1, 0, ...), and each one's gather
+// and scan overlap the end of the previous one.
 constexpr uint64_t kFlatColumns = 8192;
 constexpr uint64_t kFlatBatch = 8;
+// streams a call's flat launches are spread over (independent launch chains)
+constexpr int kFlatLanes = 3;
 struct FlatPlan {
     uint32_t lanes;       // lanes per row: 8, 16 or 32
     uint32_t span;        // rows per CTA
@@ -186,9 +188,10 @@ struct FlatPlan {
 bool flat_query_fits(uint64_t rows, uint64_t padded_dim, uint64_t batch);
 FlatPlan plan_flat_query(uint64_t rows, uint64_t padded_dim, uint64_t batch,
                          int sm_count);
-// Scratch for a workspace of `capacity` queries; zero when created, left with
-// its counters at zero by every launch.
-uint64_t flat_query_scratch_bytes(uint64_t capacity, uint64_t rows);
+// Scratch for a workspace of `capacity` queries, `slots` slots (two per
+// stream lane); zero when created, left with its counters at zero by every
+// launch.
+uint64_t flat_query_scratch_bytes(uint64_t capacity, uint64_t rows, uint32_t slots);
 void launch_flat_query(const SmallQuery& sq, const FlatPlan& plan, uint32_t batch,
                        Bound bound, ReplayInputs in, void* scratch, uint64_t capacity,
                        uint32_t slot, Result* results, double* exact_distances,

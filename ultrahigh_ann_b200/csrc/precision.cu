@@ -1068,7 +1068,14 @@ void launch_gemm_instance(const LowpPlan& plan, const CUtensorMap& rows_map,
                           const FilterArgs* filter, const RowTiles& tiles, int* error_flag,
                           cudaStream_t stream)
 {
-    if (filter != nullptr) {
+    if (filter != nullptr && plan.kblocks <= 8) {
+        // few K slices (the hierarchies' projected rows): two stages, so two
+        // CTAs share an SM and one's filter epilogue overlaps the other's
+        // loads and MMAs
+        launch_gemm_filtered<BN, 2, FP8, true>(plan, rows_map, queries_map, row_count,
+                                               batch, row_scale, query_scale, partials,
+                                               *filter, tiles, error_flag, stream);
+    } else if (filter != nullptr) {
         launch_gemm_filtered<BN, STAGES, FP8, true>(plan, rows_map, queries_map, row_count,
                                                     batch, row_scale, query_scale, partials,
                                                     *filter, tiles, error_flag, stream);
