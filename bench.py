@@ -56,6 +56,9 @@ def parse_args():
                    choices=["", "precision", "batched", "serving", "centroids", "wide",
                             "hierarchies"],
                    help="only this section of the bench (one JSON line)")
+    p.add_argument("--full-probabilities", action="store_true",
+                   help="with --only hierarchies: each index's importance "
+                        "probabilities over all its rows (minutes at 65,536 rows)")
     p.add_argument("--hier-shape", default="",
                    help="ROWS,DIM,QUERIES of the full-size hierarchical batch "
                         "(--only hierarchies; smaller shapes for profiler captures)")
@@ -775,7 +778,7 @@ def _projected_check(ix, metric, sampled64, queries64, got):
 
 
 def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=16,
-                     ref_queries=64):
+                     ref_queries=64, full_probabilities=False):
     """16 hierarchical indexes at the full size of the hierarchical batched
     configuration: rows 1,024 / 7,028 / 65,536 (row subsets of one
     65,536 x 262,144 BF16 matrix generated on the device), T = 32,
@@ -783,7 +786,10 @@ def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=1
     in one captured CUDA graph launch with autotuned scan shapes. The indexes
     are built from the device-resident matrix (no host copy of it); the
     importance probabilities are those of the first 1,024 rows (the pair
-    computation over all 65,536 rows is ~1e15 binary64 operations). Checks:
+    computation over all 65,536 rows is ~1e15 operations), or with
+    full_probabilities each row count's own probabilities over all its rows
+    (direct binary64 pair distances, binary32 column maxima, from the device
+    matrix; minutes per metric at 65,536 rows, reported). Checks:
     the same answers index by index, and a binary64 host check of `checked`
     queries per index."""
     import torch
@@ -797,9 +803,29 @@ def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=1
     torch.cuda.synchronize()
     gen_s = time.perf_counter() - t
     t = time.perf_counter()
-    head = data.rows[:1024].float().cpu().numpy()
-    probs = {"l2": uha.compute_l2_importance_probabilities_gpu(head).probabilities,
-             "l1": uha.compute_l1_importance_probabilities_gpu(head).probabilities}
+    full_report = None
+    if full_probabilities:
+        # every row count's probabilities over its own rows, from a binary32
+        # copy of the device matrix
+        probs_by_rows, full_report = {}, {}
+        for r in sorted({min(1024, rows), min(7028, rows), rows}):
+            x = data.rows[:r].float()
+            for metric, fn in (("l2", uha.compute_l2_importance_probabilities_gpu),
+                               ("l1", uha.compute_l1_importance_probabilities_gpu)):
+                res = fn(x, maxima="binary32", pair_chunks=256)
+                probs_by_rows[(metric, r)] = res.probabilities
+                full_report[f"{metric}_r{r}"] = {
+                    "pair_distance_s": round(res.inverse_distance_ms / 1e3, 2),
+                    "column_maxima_s": round(res.coordinate_maximum_ms / 1e3, 2),
+                    "total_s": round(res.total_ms / 1e3, 2),
+                    "pairs": int(res.pair_count)}
+            del x
+            torch.cuda.empty_cache()
+        probs = None
+    else:
+        head = data.rows[:1024].float().cpu().numpy()
+        probs = {"l2": uha.compute_l2_importance_probabilities_gpu(head).probabilities,
+                 "l1": uha.compute_l1_importance_probabilities_gpu(head).probabilities}
     prob_s = time.perf_counter() - t
     specs, indexes, seeds = [], [], []
     t = time.perf_counter()
@@ -812,7 +838,9 @@ def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=1
                 cls = (uha.CudaHierarchicalL2AnnIndex if metric == "l2"
                        else uha.CudaHierarchicalL1AnnIndex)
                 ix = cls(uha.DeviceMatrix.from_torch(data.rows[:r]), 32, p,
-                         uha.MT19937_64(300 + i), importance_probabilities=probs[metric])
+                         uha.MT19937_64(300 + i),
+                         importance_probabilities=(probs[metric] if probs is not None
+                                                   else probs_by_rows[(metric, r)]))
                 seeds.append(300 + i)
                 indexes.append(ix)
                 specs.append({"metric": metric, "rows": r, "T": 32, "p": p,
@@ -951,6 +979,10 @@ def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=1
                                "strategy": "L2 hierarchies gemm_bf16_rerank (k = 32), "
                                            "L1 hierarchies direct",
                                "indexes": precision},
+            "probabilities": ("all rows of each index (direct binary64 pair distances, "
+                              "binary32 column maxima)" if full_probabilities
+                              else "the first 1,024 rows"),
+            "full_probability_build": full_report,
             "setup_s": {"generate_on_device": round(gen_s, 1),
                         "probabilities": round(prob_s, 1), "build": round(build_s, 1),
                         "autotune_and_capture": round(setup_s, 1)}}
@@ -1244,6 +1276,7 @@ def run_section(args):
         if args.hier_shape:
             rows, dim, queries = (int(x) for x in args.hier_shape.split(","))
             shape = {"rows": rows, "dim": dim, "per_index": queries}
+        shape["full_probabilities"] = args.full_probabilities
         print(json.dumps({"hierarchies_full": hierarchies_full(**shape)}), flush=True)
         return
     ds = synthetic.row_dataset(rows=ROWS, classes=33, queries=4096, d=DIM, seed=1,

@@ -544,7 +544,13 @@ void uha_server_destroy(uha_server* server);
  * cuBLAS backend does (src/hnsvw25/l2/cuda_importance_sampling.cu:332-364). */
 typedef enum uha_pair_backend {
     UHA_PAIRS_DIRECT = 0,
-    UHA_PAIRS_GRAM = 1
+    UHA_PAIRS_GRAM = 1,
+    /* the same binary64 pair distances, the per-column maxima formed in
+     * binary32 (within 3e-7 relative of the binary64 maxima, inside the
+     * reference GPU path's 1e-6): for full-size builds, which the binary64
+     * pipe would otherwise bound. No reference counterpart. */
+    UHA_PAIRS_DIRECT_MAX32 = 2,
+    UHA_PAIRS_GRAM_MAX32 = 3
 } uha_pair_backend;
 
 /* Importance probabilities on the device. L2: p_j = max over row pairs of
@@ -563,6 +569,18 @@ uha_status uha_importance_probabilities(int device, uha_metric metric,
                                         uint64_t pair_chunks,
                                         double* out_probabilities,
                                         uha_probability_report* report);
+
+/* The same from a representative matrix already on `device` (row-major,
+ * `dimension` floats per row, at device_rows): no host copy, for matrices
+ * that the host cannot hold or that were built on the device. The values are
+ * checked for finiteness on the device. No reference counterpart. */
+uha_status uha_importance_probabilities_device(int device, uha_metric metric,
+                                               const float* device_rows,
+                                               uint64_t row_count, uint64_t dimension,
+                                               uha_pair_backend backend,
+                                               uint64_t pair_chunks,
+                                               double* out_probabilities,
+                                               uha_probability_report* report);
 
 /* The same probabilities on the host cores with the reference CPU policies'
  * binary64 arithmetic, bit-identical to its sequential loop for any thread

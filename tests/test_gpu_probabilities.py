@@ -87,3 +87,31 @@ def test_index_from_gpu_probabilities_samples_the_reference_set(oracle_module, m
     assert np.array_equal(s.source_columns, cols)
     assert np.array_equal(s.multiplicities, mult)
     assert s.inverse_probabilities.tobytes() == np.asarray(invp, np.float64).tobytes()
+
+
+@pytest.mark.parametrize("metric, backend", [("l2", "direct"), ("l2", "gram"),
+                                             ("l1", "direct")])
+def test_binary32_maxima_within_reference_gpu_tolerance(oracle_module, metric, backend):
+    """maxima="binary32" (the full-size build's form): the same pair distances,
+    the per-column maxima in binary32, within the reference GPU path's 1e-6
+    and within 3e-7 relative of the binary64 maxima."""
+    O = _ref(oracle_module)
+    rows = synthetic.row_dataset(rows=300, classes=6, queries=1, d=4099, seed=21).rows
+    want = O.ref_probabilities(metric, rows)
+    kwargs = {"distance_backend": backend} if metric == "l2" else {}
+    got = GPU_FN[metric](rows, maxima="binary32", pair_chunks=3, **kwargs).probabilities
+    assert np.allclose(got, want, rtol=0, atol=1e-6)
+    assert np.all(np.abs(got - want) <= 3e-7 * np.abs(want) + 1e-30)
+
+
+@pytest.mark.parametrize("metric", ["l2", "l1"])
+def test_device_matrix_input_equals_host_input(metric):
+    torch = pytest.importorskip("torch")
+    rows = synthetic.row_dataset(rows=120, classes=5, queries=1, d=1031, seed=4).rows
+    host = GPU_FN[metric](rows).probabilities
+    dev = GPU_FN[metric](torch.from_numpy(rows).cuda()).probabilities
+    assert dev.tobytes() == host.tobytes()
+    bad = torch.from_numpy(rows).cuda()
+    bad[7, 3] = float("nan")
+    with pytest.raises(uha.InvalidArgument):
+        GPU_FN[metric](bad)

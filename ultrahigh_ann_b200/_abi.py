@@ -29,6 +29,8 @@ L1 = 1
 # uha_pair_backend
 PAIRS_DIRECT = 0
 PAIRS_GRAM = 1
+PAIRS_DIRECT_MAX32 = 2
+PAIRS_GRAM_MAX32 = 3
 
 # uha_strategy
 DIRECT = 0
@@ -191,6 +193,9 @@ SIGNATURES = {
                                               POINTER(ProbabilityReport)]),
     "uha_importance_probabilities_host": (c_int, [c_int, c_void_p, c_uint64, c_uint64,
                                                    c_int, c_void_p]),
+    "uha_importance_probabilities_device": (c_int, [c_int, c_int, c_void_p, c_uint64,
+                                                     c_uint64, c_int, c_uint64, c_void_p,
+                                                     POINTER(ProbabilityReport)]),
     "uha_sha256": (c_int, [c_void_p, c_uint64, c_void_p]),
     "uha_sha256_file": (c_int, [c_char_p, c_void_p]),
     "uha_probabilities_save": (c_int, [c_char_p, c_int, c_uint64, c_void_p, c_void_p,

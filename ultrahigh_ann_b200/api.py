@@ -363,14 +363,29 @@ def _rows_input(values):
 
 
 def _probabilities_gpu(metric: int, representatives, device: int,
-                       gram: bool = False, pair_chunks: int = 128) -> ProbabilityResult:
-    rows = _matrix(representatives)
-    out = np.zeros(rows.shape[1], dtype=np.float64)
+                       gram: bool = False, pair_chunks: int = 128,
+                       maxima: str = "binary64") -> ProbabilityResult:
+    if maxima not in ("binary64", "binary32"):
+        raise InvalidArgument("column maxima are binary64 or binary32")
+    single = maxima == "binary32"
+    backend = ((_abi.PAIRS_GRAM_MAX32 if single else _abi.PAIRS_GRAM) if gram
+               else (_abi.PAIRS_DIRECT_MAX32 if single else _abi.PAIRS_DIRECT))
     rep = _abi.ProbabilityReport()
-    _check(_abi.load().uha_importance_probabilities(
-        device, metric, _ptr(rows), rows.shape[0], rows.shape[1],
-        _abi.PAIRS_GRAM if gram else _abi.PAIRS_DIRECT, ctypes.c_uint64(pair_chunks),
-        _ptr(out), ctypes.byref(rep)))
+    if isinstance(representatives, DeviceMatrix) or _is_cuda_tensor(representatives):
+        # a matrix on the device: no host copy (float32, densely packed rows)
+        m = _rows_input(representatives)
+        if m.dtype != "float32" or (m.row_stride not in (None, m.columns)):
+            raise InvalidArgument("device representatives must be dense float32 rows")
+        out = np.zeros(int(m.columns), dtype=np.float64)
+        _check(_abi.load().uha_importance_probabilities_device(
+            device, metric, ctypes.c_void_p(int(m.pointer)), int(m.rows), int(m.columns),
+            backend, ctypes.c_uint64(pair_chunks), _ptr(out), ctypes.byref(rep)))
+    else:
+        rows = _matrix(representatives)
+        out = np.zeros(rows.shape[1], dtype=np.float64)
+        _check(_abi.load().uha_importance_probabilities(
+            device, metric, _ptr(rows), rows.shape[0], rows.shape[1], backend,
+            ctypes.c_uint64(pair_chunks), _ptr(out), ctypes.byref(rep)))
     info = cuda_runtime_info(device)
     return ProbabilityResult(out, info.device_name if info else "", device,
                              rep.pair_count, rep.pair_chunks, rep.device_working_set_bytes,
@@ -381,24 +396,32 @@ def _probabilities_gpu(metric: int, representatives, device: int,
 
 def compute_l2_importance_probabilities_gpu(representatives, device: int = 0,
                                             pair_chunks: int = 128,
-                                            distance_backend: str = "direct"
+                                            distance_backend: str = "direct",
+                                            maxima: str = "binary64"
                                             ) -> ProbabilityResult:
     """include/ultrahigh_ann/hnsvw25/l2/importance_sampling.hpp:49-52;
-    distance_backend "direct" or "gram" (the reference's "cublas" backend)."""
+    distance_backend "direct" or "gram" (the reference's "cublas" backend).
+    Appended: representatives may be a DeviceMatrix or CUDA tensor (no host
+    copy), and maxima="binary32" forms the per-column maxima in binary32
+    (within 3e-7 relative; for full-size builds)."""
     if pair_chunks <= 0:
         raise InvalidArgument("GPU pair chunk count must be positive")
     if distance_backend not in ("direct", "gram", "cublas"):
         raise InvalidArgument("unknown L2 GPU distance backend")
     return _probabilities_gpu(_abi.L2, representatives, device,
-                              gram=distance_backend != "direct", pair_chunks=pair_chunks)
+                              gram=distance_backend != "direct", pair_chunks=pair_chunks,
+                              maxima=maxima)
 
 
 def compute_l1_importance_probabilities_gpu(representatives, device: int = 0,
-                                            pair_chunks: int = 128) -> ProbabilityResult:
-    """include/ultrahigh_ann/hnsvw25/l1/importance_sampling.hpp:45-48."""
+                                            pair_chunks: int = 128,
+                                            maxima: str = "binary64") -> ProbabilityResult:
+    """include/ultrahigh_ann/hnsvw25/l1/importance_sampling.hpp:45-48 (device
+    input and binary32 maxima as for L2)."""
     if pair_chunks <= 0:
         raise InvalidArgument("GPU pair chunk count must be positive")
-    return _probabilities_gpu(_abi.L1, representatives, device, pair_chunks=pair_chunks)
+    return _probabilities_gpu(_abi.L1, representatives, device, pair_chunks=pair_chunks,
+                              maxima=maxima)
 
 
 def _tune_dict(r) -> dict:

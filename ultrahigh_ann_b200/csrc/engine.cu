@@ -2182,148 +2182,190 @@ extern "C" uha_status uha_precision_scores(const uha_index* index, uha_workspace
 
 // ---------------------------------------------------------- probabilities
 
+namespace {
+
+// The probability build of uha_importance_probabilities(_device): the rows
+// either copied from the host (host_rows) or already on the device
+// (device_rows, checked for finiteness there).
+void importance_probabilities(int device, uha_metric metric, const float* host_rows,
+                              const float* device_rows, uint64_t row_count,
+                              uint64_t dimension, uha_pair_backend backend,
+                              uint64_t pair_chunks, double* out,
+                              uha_probability_report* report)
+{
+    require(pair_chunks != 0, UHA_INVALID_ARGUMENT, "GPU pair chunk count must be positive");
+    require(metric == UHA_L2 || metric == UHA_L1, UHA_INVALID_ARGUMENT, "unknown metric");
+    require(backend == UHA_PAIRS_DIRECT || backend == UHA_PAIRS_GRAM ||
+                backend == UHA_PAIRS_DIRECT_MAX32 || backend == UHA_PAIRS_GRAM_MAX32,
+            UHA_INVALID_ARGUMENT, "unknown pair-distance backend");
+    const bool gram = backend == UHA_PAIRS_GRAM || backend == UHA_PAIRS_GRAM_MAX32;
+    const bool single = backend == UHA_PAIRS_DIRECT_MAX32 || backend == UHA_PAIRS_GRAM_MAX32;
+    require(!(metric == UHA_L1 && gram), UHA_INVALID_ARGUMENT,
+            "L1 distance has no matrix-multiplication identity");
+    require(out != nullptr || dimension == 0, UHA_INVALID_ARGUMENT, "output must not be null");
+    const float* given = host_rows != nullptr ? host_rows : device_rows;
+    require(given != nullptr || row_count * dimension == 0, UHA_INVALID_ARGUMENT,
+            "representative matrix must not be null");
+    checked_mul(row_count, dimension, "representative matrix");
+    if (host_rows != nullptr) {
+        for (uint64_t i = 0; i < row_count * dimension; ++i) {
+            if (!std::isfinite(host_rows[i])) {
+                fail(UHA_INVALID_ARGUMENT, "representatives must be finite");
+            }
+        }
+    }
+    uha_probability_report rep{};
+    rep.pair_count = row_count < 2 ? 0 : row_count * (row_count - 1) / 2;
+    rep.pair_chunks = rep.pair_count == 0
+                          ? 0
+                          : (dimension == 0 ? 1 : std::min(pair_chunks, rep.pair_count));
+    for (uint64_t j = 0; j < dimension; ++j) {
+        out[j] = 0.0;
+    }
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        fail(UHA_RUNTIME_ERROR, "no usable CUDA device");
+    }
+    require(device >= 0 && device < count, UHA_INVALID_ARGUMENT,
+            "CUDA device index is out of range");
+    if (row_count < 2 || dimension == 0) {
+        if (report != nullptr) {
+            *report = rep;
+        }
+        return;
+    }
+    require(row_count <= 65535ull * 32, UHA_LENGTH_ERROR,
+            "probability construction supports at most 2097120 rows");
+    DeviceGuard guard(device);
+    const uint64_t pair_bytes =
+        checked_mul(row_count, row_count * sizeof(double), "pair matrix");
+    const uint64_t row_bytes =
+        host_rows != nullptr ? checked_mul(row_count, dimension * sizeof(float), "rows") : 0;
+    const uint64_t need = checked_add(
+        checked_add(row_bytes, gram ? checked_add(pair_bytes, pair_bytes, "pair matrix")
+                                    : pair_bytes,
+                    "probability working set"),
+        dimension * sizeof(double), "probability working set");
+    size_t free_bytes = 0;
+    size_t total_bytes = 0;
+    check_cuda(cudaMemGetInfo(&free_bytes, &total_bytes), "cannot query CUDA memory");
+    if (need > free_bytes) {
+        fail(UHA_RUNTIME_ERROR, "probability working set exceeds free device memory");
+    }
+    rep.device_working_set_bytes = need;
+    cudaStream_t stream = nullptr;
+    check_cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking),
+               "cannot create CUDA stream");
+    struct StreamOwner {
+        cudaStream_t s;
+        ~StreamOwner() { cudaStreamDestroy(s); }
+    } owner{stream};
+    cudaEvent_t ev[5];
+    for (auto& e : ev) {
+        check_cuda(cudaEventCreate(&e), "cannot create CUDA event");
+    }
+    struct EventOwner {
+        cudaEvent_t* e;
+        ~EventOwner()
+        {
+            for (int i = 0; i < 5; ++i) {
+                cudaEventDestroy(e[i]);
+            }
+        }
+    } event_owner{ev};
+    DeviceBuffer<float> copied(host_rows != nullptr ? row_count * dimension : 0);
+    DeviceBuffer<double> inverse(row_count * row_count);
+    DeviceBuffer<double> gram_matrix(gram ? row_count * row_count : 0);
+    DeviceBuffer<unsigned long long> maxima(dimension);
+    DeviceBuffer<int> flag(1);
+    const float* rows = host_rows != nullptr ? copied.get() : device_rows;
+    check_cuda(cudaEventRecord(ev[0], stream), "event");
+    if (host_rows != nullptr) {
+        check_cuda(cudaMemcpyAsync(copied.get(), host_rows, copied.bytes(),
+                                   cudaMemcpyHostToDevice, stream),
+                   "cannot copy representatives to the CUDA device");
+    } else {
+        int host_flag = 0;
+        check_cuda(cudaMemsetAsync(flag.get(), 0, sizeof(int), stream), "cannot clear flag");
+        uha::launch_finite_check(device_rows, row_count * dimension, flag.get(), stream);
+        check_cuda(cudaMemcpyAsync(&host_flag, flag.get(), sizeof(int),
+                                   cudaMemcpyDeviceToHost, stream),
+                   "cannot copy the finiteness flag");
+        check_cuda(cudaStreamSynchronize(stream), "finiteness check failed");
+        require(host_flag == 0, UHA_INVALID_ARGUMENT, "representatives must be finite");
+    }
+    check_cuda(cudaMemsetAsync(inverse.get(), 0, inverse.bytes(), stream),
+               "cannot clear pair matrix");
+    check_cuda(cudaMemsetAsync(maxima.get(), 0, maxima.bytes(), stream),
+               "cannot clear column maxima");
+    check_cuda(cudaEventRecord(ev[1], stream), "event");
+    const int m = metric == UHA_L2 ? 0 : 1;
+    if (gram) {
+        uha::launch_gram_inverse_distances(rows, row_count, dimension, gram_matrix.get(),
+                                           inverse.get(), stream);
+    } else {
+        uha::launch_pair_distances(m, rows, row_count, dimension, inverse.get(), stream);
+    }
+    check_cuda(cudaEventRecord(ev[2], stream), "event");
+    for (uint64_t c = 0; c < rep.pair_chunks; ++c) {
+        const uint64_t begin = rep.pair_count * c / rep.pair_chunks;
+        const uint64_t end = rep.pair_count * (c + 1) / rep.pair_chunks;
+        uha::launch_coordinate_maxima(m, rows, row_count, dimension, inverse.get(),
+                                      maxima.get(), begin, end, stream, single);
+    }
+    check_cuda(cudaEventRecord(ev[3], stream), "event");
+    std::vector<unsigned long long> bits(dimension);
+    check_cuda(cudaMemcpyAsync(bits.data(), maxima.get(), maxima.bytes(),
+                               cudaMemcpyDeviceToHost, stream),
+               "cannot copy probabilities from the CUDA device");
+    check_cuda(cudaEventRecord(ev[4], stream), "event");
+    check_cuda(cudaStreamSynchronize(stream), "probability kernels failed");
+    for (uint64_t j = 0; j < dimension; ++j) {
+        double v = 0.0;
+        std::memcpy(&v, &bits[j], sizeof(v));
+        out[j] = metric == UHA_L2 ? std::min(1.0, v) : v;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    rep.host_to_device_ms = ms;
+    cudaEventElapsedTime(&ms, ev[1], ev[2]);
+    rep.inverse_distance_ms = ms;
+    cudaEventElapsedTime(&ms, ev[2], ev[3]);
+    rep.coordinate_maximum_ms = ms;
+    cudaEventElapsedTime(&ms, ev[3], ev[4]);
+    rep.device_to_host_ms = ms;
+    cudaEventElapsedTime(&ms, ev[0], ev[4]);
+    rep.total_ms = ms;
+    if (report != nullptr) {
+        *report = rep;
+    }
+}
+
+}  // namespace
+
 extern "C" uha_status uha_importance_probabilities(
     int device, uha_metric metric, const float* rows, uint64_t row_count,
     uint64_t dimension, uha_pair_backend backend, uint64_t pair_chunks,
     double* out, uha_probability_report* report)
 {
     return guarded([&] {
-        require(pair_chunks != 0, UHA_INVALID_ARGUMENT,
-                "GPU pair chunk count must be positive");
-        require(metric == UHA_L2 || metric == UHA_L1, UHA_INVALID_ARGUMENT,
-                "unknown metric");
-        require(backend == UHA_PAIRS_DIRECT || backend == UHA_PAIRS_GRAM,
-                UHA_INVALID_ARGUMENT, "unknown pair-distance backend");
-        require(!(metric == UHA_L1 && backend == UHA_PAIRS_GRAM),
-                UHA_INVALID_ARGUMENT,
-                "L1 distance has no matrix-multiplication identity");
-        const bool gram = backend == UHA_PAIRS_GRAM;
-        require(out != nullptr || dimension == 0, UHA_INVALID_ARGUMENT,
-                "output must not be null");
-        require(rows != nullptr || row_count * dimension == 0,
-                UHA_INVALID_ARGUMENT, "representative matrix must not be null");
-        checked_mul(row_count, dimension, "representative matrix");
-        for (uint64_t i = 0; i < row_count * dimension; ++i) {
-            if (!std::isfinite(rows[i])) {
-                fail(UHA_INVALID_ARGUMENT, "representatives must be finite");
-            }
-        }
-        uha_probability_report rep{};
-        rep.pair_count = row_count < 2 ? 0 : row_count * (row_count - 1) / 2;
-        rep.pair_chunks = rep.pair_count == 0
-                              ? 0
-                              : (dimension == 0 ? 1 : std::min(pair_chunks, rep.pair_count));
-        for (uint64_t j = 0; j < dimension; ++j) {
-            out[j] = 0.0;
-        }
-        int count = 0;
-        if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
-            cudaGetLastError();
-            fail(UHA_RUNTIME_ERROR, "no usable CUDA device");
-        }
-        require(device >= 0 && device < count, UHA_INVALID_ARGUMENT,
-                "CUDA device index is out of range");
-        if (row_count < 2 || dimension == 0) {
-            if (report != nullptr) {
-                *report = rep;
-            }
-            return;
-        }
-        require(row_count <= 65535ull * 32, UHA_LENGTH_ERROR,
-                "probability construction supports at most 2097120 rows");
-        DeviceGuard guard(device);
-        const uint64_t pair_bytes =
-            checked_mul(row_count, row_count * sizeof(double), "pair matrix");
-        const uint64_t need = checked_add(
-            checked_add(checked_mul(row_count, dimension * sizeof(float), "rows"),
-                        gram ? checked_add(pair_bytes, pair_bytes, "pair matrix")
-                             : pair_bytes,
-                        "probability working set"),
-            dimension * sizeof(double), "probability working set");
-        size_t free_bytes = 0;
-        size_t total_bytes = 0;
-        check_cuda(cudaMemGetInfo(&free_bytes, &total_bytes),
-                   "cannot query CUDA memory");
-        if (need > free_bytes) {
-            fail(UHA_RUNTIME_ERROR,
-                 "probability working set exceeds free device memory");
-        }
-        rep.device_working_set_bytes = need;
-        cudaStream_t stream = nullptr;
-        check_cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking),
-                   "cannot create CUDA stream");
-        struct StreamOwner {
-            cudaStream_t s;
-            ~StreamOwner() { cudaStreamDestroy(s); }
-        } owner{stream};
-        cudaEvent_t ev[5];
-        for (auto& e : ev) {
-            check_cuda(cudaEventCreate(&e), "cannot create CUDA event");
-        }
-        struct EventOwner {
-            cudaEvent_t* e;
-            ~EventOwner()
-            {
-                for (int i = 0; i < 5; ++i) {
-                    cudaEventDestroy(e[i]);
-                }
-            }
-        } event_owner{ev};
-        DeviceBuffer<float> d_rows(row_count * dimension);
-        DeviceBuffer<double> inverse(row_count * row_count);
-        DeviceBuffer<double> gram_matrix(gram ? row_count * row_count : 0);
-        DeviceBuffer<unsigned long long> maxima(dimension);
-        check_cuda(cudaEventRecord(ev[0], stream), "event");
-        check_cuda(cudaMemcpyAsync(d_rows.get(), rows, d_rows.bytes(),
-                                   cudaMemcpyHostToDevice, stream),
-                   "cannot copy representatives to the CUDA device");
-        check_cuda(cudaMemsetAsync(inverse.get(), 0, inverse.bytes(), stream),
-                   "cannot clear pair matrix");
-        check_cuda(cudaMemsetAsync(maxima.get(), 0, maxima.bytes(), stream),
-                   "cannot clear column maxima");
-        check_cuda(cudaEventRecord(ev[1], stream), "event");
-        const int m = metric == UHA_L2 ? 0 : 1;
-        if (gram) {
-            uha::launch_gram_inverse_distances(d_rows.get(), row_count, dimension,
-                                               gram_matrix.get(), inverse.get(),
-                                               stream);
-        } else {
-            uha::launch_pair_distances(m, d_rows.get(), row_count, dimension,
-                                       inverse.get(), stream);
-        }
-        check_cuda(cudaEventRecord(ev[2], stream), "event");
-        for (uint64_t c = 0; c < rep.pair_chunks; ++c) {
-            const uint64_t begin = rep.pair_count * c / rep.pair_chunks;
-            const uint64_t end = rep.pair_count * (c + 1) / rep.pair_chunks;
-            uha::launch_coordinate_maxima(m, d_rows.get(), row_count, dimension,
-                                          inverse.get(), maxima.get(), begin, end,
-                                          stream);
-        }
-        check_cuda(cudaEventRecord(ev[3], stream), "event");
-        std::vector<unsigned long long> bits(dimension);
-        check_cuda(cudaMemcpyAsync(bits.data(), maxima.get(), maxima.bytes(),
-                                   cudaMemcpyDeviceToHost, stream),
-                   "cannot copy probabilities from the CUDA device");
-        check_cuda(cudaEventRecord(ev[4], stream), "event");
-        check_cuda(cudaStreamSynchronize(stream), "probability kernels failed");
-        for (uint64_t j = 0; j < dimension; ++j) {
-            double v = 0.0;
-            std::memcpy(&v, &bits[j], sizeof(v));
-            out[j] = metric == UHA_L2 ? std::min(1.0, v) : v;
-        }
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, ev[0], ev[1]);
-        rep.host_to_device_ms = ms;
-        cudaEventElapsedTime(&ms, ev[1], ev[2]);
-        rep.inverse_distance_ms = ms;
-        cudaEventElapsedTime(&ms, ev[2], ev[3]);
-        rep.coordinate_maximum_ms = ms;
-        cudaEventElapsedTime(&ms, ev[3], ev[4]);
-        rep.device_to_host_ms = ms;
-        cudaEventElapsedTime(&ms, ev[0], ev[4]);
-        rep.total_ms = ms;
-        if (report != nullptr) {
-            *report = rep;
-        }
+        require(rows != nullptr || row_count * dimension == 0, UHA_INVALID_ARGUMENT,
+                "representative matrix must not be null");
+        importance_probabilities(device, metric, rows != nullptr ? rows : nullptr, nullptr,
+                                 row_count, dimension, backend, pair_chunks, out, report);
+    });
+}
+
+extern "C" uha_status uha_importance_probabilities_device(
+    int device, uha_metric metric, const float* device_rows, uint64_t row_count,
+    uint64_t dimension, uha_pair_backend backend, uint64_t pair_chunks, double* out,
+    uha_probability_report* report)
+{
+    return guarded([&] {
+        require(device_rows != nullptr || row_count * dimension == 0, UHA_INVALID_ARGUMENT,
+                "representative matrix must not be null");
+        importance_probabilities(device, metric, nullptr, device_rows, row_count, dimension,
+                                 backend, pair_chunks, out, report);
     });
 }

@@ -433,12 +433,16 @@ void launch_gram_inverse_distances(const float* rows, uint64_t row_count,
                                    double* inverse_distances,
                                    cudaStream_t stream);
 // Folds the pairs [pair_begin, pair_end) of the row-major order of pairs
-// a < b into the per-column maxima (one launch per chunk of pairs).
+// a < b into the per-column maxima (one launch per chunk of pairs); `single`:
+// the contributions in binary32 (within 3e-7 relative).
 void launch_coordinate_maxima(int metric, const float* rows,
                               uint64_t row_count, uint64_t dim,
                               const double* inverse_distances,
                               unsigned long long* maxima_bits,
                               uint64_t pair_begin, uint64_t pair_end,
-                              cudaStream_t stream);
+                              cudaStream_t stream, bool single = false);
+// flag |= 1 when any of the `count` values is not finite
+void launch_finite_check(const float* values, uint64_t count, int* flag,
+                         cudaStream_t stream);
 
 }  // namespace uha

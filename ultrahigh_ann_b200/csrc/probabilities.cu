@@ -25,6 +25,8 @@
 #include "common.h"
 #include "kernels.h"
 
+#include <algorithm>
+
 namespace uha {
 namespace {
 
@@ -215,6 +217,13 @@ __global__ void gram_to_inverse_kernel(const double* __restrict__ gram,
     }
 }
 
+// kSingle: the contributions in binary32 (the difference, its square or
+// absolute value, the product with the binary32-rounded inverse distance and
+// the maximum: within 5 binary32 roundings, 3e-7 relative, of the binary64
+// contributions) for builds where the binary64 pipe is the limit. A 32 x 32
+// block of pairs holding a distance below 2^-100 (an inverse near or past
+// binary32's range, squares that may be subnormal) is folded in binary64.
+template <bool kSingle>
 __global__ void __launch_bounds__(kColumns)
     coordinate_max_kernel(int metric, const float* __restrict__ rows,
                           uint32_t row_count, uint64_t dim,
@@ -243,6 +252,7 @@ __global__ void __launch_bounds__(kColumns)
         sa[r * kColumns + threadIdx.x] = v;
     }
     double m = 0.0;
+    bool large = false;
     for (uint32_t tb = ta; tb < blocks; ++tb) {
         const uint32_t b0 = tb * kPairBlock;
         __syncthreads();
@@ -268,20 +278,39 @@ __global__ void __launch_bounds__(kColumns)
                 }
             }
             sinv[i] = v;
+            large = large || v > 0x1p100;
         }
-        __syncthreads();
-        for (int ra = 0; ra < kPairBlock; ++ra) {
-            const double va = sa[ra * kColumns + threadIdx.x];
+        const bool block64 = __syncthreads_or(large ? 1 : 0) != 0;
+        large = false;
+        if (kSingle && !block64) {
+            float m32 = 0.f;
+            for (int ra = 0; ra < kPairBlock; ++ra) {
+                const float va = sa[ra * kColumns + threadIdx.x];
 #pragma unroll 8
-            for (int rb = 0; rb < kPairBlock; ++rb) {
-                const double d =
-                    __dsub_rn(va, static_cast<double>(sb[rb * kColumns + threadIdx.x]));
-                const double w = sinv[ra * kPairBlock + rb];
-                // (d * d) * inverse or |d| * inverse, each product rounded as
-                // the CPU rounds it (importance_sampling.cpp:36-41 of l2, :26-30 of l1)
-                const double c = metric == 0 ? __dmul_rn(__dmul_rn(d, d), w)
-                                             : __dmul_rn(fabs(d), w);
-                m = fmax(m, c);
+                for (int rb = 0; rb < kPairBlock; ++rb) {
+                    const float d = __fsub_rn(va, sb[rb * kColumns + threadIdx.x]);
+                    const float w = __double2float_rn(sinv[ra * kPairBlock + rb]);
+                    const float c = metric == 0 ? __fmul_rn(__fmul_rn(d, d), w)
+                                                : __fmul_rn(fabsf(d), w);
+                    m32 = fmaxf(m32, c);
+                }
+            }
+            m = fmax(m, static_cast<double>(m32));
+        } else {
+            for (int ra = 0; ra < kPairBlock; ++ra) {
+                const double va = sa[ra * kColumns + threadIdx.x];
+#pragma unroll 8
+                for (int rb = 0; rb < kPairBlock; ++rb) {
+                    const double d =
+                        __dsub_rn(va, static_cast<double>(sb[rb * kColumns + threadIdx.x]));
+                    const double w = sinv[ra * kPairBlock + rb];
+                    // (d * d) * inverse or |d| * inverse, each product rounded
+                    // as the CPU rounds it (importance_sampling.cpp:36-41 of
+                    // l2, :26-30 of l1)
+                    const double c = metric == 0 ? __dmul_rn(__dmul_rn(d, d), w)
+                                                 : __dmul_rn(fabs(d), w);
+                    m = fmax(m, c);
+                }
             }
         }
     }
@@ -326,12 +355,41 @@ void launch_gram_inverse_distances(const float* rows, uint64_t row_count,
     check_cuda(cudaGetLastError(), "cannot launch Gram refinement kernel");
 }
 
+namespace {
+
+__global__ void finite_check_kernel(const float* __restrict__ values, uint64_t count,
+                                    int* flag)
+{
+    bool bad = false;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+         i < count; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        bad = bad || !isfinite(values[i]);
+    }
+    if (__any_sync(0xffffffffu, bad) && threadIdx.x % 32 == 0) {
+        atomicOr(flag, 1);
+    }
+}
+
+}  // namespace
+
+void launch_finite_check(const float* values, uint64_t count, int* flag,
+                         cudaStream_t stream)
+{
+    if (count == 0) {
+        return;
+    }
+    const uint64_t blocks = std::min<uint64_t>((count + 255) / 256, 148ull * 32);
+    finite_check_kernel<<<static_cast<uint32_t>(blocks), 256, 0, stream>>>(values, count,
+                                                                           flag);
+    check_cuda(cudaGetLastError(), "cannot launch the finiteness check");
+}
+
 void launch_coordinate_maxima(int metric, const float* rows,
                               uint64_t row_count, uint64_t dim,
                               const double* inverse_distances,
                               unsigned long long* maxima_bits,
                               uint64_t pair_begin, uint64_t pair_end,
-                              cudaStream_t stream)
+                              cudaStream_t stream, bool single)
 {
     if (pair_begin >= pair_end) {
         return;
@@ -356,17 +414,17 @@ void launch_coordinate_maxima(int metric, const float* rows,
     }
     const size_t smem = kPairBlock * kPairBlock * sizeof(double) +
                         2 * kPairBlock * kColumns * sizeof(float);
-    static bool configured[kMaxDevices] = {};
+    static bool configured[kMaxDevices][2] = {};
     const int dev = current_device();
-    if (!configured[dev]) {
-        check_cuda(cudaFuncSetAttribute(coordinate_max_kernel,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+    const auto kernel = single ? coordinate_max_kernel<true> : coordinate_max_kernel<false>;
+    if (!configured[dev][single ? 1 : 0]) {
+        check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         static_cast<int>(smem)),
                    "cannot configure probability column kernel");
-        configured[dev] = true;
+        configured[dev][single ? 1 : 0] = true;
     }
     const dim3 grid(static_cast<uint32_t>(column_blocks), last_block - first_block + 1);
-    coordinate_max_kernel<<<grid, kColumns, smem, stream>>>(
+    kernel<<<grid, kColumns, smem, stream>>>(
         metric, rows, static_cast<uint32_t>(row_count), dim, inverse_distances,
         maxima_bits, first_block, pair_begin, pair_end);
     check_cuda(cudaGetLastError(), "cannot launch probability column kernel");
