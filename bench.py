@@ -54,7 +54,7 @@ def parse_args():
                    help="only the precision-strategy table (one JSON line)")
     p.add_argument("--only", default="",
                    choices=["", "precision", "batched", "serving", "centroids", "wide",
-                            "hierarchies"],
+                            "hierarchies", "flat"],
                    help="only this section of the bench (one JSON line)")
     p.add_argument("--full-probabilities", action="store_true",
                    help="with --only hierarchies: each index's importance "
@@ -609,6 +609,34 @@ def centroids_flat(queries=3013):
 
 
 _PROBS: dict = {}
+
+
+def flat_batch1(ds, nq=2048):
+    """The flat indexes (T = 32, L2 and L1) of the r = 7,028, d = 60,660 data
+    at batch 1 and 8: one uha_query_many call of `nq` device-resident queries
+    per line after an identical warm-up call (the suite's timing, without its
+    reference checks; for profiler captures of the fused flat query)."""
+    import torch
+
+    import ultrahigh_ann_b200 as uha
+
+    qdev = torch.from_numpy(np.ascontiguousarray(ds.queries[:nq])).cuda()
+    out = []
+    for metric, cls in (("l2", uha.CudaSampledCoordinateL2AnnIndex),
+                        ("l1", uha.CudaSampledCoordinateL1AnnIndex)):
+        index = cls(ds.rows, _probabilities(metric, ds.rows), 32, uha.MT19937_64(0))
+        for B in (1, 8):
+            ws = index.make_query_workspace(B)
+            res = np.zeros(nq, np.uint64)
+            index.query_many(qdev.data_ptr(), nq, B, res, ws, on_device=True)
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            index.query_many(qdev.data_ptr(), nq, B, res, ws, on_device=True)
+            secs = time.perf_counter() - t
+            out.append({"metric": metric, "T": 32, "k": len(index.coordinate_sample),
+                        "batch": B, "queries": nq, "queries_per_s": round(nq / secs, 1),
+                        "us_per_query": round(secs / nq * 1e6, 3)})
+    return out
 
 
 def _probabilities(metric: str, rows):
@@ -1262,7 +1290,8 @@ def main():
 
 
 def run_section(args):
-    """One section (batched, serving or centroids) alone on one GPU."""
+    """One section (batched, serving, centroids, wide, hierarchies or flat)
+    alone on one GPU."""
     from ultrahigh_ann_b200 import synthetic
 
     if args.only == "centroids":
@@ -1281,6 +1310,10 @@ def run_section(args):
         return
     ds = synthetic.row_dataset(rows=ROWS, classes=33, queries=4096, d=DIM, seed=1,
                                query_stream=0)
+    if args.only == "flat":
+        print(json.dumps({"workload": f"flat_t32_r{ROWS}_d{DIM}", "flat": flat_batch1(ds)}),
+              flush=True)
+        return
     fn = batched if args.only == "batched" else serving
     print(json.dumps({"workload": f"{args.only}_r{ROWS}_d{DIM}", args.only: fn(ds)}),
           flush=True)

@@ -1,6 +1,7 @@
 """The fused candidate selection of the precision strategies (indexes of at
-least 16,384 rows, plans of one K split): the first rows are scored as a
-sample, each query's k-th smallest sample estimate is its threshold, and the
+least 16,384 rows, plans of one K split): whole row tiles spread over the
+index are scored as a sample, each query's k-th smallest sample estimate is
+its threshold, and the
 score kernel's epilogue keeps only the keys (estimate, row) at or below it; a
 selection over those keys gives the candidates.
 
@@ -10,7 +11,8 @@ and norms), so every answer is the reference CPU's argmin among them (the
 oracle over the candidate rows); a list that overflows (thousands of rows tied
 at the threshold) makes the engine answer the call again with the slab
 selection, with the same answers; an L2 hierarchy on the precision strategy
-through the fused path agrees with the oracle, alone and in a graph batch.
+through the fused path agrees with the oracle, alone and in a graph batch;
+pipelined calls of several batches answer as batches called one at a time.
 """
 from __future__ import annotations
 
@@ -101,3 +103,24 @@ def test_fused_hierarchy_agrees_with_oracle(oracle_module):
     batch = uha.QueryBatch([(index, 96, BF16)], autotune=True)
     res = batch.run([ds.queries])
     assert np.array_equal(res[0][0], got)
+
+
+@pytest.mark.parametrize("strategy", [BF16, FP8])
+def test_fused_selection_in_pipelined_calls(strategy):
+    """One query_many call of several batches (the re-score of a batch runs on
+    a second stream behind the next batch's scores) answers as the same
+    batches answered one call at a time."""
+    torch = pytest.importorskip("torch")
+    ds = synthetic.row_dataset(rows=20000, classes=17, queries=192, d=96, seed=31)
+    index = uha.CudaExactL2Index(ds.rows)
+    want, want_dist = _run(index, ds.queries, 64, strategy, 16)
+    ws = index.make_query_workspace(64)
+    ws.set_candidates(16)
+    qdev = torch.from_numpy(ds.queries).cuda()
+    got = np.zeros(192, np.uint64)
+    dist = np.zeros(192, np.float64)
+    index.query_many(qdev.data_ptr(), 192, 64, got, ws, strategy, dist, on_device=True)
+    assert np.array_equal(got, want)
+    assert np.allclose(dist, want_dist, rtol=DIST_RTOL, atol=1e-30)
+    host = index.query_many(ds.queries, 192, 64, None, ws, strategy)
+    assert np.array_equal(host, want)

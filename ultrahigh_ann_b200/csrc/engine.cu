@@ -1220,12 +1220,15 @@ uha::LowpPlan enqueue_lowp_scores(const uha_index* index, uha_workspace* ws,
 }
 
 // Whether a batch of n takes the fused selection: plans of one K split on
-// indexes of at least kFilterMinRows rows, up to 64 candidates, on the
-// workspace stream (not pipelined), and not turned off for this call.
+// indexes of at least kFilterMinRows rows, up to 64 candidates, and not
+// turned off for this call. Every kernel of the selection runs on the
+// workspace stream and writes the batch's own candidate slot before a
+// pipelined call hands the batch to its re-score stream, so the next batch
+// reuses the selection's buffers in stream order.
 bool filter_applies(const BatchContext& c, const uha::LowpPlan& plan, uint32_t k)
 {
-    return c.filter_candidates && !c.ws->filter_disabled && c.finish_stream == nullptr &&
-           plan.splits == 1 && c.index->rows >= uha::kFilterMinRows && k >= 1 && k <= 64;
+    return c.filter_candidates && !c.ws->filter_disabled && plan.splits == 1 &&
+           c.index->rows >= uha::kFilterMinRows && k >= 1 && k <= 64;
 }
 
 // The k candidates per query of a precision strategy into `candidates`; the
