@@ -334,7 +334,8 @@ def summarize(line: dict) -> dict:
                                                  for k in ("device_ms", "kernels_per_run",
                                                            "answers_equal_graph")},
                                   "l2_bf16_device_ms":
-                                      (hf.get("l2_bf16_rerank") or {}).get("device_ms")}
+                                      (hf.get("l2_bf16_rerank") or {}).get("device_ms"),
+                                  "autotune": hf.get("autotune")}
     return out
 
 
@@ -951,7 +952,14 @@ def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=1
         specs[k]["alone_ms"] = round(ls["device_ms"], 3)
         specs[k]["alone_scan_ms"] = round(ls["scan_ms"], 3)
         specs[k]["replayed"] = ls["replayed_queries"]
-        specs[k]["tuned_scan_ms"] = round(batch.tuning(k)["best_ms"], 3)
+        tune = batch.tuning(k)
+        specs[k]["tuned_scan_ms"] = round(tune["best_ms"], 3)
+        specs[k]["tuning"] = {"kernel": tune["kernel"], "candidates": tune["candidates"],
+                              "default_ms": round(tune["default_ms"], 3),
+                              "changed": bool(tune["candidates"] and
+                                              tune["best_ms"] < tune["default_ms"]),
+                              "queries_per_pass": tune["queries_per_pass"],
+                              "splits": tune["splits"]}
         del ws
     # the same batch with the L2 hierarchies on the BF16 precision strategy
     # (tensor-core projection and scores, 32 candidates, binary64 re-score)
@@ -994,6 +1002,10 @@ def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=1
     best = min(ms)
     return {"workload": f"hierarchical_16_indexes_r{rows}_d{dim}_bf16",
             "indexes": specs, "queries_per_index": per_index,
+            "autotune": {"pairs_changed": sum(1 for sp in specs if sp["tuning"]["changed"]),
+                         "median_pairs_changed": sum(1 for sp in specs
+                                                     if sp["tuning"]["kernel"] == "median"
+                                                     and sp["tuning"]["changed"])},
             "queries_per_s": round(total / (best * 1e-3), 1),
             "device_ms": round(best, 3), "device_ms_runs": [round(m, 3) for m in ms],
             "graph_nodes": st["graph_nodes"], "kernels_per_run": st["kernel_launches"],
