@@ -851,11 +851,17 @@ def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=1
             del x
             torch.cuda.empty_cache()
         probs = None
+        # reported at once: the build takes minutes
+        print(json.dumps({"full_probability_build": full_report}), file=sys.stderr,
+              flush=True)
     else:
         head = data.rows[:1024].float().cpu().numpy()
         probs = {"l2": uha.compute_l2_importance_probabilities_gpu(head).probabilities,
                  "l1": uha.compute_l1_importance_probabilities_gpu(head).probabilities}
     prob_s = time.perf_counter() - t
+
+    def probs_of(metric, r):
+        return probs[metric] if probs is not None else probs_by_rows[(metric, r)]
     specs, indexes, seeds = [], [], []
     t = time.perf_counter()
     i = 0
@@ -868,8 +874,7 @@ def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=1
                        else uha.CudaHierarchicalL1AnnIndex)
                 ix = cls(uha.DeviceMatrix.from_torch(data.rows[:r]), 32, p,
                          uha.MT19937_64(300 + i),
-                         importance_probabilities=(probs[metric] if probs is not None
-                                                   else probs_by_rows[(metric, r)]))
+                         importance_probabilities=probs_of(metric, r))
                 seeds.append(300 + i)
                 indexes.append(ix)
                 specs.append({"metric": metric, "rows": r, "T": 32, "p": p,
@@ -895,7 +900,8 @@ def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=1
         if spec["metric"] == "l2":
             gaussian.append((k, uha.CudaHierarchicalL2AnnIndex(
                 uha.DeviceMatrix.from_torch(data.rows[:spec["rows"]]), 32, spec["p"],
-                uha.MT19937_64(seeds[k]), importance_probabilities=probs["l2"],
+                uha.MT19937_64(seeds[k]),
+                importance_probabilities=probs_of("l2", spec["rows"]),
                 projection="gaussian")))
     data.rows = None
     torch.cuda.empty_cache()
@@ -993,7 +999,9 @@ def hierarchies_full(per_index=4096, dim=262_144, rows=65_536, reps=3, checked=1
         ok += _projected_check(ix, spec["metric"], sampled[k].astype(np.float64),
                                q_host[:checked, cols].astype(np.float64),
                                res[k][0][picks[:checked]])
-    reference = hierarchy_reference_parity(indexes, specs, seeds, probs, sampled,
+    reference = hierarchy_reference_parity(indexes, specs, seeds,
+                                           [probs_of(sp["metric"], sp["rows"]) for sp in specs],
+                                           sampled,
                                            q_host[:ref_queries], picks[:ref_queries],
                                            [r[0] for r in res])
     projections = gaussian_vs_rademacher(gaussian, specs, res, qdev, per_index,
@@ -1085,7 +1093,7 @@ def gaussian_vs_rademacher(gaussian, specs, res, qdev, per_index, picks, exact_d
             "exact": "binary64 squared L2 over all 262,144 coordinates"}
 
 
-def hierarchy_reference_parity(indexes, specs, seeds, probs, sampled, q_host, picks,
+def hierarchy_reference_parity(indexes, specs, seeds, spec_probs, sampled, q_host, picks,
                                answers):
     """Each hierarchy's answers on the picked queries against the reference's
     own HierarchicalL{2,1}AnnIndex (oracle/_ref) built over the same sampled
@@ -1101,8 +1109,9 @@ def hierarchy_reference_parity(indexes, specs, seeds, probs, sampled, q_host, pi
     t = time.perf_counter()
     equal, samples_equal, total = 0, 0, 0
     per_index = []
-    for ix, spec, seed, rows_k, want in zip(indexes, specs, seeds, sampled, answers):
-        cols, mult, invp, state = O.ref_sample(probs[spec["metric"]], spec["T"], seed)
+    for ix, spec, seed, rows_k, want, pr in zip(indexes, specs, seeds, sampled, answers,
+                                                spec_probs):
+        cols, mult, invp, state = O.ref_sample(pr, spec["T"], seed)
         cs = ix.coordinate_sample
         same_sample = bool(np.array_equal(cols, cs.source_columns) and
                            np.array_equal(mult, cs.multiplicities) and
