@@ -217,13 +217,6 @@ __global__ void gram_to_inverse_kernel(const double* __restrict__ gram,
     }
 }
 
-// kSingle: the contributions in binary32 (the difference, its square or
-// absolute value, the product with the binary32-rounded inverse distance and
-// the maximum: within 5 binary32 roundings, 3e-7 relative, of the binary64
-// contributions) for builds where the binary64 pipe is the limit. A 32 x 32
-// block of pairs holding a distance below 2^-100 (an inverse near or past
-// binary32's range, squares that may be subnormal) is folded in binary64.
-template <bool kSingle>
 __global__ void __launch_bounds__(kColumns)
     coordinate_max_kernel(int metric, const float* __restrict__ rows,
                           uint32_t row_count, uint64_t dim,
@@ -252,7 +245,6 @@ __global__ void __launch_bounds__(kColumns)
         sa[r * kColumns + threadIdx.x] = v;
     }
     double m = 0.0;
-    bool large = false;
     for (uint32_t tb = ta; tb < blocks; ++tb) {
         const uint32_t b0 = tb * kPairBlock;
         __syncthreads();
@@ -278,25 +270,9 @@ __global__ void __launch_bounds__(kColumns)
                 }
             }
             sinv[i] = v;
-            large = large || v > 0x1p100;
         }
-        const bool block64 = __syncthreads_or(large ? 1 : 0) != 0;
-        large = false;
-        if (kSingle && !block64) {
-            float m32 = 0.f;
-            for (int ra = 0; ra < kPairBlock; ++ra) {
-                const float va = sa[ra * kColumns + threadIdx.x];
-#pragma unroll 8
-                for (int rb = 0; rb < kPairBlock; ++rb) {
-                    const float d = __fsub_rn(va, sb[rb * kColumns + threadIdx.x]);
-                    const float w = __double2float_rn(sinv[ra * kPairBlock + rb]);
-                    const float c = metric == 0 ? __fmul_rn(__fmul_rn(d, d), w)
-                                                : __fmul_rn(fabsf(d), w);
-                    m32 = fmaxf(m32, c);
-                }
-            }
-            m = fmax(m, static_cast<double>(m32));
-        } else {
+        __syncthreads();
+        {
             for (int ra = 0; ra < kPairBlock; ++ra) {
                 const double va = sa[ra * kColumns + threadIdx.x];
 #pragma unroll 8
@@ -314,6 +290,105 @@ __global__ void __launch_bounds__(kColumns)
             }
         }
     }
+    if (col < dim && m > 0.0) {
+        atomicMax(maxima_bits + col,
+                  static_cast<unsigned long long>(__double_as_longlong(m)));
+    }
+}
+
+// The binary32 form of coordinate_max_kernel's fold (the same pairs, the
+// same contributions rounded in binary32: within 3e-7 relative), arranged for
+// the binary32 pipe: each thread's 32 values of its column of row blocks A and
+// B stay in registers (every thread reads only its own column), a pair
+// block's inverse distances are rounded to binary32 once in shared memory, and
+// the 32 x 32 pairs are unrolled: about four binary32 instructions per
+// pair-column. A pair block holding a distance below 2^-100 is folded in
+// binary64, exactly as coordinate_max_kernel folds it.
+__global__ void __launch_bounds__(kColumns)
+    coordinate_max32_kernel(int metric, const float* __restrict__ rows,
+                            uint32_t row_count, uint64_t dim,
+                            const double* __restrict__ inverse,
+                            unsigned long long* __restrict__ maxima_bits,
+                            uint32_t first_block, uint64_t pair_begin, uint64_t pair_end)
+{
+    __shared__ __align__(16) float sw[kPairBlock * kPairBlock];
+    __shared__ double sw64[kPairBlock * kPairBlock];
+    const uint64_t col = blockIdx.x * static_cast<uint64_t>(kColumns) + threadIdx.x;
+    const uint32_t ta = first_block + blockIdx.y;
+    const uint32_t a0 = ta * kPairBlock;
+    const uint32_t blocks = (row_count + kPairBlock - 1) / kPairBlock;
+    const uint64_t r64 = row_count;
+    float va[kPairBlock];
+#pragma unroll
+    for (int r = 0; r < kPairBlock; ++r) {
+        va[r] = a0 + r < row_count && col < dim
+                    ? rows[static_cast<uint64_t>(a0 + r) * dim + col]
+                    : 0.f;
+    }
+    float m32[4] = {0.f, 0.f, 0.f, 0.f};  // four chains of the maximum
+    double m = 0.0;
+    for (uint32_t tb = ta; tb < blocks; ++tb) {
+        const uint32_t b0 = tb * kPairBlock;
+        float vb[kPairBlock];
+#pragma unroll
+        for (int r = 0; r < kPairBlock; ++r) {
+            vb[r] = b0 + r < row_count && col < dim
+                        ? rows[static_cast<uint64_t>(b0 + r) * dim + col]
+                        : 0.f;
+        }
+        __syncthreads();  // the previous block's weights are no longer read
+        bool large = false;
+        for (int i = threadIdx.x; i < kPairBlock * kPairBlock; i += blockDim.x) {
+            const int ra = i / kPairBlock;
+            const int rb = i % kPairBlock;
+            double v = 0.0;
+            const uint64_t a = a0 + ra;
+            const uint64_t b = b0 + rb;
+            if (a < b && b < row_count) {
+                const uint64_t pair = a * (2 * r64 - a - 1) / 2 + (b - a - 1);
+                if (pair >= pair_begin && pair < pair_end) {
+                    v = inverse[a * row_count + b];
+                }
+            }
+            sw64[i] = v;
+            sw[i] = v > 0x1p100 ? 0.f : __double2float_rn(v);
+            large = large || v > 0x1p100;
+        }
+        if (__syncthreads_or(large ? 1 : 0) == 0) {
+#pragma unroll
+            for (int ra = 0; ra < kPairBlock; ++ra) {
+#pragma unroll
+                for (int rb = 0; rb < kPairBlock; ++rb) {
+                    const float d = __fsub_rn(va[ra], vb[rb]);
+                    const float w = sw[ra * kPairBlock + rb];
+                    const float c = metric == 0 ? __fmul_rn(__fmul_rn(d, d), w)
+                                                : __fmul_rn(fabsf(d), w);
+                    m32[ra % 4] = fmaxf(m32[ra % 4], c);
+                }
+            }
+        } else {
+#pragma unroll 1
+            for (int ra = 0; ra < kPairBlock; ++ra) {
+#pragma unroll 1
+                for (int rb = 0; rb < kPairBlock; ++rb) {
+                    // the values again from memory: runtime indices would
+                    // move va and vb out of registers
+                    const double xa = a0 + ra < row_count && col < dim
+                                          ? rows[static_cast<uint64_t>(a0 + ra) * dim + col]
+                                          : 0.f;
+                    const double xb = b0 + rb < row_count && col < dim
+                                          ? rows[static_cast<uint64_t>(b0 + rb) * dim + col]
+                                          : 0.f;
+                    const double d = __dsub_rn(xa, xb);
+                    const double w = sw64[ra * kPairBlock + rb];
+                    const double c = metric == 0 ? __dmul_rn(__dmul_rn(d, d), w)
+                                                 : __dmul_rn(fabs(d), w);
+                    m = fmax(m, c);
+                }
+            }
+        }
+    }
+    m = fmax(m, static_cast<double>(fmaxf(fmaxf(m32[0], m32[1]), fmaxf(m32[2], m32[3]))));
     if (col < dim && m > 0.0) {
         atomicMax(maxima_bits + col,
                   static_cast<unsigned long long>(__double_as_longlong(m)));
@@ -414,17 +489,24 @@ void launch_coordinate_maxima(int metric, const float* rows,
     }
     const size_t smem = kPairBlock * kPairBlock * sizeof(double) +
                         2 * kPairBlock * kColumns * sizeof(float);
-    static bool configured[kMaxDevices][2] = {};
+    const dim3 grid(static_cast<uint32_t>(column_blocks), last_block - first_block + 1);
+    if (single) {
+        coordinate_max32_kernel<<<grid, kColumns, 0, stream>>>(
+            metric, rows, static_cast<uint32_t>(row_count), dim, inverse_distances,
+            maxima_bits, first_block, pair_begin, pair_end);
+        check_cuda(cudaGetLastError(), "cannot launch probability column kernel");
+        return;
+    }
+    static bool configured[kMaxDevices] = {};
     const int dev = current_device();
-    const auto kernel = single ? coordinate_max_kernel<true> : coordinate_max_kernel<false>;
-    if (!configured[dev][single ? 1 : 0]) {
-        check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (!configured[dev]) {
+        check_cuda(cudaFuncSetAttribute(coordinate_max_kernel,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         static_cast<int>(smem)),
                    "cannot configure probability column kernel");
-        configured[dev][single ? 1 : 0] = true;
+        configured[dev] = true;
     }
-    const dim3 grid(static_cast<uint32_t>(column_blocks), last_block - first_block + 1);
-    kernel<<<grid, kColumns, smem, stream>>>(
+    coordinate_max_kernel<<<grid, kColumns, smem, stream>>>(
         metric, rows, static_cast<uint32_t>(row_count), dim, inverse_distances,
         maxima_bits, first_block, pair_begin, pair_end);
     check_cuda(cudaGetLastError(), "cannot launch probability column kernel");
