@@ -44,8 +44,10 @@ __global__ void __launch_bounds__(256)
     if (tb < ta) {
         return;
     }
-    __shared__ float sa[kPairBlock][kPairSlab + 1];
-    __shared__ float sb[kPairBlock][kPairSlab + 1];
+    // the slabs converted to binary64 once as they are staged (the values are
+    // exact), not once per pair in the loops below
+    __shared__ double sa[kPairBlock][kPairSlab + 1];
+    __shared__ double sb[kPairBlock][kPairSlab + 1];
     const int ty = threadIdx.x / 8;  // 0..31: row a within block
     const int tx = threadIdx.x % 8;  // b = tx + 8 j
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
@@ -66,8 +68,8 @@ __global__ void __launch_bounds__(256)
                     vb = rows[static_cast<uint64_t>(b0 + r) * dim + col];
                 }
             }
-            sa[r][c] = va;
-            sb[r][c] = vb;
+            sa[r][c] = static_cast<double>(va);
+            sb[r][c] = static_cast<double>(vb);
         }
         __syncthreads();
         if (metric == 0) {
@@ -78,8 +80,7 @@ __global__ void __launch_bounds__(256)
                 const double va = sa[ty][c];
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    const double d =
-                        __dsub_rn(va, static_cast<double>(sb[tx + 8 * j][c]));
+                    const double d = __dsub_rn(va, sb[tx + 8 * j][c]);
                     acc[j] = __dadd_rn(acc[j], __dmul_rn(d, d));
                 }
             }
@@ -93,7 +94,7 @@ __global__ void __launch_bounds__(256)
                 if (c0 + c + 4 <= grouped_end) {
 #pragma unroll
                     for (int j = 0; j < 4; ++j) {
-                        const float* vb = &sb[tx + 8 * j][c];
+                        const double* vb = &sb[tx + 8 * j][c];
                         const double t0 = fabs(__dsub_rn(sa[ty][c], vb[0]));
                         const double t1 = fabs(__dsub_rn(sa[ty][c + 1], vb[1]));
                         const double t2 = fabs(__dsub_rn(sa[ty][c + 2], vb[2]));
