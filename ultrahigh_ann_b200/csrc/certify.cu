@@ -1275,6 +1275,8 @@ constexpr int kFlatCopyTimeout = 16;
 constexpr uint64_t kFlatChunkBytes = 32 * 1024;
 // query entries a flat query thread gathers at a time
 constexpr int kFlatGather = 8;
+// float4 loads in flight per lane when rows are read from global memory
+constexpr int kFlatDirectLoads = 8;
 
 // Per-row accumulation of one lane: binary32, column order, four terms per
 // float4 group (the same arithmetic as small_query_kernel); the query and the
@@ -1305,7 +1307,9 @@ __device__ __forceinline__ float flat_terms(int op, float acc, const float4 a,
 // grid = (row blocks, batch), kFinalizeThreads threads. At entry one thread
 // of every CTA starts bulk copies (the TMA engine, cp.async.bulk) of its row
 // block into shared memory: `chunk_rows` rows per copy, two buffers, the next
-// chunk copied while one is scanned. Meanwhile the CTA gathers its query's
+// chunk copied while one is scanned (rows too long for a pass of the CTA in
+// one copy, chunk_rows 0, are instead loaded from global memory into
+// registers, kFlatDirectLoads per lane in flight). Meanwhile the CTA gathers its query's
 // sampled (or all) coordinates into shared memory with the preparation
 // kernels' finiteness flags (and the column weights of a weighted L1 index).
 // Then it computes the binary32 distance of each row with kLanes lanes per row
@@ -1349,7 +1353,10 @@ __global__ void __launch_bounds__(kFinalizeThreads, 3)
     const uint32_t first_row = blockIdx.x * span;
     const uint32_t end_row = min(sq.row_count, first_row + span);
     const uint32_t row_words = static_cast<uint32_t>(sq.padded_dim);
-    const uint32_t nchunks = (end_row - first_row + chunk_rows - 1) / chunk_rows;
+    // chunk_rows 0: rows too long for a pass of the CTA in one copy are read
+    // straight from global memory instead
+    const uint32_t nchunks =
+        chunk_rows != 0 ? (end_row - first_row + chunk_rows - 1) / chunk_rows : 0u;
     auto issue = [&](uint32_t c) {
         const uint32_t r0 = first_row + c * chunk_rows;
         const uint32_t bytes = min(chunk_rows, end_row - r0) * row_words * 4u;
@@ -1437,6 +1444,53 @@ __global__ void __launch_bounds__(kFinalizeThreads, 3)
         const float4* q4 = reinterpret_cast<const float4*>(qv);
         const float4* w4 = reinterpret_cast<const float4*>(wv);
         RowScan scan;
+        // the butterfly over the row's lanes, the distance and the CTA's two
+        // smallest
+        auto record = [&](float acc, uint32_t row, bool valid) {
+#pragma unroll
+            for (int o = kLanes / 2; o > 0; o /= 2) {
+                acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            }
+            if (valid && sub == 0) {
+                dist[row] = acc;
+                if (!(acc <= FLT_MAX)) {
+                    scan.overflow = true;
+                } else if (acc < scan.k1) {
+                    scan.k2 = scan.k1;
+                    scan.k1 = acc;
+                    scan.r1 = row;
+                } else if (acc < scan.k2) {
+                    scan.k2 = acc;
+                }
+            }
+        };
+        if (chunk_rows == 0 && !bad) {
+            // long rows: kFlatDirectLoads float4 loads in flight per lane, the
+            // same column order per lane
+            for (uint32_t base = first_row; base < end_row; base += kRowsPerStep) {
+                const uint32_t row = base + group;
+                const bool valid = row < end_row;
+                const float4* r4 = reinterpret_cast<const float4*>(
+                    sq.rows + static_cast<uint64_t>(valid ? row : first_row) * row_words);
+                float acc = 0.f;
+                for (uint64_t g0 = sub; g0 < groups; g0 += kFlatDirectLoads * kLanes) {
+                    float4 b[kFlatDirectLoads];
+#pragma unroll
+                    for (int j = 0; j < kFlatDirectLoads; ++j) {
+                        const uint64_t g = g0 + static_cast<uint64_t>(j) * kLanes;
+                        b[j] = g < groups ? __ldg(r4 + g) : make_float4(0.f, 0.f, 0.f, 0.f);
+                    }
+#pragma unroll
+                    for (int j = 0; j < kFlatDirectLoads; ++j) {
+                        const uint64_t g = g0 + static_cast<uint64_t>(j) * kLanes;
+                        if (g < groups) {
+                            acc = flat_terms(sq.op, acc, q4[g], b[j], w4, g);
+                        }
+                    }
+                }
+                record(acc, row, valid);
+            }
+        }
         uint32_t failed_chunk = nchunks;
         for (uint32_t c = 0; c < nchunks; ++c) {
             // every thread sees the chunk complete (or the copy given up)
@@ -1464,23 +1518,7 @@ __global__ void __launch_bounds__(kFinalizeThreads, 3)
                     for (uint64_t g = sub; g < groups; g += kLanes) {
                         acc = flat_terms(sq.op, acc, q4[g], r4[g], w4, g);
                     }
-#pragma unroll
-                    for (int o = kLanes / 2; o > 0; o /= 2) {
-                        acc += __shfl_xor_sync(0xffffffffu, acc, o);
-                    }
-                    const uint32_t row = r0 + lr;
-                    if (valid && sub == 0) {
-                        dist[row] = acc;
-                        if (!(acc <= FLT_MAX)) {
-                            scan.overflow = true;
-                        } else if (acc < scan.k1) {
-                            scan.k2 = scan.k1;
-                            scan.k1 = acc;
-                            scan.r1 = row;
-                        } else if (acc < scan.k2) {
-                            scan.k2 = acc;
-                        }
-                    }
+                    record(acc, r0 + lr, valid);
                 }
             }
             // the buffer is free again: copy chunk c + 2 into it
@@ -2470,15 +2508,14 @@ FlatPlan plan_flat_query(uint64_t rows, uint64_t padded_dim, uint64_t batch,
     plan.lanes = lanes;
     plan.span = static_cast<uint32_t>(span);
     plan.blocks = static_cast<uint32_t>((rows + span - 1) / span);
-    // rows per bulk copy: whole passes of the CTA up to kFlatChunkBytes, else
-    // as many rows as fit (at least one: a row is at most 32 KB)
+    // rows per bulk copy: whole passes of the CTA up to kFlatChunkBytes; rows
+    // too long for one pass in a copy (a pass would leave most threads idle
+    // and serialise many small copies) are read from global memory directly
+    // (chunk_rows 0)
     const uint64_t row_bytes = padded_dim * sizeof(float);
-    uint64_t chunk = kFlatChunkBytes / row_bytes / step * step;
-    if (chunk == 0) {
-        chunk = std::max<uint64_t>(1, kFlatChunkBytes / row_bytes);
-    }
+    const uint64_t chunk = kFlatChunkBytes / row_bytes / step * step;
     plan.chunk_rows = static_cast<uint32_t>(std::min<uint64_t>(chunk, span));
-    plan.buffers = plan.chunk_rows >= span ? 1u : 2u;
+    plan.buffers = plan.chunk_rows == 0 ? 0u : plan.chunk_rows >= span ? 1u : 2u;
     uint32_t log_lanes = 0;
     while ((1u << log_lanes) < lanes) {
         ++log_lanes;
