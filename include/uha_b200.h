@@ -419,12 +419,13 @@ uha_status uha_batch_create(const uha_index* const* indexes,
 /* The same batch run as two persistent, cooperative kernel launches (the
  * early stages with the tile scan's register budget, then the late stages at
  * twice the residency; captured in the batch's graph with the result
- * copies): every CTA drains, stage by
- * stage, a work list of units from all pairs (gather, projection, L2 tile
- * scan or median sample / count / survivor passes, certified argmin with
- * replay, reported distances), separated by grid-wide barriers whose waits
- * give up after about two seconds (the run then fails with
- * UHA_RUNTIME_ERROR). Each unit runs the device code of the standalone
+ * copies). Each kernel drains a device work queue of units from all pairs
+ * (gather, projection, L2 tile scan or median sample / count / survivor
+ * passes, certified argmin with replay, reported distances), ordered stage by
+ * stage: a CTA takes the next unit and waits only until that unit's pair has
+ * completed its earlier stages, so pairs overlap across stages with no
+ * grid-wide barrier. A wait gives up after about two seconds (the run then
+ * fails with UHA_RUNTIME_ERROR). Each unit runs the device code of the standalone
  * kernel it replaces, so each pair's answers equal a uha_query of the same
  * queries. Serves hierarchical indexes with the certified direct strategy
  * (projection dimension up to 256; L2 hierarchies with more than 8 queries;
@@ -444,10 +445,12 @@ uha_status uha_batch_run(uha_batch* batch, const float* const* queries,
                          int queries_on_device, uint64_t* out_indices,
                          double* out_distances);
 uha_status uha_batch_stats_get(const uha_batch* batch, uha_batch_stats* out);
-/* Stage durations of the last run of a persistent batch, in ms, as CTA 0 of
- * the kernel saw them (between the grid barriers; %globaltimer): the first
- * `count` of them into out_ms, zero past the last stage. *stages = number of
- * stages (0 for a batch that is not persistent). No reference counterpart. */
+/* Stage times of the last run of a persistent batch, in ms (%globaltimer):
+ * stage s from the time all units of the earlier stages had completed to the
+ * time all units up to stage s had (stages of different pairs overlap; the
+ * sum is the run's kernel time). The first `count` of them into out_ms, zero
+ * past the last stage. *stages = number of stages (0 for a batch that is not
+ * persistent). No reference counterpart. */
 uha_status uha_batch_stage_times(const uha_batch* batch, double* out_ms, uint64_t count,
                                  uint64_t* stages);
 uha_status uha_batch_tuning(const uha_batch* batch, uint64_t pair,

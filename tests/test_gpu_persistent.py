@@ -1,8 +1,8 @@
 """The persistent multi-index batch (uha_batch_create_persistent): two
 cooperative kernel launches per run (early and late stages) that drain every
 pair's stages (gather, projection, L2 tile scan or median sample / count /
-survivor, certified argmin with replay, reported distances) from one work
-list, with grid-wide barriers between stages.
+survivor, certified argmin with replay, reported distances) from a device work
+queue, each unit waiting only for its own pair's earlier stages.
 
 Each unit runs the device code of the standalone kernel it replaces, so every
 pair must answer exactly as query_batch of the same queries does (indices,

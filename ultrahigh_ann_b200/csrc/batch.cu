@@ -300,7 +300,8 @@ struct uha_batch {
     uha_batch_stats last{};
     // persistent form
     bool persistent = false;
-    uha::DeviceBuffer<unsigned int> barrier;  // [0] arrivals [1] generation [2] status
+    // the work queue words (kPersistentQueueWords), then the status word
+    uha::DeviceBuffer<unsigned int> queue;
     uha::PinnedBuffer<int> host_status;
     uha::DeviceBuffer<unsigned long long> clock;  // stage boundaries (ns)
     uha::PinnedBuffer<unsigned long long> host_clock;
@@ -395,18 +396,21 @@ void build_persistent(uha_batch* batch)
     uint32_t used = 0;
     uha::plan_persistent_batch(pairs.data(), count, params.segments, &used, &params.plan);
     std::copy(pairs.begin(), pairs.end(), params.pairs);
-    batch->barrier.allocate(3);
+    batch->queue.allocate(uha::kPersistentQueueWords + 1);
     batch->host_status.allocate(1);
     batch->host_status.get()[0] = 0;
     batch->clock.allocate(uha::kPersistentStages + 1);
     batch->host_clock.allocate(uha::kPersistentStages + 1);
     std::fill(batch->host_clock.get(), batch->host_clock.get() + uha::kPersistentStages + 1,
               0ull);
-    check_cuda(cudaMemsetAsync(batch->barrier.get(), 0, batch->barrier.bytes(), batch->stream),
-               "cannot clear the persistent batch barrier");
+    check_cuda(cudaMemsetAsync(batch->queue.get(), 0, batch->queue.bytes(), batch->stream),
+               "cannot clear the persistent batch queue");
+    check_cuda(cudaMemsetAsync(batch->clock.get(), 0, batch->clock.bytes(), batch->stream),
+               "cannot clear the persistent batch stage clock");
     check_cuda(cudaStreamSynchronize(batch->stream), "cannot clear the persistent batch");
-    params.plan.barrier = batch->barrier.get();
-    params.plan.status = reinterpret_cast<int*>(batch->barrier.get() + 2);
+    params.plan.queue = batch->queue.get();
+    params.plan.status =
+        reinterpret_cast<int*>(batch->queue.get() + uha::kPersistentQueueWords);
     params.plan.clock = batch->clock.get();
     for (int part = 0; part < 2; ++part) {
         batch->grid[part] = uha::persistent_grid(part, params.plan.smem_bytes[part]);
@@ -599,13 +603,13 @@ extern "C" uha_status uha_batch_run(uha_batch* batch, const float* const* querie
         check_cuda(cudaEventRecord(batch->stop, batch->stream), "event");
         check_cuda(cudaStreamSynchronize(batch->stream), "CUDA batch failed");
         if (batch->persistent && batch->host_status.get()[0] != 0) {
-            // a grid barrier wait ran out: reset the barrier for the next run
-            check_cuda(cudaMemsetAsync(batch->barrier.get(), 0, batch->barrier.bytes(),
+            // a work queue wait ran out: reset the queue for the next run
+            check_cuda(cudaMemsetAsync(batch->queue.get(), 0, batch->queue.bytes(),
                                        batch->stream),
-                       "cannot reset the persistent batch barrier");
+                       "cannot reset the persistent batch queue");
             check_cuda(cudaStreamSynchronize(batch->stream), "CUDA batch failed");
             batch->host_status.get()[0] = 0;
-            fail(UHA_RUNTIME_ERROR, "persistent batch barrier wait timed out");
+            fail(UHA_RUNTIME_ERROR, "persistent batch work queue wait timed out");
         }
         float ms = 0.f;
         check_cuda(cudaEventElapsedTime(&ms, batch->start, batch->stop), "event");
@@ -666,11 +670,21 @@ extern "C" uha_status uha_batch_stage_times(const uha_batch* batch, double* out_
         require(batch != nullptr && stages != nullptr && (out_ms != nullptr || count == 0),
                 UHA_INVALID_ARGUMENT, "batch and outputs must not be null");
         *stages = batch->persistent ? uha::kPersistentStages : 0;
+        // stages overlap (a pair's later stages run while others are in
+        // earlier ones): stage s is reported from the time every unit of the
+        // stages before it had completed to the time every unit up to s had
+        // (a stage without units, whose entry is stale, reports zero)
         const unsigned long long* c = batch->host_clock.get();
+        unsigned long long frontier = c[0];
         for (uint64_t s = 0; s < count; ++s) {
-            const bool have = batch->persistent && s < uha::kPersistentStages &&
-                              c[s + 1] >= c[s] && c[0] != 0;
-            out_ms[s] = have ? static_cast<double>(c[s + 1] - c[s]) * 1e-6 : 0.0;
+            const bool have = batch->persistent && s < uha::kPersistentStages && c[0] != 0;
+            if (!have) {
+                out_ms[s] = 0.0;
+                continue;
+            }
+            const unsigned long long e = std::max(frontier, c[s + 1]);
+            out_ms[s] = static_cast<double>(e - frontier) * 1e-6;
+            frontier = e;
         }
     });
 }

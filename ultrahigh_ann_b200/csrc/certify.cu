@@ -2030,43 +2030,26 @@ enum PersistentKind : uint32_t {
 };
 
 // about 2^23 polls of ~256 ns: seconds, far above any stage of a batch
-constexpr uint32_t kBarrierSpins = 1u << 23;
+constexpr uint32_t kQueueSpins = 1u << 23;
 
-// Grid-wide barrier of the cooperative persistent kernel (every CTA is
-// resident): thread 0 reads the generation, arrives, and the last arrival
-// resets the count and advances the generation; the others poll it with a
-// bounded wait. False (and the status set) when the wait ran out.
-__device__ bool persistent_barrier(unsigned int* bar, int* status)
+// Thread 0 of a CTA: waits until `*count` reaches `target` (bounded). False,
+// with the status set, when the wait ran out or another CTA already failed.
+__device__ bool persistent_wait(const unsigned int* count, unsigned int target, int* status)
 {
-    __shared__ int passed;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned int* generation = bar + 1;
-        const unsigned int gen = *generation;
-        __threadfence();
-        const unsigned int arrived = atomicAdd(bar, 1u);
-        if (arrived == gridDim.x - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-            passed = 1;
-        } else {
-            passed = 0;
-            for (uint32_t i = 0; i < kBarrierSpins; ++i) {
-                if (*generation != gen) {
-                    passed = 1;
-                    break;
-                }
-                __nanosleep(256);
-            }
-            if (!passed) {
-                atomicOr(status, 1);
-            }
+    const volatile unsigned int* c = count;
+    const volatile int* st = status;
+    for (uint32_t i = 0; i < kQueueSpins; ++i) {
+        if (*c >= target) {
+            __threadfence();  // the counted units' writes before this CTA's reads
+            return true;
         }
-        __threadfence();
+        if (*st != 0) {
+            return false;
+        }
+        __nanosleep(i < 64 ? 32 : 256);
     }
-    __syncthreads();
-    return passed != 0;
+    atomicOr(status, 1);
+    return false;
 }
 
 template <int PER_LANE>
@@ -2222,10 +2205,13 @@ __device__ void persistent_unit(const PersistentPair& d, uint32_t kind, uint32_t
 
 // The batch in two cooperative launches: the early stages [0, kPersistentSplit)
 // with the tile scan's register budget (2 CTAs per SM), then the late stages
-// [kPersistentSplit, kPersistentStages) at 4 CTAs per SM. Stage after stage,
-// every CTA takes units blockIdx.x, blockIdx.x + gridDim.x, ... of the
-// stage's list, then waits at the grid barrier; a barrier that ran out ends
-// the kernel (the status word stops the next kernel too).
+// [kPersistentSplit, kPersistentStages) at 4 CTAs per SM. Each CTA takes units
+// from its kernel's queue head until the queue is drained; before a unit it
+// waits for the unit's pair to have completed its units of earlier stages,
+// after it counts the unit complete for its pair and its stage (the stage
+// count also dates the stage's end). A wait that ran out, or a status set by
+// another CTA, ends the CTA; the last CTA of the late kernel to finish zeroes
+// the queue for the next run.
 __device__ __forceinline__ unsigned long long global_timer_ns()
 {
     unsigned long long t;
@@ -2238,39 +2224,81 @@ __global__ void __launch_bounds__(kFinalizeThreads, kMinBlocks)
     persistent_stages_kernel(const __grid_constant__ PersistentParams params)
 {
     extern __shared__ __align__(16) unsigned char persistent_smem[];
+    constexpr bool kLate = kFirst >= kPersistentSplit;
+    __shared__ uint32_t next_unit;
+    __shared__ int unit_ready;
     const PersistentPlan& plan = params.plan;
+    unsigned int* queue = plan.queue;
     if (*static_cast<volatile int*>(plan.status) != 0) {
         return;  // the earlier kernel of this run gave up
     }
-    const bool timer = blockIdx.x == 0 && threadIdx.x == 0 && plan.clock != nullptr;
-    if (timer) {
+    if (blockIdx.x == 0 && threadIdx.x == 0 && plan.clock != nullptr) {
         plan.clock[kFirst] = global_timer_ns();
     }
-    for (int stage = kFirst; stage < kEnd; ++stage) {
-        const uint32_t units = plan.stage_units[stage];
-        const uint32_t seg_end = plan.stage_begin[stage + 1];
-        uint32_t seg = plan.stage_begin[stage];
-        for (uint32_t u = blockIdx.x; u < units; u += gridDim.x) {
-            while (seg + 1 < seg_end && params.segments[seg + 1].first <= u) {
-                ++seg;
+    const uint32_t end = plan.stage_first[kEnd];
+    uint32_t stage = kFirst;
+    uint32_t seg = plan.stage_begin[kFirst];
+    for (;;) {
+        if (threadIdx.x == 0) {
+            uint32_t item = end;
+            if (*static_cast<volatile int*>(plan.status) == 0) {
+                item = plan.stage_first[kFirst] +
+                       atomicAdd(queue + kQueueHead + (kLate ? 1 : 0), 1u);
             }
-            const PersistentSegment sg = params.segments[seg];
-            persistent_unit<(kFirst >= kPersistentSplit)>(params.pairs[sg.pair], sg.kind,
-                                                          u - sg.first, sg.units,
-                                                          persistent_smem);
-            __syncthreads();
+            next_unit = item;
         }
-        if (stage + 1 < kEnd) {
-            if (!persistent_barrier(plan.barrier, plan.status) ||
-                *static_cast<volatile int*>(plan.status) != 0) {
-                return;
+        __syncthreads();
+        const uint32_t item = next_unit;
+        if (item >= end) {
+            break;
+        }
+        while (item >= plan.stage_first[stage + 1]) {
+            ++stage;
+        }
+        const uint32_t u = item - plan.stage_first[stage];
+        seg = max(seg, plan.stage_begin[stage]);
+        while (seg + 1 < plan.stage_begin[stage + 1] && params.segments[seg + 1].first <= u) {
+            ++seg;
+        }
+        const PersistentSegment& sg = params.segments[seg];
+        if (threadIdx.x == 0) {
+            unit_ready = persistent_wait(queue + kQueuePairDone + sg.pair,
+                                         plan.pair_wait[sg.pair][stage], plan.status)
+                             ? 1
+                             : 0;
+        }
+        __syncthreads();
+        if (unit_ready == 0) {
+            return;  // the wait ran out, or another CTA's did (status set)
+        }
+        persistent_unit<kLate>(params.pairs[sg.pair], sg.kind, u - sg.first, sg.units,
+                               persistent_smem);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();  // the unit's writes before its completion count
+            atomicAdd(queue + kQueuePairDone + sg.pair, 1u);
+            const unsigned int done = atomicAdd(queue + kQueueStageDone + stage, 1u) + 1u;
+            if (done == plan.stage_units[stage] && plan.clock != nullptr) {
+                plan.clock[stage + 1] = global_timer_ns();
             }
         }
-        if (timer) {
-            plan.clock[stage + 1] = global_timer_ns();
+    }
+    if constexpr (kLate) {
+        if (threadIdx.x == 0) {
+            __threadfence();
+            if (atomicAdd(queue + kQueueFinished, 1u) == gridDim.x - 1) {
+                // every CTA of both kernels is past its last queue access
+                __threadfence();
+                for (uint32_t w = 0; w < kPersistentQueueWords; ++w) {
+                    queue[w] = 0u;
+                }
+            }
         }
     }
 }
+
+// kernel parameters are limited to 32,764 bytes
+static_assert(sizeof(PersistentParams) <= 32764, "persistent batch parameters too large");
 
 constexpr auto persistent_early_kernel = persistent_stages_kernel<0, kPersistentSplit, 2>;
 constexpr auto persistent_late_kernel =
@@ -2789,6 +2817,27 @@ void plan_persistent_batch(const PersistentPair* pairs, uint32_t count,
         group = std::max(group, smem);
     }
     plan->stage_begin[kPersistentStages] = n;
+    // queue positions of the stages and the per-pair completion targets
+    uint64_t first = 0;
+    for (int stage = 0; stage < kPersistentStages; ++stage) {
+        plan->stage_first[stage] = static_cast<uint32_t>(first);
+        first += plan->stage_units[stage];
+        if (first > 0xffffffffull) {
+            fail(UHA_LENGTH_ERROR, "persistent batch exceeds 2^32 units");
+        }
+    }
+    plan->stage_first[kPersistentStages] = static_cast<uint32_t>(first);
+    for (uint32_t i = 0; i < kPersistentMaxPairs; ++i) {
+        uint64_t before = 0;
+        for (int stage = 0; stage < kPersistentStages; ++stage) {
+            plan->pair_wait[i][stage] = static_cast<uint32_t>(before);
+            for (uint32_t g = plan->stage_begin[stage]; g < plan->stage_begin[stage + 1]; ++g) {
+                if (segments[g].pair == i) {
+                    before += segments[g].units;
+                }
+            }
+        }
+    }
     for (int k = 0; k < 2; ++k) {
         plan->smem_bytes[k] = static_cast<uint32_t>((smem_group[k] + 15) / 16 * 16);
     }

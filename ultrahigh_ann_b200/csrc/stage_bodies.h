@@ -2,20 +2,29 @@
 // and the shapes of the stage kernels they stand in for.
 //
 // Two kernels answer many (hierarchical index, query batch) pairs, one
-// cooperative launch each: every CTA drains, stage after stage, a work list of
-// units drawn from all pairs (a unit is one block of the stage kernel that the
-// standalone path would launch for that pair, run by the same device code from
+// cooperative launch each. A kernel's work is a device queue of units drawn
+// from all pairs (a unit is one block of the stage kernel that the standalone
+// path would launch for that pair, run by the same device code from
 // tile_body.cuh, hier_body.cuh and certify.cu, so both paths compute the same
-// values), with a grid-wide barrier between stages. The stages:
+// values), ordered stage by stage. Every CTA takes the next unit from the
+// queue head (one atomic), waits until the unit's pair has completed all its
+// units of earlier stages (a per-pair completion count), runs it and counts it
+// complete. There is no grid-wide barrier: a pair's later stages run while
+// other pairs are still in earlier ones, and a heavy unit delays only the
+// units that depend on it. The stages:
 //   0 clear per-pair counters and accumulators   4 median counts (L1)
 //   1 gather of the sampled coordinates          5 median survivors (L1), argmin (L2)
 //   2 binary32 projection with its error bound   6 argmin (L1), reported distances (L2)
 //   3 L2 tile scan + error root, median samples  7 reported distances (L1)
 // Stages 0-3 run in the first kernel (the tile scan's register budget, 2 CTAs
-// per SM), stages 4-7 in the second (4 CTAs per SM). A barrier wait gives up
-// after about two seconds, sets the batch status and ends the kernel (every
-// CTA then does the same at its next barrier, and the second kernel returns
-// at once), so a fault can never hold the GPU.
+// per SM), stages 4-7 in the second (4 CTAs per SM).
+//
+// Progress: units leave the queue in order, and a unit waits only on units of
+// its own pair earlier in the queue, all of them already taken by CTAs that
+// are resident (cooperative launch); the earliest unfinished unit never
+// waits. A wait still gives up after about two seconds: it sets the batch
+// status and ends its CTA (the others stop taking units, and the second
+// kernel returns at once), so a fault can never hold the GPU.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -131,24 +140,39 @@ struct PersistentSegment {
     uint32_t first;
 };
 
+constexpr uint32_t kPersistentMaxPairs = 32;
+constexpr uint32_t kPersistentMaxSegments = 2 * kPersistentMaxPairs * kPersistentStages + 1;
+
+// Words of the work queue's device state (zero at creation; the last CTA of
+// the second kernel zeroes them again at the end of a run):
+constexpr uint32_t kQueueHead = 0;       // [0, 2): units taken, per kernel
+constexpr uint32_t kQueueFinished = 2;   // CTAs of the second kernel done
+constexpr uint32_t kQueueStageDone = 3;  // units completed, per stage
+constexpr uint32_t kQueuePairDone = kQueueStageDone + kPersistentStages;  // per pair
+constexpr uint32_t kPersistentQueueWords = kQueuePairDone + kPersistentMaxPairs;
+
 struct PersistentPlan {
     uint32_t stage_begin[kPersistentStages + 1];  // segment ranges per stage
     uint32_t stage_units[kPersistentStages];
-    unsigned int* barrier;  // device: [0] arrivals, [1] generation (zero at creation)
-    int* status;            // device: nonzero when a barrier wait ran out
-    // device, kPersistentStages + 1 entries: %globaltimer (ns) at the start
-    // and at the end of each stage, as CTA 0 sees them (after each barrier;
-    // the last entry when CTA 0 finishes its units of the last stage)
+    // queue position of each stage's first unit (the units of all earlier
+    // stages, both kernels counted)
+    uint32_t stage_first[kPersistentStages + 1];
+    // a pair's units in stages before each stage: a unit of stage s starts
+    // once its pair has completed pair_wait[pair][s] units
+    uint32_t pair_wait[kPersistentMaxPairs][kPersistentStages];
+    unsigned int* queue;  // device, kPersistentQueueWords words
+    int* status;          // device: nonzero when a wait ran out
+    // device, kPersistentStages + 1 entries (%globaltimer, ns): [s] for the
+    // first stage of a kernel its start as CTA 0 sees it, [s + 1] when the
+    // last unit of stage s completed (untouched for a stage without units)
     unsigned long long* clock;
     uint32_t smem_bytes[2];  // dynamic shared memory of the two kernels
 };
 
-// The kernels' one parameter (about 25 KB, read from the constant bank like
+// The kernels' one parameter (about 26 KB, read from the constant bank like
 // any kernel argument: the units address the pairs' fields in place instead
 // of copying them into registers): the plan, the pairs and the segments,
 // grouped by stage.
-constexpr uint32_t kPersistentMaxPairs = 32;
-constexpr uint32_t kPersistentMaxSegments = 2 * kPersistentMaxPairs * kPersistentStages + 1;
 struct PersistentParams {
     PersistentPlan plan;
     PersistentPair pairs[kPersistentMaxPairs];
