@@ -1012,8 +1012,10 @@ class QueryBatch:
                 "replayed_queries": st.replayed_queries, "device_ms": st.device_ms}
 
     def stage_ms(self) -> list[float]:
-        """Stage durations (ms) of the last run of a persistent batch, as the
-        kernel's first CTA saw them between its grid barriers; [] otherwise."""
+        """Stage times (ms) of the last run of a persistent batch: stage s from
+        the completion of every unit of the earlier stages to the completion
+        of every unit up to s (pairs' stages overlap; the sum is the run's
+        kernel time); [] otherwise."""
         out = np.zeros(16, np.float64)
         stages = ctypes.c_uint64(0)
         _check(_abi.load().uha_batch_stage_times(self._handle, out.ctypes.data, 16,
