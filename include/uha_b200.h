@@ -416,10 +416,10 @@ uha_status uha_batch_create(const uha_index* const* indexes,
                             const uint64_t* query_counts,
                             const uha_strategy* strategies, uint64_t count,
                             int autotune, uha_batch** out);
-/* The same batch run as two persistent, cooperative kernel launches (the
- * early stages with the tile scan's register budget, then the late stages at
- * twice the residency; captured in the batch's graph with the result
- * copies). Each kernel drains a device work queue of units from all pairs
+/* The same batch run as three persistent, cooperative kernel launches (the
+ * gather and projection at 8 CTAs per SM, the tile scans and median samples
+ * with the tile scan's register budget, then the late stages at 4 CTAs per
+ * SM; captured in the batch's graph with the result copies). Each kernel drains a device work queue of units from all pairs
  * (gather, projection, L2 tile scan or median sample / count / survivor
  * passes, certified argmin with replay, reported distances), ordered stage by
  * stage: a CTA takes the next unit and waits only until that unit's pair has

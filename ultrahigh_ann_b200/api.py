@@ -930,8 +930,8 @@ class QueryBatch:
     CUDA graph launch (uha_batch_*): each pair's pipeline is captured on its
     own graph branch; with autotune each pair's scan shape is tuned first.
     With persistent=True (hierarchical indexes, direct strategy) the graph
-    holds one cooperative launch of the persistent batch kernel instead, which
-    drains every pair's stages from one work list
+    holds the three cooperative launches of the persistent batch kernels
+    instead, each draining a device work queue of every pair's units
     (uha_batch_create_persistent). Each pair's answers equal a query_batch of
     the same queries."""
 

@@ -13,10 +13,11 @@
 // into one CUDA graph: each pair's preparation, projection, scan, argmin /
 // re-score and result copies run on their own branch, forked from and joined
 // into one stream, so small indexes overlap on the device and the host issues
-// one launch per run. uha_batch_create_persistent captures instead one
-// cooperative launch of the persistent batch kernel (stage_bodies.h) that
-// drains every pair's stages from one work list (two cooperative launches:
-// the early and the late stages), plus the result copies.
+// one launch per run. uha_batch_create_persistent captures instead the
+// cooperative launches of the persistent batch kernels (stage_bodies.h:
+// gather and projection, tile scans and median samples, the late stages),
+// each draining a device work queue of every pair's units, plus the result
+// copies.
 #include "common.h"
 #include "engine_internal.h"
 #include "index_types.h"
@@ -306,7 +307,7 @@ struct uha_batch {
     uha::DeviceBuffer<unsigned long long> clock;  // stage boundaries (ns)
     uha::PinnedBuffer<unsigned long long> host_clock;
     std::unique_ptr<uha::PersistentParams> params;  // the kernels' parameter
-    uint32_t grid[2] = {0, 0};  // CTAs of the two persistent kernels
+    uint32_t grid[uha::kPersistentKernels] = {};  // CTAs of the persistent kernels
 
     ~uha_batch()
     {
@@ -412,7 +413,7 @@ void build_persistent(uha_batch* batch)
     params.plan.status =
         reinterpret_cast<int*>(batch->queue.get() + uha::kPersistentQueueWords);
     params.plan.clock = batch->clock.get();
-    for (int part = 0; part < 2; ++part) {
+    for (int part = 0; part < uha::kPersistentKernels; ++part) {
         batch->grid[part] = uha::persistent_grid(part, params.plan.smem_bytes[part]);
         require(batch->grid[part] != 0, UHA_RUNTIME_ERROR,
                 "the persistent batch kernel cannot be resident with its shared memory");
@@ -491,7 +492,7 @@ uha_status create_batch(const uha_index* const* indexes, const uint64_t* query_c
         try {
             if (batch->persistent) {
                 uha::launch_persistent_batch(*batch->params, batch->grid, batch->stream);
-                launches = 2;
+                launches = uha::kPersistentKernels;
                 for (uha_batch::Pair& p : batch->pairs) {
                     if (p.trivial) {
                         continue;

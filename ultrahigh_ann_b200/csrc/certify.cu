@@ -731,9 +731,32 @@ __device__ __forceinline__ float load_distance(const PartialView& v, uint32_t q,
     }
 }
 
+// One row of a thread's keyed scan (plain and projected bounds): binary32
+// overflow (inf or NaN) sets the flag, any other distance updates the two
+// smallest (the first row keeps a tie: rows arrive in increasing order).
+__device__ __forceinline__ void scan_keyed_row(RowScan& scan, float x, uint32_t row)
+{
+    if (!(x <= FLT_MAX)) {
+        scan.overflow = true;
+    } else if (x < scan.k1) {
+        scan.k2 = scan.k1;
+        scan.k1 = x;
+        scan.r1 = row;
+    } else if (x < scan.k2) {
+        scan.k2 = x;
+    }
+}
+
 // kArgminUnroll rows per thread per step, their loads issued together (with
 // one partial slab the load is a single instruction the compiler can batch).
-template <bool kSingleChunk>
+// Keyed bounds take a full step at once when its distances are finite (their
+// sum is): the step's smallest m and second smallest s2 (with multiplicity)
+// by min / max, then one merge with the thread's two smallest; the row of m
+// (its first occurrence) is looked up only when m is a new smallest. The
+// result equals scan_keyed_row applied row by row. Other steps (the last,
+// partial one; inf or NaN distances), and every step when !kStepMerge (the
+// persistent kernel's register budget), go row by row.
+template <bool kSingleChunk, bool kStepMerge>
 __device__ __forceinline__ void scan_rows(const PartialView& view, const Bound& bound,
                                           uint32_t q, uint32_t first_row, uint32_t end_row,
                                           RowScan& scan, Summary& s)
@@ -741,6 +764,50 @@ __device__ __forceinline__ void scan_rows(const PartialView& view, const Bound& 
     const bool keyed = bound.mode != BoundMode::median;
     for (uint32_t base = first_row + threadIdx.x; base < end_row;
          base += kFinalizeThreads * kArgminUnroll) {
+        if (kStepMerge && keyed && base + (kArgminUnroll - 1) * kFinalizeThreads < end_row) {
+            float d[kArgminUnroll];
+#pragma unroll
+            for (int u = 0; u < kArgminUnroll; ++u) {
+                d[u] = load_distance<kSingleChunk>(view, q, base + u * kFinalizeThreads);
+            }
+            float sum = d[0];
+#pragma unroll
+            for (int u = 1; u < kArgminUnroll; ++u) {
+                sum += d[u];
+            }
+            if (fabsf(sum) <= FLT_MAX) {
+                float m = d[0];
+                float s2 = __int_as_float(0x7f800000);
+#pragma unroll
+                for (int u = 1; u < kArgminUnroll; ++u) {
+                    s2 = fminf(s2, fmaxf(m, d[u]));
+                    m = fminf(m, d[u]);
+                }
+                if (m < scan.k1) {
+                    // the first row holding m, and its own value (m's sign
+                    // of zero may differ)
+                    uint32_t first = kArgminUnroll - 1;
+                    float value = d[kArgminUnroll - 1];
+#pragma unroll
+                    for (int u = kArgminUnroll - 2; u >= 0; --u) {
+                        const bool hit = d[u] == m;
+                        first = hit ? u : first;
+                        value = hit ? d[u] : value;
+                    }
+                    scan.k2 = fminf(scan.k1, s2);
+                    scan.k1 = value;
+                    scan.r1 = base + first * kFinalizeThreads;
+                } else {
+                    scan.k2 = fminf(scan.k2, m);
+                }
+            } else {
+#pragma unroll
+                for (int u = 0; u < kArgminUnroll; ++u) {
+                    scan_keyed_row(scan, d[u], base + u * kFinalizeThreads);
+                }
+            }
+            continue;
+        }
         float d[kArgminUnroll];
 #pragma unroll
         for (int u = 0; u < kArgminUnroll; ++u) {
@@ -780,7 +847,7 @@ __device__ __forceinline__ void scan_rows(const PartialView& view, const Bound& 
 // candidate row (D - err <= U*) in binary64, one warp per candidate, and keeps
 // the lexicographic minimum of (distance, row). exact_distances[q] is the
 // replayed distance, or NaN when the query was certified.
-template <bool kEmulated>
+template <bool kEmulated, bool kStepMerge = true>
 __device__ __forceinline__ void argmin_block(const PartialView& view, const Bound& bound,
                                              const ReplayInputs& in, Result* results,
                                              double* exact_distances,
@@ -803,9 +870,9 @@ __device__ __forceinline__ void argmin_block(const PartialView& view, const Boun
     // own bounds. Binary32 overflows enter as a lower bound of 0.
     RowScan scan;
     if (view.chunks == 1) {
-        scan_rows<true>(view, bound, q, first_row, end_row, scan, s);
+        scan_rows<true, kStepMerge>(view, bound, q, first_row, end_row, scan, s);
     } else {
-        scan_rows<false>(view, bound, q, first_row, end_row, scan, s);
+        scan_rows<false, kStepMerge>(view, bound, q, first_row, end_row, scan, s);
     }
     if (bound.mode != BoundMode::median && scan.r1 != 0xffffffffu) {
         const Bounds2 b1 = bound_of(scan.k1, bound, scan.r1, q);
@@ -2083,16 +2150,15 @@ __device__ __forceinline__ void persistent_count(const MedianArgs& a, uint32_t b
 
 // Unit u (of `units`) of one kind for one pair: one block of the stage kernel
 // the standalone path launches for it.
-// Units of the early stages (0-3: clear, gather, projection, tile scan,
-// median samples) when !kLate, of the late stages (4-7: median counts and
-// survivors, argmin, reported distances) when kLate; each kernel compiles
-// only its own kinds, so the late kernel's register budget is not the tile
-// scan's.
-template <bool kLate>
+// Units of kernel kPart's stages only (0: clear, gather, projection; 1: L2
+// error roots, tile scans, median samples; 2: median counts and survivors,
+// argmin, reported distances), so no kernel carries another's register
+// budget.
+template <int kPart>
 __device__ void persistent_unit(const PersistentPair& d, uint32_t kind, uint32_t u,
                                 uint32_t units, unsigned char* smem)
 {
-    if constexpr (!kLate) {
+    if constexpr (kPart == 0) {
     int* error_flag = reinterpret_cast<int*>(d.counters + 1);
     switch (kind) {
     case kUnitClear: {
@@ -2123,6 +2189,11 @@ __device__ void persistent_unit(const PersistentPair& d, uint32_t kind, uint32_t
             d.l2 != 0, error_flag, u % d.proj_gx, u / d.proj_gx,
             *reinterpret_cast<hierbody::ProjShared*>(smem));
         break;
+    default:
+        break;
+    }
+    } else if constexpr (kPart == 1) {
+    switch (kind) {
     case kUnitFinishErr:
         hierbody::finish_query_err_loop(d.query_err, d.batch, true, u, units, kFinalizeThreads);
         break;
@@ -2187,7 +2258,7 @@ __device__ void persistent_unit(const PersistentPair& d, uint32_t kind, uint32_t
         break;
     }
     case kUnitArgmin: {
-        argmin_block<false>(d.view, d.bound, d.replay, d.results, d.exact_distances,
+        argmin_block<false, false>(d.view, d.bound, d.replay, d.results, d.exact_distances,
                             static_cast<Summary*>(d.summaries), d.done, d.counters,
                             d.argmin_span, u % d.argmin_gx, u / d.argmin_gx, d.argmin_gx,
                             reinterpret_cast<double*>(smem));
@@ -2203,14 +2274,16 @@ __device__ void persistent_unit(const PersistentPair& d, uint32_t kind, uint32_t
     }
 }
 
-// The batch in two cooperative launches: the early stages [0, kPersistentSplit)
-// with the tile scan's register budget (2 CTAs per SM), then the late stages
-// [kPersistentSplit, kPersistentStages) at 4 CTAs per SM. Each CTA takes units
+// The batch in three cooperative launches: stages [0, kPersistentSplit0)
+// (clear, gather, projection) at 8 CTAs per SM, stage kPersistentSplit0 (tile
+// scans, median samples) with the tile scan's register budget (2 CTAs per
+// SM), then the late stages [kPersistentSplit, kPersistentStages) at 4 CTAs
+// per SM. Each CTA takes units
 // from its kernel's queue head until the queue is drained; before a unit it
 // waits for the unit's pair to have completed its units of earlier stages,
 // after it counts the unit complete for its pair and its stage (the stage
 // count also dates the stage's end). A wait that ran out, or a status set by
-// another CTA, ends the CTA; the last CTA of the late kernel to finish zeroes
+// another CTA, ends the CTA; the last CTA of the last kernel to finish zeroes
 // the queue for the next run.
 __device__ __forceinline__ unsigned long long global_timer_ns()
 {
@@ -2219,12 +2292,12 @@ __device__ __forceinline__ unsigned long long global_timer_ns()
     return t;
 }
 
-template <int kFirst, int kEnd, int kMinBlocks>
+template <int kPart, int kFirst, int kEnd, int kMinBlocks>
 __global__ void __launch_bounds__(kFinalizeThreads, kMinBlocks)
     persistent_stages_kernel(const __grid_constant__ PersistentParams params)
 {
     extern __shared__ __align__(16) unsigned char persistent_smem[];
-    constexpr bool kLate = kFirst >= kPersistentSplit;
+    constexpr bool kLast = kPart == kPersistentKernels - 1;
     __shared__ uint32_t next_unit;
     __shared__ int unit_ready;
     const PersistentPlan& plan = params.plan;
@@ -2243,7 +2316,7 @@ __global__ void __launch_bounds__(kFinalizeThreads, kMinBlocks)
             uint32_t item = end;
             if (*static_cast<volatile int*>(plan.status) == 0) {
                 item = plan.stage_first[kFirst] +
-                       atomicAdd(queue + kQueueHead + (kLate ? 1 : 0), 1u);
+                       atomicAdd(queue + kQueueHead + kPart, 1u);
             }
             next_unit = item;
         }
@@ -2271,7 +2344,7 @@ __global__ void __launch_bounds__(kFinalizeThreads, kMinBlocks)
         if (unit_ready == 0) {
             return;  // the wait ran out, or another CTA's did (status set)
         }
-        persistent_unit<kLate>(params.pairs[sg.pair], sg.kind, u - sg.first, sg.units,
+        persistent_unit<kPart>(params.pairs[sg.pair], sg.kind, u - sg.first, sg.units,
                                persistent_smem);
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -2283,11 +2356,11 @@ __global__ void __launch_bounds__(kFinalizeThreads, kMinBlocks)
             }
         }
     }
-    if constexpr (kLate) {
+    if constexpr (kLast) {
         if (threadIdx.x == 0) {
             __threadfence();
             if (atomicAdd(queue + kQueueFinished, 1u) == gridDim.x - 1) {
-                // every CTA of both kernels is past its last queue access
+                // every CTA of every kernel is past its last queue access
                 __threadfence();
                 for (uint32_t w = 0; w < kPersistentQueueWords; ++w) {
                     queue[w] = 0u;
@@ -2300,9 +2373,11 @@ __global__ void __launch_bounds__(kFinalizeThreads, kMinBlocks)
 // kernel parameters are limited to 32,764 bytes
 static_assert(sizeof(PersistentParams) <= 32764, "persistent batch parameters too large");
 
-constexpr auto persistent_early_kernel = persistent_stages_kernel<0, kPersistentSplit, 2>;
+constexpr auto persistent_gather_kernel = persistent_stages_kernel<0, 0, kPersistentSplit0, 8>;
+constexpr auto persistent_scan_kernel =
+    persistent_stages_kernel<1, kPersistentSplit0, kPersistentSplit, 2>;
 constexpr auto persistent_late_kernel =
-    persistent_stages_kernel<kPersistentSplit, kPersistentStages, 4>;
+    persistent_stages_kernel<2, kPersistentSplit, kPersistentStages, 4>;
 
 // Raises a kernel's dynamic shared-memory limit when a launch needs more than
 // the default allows: 48 KB less the kernel's static shared memory (read once
@@ -2728,7 +2803,7 @@ void plan_persistent_batch(const PersistentPair* pairs, uint32_t count,
                            PersistentPlan* plan)
 {
     uint32_t n = 0;
-    uint64_t smem_group[2] = {0, 0};
+    uint64_t smem_group[kPersistentKernels] = {};
     uint64_t smem = 0;
     auto add = [&](int stage, uint32_t pair, uint32_t kind, uint64_t units) {
         if (units == 0) {
@@ -2813,7 +2888,7 @@ void plan_persistent_batch(const PersistentPair* pairs, uint32_t count,
                 break;
             }
         }
-        uint64_t& group = smem_group[stage < kPersistentSplit ? 0 : 1];
+        uint64_t& group = smem_group[persistent_part_of(stage)];
         group = std::max(group, smem);
     }
     plan->stage_begin[kPersistentStages] = n;
@@ -2838,7 +2913,7 @@ void plan_persistent_batch(const PersistentPair* pairs, uint32_t count,
             }
         }
     }
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < kPersistentKernels; ++k) {
         plan->smem_bytes[k] = static_cast<uint32_t>((smem_group[k] + 15) / 16 * 16);
     }
     *segment_count = n;
@@ -2848,8 +2923,9 @@ namespace {
 
 const void* persistent_kernel(int part)
 {
-    return part == 0 ? reinterpret_cast<const void*>(persistent_early_kernel)
-                     : reinterpret_cast<const void*>(persistent_late_kernel);
+    return part == 0   ? reinterpret_cast<const void*>(persistent_gather_kernel)
+           : part == 1 ? reinterpret_cast<const void*>(persistent_scan_kernel)
+                       : reinterpret_cast<const void*>(persistent_late_kernel);
 }
 
 }  // namespace
@@ -2868,11 +2944,11 @@ uint32_t persistent_grid(int part, uint32_t smem_bytes)
     return static_cast<uint32_t>(std::max(0, per_sm) * sms);
 }
 
-void launch_persistent_batch(const PersistentParams& params, const uint32_t grid[2],
-                             cudaStream_t stream)
+void launch_persistent_batch(const PersistentParams& params,
+                             const uint32_t grid[kPersistentKernels], cudaStream_t stream)
 {
     const PersistentPlan& plan = params.plan;
-    for (int part = 0; part < 2; ++part) {
+    for (int part = 0; part < kPersistentKernels; ++part) {
         const void* kernel = persistent_kernel(part);
         set_dynamic_smem(kernel, plan.smem_bytes[part]);
         cudaLaunchConfig_t config{};
@@ -2881,8 +2957,8 @@ void launch_persistent_batch(const PersistentParams& params, const uint32_t grid
         config.dynamicSmemBytes = plan.smem_bytes[part];
         config.stream = stream;
         cudaLaunchAttribute attr[1];
-        // every CTA resident at once: the grid barrier never waits for a CTA
-        // that has not started
+        // every CTA resident at once: a unit never waits for one taken by a
+        // CTA that has not started
         attr[0].id = cudaLaunchAttributeCooperative;
         attr[0].val.cooperative = 1;
         config.attrs = attr;

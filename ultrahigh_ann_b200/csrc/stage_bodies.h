@@ -1,7 +1,7 @@
 // The persistent multi-index batch kernels (certify.cu, launch_persistent_batch)
 // and the shapes of the stage kernels they stand in for.
 //
-// Two kernels answer many (hierarchical index, query batch) pairs, one
+// Three kernels answer many (hierarchical index, query batch) pairs, one
 // cooperative launch each. A kernel's work is a device queue of units drawn
 // from all pairs (a unit is one block of the stage kernel that the standalone
 // path would launch for that pair, run by the same device code from
@@ -16,15 +16,16 @@
 //   1 gather of the sampled coordinates          5 median survivors (L1), argmin (L2)
 //   2 binary32 projection with its error bound   6 argmin (L1), reported distances (L2)
 //   3 L2 tile scan + error root, median samples  7 reported distances (L1)
-// Stages 0-3 run in the first kernel (the tile scan's register budget, 2 CTAs
-// per SM), stages 4-7 in the second (4 CTAs per SM).
+// Stages 0-2 run in a first kernel (8 CTAs per SM), stage 3 in a second (the
+// tile scan's register budget, 2 CTAs per SM), stages 4-7 in a third (4 CTAs
+// per SM).
 //
 // Progress: units leave the queue in order, and a unit waits only on units of
 // its own pair earlier in the queue, all of them already taken by CTAs that
 // are resident (cooperative launch); the earliest unfinished unit never
 // waits. A wait still gives up after about two seconds: it sets the batch
-// status and ends its CTA (the others stop taking units, and the second
-// kernel returns at once), so a fault can never hold the GPU.
+// status and ends its CTA (the others stop taking units, and the later
+// kernels return at once), so a fault can never hold the GPU.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -78,9 +79,18 @@ uint32_t refine_group_blocks(uint32_t batch);
 
 // ---- the persistent batch
 constexpr int kPersistentStages = 8;
-// stages [0, kPersistentSplit) run in the first kernel of a run, the rest in
-// the second
+// The kernels of a run: stages [0, kPersistentSplit0) (clear, gather,
+// projection: latency-bound, run at 8 CTAs per SM), [kPersistentSplit0,
+// kPersistentSplit) (tile scans and median samples, at the tile scan's
+// register budget, 2 CTAs per SM) and [kPersistentSplit, kPersistentStages)
+// (4 CTAs per SM).
+constexpr int kPersistentKernels = 3;
+constexpr int kPersistentSplit0 = 3;
 constexpr int kPersistentSplit = 4;
+constexpr int persistent_part_of(int stage)
+{
+    return stage < kPersistentSplit0 ? 0 : stage < kPersistentSplit ? 1 : 2;
+}
 
 // Everything one pair's stages read and write (device pointers into the
 // pair's workspace and index).
@@ -144,10 +154,10 @@ constexpr uint32_t kPersistentMaxPairs = 32;
 constexpr uint32_t kPersistentMaxSegments = 2 * kPersistentMaxPairs * kPersistentStages + 1;
 
 // Words of the work queue's device state (zero at creation; the last CTA of
-// the second kernel zeroes them again at the end of a run):
-constexpr uint32_t kQueueHead = 0;       // [0, 2): units taken, per kernel
-constexpr uint32_t kQueueFinished = 2;   // CTAs of the second kernel done
-constexpr uint32_t kQueueStageDone = 3;  // units completed, per stage
+// the last kernel zeroes them again at the end of a run):
+constexpr uint32_t kQueueHead = 0;  // [0, kPersistentKernels): units taken, per kernel
+constexpr uint32_t kQueueFinished = kPersistentKernels;  // CTAs of the last kernel done
+constexpr uint32_t kQueueStageDone = kQueueFinished + 1;  // units completed, per stage
 constexpr uint32_t kQueuePairDone = kQueueStageDone + kPersistentStages;  // per pair
 constexpr uint32_t kPersistentQueueWords = kQueuePairDone + kPersistentMaxPairs;
 
@@ -166,7 +176,7 @@ struct PersistentPlan {
     // first stage of a kernel its start as CTA 0 sees it, [s + 1] when the
     // last unit of stage s completed (untouched for a stage without units)
     unsigned long long* clock;
-    uint32_t smem_bytes[2];  // dynamic shared memory of the two kernels
+    uint32_t smem_bytes[kPersistentKernels];  // dynamic shared memory per kernel
 };
 
 // The kernels' one parameter (about 26 KB, read from the constant bank like
@@ -186,12 +196,12 @@ void plan_persistent_batch(const PersistentPair* pairs, uint32_t count,
                            PersistentSegment* segments, uint32_t* segment_count,
                            PersistentPlan* plan);
 uint32_t persistent_segment_capacity(uint32_t count);
-// CTAs of one cooperative launch of kernel `part` (0: early stages, 1: late
-// stages) on the current device for `smem_bytes` of dynamic shared memory
-// (all resident at once); 0 if it cannot be launched.
+// CTAs of one cooperative launch of kernel `part` (< kPersistentKernels) on
+// the current device for `smem_bytes` of dynamic shared memory (all resident
+// at once); 0 if it cannot be launched.
 uint32_t persistent_grid(int part, uint32_t smem_bytes);
-// The run's two cooperative launches (capturable in a graph).
-void launch_persistent_batch(const PersistentParams& params, const uint32_t grid[2],
-                             cudaStream_t stream);
+// The run's cooperative launches, one per kernel (capturable in a graph).
+void launch_persistent_batch(const PersistentParams& params,
+                             const uint32_t grid[kPersistentKernels], cudaStream_t stream);
 
 }  // namespace uha
