@@ -747,65 +747,85 @@ __device__ __forceinline__ void scan_keyed_row(RowScan& scan, float x, uint32_t 
     }
 }
 
+// One full step of kArgminUnroll keyed distances (rows base, base +
+// kFinalizeThreads, ...) into a thread's two smallest: when the distances are
+// finite (their sum is), the step's smallest m and second smallest s2 (with
+// multiplicity) by min / max and one merge, the row of m (its first
+// occurrence) looked up only when m is a new smallest; otherwise row by row.
+// Equal to scan_keyed_row applied to the rows in order.
+__device__ __forceinline__ void merge_step(RowScan& scan, const float* d, uint32_t base)
+{
+    float sum = d[0];
+#pragma unroll
+    for (int u = 1; u < kArgminUnroll; ++u) {
+        sum += d[u];
+    }
+    if (fabsf(sum) <= FLT_MAX) {
+        float m = d[0];
+        float s2 = __int_as_float(0x7f800000);
+#pragma unroll
+        for (int u = 1; u < kArgminUnroll; ++u) {
+            s2 = fminf(s2, fmaxf(m, d[u]));
+            m = fminf(m, d[u]);
+        }
+        if (m < scan.k1) {
+            // the first row holding m, and its own value (m's sign of zero
+            // may differ)
+            uint32_t first = kArgminUnroll - 1;
+            float value = d[kArgminUnroll - 1];
+#pragma unroll
+            for (int u = kArgminUnroll - 2; u >= 0; --u) {
+                const bool hit = d[u] == m;
+                first = hit ? u : first;
+                value = hit ? d[u] : value;
+            }
+            scan.k2 = fminf(scan.k1, s2);
+            scan.k1 = value;
+            scan.r1 = base + first * kFinalizeThreads;
+        } else {
+            scan.k2 = fminf(scan.k2, m);
+        }
+    } else {
+#pragma unroll
+        for (int u = 0; u < kArgminUnroll; ++u) {
+            scan_keyed_row(scan, d[u], base + u * kFinalizeThreads);
+        }
+    }
+}
+
 // kArgminUnroll rows per thread per step, their loads issued together (with
 // one partial slab the load is a single instruction the compiler can batch).
-// Keyed bounds take a full step at once when its distances are finite (their
-// sum is): the step's smallest m and second smallest s2 (with multiplicity)
-// by min / max, then one merge with the thread's two smallest; the row of m
-// (its first occurrence) is looked up only when m is a new smallest. The
-// result equals scan_keyed_row applied row by row. Other steps (the last,
-// partial one; inf or NaN distances), and every step when !kStepMerge (the
-// persistent kernel's register budget), go row by row.
+// Keyed bounds take full steps by merge_step, two steps' loads (16 rows) in
+// flight while two whole steps remain; the last, partial step, and every
+// step when !kStepMerge (the persistent kernel's register budget), go row by
+// row.
 template <bool kSingleChunk, bool kStepMerge>
 __device__ __forceinline__ void scan_rows(const PartialView& view, const Bound& bound,
                                           uint32_t q, uint32_t first_row, uint32_t end_row,
                                           RowScan& scan, Summary& s)
 {
     const bool keyed = bound.mode != BoundMode::median;
-    for (uint32_t base = first_row + threadIdx.x; base < end_row;
-         base += kFinalizeThreads * kArgminUnroll) {
+    uint32_t base = first_row + threadIdx.x;
+    if (kStepMerge && keyed) {
+        for (; base + (2 * kArgminUnroll - 1) * kFinalizeThreads < end_row;
+             base += 2 * kFinalizeThreads * kArgminUnroll) {
+            float d[2 * kArgminUnroll];
+#pragma unroll
+            for (int u = 0; u < 2 * kArgminUnroll; ++u) {
+                d[u] = load_distance<kSingleChunk>(view, q, base + u * kFinalizeThreads);
+            }
+            merge_step(scan, d, base);
+            merge_step(scan, d + kArgminUnroll, base + kArgminUnroll * kFinalizeThreads);
+        }
+    }
+    for (; base < end_row; base += kFinalizeThreads * kArgminUnroll) {
         if (kStepMerge && keyed && base + (kArgminUnroll - 1) * kFinalizeThreads < end_row) {
             float d[kArgminUnroll];
 #pragma unroll
             for (int u = 0; u < kArgminUnroll; ++u) {
                 d[u] = load_distance<kSingleChunk>(view, q, base + u * kFinalizeThreads);
             }
-            float sum = d[0];
-#pragma unroll
-            for (int u = 1; u < kArgminUnroll; ++u) {
-                sum += d[u];
-            }
-            if (fabsf(sum) <= FLT_MAX) {
-                float m = d[0];
-                float s2 = __int_as_float(0x7f800000);
-#pragma unroll
-                for (int u = 1; u < kArgminUnroll; ++u) {
-                    s2 = fminf(s2, fmaxf(m, d[u]));
-                    m = fminf(m, d[u]);
-                }
-                if (m < scan.k1) {
-                    // the first row holding m, and its own value (m's sign
-                    // of zero may differ)
-                    uint32_t first = kArgminUnroll - 1;
-                    float value = d[kArgminUnroll - 1];
-#pragma unroll
-                    for (int u = kArgminUnroll - 2; u >= 0; --u) {
-                        const bool hit = d[u] == m;
-                        first = hit ? u : first;
-                        value = hit ? d[u] : value;
-                    }
-                    scan.k2 = fminf(scan.k1, s2);
-                    scan.k1 = value;
-                    scan.r1 = base + first * kFinalizeThreads;
-                } else {
-                    scan.k2 = fminf(scan.k2, m);
-                }
-            } else {
-#pragma unroll
-                for (int u = 0; u < kArgminUnroll; ++u) {
-                    scan_keyed_row(scan, d[u], base + u * kFinalizeThreads);
-                }
-            }
+            merge_step(scan, d, base);
             continue;
         }
         float d[kArgminUnroll];
