@@ -793,18 +793,65 @@ __device__ __forceinline__ void merge_step(RowScan& scan, const float* d, uint32
     }
 }
 
+// One median-mode distance of a thread's scan: overflow sets the flag, a row
+// the median scan set aside (-T) joins the shared lower bound, a computed
+// median is inserted with its own bounds.
+__device__ __forceinline__ void scan_median_row(RowScan& scan, Summary& s, float x,
+                                                const Bound& bound, uint32_t row, uint32_t q)
+{
+    if (!(x <= FLT_MAX)) {
+        scan.overflow = true;
+    } else if (x < 0.f) {
+        scan.set_aside = fminf(scan.set_aside, -x);
+    } else {
+        const Bounds2 b = bound_of(x, bound, row, q);
+        summary_insert(s, b.lower, b.upper, row, x);
+    }
+}
+
+// One full step of kArgminUnroll median-mode distances: when all are rows set
+// aside (finite and negative: their sum finite, their maximum negative), one
+// minimum into the shared lower bound; otherwise row by row. Equal to
+// scan_median_row applied to the rows in order.
+__device__ __forceinline__ void merge_step_median(RowScan& scan, Summary& s, const float* d,
+                                                  const Bound& bound, uint32_t base, uint32_t q)
+{
+    float sum = d[0];
+    float mx = d[0];
+#pragma unroll
+    for (int u = 1; u < kArgminUnroll; ++u) {
+        sum += d[u];
+        mx = fmaxf(mx, d[u]);
+    }
+    if (fabsf(sum) <= FLT_MAX && mx < 0.f) {
+        scan.set_aside = fminf(scan.set_aside, -mx);
+    } else {
+#pragma unroll
+        for (int u = 0; u < kArgminUnroll; ++u) {
+            scan_median_row(scan, s, d[u], bound, base + u * kFinalizeThreads, q);
+        }
+    }
+}
+
 // kArgminUnroll rows per thread per step, their loads issued together (with
 // one partial slab the load is a single instruction the compiler can batch).
-// Keyed bounds take full steps by merge_step, two steps' loads (16 rows) in
-// flight while two whole steps remain; the last, partial step, and every
-// step when !kStepMerge (the persistent kernel's register budget), go row by
-// row.
+// Full steps go by merge_step (keyed bounds; two steps' loads, 16 rows, in
+// flight while two whole steps remain) or merge_step_median; the last,
+// partial step, and every step when !kStepMerge (the persistent kernel's
+// register budget), go row by row.
 template <bool kSingleChunk, bool kStepMerge>
 __device__ __forceinline__ void scan_rows(const PartialView& view, const Bound& bound,
                                           uint32_t q, uint32_t first_row, uint32_t end_row,
                                           RowScan& scan, Summary& s)
 {
     const bool keyed = bound.mode != BoundMode::median;
+    auto merge = [&](const float* d, uint32_t at) {
+        if (keyed) {
+            merge_step(scan, d, at);
+        } else {
+            merge_step_median(scan, s, d, bound, at, q);
+        }
+    };
     uint32_t base = first_row + threadIdx.x;
     if (kStepMerge && keyed) {
         for (; base + (2 * kArgminUnroll - 1) * kFinalizeThreads < end_row;
@@ -819,13 +866,13 @@ __device__ __forceinline__ void scan_rows(const PartialView& view, const Bound& 
         }
     }
     for (; base < end_row; base += kFinalizeThreads * kArgminUnroll) {
-        if (kStepMerge && keyed && base + (kArgminUnroll - 1) * kFinalizeThreads < end_row) {
+        if (kStepMerge && base + (kArgminUnroll - 1) * kFinalizeThreads < end_row) {
             float d[kArgminUnroll];
 #pragma unroll
             for (int u = 0; u < kArgminUnroll; ++u) {
                 d[u] = load_distance<kSingleChunk>(view, q, base + u * kFinalizeThreads);
             }
-            merge_step(scan, d, base);
+            merge(d, base);
             continue;
         }
         float d[kArgminUnroll];
